@@ -1,0 +1,217 @@
+/* ccdgpu — B200-native Coupled-Cluster-Doubles T2 iteration behind a C ABI.
+ *
+ * Drop-in for the CCD fixed-point loop that the reference driver runs in main.cpp:491-682:
+ * the four calc.cpp stages (calcT2Diff_p2_p1hh, calcT2Diff_h2pp_h1, calcT2Diff_phhp,
+ * calcT2Diff_pphh), the eight Chain::mapFromDistributed gathers, calcT2_pphh (denominator,
+ * mixing, energy) and the Chain::set + five Chain::mapToDistributed scatters.  The host keeps
+ * the basis, channel construction, V loaders and loadMaps; it hands their outputs to
+ * ccdgpu_create() through plain pointers, in the reference's own memory layouts:
+ *
+ *   ccdgpu_pair            == PQBundle              (SPBasis.hpp:32-44)
+ *   ccdgpu_triple          == PQRBundle             (SPBasis.hpp:46-63)
+ *   ccdgpu_channel_dims    == ChannelDims           (SPBasis.hpp:69-74)
+ *   ccdgpu_channel_maps    == ChannelMaps           (SPBasis.hpp:80-86)
+ *   ccdgpu_three_body_dims == ThreeBodyChannelDims  (SPBasis.hpp:88-91)
+ *   ccdgpu_chain_index     == ChainIndex            (Chain.hpp:7-11)
+ *   V and map blocks       == Chain<T>::get(channel) block pointers (Chain.hpp:108-120),
+ *                             dense row-major, NULL for empty blocks.
+ *
+ * Every entry point returns CCDGPU_OK (0) or a negative ccdgpu_status; none exits, traps or
+ * prints.  A handle owns one CUDA stream and its device memory; it is not thread-safe.
+ * All sizes are 64-bit.  T2 on the host is in the reference's t2_pphh data order: channel
+ * blocks in channel order, each pp x hh row-major, empty channels contributing nothing.
+ */
+#ifndef CCDGPU_H
+#define CCDGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ccdgpu_pair { uint64_t p, q; } ccdgpu_pair;
+typedef struct ccdgpu_triple { uint64_t p, q, r; } ccdgpu_triple;
+typedef struct ccdgpu_channel_dims { uint64_t pp, hh, hp, ph; } ccdgpu_channel_dims;
+typedef struct ccdgpu_channel_maps {
+  const ccdgpu_pair *pp, *hh, *hp, *ph;
+} ccdgpu_channel_maps;
+typedef struct ccdgpu_three_body_dims { uint64_t phh, hpp; } ccdgpu_three_body_dims;
+typedef struct ccdgpu_chain_index { uint64_t channel, row, column; } ccdgpu_chain_index;
+
+/* Order of the eight remap tables of loadMaps (load.cpp:391-398, main.cpp:236-243). */
+enum ccdgpu_map_id {
+  CCDGPU_MAP_IAB_J = 0, /* map_pphh_iab_j_hpp_h */
+  CCDGPU_MAP_JAB_I = 1, /* map_pphh_jab_i_hpp_h */
+  CCDGPU_MAP_A_BIJ = 2, /* map_pphh_a_bij_p_phh */
+  CCDGPU_MAP_B_AIJ = 3, /* map_pphh_b_aij_p_phh */
+  CCDGPU_MAP_AI_JB = 4, /* map_pphh_ai_jb_phhp  */
+  CCDGPU_MAP_AJ_IB = 5, /* map_pphh_aj_ib_phhp  */
+  CCDGPU_MAP_BI_JA = 6, /* map_pphh_bi_ja_phhp  */
+  CCDGPU_MAP_BJ_IA = 7  /* map_pphh_bj_ia_phhp  */
+};
+
+/* Interaction model, for generating V_pppp blocks on the device instead of uploading them
+ * (the reference's saveMemory mode regenerates blocks through SPBasis::calcTBME,
+ * calc.cpp:233-262, load.cpp:220-239). */
+enum ccdgpu_model_kind {
+  CCDGPU_MODEL_NONE = 0,
+  CCDGPU_MODEL_PAIRING = 1,       /* PairingSPBasis::calcTBME, PairingSPBasis.cpp:127-141 */
+  CCDGPU_MODEL_INF_MATTER = 2,    /* Minnesota, InfMatterSPBasis.cpp:361-437 */
+  CCDGPU_MODEL_ELECTRON_GAS = 3   /* Coulomb, ElectronGasSPBasis.cpp:424-471 */
+};
+typedef struct ccdgpu_model {
+  int32_t kind;                 /* ccdgpu_model_kind */
+  int32_t qn_stride;            /* ints per orbital in qn (5 for plane waves, 2 for pairing) */
+  const int32_t *qn;            /* [n_sp * qn_stride]: SPBasis::indexMap rows */
+  double params[8];             /* EG: {L, e_sq}; PNM: {L}; pairing: {g} */
+} ccdgpu_model;
+
+typedef struct ccdgpu_problem {
+  uint64_t n_sp;                /* SPBasis::nSpstates; orbitals < n_particles are holes */
+  uint64_t n_particles;         /* SPBasis::nParticles */
+  uint64_t n_channels;          /* SPBasis::nChannels (regular and modified channel slots) */
+  const double *sp_energy;      /* [n_sp] normal-ordered energies (after rotateSpEnergiesToNormalOrdered) */
+  const ccdgpu_channel_dims *chan_dims;        /* [n_channels] regular channels, permuted order */
+  const ccdgpu_channel_dims *chan_mod_dims;    /* [n_channels] modified (ph') channels */
+  const ccdgpu_channel_maps *chan_maps;        /* [n_channels] pp and hh maps are read */
+  const ccdgpu_channel_maps *chan_mod_maps;    /* [n_channels] ph and hp maps are read */
+  const ccdgpu_three_body_dims *three_body_dims; /* [n_sp] hpp for holes, phh for particles */
+  const double *const *v_hhhh;      /* [n_channels] hh x hh  (vnn_hhhh) */
+  const double *const *v_hhpp;      /* [n_channels] hh x pp  (vnn_hhpp) */
+  const double *const *v_pppp;      /* [n_channels] pp x pp  (vnn_pppp); may be NULL if model given */
+  const double *const *v_hpph_mod;  /* [n_channels] hp' x ph' (vnn_hhpp_hpph_mod) */
+  const double *const *v_hphp_mod;  /* [n_channels] hp' x hp' (vnn_hpph_hphp_mod) */
+  const double *const *v_h_hpp;     /* [n_particles] 1 x hpp  (vnn_h_hpp); NULL allowed (fused path) */
+  const double *const *v_phh_p;     /* [n_sp - n_particles] phh x 1 (vnn_phh_p); NULL allowed */
+  const ccdgpu_chain_index *const *maps[8]; /* [n_channels] pp x hh blocks, ccdgpu_map_id order */
+  const ccdgpu_model *model;        /* optional, required for CCDGPU_V_ON_THE_FLY */
+} ccdgpu_problem;
+
+enum ccdgpu_status {
+  CCDGPU_OK = 0,
+  CCDGPU_ERR_INVALID_ARGUMENT = -1,
+  CCDGPU_ERR_CUDA = -2,
+  CCDGPU_ERR_OUT_OF_MEMORY = -3,
+  CCDGPU_ERR_BAD_TABLE = -4,       /* a remap table entry is out of range or not a bijection */
+  CCDGPU_ERR_NONFINITE = -5,       /* NaN/Inf in the amplitudes or the energy */
+  CCDGPU_ERR_NO_DEVICE = -6,
+  CCDGPU_ERR_UNSUPPORTED = -7,
+  CCDGPU_ERR_NOT_CONVERGED = -8,   /* only from ccdgpu_solve when require_convergence is set */
+  CCDGPU_ERR_TIMEOUT = -9          /* wall-clock limit of ccdgpu_solve reached */
+};
+
+enum ccdgpu_precision {
+  CCDGPU_PREC_FP64 = 0,        /* FP64 throughout (DMMA contractions) */
+  CCDGPU_PREC_MIXED_BF16 = 1   /* split-BF16 contractions, FP32 accumulate, FP64 polish */
+};
+enum ccdgpu_v_mode {
+  CCDGPU_V_STORED = 0,         /* V_pppp uploaded from the host blocks */
+  CCDGPU_V_ON_THE_FLY = 1      /* V_pppp regenerated inside the pp-ladder kernel from the model */
+};
+enum ccdgpu_path {
+  CCDGPU_PATH_FUSED = 0,       /* fused kernels: one-body terms from the ladder intermediates,
+                                  remaps folded into the assembly kernel */
+  CCDGPU_PATH_TABLES = 1       /* stage by stage exactly as main.cpp:591-665: 8 gathers and
+                                  5 scatters through the loadMaps tables */
+};
+
+typedef struct ccdgpu_options {
+  int32_t device;              /* CUDA device ordinal */
+  int32_t precision;           /* ccdgpu_precision */
+  int32_t v_mode;              /* ccdgpu_v_mode */
+  int32_t path;                /* ccdgpu_path */
+  double polish_threshold;     /* mixed: switch to FP64 once |dE| falls below this */
+  int32_t use_graph;           /* capture one iteration as a CUDA graph (fused path) */
+  int32_t reserved[7];
+} ccdgpu_options;
+
+typedef struct ccdgpu_result {
+  double e_corr;               /* correlation energy after the last iteration (corrCCD) */
+  double e_diff;               /* last energy change (energyDiff) */
+  int64_t iterations;          /* iterations performed, counted as main.cpp:681 does */
+  int32_t converged;           /* 1 when |e_diff| <= tolerance, 0 when the cap was hit */
+  int32_t polish_iterations;   /* mixed precision: iterations run in FP64 polish */
+  double seconds;              /* wall time of the loop (cc_diagrams_time counterpart) */
+} ccdgpu_result;
+
+typedef struct ccdgpu_handle ccdgpu_handle;
+
+/* Defaults: device 0, FP64, stored V, fused path, graph capture on, polish 1e-9. */
+void ccdgpu_default_options(ccdgpu_options *opt);
+
+/* Deep-copies the problem to the device and validates every remap table (range and
+ * bijection).  Replaces main.cpp:222-455 allocation/loading as far as the device is
+ * concerned; the host data may be freed afterwards.  T2 starts at zero (main.cpp:497-503). */
+int ccdgpu_create(const ccdgpu_problem *prob, const ccdgpu_options *opt, ccdgpu_handle **out);
+void ccdgpu_destroy(ccdgpu_handle *h);
+const char *ccdgpu_strerror(int status);
+
+/* Zero every amplitude chain (main.cpp:497-503). */
+int ccdgpu_reset(ccdgpu_handle *h);
+/* Load / read T2 in t2_pphh order (n = sum of pp*hh).  Loading also refreshes t2Old and
+ * the scattered layouts, as main.cpp:660-665 would after an iteration. */
+int ccdgpu_set_t2(ccdgpu_handle *h, const double *t2_pphh, uint64_t n);
+int ccdgpu_get_t2(ccdgpu_handle *h, double *t2_pphh, uint64_t n);
+uint64_t ccdgpu_t2_size(const ccdgpu_handle *h);
+
+/* One CCD iteration (main.cpp:589-670) with the path and precision chosen at create time.
+ * Writes the new correlation energy (corrCCD) to *e_corr. */
+int ccdgpu_step(ccdgpu_handle *h, double mixing, double *e_corr);
+
+/* Iterate from the current T2 until |E - E_prev| <= tol or iterations exceed max_iters,
+ * with E_prev starting at 100 (main.cpp:491-519).  max_iters = 100 reproduces the
+ * reference's cap (at most 101 iterations). */
+int ccdgpu_solve(ccdgpu_handle *h, double tol, int64_t max_iters, double mixing,
+                 ccdgpu_result *res);
+
+/* Stage entry points with the reference's names, for stage-level parity tests and for a
+ * host that keeps the reference loop structure.  They act on the handle's device chains. */
+int ccdgpu_calc_t2diff_p2_p1hh(ccdgpu_handle *h);   /* calc.cpp:27-43 */
+int ccdgpu_calc_t2diff_h2pp_h1(ccdgpu_handle *h);   /* calc.cpp:91-107 */
+int ccdgpu_calc_t2diff_phhp(ccdgpu_handle *h);      /* calc.cpp:315-339 */
+int ccdgpu_calc_t2diff_pphh(ccdgpu_handle *h);      /* calc.cpp:205-231 */
+int ccdgpu_map_from_distributed(ccdgpu_handle *h);  /* the 8 gathers, main.cpp:632-639 */
+int ccdgpu_calc_t2_pphh(ccdgpu_handle *h, double mixing, double *corr); /* calc.cpp:423-459 */
+int ccdgpu_map_to_distributed(ccdgpu_handle *h);    /* Chain::set + 5 scatters, main.cpp:660-665 */
+
+/* Chain identifiers for ccdgpu_read_chain (device intermediates, copied to the host). */
+enum ccdgpu_chain_id {
+  CCDGPU_CHAIN_T2 = 0,          /* t2_pphh          (pp x hh) */
+  CCDGPU_CHAIN_T2_OLD = 1,      /* t2Old_pphh       (pp x hh) */
+  CCDGPU_CHAIN_DIFF_PPHH = 2,   /* t2Diff_pphh      (pp x hh) */
+  CCDGPU_CHAIN_DIFF_PHHP = 3,   /* t2Diff_phhp      (ph' x hp') */
+  CCDGPU_CHAIN_OLD_PHHP = 4,    /* t2Old_phhp       (ph' x hp') */
+  CCDGPU_CHAIN_DIFF_H2PP_H1 = 5,/* t2Diff_h2pp_h1   (hpp x 1, per hole) */
+  CCDGPU_CHAIN_DIFF_P2_P1HH = 6,/* t2Diff_p2_p1hh   (1 x phh, per particle) */
+  CCDGPU_CHAIN_GATHERED0 = 8    /* + k: the k-th gathered pphh chain, ccdgpu_map_id order */
+};
+/* Copies a device chain into out (n doubles); returns its length through *n_out when out is
+ * NULL. */
+int ccdgpu_read_chain(ccdgpu_handle *h, int32_t chain, double *out, uint64_t n, uint64_t *n_out);
+
+/* Device timing of the last ccdgpu_solve / ccdgpu_step, per kernel family, in
+ * milliseconds summed over the iterations, and launch counts. */
+typedef struct ccdgpu_profile {
+  double ms_ladder;      /* pp/hh ladder GEMMs (calc.cpp:132-203) */
+  double ms_ring;        /* ring GEMMs (calc.cpp:264-313) */
+  double ms_onebody;     /* one-body terms (calc.cpp:9-25, 73-89) */
+  double ms_assemble;    /* assembly / remaps / energy (calc.cpp:368-421, Chain.hpp:710-802) */
+  double ms_total;
+  int64_t launches;      /* kernels launched by this library */
+  int64_t iterations;
+} ccdgpu_profile;
+int ccdgpu_get_profile(ccdgpu_handle *h, ccdgpu_profile *prof);
+int ccdgpu_enable_profiling(ccdgpu_handle *h, int32_t on);
+
+/* Algorithmic work of one iteration for roofline reporting: reference GEMM flops
+ * (sum over channels of 2 pp^2 hh + 4 pp hh^2 + 4 ph' hp'^2) and V_pppp bytes. */
+int ccdgpu_work_per_iteration(const ccdgpu_handle *h, double *flops, double *v_pppp_bytes,
+                              double *ladder_flops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CCDGPU_H */
