@@ -69,9 +69,9 @@ class Result(ctypes.Structure):
 
 
 class Profile(ctypes.Structure):
-    _fields_ = [("ms_ladder", c_dbl), ("ms_ring", c_dbl), ("ms_onebody", c_dbl),
-                ("ms_assemble", c_dbl), ("ms_total", c_dbl), ("launches", c_i64),
-                ("iterations", c_i64)]
+    _fields_ = [("ms_ladder", c_dbl), ("ms_hh_ladder", c_dbl), ("ms_ring", c_dbl),
+                ("ms_onebody", c_dbl), ("ms_assemble", c_dbl), ("ms_total", c_dbl),
+                ("launches", c_i64), ("iterations", c_i64)]
 
 
 _host = None
@@ -113,6 +113,7 @@ GPU_SYMBOLS = [
     "ccdgpu_calc_t2diff_phhp", "ccdgpu_calc_t2diff_pphh", "ccdgpu_map_from_distributed",
     "ccdgpu_calc_t2_pphh", "ccdgpu_map_to_distributed", "ccdgpu_read_chain",
     "ccdgpu_get_profile", "ccdgpu_enable_profiling", "ccdgpu_work_per_iteration",
+    "ccdgpu_energy_history", "ccdgpu_stream",
 ]
 
 
@@ -148,5 +149,8 @@ def gpu_lib():
         lib.ccdgpu_get_profile.argtypes = [vp, P(Profile)]
         lib.ccdgpu_enable_profiling.argtypes = [vp, c_i32]
         lib.ccdgpu_work_per_iteration.argtypes = [vp, P(c_dbl), P(c_dbl), P(c_dbl)]
+        lib.ccdgpu_energy_history.argtypes = [vp, P(c_dbl), c_i64, P(c_i64)]
+        lib.ccdgpu_stream.argtypes = [vp]
+        lib.ccdgpu_stream.restype = vp
         _gpu = lib
     return _gpu

@@ -166,6 +166,10 @@ int ccdgpu_step(ccdgpu_handle *h, double mixing, double *e_corr);
 int ccdgpu_solve(ccdgpu_handle *h, double tol, int64_t max_iters, double mixing,
                  ccdgpu_result *res);
 
+/* corrCCD after each iteration of the last ccdgpu_solve (first 128 iterations); *n_out gets
+ * the number of iterations stored.  The per-iteration printout of main.cpp:672-680. */
+int ccdgpu_energy_history(ccdgpu_handle *h, double *out, int64_t cap, int64_t *n_out);
+
 /* Stage entry points with the reference's names, for stage-level parity tests and for a
  * host that keeps the reference loop structure.  They act on the handle's device chains. */
 int ccdgpu_calc_t2diff_p2_p1hh(ccdgpu_handle *h);   /* calc.cpp:27-43 */
@@ -194,16 +198,21 @@ int ccdgpu_read_chain(ccdgpu_handle *h, int32_t chain, double *out, uint64_t n, 
 /* Device timing of the last ccdgpu_solve / ccdgpu_step, per kernel family, in
  * milliseconds summed over the iterations, and launch counts. */
 typedef struct ccdgpu_profile {
-  double ms_ladder;      /* pp/hh ladder GEMMs (calc.cpp:132-203) */
-  double ms_ring;        /* ring GEMMs (calc.cpp:264-313) */
+  double ms_ladder;      /* pp ladder + T X GEMM (calc.cpp:162-202) */
+  double ms_hh_ladder;   /* hh ladder intermediate X (calc.cpp:141-160) */
+  double ms_ring;        /* ring GEMMs (calc.cpp:264-313), on the second stream */
   double ms_onebody;     /* one-body terms (calc.cpp:9-25, 73-89) */
-  double ms_assemble;    /* assembly / remaps / energy (calc.cpp:368-421, Chain.hpp:710-802) */
-  double ms_total;
-  int64_t launches;      /* kernels launched by this library */
-  int64_t iterations;
+  double ms_assemble;    /* assembly + remaps + energy (calc.cpp:368-421, Chain.hpp:710-802) */
+  double ms_total;       /* whole iterations */
+  int64_t launches;      /* kernels launched by this library since create */
+  int64_t iterations;    /* iterations covered by the ms_* sums */
 } ccdgpu_profile;
 int ccdgpu_get_profile(ccdgpu_handle *h, ccdgpu_profile *prof);
+/* When on, ccdgpu_solve runs the fused iteration without graph capture and brackets each
+ * kernel family with CUDA events on the handle's streams (one host sync per iteration). */
 int ccdgpu_enable_profiling(ccdgpu_handle *h, int32_t on);
+/* The handle's main CUDA stream (cudaStream_t), for callers that time or order work on it. */
+void *ccdgpu_stream(ccdgpu_handle *h);
 
 /* Algorithmic work of one iteration for roofline reporting: reference GEMM flops
  * (sum over channels of 2 pp^2 hh + 4 pp hh^2 + 4 ph' hp'^2) and V_pppp bytes. */

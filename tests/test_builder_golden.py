@@ -1,0 +1,55 @@
+"""The host problem builder reproduces the reference's inputs bit for bit.
+
+Compares, per golden configuration, the builder's orbital energies, channel dimensions,
+channel / three-body maps, the 8 loadMaps remap tables (load.cpp:389-532) and every V chain
+(load.cpp:112-318) with FNV-1a hashes of the reference's own dumps, and E_ref / E_MBPT2 for
+exact equality.
+"""
+import pytest
+
+from helpers import MAPS, SMALL, STRUCT, VKINDS, golden, system_for
+from oracle.oracle import fnv1a
+
+
+@pytest.mark.parametrize("name", SMALL + ["eg54_s19"])
+def test_builder_matches_reference(name):
+    g = golden(name)
+    with system_for(g) as s:
+        assert s.n_sp == int(g["header"][0])
+        assert s.n_particles == int(g["header"][1])
+        assert s.n_channels == int(g["header"][2])
+        assert s.reference_energy == float(g["scalars"][0])
+        assert s.mbpt2 == float(g["scalars"][1])
+        for k, n in enumerate(STRUCT):
+            assert fnv1a(s.array(n)) == int(g["struct_hashes"][k]), n
+        for k, n in enumerate(MAPS):
+            assert fnv1a(s.array(n)) == int(g["map_hashes"][k]), n
+        for k, n in enumerate(VKINDS):
+            assert fnv1a(s.array(n)) == int(g["v_hashes"][k]), n
+
+
+def test_builder_without_v_pppp_keeps_everything_else():
+    g = golden("eg14_s19")
+    with system_for(g, load_v_pppp=False) as s:
+        assert s.array("v_pppp").size == 0
+        assert not s.problem.contents.v_pppp
+        for k, n in enumerate(MAPS):
+            assert fnv1a(s.array(n)) == int(g["map_hashes"][k]), n
+
+
+@pytest.mark.parametrize("args", [dict(xi=1.0, g=0.5, n_pair_states=4, n_particles=8),
+                                  dict(xi=1.0, g=0.5, n_pair_states=0, n_particles=0)])
+def test_builder_rejects_bad_pairing_input(args):
+    from coupled_cluster_doubles_b200 import System
+    from coupled_cluster_doubles_b200.system import BuildError
+    with pytest.raises(BuildError):
+        System.pairing(**args)
+
+
+def test_builder_rejects_bad_plane_wave_input():
+    from coupled_cluster_doubles_b200 import System
+    from coupled_cluster_doubles_b200.system import BuildError
+    with pytest.raises(BuildError):
+        System.electron_gas(r_s=1.0, n_shells=2, n_particle_shells=4)
+    with pytest.raises(BuildError):
+        System.inf_matter(density=0.08, tz_max=3, n_shells=4, n_particle_shells=2)

@@ -1,0 +1,167 @@
+"""GPU parity: the CUDA path through the C ABI against the reference's goldens and the oracle.
+
+Tolerances (FP64 path): correlation energy per particle within 1e-10 relative of the
+reference, T2 within 1e-9 max-abs; stage intermediates within 1e-12 of the oracle relative to
+the chain's largest element.
+"""
+import numpy as np
+import pytest
+
+from coupled_cluster_doubles_b200 import CCDGPUError, CCDSolver, solver as solver_mod
+from helpers import SMALL, golden, system_for, t2_sample
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+E_RTOL = 1e-10
+T2_ATOL = 1e-9
+
+
+def check_against_golden(g, sol, res):
+    ref = g["energies"]
+    hist = sol.energy_history()
+    # The stop decision compares |dE| with tol; rounding differences of ~1e-16 may move it by
+    # at most one iteration when the last |dE| sits right at tol.
+    assert abs(res.iterations - len(ref)) <= 1
+    m = min(len(hist), len(ref))
+    np.testing.assert_allclose(hist[:m], ref[:m], rtol=E_RTOL, atol=1e-14)
+    assert abs(res.e_corr - ref[-1]) <= E_RTOL * abs(ref[-1]) + 1e-14
+    t2 = sol.t2()
+    assert np.max(np.abs(t2_sample(g, t2) - g["t2"])) < T2_ATOL
+    np.testing.assert_allclose(float(np.dot(t2, t2)), float(g["t2_sumsq"][0]), rtol=1e-8)
+
+
+@pytest.mark.parametrize("path", ["fused", "tables"])
+@pytest.mark.parametrize("name", SMALL + ["eg54_s19"])
+def test_solve_matches_reference(name, path):
+    g = golden(name)
+    with system_for(g) as s, CCDSolver(s, path=path) as sol:
+        res = sol.solve(tol=g["tol"], max_iters=100, mixing=0.5)
+        check_against_golden(g, sol, res)
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_fused_graph_and_stream_paths_agree(use_graph):
+    g = golden("eg14_s19")
+    with system_for(g) as s, CCDSolver(s, use_graph=use_graph) as sol:
+        res = sol.solve(tol=g["tol"])
+        check_against_golden(g, sol, res)
+        # a second solve from the converged amplitudes stops after one or two iterations
+        sol2 = sol.solve(tol=1e-6)
+        assert sol2.iterations <= 2
+
+
+def test_iteration_cap_matches_reference():
+    g = golden("pairing_gp1.0")
+    with system_for(g) as s, CCDSolver(s) as sol:
+        res = sol.solve(tol=1e-12, max_iters=100)
+        assert res.iterations == 101 and not res.converged
+        sol.reset()
+        res = sol.solve(tol=1e-12, max_iters=5)
+        assert res.iterations == 6
+
+
+@pytest.mark.parametrize("path", ["fused", "tables"])
+def test_steps_match_oracle(path):
+    g = golden("pnm14_s4")
+    with system_for(g) as s, CCDSolver(s, path=path) as sol:
+        o = Oracle(s)
+        for _ in range(4):
+            e_ref = o.step(0.5)
+            e = sol.step(0.5)
+            assert abs(e - e_ref) <= 1e-12 * abs(e_ref)
+        np.testing.assert_allclose(sol.t2(), o.t2(), rtol=0, atol=1e-13)
+        o.close()
+
+
+def _close(a, b, rel=1e-12):
+    scale = max(float(np.max(np.abs(b))) if b.size else 0.0, 1e-300)
+    assert np.max(np.abs(a - b)) <= rel * scale + 1e-300, (np.max(np.abs(a - b)), scale)
+
+
+@pytest.mark.parametrize("name", ["pnm14_s4", "eg14_s19", "pairing_gm0.5"])
+def test_stage_by_stage_against_oracle(name):
+    """Every calc.cpp stage and every remap, from the same non-trivial T2."""
+    g = golden(name)
+    with system_for(g) as s:
+        o = Oracle(s)
+        for _ in range(3):
+            o.step(0.5)
+        t2 = o.t2()
+        o.set_t2(t2)
+        with CCDSolver(s, path="tables") as sol:
+            sol.set_t2(t2)
+            _close(sol.chain(solver_mod.CHAIN_OLD_PHHP), o.chain(solver_mod.CHAIN_OLD_PHHP), 0)
+            o.calc_t2diff_p2_p1hh(); sol.calc_t2diff_p2_p1hh()
+            _close(sol.chain(solver_mod.CHAIN_DIFF_P2_P1HH), o.chain(solver_mod.CHAIN_DIFF_P2_P1HH))
+            o.calc_t2diff_h2pp_h1(); sol.calc_t2diff_h2pp_h1()
+            _close(sol.chain(solver_mod.CHAIN_DIFF_H2PP_H1), o.chain(solver_mod.CHAIN_DIFF_H2PP_H1))
+            o.calc_t2diff_phhp(); sol.calc_t2diff_phhp()
+            _close(sol.chain(solver_mod.CHAIN_DIFF_PHHP), o.chain(solver_mod.CHAIN_DIFF_PHHP))
+            o.calc_t2diff_pphh(); sol.calc_t2diff_pphh()
+            _close(sol.chain(solver_mod.CHAIN_DIFF_PPHH), o.chain(solver_mod.CHAIN_DIFF_PPHH))
+            o.map_from_distributed(); sol.map_from_distributed()
+            for k in range(8):
+                _close(sol.chain(solver_mod.CHAIN_GATHERED0 + k), o.chain(solver_mod.CHAIN_GATHERED0 + k))
+            e_ref = o.calc_t2_pphh(0.5)
+            e = sol.calc_t2_pphh(0.5)
+            assert abs(e - e_ref) <= 1e-12 * abs(e_ref)
+            _close(sol.chain(solver_mod.CHAIN_T2), o.chain(solver_mod.CHAIN_T2))
+            o.map_to_distributed(); sol.map_to_distributed()
+            _close(sol.chain(solver_mod.CHAIN_T2_OLD), o.chain(solver_mod.CHAIN_T2_OLD))
+            _close(sol.chain(solver_mod.CHAIN_OLD_PHHP), o.chain(solver_mod.CHAIN_OLD_PHHP))
+        o.close()
+
+
+def test_set_get_roundtrip_and_reset():
+    g = golden("eg14_s19")
+    with system_for(g) as s, CCDSolver(s) as sol:
+        x = np.random.default_rng(7).standard_normal(sol.n_t2) * 1e-3
+        sol.set_t2(x)
+        np.testing.assert_array_equal(sol.t2(), x)
+        sol.reset()
+        assert not np.any(sol.t2())
+
+
+def test_fused_path_keeps_antisymmetry():
+    """Size-independent property at the largest golden size: t_ab,ij = -t_ab,ji = -t_ba,ij."""
+    g = golden("eg54_s19")
+    with system_for(g) as s, CCDSolver(s) as sol:
+        sol.solve(tol=g["tol"])
+        t2 = sol.t2()
+        d = s.chan_dims()
+        pp_map = s.array("pp_map").reshape(-1, 2)
+        hh_map = s.array("hh_map").reshape(-1, 2)
+        off = po = ho = 0
+        worst = 0.0
+        for c in range(s.n_channels):
+            pp, hh = int(d[c, 0]), int(d[c, 1])
+            if pp and hh:
+                blk = t2[off:off + pp * hh].reshape(pp, hh)
+                P = {tuple(x): k for k, x in enumerate(pp_map[po:po + pp].tolist())}
+                H = {tuple(x): k for k, x in enumerate(hh_map[ho:ho + hh].tolist())}
+                sp = [P[(b, a)] for a, b in pp_map[po:po + pp].tolist()]
+                sh = [H[(j, i)] for i, j in hh_map[ho:ho + hh].tolist()]
+                worst = max(worst, np.max(np.abs(blk + blk[:, sh])), np.max(np.abs(blk + blk[sp, :])))
+            off += pp * hh
+            po += pp
+            ho += hh
+        assert worst < 1e-13
+
+
+def test_bad_table_is_rejected_before_any_launch():
+    """A remap entry that points outside its target chain is caught by create's validation."""
+    g = golden("pnm14_s4")
+    with system_for(g) as s:
+        p = s.problem.contents
+        d = s.chan_dims()
+        c = int(np.nonzero((d[:, 0] > 0) & (d[:, 1] > 0))[0][0])
+        entry = p.maps[4][c][0]
+        saved = entry.row
+        entry.row = 10 ** 9
+        with pytest.raises(CCDGPUError) as ei:
+            CCDSolver(s)
+        assert ei.value.status == -4
+        entry.row = saved
+        with CCDSolver(s) as sol:
+            assert sol.n_t2 == s.t2_size()
