@@ -6,41 +6,63 @@
 
 namespace ccd {
 
-// pp-ladder / hh-ladder tiling.  Operand tiles are stored in HBM already in their shared-memory
-// image: [rows][kBK] doubles, column index XOR-swizzled by (row & 3) << 2 so that the FP64
-// mma.m16n8k4 fragment loads (4 rows x 4 k per half-warp) hit 16 distinct 8-byte bank pairs.
-constexpr int kBM = 64;        // rows of D per work tile (4 consumer warps x 16 rows)
+// pp-ladder tiling.  V_pppp is antisymmetric in both pair indices (calcTBME is
+// f(p,q,r,s) - f(p,q,s,r)), so D[ab,ij] = 1/2 sum_cd V[ab,cd] T[cd,ij] is evaluated as
+// sum_{c<d} V[ab,cd] T[cd,ij] over rows a<=b and mirrored to the b>a rows with a sign flip:
+// one quarter of the V bytes and flops of the full product.
+//
+// Operand tiles are stored in HBM already in their shared-memory image so that one bulk copy
+// (TMA) moves a whole stage:
+//   A tiles  [bm rows][kBK]   row-major, column XOR-swizzled by (row & 15): a warp reading
+//                              16 consecutive rows at one k hits 16 distinct bank pairs;
+//   B tiles  [kBK][nb]        k-major (nb = 8 * cg padded hh columns), read as broadcasts.
 constexpr int kBK = 16;        // K depth of one pipeline stage
-constexpr int kStages = 6;     // bulk-copy pipeline depth
-constexpr int kMaxFrag = 9;    // up to 72 hh columns (8 per n-fragment)
-constexpr int kLadderThreads = 160;  // 4 consumer warps + 1 producer warp
+constexpr int kStages = 4;     // bulk-copy pipeline depth
+constexpr int kMaxCG = 9;      // column groups of 8 -> up to 72 hh columns
+constexpr int kNarrowCG = 4;   // channels up to 32 hh columns use the narrow instantiation
+constexpr int kLadderConsumers = 128;
+constexpr int kLadderThreads = kLadderConsumers + 32;  // + 1 producer warp
+constexpr int kMaxBM = 128;
 
-__host__ __device__ inline int swz(int row, int k) { return row * kBK + (k ^ ((row & 3) << 2)); }
+__host__ __device__ inline int swzA(int row, int k) { return row * kBK + (k ^ (row & 15)); }
+// Rows per tile for a channel with cg column groups: each consumer thread owns cg rows
+// (strided by the number of row groups) and 8 columns.
+__host__ __device__ inline int ladder_bm(int cg) { return (kLadderConsumers / cg) * cg; }
 
-// One pp-ladder work tile: rows [mt*kBM, mt*kBM+kBM) of channel `ch`'s D block.
+// One pp-ladder work tile: packed rows [mt*bm, mt*bm+bm) of channel `ch`.
 struct LadderTile {
   int32_t ch;        // active-channel index
   int32_t mt;        // row tile
-  int32_t nkc;       // K chunks over pp (V_pppp x T part)
-  int32_t nkh;       // K chunks over hh (T x X part)
-  int32_t nfrag;     // n-fragments of 8 columns (ceil(hh/8))
-  int32_t pp, hh;
-  int32_t pad;
-  int64_t v_base;    // V_pppp tiles: + (mt*nkc + kc) * kBM*kBK
-  int64_t tkt_base;  // T^T tiles (B operand of V T): + kc * (8*nfrag)*kBK
-  int64_t tmt_base;  // T row tiles (A operand of T X): + (mt*nkh + kh) * kBM*kBK
-  int64_t xt_base;   // X^T tiles (B operand of T X): + kh * (8*nfrag)*kBK
+  int32_t nkc;       // K chunks over the c<d pairs (V T part)
+  int32_t nkh;       // K chunks over hh (T X part)
+  int32_t cg;        // column groups (ceil(hh/8))
+  int32_t bm;        // rows per tile
+  int32_t pr;        // packed rows (a<=b) of the channel
+  int32_t hh;
+  int64_t v_base;    // A tiles of V:  + (mt*nkc + kc) * bm*kBK
+  int64_t tkt_base;  // B tiles of T:  + kc * kBK*nb
+  int64_t tmt_base;  // A tiles of T (rows a<=b, K = hh): + (mt*nkh + kh) * bm*kBK
+  int64_t xt_base;   // B tiles of X/2: + kh * kBK*nb
   int64_t t_off;     // offset of the channel's pp x hh block in the t2 layout
+  int64_t row_off;   // offset into rowmap / mirror
 };
 
 // Per active regular channel.
 struct ChanInfo {
-  int32_t pp, hh, nfrag, nkc, nkh, nmt;
+  int32_t pp, hh, cg, nkc, nkh, nmt, bm, pr, pk, nhht;
   int64_t t_off;     // pphh block offset (reference t2 layout)
-  int64_t pp_off;    // offset into pp_pairs / pp_swap / r
+  int64_t pp_off;    // offset into pp_pairs / pp_swap / pk_idx / r
   int64_t hh_off;    // offset into hh_pairs / hh_swap / s
   int64_t x_off;     // hh x hh block offset (V_hhhh and X)
   int64_t tkt_base, tmt_base, xt_base, vkt_base;
+  int64_t row_off;   // offset into rowmap / mirror (pr entries)
+  int64_t part_off;  // hh-ladder partial products: nhht * hh*hh doubles
+  int64_t hht0;      // first hh-ladder tile of the channel
+};
+
+// hh-ladder split-K tile: rows [k0, k0+kHHRows) of channel ch.
+struct HHTile {
+  int32_t ch, k0, idx, pad;  // idx = tile index within the channel
 };
 
 // Per active modified channel.

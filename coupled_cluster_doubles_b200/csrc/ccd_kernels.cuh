@@ -2,8 +2,9 @@
 //
 // Reference correspondence (calc.cpp / Chain.hpp of justinlietz/coupled_cluster_doubles):
 //   pp_ladder_kernel        D = 0.5 T X + 0.5 V_pppp T              calc.cpp:162-202
+//                           (antisymmetry-packed, FP64 FMA pipe)
 //   hh_ladder_kernel        X = V_hhhh + 0.5 V_hhpp T                calc.cpp:141-160
-//   ring_kernel             Y = V_hphp + 0.5 V_hpph T'; R = T' Y     calc.cpp:264-313
+//   ring_*_kernel           Y = V_hphp + 0.5 V_hpph T'; R = T' Y     calc.cpp:264-313
 //   onebody_tables_kernel   calcChannelT2Diff_h2pp_h1 / _p2_p1hh     calc.cpp:9-25, 73-89
 //   onebody_fused_kernel    the same dot products, read from the ladder intermediates
 //   gather8_kernel          Chain::mapFromDistributed x 8            Chain.hpp:710-755
@@ -59,53 +60,115 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t
       "l"(src), "r"(bytes), "r"(bar)
       : "memory");
 }
-// FP64 tensor-core MMA: C[16x8] += A[16x4] B[4x8].
-__device__ __forceinline__ void dmma16x8x4(double (&c)[4], double a0, double a1, double b0) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
-      "{%0,%1,%2,%3};"
-      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
-      : "d"(a0), "d"(a1), "d"(b0));
-}
-
 __device__ __forceinline__ bool skip_iteration(const Control *ctl) {
   return ctl->active && ctl->done;
 }
 
 // ------------------------------------------------------------------------------------------
-// pp ladder + hh-ladder output: D[rows of tile] = 0.5 * (V_pppp T + T X).
-// Warp 4 is the producer: one lane streams pre-tiled operand blocks with bulk copies into a
-// kStages-deep ring of shared-memory stages.  Warps 0-3 each own 16 rows of the 64-row tile
-// and all n-fragments, and run FP64 m16n8k4 MMAs.  K runs over pp (V T) and then over hh
-// (T X) with the same pipeline.
+// pp ladder + hh-ladder output on the FP64 FMA pipe:
+//   D[ab,:] = sum_{c<d} V[ab,cd] T[cd,:] + T[ab,:] (X/2)     for packed rows a <= b,
+//   D[ba,:] = -D[ab,:]                                        (antisymmetry of V and T).
+// Warp 4 is the producer: one lane streams pre-tiled A/B stages with bulk copies (TMA, no
+// multicast) into a kStages-deep shared-memory ring guarded by mbarriers.  The 128 consumer
+// threads each own `cg` rows x 8 columns of the tile and run register-blocked DFMAs; V rows
+// come from shared memory conflict-free (XOR swizzle), T / X columns are warp broadcasts.
+// K runs over the c<d pairs (V T) and then over hh (T X) with the same pipeline.
 // ------------------------------------------------------------------------------------------
+template <int CG>
+__device__ __forceinline__ void ladder_consume(const LadderTile &tile, const double *As,
+                                               const double *Bs, uint64_t *bars, int tid,
+                                               const int32_t *__restrict__ rowmap,
+                                               const int32_t *__restrict__ mirror,
+                                               double *__restrict__ d, int32_t *err) {
+  constexpr int TM = CG, RG = kLadderConsumers / CG, NB = 8 * CG;
+  const int rg = tid / CG, cg = tid - rg * CG;
+  const bool worker = rg < RG;
+  const int lane = tid & 31;
+  double acc[TM][8];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+  const int nchunks = tile.nkc + tile.nkh;
+  for (int c = 0; c < nchunks; ++c) {
+    const int s = c % kStages;
+    if (!mbar_wait(smem_u32(&bars[s]), (c / kStages) & 1)) {
+      atomicOr(err, kErrTimeout);
+      return;
+    }
+    const double *A = As + s * (kMaxBM * kBK);
+    const double *B = Bs + s * (kBK * kMaxCG * 8);
+    if (worker) {
+#pragma unroll 4
+      for (int k = 0; k < kBK; ++k) {
+        double a[TM];
+#pragma unroll
+        for (int i = 0; i < TM; ++i) a[i] = A[swzA(rg + i * RG, k)];
+        const double2 *bp = reinterpret_cast<const double2 *>(B + k * NB + cg * 8);
+        double b[8];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const double2 v = bp[j];
+          b[2 * j] = v.x;
+          b[2 * j + 1] = v.y;
+        }
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+#pragma unroll
+          for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(smem_u32(&bars[kStages + s]));
+  }
+  if (!worker) return;
+  double *dblk = d + tile.t_off;
+#pragma unroll
+  for (int i = 0; i < TM; ++i) {
+    const int u = tile.mt * tile.bm + rg + i * RG;
+    if (u >= tile.pr) continue;
+    const int ab = rowmap[tile.row_off + u], mir = mirror[tile.row_off + u];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int col = cg * 8 + j;
+      if (col < tile.hh) {
+        dblk[(int64_t)ab * tile.hh + col] = acc[i][j];
+        if (mir >= 0) dblk[(int64_t)mir * tile.hh + col] = -acc[i][j];
+      }
+    }
+  }
+}
+
+// CG_LO..CG_HI: the column-group range a launch handles (separate instantiations keep the
+// register budget of narrow channels independent of the 72-column case).
+template <int CG_LO, int CG_HI>
 __global__ void __launch_bounds__(kLadderThreads, 2)
 pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict__ v_t,
                  const double *__restrict__ t_kt, const double *__restrict__ t_mt,
-                 const double *__restrict__ x_t, double *__restrict__ d, const Control *ctl,
-                 int32_t *err, int maxfrag) {
+                 const double *__restrict__ x_t, const int32_t *__restrict__ rowmap,
+                 const int32_t *__restrict__ mirror, double *__restrict__ d, const Control *ctl,
+                 int32_t *err) {
   if (skip_iteration(ctl)) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  const int bstride = maxfrag * 8 * kBK;
   double *As = reinterpret_cast<double *>(smem_raw);
-  double *Bs = As + kStages * kBM * kBK;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(Bs + kStages * bstride);
+  double *Bs = As + kStages * kMaxBM * kBK;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(Bs + kStages * kBK * kMaxCG * 8);
   const LadderTile tile = tiles[blockIdx.x];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nchunks = tile.nkc + tile.nkh;
-  const int nb = tile.nfrag * 8;
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(smem_u32(&bars[s]), 1);
-      mbar_init(smem_u32(&bars[kStages + s]), 4);
+      mbar_init(smem_u32(&bars[kStages + s]), kLadderConsumers / 32);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
 
-  if (warp == 4) {
+  if (warp == kLadderConsumers / 32) {
     if (lane == 0) {
-      const uint32_t abytes = kBM * kBK * 8, bbytes = nb * kBK * 8;
+      const int nb = 8 * tile.cg;
+      const uint32_t abytes = tile.bm * kBK * 8, bbytes = kBK * nb * 8;
+      const int nchunks = tile.nkc + tile.nkh;
       for (int c = 0; c < nchunks; ++c) {
         const int s = c % kStages;
         if (c >= kStages && !mbar_wait(smem_u32(&bars[kStages + s]), ((c / kStages) - 1) & 1)) {
@@ -114,133 +177,144 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict_
         }
         const double *asrc, *bsrc;
         if (c < tile.nkc) {
-          asrc = v_t + tile.v_base + (int64_t)(tile.mt * tile.nkc + c) * (kBM * kBK);
-          bsrc = t_kt + tile.tkt_base + (int64_t)c * nb * kBK;
+          asrc = v_t + tile.v_base + (int64_t)(tile.mt * tile.nkc + c) * tile.bm * kBK;
+          bsrc = t_kt + tile.tkt_base + (int64_t)c * kBK * nb;
         } else {
           const int kh = c - tile.nkc;
-          asrc = t_mt + tile.tmt_base + (int64_t)(tile.mt * tile.nkh + kh) * (kBM * kBK);
-          bsrc = x_t + tile.xt_base + (int64_t)kh * nb * kBK;
+          asrc = t_mt + tile.tmt_base + (int64_t)(tile.mt * tile.nkh + kh) * tile.bm * kBK;
+          bsrc = x_t + tile.xt_base + (int64_t)kh * kBK * nb;
         }
         const uint32_t full = smem_u32(&bars[s]);
         mbar_expect_tx(full, abytes + bbytes);
-        bulk_g2s(smem_u32(As + s * kBM * kBK), asrc, abytes, full);
-        bulk_g2s(smem_u32(Bs + s * bstride), bsrc, bbytes, full);
+        bulk_g2s(smem_u32(As + s * kMaxBM * kBK), asrc, abytes, full);
+        bulk_g2s(smem_u32(Bs + s * kBK * kMaxCG * 8), bsrc, bbytes, full);
       }
     }
     return;
   }
-
-  double acc[kMaxFrag][4];
-#pragma unroll
-  for (int f = 0; f < kMaxFrag; ++f) acc[f][0] = acc[f][1] = acc[f][2] = acc[f][3] = 0.0;
-  const int g = lane >> 2, t = lane & 3;
-  const int r0 = warp * 16 + g;
-  for (int c = 0; c < nchunks; ++c) {
-    const int s = c % kStages;
-    if (!mbar_wait(smem_u32(&bars[s]), (c / kStages) & 1)) {
-      atomicOr(err, kErrTimeout);
-      return;
-    }
-    const double *A = As + s * kBM * kBK;
-    const double *B = Bs + s * bstride;
-#pragma unroll
-    for (int kk = 0; kk < kBK; kk += 4) {
-      const double a0 = A[swz(r0, kk + t)], a1 = A[swz(r0 + 8, kk + t)];
-#pragma unroll
-      for (int f = 0; f < kMaxFrag; ++f)
-        if (f < tile.nfrag) dmma16x8x4(acc[f], a0, a1, B[swz(f * 8 + g, kk + t)]);
-    }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(smem_u32(&bars[kStages + s]));
+  const int tid = threadIdx.x;
+#define CCD_LADDER_CASE(n) \
+  case n: if (n >= CG_LO && n <= CG_HI) ladder_consume<n>(tile, As, Bs, bars, tid, rowmap, mirror, d, err); break;
+  switch (tile.cg) {
+    CCD_LADDER_CASE(1) CCD_LADDER_CASE(2) CCD_LADDER_CASE(3) CCD_LADDER_CASE(4)
+    CCD_LADDER_CASE(5) CCD_LADDER_CASE(6) CCD_LADDER_CASE(7) CCD_LADDER_CASE(8)
+    CCD_LADDER_CASE(9)
+    default: break;
   }
-
-  double *dblk = d + tile.t_off;
-  const int row = tile.mt * kBM + r0;
-#pragma unroll
-  for (int f = 0; f < kMaxFrag; ++f) {
-    if (f >= tile.nfrag) break;
-    const int col = f * 8 + 2 * t;
-    if (row < tile.pp) {
-      if (col < tile.hh) dblk[(int64_t)row * tile.hh + col] = 0.5 * acc[f][0];
-      if (col + 1 < tile.hh) dblk[(int64_t)row * tile.hh + col + 1] = 0.5 * acc[f][1];
-    }
-    if (row + 8 < tile.pp) {
-      if (col < tile.hh) dblk[(int64_t)(row + 8) * tile.hh + col] = 0.5 * acc[f][2];
-      if (col + 1 < tile.hh) dblk[(int64_t)(row + 8) * tile.hh + col + 1] = 0.5 * acc[f][3];
-    }
-  }
+#undef CCD_LADDER_CASE
 }
 
 // ------------------------------------------------------------------------------------------
-// hh ladder intermediate, one CTA per channel:
-//   P = V_hhpp T (K = pp),  X = V_hhhh + 0.5 P  (reference layout and X^T operand tiles),
+// hh ladder intermediate, split over 64-row K slices of each channel:
+//   P = V_hhpp T (K = pp),  X = V_hhhh + 0.5 P  (reference layout, and X/2 as B tiles),
 //   s[IJ] = P[IJ][IJ]            (x_k = sum over IJ with first hole k, calc.cpp:82-84),
 //   r[AB] = sum_IJ V[IJ][AB] T[AB][IJ]  (y_a = sum over AB with first particle a, calc.cpp:18-20).
-// V_hhpp is held transposed (V_pphh, pp x hh) so it streams row-aligned with T.
+// Each CTA writes its slice's partial P; the last CTA of a channel (atomic ticket) sums the
+// partials in slice order, so the result does not depend on scheduling.  V_hhpp is held
+// transposed (pp x hh) so a slice is one contiguous stretch, like the T slice.
 // ------------------------------------------------------------------------------------------
 constexpr int kHHThreads = 256;
-constexpr int kHHRows = 32;
+constexpr int kHHRows = 64;
 constexpr int kHHAcc = 21;  // (72*72)/256 rounded up
 
 __global__ void __launch_bounds__(kHHThreads)
-hh_ladder_kernel(const ChanInfo *__restrict__ chans, const double *__restrict__ v_pphh,
-                 const double *__restrict__ v_hhhh, const double *tbuf0, const double *tbuf1,
+hh_ladder_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ chans,
+                 const double *__restrict__ v_pphh, const double *__restrict__ v_hhhh,
+                 const double *tbuf0, const double *tbuf1, double *part, int32_t *counters,
                  double *__restrict__ x_ref, double *__restrict__ x_t, double *__restrict__ s_out,
                  double *__restrict__ r_out, const Control *ctl) {
   if (skip_iteration(ctl)) return;
-  __shared__ double Vs[kHHRows * 72];
-  __shared__ double Ts[kHHRows * 72];
-  const ChanInfo ch = chans[blockIdx.x];
+  extern __shared__ __align__(16) double hsm[];
+  __shared__ int last;
+  const HHTile tt = tiles[blockIdx.x];
+  const ChanInfo ch = chans[tt.ch];
   const double *t_old = ctl->parity ? tbuf1 : tbuf0;
-  const int pp = ch.pp, hh = ch.hh, tid = threadIdx.x;
-  const double *vb = v_pphh + ch.t_off, *tb = t_old + ch.t_off;
-  double acc[kHHAcc];
-#pragma unroll
-  for (int q = 0; q < kHHAcc; ++q) acc[q] = 0.0;
-  const int nout = hh * hh;
-  for (int k0 = 0; k0 < pp; k0 += kHHRows) {
-    const int rows = min(kHHRows, pp - k0);
-    const int n = rows * hh;
-    for (int e = tid; e < n; e += kHHThreads) {
-      Vs[e] = vb[(int64_t)k0 * hh + e];
-      Ts[e] = tb[(int64_t)k0 * hh + e];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < kHHAcc; ++q) {
-      const int idx = tid + q * kHHThreads;
-      if (idx < nout) {
-        const int kl = idx / hh, ij = idx - kl * hh;
-        double a = acc[q];
-        for (int k = 0; k < rows; ++k) a += Vs[k * hh + kl] * Ts[k * hh + ij];
-        acc[q] = a;
-      }
-    }
-    if (tid < rows) {
-      double rr = 0.0;
-      for (int ij = 0; ij < hh; ++ij) rr += Vs[tid * hh + ij] * Ts[tid * hh + ij];
-      r_out[ch.pp_off + k0 + tid] = rr;
-    }
-    __syncthreads();
+  const int hh = ch.hh, tid = threadIdx.x;
+  const int rows = min(kHHRows, ch.pp - tt.k0);
+  double *Vs = hsm, *Ts = hsm + kHHRows * hh;
+  const double *vb = v_pphh + ch.t_off + (int64_t)tt.k0 * hh;
+  const double *tb = t_old + ch.t_off + (int64_t)tt.k0 * hh;
+  for (int e = tid; e < rows * hh; e += kHHThreads) {
+    Vs[e] = vb[e];
+    Ts[e] = tb[e];
   }
-  const int nb = ch.nfrag * 8;
+  __syncthreads();
+  const int nout = hh * hh;
+  double *mypart = part + ch.part_off + (int64_t)tt.idx * nout;
 #pragma unroll
   for (int q = 0; q < kHHAcc; ++q) {
     const int idx = tid + q * kHHThreads;
     if (idx < nout) {
       const int kl = idx / hh, ij = idx - kl * hh;
-      const double x = v_hhhh[ch.x_off + idx] + 0.5 * acc[q];
-      x_ref[ch.x_off + idx] = x;
-      x_t[ch.xt_base + (int64_t)(kl / kBK) * nb * kBK + swz(ij, kl % kBK)] = x;
-      if (kl == ij) s_out[ch.hh_off + ij] = acc[q];
+      double a = 0.0;
+      for (int k = 0; k < rows; ++k) a += Vs[k * hh + kl] * Ts[k * hh + ij];
+      mypart[idx] = a;
     }
   }
+  if (tid < rows) {
+    double rr = 0.0;
+    for (int ij = 0; ij < hh; ++ij) rr += Vs[tid * hh + ij] * Ts[tid * hh + ij];
+    r_out[ch.pp_off + tt.k0 + tid] = rr;
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = (atomicAdd(&counters[tt.ch], 1) == ch.nhht - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int nb = 8 * ch.cg;
+  const double *pbase = part + ch.part_off;
+  for (int idx = tid; idx < nout; idx += kHHThreads) {
+    double p = 0.0;
+    for (int t = 0; t < ch.nhht; ++t) p += __ldcg(pbase + (int64_t)t * nout + idx);
+    const int kl = idx / hh, ij = idx - kl * hh;
+    const double x = v_hhhh[ch.x_off + idx] + 0.5 * p;
+    x_ref[ch.x_off + idx] = x;
+    x_t[ch.xt_base + (int64_t)(kl / kBK) * kBK * nb + (kl % kBK) * nb + ij] = 0.5 * x;
+    if (kl == ij) s_out[ch.hh_off + ij] = p;
+  }
+  if (tid == 0) counters[tt.ch] = 0;
 }
 
 // ------------------------------------------------------------------------------------------
-// Ring term, one CTA per modified channel: Y = V_hphp + 0.5 V_hpph T', R = T' Y.
+// Ring term: Y = V_hphp + 0.5 V_hpph T', R = T' Y per modified channel.
+// Channels with ph', hp' <= kRingSmall run one per warp; larger ones one per CTA.
 // ------------------------------------------------------------------------------------------
 constexpr int kRingThreads = 256;
+constexpr int kRingSmall = 16;
+
+__global__ void __launch_bounds__(256)
+ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restrict__ v_hpph,
+                  const double *__restrict__ v_hphp, const double *__restrict__ t_phhp,
+                  double *__restrict__ r_phhp, const Control *ctl) {
+  if (skip_iteration(ctl)) return;
+  __shared__ double buf[8][3 * kRingSmall * kRingSmall];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int mi = blockIdx.x * 8 + w;
+  if (mi >= n) return;
+  const ModInfo m = mods[mi];
+  const int ph = m.ph, hp = m.hp;
+  double *Ts = buf[w], *Va = Ts + ph * hp, *Ys = Va + hp * ph;
+  for (int e = lane; e < ph * hp; e += 32) {
+    Ts[e] = t_phhp[m.m_off + e];
+    Va[e] = v_hpph[m.m_off + e];
+  }
+  for (int e = lane; e < hp * hp; e += 32) Ys[e] = v_hphp[m.y_off + e];
+  __syncwarp();
+  for (int e = lane; e < hp * hp; e += 32) {
+    const int i = e / hp, j = e - i * hp;
+    double a = 0.0;
+    for (int k = 0; k < ph; ++k) a += Va[i * ph + k] * Ts[k * hp + j];
+    Ys[e] = 0.5 * a + Ys[e];
+  }
+  __syncwarp();
+  for (int e = lane; e < ph * hp; e += 32) {
+    const int i = e / hp, j = e - i * hp;
+    double a = 0.0;
+    for (int k = 0; k < hp; ++k) a += Ts[i * hp + k] * Ys[k * hp + j];
+    r_phhp[m.m_off + e] = a;
+  }
+}
 
 __global__ void __launch_bounds__(kRingThreads)
 ring_kernel(const ModInfo *__restrict__ mods, const double *__restrict__ v_hpph,
@@ -346,13 +420,17 @@ __global__ void onebody_fused_kernel(int np, int nsp, const int64_t *__restrict_
   }
 }
 
-// Scatter helpers for the operand tiles of the ladder kernels.
-__device__ __forceinline__ void write_t_tiles(const ChanInfo &ch, int ab, int ij, double t,
-                                              double *t_kt, double *t_mt) {
-  const int nb = ch.nfrag * 8;
-  t_kt[ch.tkt_base + (int64_t)(ab / kBK) * nb * kBK + swz(ij, ab % kBK)] = t;
-  t_mt[ch.tmt_base + (int64_t)((ab / kBM) * ch.nkh + ij / kBK) * (kBM * kBK) +
-       swz(ab % kBM, ij % kBK)] = t;
+// Writes one amplitude into the ladder operand tiles: the B tiles of V T (rows c<d) and the A
+// tiles of T X (rows a<=b).  pk_idx[AB] = (K index or -1, packed row or -1).
+__device__ __forceinline__ void write_t_tiles(const ChanInfo &ch, const int2 *__restrict__ pk_idx,
+                                              int ab, int ij, double t, double *t_kt,
+                                              double *t_mt) {
+  const int2 q = pk_idx[ch.pp_off + ab];
+  const int nb = 8 * ch.cg;
+  if (q.x >= 0) t_kt[ch.tkt_base + (int64_t)(q.x / kBK) * kBK * nb + (q.x % kBK) * nb + ij] = t;
+  if (q.y >= 0)
+    t_mt[ch.tmt_base + (int64_t)((q.y / ch.bm) * ch.nkh + ij / kBK) * ch.bm * kBK +
+         swzA(q.y % ch.bm, ij % kBK)] = t;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -365,12 +443,13 @@ __device__ __forceinline__ void write_t_tiles(const ChanInfo &ch, int ab, int ij
 // (mapToDistributed ai_jb) and into the ladder operand tiles.
 // ------------------------------------------------------------------------------------------
 constexpr int kAsmThreads = 256;
-constexpr int kAsmPerThread = 4;
+constexpr int kAsmPerThread = 1;
 
 __global__ void __launch_bounds__(kAsmThreads)
 assemble_fused_kernel(const ElemRange *__restrict__ ranges, const ChanInfo *__restrict__ chans,
                       const int2 *__restrict__ pp_pairs, const int2 *__restrict__ hh_pairs,
                       const int32_t *__restrict__ pp_swap, const int32_t *__restrict__ hh_swap,
+                      const int2 *__restrict__ pk_idx,
                       const double *__restrict__ v_pphh, const double *__restrict__ dmat,
                       const double *__restrict__ r_phhp, const int32_t *__restrict__ g_ai_jb,
                       const int32_t *__restrict__ g_aj_ib, const int32_t *__restrict__ g_bi_ja,
@@ -410,7 +489,7 @@ assemble_fused_kernel(const ElemRange *__restrict__ ranges, const ChanInfo *__re
     value = mixing * value + (1. - mixing) * to;
     t_new[e] = value;
     old_phhp[g_ai_jb[e]] = value;
-    write_t_tiles(ch, ab, ij, value, t_kt, t_mt);
+    write_t_tiles(ch, pk_idx, ab, ij, value, t_kt, t_mt);
     corr += v * value;
   }
   const double sum = block_sum<kAsmThreads>(corr, scratch);
@@ -470,7 +549,8 @@ __global__ void gather8_kernel(int64_t n_t, const int32_t *__restrict__ flat,
 
 // Chain::set + the five mapToDistributed scatters, plus the ladder operand tiles.
 __global__ void map_to_kernel(const ElemRange *__restrict__ ranges, const ChanInfo *__restrict__ chans,
-                              const int32_t *__restrict__ flat, int64_t n_t,
+                              const int2 *__restrict__ pk_idx, const int32_t *__restrict__ flat,
+                              int64_t n_t,
                               const double *__restrict__ t2, double *__restrict__ t2_old,
                               double *__restrict__ old_h2pp_h1, double *__restrict__ old_h1pp_h2,
                               double *__restrict__ old_p1_p2hh, double *__restrict__ old_p2_p1hh,
@@ -490,7 +570,7 @@ __global__ void map_to_kernel(const ElemRange *__restrict__ ranges, const ChanIn
     old_phhp[flat[4 * n_t + e]] = t;       // ai_jb
     const int64_t loc = e - ch.t_off;
     const int ab = (int)(loc / ch.hh), ij = (int)(loc - (int64_t)ab * ch.hh);
-    write_t_tiles(ch, ab, ij, t, t_kt, t_mt);
+    write_t_tiles(ch, pk_idx, ab, ij, t, t_kt, t_mt);
   }
 }
 

@@ -41,14 +41,19 @@ struct ccdgpu_handle {
   cudaEvent_t ev[10] = {};
   uint64_t nch = 0, nsp = 0, np = 0, npart = 0;
   int64_t n_t = 0, n_m = 0, n_h = 0, n_p = 0;
-  int n_act = 0, n_mod = 0, n_tiles = 0, n_ranges = 0, maxfrag = 1;
-  size_t ladder_smem = 0, ring_smem = 0;
+  int n_act = 0, n_mod = 0, n_mod_small = 0, n_tiles = 0, n_tiles_narrow = 0, n_hh_tiles = 0,
+      n_ranges = 0;
+  size_t ladder_smem = 0, ring_smem = 0, hh_smem = 0;
   bool have_3body = false;
   std::vector<DevBuf> allocs;
 
   ChanInfo *chans = nullptr;
-  ModInfo *mods = nullptr;
+  ModInfo *mods = nullptr;        // small channels first (n_mod_small), then the others
   LadderTile *tiles = nullptr;
+  HHTile *hh_tiles = nullptr;
+  int32_t *rowmap = nullptr, *mirror = nullptr, *counters = nullptr;
+  int2 *pk_idx = nullptr;
+  double *part = nullptr;
   ElemRange *ranges = nullptr;
   int2 *pp_pairs = nullptr, *hh_pairs = nullptr;
   int32_t *pp_swap = nullptr, *hh_swap = nullptr;
@@ -159,32 +164,61 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
 
   std::vector<ChanInfo> chans;
   std::vector<int64_t> act_of(nch, -1);
-  int64_t pp_tot = 0, hh_tot = 0, x_tot = 0, tkt = 0, tmt = 0, xt = 0, vt = 0;
-  int maxfrag = 1;
+  // Packed rows (a<=b) and K pairs (c<d) per channel, from the sorted pp map.
+  std::vector<int32_t> rowmap, mirror;
+  std::vector<int2> pk_idx;
+  std::vector<HHTile> hh_tiles;
+  int64_t pp_tot = 0, hh_tot = 0, x_tot = 0, tkt = 0, tmt = 0, xt = 0, vt = 0, part_tot = 0;
   for (uint64_t c = 0; c < nch; c++) {
     const int64_t pp = D[c].pp, hh = D[c].hh;
     if (!pp || !hh) continue;
-    if (hh > 8 * kMaxFrag || pp > (1 << 20)) return CCDGPU_ERR_UNSUPPORTED;
+    if (hh > 8 * kMaxCG || pp > (1 << 20)) return CCDGPU_ERR_UNSUPPORTED;
+    const ccdgpu_pair *pm = P->chan_maps[c].pp;
+    if (!pm || !P->chan_maps[c].hh) return CCDGPU_ERR_INVALID_ARGUMENT;
     ChanInfo ci{};
     ci.pp = (int)pp; ci.hh = (int)hh;
-    ci.nfrag = (int)ceil_div(hh, 8);
-    ci.nkc = (int)ceil_div(pp, kBK);
+    ci.cg = (int)ceil_div(hh, 8);
+    ci.bm = ladder_bm(ci.cg);
+    ci.row_off = (int64_t)rowmap.size();
+    int pr = 0, pk = 0;
+    for (int k = 0; k < ci.pp; k++) {
+      int2 q = make_int2(-1, -1);
+      if (pm[k].p < pm[k].q) q.x = pk++;
+      if (pm[k].p <= pm[k].q) {
+        q.y = pr++;
+        rowmap.push_back(k);
+        int mir = -1;
+        if (pm[k].p < pm[k].q) {
+          mir = find_pair(pm, ci.pp, pm[k].q, pm[k].p);
+          if (mir < 0) return CCDGPU_ERR_BAD_TABLE;
+        }
+        mirror.push_back(mir);
+      }
+      pk_idx.push_back(q);
+    }
+    ci.pr = pr; ci.pk = pk;
+    ci.nkc = (int)ceil_div(pk, kBK);
     ci.nkh = (int)ceil_div(hh, kBK);
-    ci.nmt = (int)ceil_div(pp, kBM);
+    ci.nmt = (int)ceil_div(pr, ci.bm);
+    ci.nhht = (int)ceil_div(pp, kHHRows);
     ci.t_off = o_t[c];
     ci.pp_off = pp_tot; ci.hh_off = hh_tot; ci.x_off = x_tot;
     ci.tkt_base = tkt; ci.tmt_base = tmt; ci.xt_base = xt; ci.vkt_base = vt;
+    ci.part_off = part_tot;
+    ci.hht0 = (int64_t)hh_tiles.size();
+    const int nb = 8 * ci.cg;
     pp_tot += pp; hh_tot += hh; x_tot += hh * hh;
-    tkt += (int64_t)ci.nkc * ci.nfrag * 8 * kBK;
-    tmt += (int64_t)ci.nmt * ci.nkh * kBM * kBK;
-    xt += (int64_t)ci.nkh * ci.nfrag * 8 * kBK;
-    vt += (int64_t)ci.nmt * ci.nkc * kBM * kBK;
-    maxfrag = std::max(maxfrag, ci.nfrag);
+    tkt += (int64_t)ci.nkc * kBK * nb;
+    tmt += (int64_t)ci.nmt * ci.nkh * ci.bm * kBK;
+    xt += (int64_t)ci.nkh * kBK * nb;
+    vt += (int64_t)ci.nmt * ci.nkc * ci.bm * kBK;
+    part_tot += (int64_t)ci.nhht * hh * hh;
     act_of[c] = (int64_t)chans.size();
+    for (int t = 0; t < ci.nhht; t++) hh_tiles.push_back({(int32_t)chans.size(), t * kHHRows, t, 0});
     chans.push_back(ci);
   }
   h->n_act = (int)chans.size();
-  h->maxfrag = maxfrag;
+  h->n_hh_tiles = (int)hh_tiles.size();
 
   // Pair tables, swaps and one-body segment lists.
   std::vector<int2> pp_pairs(pp_tot), hh_pairs(hh_tot);
@@ -218,7 +252,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   for (uint64_t w = 0; w < nsp; w++) std::copy(seg[w].begin(), seg[w].end(), list.begin() + list_off[w]);
 
   // Modified channels.
-  std::vector<ModInfo> mods;
+  std::vector<ModInfo> mods, mods_big;
+  std::vector<int64_t> mod_y(nch, -1);
   int64_t y_tot = 0;
   size_t ring_smem = 0;
   for (uint64_t c = 0; c < nch; c++) {
@@ -226,10 +261,17 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     if (!ph || !hp) continue;
     ModInfo m{};
     m.ph = (int)ph; m.hp = (int)hp; m.m_off = o_m[c]; m.y_off = y_tot;
+    mod_y[c] = y_tot;
     y_tot += hp * hp;
-    ring_smem = std::max(ring_smem, (size_t)(2 * ph * hp + hp * hp) * 8);
-    mods.push_back(m);
+    if (ph <= kRingSmall && hp <= kRingSmall) {
+      mods.push_back(m);
+    } else {
+      ring_smem = std::max(ring_smem, (size_t)(2 * ph * hp + hp * hp) * 8);
+      mods_big.push_back(m);
+    }
   }
+  h->n_mod_small = (int)mods.size();
+  mods.insert(mods.end(), mods_big.begin(), mods_big.end());
   h->n_mod = (int)mods.size();
   h->ring_smem = ring_smem;
 
@@ -303,22 +345,26 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     for (int ij = 0; ij < a.hh; ij++)
       for (int ab = 0; ab < a.pp; ab++) v_pphh[a.t_off + (int64_t)ab * a.hh + ij] = vx[(int64_t)ij * a.pp + ab];
     std::memcpy(&v_hhhh[a.x_off], vh, sizeof(double) * a.hh * a.hh);
-    for (int ab = 0; ab < a.pp; ab++)
-      for (int cd = 0; cd < a.pp; cd++)
-        v_t[a.vkt_base + (int64_t)((ab / kBM) * a.nkc + cd / kBK) * (kBM * kBK) + swz(ab % kBM, cd % kBK)] =
-            vp[(int64_t)ab * a.pp + cd];
+    // Packed V tiles: rows a<=b (rowmap), columns c<d (pk_idx.x), zero padding elsewhere.
+    std::vector<int32_t> kcol(a.pk);
+    for (int k = 0; k < a.pp; k++)
+      if (pk_idx[a.pp_off + k].x >= 0) kcol[pk_idx[a.pp_off + k].x] = k;
+    for (int u = 0; u < a.pr; u++) {
+      const int ab = rowmap[a.row_off + u];
+      const int64_t tb = a.vkt_base + (int64_t)(u / a.bm) * a.nkc * a.bm * kBK;
+      for (int w = 0; w < a.pk; w++)
+        v_t[tb + (int64_t)(w / kBK) * a.bm * kBK + swzA(u % a.bm, w % kBK)] =
+            vp[(int64_t)ab * a.pp + kcol[w]];
+    }
   }
   if (bad) return CCDGPU_ERR_INVALID_ARGUMENT;
-  {
-    size_t q = 0;
-    for (uint64_t c = 0; c < nch; c++) {
-      if (!MD[c].ph || !MD[c].hp) continue;
-      const ModInfo &m = mods[q++];
-      const double *va = P->v_hpph_mod[c], *vb = P->v_hphp_mod[c];
-      if (!va || !vb) return CCDGPU_ERR_INVALID_ARGUMENT;
-      std::memcpy(&v_hpph[m.m_off], va, sizeof(double) * m.ph * m.hp);
-      std::memcpy(&v_hphp[m.y_off], vb, sizeof(double) * m.hp * m.hp);
-    }
+  for (uint64_t c = 0; c < nch; c++) {
+    const int64_t ph = MD[c].ph, hp = MD[c].hp;
+    if (!ph || !hp) continue;
+    const double *va = P->v_hpph_mod[c], *vb = P->v_hphp_mod[c];
+    if (!va || !vb) return CCDGPU_ERR_INVALID_ARGUMENT;
+    std::memcpy(&v_hpph[o_m[c]], va, sizeof(double) * ph * hp);
+    std::memcpy(&v_hphp[mod_y[c]], vb, sizeof(double) * hp * hp);
   }
   std::vector<double> v_h_hpp, v_phh_p;
   h->have_3body = P->v_h_hpp && P->v_phh_p;
@@ -343,16 +389,22 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     const ChanInfo &a = chans[ai];
     for (int mt = 0; mt < a.nmt; mt++) {
       LadderTile tl{};
-      tl.ch = ai; tl.mt = mt; tl.nkc = a.nkc; tl.nkh = a.nkh; tl.nfrag = a.nfrag;
-      tl.pp = a.pp; tl.hh = a.hh;
+      tl.ch = ai; tl.mt = mt; tl.nkc = a.nkc; tl.nkh = a.nkh; tl.cg = a.cg; tl.bm = a.bm;
+      tl.pr = a.pr; tl.hh = a.hh;
       tl.v_base = a.vkt_base; tl.tkt_base = a.tkt_base; tl.tmt_base = a.tmt_base;
-      tl.xt_base = a.xt_base; tl.t_off = a.t_off;
+      tl.xt_base = a.xt_base; tl.t_off = a.t_off; tl.row_off = a.row_off;
       tiles.push_back(tl);
     }
   }
+  // Narrow channels (<= 32 hh columns) first, then wide ones; within each class the longest
+  // K streams first so the hardware block scheduler fills in the short ones.
   std::stable_sort(tiles.begin(), tiles.end(), [](const LadderTile &x, const LadderTile &y) {
-    return (int64_t)(x.nkc + x.nkh) * (kBM + 8 * x.nfrag) > (int64_t)(y.nkc + y.nkh) * (kBM + 8 * y.nfrag);
+    const bool nx = x.cg <= kNarrowCG, ny = y.cg <= kNarrowCG;
+    if (nx != ny) return nx;
+    return (int64_t)(x.nkc + x.nkh) * (x.bm + 8 * x.cg) > (int64_t)(y.nkc + y.nkh) * (y.bm + 8 * y.cg);
   });
+  h->n_tiles_narrow = 0;
+  for (const LadderTile &t : tiles) h->n_tiles_narrow += t.cg <= kNarrowCG;
   h->n_tiles = (int)tiles.size();
   std::vector<ElemRange> ranges;
   const int64_t per = (int64_t)kAsmThreads * kAsmPerThread;
@@ -379,6 +431,12 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   TRY(upload(h, &h->chans, chans));
   TRY(upload(h, &h->mods, mods));
   TRY(upload(h, &h->tiles, tiles));
+  TRY(upload(h, &h->hh_tiles, hh_tiles));
+  TRY(upload(h, &h->rowmap, rowmap));
+  TRY(upload(h, &h->mirror, mirror));
+  TRY(upload(h, &h->pk_idx, pk_idx));
+  TRY(dalloc(h, &h->counters, h->n_act));
+  TRY(dalloc(h, &h->part, part_tot));
   TRY(upload(h, &h->ranges, ranges));
   TRY(upload(h, &h->pp_pairs, pp_pairs));
   TRY(upload(h, &h->hh_pairs, hh_pairs));
@@ -428,9 +486,19 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   CK(cudaMallocHost(&h->h_ctl, sizeof(Control)));
   std::memset(h->h_ctl, 0, sizeof(Control));
 
-  h->ladder_smem = (size_t)kStages * (kBM * kBK + maxfrag * 8 * kBK) * 8 + 2 * kStages * 8;
-  CK(cudaFuncSetAttribute(pp_ladder_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  h->ladder_smem = (size_t)kStages * (kMaxBM * kBK + kBK * kMaxCG * 8) * 8 + 2 * kStages * 8;
+  CK(cudaFuncSetAttribute(pp_ladder_kernel<1, kNarrowCG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)h->ladder_smem));
+  CK(cudaFuncSetAttribute(pp_ladder_kernel<1, kNarrowCG>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  CK(cudaFuncSetAttribute(pp_ladder_kernel<kNarrowCG + 1, kMaxCG>,
+                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->ladder_smem));
+  CK(cudaFuncSetAttribute(pp_ladder_kernel<kNarrowCG + 1, kMaxCG>,
+                          cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  int maxhh = 1;
+  for (const ChanInfo &a : chans) maxhh = std::max(maxhh, a.hh);
+  h->hh_smem = (size_t)2 * kHHRows * maxhh * 8;
+  CK(cudaFuncSetAttribute(hh_ladder_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)h->hh_smem));
   CK(cudaFuncSetAttribute(ring_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)std::max<size_t>(h->ring_smem, 16)));
   CK(cudaStreamSynchronize(h->s0));
@@ -440,25 +508,45 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
 // ---- launches -------------------------------------------------------------------------
 
 int launch_hh_ladder(ccdgpu_handle *h, cudaStream_t st) {
-  if (!h->n_act) return CCDGPU_OK;
-  hh_ladder_kernel<<<h->n_act, kHHThreads, 0, st>>>(h->chans, h->v_pphh, h->v_hhhh, h->t[0], h->t[1],
-                                                     h->x, h->x_t, h->s, h->r, h->ctl);
+  if (!h->n_hh_tiles) return CCDGPU_OK;
+  hh_ladder_kernel<<<h->n_hh_tiles, kHHThreads, h->hh_smem, st>>>(
+      h->hh_tiles, h->chans, h->v_pphh, h->v_hhhh, h->t[0], h->t[1], h->part, h->counters, h->x,
+      h->x_t, h->s, h->r, h->ctl);
   h->launches++;
   return cuda_status(cudaGetLastError());
 }
 int launch_pp_ladder(ccdgpu_handle *h, cudaStream_t st) {
-  if (!h->n_tiles) return CCDGPU_OK;
-  pp_ladder_kernel<<<h->n_tiles, kLadderThreads, h->ladder_smem, st>>>(
-      h->tiles, h->v_t, h->t_kt, h->t_mt, h->x_t, h->dmat, h->ctl, h->err, h->maxfrag);
-  h->launches++;
-  return cuda_status(cudaGetLastError());
+  if (h->n_tiles_narrow) {
+    pp_ladder_kernel<1, kNarrowCG><<<h->n_tiles_narrow, kLadderThreads, h->ladder_smem, st>>>(
+        h->tiles, h->v_t, h->t_kt, h->t_mt, h->x_t, h->rowmap, h->mirror, h->dmat, h->ctl, h->err);
+    h->launches++;
+    CK(cudaGetLastError());
+  }
+  const int nwide = h->n_tiles - h->n_tiles_narrow;
+  if (nwide) {
+    pp_ladder_kernel<kNarrowCG + 1, kMaxCG><<<nwide, kLadderThreads, h->ladder_smem, st>>>(
+        h->tiles + h->n_tiles_narrow, h->v_t, h->t_kt, h->t_mt, h->x_t, h->rowmap, h->mirror,
+        h->dmat, h->ctl, h->err);
+    h->launches++;
+    CK(cudaGetLastError());
+  }
+  return CCDGPU_OK;
 }
 int launch_ring(ccdgpu_handle *h, cudaStream_t st) {
-  if (!h->n_mod) return CCDGPU_OK;
-  ring_kernel<<<h->n_mod, kRingThreads, std::max<size_t>(h->ring_smem, 16), st>>>(
-      h->mods, h->v_hpph, h->v_hphp, h->old_phhp, h->r_phhp, h->ctl);
-  h->launches++;
-  return cuda_status(cudaGetLastError());
+  if (h->n_mod_small) {
+    ring_small_kernel<<<(int)ceil_div(h->n_mod_small, 8), 256, 0, st>>>(
+        h->mods, h->n_mod_small, h->v_hpph, h->v_hphp, h->old_phhp, h->r_phhp, h->ctl);
+    h->launches++;
+    CK(cudaGetLastError());
+  }
+  const int nbig = h->n_mod - h->n_mod_small;
+  if (nbig) {
+    ring_kernel<<<nbig, kRingThreads, std::max<size_t>(h->ring_smem, 16), st>>>(
+        h->mods + h->n_mod_small, h->v_hpph, h->v_hphp, h->old_phhp, h->r_phhp, h->ctl);
+    h->launches++;
+    CK(cudaGetLastError());
+  }
+  return CCDGPU_OK;
 }
 int launch_onebody_fused(ccdgpu_handle *h, cudaStream_t st) {
   const int warps_per_block = 8;
@@ -472,7 +560,8 @@ int launch_assemble_fused(ccdgpu_handle *h, cudaStream_t st) {
   if (!h->n_ranges) return CCDGPU_OK;
   const int64_t n_t = h->n_t;
   assemble_fused_kernel<<<h->n_ranges, kAsmThreads, 0, st>>>(
-      h->ranges, h->chans, h->pp_pairs, h->hh_pairs, h->pp_swap, h->hh_swap, h->v_pphh, h->dmat,
+      h->ranges, h->chans, h->pp_pairs, h->hh_pairs, h->pp_swap, h->hh_swap, h->pk_idx, h->v_pphh,
+      h->dmat,
       h->r_phhp, h->flat + 4 * n_t, h->flat + 5 * n_t, h->flat + 6 * n_t, h->flat + 7 * n_t, h->xh,
       h->yp, h->eps, (int)h->np, h->t[0], h->t[1], h->old_phhp, h->t_kt, h->t_mt, h->epart, h->ctl);
   h->launches++;
@@ -485,7 +574,7 @@ int launch_energy(ccdgpu_handle *h, cudaStream_t st, int flags) {
 }
 int launch_map_to(ccdgpu_handle *h, cudaStream_t st, const double *src, double *dst) {
   if (!h->n_ranges) return CCDGPU_OK;
-  map_to_kernel<<<h->n_ranges, 256, 0, st>>>(h->ranges, h->chans, h->flat, h->n_t, src, dst,
+  map_to_kernel<<<h->n_ranges, 256, 0, st>>>(h->ranges, h->chans, h->pk_idx, h->flat, h->n_t, src, dst,
                                                h->old_h2pp_h1, h->old_h1pp_h2, h->old_p1_p2hh,
                                                h->old_p2_p1hh, h->old_phhp, h->t_kt, h->t_mt,
                                                h->have_3body ? 1 : 0);
