@@ -274,12 +274,9 @@ def main():
         peaks, peak_kind = measured_peaks()
         it_p = max(prof["iterations"], 1)
         ladder_ms = prof["ms_ladder"] / it_p
-        d = system.chan_dims()
-        act = (d[:, 0] > 0) & (d[:, 1] > 0)
-        pp = d[act, 0].astype(np.float64)
-        hh = d[act, 1].astype(np.float64)
-        # Algorithmic bytes of one pp-ladder launch: V_pppp, T read, X read, D written.
-        ladder_bytes = 8.0 * float((pp * pp).sum() + 2 * (pp * hh).sum() + (hh * hh).sum())
+        # Algorithmic bytes of one pp-ladder launch: antisymmetry-packed V_pppp (rows a<=b,
+        # columns c<d), the T and X operands and D written in full.
+        ladder_bytes = work["ladder_bytes"]
         achieved = ladder_bytes / (ladder_ms / 1000.0) / 1e9
         cpu = None
         if not args.no_cpu_baseline:
@@ -323,8 +320,10 @@ def main():
 
 
 def _problem_bytes(system):
-    """Bytes ccdgpu_create copies host -> device for this system (V blocks, maps as int32
-    offsets, pair lists, energies)."""
+    """Bytes ccdgpu_create copies host -> device for this system: V blocks in their reference
+    layouts (V_pppp, V_hhpp, V_hhhh of amplitude-carrying channels, both modified-channel V,
+    the three-body V), the eight ChainIndex tables (24 bytes per entry), the energies and the
+    O(sum pp) pair metadata."""
     import numpy as np
     d = system.chan_dims()
     act = (d[:, 0] > 0) & (d[:, 1] > 0)
@@ -334,9 +333,10 @@ def _problem_bytes(system):
     hp = md[:, 2].astype(np.int64)
     ph = md[:, 3].astype(np.int64)
     n_t = int((pp * hh).sum())
-    v = 8 * int((pp * pp).sum() + (hh * hh).sum() + n_t + (ph * hp).sum() + (hp * hp).sum())
-    v += 8 * 2 * n_t  # three-body V (hpp and phh chains)
-    return v + 4 * 8 * n_t + 8 * system.n_sp
+    v = 8 * int((pp * pp).sum() + n_t + (hh * hh).sum() + (ph * hp).sum() + (hp * hp).sum())
+    v += 8 * 2 * n_t
+    meta = 24 * int(pp.sum()) + 16 * int(hh.sum()) + 8 * system.n_sp
+    return v + 24 * 8 * n_t + meta
 
 
 def _cpu_baseline(cfg):

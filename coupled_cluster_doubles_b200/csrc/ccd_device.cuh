@@ -13,49 +13,60 @@ namespace ccd {
 //
 // Operand tiles are stored in HBM already in their shared-memory image so that one bulk copy
 // (TMA) moves a whole stage:
-//   A tiles  [bm rows][kBK]   row-major, column XOR-swizzled by (row & 15): a warp reading
-//                              16 consecutive rows at one k hits 16 distinct bank pairs;
-//   B tiles  [kBK][nb]        k-major (nb = 8 * cg padded hh columns), read as broadcasts.
+//   A tiles  [rows][kBK]  row-major, column XOR-swizzled by (row & 15): a warp reading 16
+//                         consecutive rows at one k hits 16 distinct bank pairs.  The last row
+//                         tile of a channel is stored compact (only its real rows).
+//   B tiles  [kBK][nb]    k-major, nb = padded hh columns, read as warp broadcasts.
+// Column classes: thin channels (hh <= 8) use nb in {2, 4, 8} with one row per consumer
+// thread; wide channels use nb = 8*cg with cg rows x 8 columns per consumer thread.
 constexpr int kBK = 16;        // K depth of one pipeline stage
 constexpr int kStages = 4;     // bulk-copy pipeline depth
 constexpr int kMaxCG = 9;      // column groups of 8 -> up to 72 hh columns
-constexpr int kNarrowCG = 4;   // channels up to 32 hh columns use the narrow instantiation
 constexpr int kLadderConsumers = 128;
 constexpr int kLadderThreads = kLadderConsumers + 32;  // + 1 producer warp
 constexpr int kMaxBM = 128;
+constexpr int kMaxNB = 8 * kMaxCG;
 
 __host__ __device__ inline int swzA(int row, int k) { return row * kBK + (k ^ (row & 15)); }
-// Rows per tile for a channel with cg column groups: each consumer thread owns cg rows
-// (strided by the number of row groups) and 8 columns.
-__host__ __device__ inline int ladder_bm(int cg) { return (kLadderConsumers / cg) * cg; }
+// Padded column count of a channel with hh hole pairs.
+__host__ __device__ inline int ladder_nb(int hh) {
+  return hh <= 2 ? 2 : hh <= 4 ? 4 : 8 * ((hh + 7) / 8);
+}
+// Rows per consumer thread for a wide channel with cg column groups of 8.
+__host__ __device__ constexpr int ladder_tm(int cg) { return cg <= 4 ? cg : 4; }
+// Rows per tile: thin channels one row per consumer thread; wide ones ladder_tm(cg) rows x 8
+// columns per thread, 128/cg row groups.
+__host__ __device__ inline int ladder_bm(int nb) {
+  if (nb <= 8) return kLadderConsumers;
+  const int cg = nb / 8;
+  return (kLadderConsumers / cg) * ladder_tm(cg);
+}
 
-// One pp-ladder work tile: packed rows [mt*bm, mt*bm+bm) of channel `ch`.
+// One pp-ladder work tile: packed rows [mt*bm, mt*bm+rows) of channel `ch`, V-part K chunks
+// [kc0, kc0+nks).  Tiles of one row block that split K write partial sums; the last one to
+// finish (ticket on counter `group`) adds them in segment order.  The segment with seg ==
+// nseg-1 also runs the T X chunks.
 struct LadderTile {
-  int32_t ch;        // active-channel index
-  int32_t mt;        // row tile
-  int32_t nkc;       // K chunks over the c<d pairs (V T part)
-  int32_t nkh;       // K chunks over hh (T X part)
-  int32_t cg;        // column groups (ceil(hh/8))
-  int32_t bm;        // rows per tile
-  int32_t pr;        // packed rows (a<=b) of the channel
-  int32_t hh;
-  int64_t v_base;    // A tiles of V:  + (mt*nkc + kc) * bm*kBK
+  int32_t ch, mt, kc0, nks, nkc, nkh, nb, bm, rows, pr, hh, seg, nseg, group;
+  int64_t v_base;    // A tiles of V:  tile base + kc * rows*kBK (tile base = mt*bm*nkc*kBK)
   int64_t tkt_base;  // B tiles of T:  + kc * kBK*nb
-  int64_t tmt_base;  // A tiles of T (rows a<=b, K = hh): + (mt*nkh + kh) * bm*kBK
+  int64_t tmt_base;  // A tiles of T (rows a<=b, K = hh): + mt*bm*nkh*kBK + kh * rows*kBK
   int64_t xt_base;   // B tiles of X/2: + kh * kBK*nb
   int64_t t_off;     // offset of the channel's pp x hh block in the t2 layout
   int64_t row_off;   // offset into rowmap / mirror
+  int64_t part_base; // partial sums of this row block: nseg * bm * nb doubles
 };
 
 // Per active regular channel.
 struct ChanInfo {
-  int32_t pp, hh, cg, nkc, nkh, nmt, bm, pr, pk, nhht;
+  int32_t pp, hh, nb, nkc, nkh, nmt, bm, pr, pk, nhht;
   int64_t t_off;     // pphh block offset (reference t2 layout)
   int64_t pp_off;    // offset into pp_pairs / pp_swap / pk_idx / r
   int64_t hh_off;    // offset into hh_pairs / hh_swap / s
   int64_t x_off;     // hh x hh block offset (V_hhhh and X)
   int64_t tkt_base, tmt_base, xt_base, vkt_base;
   int64_t row_off;   // offset into rowmap / mirror (pr entries)
+  int64_t pk_off;    // offset into kcol (pk entries)
   int64_t part_off;  // hh-ladder partial products: nhht * hh*hh doubles
   int64_t hht0;      // first hh-ladder tile of the channel
 };

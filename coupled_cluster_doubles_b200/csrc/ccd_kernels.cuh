@@ -19,7 +19,7 @@
 
 namespace ccd {
 
-constexpr uint32_t kSpinLimit = 1u << 24;  // bounded mbarrier waits (~1 s with backoff)
+constexpr uint64_t kWaitLimitNs = 1000000000ull;  // bounded mbarrier waits: 1 s of globaltimer
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -43,13 +43,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait on an mbarrier phase; false once the spin budget is spent.
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait on an mbarrier phase: try_wait suspends the thread in hardware until the phase
+// completes or a short internal time limit passes; give up (false) after kWaitLimitNs.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (uint32_t it = 0; it < kSpinLimit; ++it) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if (it > 32) __nanosleep(64);
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (;;) {
+#pragma unroll 1
+    for (int i = 0; i < 256; ++i)
+      if (mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > kWaitLimitNs) return false;
   }
-  return false;
 }
 // 1-D bulk copy global -> shared, completion counted on an mbarrier (TMA unit, no multicast).
 __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes,
@@ -60,7 +69,31 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t
       "l"(src), "r"(bytes), "r"(bar)
       : "memory");
 }
+// sum_k a[k*sa] * b[k*sb] for k < n with four interleaved partial sums (more independent FMA
+// chains in flight), combined in a fixed order.
+__device__ __forceinline__ double dot4(const double *a, int sa, const double *b, int sb, int n) {
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  int k = 0;
+  for (; k + 4 <= n; k += 4) {
+    s0 = fma(a[k * sa], b[k * sb], s0);
+    s1 = fma(a[(k + 1) * sa], b[(k + 1) * sb], s1);
+    s2 = fma(a[(k + 2) * sa], b[(k + 2) * sb], s2);
+    s3 = fma(a[(k + 3) * sa], b[(k + 3) * sb], s3);
+  }
+  for (; k < n; ++k) s0 = fma(a[k * sa], b[k * sb], s0);
+  return (s0 + s1) + (s2 + s3);
+}
+
+// Programmatic dependent launch: wait until the preceding kernel of the stream has completed
+// (its writes are visible), then allow the next kernel to begin launching once every CTA of
+// this grid is resident.  Both are no-ops for kernels launched without the PDL attribute.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ bool skip_iteration(const Control *ctl) {
+  pdl_enter();
   return ctl->active && ctl->done;
 }
 
@@ -70,17 +103,108 @@ __device__ __forceinline__ bool skip_iteration(const Control *ctl) {
 //   D[ba,:] = -D[ab,:]                                        (antisymmetry of V and T).
 // Warp 4 is the producer: one lane streams pre-tiled A/B stages with bulk copies (TMA, no
 // multicast) into a kStages-deep shared-memory ring guarded by mbarriers.  The 128 consumer
-// threads each own `cg` rows x 8 columns of the tile and run register-blocked DFMAs; V rows
-// come from shared memory conflict-free (XOR swizzle), T / X columns are warp broadcasts.
-// K runs over the c<d pairs (V T) and then over hh (T X) with the same pipeline.
+// threads run register-blocked DFMAs: V rows come from shared memory conflict-free (XOR
+// swizzle), T / X columns are warp broadcasts.  K runs over the c<d pairs (V T) and then over
+// hh (T X) with the same pipeline.  Row blocks whose K is split over several tiles write
+// partial sums that the last tile to finish adds in segment order (deterministic).
 // ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void consumers_sync() {
+  asm volatile("bar.sync 1, %0;" ::"n"(kLadderConsumers) : "memory");
+}
+
+// Stores the finished values of packed row u_local (cols [c0, c0+n)), or its partial sum.
+struct LadderOut {
+  const LadderTile &tile;
+  const int32_t *rowmap, *mirror;
+  double *d, *part;
+  __device__ __forceinline__ void row(int u_local, int c0, const double *v, int n) const {
+    if (u_local >= tile.rows) return;
+    if (tile.nseg > 1) {
+      double *pp = part + tile.part_base + ((int64_t)tile.seg * tile.bm + u_local) * tile.nb + c0;
+      for (int j = 0; j < n; ++j) pp[j] = v[j];
+      return;
+    }
+    const int u = tile.mt * tile.bm + u_local;
+    const int ab = rowmap[tile.row_off + u], mir = mirror[tile.row_off + u];
+    double *dr = d + tile.t_off + (int64_t)ab * tile.hh;
+    double *mr = d + tile.t_off + (int64_t)mir * tile.hh;
+    for (int j = 0; j < n && c0 + j < tile.hh; ++j) {
+      dr[c0 + j] = v[j];
+      if (mir >= 0) mr[c0 + j] = -v[j];
+    }
+  }
+};
+
+// After partial sums are written: the last tile of the row block adds them in order.
+__device__ __forceinline__ void ladder_reduce(const LadderTile &tile, int tid, int32_t *counters,
+                                              const int32_t *rowmap, const int32_t *mirror,
+                                              double *d, const double *part) {
+  __shared__ int last;
+  __threadfence();
+  consumers_sync();
+  if (tid == 0) last = (atomicAdd(&counters[tile.group], 1) == tile.nseg - 1);
+  consumers_sync();
+  if (!last) return;
+  __threadfence();
+  const int n = tile.rows * tile.nb;
+  for (int e = tid; e < n; e += kLadderConsumers) {
+    const int u_local = e / tile.nb, col = e - u_local * tile.nb;
+    if (col >= tile.hh) continue;
+    double v = 0.0;
+    for (int sg = 0; sg < tile.nseg; ++sg)
+      v += __ldcg(part + tile.part_base + ((int64_t)sg * tile.bm + u_local) * tile.nb + col);
+    const int u = tile.mt * tile.bm + u_local;
+    const int ab = rowmap[tile.row_off + u], mir = mirror[tile.row_off + u];
+    d[tile.t_off + (int64_t)ab * tile.hh + col] = v;
+    if (mir >= 0) d[tile.t_off + (int64_t)mir * tile.hh + col] = -v;
+  }
+  if (tid == 0) counters[tile.group] = 0;
+}
+
+// Thin channels (nb in {2,4,8}): consumer thread = one packed row, all nb columns.
+// bstage: doubles between consecutive B stages (the producer's layout).
+template <int NB>
+__device__ __forceinline__ bool consume_thin(const LadderTile &tile, const double *As,
+                                             const double *Bs, int bstage, uint64_t *bars,
+                                             int tid, const LadderOut &out, int32_t *err) {
+  const int lane = tid & 31;
+  double acc[NB];
+#pragma unroll
+  for (int j = 0; j < NB; ++j) acc[j] = 0.0;
+  const int nchunks = tile.nks + tile.nkh;
+  for (int c = 0; c < nchunks; ++c) {
+    const int s = c % kStages;
+    if (!mbar_wait(smem_u32(&bars[s]), (c / kStages) & 1)) {
+      atomicOr(err, kErrTimeout);
+      return false;
+    }
+    const double *A = As + s * (kMaxBM * kBK);
+    const double *B = Bs + s * bstage;
+#pragma unroll
+    for (int k = 0; k < kBK; ++k) {
+      const double a = A[swzA(tid, k)];
+      const double2 *bp = reinterpret_cast<const double2 *>(B + k * NB);
+#pragma unroll
+      for (int j = 0; j < NB / 2; ++j) {
+        const double2 b = bp[j];
+        acc[2 * j] = fma(a, b.x, acc[2 * j]);
+        acc[2 * j + 1] = fma(a, b.y, acc[2 * j + 1]);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(smem_u32(&bars[kStages + s]));
+  }
+  out.row(tid, 0, acc, NB);
+  return true;
+}
+
+// Wide channels (nb = 8*CG): consumer thread = ladder_tm(CG) rows (strided by the row-group
+// count) x 8 columns; V values are reused across the CG column groups, T values across rows.
 template <int CG>
-__device__ __forceinline__ void ladder_consume(const LadderTile &tile, const double *As,
-                                               const double *Bs, uint64_t *bars, int tid,
-                                               const int32_t *__restrict__ rowmap,
-                                               const int32_t *__restrict__ mirror,
-                                               double *__restrict__ d, int32_t *err) {
-  constexpr int TM = CG, RG = kLadderConsumers / CG, NB = 8 * CG;
+__device__ __forceinline__ bool consume_wide(const LadderTile &tile, const double *As,
+                                             const double *Bs, int bstage, uint64_t *bars,
+                                             int tid, const LadderOut &out, int32_t *err) {
+  constexpr int TM = ladder_tm(CG), RG = kLadderConsumers / CG, NB = 8 * CG;
   const int rg = tid / CG, cg = tid - rg * CG;
   const bool worker = rg < RG;
   const int lane = tid & 31;
@@ -89,15 +213,15 @@ __device__ __forceinline__ void ladder_consume(const LadderTile &tile, const dou
   for (int i = 0; i < TM; ++i)
 #pragma unroll
     for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
-  const int nchunks = tile.nkc + tile.nkh;
+  const int nchunks = tile.nks + tile.nkh;
   for (int c = 0; c < nchunks; ++c) {
     const int s = c % kStages;
     if (!mbar_wait(smem_u32(&bars[s]), (c / kStages) & 1)) {
       atomicOr(err, kErrTimeout);
-      return;
+      return false;
     }
     const double *A = As + s * (kMaxBM * kBK);
-    const double *B = Bs + s * (kBK * kMaxCG * 8);
+    const double *B = Bs + s * bstage;
     if (worker) {
 #pragma unroll 4
       for (int k = 0; k < kBK; ++k) {
@@ -121,38 +245,29 @@ __device__ __forceinline__ void ladder_consume(const LadderTile &tile, const dou
     __syncwarp();
     if (lane == 0) mbar_arrive(smem_u32(&bars[kStages + s]));
   }
-  if (!worker) return;
-  double *dblk = d + tile.t_off;
+  if (worker) {
 #pragma unroll
-  for (int i = 0; i < TM; ++i) {
-    const int u = tile.mt * tile.bm + rg + i * RG;
-    if (u >= tile.pr) continue;
-    const int ab = rowmap[tile.row_off + u], mir = mirror[tile.row_off + u];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int col = cg * 8 + j;
-      if (col < tile.hh) {
-        dblk[(int64_t)ab * tile.hh + col] = acc[i][j];
-        if (mir >= 0) dblk[(int64_t)mir * tile.hh + col] = -acc[i][j];
-      }
-    }
+    for (int i = 0; i < TM; ++i) out.row(rg + i * RG, cg * 8, acc[i], 8);
   }
+  return true;
 }
 
-// CG_LO..CG_HI: the column-group range a launch handles (separate instantiations keep the
-// register budget of narrow channels independent of the 72-column case).
-template <int CG_LO, int CG_HI>
-__global__ void __launch_bounds__(kLadderThreads, 2)
+// Column classes: CLS 0 = thin (nb <= 8), 1 = mid (nb 16..32), 2 = wide (nb 40..72).  Separate
+// instantiations keep the register budget of narrow channels independent of the 72-column case.
+template <int CLS>
+__global__ void __launch_bounds__(kLadderThreads, CLS == 0 ? 3 : 2)
 pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict__ v_t,
                  const double *__restrict__ t_kt, const double *__restrict__ t_mt,
                  const double *__restrict__ x_t, const int32_t *__restrict__ rowmap,
-                 const int32_t *__restrict__ mirror, double *__restrict__ d, const Control *ctl,
-                 int32_t *err) {
+                 const int32_t *__restrict__ mirror, double *__restrict__ d, double *part,
+                 int32_t *counters, const Control *ctl, int32_t *err) {
   if (skip_iteration(ctl)) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double *As = reinterpret_cast<double *>(smem_raw);
   double *Bs = As + kStages * kMaxBM * kBK;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(Bs + kStages * kBK * kMaxCG * 8);
+  constexpr bool WIDE = CLS > 0;
+  const int bstage = WIDE ? kBK * kMaxNB : kBK * 8;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(Bs + kStages * bstage);
   const LadderTile tile = tiles[blockIdx.x];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -166,9 +281,10 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict_
 
   if (warp == kLadderConsumers / 32) {
     if (lane == 0) {
-      const int nb = 8 * tile.cg;
-      const uint32_t abytes = tile.bm * kBK * 8, bbytes = kBK * nb * 8;
-      const int nchunks = tile.nkc + tile.nkh;
+      const uint32_t abytes = tile.rows * kBK * 8, bbytes = kBK * tile.nb * 8;
+      const int nchunks = tile.nks + tile.nkh;
+      const int64_t vtile = tile.v_base + (int64_t)tile.mt * tile.bm * tile.nkc * kBK;
+      const int64_t ttile = tile.tmt_base + (int64_t)tile.mt * tile.bm * tile.nkh * kBK;
       for (int c = 0; c < nchunks; ++c) {
         const int s = c % kStages;
         if (c >= kStages && !mbar_wait(smem_u32(&bars[kStages + s]), ((c / kStages) - 1) & 1)) {
@@ -176,32 +292,49 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict_
           break;
         }
         const double *asrc, *bsrc;
-        if (c < tile.nkc) {
-          asrc = v_t + tile.v_base + (int64_t)(tile.mt * tile.nkc + c) * tile.bm * kBK;
-          bsrc = t_kt + tile.tkt_base + (int64_t)c * kBK * nb;
+        if (c < tile.nks) {
+          const int kc = tile.kc0 + c;
+          asrc = v_t + vtile + (int64_t)kc * tile.rows * kBK;
+          bsrc = t_kt + tile.tkt_base + (int64_t)kc * kBK * tile.nb;
         } else {
-          const int kh = c - tile.nkc;
-          asrc = t_mt + tile.tmt_base + (int64_t)(tile.mt * tile.nkh + kh) * tile.bm * kBK;
-          bsrc = x_t + tile.xt_base + (int64_t)kh * kBK * nb;
+          const int kh = c - tile.nks;
+          asrc = t_mt + ttile + (int64_t)kh * tile.rows * kBK;
+          bsrc = x_t + tile.xt_base + (int64_t)kh * kBK * tile.nb;
         }
         const uint32_t full = smem_u32(&bars[s]);
         mbar_expect_tx(full, abytes + bbytes);
         bulk_g2s(smem_u32(As + s * kMaxBM * kBK), asrc, abytes, full);
-        bulk_g2s(smem_u32(Bs + s * kBK * kMaxCG * 8), bsrc, bbytes, full);
+        bulk_g2s(smem_u32(Bs + s * bstage), bsrc, bbytes, full);
       }
     }
     return;
   }
   const int tid = threadIdx.x;
-#define CCD_LADDER_CASE(n) \
-  case n: if (n >= CG_LO && n <= CG_HI) ladder_consume<n>(tile, As, Bs, bars, tid, rowmap, mirror, d, err); break;
-  switch (tile.cg) {
-    CCD_LADDER_CASE(1) CCD_LADDER_CASE(2) CCD_LADDER_CASE(3) CCD_LADDER_CASE(4)
-    CCD_LADDER_CASE(5) CCD_LADDER_CASE(6) CCD_LADDER_CASE(7) CCD_LADDER_CASE(8)
-    CCD_LADDER_CASE(9)
-    default: break;
+  const LadderOut out{tile, rowmap, mirror, d, part};
+  bool ok = true;
+  if (!WIDE) {
+    switch (tile.nb) {
+      case 2: ok = consume_thin<2>(tile, As, Bs, bstage, bars, tid, out, err); break;
+      case 4: ok = consume_thin<4>(tile, As, Bs, bstage, bars, tid, out, err); break;
+      default: ok = consume_thin<8>(tile, As, Bs, bstage, bars, tid, out, err); break;
+    }
+  } else {
+#define CCD_WIDE_CASE(n) \
+  case n: ok = consume_wide<n>(tile, As, Bs, bstage, bars, tid, out, err); break;
+    if (CLS == 1) {
+      switch (tile.nb / 8) { CCD_WIDE_CASE(2) CCD_WIDE_CASE(3) CCD_WIDE_CASE(4) default: break; }
+    } else {
+      switch (tile.nb / 8) {
+        CCD_WIDE_CASE(5) CCD_WIDE_CASE(6) CCD_WIDE_CASE(7) CCD_WIDE_CASE(8) CCD_WIDE_CASE(9)
+        default: break;
+      }
+    }
+#undef CCD_WIDE_CASE
   }
-#undef CCD_LADDER_CASE
+  if (tile.nseg > 1) {
+    if (!ok) return;  // a timed-out tile leaves its row block unfinished (error already set)
+    ladder_reduce(tile, tid, counters, rowmap, mirror, d, part);
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -246,23 +379,17 @@ hh_ladder_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ 
     const int idx = tid + q * kHHThreads;
     if (idx < nout) {
       const int kl = idx / hh, ij = idx - kl * hh;
-      double a = 0.0;
-      for (int k = 0; k < rows; ++k) a += Vs[k * hh + kl] * Ts[k * hh + ij];
-      mypart[idx] = a;
+      mypart[idx] = dot4(Vs + kl, hh, Ts + ij, hh, rows);
     }
   }
-  if (tid < rows) {
-    double rr = 0.0;
-    for (int ij = 0; ij < hh; ++ij) rr += Vs[tid * hh + ij] * Ts[tid * hh + ij];
-    r_out[ch.pp_off + tt.k0 + tid] = rr;
-  }
+  if (tid < rows) r_out[ch.pp_off + tt.k0 + tid] = dot4(Vs + tid * hh, 1, Ts + tid * hh, 1, hh);
   __threadfence();
   __syncthreads();
   if (tid == 0) last = (atomicAdd(&counters[tt.ch], 1) == ch.nhht - 1);
   __syncthreads();
   if (!last) return;
   __threadfence();
-  const int nb = 8 * ch.cg;
+  const int nb = ch.nb;
   const double *pbase = part + ch.part_off;
   for (int idx = tid; idx < nout; idx += kHHThreads) {
     double p = 0.0;
@@ -303,16 +430,12 @@ ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restr
   __syncwarp();
   for (int e = lane; e < hp * hp; e += 32) {
     const int i = e / hp, j = e - i * hp;
-    double a = 0.0;
-    for (int k = 0; k < ph; ++k) a += Va[i * ph + k] * Ts[k * hp + j];
-    Ys[e] = 0.5 * a + Ys[e];
+    Ys[e] = 0.5 * dot4(Va + i * ph, 1, Ts + j, hp, ph) + Ys[e];
   }
   __syncwarp();
   for (int e = lane; e < ph * hp; e += 32) {
     const int i = e / hp, j = e - i * hp;
-    double a = 0.0;
-    for (int k = 0; k < hp; ++k) a += Ts[i * hp + k] * Ys[k * hp + j];
-    r_phhp[m.m_off + e] = a;
+    r_phhp[m.m_off + e] = dot4(Ts + i * hp, 1, Ys + j, hp, hp);
   }
 }
 
@@ -335,16 +458,12 @@ ring_kernel(const ModInfo *__restrict__ mods, const double *__restrict__ v_hpph,
   __syncthreads();
   for (int e = tid; e < hp * hp; e += kRingThreads) {
     const int i = e / hp, j = e - i * hp;
-    double a = 0.0;
-    for (int k = 0; k < ph; ++k) a += Va[i * ph + k] * Ts[k * hp + j];
-    Ys[e] = 0.5 * a + Ys[e];
+    Ys[e] = 0.5 * dot4(Va + i * ph, 1, Ts + j, hp, ph) + Ys[e];
   }
   __syncthreads();
   for (int e = tid; e < ph * hp; e += kRingThreads) {
     const int i = e / hp, j = e - i * hp;
-    double a = 0.0;
-    for (int k = 0; k < hp; ++k) a += Ts[i * hp + k] * Ys[k * hp + j];
-    r_phhp[m.m_off + e] = a;
+    r_phhp[m.m_off + e] = dot4(Ts + i * hp, 1, Ys + j, hp, hp);
   }
 }
 
@@ -410,8 +529,18 @@ __global__ void onebody_fused_kernel(int np, int nsp, const int64_t *__restrict_
   if (w >= nsp) return;
   const bool hole = w < np;
   const double *src = hole ? s : r;
-  double v = 0.0;
-  for (int64_t e = list_off[w] + lane; e < list_off[w + 1]; e += 32) v += src[list[e]];
+  double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+  const int64_t hi = list_off[w + 1];
+  int64_t e = list_off[w] + lane;
+  for (; e + 96 < hi; e += 128) {
+    const int32_t i0 = list[e], i1 = list[e + 32], i2 = list[e + 64], i3 = list[e + 96];
+    v0 += src[i0];
+    v1 += src[i1];
+    v2 += src[i2];
+    v3 += src[i3];
+  }
+  for (; e < hi; e += 32) v0 += src[list[e]];
+  double v = (v0 + v1) + (v2 + v3);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   if (lane == 0) {
@@ -421,16 +550,18 @@ __global__ void onebody_fused_kernel(int np, int nsp, const int64_t *__restrict_
 }
 
 // Writes one amplitude into the ladder operand tiles: the B tiles of V T (rows c<d) and the A
-// tiles of T X (rows a<=b).  pk_idx[AB] = (K index or -1, packed row or -1).
+// tiles of T X (rows a<=b, compact last row tile).  pk_idx[AB] = (K index or -1, packed row
+// or -1).
 __device__ __forceinline__ void write_t_tiles(const ChanInfo &ch, const int2 *__restrict__ pk_idx,
                                               int ab, int ij, double t, double *t_kt,
                                               double *t_mt) {
   const int2 q = pk_idx[ch.pp_off + ab];
-  const int nb = 8 * ch.cg;
-  if (q.x >= 0) t_kt[ch.tkt_base + (int64_t)(q.x / kBK) * kBK * nb + (q.x % kBK) * nb + ij] = t;
-  if (q.y >= 0)
-    t_mt[ch.tmt_base + (int64_t)((q.y / ch.bm) * ch.nkh + ij / kBK) * ch.bm * kBK +
-         swzA(q.y % ch.bm, ij % kBK)] = t;
+  if (q.x >= 0) t_kt[ch.tkt_base + (int64_t)(q.x / kBK) * kBK * ch.nb + (q.x % kBK) * ch.nb + ij] = t;
+  if (q.y >= 0) {
+    const int mt = q.y / ch.bm, rows = min(ch.bm, ch.pr - mt * ch.bm);
+    t_mt[ch.tmt_base + (int64_t)mt * ch.bm * ch.nkh * kBK + (int64_t)(ij / kBK) * rows * kBK +
+         swzA(q.y - mt * ch.bm, ij % kBK)] = t;
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -444,6 +575,8 @@ __device__ __forceinline__ void write_t_tiles(const ChanInfo &ch, const int2 *__
 // ------------------------------------------------------------------------------------------
 constexpr int kAsmThreads = 256;
 constexpr int kAsmPerThread = 1;
+__device__ __forceinline__ void energy_reduce(const double *epart, int n, Control *ctl, int flags,
+                                              double *e_out);
 
 __global__ void __launch_bounds__(kAsmThreads)
 assemble_fused_kernel(const ElemRange *__restrict__ ranges, const ChanInfo *__restrict__ chans,
@@ -457,9 +590,10 @@ assemble_fused_kernel(const ElemRange *__restrict__ ranges, const ChanInfo *__re
                       const double *__restrict__ yp, const double *__restrict__ eps, int np,
                       double *tbuf0, double *tbuf1, double *__restrict__ old_phhp,
                       double *__restrict__ t_kt, double *__restrict__ t_mt,
-                      double *__restrict__ epart, const Control *ctl) {
+                      double *__restrict__ epart, int32_t *ticket, Control *ctl) {
   if (skip_iteration(ctl)) return;
   __shared__ double scratch[32];
+  __shared__ int last;
   const ElemRange rg = ranges[blockIdx.x];
   const ChanInfo ch = chans[rg.ch];
   const double *t_old = ctl->parity ? tbuf1 : tbuf0;
@@ -493,7 +627,17 @@ assemble_fused_kernel(const ElemRange *__restrict__ ranges, const ChanInfo *__re
     corr += v * value;
   }
   const double sum = block_sum<kAsmThreads>(corr, scratch);
-  if (threadIdx.x == 0) epart[blockIdx.x] = sum;
+  // The last CTA to finish sums the partials and applies the stop rule (no extra launch).
+  if (threadIdx.x == 0) {
+    epart[blockIdx.x] = sum;
+    __threadfence();
+    last = (atomicAdd(ticket, 1) == (int)gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  energy_reduce(epart, gridDim.x, ctl, 3, nullptr);
+  if (threadIdx.x == 0) *ticket = 0;
 }
 
 // Table path assembly: exactly calcChannelT2_pphh over the eight gathered chains.
@@ -574,16 +718,16 @@ __global__ void map_to_kernel(const ElemRange *__restrict__ ranges, const ChanIn
   }
 }
 
-// Sum of the per-CTA energy partials (Neumaier-compensated, fixed order), then the
-// reference's stop rule on the device.  flags: 1 = flip the amplitude buffer parity,
-// 2 = count this as an iteration of the solve loop.
-__global__ void energy_kernel(const double *__restrict__ epart, int n, Control *ctl, int flags,
-                              double *e_out) {
-  if (skip_iteration(ctl)) return;
-  __shared__ double ss[1024], cs[1024];
+// Sum of the per-CTA energy partials (Neumaier-compensated, fixed order) by one block of
+// kEnergyThreads threads, then the reference's stop rule on the device.  flags: 1 = flip the
+// amplitude buffer parity, 2 = count this as an iteration of the solve loop.
+constexpr int kEnergyThreads = 256;
+__device__ __forceinline__ void energy_reduce(const double *epart, int n, Control *ctl, int flags,
+                                              double *e_out) {
+  __shared__ double ss[kEnergyThreads], cs[kEnergyThreads];
   double s = 0.0, c = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const double x = epart[i];
+  for (int i = threadIdx.x; i < n; i += kEnergyThreads) {
+    const double x = __ldcg(epart + i);
     const double t = s + x;
     c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
     s = t;
@@ -591,7 +735,7 @@ __global__ void energy_kernel(const double *__restrict__ epart, int n, Control *
   ss[threadIdx.x] = s;
   cs[threadIdx.x] = c;
   __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+  for (int w = kEnergyThreads / 2; w > 0; w >>= 1) {
     if (threadIdx.x < w) {
       const double a = ss[threadIdx.x], b = ss[threadIdx.x + w];
       const double t = a + b;
@@ -619,6 +763,12 @@ __global__ void energy_kernel(const double *__restrict__ epart, int n, Control *
     }
     if (flags & 1) ctl->parity ^= 1;
   }
+}
+
+__global__ void __launch_bounds__(kEnergyThreads)
+energy_kernel(const double *__restrict__ epart, int n, Control *ctl, int flags, double *e_out) {
+  if (skip_iteration(ctl)) return;
+  energy_reduce(epart, n, ctl, flags, e_out);
 }
 
 }  // namespace ccd

@@ -1,0 +1,95 @@
+// Device-side setup kernels run once by ccdgpu_create: they turn the reference-layout inputs
+// (uploaded as they are) into the solver's layouts, so that create does no O(V) host work.
+#pragma once
+
+#include <cstdint>
+
+#include "ccd_device.cuh"
+
+namespace ccd {
+
+// ChainIndex (Chain.hpp:7-11) as it arrives from the host: three size_t.
+struct RawIndex {
+  uint64_t channel, row, column;
+};
+
+// V_hhpp (hh x pp per channel) -> V_pphh (pp x hh), aligned with the t2 layout.
+__global__ void transpose_hhpp_kernel(const ElemRange *__restrict__ ranges,
+                                      const ChanInfo *__restrict__ chans,
+                                      const double *__restrict__ raw, double *__restrict__ out) {
+  const ElemRange rg = ranges[blockIdx.x];
+  const ChanInfo ch = chans[rg.ch];
+  for (int64_t e = rg.e0 + threadIdx.x; e < rg.e1; e += blockDim.x) {
+    const int64_t loc = e - ch.t_off;
+    const int ab = (int)(loc / ch.hh), ij = (int)(loc - (int64_t)ab * ch.hh);
+    out[e] = raw[ch.t_off + (int64_t)ij * ch.pp + ab];
+  }
+}
+
+// Packed, tiled V_pppp: one CTA per packed row u of one channel.
+// items[i] = (active channel, packed row); kcol[pk_off + w] = pp index of the w-th c<d pair.
+__global__ void tile_v_kernel(const ChanInfo *__restrict__ chans, const int2 *__restrict__ items,
+                              const int32_t *__restrict__ rowmap, const int32_t *__restrict__ kcol,
+                              const int64_t *__restrict__ vraw_off, const double *__restrict__ vraw,
+                              double *__restrict__ v_t) {
+  const int2 it = items[blockIdx.x];
+  const ChanInfo ch = chans[it.x];
+  const int u = it.y;
+  const int ab = rowmap[ch.row_off + u];
+  const double *src = vraw + vraw_off[it.x] + (int64_t)ab * ch.pp;
+  const int mt = u / ch.bm, rows = min(ch.bm, ch.pr - mt * ch.bm);
+  const int64_t tb = ch.vkt_base + (int64_t)mt * ch.bm * ch.nkc * kBK;
+  for (int w = threadIdx.x; w < ch.pk; w += blockDim.x)
+    v_t[tb + (int64_t)(w / kBK) * rows * kBK + swzA(u - mt * ch.bm, w % kBK)] = src[kcol[ch.pk_off + w]];
+}
+
+// The eight loadMaps tables -> int32 flat offsets into their target chains, with range checks
+// and, for the five tables that are also scatter targets (mapToDistributed), hit counts that
+// check_counts_kernel then requires to be exactly one.
+struct TableGeometry {
+  const int64_t *o_h;      // [np+1] hpp chain offsets
+  const int64_t *o_p;      // [npart+1] phh chain offsets
+  const int64_t *o_m;      // [nch+1] phhp chain offsets
+  const int2 *mod_dims;    // [nch] (ph', hp')
+  uint64_t nch, np, npart;
+};
+
+__global__ void convert_tables_kernel(const ElemRange *__restrict__ ranges, const RawIndex *raw,
+                                      int64_t n_t, TableGeometry geo, int32_t *__restrict__ flat,
+                                      int32_t *__restrict__ counts, int32_t *err) {
+  const ElemRange rg = ranges[blockIdx.x];
+  for (int64_t e = rg.e0 + threadIdx.x; e < rg.e1; e += blockDim.x) {
+#pragma unroll 1
+    for (int k = 0; k < 8; ++k) {
+      const RawIndex x = raw[(int64_t)k * n_t + e];
+      int64_t f = -1;
+      if (k <= 1) {
+        if (x.channel < geo.np && x.column == 0 &&
+            x.row < (uint64_t)(geo.o_h[x.channel + 1] - geo.o_h[x.channel]))
+          f = geo.o_h[x.channel] + (int64_t)x.row;
+      } else if (k <= 3) {
+        if (x.channel < geo.npart && x.row == 0 &&
+            x.column < (uint64_t)(geo.o_p[x.channel + 1] - geo.o_p[x.channel]))
+          f = geo.o_p[x.channel] + (int64_t)x.column;
+      } else if (x.channel < geo.nch) {
+        const int2 md = geo.mod_dims[x.channel];
+        if (x.row < (uint64_t)md.x && x.column < (uint64_t)md.y)
+          f = geo.o_m[x.channel] + (int64_t)x.row * md.y + (int64_t)x.column;
+      }
+      if (f < 0 || f >= n_t) {
+        atomicOr(err, kErrBadIndex);
+        f = 0;
+      }
+      flat[(int64_t)k * n_t + e] = (int32_t)f;
+      if (k <= 4) atomicAdd(&counts[(int64_t)k * n_t + f], 1);
+    }
+  }
+}
+
+__global__ void check_counts_kernel(const int32_t *__restrict__ counts, int64_t n, int32_t *err) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    if (counts[i] != 1) atomicOr(err, kErrBadIndex);
+}
+
+}  // namespace ccd

@@ -21,6 +21,7 @@
 
 #include "ccd_device.cuh"
 #include "ccd_kernels.cuh"
+#include "ccd_setup.cuh"
 #include "ccdgpu.h"
 
 using namespace ccd;
@@ -36,13 +37,14 @@ struct DevBuf {
 
 struct ccdgpu_handle {
   ccdgpu_options opt{};
-  cudaStream_t s0 = nullptr, s1 = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t s0 = nullptr, s1 = nullptr, s2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork2 = nullptr, ev_join2 = nullptr;
   cudaEvent_t ev[10] = {};
   uint64_t nch = 0, nsp = 0, np = 0, npart = 0;
   int64_t n_t = 0, n_m = 0, n_h = 0, n_p = 0;
-  int n_act = 0, n_mod = 0, n_mod_small = 0, n_tiles = 0, n_tiles_narrow = 0, n_hh_tiles = 0,
-      n_ranges = 0;
+  int n_act = 0, n_mod = 0, n_mod_small = 0, n_tiles = 0, n_hh_tiles = 0, n_ranges = 0;
+  int n_cls[3] = {0, 0, 0};  // pp-ladder tiles per column class (thin, mid, wide), in that order
+  size_t ladder_smem_thin = 0;
   size_t ladder_smem = 0, ring_smem = 0, hh_smem = 0;
   bool have_3body = false;
   std::vector<DevBuf> allocs;
@@ -51,9 +53,9 @@ struct ccdgpu_handle {
   ModInfo *mods = nullptr;        // small channels first (n_mod_small), then the others
   LadderTile *tiles = nullptr;
   HHTile *hh_tiles = nullptr;
-  int32_t *rowmap = nullptr, *mirror = nullptr, *counters = nullptr;
+  int32_t *rowmap = nullptr, *mirror = nullptr, *counters = nullptr, *lcounters = nullptr;
   int2 *pk_idx = nullptr;
-  double *part = nullptr;
+  double *part = nullptr, *lpart = nullptr;
   ElemRange *ranges = nullptr;
   int2 *pp_pairs = nullptr, *hh_pairs = nullptr;
   int32_t *pp_swap = nullptr, *hh_swap = nullptr;
@@ -72,6 +74,7 @@ struct ccdgpu_handle {
   double *gath = nullptr;
   Control *ctl = nullptr;
   Control *h_ctl = nullptr;  // pinned mirror
+  int32_t *ticket = nullptr;  // assembly's last-CTA ticket
   double *e_out = nullptr;
   int32_t *err = nullptr;
 
@@ -79,7 +82,8 @@ struct ccdgpu_handle {
   int64_t kernels_per_graph = 0;
   bool profiling = false;
   ccdgpu_profile prof{};
-  double flops = 0, v_bytes = 0, ladder_flops = 0;
+  double flops = 0, v_bytes = 0, v_packed_bytes = 0, ladder_flops = 0, ladder_bytes = 0;
+  int64_t n_tkt = 0, n_tmt = 0;
   int64_t launches = 0;
 };
 
@@ -100,24 +104,6 @@ int cuda_status(cudaError_t e) {
       return cuda_status(e_);                 \
     }                                         \
   } while (0)
-
-template <typename T>
-int dalloc(ccdgpu_handle *h, T **p, size_t count, bool zero = true) {
-  size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-  void *q = nullptr;
-  CK(cudaMalloc(&q, bytes));
-  h->allocs.push_back({q, bytes});
-  if (zero) CK(cudaMemsetAsync(q, 0, bytes, h->s0));
-  *p = static_cast<T *>(q);
-  return CCDGPU_OK;
-}
-template <typename T>
-int upload(ccdgpu_handle *h, T **p, const std::vector<T> &v) {
-  int rc = dalloc(h, p, v.size(), false);
-  if (rc) return rc;
-  if (!v.empty()) CK(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
-  return CCDGPU_OK;
-}
 
 int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
@@ -142,16 +128,72 @@ void release(ccdgpu_handle *h) {
     if (e) cudaEventDestroy(e);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
   if (h->ev_join) cudaEventDestroy(h->ev_join);
+  if (h->ev_fork2) cudaEventDestroy(h->ev_fork2);
+  if (h->ev_join2) cudaEventDestroy(h->ev_join2);
+  if (h->s2) cudaStreamDestroy(h->s2);
   if (h->s1) cudaStreamDestroy(h->s1);
   if (h->s0) cudaStreamDestroy(h->s0);
+}
+
+// Bump allocator over one device allocation (256-byte aligned pieces).
+struct Arena {
+  size_t used = 0;
+  std::vector<std::pair<void **, size_t>> reqs;
+  template <typename T>
+  void add(T **p, size_t count) {
+    size_t bytes = (std::max<size_t>(count, 1) * sizeof(T) + 255) & ~size_t(255);
+    reqs.push_back({reinterpret_cast<void **>(p), used});
+    used += bytes;
+  }
+  int commit(ccdgpu_handle *h) {
+    void *base = nullptr;
+    CK(cudaMalloc(&base, used));
+    h->allocs.push_back({base, used});
+    CK(cudaMemsetAsync(base, 0, used, h->s0));
+    for (auto &r : reqs) *r.first = static_cast<char *>(base) + r.second;
+    return CCDGPU_OK;
+  }
+};
+
+// Copies per-channel host blocks (block k of `count[k]` elements at src[k]) to consecutive
+// device positions, one cudaMemcpy per run of blocks that are adjacent in host memory.
+template <typename T>
+int upload_runs(ccdgpu_handle *h, T *dst, const std::vector<const T *> &src,
+                const std::vector<int64_t> &count) {
+  const T *run_src = nullptr;
+  int64_t run_len = 0, pos = 0, run_dst = 0;
+  auto flush = [&]() -> int {
+    if (run_len) CK(cudaMemcpyAsync(dst + run_dst, run_src, run_len * sizeof(T),
+                                    cudaMemcpyHostToDevice, h->s0));
+    return CCDGPU_OK;
+  };
+  for (size_t k = 0; k < src.size(); k++) {
+    if (!count[k]) continue;
+    if (run_len && src[k] == run_src + run_len) {
+      run_len += count[k];
+    } else {
+      int rc = flush();
+      if (rc) return rc;
+      run_src = src[k];
+      run_len = count[k];
+      run_dst = pos;
+    }
+    pos += count[k];
+  }
+  return flush();
 }
 
 int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   const uint64_t nch = P->n_channels, nsp = P->n_sp, np = P->n_particles;
   h->nch = nch; h->nsp = nsp; h->np = np; h->npart = nsp - np;
   const ccdgpu_channel_dims *D = P->chan_dims, *MD = P->chan_mod_dims;
+  const bool on_the_fly = h->opt.v_mode == CCDGPU_V_ON_THE_FLY;
+  if (on_the_fly) return CCDGPU_ERR_UNSUPPORTED;  // generated V_pppp: not built yet
+  if (!P->v_pppp || !P->v_hhpp || !P->v_hhhh || !P->v_hpph_mod || !P->v_hphp_mod)
+    return CCDGPU_ERR_INVALID_ARGUMENT;
+  for (int k = 0; k < 8; k++)
+    if (!P->maps[k]) return CCDGPU_ERR_INVALID_ARGUMENT;
 
-  // Regular channels carrying amplitudes, in channel order.
   std::vector<int64_t> o_t(nch + 1, 0), o_m(nch + 1, 0);
   for (uint64_t c = 0; c < nch; c++) {
     o_t[c + 1] = o_t[c] + (int64_t)(D[c].pp * D[c].hh);
@@ -160,41 +202,62 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   h->n_t = o_t[nch];
   h->n_m = o_m[nch];
   if (h->n_t != h->n_m) return CCDGPU_ERR_BAD_TABLE;  // pphh <-> phhp must be a bijection
-  if (h->n_t >= (int64_t)INT32_MAX) return CCDGPU_ERR_UNSUPPORTED;
+  if (h->n_t >= (int64_t)INT32_MAX / 2) return CCDGPU_ERR_UNSUPPORTED;
+  const int64_t n_t = h->n_t;
 
+  // ---- per-channel metadata (O(sum pp) host work) ----
   std::vector<ChanInfo> chans;
-  std::vector<int64_t> act_of(nch, -1);
-  // Packed rows (a<=b) and K pairs (c<d) per channel, from the sorted pp map.
-  std::vector<int32_t> rowmap, mirror;
-  std::vector<int2> pk_idx;
+  std::vector<uint64_t> act_chan;  // reference channel of each active channel
+  std::vector<int32_t> rowmap, mirror, kcol;
+  std::vector<int2> pk_idx, pp_pairs, hh_pairs, vrows;
+  std::vector<int32_t> pp_swap, hh_swap;
   std::vector<HHTile> hh_tiles;
+  std::vector<std::vector<int32_t>> seg(nsp);
   int64_t pp_tot = 0, hh_tot = 0, x_tot = 0, tkt = 0, tmt = 0, xt = 0, vt = 0, part_tot = 0;
+  int64_t vraw_tot = 0;
+  std::vector<int64_t> vraw_off;
+  int maxhh = 1;
   for (uint64_t c = 0; c < nch; c++) {
     const int64_t pp = D[c].pp, hh = D[c].hh;
     if (!pp || !hh) continue;
     if (hh > 8 * kMaxCG || pp > (1 << 20)) return CCDGPU_ERR_UNSUPPORTED;
-    const ccdgpu_pair *pm = P->chan_maps[c].pp;
-    if (!pm || !P->chan_maps[c].hh) return CCDGPU_ERR_INVALID_ARGUMENT;
+    const ccdgpu_pair *pm = P->chan_maps[c].pp, *hm = P->chan_maps[c].hh;
+    if (!pm || !hm) return CCDGPU_ERR_INVALID_ARGUMENT;
     ChanInfo ci{};
     ci.pp = (int)pp; ci.hh = (int)hh;
-    ci.cg = (int)ceil_div(hh, 8);
-    ci.bm = ladder_bm(ci.cg);
+    ci.nb = ladder_nb((int)hh);
+    ci.bm = ladder_bm(ci.nb);
     ci.row_off = (int64_t)rowmap.size();
+    ci.pk_off = (int64_t)kcol.size();
+    ci.pp_off = pp_tot; ci.hh_off = hh_tot; ci.x_off = x_tot;
+    const int ai = (int)chans.size();
     int pr = 0, pk = 0;
     for (int k = 0; k < ci.pp; k++) {
+      const uint64_t a = pm[k].p, b = pm[k].q;
+      if (a < np || b < np || a >= nsp || b >= nsp) return CCDGPU_ERR_BAD_TABLE;
+      const int sw = find_pair(pm, ci.pp, b, a);
+      if (sw < 0) return CCDGPU_ERR_BAD_TABLE;
+      pp_pairs.push_back(make_int2((int)a, (int)b));
+      pp_swap.push_back(sw);
+      seg[a].push_back((int32_t)(pp_tot + k));
       int2 q = make_int2(-1, -1);
-      if (pm[k].p < pm[k].q) q.x = pk++;
-      if (pm[k].p <= pm[k].q) {
+      if (a < b) { q.x = pk++; kcol.push_back(k); }
+      if (a <= b) {
         q.y = pr++;
         rowmap.push_back(k);
-        int mir = -1;
-        if (pm[k].p < pm[k].q) {
-          mir = find_pair(pm, ci.pp, pm[k].q, pm[k].p);
-          if (mir < 0) return CCDGPU_ERR_BAD_TABLE;
-        }
-        mirror.push_back(mir);
+        mirror.push_back(a < b ? sw : -1);
+        vrows.push_back(make_int2(ai, q.y));
       }
       pk_idx.push_back(q);
+    }
+    for (int k = 0; k < ci.hh; k++) {
+      const uint64_t i = hm[k].p, j = hm[k].q;
+      if (i >= np || j >= np) return CCDGPU_ERR_BAD_TABLE;
+      const int sw = find_pair(hm, ci.hh, j, i);
+      if (sw < 0) return CCDGPU_ERR_BAD_TABLE;
+      hh_pairs.push_back(make_int2((int)i, (int)j));
+      hh_swap.push_back(sw);
+      seg[i].push_back((int32_t)(hh_tot + k));
     }
     ci.pr = pr; ci.pk = pk;
     ci.nkc = (int)ceil_div(pk, kBK);
@@ -202,67 +265,47 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     ci.nmt = (int)ceil_div(pr, ci.bm);
     ci.nhht = (int)ceil_div(pp, kHHRows);
     ci.t_off = o_t[c];
-    ci.pp_off = pp_tot; ci.hh_off = hh_tot; ci.x_off = x_tot;
     ci.tkt_base = tkt; ci.tmt_base = tmt; ci.xt_base = xt; ci.vkt_base = vt;
     ci.part_off = part_tot;
     ci.hht0 = (int64_t)hh_tiles.size();
-    const int nb = 8 * ci.cg;
+    const int nb = ci.nb;
     pp_tot += pp; hh_tot += hh; x_tot += hh * hh;
     tkt += (int64_t)ci.nkc * kBK * nb;
-    tmt += (int64_t)ci.nmt * ci.nkh * ci.bm * kBK;
+    tmt += (int64_t)ci.nkh * ci.pr * kBK;  // compact row tiles
     xt += (int64_t)ci.nkh * kBK * nb;
-    vt += (int64_t)ci.nmt * ci.nkc * ci.bm * kBK;
+    vt += (int64_t)ci.nkc * ci.pr * kBK;
     part_tot += (int64_t)ci.nhht * hh * hh;
-    act_of[c] = (int64_t)chans.size();
-    for (int t = 0; t < ci.nhht; t++) hh_tiles.push_back({(int32_t)chans.size(), t * kHHRows, t, 0});
+    vraw_off.push_back(vraw_tot);
+    vraw_tot += pp * pp;
+    maxhh = std::max<int>(maxhh, (int)hh);
+    for (int t = 0; t < ci.nhht; t++) hh_tiles.push_back({ai, t * kHHRows, t, 0});
     chans.push_back(ci);
+    act_chan.push_back(c);
   }
   h->n_act = (int)chans.size();
   h->n_hh_tiles = (int)hh_tiles.size();
-
-  // Pair tables, swaps and one-body segment lists.
-  std::vector<int2> pp_pairs(pp_tot), hh_pairs(hh_tot);
-  std::vector<int32_t> pp_swap(pp_tot), hh_swap(hh_tot);
-  std::vector<std::vector<int32_t>> seg(nsp);
-  for (uint64_t c = 0; c < nch; c++) {
-    if (act_of[c] < 0) continue;
-    const ChanInfo &ci = chans[act_of[c]];
-    const ccdgpu_pair *pp = P->chan_maps[c].pp, *hh = P->chan_maps[c].hh;
-    if (!pp || !hh) return CCDGPU_ERR_INVALID_ARGUMENT;
-    for (int k = 0; k < ci.pp; k++) {
-      if (pp[k].p < np || pp[k].q < np || pp[k].p >= nsp || pp[k].q >= nsp) return CCDGPU_ERR_BAD_TABLE;
-      pp_pairs[ci.pp_off + k] = make_int2((int)pp[k].p, (int)pp[k].q);
-      int sw = find_pair(pp, ci.pp, pp[k].q, pp[k].p);
-      if (sw < 0) return CCDGPU_ERR_BAD_TABLE;
-      pp_swap[ci.pp_off + k] = sw;
-      seg[pp[k].p].push_back((int32_t)(ci.pp_off + k));
-    }
-    for (int k = 0; k < ci.hh; k++) {
-      if (hh[k].p >= np || hh[k].q >= np) return CCDGPU_ERR_BAD_TABLE;
-      hh_pairs[ci.hh_off + k] = make_int2((int)hh[k].p, (int)hh[k].q);
-      int sw = find_pair(hh, ci.hh, hh[k].q, hh[k].p);
-      if (sw < 0) return CCDGPU_ERR_BAD_TABLE;
-      hh_swap[ci.hh_off + k] = sw;
-      seg[hh[k].p].push_back((int32_t)(ci.hh_off + k));
-    }
-  }
   std::vector<int64_t> list_off(nsp + 1, 0);
   for (uint64_t w = 0; w < nsp; w++) list_off[w + 1] = list_off[w] + (int64_t)seg[w].size();
   std::vector<int32_t> list(list_off[nsp]);
   for (uint64_t w = 0; w < nsp; w++) std::copy(seg[w].begin(), seg[w].end(), list.begin() + list_off[w]);
 
-  // Modified channels.
+  // Modified channels: small ones (one warp each) first.
   std::vector<ModInfo> mods, mods_big;
-  std::vector<int64_t> mod_y(nch, -1);
+  std::vector<int2> mod_dims(nch);
   int64_t y_tot = 0;
   size_t ring_smem = 0;
+  std::vector<const double *> src_hpph, src_hphp;
+  std::vector<int64_t> cnt_hpph, cnt_hphp;
   for (uint64_t c = 0; c < nch; c++) {
     const int64_t ph = MD[c].ph, hp = MD[c].hp;
+    mod_dims[c] = make_int2((int)ph, (int)hp);
     if (!ph || !hp) continue;
+    if (!P->v_hpph_mod[c] || !P->v_hphp_mod[c]) return CCDGPU_ERR_INVALID_ARGUMENT;
     ModInfo m{};
     m.ph = (int)ph; m.hp = (int)hp; m.m_off = o_m[c]; m.y_off = y_tot;
-    mod_y[c] = y_tot;
     y_tot += hp * hp;
+    src_hpph.push_back(P->v_hpph_mod[c]); cnt_hpph.push_back(ph * hp);
+    src_hphp.push_back(P->v_hphp_mod[c]); cnt_hphp.push_back(hp * hp);
     if (ph <= kRingSmall && hp <= kRingSmall) {
       mods.push_back(m);
     } else {
@@ -275,137 +318,63 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   h->n_mod = (int)mods.size();
   h->ring_smem = ring_smem;
 
-  // Three-body chain offsets.
   std::vector<int64_t> o_h(np + 1, 0), o_p(h->npart + 1, 0);
   for (uint64_t k = 0; k < np; k++) o_h[k + 1] = o_h[k] + (int64_t)P->three_body_dims[k].hpp;
   for (uint64_t a = 0; a < h->npart; a++)
     o_p[a + 1] = o_p[a] + (int64_t)P->three_body_dims[np + a].phh;
   h->n_h = o_h[np];
   h->n_p = o_p[h->npart];
-
-  // Remap tables -> flat int32 offsets, with range and bijection checks.
-  const int64_t n_t = h->n_t;
-  std::vector<int32_t> flat((size_t)8 * n_t);
-  int bad = 0;
-  for (int k = 0; k < 8; k++) {
-    if (!P->maps[k]) return CCDGPU_ERR_INVALID_ARGUMENT;
-#pragma omp parallel for schedule(dynamic) reduction(| : bad)
-    for (int64_t ci = 0; ci < (int64_t)nch; ci++) {
-      const uint64_t c = (uint64_t)ci;
-      const int64_t n = o_t[c + 1] - o_t[c];
-      if (!n) continue;
-      const ccdgpu_chain_index *m = P->maps[k][c];
-      if (!m) { bad |= 1; continue; }
-      for (int64_t e = 0; e < n; e++) {
-        const uint64_t ch = m[e].channel, row = m[e].row, col = m[e].column;
-        int64_t f = -1;
-        if (k <= 1) {
-          if (ch < np && col == 0 && row < P->three_body_dims[ch].hpp) f = o_h[ch] + (int64_t)row;
-        } else if (k <= 3) {
-          if (ch < h->npart && row == 0 && col < P->three_body_dims[np + ch].phh) f = o_p[ch] + (int64_t)col;
-        } else {
-          if (ch < nch && row < MD[ch].ph && col < MD[ch].hp) f = o_m[ch] + (int64_t)(row * MD[ch].hp + col);
-        }
-        if (f < 0) { bad |= 1; continue; }
-        flat[(size_t)k * n_t + o_t[c] + e] = (int32_t)f;
-      }
-    }
-  }
-  if (bad) return CCDGPU_ERR_BAD_TABLE;
-  // Scatter targets must be hit exactly once (Chain::mapToDistributed writes every slot).
-  {
-    const int scat[5] = {CCDGPU_MAP_IAB_J, CCDGPU_MAP_JAB_I, CCDGPU_MAP_A_BIJ, CCDGPU_MAP_B_AIJ,
-                         CCDGPU_MAP_AI_JB};
-    const int64_t tgt[5] = {h->n_h, h->n_h, h->n_p, h->n_p, h->n_m};
-    for (int q = 0; q < 5; q++) {
-      if (tgt[q] != n_t) return CCDGPU_ERR_BAD_TABLE;
-      std::vector<uint8_t> hit(n_t, 0);
-      const int32_t *f = &flat[(size_t)scat[q] * n_t];
-      for (int64_t e = 0; e < n_t; e++) {
-        if (hit[f[e]]) return CCDGPU_ERR_BAD_TABLE;
-        hit[f[e]] = 1;
-      }
-    }
-  }
-
-  // V blocks.
-  std::vector<double> v_pphh(n_t), v_hhhh(x_tot), v_t(vt, 0.0), v_hpph(h->n_m), v_hphp(y_tot);
-  const bool on_the_fly = h->opt.v_mode == CCDGPU_V_ON_THE_FLY;
-  if (on_the_fly) return CCDGPU_ERR_UNSUPPORTED;  // generated V_pppp: not built yet
-  if (!P->v_pppp || !P->v_hhpp || !P->v_hhhh || !P->v_hpph_mod || !P->v_hphp_mod)
-    return CCDGPU_ERR_INVALID_ARGUMENT;
-  bad = 0;
-#pragma omp parallel for schedule(dynamic) reduction(| : bad)
-  for (int64_t ci = 0; ci < (int64_t)nch; ci++) {
-    const uint64_t c = (uint64_t)ci;
-    if (act_of[c] < 0) continue;
-    const ChanInfo &a = chans[act_of[c]];
-    const double *vx = P->v_hhpp[c], *vh = P->v_hhhh[c], *vp = P->v_pppp[c];
-    if (!vx || !vh || !vp) { bad |= 1; continue; }
-    for (int ij = 0; ij < a.hh; ij++)
-      for (int ab = 0; ab < a.pp; ab++) v_pphh[a.t_off + (int64_t)ab * a.hh + ij] = vx[(int64_t)ij * a.pp + ab];
-    std::memcpy(&v_hhhh[a.x_off], vh, sizeof(double) * a.hh * a.hh);
-    // Packed V tiles: rows a<=b (rowmap), columns c<d (pk_idx.x), zero padding elsewhere.
-    std::vector<int32_t> kcol(a.pk);
-    for (int k = 0; k < a.pp; k++)
-      if (pk_idx[a.pp_off + k].x >= 0) kcol[pk_idx[a.pp_off + k].x] = k;
-    for (int u = 0; u < a.pr; u++) {
-      const int ab = rowmap[a.row_off + u];
-      const int64_t tb = a.vkt_base + (int64_t)(u / a.bm) * a.nkc * a.bm * kBK;
-      for (int w = 0; w < a.pk; w++)
-        v_t[tb + (int64_t)(w / kBK) * a.bm * kBK + swzA(u % a.bm, w % kBK)] =
-            vp[(int64_t)ab * a.pp + kcol[w]];
-    }
-  }
-  if (bad) return CCDGPU_ERR_INVALID_ARGUMENT;
-  for (uint64_t c = 0; c < nch; c++) {
-    const int64_t ph = MD[c].ph, hp = MD[c].hp;
-    if (!ph || !hp) continue;
-    const double *va = P->v_hpph_mod[c], *vb = P->v_hphp_mod[c];
-    if (!va || !vb) return CCDGPU_ERR_INVALID_ARGUMENT;
-    std::memcpy(&v_hpph[o_m[c]], va, sizeof(double) * ph * hp);
-    std::memcpy(&v_hphp[mod_y[c]], vb, sizeof(double) * hp * hp);
-  }
-  std::vector<double> v_h_hpp, v_phh_p;
+  if (h->n_h != n_t || h->n_p != n_t) return CCDGPU_ERR_BAD_TABLE;
   h->have_3body = P->v_h_hpp && P->v_phh_p;
-  if (h->have_3body) {
-    v_h_hpp.resize(h->n_h);
-    v_phh_p.resize(h->n_p);
-    for (uint64_t k = 0; k < np; k++) {
-      const int64_t n = o_h[k + 1] - o_h[k];
-      if (n && !P->v_h_hpp[k]) return CCDGPU_ERR_INVALID_ARGUMENT;
-      if (n) std::memcpy(&v_h_hpp[o_h[k]], P->v_h_hpp[k], sizeof(double) * n);
-    }
-    for (uint64_t a = 0; a < h->npart; a++) {
-      const int64_t n = o_p[a + 1] - o_p[a];
-      if (n && !P->v_phh_p[a]) return CCDGPU_ERR_INVALID_ARGUMENT;
-      if (n) std::memcpy(&v_phh_p[o_p[a]], P->v_phh_p[a], sizeof(double) * n);
-    }
-  }
 
-  // pp-ladder work tiles, heaviest first (the on-device analogue of ffdBalance).
+  // pp-ladder work tiles.  Thin row blocks stream at full bandwidth on their own, so K is
+  // split only when there are fewer of them than SMs.  Mid/wide tiles are compute-latency
+  // bound per CTA, so their K is split into segments of at least four chunks until the class
+  // has about three tiles per SM.  Split tiles are reduced deterministically (ladder_reduce).
+  auto cls_of = [](int nb) { return nb <= 8 ? 0 : nb <= 32 ? 1 : 2; };
+  int64_t blocks_thin = 0, blocks_wide = 0;
+  for (const ChanInfo &a : chans) (a.nb <= 8 ? blocks_thin : blocks_wide) += a.nmt;
+  const int64_t kSMs = 148;
+  const int want_thin = blocks_thin >= kSMs ? 1 : (int)std::min<int64_t>(8, ceil_div(kSMs, std::max<int64_t>(blocks_thin, 1)));
+  const int want_wide = (int)std::min<int64_t>(32, std::max<int64_t>(1, ceil_div(3 * kSMs, std::max<int64_t>(blocks_wide, 1))));
   std::vector<LadderTile> tiles;
+  int64_t lpart_tot = 0;
+  int32_t groups = 0;
   for (int ai = 0; ai < h->n_act; ai++) {
     const ChanInfo &a = chans[ai];
+    const int want = a.nb <= 8 ? want_thin : want_wide;
+    const int min_chunks = 4;
+    const int nseg = std::max(1, std::min(want, a.nkc / min_chunks));
     for (int mt = 0; mt < a.nmt; mt++) {
-      LadderTile tl{};
-      tl.ch = ai; tl.mt = mt; tl.nkc = a.nkc; tl.nkh = a.nkh; tl.cg = a.cg; tl.bm = a.bm;
-      tl.pr = a.pr; tl.hh = a.hh;
-      tl.v_base = a.vkt_base; tl.tkt_base = a.tkt_base; tl.tmt_base = a.tmt_base;
-      tl.xt_base = a.xt_base; tl.t_off = a.t_off; tl.row_off = a.row_off;
-      tiles.push_back(tl);
+      const int rows = std::min(a.bm, a.pr - mt * a.bm);
+      const int64_t pbase = lpart_tot;
+      if (nseg > 1) lpart_tot += (int64_t)nseg * a.bm * a.nb;
+      for (int sg = 0; sg < nseg; sg++) {
+        LadderTile tl{};
+        tl.ch = ai; tl.mt = mt;
+        tl.kc0 = (int)((int64_t)a.nkc * sg / nseg);
+        tl.nks = (int)((int64_t)a.nkc * (sg + 1) / nseg) - tl.kc0;
+        tl.nkc = a.nkc;
+        tl.nkh = (sg == nseg - 1) ? a.nkh : 0;
+        tl.nb = a.nb; tl.bm = a.bm; tl.rows = rows; tl.pr = a.pr; tl.hh = a.hh;
+        tl.seg = sg; tl.nseg = nseg; tl.group = groups;
+        tl.v_base = a.vkt_base; tl.tkt_base = a.tkt_base; tl.tmt_base = a.tmt_base;
+        tl.xt_base = a.xt_base; tl.t_off = a.t_off; tl.row_off = a.row_off;
+        tl.part_base = pbase;
+        tiles.push_back(tl);
+      }
+      groups++;
     }
   }
-  // Narrow channels (<= 32 hh columns) first, then wide ones; within each class the longest
-  // K streams first so the hardware block scheduler fills in the short ones.
-  std::stable_sort(tiles.begin(), tiles.end(), [](const LadderTile &x, const LadderTile &y) {
-    const bool nx = x.cg <= kNarrowCG, ny = y.cg <= kNarrowCG;
-    if (nx != ny) return nx;
-    return (int64_t)(x.nkc + x.nkh) * (x.bm + 8 * x.cg) > (int64_t)(y.nkc + y.nkh) * (y.bm + 8 * y.cg);
+  // Thin channels first, then wide ones; within each class the longest K streams first so
+  // the hardware block scheduler fills in the short ones.
+  std::stable_sort(tiles.begin(), tiles.end(), [&](const LadderTile &x, const LadderTile &y) {
+    const int cx = cls_of(x.nb), cy = cls_of(y.nb);
+    if (cx != cy) return cx < cy;
+    return (int64_t)(x.nks + x.nkh) * (x.rows + x.nb) > (int64_t)(y.nks + y.nkh) * (y.rows + y.nb);
   });
-  h->n_tiles_narrow = 0;
-  for (const LadderTile &t : tiles) h->n_tiles_narrow += t.cg <= kNarrowCG;
   h->n_tiles = (int)tiles.size();
+  for (const LadderTile &t : tiles) h->n_cls[cls_of(t.nb)]++;
   std::vector<ElemRange> ranges;
   const int64_t per = (int64_t)kAsmThreads * kAsmPerThread;
   for (int ai = 0; ai < h->n_act; ai++) {
@@ -416,122 +385,239 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   h->n_ranges = (int)ranges.size();
 
   // Work estimate (reference GEMM flops) for roofline reporting.
-  double fl = 0, lf = 0, vb = 0;
+  double fl = 0, lf = 0, vb = 0, vbp = 0;
   for (const ChanInfo &a : chans) {
     lf += 2.0 * a.pp * a.pp * a.hh;
     fl += 2.0 * a.pp * a.pp * a.hh + 4.0 * a.pp * a.hh * (double)a.hh;
     vb += 8.0 * a.pp * a.pp;
+    vbp += 8.0 * a.pr * (double)a.pk;
   }
   for (const ModInfo &m : mods) fl += 4.0 * m.ph * (double)m.hp * m.hp;
-  h->flops = fl; h->ladder_flops = lf; h->v_bytes = vb;
+  h->flops = fl; h->ladder_flops = lf; h->v_bytes = vb; h->v_packed_bytes = vbp;
+  // Bytes one pp-ladder launch must move: packed V, the T operand rows (c<d for V T, a<=b
+  // for T X), X, and D written in full.
+  double lb = vbp;
+  for (const ChanInfo &a : chans)
+    lb += 8.0 * ((double)a.pk * a.hh + (double)a.pr * a.hh + (double)a.hh * a.hh + (double)a.pp * a.hh);
+  h->ladder_bytes = lb;
+  h->n_tkt = tkt;
+  h->n_tmt = tmt;
 
-  // Device allocations and uploads.
+  // ---- one device allocation ----
+  Arena ar;
+  ar.add(&h->chans, chans.size()); ar.add(&h->mods, mods.size());
+  ar.add(&h->tiles, tiles.size()); ar.add(&h->hh_tiles, hh_tiles.size());
+  ar.add(&h->ranges, ranges.size());
+  ar.add(&h->pp_pairs, pp_pairs.size()); ar.add(&h->hh_pairs, hh_pairs.size());
+  ar.add(&h->pp_swap, pp_swap.size()); ar.add(&h->hh_swap, hh_swap.size());
+  ar.add(&h->list_off, list_off.size()); ar.add(&h->list, list.size());
+  ar.add(&h->rowmap, rowmap.size()); ar.add(&h->mirror, mirror.size());
+  ar.add(&h->pk_idx, pk_idx.size());
+  ar.add(&h->counters, h->n_act); ar.add(&h->part, part_tot);
+  ar.add(&h->lcounters, groups); ar.add(&h->lpart, lpart_tot);
+  ar.add(&h->eps, nsp);
+  ar.add(&h->v_pphh, n_t); ar.add(&h->v_hhhh, x_tot); ar.add(&h->v_t, vt);
+  ar.add(&h->v_hpph, h->n_m); ar.add(&h->v_hphp, y_tot);
+  ar.add(&h->flat, (size_t)8 * n_t); ar.add(&h->o_h, o_h.size()); ar.add(&h->o_p, o_p.size());
+  ar.add(&h->t[0], n_t); ar.add(&h->t[1], n_t); ar.add(&h->dmat, n_t);
+  ar.add(&h->old_phhp, h->n_m); ar.add(&h->r_phhp, h->n_m);
+  ar.add(&h->x, x_tot); ar.add(&h->x_t, xt); ar.add(&h->t_kt, tkt); ar.add(&h->t_mt, tmt);
+  ar.add(&h->s, hh_tot); ar.add(&h->r, pp_tot); ar.add(&h->xh, np); ar.add(&h->yp, h->npart);
+  ar.add(&h->epart, h->n_ranges); ar.add(&h->ctl, 1); ar.add(&h->e_out, 1); ar.add(&h->err, 1);
+  ar.add(&h->ticket, 1);
+  if (h->have_3body) {
+    ar.add(&h->v_h_hpp, h->n_h); ar.add(&h->v_phh_p, h->n_p);
+    ar.add(&h->old_h1pp_h2, h->n_h); ar.add(&h->old_h2pp_h1, h->n_h); ar.add(&h->diff_h2pp_h1, h->n_h);
+    ar.add(&h->old_p1_p2hh, h->n_p); ar.add(&h->old_p2_p1hh, h->n_p); ar.add(&h->diff_p2_p1hh, h->n_p);
+    ar.add(&h->gath, (size_t)8 * n_t);
+  }
   int rc;
 #define TRY(x) do { rc = (x); if (rc) return rc; } while (0)
-  TRY(upload(h, &h->chans, chans));
-  TRY(upload(h, &h->mods, mods));
-  TRY(upload(h, &h->tiles, tiles));
-  TRY(upload(h, &h->hh_tiles, hh_tiles));
-  TRY(upload(h, &h->rowmap, rowmap));
-  TRY(upload(h, &h->mirror, mirror));
-  TRY(upload(h, &h->pk_idx, pk_idx));
-  TRY(dalloc(h, &h->counters, h->n_act));
-  TRY(dalloc(h, &h->part, part_tot));
-  TRY(upload(h, &h->ranges, ranges));
-  TRY(upload(h, &h->pp_pairs, pp_pairs));
-  TRY(upload(h, &h->hh_pairs, hh_pairs));
-  TRY(upload(h, &h->pp_swap, pp_swap));
-  TRY(upload(h, &h->hh_swap, hh_swap));
-  TRY(upload(h, &h->list_off, list_off));
-  TRY(upload(h, &h->list, list));
-  std::vector<double> eps(P->sp_energy, P->sp_energy + nsp);
-  TRY(upload(h, &h->eps, eps));
-  TRY(upload(h, &h->v_pphh, v_pphh));
-  TRY(upload(h, &h->v_hhhh, v_hhhh));
-  TRY(upload(h, &h->v_t, v_t));
-  TRY(upload(h, &h->v_hpph, v_hpph));
-  TRY(upload(h, &h->v_hphp, v_hphp));
-  TRY(upload(h, &h->flat, flat));
-  TRY(upload(h, &h->o_h, o_h));
-  TRY(upload(h, &h->o_p, o_p));
-  TRY(dalloc(h, &h->t[0], n_t));
-  TRY(dalloc(h, &h->t[1], n_t));
-  TRY(dalloc(h, &h->dmat, n_t));
-  TRY(dalloc(h, &h->old_phhp, h->n_m));
-  TRY(dalloc(h, &h->r_phhp, h->n_m));
-  TRY(dalloc(h, &h->x, x_tot));
-  TRY(dalloc(h, &h->x_t, xt));
-  TRY(dalloc(h, &h->t_kt, tkt));
-  TRY(dalloc(h, &h->t_mt, tmt));
-  TRY(dalloc(h, &h->s, hh_tot));
-  TRY(dalloc(h, &h->r, pp_tot));
-  TRY(dalloc(h, &h->xh, np));
-  TRY(dalloc(h, &h->yp, h->npart));
-  TRY(dalloc(h, &h->epart, h->n_ranges));
-  TRY(dalloc(h, &h->ctl, 1));
-  TRY(dalloc(h, &h->e_out, 1));
-  TRY(dalloc(h, &h->err, 1));
-  if (h->have_3body) {
-    TRY(upload(h, &h->v_h_hpp, v_h_hpp));
-    TRY(upload(h, &h->v_phh_p, v_phh_p));
-    TRY(dalloc(h, &h->old_h1pp_h2, h->n_h));
-    TRY(dalloc(h, &h->old_h2pp_h1, h->n_h));
-    TRY(dalloc(h, &h->diff_h2pp_h1, h->n_h));
-    TRY(dalloc(h, &h->old_p1_p2hh, h->n_p));
-    TRY(dalloc(h, &h->old_p2_p1hh, h->n_p));
-    TRY(dalloc(h, &h->diff_p2_p1hh, h->n_p));
-    TRY(dalloc(h, &h->gath, (size_t)8 * n_t));
+  TRY(ar.commit(h));
+  // Scratch for the raw inputs, released at the end of create.
+  Arena sc;
+  double *vraw = nullptr, *hhpp_raw = nullptr;
+  RawIndex *raw_idx = nullptr;
+  int32_t *counts = nullptr;
+  int2 *d_vrows = nullptr, *d_mod_dims = nullptr;
+  int32_t *d_kcol = nullptr;
+  int64_t *d_vraw_off = nullptr, *d_o_m = nullptr;
+  sc.add(&vraw, vraw_tot); sc.add(&hhpp_raw, n_t); sc.add(&raw_idx, (size_t)8 * n_t);
+  sc.add(&counts, (size_t)5 * n_t); sc.add(&d_vrows, vrows.size()); sc.add(&d_kcol, kcol.size());
+  sc.add(&d_vraw_off, vraw_off.size()); sc.add(&d_mod_dims, mod_dims.size()); sc.add(&d_o_m, o_m.size());
+  const size_t n_allocs = h->allocs.size();
+  TRY(sc.commit(h));
+
+  auto put = [&](auto *dst, const auto &v) -> int {
+    if (!v.empty()) CK(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice, h->s0));
+    return CCDGPU_OK;
+  };
+  TRY(put(h->chans, chans)); TRY(put(h->mods, mods)); TRY(put(h->tiles, tiles));
+  TRY(put(h->hh_tiles, hh_tiles)); TRY(put(h->ranges, ranges));
+  TRY(put(h->pp_pairs, pp_pairs)); TRY(put(h->hh_pairs, hh_pairs));
+  TRY(put(h->pp_swap, pp_swap)); TRY(put(h->hh_swap, hh_swap));
+  TRY(put(h->list_off, list_off)); TRY(put(h->list, list));
+  TRY(put(h->rowmap, rowmap)); TRY(put(h->mirror, mirror)); TRY(put(h->pk_idx, pk_idx));
+  TRY(put(h->o_h, o_h)); TRY(put(h->o_p, o_p));
+  TRY(put(d_vrows, vrows)); TRY(put(d_kcol, kcol)); TRY(put(d_vraw_off, vraw_off));
+  TRY(put(d_mod_dims, mod_dims)); TRY(put(d_o_m, o_m));
+  CK(cudaMemcpyAsync(h->eps, P->sp_energy, nsp * 8, cudaMemcpyHostToDevice, h->s0));
+
+  // V blocks and tables, uploaded in their reference layouts (runs of adjacent blocks).
+  {
+    std::vector<const double *> sp, sx, sh;
+    std::vector<int64_t> np2, nx, nh;
+    std::vector<const ccdgpu_chain_index *> sm[8];
+    std::vector<int64_t> nm;
+    for (size_t ai = 0; ai < chans.size(); ai++) {
+      const uint64_t c = act_chan[ai];
+      const ChanInfo &a = chans[ai];
+      if (!P->v_pppp[c] || !P->v_hhpp[c] || !P->v_hhhh[c]) return CCDGPU_ERR_INVALID_ARGUMENT;
+      sp.push_back(P->v_pppp[c]); np2.push_back((int64_t)a.pp * a.pp);
+      sx.push_back(P->v_hhpp[c]); nx.push_back((int64_t)a.pp * a.hh);
+      sh.push_back(P->v_hhhh[c]); nh.push_back((int64_t)a.hh * a.hh);
+      for (int k = 0; k < 8; k++) {
+        if (!P->maps[k][c]) return CCDGPU_ERR_INVALID_ARGUMENT;
+        sm[k].push_back(P->maps[k][c]);
+      }
+      nm.push_back((int64_t)a.pp * a.hh);
+    }
+    TRY(upload_runs(h, vraw, sp, np2));
+    TRY(upload_runs(h, hhpp_raw, sx, nx));
+    TRY(upload_runs(h, h->v_hhhh, sh, nh));
+    static_assert(sizeof(RawIndex) == sizeof(ccdgpu_chain_index), "ChainIndex layout");
+    for (int k = 0; k < 8; k++)
+      TRY(upload_runs(h, reinterpret_cast<ccdgpu_chain_index *>(raw_idx) + (size_t)k * n_t, sm[k], nm));
+    TRY(upload_runs(h, h->v_hpph, src_hpph, cnt_hpph));
+    TRY(upload_runs(h, h->v_hphp, src_hphp, cnt_hphp));
+    if (h->have_3body) {
+      std::vector<const double *> s5, s6;
+      std::vector<int64_t> n5, n6;
+      for (uint64_t k = 0; k < np; k++) {
+        const int64_t n = o_h[k + 1] - o_h[k];
+        if (n && !P->v_h_hpp[k]) return CCDGPU_ERR_INVALID_ARGUMENT;
+        s5.push_back(P->v_h_hpp[k]); n5.push_back(n);
+      }
+      for (uint64_t a = 0; a < h->npart; a++) {
+        const int64_t n = o_p[a + 1] - o_p[a];
+        if (n && !P->v_phh_p[a]) return CCDGPU_ERR_INVALID_ARGUMENT;
+        s6.push_back(P->v_phh_p[a]); n6.push_back(n);
+      }
+      TRY(upload_runs(h, h->v_h_hpp, s5, n5));
+      TRY(upload_runs(h, h->v_phh_p, s6, n6));
+    }
   }
+  // Device layout transforms.
+  if (h->n_ranges) {
+    transpose_hhpp_kernel<<<h->n_ranges, 256, 0, h->s0>>>(h->ranges, h->chans, hhpp_raw, h->v_pphh);
+    CK(cudaGetLastError());
+    TableGeometry geo{h->o_h, h->o_p, d_o_m, d_mod_dims, nch, np, h->npart};
+    convert_tables_kernel<<<h->n_ranges, 256, 0, h->s0>>>(h->ranges, raw_idx, n_t, geo, h->flat,
+                                                          counts, h->err);
+    CK(cudaGetLastError());
+    const int nb = (int)std::min<int64_t>(ceil_div(5 * n_t, 256), 148 * 32);
+    check_counts_kernel<<<std::max(nb, 1), 256, 0, h->s0>>>(counts, 5 * n_t, h->err);
+    CK(cudaGetLastError());
+  }
+  if (!vrows.empty()) {
+    tile_v_kernel<<<(unsigned)vrows.size(), 128, 0, h->s0>>>(h->chans, d_vrows, h->rowmap, d_kcol,
+                                                             d_vraw_off, vraw, h->v_t);
+    CK(cudaGetLastError());
+  }
+  int32_t e = 0;
+  CK(cudaMemcpyAsync(&e, h->err, sizeof(e), cudaMemcpyDeviceToHost, h->s0));
+  CK(cudaStreamSynchronize(h->s0));
+  // Release the scratch allocation.
+  for (size_t i = n_allocs; i < h->allocs.size(); i++) cudaFree(h->allocs[i].p);
+  h->allocs.resize(n_allocs);
+  if (e & kErrBadIndex) return CCDGPU_ERR_BAD_TABLE;
+  if (e) return CCDGPU_ERR_CUDA;
 #undef TRY
   CK(cudaMallocHost(&h->h_ctl, sizeof(Control)));
   std::memset(h->h_ctl, 0, sizeof(Control));
 
-  h->ladder_smem = (size_t)kStages * (kMaxBM * kBK + kBK * kMaxCG * 8) * 8 + 2 * kStages * 8;
-  CK(cudaFuncSetAttribute(pp_ladder_kernel<1, kNarrowCG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  h->ladder_smem = (size_t)kStages * (kMaxBM * kBK + kBK * kMaxNB) * 8 + 2 * kStages * 8;
+  h->ladder_smem_thin = (size_t)kStages * (kMaxBM * kBK + kBK * 8) * 8 + 2 * kStages * 8;
+  CK(cudaFuncSetAttribute(pp_ladder_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)h->ladder_smem_thin));
+  CK(cudaFuncSetAttribute(pp_ladder_kernel<0>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  CK(cudaFuncSetAttribute(pp_ladder_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)h->ladder_smem));
-  CK(cudaFuncSetAttribute(pp_ladder_kernel<1, kNarrowCG>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-  CK(cudaFuncSetAttribute(pp_ladder_kernel<kNarrowCG + 1, kMaxCG>,
-                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->ladder_smem));
-  CK(cudaFuncSetAttribute(pp_ladder_kernel<kNarrowCG + 1, kMaxCG>,
-                          cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-  int maxhh = 1;
-  for (const ChanInfo &a : chans) maxhh = std::max(maxhh, a.hh);
+  CK(cudaFuncSetAttribute(pp_ladder_kernel<1>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  CK(cudaFuncSetAttribute(pp_ladder_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)h->ladder_smem));
+  CK(cudaFuncSetAttribute(pp_ladder_kernel<2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   h->hh_smem = (size_t)2 * kHHRows * maxhh * 8;
   CK(cudaFuncSetAttribute(hh_ladder_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)h->hh_smem));
   CK(cudaFuncSetAttribute(ring_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)std::max<size_t>(h->ring_smem, 16)));
-  CK(cudaStreamSynchronize(h->s0));
   return CCDGPU_OK;
 }
 
 // ---- launches -------------------------------------------------------------------------
 
+// Launch with the programmatic-stream-serialization attribute (PDL): the kernel may begin
+// launching while its stream predecessor drains; it waits in griddepcontrol.wait before
+// touching the predecessor's results (skip_iteration / pdl_enter in every kernel).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem,
+                       cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 int launch_hh_ladder(ccdgpu_handle *h, cudaStream_t st) {
   if (!h->n_hh_tiles) return CCDGPU_OK;
-  hh_ladder_kernel<<<h->n_hh_tiles, kHHThreads, h->hh_smem, st>>>(
-      h->hh_tiles, h->chans, h->v_pphh, h->v_hhhh, h->t[0], h->t[1], h->part, h->counters, h->x,
-      h->x_t, h->s, h->r, h->ctl);
   h->launches++;
-  return cuda_status(cudaGetLastError());
+  return cuda_status(launch_pdl(hh_ladder_kernel, h->n_hh_tiles, kHHThreads, h->hh_smem, st,
+                                h->hh_tiles, h->chans, h->v_pphh, h->v_hhhh, h->t[0], h->t[1],
+                                h->part, h->counters, h->x, h->x_t, h->s, h->r, h->ctl));
 }
+// The three column classes run concurrently: mid and wide go to stream s2 (wide first, they
+// are the longest tiles), thin to `st`; s2 is joined back into `st` before returning.
 int launch_pp_ladder(ccdgpu_handle *h, cudaStream_t st) {
-  if (h->n_tiles_narrow) {
-    pp_ladder_kernel<1, kNarrowCG><<<h->n_tiles_narrow, kLadderThreads, h->ladder_smem, st>>>(
-        h->tiles, h->v_t, h->t_kt, h->t_mt, h->x_t, h->rowmap, h->mirror, h->dmat, h->ctl, h->err);
-    h->launches++;
-    CK(cudaGetLastError());
+  const LadderTile *t_thin = h->tiles, *t_mid = h->tiles + h->n_cls[0];
+  const LadderTile *t_wide = t_mid + h->n_cls[1];
+  const bool side = h->n_cls[1] || h->n_cls[2];
+  if (side) {
+    CK(cudaEventRecord(h->ev_fork2, st));
+    CK(cudaStreamWaitEvent(h->s2, h->ev_fork2, 0));
+    if (h->n_cls[2]) {
+      pp_ladder_kernel<2><<<h->n_cls[2], kLadderThreads, h->ladder_smem, h->s2>>>(
+          t_wide, h->v_t, h->t_kt, h->t_mt, h->x_t, h->rowmap, h->mirror, h->dmat, h->lpart,
+          h->lcounters, h->ctl, h->err);
+      h->launches++;
+      CK(cudaGetLastError());
+    }
+    if (h->n_cls[1]) {
+      pp_ladder_kernel<1><<<h->n_cls[1], kLadderThreads, h->ladder_smem, h->s2>>>(
+          t_mid, h->v_t, h->t_kt, h->t_mt, h->x_t, h->rowmap, h->mirror, h->dmat, h->lpart,
+          h->lcounters, h->ctl, h->err);
+      h->launches++;
+      CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(h->ev_join2, h->s2));
   }
-  const int nwide = h->n_tiles - h->n_tiles_narrow;
-  if (nwide) {
-    pp_ladder_kernel<kNarrowCG + 1, kMaxCG><<<nwide, kLadderThreads, h->ladder_smem, st>>>(
-        h->tiles + h->n_tiles_narrow, h->v_t, h->t_kt, h->t_mt, h->x_t, h->rowmap, h->mirror,
-        h->dmat, h->ctl, h->err);
+  if (h->n_cls[0]) {
+    CK(launch_pdl(pp_ladder_kernel<0>, h->n_cls[0], kLadderThreads, h->ladder_smem_thin, st,
+                  t_thin, h->v_t, h->t_kt, h->t_mt, h->x_t, h->rowmap, h->mirror, h->dmat,
+                  h->lpart, h->lcounters, h->ctl, h->err));
     h->launches++;
-    CK(cudaGetLastError());
   }
+  if (side) CK(cudaStreamWaitEvent(st, h->ev_join2, 0));
   return CCDGPU_OK;
 }
+
 int launch_ring(ccdgpu_handle *h, cudaStream_t st) {
   if (h->n_mod_small) {
     ring_small_kernel<<<(int)ceil_div(h->n_mod_small, 8), 256, 0, st>>>(
@@ -551,24 +637,24 @@ int launch_ring(ccdgpu_handle *h, cudaStream_t st) {
 int launch_onebody_fused(ccdgpu_handle *h, cudaStream_t st) {
   const int warps_per_block = 8;
   const int blocks = (int)ceil_div((int64_t)h->nsp, warps_per_block);
-  onebody_fused_kernel<<<blocks, warps_per_block * 32, 0, st>>>((int)h->np, (int)h->nsp, h->list_off,
-                                                                 h->list, h->s, h->r, h->xh, h->yp, h->ctl);
   h->launches++;
-  return cuda_status(cudaGetLastError());
+  return cuda_status(launch_pdl(onebody_fused_kernel, blocks, warps_per_block * 32, 0, st,
+                                (int)h->np, (int)h->nsp, h->list_off, h->list, h->s, h->r, h->xh,
+                                h->yp, h->ctl));
 }
 int launch_assemble_fused(ccdgpu_handle *h, cudaStream_t st) {
   if (!h->n_ranges) return CCDGPU_OK;
   const int64_t n_t = h->n_t;
-  assemble_fused_kernel<<<h->n_ranges, kAsmThreads, 0, st>>>(
-      h->ranges, h->chans, h->pp_pairs, h->hh_pairs, h->pp_swap, h->hh_swap, h->pk_idx, h->v_pphh,
-      h->dmat,
-      h->r_phhp, h->flat + 4 * n_t, h->flat + 5 * n_t, h->flat + 6 * n_t, h->flat + 7 * n_t, h->xh,
-      h->yp, h->eps, (int)h->np, h->t[0], h->t[1], h->old_phhp, h->t_kt, h->t_mt, h->epart, h->ctl);
   h->launches++;
-  return cuda_status(cudaGetLastError());
+  return cuda_status(launch_pdl(
+      assemble_fused_kernel, h->n_ranges, kAsmThreads, 0, st, h->ranges, h->chans, h->pp_pairs,
+      h->hh_pairs, h->pp_swap, h->hh_swap, h->pk_idx, h->v_pphh, h->dmat, h->r_phhp,
+      h->flat + 4 * n_t, h->flat + 5 * n_t, h->flat + 6 * n_t, h->flat + 7 * n_t, h->xh, h->yp,
+      h->eps, (int)h->np, h->t[0], h->t[1], h->old_phhp, h->t_kt, h->t_mt, h->epart, h->ticket,
+      h->ctl));
 }
 int launch_energy(ccdgpu_handle *h, cudaStream_t st, int flags) {
-  energy_kernel<<<1, 1024, 0, st>>>(h->epart, h->n_ranges, h->ctl, flags, h->e_out);
+  energy_kernel<<<1, kEnergyThreads, 0, st>>>(h->epart, h->n_ranges, h->ctl, flags, h->e_out);
   h->launches++;
   return cuda_status(cudaGetLastError());
 }
@@ -603,7 +689,6 @@ int enqueue_fused_iteration(ccdgpu_handle *h) {
     CK(cudaEventRecord(h->ev[8], h->s0));
     if ((rc = launch_assemble_fused(h, h->s0))) return rc;
     CK(cudaEventRecord(h->ev[6], h->s0));
-    if ((rc = launch_energy(h, h->s0, 3))) return rc;
     CK(cudaEventRecord(h->ev[7], h->s0));
     return CCDGPU_OK;
   }
@@ -615,8 +700,7 @@ int enqueue_fused_iteration(ccdgpu_handle *h) {
   if ((rc = launch_onebody_fused(h, h->s0))) return rc;
   if ((rc = launch_pp_ladder(h, h->s0))) return rc;
   CK(cudaStreamWaitEvent(h->s0, h->ev_join, 0));
-  if ((rc = launch_assemble_fused(h, h->s0))) return rc;
-  return launch_energy(h, h->s0, 3);
+  return launch_assemble_fused(h, h->s0);  // includes the energy reduction and stop rule
 }
 
 // Table path stages (mirrors main.cpp:591-665).
@@ -770,6 +854,9 @@ int ccdgpu_create(const ccdgpu_problem *prob, const ccdgpu_options *opt, ccdgpu_
   if (!rc) rc = cuda_status(cudaStreamCreateWithFlags(&h->s1, cudaStreamNonBlocking));
   if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
   if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+  if (!rc) rc = cuda_status(cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking));
+  if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->ev_fork2, cudaEventDisableTiming));
+  if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->ev_join2, cudaEventDisableTiming));
   for (int i = 0; i < 10 && !rc; i++) rc = cuda_status(cudaEventCreate(&h->ev[i]));
   if (!rc) rc = build(h, prob);
   if (!rc) rc = set_ctl(h, 0, 0.0, 100, 0.5, true);
@@ -791,13 +878,12 @@ uint64_t ccdgpu_t2_size(const ccdgpu_handle *h) { return h ? (uint64_t)h->n_t : 
 int ccdgpu_reset(ccdgpu_handle *h) {
   if (!h) return CCDGPU_ERR_INVALID_ARGUMENT;
   CK(cudaSetDevice(h->opt.device));
-  double *z[] = {h->t[0], h->t[1], h->old_phhp, h->t_kt, h->t_mt, h->old_h1pp_h2, h->old_h2pp_h1,
-                 h->old_p1_p2hh, h->old_p2_p1hh};
-  for (double *p : z) {
-    if (!p) continue;
-    for (auto &b : h->allocs)
-      if (b.p == p) CK(cudaMemsetAsync(p, 0, b.bytes, h->s0));
-  }
+  const std::pair<double *, int64_t> z[] = {
+      {h->t[0], h->n_t}, {h->t[1], h->n_t}, {h->old_phhp, h->n_m}, {h->t_kt, h->n_tkt},
+      {h->t_mt, h->n_tmt}, {h->old_h1pp_h2, h->n_h}, {h->old_h2pp_h1, h->n_h},
+      {h->old_p1_p2hh, h->n_p}, {h->old_p2_p1hh, h->n_p}};
+  for (const auto &b : z)
+    if (b.first && b.second) CK(cudaMemsetAsync(b.first, 0, b.second * 8, h->s0));
   return set_ctl(h, 0, h->h_ctl->tol, h->h_ctl->max_iters, h->h_ctl->mixing, true, 0);
 }
 
@@ -1010,7 +1096,7 @@ int ccdgpu_work_per_iteration(const ccdgpu_handle *h, double *flops, double *v_p
                               double *ladder_flops) {
   if (!h) return CCDGPU_ERR_INVALID_ARGUMENT;
   if (flops) *flops = h->flops;
-  if (v_pppp_bytes) *v_pppp_bytes = h->v_bytes;
+  if (v_pppp_bytes) *v_pppp_bytes = h->ladder_bytes;
   if (ladder_flops) *ladder_flops = h->ladder_flops;
   return CCDGPU_OK;
 }

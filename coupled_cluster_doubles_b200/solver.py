@@ -160,7 +160,7 @@ class CCDSolver:
         f, b, lf = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         _check(_native.gpu_lib().ccdgpu_work_per_iteration(
             self._h, ctypes.byref(f), ctypes.byref(b), ctypes.byref(lf)), "work")
-        return {"flops": f.value, "v_pppp_bytes": b.value, "ladder_flops": lf.value}
+        return {"flops": f.value, "ladder_bytes": b.value, "ladder_flops": lf.value}
 
     # Stage entry points with the reference's names (calc.hpp, Chain.hpp, main.cpp:591-665).
     def calc_t2diff_p2_p1hh(self):

@@ -214,9 +214,11 @@ int ccdgpu_enable_profiling(ccdgpu_handle *h, int32_t on);
 /* The handle's main CUDA stream (cudaStream_t), for callers that time or order work on it. */
 void *ccdgpu_stream(ccdgpu_handle *h);
 
-/* Algorithmic work of one iteration for roofline reporting: reference GEMM flops
- * (sum over channels of 2 pp^2 hh + 4 pp hh^2 + 4 ph' hp'^2) and V_pppp bytes. */
-int ccdgpu_work_per_iteration(const ccdgpu_handle *h, double *flops, double *v_pppp_bytes,
+/* Work of one iteration for roofline reporting: *flops = reference GEMM flops (sum over
+ * channels of 2 pp^2 hh + 4 pp hh^2 + 4 ph' hp'^2); *ladder_bytes = bytes one pp-ladder launch
+ * moves (antisymmetry-packed V_pppp, the T and X operands, D); *ladder_flops = the pp-ladder
+ * share of the reference flops (2 pp^2 hh). */
+int ccdgpu_work_per_iteration(const ccdgpu_handle *h, double *flops, double *ladder_bytes,
                               double *ladder_flops);
 
 #ifdef __cplusplus
