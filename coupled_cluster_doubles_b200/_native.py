@@ -113,7 +113,7 @@ GPU_SYMBOLS = [
     "ccdgpu_calc_t2diff_phhp", "ccdgpu_calc_t2diff_pphh", "ccdgpu_map_from_distributed",
     "ccdgpu_calc_t2_pphh", "ccdgpu_map_to_distributed", "ccdgpu_read_chain",
     "ccdgpu_get_profile", "ccdgpu_enable_profiling", "ccdgpu_work_per_iteration",
-    "ccdgpu_energy_history", "ccdgpu_stream",
+    "ccdgpu_energy_history", "ccdgpu_stream", "ccdgpu_calc_channel_t2diff_pphh_noalloc",
 ]
 
 
@@ -152,5 +152,7 @@ def gpu_lib():
         lib.ccdgpu_energy_history.argtypes = [vp, P(c_dbl), c_i64, P(c_i64)]
         lib.ccdgpu_stream.argtypes = [vp]
         lib.ccdgpu_stream.restype = vp
+        lib.ccdgpu_calc_channel_t2diff_pphh_noalloc.argtypes = [vp, vp, vp, vp, vp, c_i64, c_i64, vp]
+        lib.ccdgpu_calc_channel_t2diff_pphh_noalloc.restype = ctypes.c_int
         _gpu = lib
     return _gpu

@@ -44,12 +44,12 @@ def build_host(force=False):
 
 def build_gpu(force=False, verbose=False):
     out = os.path.join(HERE, "libccdgpu.so")
-    src = os.path.join(CSRC, "ccdgpu.cu")
+    srcs = [os.path.join(CSRC, "ccdgpu.cu"), os.path.join(CSRC, "ccd_noalloc.cu")]
     deps = _sources(CSRC, (".cu", ".cuh")) + [os.path.join(INC, "ccdgpu.h")]
     if not force and _newer(out, deps):
         return out
     cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
-           "-Xcompiler", "-fopenmp", "-I" + INC, "-I" + CSRC, src, "-o", out, "-lgomp"]
+           "-Xcompiler", "-fopenmp", "-I" + INC, "-I" + CSRC, *srcs, "-o", out, "-lgomp"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     # Point nvcc at the system compiler (the image's default CXX lacks libgomp).

@@ -221,6 +221,25 @@ void *ccdgpu_stream(ccdgpu_handle *h);
 int ccdgpu_work_per_iteration(const ccdgpu_handle *h, double *flops, double *ladder_bytes,
                               double *ladder_flops);
 
+/* No counterpart in the reference.  The ladder term of one regular channel,
+ * D = 0.5 T X + 0.5 V_pppp T with X = V_hhhh + 0.5 V_hhpp T (the arithmetic of
+ * calcChannelT2Diff_pphh), for callers that cannot allocate device memory, such as a host
+ * that owns all device memory through its own pool or budget.  Nothing is allocated: every
+ * argument is a caller-provided device buffer (reference row-major layouts: v_pppp pp x pp,
+ * v_hhpp hh x pp, v_hhhh hh x hh, t2 pp x hh, d pp x hh), and the intermediate X with its
+ * split-K partial sums lives in a fixed 2 MiB scratch array built into the library (one per
+ * GPU that loads it, kept until the process exits).  Limits: hh <= 72 and
+ * 32 + (ceil(pp/64) + 1) * hh^2 <= 262144 doubles; larger sizes return
+ * CCDGPU_ERR_UNSUPPORTED without launching anything.  Work is enqueued on `stream`
+ * (a cudaStream_t; NULL = legacy default stream) for the current device.  The first call on a
+ * device looks up the scratch address (cudaGetSymbolAddress) and sets a kernel attribute; make
+ * that first call before any stream capture.  Every call shares the one scratch array, which
+ * keeps the last call's contents: calls whose work overlaps on the GPU (different streams
+ * without ordering) race and must not be issued. */
+int ccdgpu_calc_channel_t2diff_pphh_noalloc(const double *v_pppp, const double *v_hhpp,
+                                            const double *v_hhhh, const double *t2, double *d,
+                                            int64_t pp, int64_t hh, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
