@@ -163,6 +163,17 @@ def run_reference_arm(args):
     print(json.dumps(line))
 
 
+FP64_PEAK_TFLOPS = 35.47  # cuBLAS DGEMM 8192^3 measured on this pool's B200 (FP64 pipe)
+PRECISIONS = {"mixed": "mixed_bf16", "fp64": "fp64"}
+
+
+def stop_tol(n_particles):
+    """|dE| bound of the stop rule that keeps the converged energy within 1e-7 per particle
+    of the fully converged FP64 value (a factor-10 margin over the linear convergence tail;
+    the achieved error is measured and reported)."""
+    return 1e-8 * n_particles
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -171,7 +182,11 @@ def main():
     ap.add_argument("--config", default="eg14", choices=list(CONFIGS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--path", default="fused", choices=["fused", "tables"])
+    ap.add_argument("--precision", default="mixed", choices=list(PRECISIONS),
+                    help="headline arm; the other precision is timed beside it")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--single-arm", action="store_true",
+                    help="time only the headline precision (for profiler launch lists)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -189,74 +204,94 @@ def main():
     if world > 1:
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    desc, kind, params, cli, tol = CONFIGS[args.config]
+    desc, kind, params, cli, _ = CONFIGS[args.config]
     system = getattr(System, kind)(**params)
-    solver = CCDSolver(system, device=local, path=args.path)
-    stream = torch.cuda.ExternalStream(solver.stream_ptr(), device=local)
+    n_part = system.n_particles
+    tol = stop_tol(n_part)
+    if args.path == "tables" and args.precision == "mixed":
+        args.precision = "fp64"  # the table path is FP64 only
+    arms = [args.precision] + ([p for p in PRECISIONS if p != args.precision]
+                               if args.path == "fused" and not args.single_arm else [])
+    solvers = {a: CCDSolver(system, device=local, path=args.path, precision=PRECISIONS[a])
+               for a in arms}
+    stream = {a: torch.cuda.ExternalStream(solvers[a].stream_ptr(), device=local) for a in arms}
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
 
-    def one_solve():
-        solver.reset()
-        return solver.solve(tol=tol, max_iters=100, mixing=0.5)
+    # Fully converged FP64 energy (untimed) for the |dE/N| check.
+    e_conv = float("nan")
+    if not args.single_arm:
+        ref_solver = solvers.get("fp64") or CCDSolver(system, device=local, path=args.path)
+        ref_solver.reset()
+        e_conv = ref_solver.solve(tol=1e-12, max_iters=100, mixing=0.5).e_corr
 
-    for _ in range(args.warmup):
-        one_solve()
+    for a in arms:
+        for _ in range(args.warmup):
+            solvers[a].reset()
+            solvers[a].solve(tol=tol, max_iters=100, mixing=0.5)
     torch.cuda.synchronize()
 
     def barrier():
         if world > 1:
             torch.distributed.barrier()
 
-    # Timed region: K solves, L2 flushed (256 MiB write) before each on the solver's stream.
-    iters = 0
-    dev_ms = 0.0
-    results = []
+    # Timed region per arm: K solves from T2 = 0, L2 flushed (256 MiB write) before each, on
+    # the solver's own stream; device time between CUDA events on that stream.
+    timing = {}
+    launches0 = {a: solvers[a].profile()["launches"] for a in arms}
     with ClockSampler(local) as clocks:
-        barrier()
-        torch.cuda.synchronize()
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(1.0)
-            solver.reset()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            r = solver.solve(tol=tol, max_iters=100, mixing=0.5)
-            e1.record(stream)
-            e1.synchronize()
-            dev_ms += e0.elapsed_time(e1)
-            iters += r.iterations
-            results.append(r)
-        torch.cuda.synchronize()
-        barrier()
-    ms = torch.tensor([dev_ms], dtype=torch.float64, device=f"cuda:{local}")
-    it_t = torch.tensor([float(iters)], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        torch.distributed.all_reduce(ms, op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(it_t, op=torch.distributed.ReduceOp.SUM)
-    max_ms = float(ms.item())
-    total_iters = float(it_t.item())
-    value = total_iters / (max_ms / 1000.0)
-    launches = solver.profile()["launches"]
+        for a in arms:
+            sol, st = solvers[a], stream[a]
+            iters, dev_ms, last = 0, 0.0, None
+            barrier()
+            torch.cuda.synchronize()
+            for _ in range(args.steps):
+                with torch.cuda.stream(st):
+                    flush.fill_(1.0)
+                sol.reset()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                last = sol.solve(tol=tol, max_iters=100, mixing=0.5)
+                e1.record(st)
+                e1.synchronize()
+                dev_ms += e0.elapsed_time(e1)
+                iters += last.iterations
+            torch.cuda.synchronize()
+            barrier()
+            ms = torch.tensor([dev_ms], dtype=torch.float64, device=f"cuda:{local}")
+            it_t = torch.tensor([float(iters)], dtype=torch.float64, device=f"cuda:{local}")
+            if world > 1:
+                torch.distributed.all_reduce(ms, op=torch.distributed.ReduceOp.MAX)
+                torch.distributed.all_reduce(it_t, op=torch.distributed.ReduceOp.SUM)
+            timing[a] = {"max_ms": float(ms.item()), "iters": float(it_t.item()),
+                         "iters_per_solve": last.iterations,
+                         "polish_per_solve": last.polish_iterations,
+                         "e_corr": last.e_corr,
+                         "de_per_particle": abs(last.e_corr - e_conv) / n_part,
+                         "launches": solvers[a].profile()["launches"] - launches0[a]}
 
-    # Kernel-level pass: the same solve with CUDA events around every kernel family.
-    solver.reset()
-    solver.enable_profiling(True)
-    flush.fill_(1.0)
-    torch.cuda.synchronize()
-    rp = solver.solve(tol=tol, max_iters=100, mixing=0.5)
-    prof = solver.profile()
-    solver.enable_profiling(False)
-    work = solver.work_per_iteration()
-    n_t2 = solver.n_t2
+    # Kernel-level pass per arm: one solve with CUDA events around every kernel family.
+    prof, work = {}, {}
+    for a in arms:
+        sol = solvers[a]
+        sol.reset()
+        sol.enable_profiling(True)
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        sol.solve(tol=tol, max_iters=100, mixing=0.5)
+        prof[a] = sol.profile()
+        sol.enable_profiling(False)
+        work[a] = sol.work_per_iteration()
+    n_t2 = solvers[arms[0]].n_t2
 
-    # e2e: the public API from host buffers, every step: create (H2D) + solve + T2 read-back.
+    # e2e (headline arm): the public API from host buffers, every step: create (H2D upload)
+    # + solve + T2 read-back.
     host_t2 = np.empty(n_t2)
     e2e_secs, e2e_iters = 0.0, 0
     h2d = _problem_bytes(system)
     for k in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        s2 = CCDSolver(system, device=local, path=args.path)
+        s2 = CCDSolver(system, device=local, path=args.path, precision=PRECISIONS[arms[0]])
         r2 = s2.solve(tol=tol, max_iters=100, mixing=0.5)
         s2.t2(host_t2)
         s2.close()
@@ -272,49 +307,87 @@ def main():
 
     if rank == 0:
         peaks, peak_kind = measured_peaks()
-        it_p = max(prof["iterations"], 1)
-        ladder_ms = prof["ms_ladder"] / it_p
-        # Algorithmic bytes of one pp-ladder launch: antisymmetry-packed V_pppp (rows a<=b,
-        # columns c<d), the T and X operands and D written in full.
-        ladder_bytes = work["ladder_bytes"]
+        per_it = {}
+        for a in arms:
+            p = prof[a]
+            it_p = max(p["iterations"], 1)
+            per_it[a] = {"pp_ladder": p["ms_ladder"] / it_p, "hh_ladder": p["ms_hh_ladder"] / it_p,
+                         "ring": p["ms_ring"] / it_p, "onebody": p["ms_onebody"] / it_p,
+                         "assemble_energy": p["ms_assemble"] / it_p,
+                         "iteration": p["ms_total"] / it_p}
+        head = arms[0]
+        t = timing[head]
+        value = t["iters"] / (t["max_ms"] / 1000.0)
+        # Roofline of the dominant kernel of the headline arm, the pp ladder: algorithmic
+        # bytes of one launch (antisymmetry-packed V_pppp, T and X operands at the arm's
+        # precision, D written in full) over its average device time.
+        ladder_ms = per_it[head]["pp_ladder"]
+        ladder_bytes = work[head]["ladder_bytes"]
         achieved = ladder_bytes / (ladder_ms / 1000.0) / 1e9
+        kname = "pp_ladder_tc_kernel<2>" if head == "mixed" else "pp_ladder_kernel<0,1,2>"
+        arms_out = {}
+        for a in arms:
+            ta = timing[a]
+            lms = per_it[a]["pp_ladder"]
+            arms_out[a] = {
+                "iter_per_s": ta["iters"] / (ta["max_ms"] / 1000.0),
+                "time_to_converge_ms": ta["max_ms"] / args.steps,
+                "iterations_per_solve": ta["iters_per_solve"],
+                "polish_iterations_per_solve": ta["polish_per_solve"],
+                "e_corr": ta["e_corr"],
+                "abs_de_per_particle_vs_fp64_converged": ta["de_per_particle"],
+                "kernel_ms_per_iteration": per_it[a],
+                "pp_ladder_tflops_algorithmic": work[a]["ladder_flops"] / (lms / 1000.0) / 1e12,
+                "pp_ladder_gbs": work[a]["ladder_bytes"] / (lms / 1000.0) / 1e9,
+                "gpu_launches": int(ta["launches"]),
+            }
+        if "fp64" in arms_out:
+            # Executed FP64 rate: the antisymmetry-packed ladder runs about a quarter of the
+            # reference's 2 pp^2 hh flops (rows a<=b, K over c<d).
+            f = arms_out["fp64"]
+            f["pp_ladder_tflops_executed_approx"] = f["pp_ladder_tflops_algorithmic"] / 4
+            f["pp_ladder_frac_of_fp64_peak"] = f["pp_ladder_tflops_executed_approx"] / FP64_PEAK_TFLOPS
+            f["fp64_peak_tflops"] = FP64_PEAK_TFLOPS
         cpu = None
         if not args.no_cpu_baseline:
             cpu = _cpu_baseline(args.config)
-        r0 = results[-1]
         line = {
             "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": desc, "precision": "fp64", "path": args.path,
-                       "tol": tol, "iterations_per_solve": r0.iterations,
-                       "e_corr": r0.e_corr, "e_corr_per_particle": r0.e_corr / system.n_particles,
-                       "time_to_converge_ms": max_ms / args.steps,
+            "ms_per_step": t["max_ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": ("bf16 2-term split operands, f32 accumulate (pp ladder) + f64"
+                      if head == "mixed" else "f64"),
+            "data": "synthetic",
+            "config": {"workload": desc, "precision": PRECISIONS[head], "path": args.path,
+                       "stop_rule": f"|dE| <= 1e-8 N = {tol:g} (guarantees |dE/N| <= 1e-7)",
+                       "iterations_per_solve": t["iters_per_solve"],
+                       "polish_iterations_per_solve": t["polish_per_solve"],
+                       "e_corr_per_particle": t["e_corr"] / n_part,
+                       "abs_de_per_particle_vs_fp64_converged": t["de_per_particle"],
+                       "time_to_converge_ms": t["max_ms"] / args.steps,
                        "l2": "flushed (256 MiB write) before every step",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
+            "arms": arms_out,
             "e2e": {"value": e2e_i.item() / e2e_t.item(), "unit": "iter/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * n_t2,
                     "what": "ccdgpu_create from host buffers + ccdgpu_solve + ccdgpu_get_t2"},
-            "roofline": {"kernel": "pp_ladder_kernel", "bound": "hbm", "achieved": achieved,
+            "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved,
                          "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "peak_source": peak_kind,
                          "traffic": None, "algorithmic_bytes_per_launch": ladder_bytes,
-                         "avg_launch_ms": ladder_ms,
-                         "flops_per_launch": work["ladder_flops"],
-                         "tflops": work["ladder_flops"] / (ladder_ms / 1000.0) / 1e12},
-            "kernel_ms_per_iteration": {
-                "pp_ladder": ladder_ms, "hh_ladder": prof["ms_hh_ladder"] / it_p,
-                "ring": prof["ms_ring"] / it_p, "onebody": prof["ms_onebody"] / it_p,
-                "assemble_energy": prof["ms_assemble"] / it_p,
-                "iteration": prof["ms_total"] / it_p},
-            "gpu_launches": int(launches),
+                         "avg_launch_ms": ladder_ms},
+            "gpu_launches": int(t["launches"]),
             "clocks": clocks.summary(),
         }
+        if "fp64" in arms_out and head != "fp64":
+            line["config"]["speedup_time_to_converge_vs_fp64"] = (
+                arms_out["fp64"]["time_to_converge_ms"] / arms_out[head]["time_to_converge_ms"])
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line))
-    solver.close()
+    for sol in solvers.values():
+        sol.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 

@@ -1,8 +1,10 @@
 // Device-side data structures and small helpers shared by the CCD kernels.
 #pragma once
 
-#include <cstdint>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
+
+#include <cstdint>
 
 namespace ccd {
 
@@ -42,6 +44,32 @@ __host__ __device__ inline int ladder_bm(int nb) {
   return (kLadderConsumers / cg) * ladder_tm(cg);
 }
 
+// Mixed-precision pp-ladder images (tensor-core operands, ccd_tc.cuh).  A K chunk of a
+// 128-row tile holds kTcKC bf16 per row in 8 x 8 core matrices, K-major, no swizzle:
+//   element (r, k) -> (r / 8) * kTcGroup + (k / 8) * 64 + (r % 8) * 8 + k % 8.
+constexpr int kTcKC = 32;                    // K depth of one chunk (bf16 elements)
+constexpr int kTcBM = 128;                   // rows per tile = UMMA M
+constexpr int kTcMaxNB = 80;                 // padded columns = UMMA N (multiple of 16)
+constexpr int kTcThreads = 192;
+constexpr int kTcAPlane = kTcBM * kTcKC;     // bf16 elements of one A term per stage (8 KB)
+constexpr int kTcBPlane = kTcMaxNB * kTcKC;  // one B term per stage (5 KB)
+constexpr int kTcGroup = 8 * kTcKC;          // bf16 elements of one 8-row group of a chunk
+
+// Padded UMMA N for hh columns.
+__host__ __device__ inline int tc_nb(int hh) { return 16 * ((hh + 15) / 16); }
+// Offset of element (r, k) inside a chunk image (bf16 units), 0 <= k < kTcKC.
+__host__ __device__ inline int tc_off(int r, int k) {
+  return (r >> 3) * kTcGroup + (k >> 3) * 64 + (r & 7) * 8 + (k & 7);
+}
+// x -> nt bf16 terms, each the round-to-nearest of what the previous ones leave (the
+// remainders are exact in double).
+__device__ __forceinline__ void split_bf16(double x, __nv_bfloat16 *out, int nt) {
+  for (int p = 0; p < nt; ++p) {
+    out[p] = __double2bfloat16(x);
+    x -= (double)__bfloat162float(out[p]);
+  }
+}
+
 // One pp-ladder work tile: packed rows [mt*bm, mt*bm+rows) of channel `ch`, V-part K chunks
 // [kc0, kc0+nks).  Tiles of one row block that split K write partial sums; the last one to
 // finish (ticket on counter `group`) adds them in segment order.  The segment with seg ==
@@ -69,6 +97,10 @@ struct ChanInfo {
   int64_t pk_off;    // offset into kcol (pk entries)
   int64_t part_off;  // hh-ladder partial products: nhht * hh*hh doubles
   int64_t hht0;      // first hh-ladder tile of the channel
+  // Mixed-precision operand images (bf16 terms, tensor-core layout; see ccd_tc.cuh):
+  // nbt = UMMA N, nkct / nkht = 32-deep K chunks of V T / T X.
+  int32_t nbt, nkct, nkht, pad_tc;
+  int64_t vtc_base, tkt_tc_base, tmt_tc_base, xt_tc_base;
 };
 
 // hh-ladder split-K tile: rows [k0, k0+kHHRows) of channel ch.
@@ -104,6 +136,10 @@ struct Control {
   int32_t parity;        // which t2 buffer holds the current amplitudes
   int32_t error;         // bit flags, see kErr*
   int32_t active;        // 1 while a solve is running (0: kernels run unconditionally)
+  int32_t phase;         // mixed-precision solve: 1 = split-bf16 ladder, 2 = FP64 polish
+  int32_t pad;
+  double polish_rel;     // phase 1 -> 2 once |dE| <= max(tol, polish_rel * |E|)
+  int64_t polish_iters;  // iterations run in phase 2
   double energies[128];  // corrCCD per iteration (first 128)
 };
 

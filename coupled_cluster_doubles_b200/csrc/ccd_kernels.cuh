@@ -15,6 +15,8 @@
 
 #include <cstdint>
 
+#include <cuda_bf16.h>
+
 #include "ccd_device.cuh"
 
 namespace ccd {
@@ -92,9 +94,13 @@ __device__ __forceinline__ void pdl_enter() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
-__device__ __forceinline__ bool skip_iteration(const Control *ctl) {
+// gate 0: kernel of an FP64 iteration, gate 1: kernel of a mixed-precision iteration.  During
+// a solve, an iteration whose precision does not match the phase is a no-op (a replayed batch
+// can straddle the switch to the FP64 polish).
+__device__ __forceinline__ bool skip_iteration(const Control *ctl, int gate) {
   pdl_enter();
-  return ctl->active && ctl->done;
+  if (!ctl->active) return false;
+  return ctl->done || ((gate == 1) != (ctl->phase == 1));
 }
 
 // ------------------------------------------------------------------------------------------
@@ -260,8 +266,8 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict_
                  const double *__restrict__ t_kt, const double *__restrict__ t_mt,
                  const double *__restrict__ x_t, const int32_t *__restrict__ rowmap,
                  const int32_t *__restrict__ mirror, double *__restrict__ d, double *part,
-                 int32_t *counters, const Control *ctl, int32_t *err) {
-  if (skip_iteration(ctl)) return;
+                 int32_t *counters, const Control *ctl, int32_t *err, int gate) {
+  if (skip_iteration(ctl, gate)) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double *As = reinterpret_cast<double *>(smem_raw);
   double *Bs = As + kStages * kMaxBM * kBK;
@@ -355,8 +361,9 @@ hh_ladder_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ 
                  const double *__restrict__ v_pphh, const double *__restrict__ v_hhhh,
                  const double *tbuf0, const double *tbuf1, double *part, int32_t *counters,
                  double *__restrict__ x_ref, double *__restrict__ x_t, double *__restrict__ s_out,
-                 double *__restrict__ r_out, const Control *ctl) {
-  if (skip_iteration(ctl)) return;
+                 double *__restrict__ r_out, __nv_bfloat16 *__restrict__ xt_tc,
+                 int64_t xt_tc_stride, int nt, const Control *ctl, int gate) {
+  if (skip_iteration(ctl, gate)) return;
   extern __shared__ __align__(16) double hsm[];
   __shared__ int last;
   const HHTile tt = tiles[blockIdx.x];
@@ -398,6 +405,13 @@ hh_ladder_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ 
     const double x = v_hhhh[ch.x_off + idx] + 0.5 * p;
     x_ref[ch.x_off + idx] = x;
     x_t[ch.xt_base + (int64_t)(kl / kBK) * kBK * nb + (kl % kBK) * nb + ij] = 0.5 * x;
+    if (nt) {
+      __nv_bfloat16 hv[3];
+      split_bf16(0.5 * x, hv, nt);
+      const int64_t o =
+          ch.xt_tc_base + (int64_t)(kl >> 5) * (ch.nbt >> 3) * kTcGroup + tc_off(ij, kl & 31);
+      for (int p = 0; p < nt; ++p) xt_tc[p * xt_tc_stride + o] = hv[p];
+    }
     if (kl == ij) s_out[ch.hh_off + ij] = p;
   }
   if (tid == 0) counters[tt.ch] = 0;
@@ -413,8 +427,8 @@ constexpr int kRingSmall = 16;
 __global__ void __launch_bounds__(256)
 ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restrict__ v_hpph,
                   const double *__restrict__ v_hphp, const double *__restrict__ t_phhp,
-                  double *__restrict__ r_phhp, const Control *ctl) {
-  if (skip_iteration(ctl)) return;
+                  double *__restrict__ r_phhp, const Control *ctl, int gate) {
+  if (skip_iteration(ctl, gate)) return;
   __shared__ double buf[8][3 * kRingSmall * kRingSmall];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int mi = blockIdx.x * 8 + w;
@@ -442,8 +456,8 @@ ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restr
 __global__ void __launch_bounds__(kRingThreads)
 ring_kernel(const ModInfo *__restrict__ mods, const double *__restrict__ v_hpph,
             const double *__restrict__ v_hphp, const double *__restrict__ t_phhp,
-            double *__restrict__ r_phhp, const Control *ctl) {
-  if (skip_iteration(ctl)) return;
+            double *__restrict__ r_phhp, const Control *ctl, int gate) {
+  if (skip_iteration(ctl, gate)) return;
   extern __shared__ __align__(16) double rs[];
   const ModInfo m = mods[blockIdx.x];
   const int ph = m.ph, hp = m.hp, tid = threadIdx.x;
@@ -523,8 +537,8 @@ onebody_tables_kernel(int np, const int64_t *__restrict__ o_h, const int64_t *__
 __global__ void onebody_fused_kernel(int np, int nsp, const int64_t *__restrict__ list_off,
                                      const int32_t *__restrict__ list, const double *__restrict__ s,
                                      const double *__restrict__ r, double *__restrict__ xh,
-                                     double *__restrict__ yp, const Control *ctl) {
-  if (skip_iteration(ctl)) return;
+                                     double *__restrict__ yp, const Control *ctl, int gate) {
+  if (skip_iteration(ctl, gate)) return;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (w >= nsp) return;
   const bool hole = w < np;
@@ -564,6 +578,31 @@ __device__ __forceinline__ void write_t_tiles(const ChanInfo &ch, const int2 *__
   }
 }
 
+// The same amplitude into the mixed-precision operand images: nt bf16 terms of T in the
+// tensor-core chunk layout (tc_off), V T operand B (K = c<d pair) and T X operand A (rows a<=b,
+// compact last 128-row tile, K = hh).
+__device__ __forceinline__ void write_t_tiles_tc(const ChanInfo &ch,
+                                                 const int2 *__restrict__ pk_idx, int ab, int ij,
+                                                 double t, int nt, __nv_bfloat16 *tkt_tc,
+                                                 int64_t tkt_stride, __nv_bfloat16 *tmt_tc,
+                                                 int64_t tmt_stride) {
+  const int2 q = pk_idx[ch.pp_off + ab];
+  __nv_bfloat16 hv[3];
+  split_bf16(t, hv, nt);
+  if (q.x >= 0) {
+    const int64_t o =
+        ch.tkt_tc_base + (int64_t)(q.x >> 5) * (ch.nbt >> 3) * kTcGroup + tc_off(ij, q.x & 31);
+    for (int p = 0; p < nt; ++p) tkt_tc[p * tkt_stride + o] = hv[p];
+  }
+  if (q.y >= 0) {
+    const int mt = q.y >> 7, r = q.y & 127;
+    const int rg = (min(kTcBM, ch.pr - mt * kTcBM) + 7) >> 3;
+    const int64_t o = ch.tmt_tc_base + (int64_t)mt * kTcBM * ch.nkht * kTcKC +
+                      (int64_t)(ij >> 5) * rg * kTcGroup + tc_off(r, ij & 31);
+    for (int p = 0; p < nt; ++p) tmt_tc[p * tmt_stride + o] = hv[p];
+  }
+}
+
 // ------------------------------------------------------------------------------------------
 // Fused assembly (calc.cpp:384-418 plus the remaps folded in):
 //   value = V + D + R_ai,jb - R_aj,ib - R_bi,ja + R_bj,ia          (4 gathers from R in phhp layout)
@@ -590,8 +629,11 @@ assemble_fused_kernel(const ElemRange *__restrict__ ranges, const ChanInfo *__re
                       const double *__restrict__ yp, const double *__restrict__ eps, int np,
                       double *tbuf0, double *tbuf1, double *__restrict__ old_phhp,
                       double *__restrict__ t_kt, double *__restrict__ t_mt,
-                      double *__restrict__ epart, int32_t *ticket, Control *ctl) {
-  if (skip_iteration(ctl)) return;
+                      double *__restrict__ epart, int32_t *ticket, Control *ctl,
+                      __nv_bfloat16 *__restrict__ tkt_tc, int64_t tkt_tc_stride,
+                      __nv_bfloat16 *__restrict__ tmt_tc, int64_t tmt_tc_stride, int nt,
+                      int gate) {
+  if (skip_iteration(ctl, gate)) return;
   __shared__ double scratch[32];
   __shared__ int last;
   const ElemRange rg = ranges[blockIdx.x];
@@ -624,6 +666,8 @@ assemble_fused_kernel(const ElemRange *__restrict__ ranges, const ChanInfo *__re
     t_new[e] = value;
     old_phhp[g_ai_jb[e]] = value;
     write_t_tiles(ch, pk_idx, ab, ij, value, t_kt, t_mt);
+    if (nt) write_t_tiles_tc(ch, pk_idx, ab, ij, value, nt, tkt_tc, tkt_tc_stride, tmt_tc,
+                             tmt_tc_stride);
     corr += v * value;
   }
   const double sum = block_sum<kAsmThreads>(corr, scratch);
@@ -699,7 +743,9 @@ __global__ void map_to_kernel(const ElemRange *__restrict__ ranges, const ChanIn
                               double *__restrict__ old_h2pp_h1, double *__restrict__ old_h1pp_h2,
                               double *__restrict__ old_p1_p2hh, double *__restrict__ old_p2_p1hh,
                               double *__restrict__ old_phhp, double *__restrict__ t_kt,
-                              double *__restrict__ t_mt, int with_3body) {
+                              double *__restrict__ t_mt, int with_3body,
+                              __nv_bfloat16 *__restrict__ tkt_tc, int64_t tkt_tc_stride,
+                              __nv_bfloat16 *__restrict__ tmt_tc, int64_t tmt_tc_stride, int nt) {
   const ElemRange rg = ranges[blockIdx.x];
   const ChanInfo ch = chans[rg.ch];
   for (int64_t e = rg.e0 + threadIdx.x; e < rg.e1; e += blockDim.x) {
@@ -715,6 +761,8 @@ __global__ void map_to_kernel(const ElemRange *__restrict__ ranges, const ChanIn
     const int64_t loc = e - ch.t_off;
     const int ab = (int)(loc / ch.hh), ij = (int)(loc - (int64_t)ab * ch.hh);
     write_t_tiles(ch, pk_idx, ab, ij, t, t_kt, t_mt);
+    if (nt) write_t_tiles_tc(ch, pk_idx, ab, ij, t, nt, tkt_tc, tkt_tc_stride, tmt_tc,
+                             tmt_tc_stride);
   }
 }
 
@@ -749,25 +797,36 @@ __device__ __forceinline__ void energy_reduce(const double *epart, int n, Contro
     const double corr = 0.25 * (ss[0] + cs[0]);
     if (e_out) *e_out = corr;
     if (flags & 2) {
-      const double diff = corr - ctl->e_prev;
+      const double diff = corr - ctl->e_prev, prev_diff = ctl->e_diff;
       ctl->e_prev = corr;
       ctl->e_corr = corr;
       ctl->e_diff = diff;
       if (ctl->iterations < 128) ctl->energies[ctl->iterations] = corr;
       ctl->iterations += 1;
+      if (ctl->active && ctl->phase == 2) ctl->polish_iters += 1;
       if (!isfinite(corr)) {
         ctl->error |= kErrNonFinite;
         ctl->done = 1;
       }
-      if (fabs(diff) <= ctl->tol || ctl->iterations > ctl->max_iters) ctl->done = 1;
+      if (ctl->active && ctl->phase == 1) {
+        // Mixed phase: hand over to FP64 iterations once the energy change reaches the
+        // rounding floor of the split-bf16 ladder, or stops shrinking.
+        if (fabs(diff) <= fmax(ctl->tol, ctl->polish_rel * fabs(corr)) ||
+            (ctl->iterations > 2 && fabs(diff) >= fabs(prev_diff)))
+          ctl->phase = 2;
+        if (ctl->iterations > ctl->max_iters) ctl->done = 1;
+      } else if (fabs(diff) <= ctl->tol || ctl->iterations > ctl->max_iters) {
+        ctl->done = 1;
+      }
     }
     if (flags & 1) ctl->parity ^= 1;
   }
 }
 
 __global__ void __launch_bounds__(kEnergyThreads)
-energy_kernel(const double *__restrict__ epart, int n, Control *ctl, int flags, double *e_out) {
-  if (skip_iteration(ctl)) return;
+energy_kernel(const double *__restrict__ epart, int n, Control *ctl, int flags, double *e_out,
+              int gate) {
+  if (skip_iteration(ctl, gate)) return;
   energy_reduce(epart, n, ctl, flags, e_out);
 }
 

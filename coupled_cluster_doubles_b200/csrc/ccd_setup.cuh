@@ -43,6 +43,28 @@ __global__ void tile_v_kernel(const ChanInfo *__restrict__ chans, const int2 *__
     v_t[tb + (int64_t)(w / kBK) * rows * kBK + swzA(u - mt * ch.bm, w % kBK)] = src[kcol[ch.pk_off + w]];
 }
 
+// Packed V_pppp as nt bf16 terms in the tensor-core chunk images of the mixed-precision
+// ladder (128-row tiles, 32-deep K chunks, compact last tile); one CTA per packed row.
+__global__ void tile_v_tc_kernel(const ChanInfo *__restrict__ chans, const int2 *__restrict__ items,
+                                 const int32_t *__restrict__ rowmap, const int32_t *__restrict__ kcol,
+                                 const int64_t *__restrict__ vraw_off, const double *__restrict__ vraw,
+                                 __nv_bfloat16 *__restrict__ v_tc, int64_t stride, int nt) {
+  const int2 it = items[blockIdx.x];
+  const ChanInfo ch = chans[it.x];
+  const int u = it.y;
+  const int ab = rowmap[ch.row_off + u];
+  const double *src = vraw + vraw_off[it.x] + (int64_t)ab * ch.pp;
+  const int mt = u >> 7, r = u & 127;
+  const int rg = (min(kTcBM, ch.pr - mt * kTcBM) + 7) >> 3;
+  const int64_t tb = ch.vtc_base + (int64_t)mt * kTcBM * ch.nkct * kTcKC;
+  for (int w = threadIdx.x; w < ch.pk; w += blockDim.x) {
+    __nv_bfloat16 hv[3];
+    split_bf16(src[kcol[ch.pk_off + w]], hv, nt);
+    const int64_t o = tb + (int64_t)(w >> 5) * rg * kTcGroup + tc_off(r, w & 31);
+    for (int p = 0; p < nt; ++p) v_tc[p * stride + o] = hv[p];
+  }
+}
+
 // The eight loadMaps tables -> int32 flat offsets into their target chains, with range checks
 // and, for the five tables that are also scatter targets (mapToDistributed), hit counts that
 // check_counts_kernel then requires to be exactly one.

@@ -1,0 +1,270 @@
+// Mixed-precision pp ladder on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+//   D[ab,:] = sum_{c<d} V[ab,cd] T[cd,:] + T[ab,:] (X/2)        packed rows a <= b
+//
+// is the same antisymmetry-packed product as pp_ladder_kernel (calc.cpp:162-202), with every
+// operand split into NT bf16 terms, x = x_0 + x_1 (+ x_2), each term the bf16 rounding of what
+// the previous ones leave.  The products x_p y_q with p + q < NT are summed by
+// tcgen05.mma.kind::f16 (bf16 inputs, FP32 accumulator in tensor memory): NT = 2 carries
+// about 17 significant bits per operand, NT = 3 about 25.  The ladder is the only mixed
+// contraction; the CCD iteration around it stays FP64, and the solver finishes with FP64
+// iterations (the fixed point does not depend on how D was rounded on the way).
+//
+// Operand images.  A 128-row x 32-deep K chunk of one term is stored in HBM exactly as the
+// tensor core reads it from shared memory: the K-major, non-swizzled canonical layout made of
+// 8 x 8 "core matrices" (8 rows of 16 bytes, 128 contiguous bytes):
+//   element (r, k) of a chunk -> (r / 8) * 256 + (k / 8) * 64 + (r % 8) * 8 + k % 8   (bf16)
+// (tc_off in ccd_device.cuh), so one 1-D bulk copy per term moves a stage, and the smem
+// descriptors use LBO = 128 bytes (next core matrix along K) and SBO = 512 bytes (next 8-row
+// group).  The last row tile of a channel is compact (only its ceil(rows/8) row groups are
+// stored); the rows beyond it in shared memory are stale and only reach accumulator rows that
+// the epilogue never reads.  K padding is zero in both operands.
+//
+// CTA roles (192 threads): warps 0-3 read the accumulator back (warp w owns TMEM lanes
+// 32w..32w+31 = tile rows), warp 4 is the bulk-copy producer, warp 5 allocates tensor memory
+// and one of its lanes issues the MMAs.  Every mbarrier wait is bounded (kWaitLimitNs); on a
+// timeout the kernel sets kErrTimeout, lets the copies it issued land, waits for its MMAs and
+// frees its tensor memory before returning.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include <cstdint>
+
+#include "ccd_device.cuh"
+#include "ccd_kernels.cuh"
+
+namespace ccd {
+
+__host__ __device__ constexpr int tc_stages(int nt) { return nt == 2 ? 4 : 3; }
+__host__ __device__ constexpr size_t tc_stage_bytes(int nt) {
+  return (size_t)nt * (kTcAPlane + kTcBPlane) * 2;
+}
+// Dynamic shared memory: 1024 bytes of alignment slack, the stages, then the barriers.
+__host__ __device__ constexpr size_t tc_smem_bytes(int nt) {
+  return 1024 + tc_stages(nt) * tc_stage_bytes(nt) + 256;
+}
+
+// --- tcgen05 / descriptor helpers --------------------------------------------------------
+
+// Shared-memory matrix descriptor, K-major, no swizzle (sm_100 version 1 descriptor).
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) |
+         ((uint64_t)(512 >> 4) << 32) | (1ull << 46);
+}
+// Instruction descriptor: bf16 x bf16 -> f32, both K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t tc_idesc(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(kTcBM >> 4) << 24);
+}
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+// Arrive (once) on an mbarrier when every tcgen05 operation this thread issued so far is done.
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// 32 lanes x 16 consecutive 32-bit columns: thread t of the warp gets lane (base + t).
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float *v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Tensor-memory columns for an N-column FP32 accumulator (a power of two, at least 32).
+__host__ __device__ inline uint32_t tc_tmem_cols(int nb) {
+  return nb <= 32 ? 32u : nb <= 64 ? 64u : 128u;
+}
+
+// AND of a predicate over the 128 epilogue threads (named barrier 1): a uniform decision.
+__device__ __forceinline__ bool consumers_all(bool v) {
+  uint32_t r;
+  asm volatile(
+      "{ .reg .pred p, q; setp.ne.u32 p, %1, 0; bar.red.and.pred q, 1, %2, p; "
+      "selp.u32 %0, 1, 0, q; }"
+      : "=r"(r)
+      : "r"((uint32_t)v), "n"(kLadderConsumers)
+      : "memory");
+  return r != 0;
+}
+__device__ __forceinline__ int read_flag(const int *f) { return *(const volatile int *)f; }
+
+// Bulk copies of the stages that were issued but may not have landed (error path only).
+__device__ __forceinline__ void tc_drain(const uint64_t *full, int issued, int stages) {
+  for (int c = issued - stages < 0 ? 0 : issued - stages; c < issued; ++c)
+    (void)mbar_wait(smem_u32(&full[c % stages]), (c / stages) & 1);
+}
+
+// One CTA = one LadderTile (bm = 128, nb = UMMA N, K chunks of kTcKC).  Image arrays hold NT
+// planes each, plane p at base + p * stride.  A mixed-phase kernel (gate 1 of skip_iteration).
+template <int NT>
+__global__ void __launch_bounds__(kTcThreads, 1)
+pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const __nv_bfloat16 *__restrict__ v_tc,
+                    int64_t v_stride, const __nv_bfloat16 *__restrict__ tkt_tc, int64_t tkt_stride,
+                    const __nv_bfloat16 *__restrict__ tmt_tc, int64_t tmt_stride,
+                    const __nv_bfloat16 *__restrict__ xt_tc, int64_t xt_stride,
+                    const int32_t *__restrict__ rowmap, const int32_t *__restrict__ mirror,
+                    double *__restrict__ d, double *part, int32_t *counters, const Control *ctl,
+                    int32_t *err) {
+  if (skip_iteration(ctl, 1)) return;
+  constexpr int S = tc_stages(NT);
+  constexpr uint32_t kStageBytes = (uint32_t)tc_stage_bytes(NT);
+  extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
+  __shared__ uint32_t tmem_holder;
+  __shared__ int abort_flag, issued_chunks;
+  const uint32_t raw = smem_u32(tc_smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;  // stage s at base + s * kStageBytes
+  uint64_t *bars = reinterpret_cast<uint64_t *>(tc_smem_raw + (base - raw) + S * kStageBytes);
+  uint64_t *full = bars, *empty = bars + S, *done = bars + 2 * S;
+  const LadderTile tile = tiles[blockIdx.x];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t ncols = tc_tmem_cols(tile.nb);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(smem_u32(&full[s]), 1);
+      mbar_init(smem_u32(&empty[s]), 1);
+    }
+    mbar_init(smem_u32(done), 1);
+    abort_flag = 0;
+    issued_chunks = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 5) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 ::"r"(smem_u32(&tmem_holder)), "r"(ncols) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_holder;
+  const int nchunks = tile.nks + tile.nkh;
+  const int rg = (tile.rows + 7) >> 3;   // stored row groups of this row tile's A chunks
+  const int ng = tile.nb >> 3;           // row groups of a B chunk
+  const uint32_t abytes = (uint32_t)rg * kTcGroup * 2, bbytes = (uint32_t)ng * kTcGroup * 2;
+
+  if (warp == 4) {
+    // ---- producer ----
+    if (lane == 0) {
+      const int64_t vtile = tile.v_base + (int64_t)tile.mt * kTcBM * tile.nkc * kTcKC;
+      const int64_t ttile = tile.tmt_base + (int64_t)tile.mt * kTcBM * tile.nkh * kTcKC;
+      int issued = 0;
+      for (int c = 0; c < nchunks; ++c) {
+        const int s = c % S;
+        if (c >= S && !mbar_wait(smem_u32(&empty[s]), ((c / S) - 1) & 1)) {
+          atomicOr(err, kErrTimeout);
+          atomicExch(&abort_flag, 1);
+          break;
+        }
+        const __nv_bfloat16 *asrc, *bsrc;
+        int64_t as, bs;
+        if (c < tile.nks) {
+          const int kc = tile.kc0 + c;
+          asrc = v_tc + vtile + (int64_t)kc * rg * kTcGroup;
+          bsrc = tkt_tc + tile.tkt_base + (int64_t)kc * ng * kTcGroup;
+          as = v_stride;
+          bs = tkt_stride;
+        } else {
+          const int kh = c - tile.nks;
+          asrc = tmt_tc + ttile + (int64_t)kh * rg * kTcGroup;
+          bsrc = xt_tc + tile.xt_base + (int64_t)kh * ng * kTcGroup;
+          as = tmt_stride;
+          bs = xt_stride;
+        }
+        const uint32_t fb = smem_u32(&full[s]);
+        const uint32_t sa = base + s * kStageBytes, sb = sa + NT * kTcAPlane * 2;
+        mbar_expect_tx(fb, NT * (abytes + bbytes));
+#pragma unroll
+        for (int p = 0; p < NT; ++p) {
+          bulk_g2s(sa + p * kTcAPlane * 2, asrc + p * as, abytes, fb);
+          bulk_g2s(sb + p * kTcBPlane * 2, bsrc + p * bs, bbytes, fb);
+        }
+        ++issued;
+      }
+      issued_chunks = issued;
+    }
+  } else if (warp == 5) {
+    // ---- MMA issuer ----
+    if (lane == 0) {
+      const uint32_t idesc = tc_idesc(tile.nb);
+      for (int c = 0; c < nchunks; ++c) {
+        const int s = c % S;
+        if (read_flag(&abort_flag) || !mbar_wait(smem_u32(&full[s]), (c / S) & 1)) {
+          atomicOr(err, kErrTimeout);
+          atomicExch(&abort_flag, 1);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = base + s * kStageBytes, sb = sa + NT * kTcAPlane * 2;
+#pragma unroll
+        for (int j = 0; j < kTcKC / 16; ++j) {
+#pragma unroll
+          for (int pa = 0; pa < NT; ++pa)
+#pragma unroll
+            for (int pb = 0; pb < NT - pa; ++pb)
+              tc_mma(tmem, tc_desc(sa + pa * kTcAPlane * 2 + j * 256),
+                     tc_desc(sb + pb * kTcBPlane * 2 + j * 256), idesc,
+                     (c | j | pa | pb) != 0 ? 1u : 0u);
+        }
+        tc_commit(smem_u32(&empty[s]));
+      }
+      tc_commit(smem_u32(done));  // also after an abort: the epilogue waits for issued MMAs
+    }
+  } else {
+    // ---- epilogue: accumulator rows -> D (or split-K partials) ----
+    const bool ok = mbar_wait(smem_u32(done), 0);
+    tc_fence_after();
+    const int tid = threadIdx.x;
+    const LadderOut out{tile, rowmap, mirror, d, part};
+    if (!ok) atomicOr(err, kErrTimeout);
+    // One decision for all four warps (ladder_reduce synchronises them again).
+    if (consumers_all(ok && !read_flag(&abort_flag) && nchunks > 0)) {
+      const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+      for (int c0 = 0; c0 < tile.nb; c0 += 16) {
+        float v[16];
+        tc_ld16(lane_addr + c0, v);
+        double dv[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) dv[i] = (double)v[i];
+        out.row(tid, c0, dv, 16);
+      }
+      if (tile.nseg > 1) ladder_reduce(tile, tid, counters, rowmap, mirror, d, part);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  // After an abort, copies the MMA warp never waited for may still be in flight: let them land
+  // before the CTA's shared memory is released.
+  if (warp == 4 && lane == 0 && read_flag(&abort_flag)) tc_drain(full, issued_chunks, S);
+  if (warp == 5) {
+    // The MMAs this CTA issued are complete once `done` has fired (it was committed on every
+    // path); only then is the accumulator released.
+    (void)mbar_wait(smem_u32(done), 0);
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols)
+                 : "memory");
+  }
+}
+
+}  // namespace ccd

@@ -22,6 +22,7 @@
 #include "ccd_device.cuh"
 #include "ccd_kernels.cuh"
 #include "ccd_setup.cuh"
+#include "ccd_tc.cuh"
 #include "ccdgpu.h"
 
 using namespace ccd;
@@ -85,6 +86,19 @@ struct ccdgpu_handle {
   double flops = 0, v_bytes = 0, v_packed_bytes = 0, ladder_flops = 0, ladder_bytes = 0;
   int64_t n_tkt = 0, n_tmt = 0;
   int64_t launches = 0;
+
+  // Mixed precision (nt bf16 terms per operand; 0 for an FP64 handle).
+  int nt = 0;
+  int n_tc_tiles = 0;
+  LadderTile *tc_tiles = nullptr;
+  int32_t *tc_counters = nullptr;
+  double *tc_part = nullptr;
+  __nv_bfloat16 *v_tc = nullptr, *tkt_tc = nullptr, *tmt_tc = nullptr, *xt_tc = nullptr;
+  int64_t n_vtc = 0, n_tkttc = 0, n_tmttc = 0, n_xttc = 0;  // plane strides (elements)
+  size_t tc_smem = 0;
+  double ladder_bytes_tc = 0;
+  cudaGraphExec_t graph_tc = nullptr;
+  int64_t kernels_per_graph_tc = 0;
 };
 
 namespace {
@@ -121,6 +135,7 @@ int find_pair(const ccdgpu_pair *list, int64_t n, uint64_t p, uint64_t q) {
 void release(ccdgpu_handle *h) {
   if (!h) return;
   if (h->graph) cudaGraphExecDestroy(h->graph);
+  if (h->graph_tc) cudaGraphExecDestroy(h->graph_tc);
   for (auto &b : h->allocs) cudaFree(b.p);
   h->allocs.clear();
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
@@ -215,6 +230,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   std::vector<std::vector<int32_t>> seg(nsp);
   int64_t pp_tot = 0, hh_tot = 0, x_tot = 0, tkt = 0, tmt = 0, xt = 0, vt = 0, part_tot = 0;
   int64_t vraw_tot = 0;
+  int64_t vtc = 0, tkttc = 0, tmttc = 0, xttc = 0;
   std::vector<int64_t> vraw_off;
   int maxhh = 1;
   for (uint64_t c = 0; c < nch; c++) {
@@ -268,6 +284,14 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     ci.tkt_base = tkt; ci.tmt_base = tmt; ci.xt_base = xt; ci.vkt_base = vt;
     ci.part_off = part_tot;
     ci.hht0 = (int64_t)hh_tiles.size();
+    ci.nbt = tc_nb(ci.hh);
+    ci.nkct = (int)ceil_div(pk, kTcKC);
+    ci.nkht = (int)ceil_div(hh, kTcKC);
+    ci.vtc_base = vtc; ci.tkt_tc_base = tkttc; ci.tmt_tc_base = tmttc; ci.xt_tc_base = xttc;
+    vtc += (int64_t)ci.nkct * kTcGroup * ceil_div(pr, 8);
+    tmttc += (int64_t)ci.nkht * kTcGroup * ceil_div(pr, 8);
+    tkttc += (int64_t)ci.nkct * (ci.nbt / 8) * kTcGroup;
+    xttc += (int64_t)ci.nkht * (ci.nbt / 8) * kTcGroup;
     const int nb = ci.nb;
     pp_tot += pp; hh_tot += hh; x_tot += hh * hh;
     tkt += (int64_t)ci.nkc * kBK * nb;
@@ -375,6 +399,48 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   });
   h->n_tiles = (int)tiles.size();
   for (const LadderTile &t : tiles) h->n_cls[cls_of(t.nb)]++;
+
+  // Mixed-precision ladder tiles: 128-row tiles of every channel in one launch.  The tensor
+  // cores leave each CTA bandwidth bound, so K is split (deterministic reduction) until there
+  // are about two tiles per SM.
+  std::vector<LadderTile> tc_tiles;
+  int64_t tcpart_tot = 0;
+  int32_t tc_groups = 0;
+  if (h->nt) {
+    int64_t blocks = 0;
+    for (const ChanInfo &a : chans) blocks += ceil_div(a.pr, kTcBM);
+    const int want = (int)std::min<int64_t>(16, std::max<int64_t>(1, ceil_div(2 * kSMs, blocks)));
+    for (int ai = 0; ai < h->n_act; ai++) {
+      const ChanInfo &a = chans[ai];
+      const int nmt = (int)ceil_div(a.pr, kTcBM);
+      const int nseg = std::max(1, std::min(want, a.nkct / 4));
+      for (int mt = 0; mt < nmt; mt++) {
+        const int rows = std::min(kTcBM, a.pr - mt * kTcBM);
+        const int64_t pbase = tcpart_tot;
+        if (nseg > 1) tcpart_tot += (int64_t)nseg * kTcBM * a.nbt;
+        for (int sg = 0; sg < nseg; sg++) {
+          LadderTile tl{};
+          tl.ch = ai; tl.mt = mt;
+          tl.kc0 = (int)((int64_t)a.nkct * sg / nseg);
+          tl.nks = (int)((int64_t)a.nkct * (sg + 1) / nseg) - tl.kc0;
+          tl.nkc = a.nkct;
+          tl.nkh = (sg == nseg - 1) ? a.nkht : 0;
+          tl.nb = a.nbt; tl.bm = kTcBM; tl.rows = rows; tl.pr = a.pr; tl.hh = a.hh;
+          tl.seg = sg; tl.nseg = nseg; tl.group = tc_groups;
+          tl.v_base = a.vtc_base; tl.tkt_base = a.tkt_tc_base; tl.tmt_base = a.tmt_tc_base;
+          tl.xt_base = a.xt_tc_base; tl.t_off = a.t_off; tl.row_off = a.row_off;
+          tl.part_base = pbase;
+          tc_tiles.push_back(tl);
+        }
+        tc_groups++;
+      }
+    }
+    // Largest byte streams first.
+    std::stable_sort(tc_tiles.begin(), tc_tiles.end(), [](const LadderTile &x, const LadderTile &y) {
+      return (int64_t)(x.nks + x.nkh) * (x.rows + x.nb) > (int64_t)(y.nks + y.nkh) * (y.rows + y.nb);
+    });
+  }
+  h->n_tc_tiles = (int)tc_tiles.size();
   std::vector<ElemRange> ranges;
   const int64_t per = (int64_t)kAsmThreads * kAsmPerThread;
   for (int ai = 0; ai < h->n_act; ai++) {
@@ -400,6 +466,11 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   for (const ChanInfo &a : chans)
     lb += 8.0 * ((double)a.pk * a.hh + (double)a.pr * a.hh + (double)a.hh * a.hh + (double)a.pp * a.hh);
   h->ladder_bytes = lb;
+  double lbt = 0;
+  for (const ChanInfo &a : chans)
+    lbt += 2.0 * h->nt * ((double)a.pr * a.pk + (double)a.pk * a.hh + (double)a.pr * a.hh +
+                          (double)a.hh * a.hh) + 8.0 * a.pp * (double)a.hh;
+  h->ladder_bytes_tc = lbt;
   h->n_tkt = tkt;
   h->n_tmt = tmt;
 
@@ -425,6 +496,15 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   ar.add(&h->s, hh_tot); ar.add(&h->r, pp_tot); ar.add(&h->xh, np); ar.add(&h->yp, h->npart);
   ar.add(&h->epart, h->n_ranges); ar.add(&h->ctl, 1); ar.add(&h->e_out, 1); ar.add(&h->err, 1);
   ar.add(&h->ticket, 1);
+  if (h->nt) {
+    auto round_up = [](int64_t n) { return std::max<int64_t>(256, (n + 255) / 256 * 256); };
+    h->n_vtc = round_up(vtc); h->n_tkttc = round_up(tkttc);
+    h->n_tmttc = round_up(tmttc); h->n_xttc = round_up(xttc);
+    ar.add(&h->tc_tiles, tc_tiles.size()); ar.add(&h->tc_counters, tc_groups);
+    ar.add(&h->tc_part, tcpart_tot);
+    ar.add(&h->v_tc, (size_t)h->nt * h->n_vtc); ar.add(&h->tkt_tc, (size_t)h->nt * h->n_tkttc);
+    ar.add(&h->tmt_tc, (size_t)h->nt * h->n_tmttc); ar.add(&h->xt_tc, (size_t)h->nt * h->n_xttc);
+  }
   if (h->have_3body) {
     ar.add(&h->v_h_hpp, h->n_h); ar.add(&h->v_phh_p, h->n_p);
     ar.add(&h->old_h1pp_h2, h->n_h); ar.add(&h->old_h2pp_h1, h->n_h); ar.add(&h->diff_h2pp_h1, h->n_h);
@@ -454,6 +534,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   };
   TRY(put(h->chans, chans)); TRY(put(h->mods, mods)); TRY(put(h->tiles, tiles));
   TRY(put(h->hh_tiles, hh_tiles)); TRY(put(h->ranges, ranges));
+  if (h->nt) TRY(put(h->tc_tiles, tc_tiles));
   TRY(put(h->pp_pairs, pp_pairs)); TRY(put(h->hh_pairs, hh_pairs));
   TRY(put(h->pp_swap, pp_swap)); TRY(put(h->hh_swap, hh_swap));
   TRY(put(h->list_off, list_off)); TRY(put(h->list, list));
@@ -523,6 +604,11 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     tile_v_kernel<<<(unsigned)vrows.size(), 128, 0, h->s0>>>(h->chans, d_vrows, h->rowmap, d_kcol,
                                                              d_vraw_off, vraw, h->v_t);
     CK(cudaGetLastError());
+    if (h->nt) {
+      tile_v_tc_kernel<<<(unsigned)vrows.size(), 128, 0, h->s0>>>(
+          h->chans, d_vrows, h->rowmap, d_kcol, d_vraw_off, vraw, h->v_tc, h->n_vtc, h->nt);
+      CK(cudaGetLastError());
+    }
   }
   int32_t e = 0;
   CK(cudaMemcpyAsync(&e, h->err, sizeof(e), cudaMemcpyDeviceToHost, h->s0));
@@ -552,6 +638,15 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
                           (int)h->hh_smem));
   CK(cudaFuncSetAttribute(ring_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)std::max<size_t>(h->ring_smem, 16)));
+  if (h->nt) {
+    h->tc_smem = tc_smem_bytes(h->nt);
+    if (h->nt == 2)
+      CK(cudaFuncSetAttribute(pp_ladder_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)h->tc_smem));
+    else
+      CK(cudaFuncSetAttribute(pp_ladder_tc_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)h->tc_smem));
+  }
   return CCDGPU_OK;
 }
 
@@ -576,12 +671,28 @@ cudaError_t launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, 
   return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
 }
 
-int launch_hh_ladder(ccdgpu_handle *h, cudaStream_t st) {
+// gate: 0 = kernel of an FP64 iteration, 1 = of a mixed-precision iteration (which also writes
+// the bf16 operand images of the tensor-core ladder).
+int launch_hh_ladder(ccdgpu_handle *h, cudaStream_t st, int gate) {
   if (!h->n_hh_tiles) return CCDGPU_OK;
   h->launches++;
   return cuda_status(launch_pdl(hh_ladder_kernel, h->n_hh_tiles, kHHThreads, h->hh_smem, st,
                                 h->hh_tiles, h->chans, h->v_pphh, h->v_hhhh, h->t[0], h->t[1],
-                                h->part, h->counters, h->x, h->x_t, h->s, h->r, h->ctl));
+                                h->part, h->counters, h->x, h->x_t, h->s, h->r, h->xt_tc,
+                                h->n_xttc, gate ? h->nt : 0, h->ctl, gate));
+}
+int launch_pp_ladder_tc(ccdgpu_handle *h, cudaStream_t st) {
+  if (!h->n_tc_tiles) return CCDGPU_OK;
+  h->launches++;
+  if (h->nt == 2)
+    return cuda_status(launch_pdl(pp_ladder_tc_kernel<2>, h->n_tc_tiles, kTcThreads, h->tc_smem,
+                                  st, h->tc_tiles, h->v_tc, h->n_vtc, h->tkt_tc, h->n_tkttc,
+                                  h->tmt_tc, h->n_tmttc, h->xt_tc, h->n_xttc, h->rowmap,
+                                  h->mirror, h->dmat, h->tc_part, h->tc_counters, h->ctl, h->err));
+  return cuda_status(launch_pdl(pp_ladder_tc_kernel<3>, h->n_tc_tiles, kTcThreads, h->tc_smem,
+                                st, h->tc_tiles, h->v_tc, h->n_vtc, h->tkt_tc, h->n_tkttc,
+                                h->tmt_tc, h->n_tmttc, h->xt_tc, h->n_xttc, h->rowmap, h->mirror,
+                                h->dmat, h->tc_part, h->tc_counters, h->ctl, h->err));
 }
 // The three column classes run concurrently: mid and wide go to stream s2 (wide first, they
 // are the longest tiles), thin to `st`; s2 is joined back into `st` before returning.
@@ -595,14 +706,14 @@ int launch_pp_ladder(ccdgpu_handle *h, cudaStream_t st) {
     if (h->n_cls[2]) {
       pp_ladder_kernel<2><<<h->n_cls[2], kLadderThreads, h->ladder_smem, h->s2>>>(
           t_wide, h->v_t, h->t_kt, h->t_mt, h->x_t, h->rowmap, h->mirror, h->dmat, h->lpart,
-          h->lcounters, h->ctl, h->err);
+          h->lcounters, h->ctl, h->err, 0);
       h->launches++;
       CK(cudaGetLastError());
     }
     if (h->n_cls[1]) {
       pp_ladder_kernel<1><<<h->n_cls[1], kLadderThreads, h->ladder_smem, h->s2>>>(
           t_mid, h->v_t, h->t_kt, h->t_mt, h->x_t, h->rowmap, h->mirror, h->dmat, h->lpart,
-          h->lcounters, h->ctl, h->err);
+          h->lcounters, h->ctl, h->err, 0);
       h->launches++;
       CK(cudaGetLastError());
     }
@@ -611,38 +722,38 @@ int launch_pp_ladder(ccdgpu_handle *h, cudaStream_t st) {
   if (h->n_cls[0]) {
     CK(launch_pdl(pp_ladder_kernel<0>, h->n_cls[0], kLadderThreads, h->ladder_smem_thin, st,
                   t_thin, h->v_t, h->t_kt, h->t_mt, h->x_t, h->rowmap, h->mirror, h->dmat,
-                  h->lpart, h->lcounters, h->ctl, h->err));
+                  h->lpart, h->lcounters, h->ctl, h->err, 0));
     h->launches++;
   }
   if (side) CK(cudaStreamWaitEvent(st, h->ev_join2, 0));
   return CCDGPU_OK;
 }
 
-int launch_ring(ccdgpu_handle *h, cudaStream_t st) {
+int launch_ring(ccdgpu_handle *h, cudaStream_t st, int gate) {
   if (h->n_mod_small) {
     ring_small_kernel<<<(int)ceil_div(h->n_mod_small, 8), 256, 0, st>>>(
-        h->mods, h->n_mod_small, h->v_hpph, h->v_hphp, h->old_phhp, h->r_phhp, h->ctl);
+        h->mods, h->n_mod_small, h->v_hpph, h->v_hphp, h->old_phhp, h->r_phhp, h->ctl, gate);
     h->launches++;
     CK(cudaGetLastError());
   }
   const int nbig = h->n_mod - h->n_mod_small;
   if (nbig) {
     ring_kernel<<<nbig, kRingThreads, std::max<size_t>(h->ring_smem, 16), st>>>(
-        h->mods + h->n_mod_small, h->v_hpph, h->v_hphp, h->old_phhp, h->r_phhp, h->ctl);
+        h->mods + h->n_mod_small, h->v_hpph, h->v_hphp, h->old_phhp, h->r_phhp, h->ctl, gate);
     h->launches++;
     CK(cudaGetLastError());
   }
   return CCDGPU_OK;
 }
-int launch_onebody_fused(ccdgpu_handle *h, cudaStream_t st) {
+int launch_onebody_fused(ccdgpu_handle *h, cudaStream_t st, int gate) {
   const int warps_per_block = 8;
   const int blocks = (int)ceil_div((int64_t)h->nsp, warps_per_block);
   h->launches++;
   return cuda_status(launch_pdl(onebody_fused_kernel, blocks, warps_per_block * 32, 0, st,
                                 (int)h->np, (int)h->nsp, h->list_off, h->list, h->s, h->r, h->xh,
-                                h->yp, h->ctl));
+                                h->yp, h->ctl, gate));
 }
-int launch_assemble_fused(ccdgpu_handle *h, cudaStream_t st) {
+int launch_assemble_fused(ccdgpu_handle *h, cudaStream_t st, int gate) {
   if (!h->n_ranges) return CCDGPU_OK;
   const int64_t n_t = h->n_t;
   h->launches++;
@@ -651,10 +762,10 @@ int launch_assemble_fused(ccdgpu_handle *h, cudaStream_t st) {
       h->hh_pairs, h->pp_swap, h->hh_swap, h->pk_idx, h->v_pphh, h->dmat, h->r_phhp,
       h->flat + 4 * n_t, h->flat + 5 * n_t, h->flat + 6 * n_t, h->flat + 7 * n_t, h->xh, h->yp,
       h->eps, (int)h->np, h->t[0], h->t[1], h->old_phhp, h->t_kt, h->t_mt, h->epart, h->ticket,
-      h->ctl));
+      h->ctl, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc, gate ? h->nt : 0, gate));
 }
 int launch_energy(ccdgpu_handle *h, cudaStream_t st, int flags) {
-  energy_kernel<<<1, kEnergyThreads, 0, st>>>(h->epart, h->n_ranges, h->ctl, flags, h->e_out);
+  energy_kernel<<<1, kEnergyThreads, 0, st>>>(h->epart, h->n_ranges, h->ctl, flags, h->e_out, 0);
   h->launches++;
   return cuda_status(cudaGetLastError());
 }
@@ -663,44 +774,50 @@ int launch_map_to(ccdgpu_handle *h, cudaStream_t st, const double *src, double *
   map_to_kernel<<<h->n_ranges, 256, 0, st>>>(h->ranges, h->chans, h->pk_idx, h->flat, h->n_t, src, dst,
                                                h->old_h2pp_h1, h->old_h1pp_h2, h->old_p1_p2hh,
                                                h->old_p2_p1hh, h->old_phhp, h->t_kt, h->t_mt,
-                                               h->have_3body ? 1 : 0);
+                                               h->have_3body ? 1 : 0, h->tkt_tc, h->n_tkttc,
+                                               h->tmt_tc, h->n_tmttc, h->nt);
   h->launches++;
   return cuda_status(cudaGetLastError());
 }
 
 // One fused iteration: hh ladder and ring concurrently, then one-body, pp ladder, assembly.
-int enqueue_fused_iteration(ccdgpu_handle *h) {
+// mixed: the pp ladder runs on the tensor cores (split bf16) instead of the FP64 pipe.
+int enqueue_fused_iteration(ccdgpu_handle *h, bool mixed) {
   int rc;
+  const int gate = mixed ? 1 : 0;
+  auto ladder = [&](cudaStream_t st) {
+    return mixed ? launch_pp_ladder_tc(h, st) : launch_pp_ladder(h, st);
+  };
   if (h->profiling) {
     // ev: 0 start, 1 after hh ladder, 2 after one-body, 3 after pp ladder, 4/5 ring on s1,
     // 6 after assembly, 7 after the energy reduction.
     CK(cudaEventRecord(h->ev[0], h->s0));
     CK(cudaStreamWaitEvent(h->s1, h->ev[0], 0));
     CK(cudaEventRecord(h->ev[4], h->s1));
-    if ((rc = launch_ring(h, h->s1))) return rc;
+    if ((rc = launch_ring(h, h->s1, gate))) return rc;
     CK(cudaEventRecord(h->ev[5], h->s1));
-    if ((rc = launch_hh_ladder(h, h->s0))) return rc;
+    if ((rc = launch_hh_ladder(h, h->s0, gate))) return rc;
     CK(cudaEventRecord(h->ev[1], h->s0));
-    if ((rc = launch_onebody_fused(h, h->s0))) return rc;
+    if ((rc = launch_onebody_fused(h, h->s0, gate))) return rc;
     CK(cudaEventRecord(h->ev[2], h->s0));
-    if ((rc = launch_pp_ladder(h, h->s0))) return rc;
+    if ((rc = ladder(h->s0))) return rc;
     CK(cudaEventRecord(h->ev[3], h->s0));
     CK(cudaStreamWaitEvent(h->s0, h->ev[5], 0));
     CK(cudaEventRecord(h->ev[8], h->s0));
-    if ((rc = launch_assemble_fused(h, h->s0))) return rc;
+    if ((rc = launch_assemble_fused(h, h->s0, gate))) return rc;
     CK(cudaEventRecord(h->ev[6], h->s0));
     CK(cudaEventRecord(h->ev[7], h->s0));
     return CCDGPU_OK;
   }
   CK(cudaEventRecord(h->ev_fork, h->s0));
   CK(cudaStreamWaitEvent(h->s1, h->ev_fork, 0));
-  if ((rc = launch_ring(h, h->s1))) return rc;
+  if ((rc = launch_ring(h, h->s1, gate))) return rc;
   CK(cudaEventRecord(h->ev_join, h->s1));
-  if ((rc = launch_hh_ladder(h, h->s0))) return rc;
-  if ((rc = launch_onebody_fused(h, h->s0))) return rc;
-  if ((rc = launch_pp_ladder(h, h->s0))) return rc;
+  if ((rc = launch_hh_ladder(h, h->s0, gate))) return rc;
+  if ((rc = launch_onebody_fused(h, h->s0, gate))) return rc;
+  if ((rc = ladder(h->s0))) return rc;
   CK(cudaStreamWaitEvent(h->s0, h->ev_join, 0));
-  return launch_assemble_fused(h, h->s0);  // includes the energy reduction and stop rule
+  return launch_assemble_fused(h, h->s0, gate);  // includes the energy reduction and stop rule
 }
 
 // Table path stages (mirrors main.cpp:591-665).
@@ -748,7 +865,7 @@ int check_errors(ccdgpu_handle *h) {
 }
 
 int set_ctl(ccdgpu_handle *h, int active, double tol, int64_t max_iters, double mixing,
-            bool reset_loop, int parity = -1) {
+            bool reset_loop, int parity = -1, int phase = 0) {
   int rc = sync_ctl(h);
   if (rc) return rc;
   Control &c = *h->h_ctl;
@@ -759,8 +876,11 @@ int set_ctl(ccdgpu_handle *h, int active, double tol, int64_t max_iters, double 
     c.iterations = 0;
     c.done = 0;
     c.error = 0;
+    c.polish_iters = 0;
     std::memset(c.energies, 0, sizeof(c.energies));
   }
+  c.phase = phase;
+  c.polish_rel = h->opt.polish_threshold;
   c.active = active;
   c.tol = tol;
   c.max_iters = max_iters;
@@ -770,18 +890,19 @@ int set_ctl(ccdgpu_handle *h, int active, double tol, int64_t max_iters, double 
   return CCDGPU_OK;
 }
 
-int fused_ready_graph(ccdgpu_handle *h) {
-  if (h->graph) return CCDGPU_OK;
+int fused_ready_graph(ccdgpu_handle *h, bool mixed) {
+  cudaGraphExec_t &exec = mixed ? h->graph_tc : h->graph;
+  if (exec) return CCDGPU_OK;
   cudaGraph_t g = nullptr;
   const int64_t before = h->launches;
   CK(cudaStreamBeginCapture(h->s0, cudaStreamCaptureModeThreadLocal));
-  int rc = enqueue_fused_iteration(h);
-  h->kernels_per_graph = h->launches - before;
+  int rc = enqueue_fused_iteration(h, mixed);
+  (mixed ? h->kernels_per_graph_tc : h->kernels_per_graph) = h->launches - before;
   h->launches = before;
   cudaError_t e = cudaStreamEndCapture(h->s0, &g);
   if (rc) { if (g) cudaGraphDestroy(g); return rc; }
   CK(e);
-  e = cudaGraphInstantiate(&h->graph, g, 0);
+  e = cudaGraphInstantiate(&exec, g, 0);
   cudaGraphDestroy(g);
   CK(e);
   return CCDGPU_OK;
@@ -792,8 +913,8 @@ int tables_iteration(ccdgpu_handle *h, double mixing, double *corr) {
   int rc;
   if ((rc = stage_onebody_tables(h, 0, 1))) return rc;     // calcT2Diff_p2_p1hh
   if ((rc = stage_onebody_tables(h, 1, 0))) return rc;     // calcT2Diff_h2pp_h1
-  if ((rc = launch_ring(h, h->s0))) return rc;             // calcT2Diff_phhp
-  if ((rc = launch_hh_ladder(h, h->s0))) return rc;        // calcT2Diff_pphh
+  if ((rc = launch_ring(h, h->s0, 0))) return rc;          // calcT2Diff_phhp
+  if ((rc = launch_hh_ladder(h, h->s0, 0))) return rc;     // calcT2Diff_pphh
   if ((rc = launch_pp_ladder(h, h->s0))) return rc;
   if ((rc = stage_gather(h))) return rc;                   // 8 x mapFromDistributed
   if ((rc = stage_assemble_tables(h, mixing))) return rc;  // calcT2_pphh
@@ -814,7 +935,7 @@ void ccdgpu_default_options(ccdgpu_options *opt) {
   opt->precision = CCDGPU_PREC_FP64;
   opt->v_mode = CCDGPU_V_STORED;
   opt->path = CCDGPU_PATH_FUSED;
-  opt->polish_threshold = 1e-9;
+  opt->polish_threshold = 1e-6;
   opt->use_graph = 1;
 }
 
@@ -844,7 +965,14 @@ int ccdgpu_create(const ccdgpu_problem *prob, const ccdgpu_options *opt, ccdgpu_
   if (!h) return CCDGPU_ERR_OUT_OF_MEMORY;
   if (opt) h->opt = *opt;
   else ccdgpu_default_options(&h->opt);
-  if (h->opt.precision != CCDGPU_PREC_FP64) { delete h; return CCDGPU_ERR_UNSUPPORTED; }
+  switch (h->opt.precision) {
+    case CCDGPU_PREC_FP64: h->nt = 0; break;
+    case CCDGPU_PREC_MIXED_BF16: h->nt = 2; break;
+    case CCDGPU_PREC_MIXED_BF16X3: h->nt = 3; break;
+    default: delete h; return CCDGPU_ERR_UNSUPPORTED;
+  }
+  if (h->nt && h->opt.path != CCDGPU_PATH_FUSED) { delete h; return CCDGPU_ERR_UNSUPPORTED; }
+  if (h->nt && !(h->opt.polish_threshold >= 0)) { delete h; return CCDGPU_ERR_INVALID_ARGUMENT; }
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev == 0) { (void)cudaGetLastError(); delete h; return CCDGPU_ERR_NO_DEVICE; }
@@ -884,6 +1012,10 @@ int ccdgpu_reset(ccdgpu_handle *h) {
       {h->old_p1_p2hh, h->n_p}, {h->old_p2_p1hh, h->n_p}};
   for (const auto &b : z)
     if (b.first && b.second) CK(cudaMemsetAsync(b.first, 0, b.second * 8, h->s0));
+  if (h->nt) {
+    CK(cudaMemsetAsync(h->tkt_tc, 0, (size_t)h->nt * h->n_tkttc * 2, h->s0));
+    CK(cudaMemsetAsync(h->tmt_tc, 0, (size_t)h->nt * h->n_tmttc * 2, h->s0));
+  }
   return set_ctl(h, 0, h->h_ctl->tol, h->h_ctl->max_iters, h->h_ctl->mixing, true, 0);
 }
 
@@ -918,7 +1050,7 @@ int ccdgpu_step(ccdgpu_handle *h, double mixing, double *e_corr) {
   int rc = set_ctl(h, 0, h->h_ctl->tol, INT64_MAX / 2, mixing, false);
   if (rc) return rc;
   if (h->opt.path == CCDGPU_PATH_TABLES) rc = tables_iteration(h, mixing, nullptr);
-  else rc = enqueue_fused_iteration(h);
+  else rc = enqueue_fused_iteration(h, h->nt > 0);
   if (rc) return rc;
   if ((rc = sync_ctl(h))) return rc;
   if ((rc = check_errors(h))) return rc;
@@ -929,11 +1061,14 @@ int ccdgpu_step(ccdgpu_handle *h, double mixing, double *e_corr) {
 int ccdgpu_solve(ccdgpu_handle *h, double tol, int64_t max_iters, double mixing, ccdgpu_result *res) {
   if (!h || max_iters < 0 || !(tol >= 0)) return CCDGPU_ERR_INVALID_ARGUMENT;
   CK(cudaSetDevice(h->opt.device));
-  int rc = set_ctl(h, 1, tol, max_iters, mixing, true);
-  if (rc) return rc;
   const bool fused = h->opt.path == CCDGPU_PATH_FUSED;
+  const bool mixed = fused && h->nt > 0;
+  // A mixed solve starts in phase 1 (tensor-core ladder) and finishes in phase 2 (FP64).
+  int rc = set_ctl(h, 1, tol, max_iters, mixing, true, -1, mixed ? 1 : 0);
+  if (rc) return rc;
   const bool graph = fused && h->opt.use_graph && !h->profiling;
-  if (graph && (rc = fused_ready_graph(h))) return rc;
+  if (graph && (rc = fused_ready_graph(h, false))) return rc;
+  if (graph && mixed && (rc = fused_ready_graph(h, true))) return rc;
   auto t0 = std::chrono::steady_clock::now();
   int64_t launched = 0;
   const int64_t cap = max_iters + 1;
@@ -942,15 +1077,18 @@ int ccdgpu_solve(ccdgpu_handle *h, double tol, int64_t max_iters, double mixing,
     // launches of the batch return immediately.
     const int64_t batch =
         (fused && !h->profiling) ? std::min<int64_t>(launched < 8 ? 4 : 8, cap - launched) : 1;
+    // The phase can only change inside a batch from 1 to 2; mixed iterations that follow
+    // the switch in the same batch are no-ops on the device.
+    const bool mphase = mixed && h->h_ctl->phase == 1;
     for (int64_t b = 0; b < batch; b++) {
-      if (graph) CK(cudaGraphLaunch(h->graph, h->s0));
-      else if (fused) { if ((rc = enqueue_fused_iteration(h))) return rc; }
+      if (graph) CK(cudaGraphLaunch(mphase ? h->graph_tc : h->graph, h->s0));
+      else if (fused) { if ((rc = enqueue_fused_iteration(h, mphase))) return rc; }
       else {
         if ((rc = tables_iteration(h, mixing, nullptr))) return rc;
       }
     }
     launched += batch;
-    if (graph) h->launches += batch * h->kernels_per_graph;
+    if (graph) h->launches += batch * (mphase ? h->kernels_per_graph_tc : h->kernels_per_graph);
     if ((rc = sync_ctl(h))) return rc;
     if (h->profiling && fused && !graph) {
       float a = 0, b = 0, c = 0, d = 0, e = 0, f = 0;
@@ -978,7 +1116,7 @@ int ccdgpu_solve(ccdgpu_handle *h, double tol, int64_t max_iters, double mixing,
     res->e_diff = c.e_diff;
     res->iterations = c.iterations;
     res->converged = std::fabs(c.e_diff) <= tol ? 1 : 0;
-    res->polish_iterations = 0;
+    res->polish_iterations = (int32_t)c.polish_iters;
     res->seconds = std::chrono::duration<double>(t1 - t0).count();
   }
   return CCDGPU_OK;
@@ -1012,14 +1150,14 @@ int ccdgpu_calc_t2diff_h2pp_h1(ccdgpu_handle *h) {
 int ccdgpu_calc_t2diff_phhp(ccdgpu_handle *h) {
   if (!h) return CCDGPU_ERR_INVALID_ARGUMENT;
   int rc = set_ctl(h, 0, h->h_ctl->tol, h->h_ctl->max_iters, h->h_ctl->mixing, false);
-  if (rc || (rc = launch_ring(h, h->s0))) return rc;
+  if (rc || (rc = launch_ring(h, h->s0, 0))) return rc;
   CK(cudaStreamSynchronize(h->s0));
   return CCDGPU_OK;
 }
 int ccdgpu_calc_t2diff_pphh(ccdgpu_handle *h) {
   if (!h) return CCDGPU_ERR_INVALID_ARGUMENT;
   int rc = set_ctl(h, 0, h->h_ctl->tol, h->h_ctl->max_iters, h->h_ctl->mixing, false);
-  if (rc || (rc = launch_hh_ladder(h, h->s0)) || (rc = launch_pp_ladder(h, h->s0))) return rc;
+  if (rc || (rc = launch_hh_ladder(h, h->s0, 0)) || (rc = launch_pp_ladder(h, h->s0))) return rc;
   CK(cudaStreamSynchronize(h->s0));
   return check_errors(h);
 }
@@ -1096,7 +1234,7 @@ int ccdgpu_work_per_iteration(const ccdgpu_handle *h, double *flops, double *v_p
                               double *ladder_flops) {
   if (!h) return CCDGPU_ERR_INVALID_ARGUMENT;
   if (flops) *flops = h->flops;
-  if (v_pppp_bytes) *v_pppp_bytes = h->ladder_bytes;
+  if (v_pppp_bytes) *v_pppp_bytes = h->nt ? h->ladder_bytes_tc : h->ladder_bytes;
   if (ladder_flops) *ladder_flops = h->ladder_flops;
   return CCDGPU_OK;
 }

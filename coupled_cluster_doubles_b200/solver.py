@@ -18,7 +18,7 @@ import numpy as np
 
 from . import _native
 
-PREC = {"fp64": 0, "mixed": 1, "mixed_bf16": 1}
+PREC = {"fp64": 0, "mixed": 1, "mixed_bf16": 1, "mixed_bf16x3": 2}
 PATH = {"fused": 0, "tables": 1}
 VMODE = {"stored": 0, "on_the_fly": 1}
 
@@ -63,7 +63,7 @@ class Result:
 
 class CCDSolver:
     def __init__(self, system, precision="fp64", path="fused", v_mode="stored", device=0,
-                 use_graph=True, polish_threshold=1e-9):
+                 use_graph=True, polish_threshold=1e-6):
         lib = _native.gpu_lib()
         self.system = system  # keeps the host problem alive during create
         opt = _native.Options()

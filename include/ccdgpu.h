@@ -103,8 +103,10 @@ enum ccdgpu_status {
 };
 
 enum ccdgpu_precision {
-  CCDGPU_PREC_FP64 = 0,        /* FP64 throughout (DMMA contractions) */
-  CCDGPU_PREC_MIXED_BF16 = 1   /* split-BF16 contractions, FP32 accumulate, FP64 polish */
+  CCDGPU_PREC_FP64 = 0,        /* FP64 throughout (FP64 FMA-pipe contractions) */
+  CCDGPU_PREC_MIXED_BF16 = 1,  /* pp ladder on tensor cores with 2-term bf16 split operands,
+                                  FP32 accumulation; FP64 polish iterations at the end */
+  CCDGPU_PREC_MIXED_BF16X3 = 2 /* the same with 3-term bf16 split operands */
 };
 enum ccdgpu_v_mode {
   CCDGPU_V_STORED = 0,         /* V_pppp uploaded from the host blocks */
@@ -122,7 +124,8 @@ typedef struct ccdgpu_options {
   int32_t precision;           /* ccdgpu_precision */
   int32_t v_mode;              /* ccdgpu_v_mode */
   int32_t path;                /* ccdgpu_path */
-  double polish_threshold;     /* mixed: switch to FP64 once |dE| falls below this */
+  double polish_threshold;     /* mixed: switch to FP64 iterations once |dE| <= max(tol,
+                                  polish_threshold * |E|) or |dE| stops decreasing */
   int32_t use_graph;           /* capture one iteration as a CUDA graph (fused path) */
   int32_t reserved[7];
 } ccdgpu_options;
@@ -138,7 +141,7 @@ typedef struct ccdgpu_result {
 
 typedef struct ccdgpu_handle ccdgpu_handle;
 
-/* Defaults: device 0, FP64, stored V, fused path, graph capture on, polish 1e-9. */
+/* Defaults: device 0, FP64, stored V, fused path, graph capture on, polish 1e-6. */
 void ccdgpu_default_options(ccdgpu_options *opt);
 
 /* Deep-copies the problem to the device and validates every remap table (range and
@@ -216,8 +219,9 @@ void *ccdgpu_stream(ccdgpu_handle *h);
 
 /* Work of one iteration for roofline reporting: *flops = reference GEMM flops (sum over
  * channels of 2 pp^2 hh + 4 pp hh^2 + 4 ph' hp'^2); *ladder_bytes = bytes one pp-ladder launch
- * moves (antisymmetry-packed V_pppp, the T and X operands, D); *ladder_flops = the pp-ladder
- * share of the reference flops (2 pp^2 hh). */
+ * moves (antisymmetry-packed V_pppp, the T and X operands, D) at the handle's precision (FP64
+ * operands, or the bf16 terms of a mixed handle); *ladder_flops = the pp-ladder share of the
+ * reference flops (2 pp^2 hh). */
 int ccdgpu_work_per_iteration(const ccdgpu_handle *h, double *flops, double *ladder_bytes,
                               double *ladder_flops);
 
