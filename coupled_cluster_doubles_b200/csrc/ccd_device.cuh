@@ -103,9 +103,9 @@ struct ChanInfo {
   int64_t vtc_base, tkt_tc_base, tmt_tc_base, xt_tc_base;
 };
 
-// hh-ladder split-K tile: rows [k0, k0+kHHRows) of channel ch.
+// hh-ladder split-K tile: rows [k0, k0+rows) of channel ch.
 struct HHTile {
-  int32_t ch, k0, idx, pad;  // idx = tile index within the channel
+  int32_t ch, k0, idx, rows;  // idx = tile index within the channel
 };
 
 // Per active modified channel.
@@ -146,5 +146,6 @@ struct Control {
 constexpr int32_t kErrNonFinite = 1;
 constexpr int32_t kErrTimeout = 2;
 constexpr int32_t kErrBadIndex = 4;
+constexpr int32_t kErrRingMaps = 8;  // aj_ib / bi_ja / bj_ia are not ai_jb under the swaps
 
 }  // namespace ccd

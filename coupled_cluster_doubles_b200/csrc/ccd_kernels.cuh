@@ -344,19 +344,98 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict_
 }
 
 // ------------------------------------------------------------------------------------------
-// hh ladder intermediate, split over 64-row K slices of each channel:
+// hh ladder intermediate, split into K slices of each channel:
 //   P = V_hhpp T (K = pp),  X = V_hhhh + 0.5 P  (reference layout, and X/2 as B tiles),
 //   s[IJ] = P[IJ][IJ]            (x_k = sum over IJ with first hole k, calc.cpp:82-84),
 //   r[AB] = sum_IJ V[IJ][AB] T[AB][IJ]  (y_a = sum over AB with first particle a, calc.cpp:18-20).
-// Each CTA writes its slice's partial P; the last CTA of a channel (atomic ticket) sums the
-// partials in slice order, so the result does not depend on scheduling.  V_hhpp is held
-// transposed (pp x hh) so a slice is one contiguous stretch, like the T slice.
+// V_hhpp is held transposed (pp x hh), so a slice of V and of T are both contiguous row ranges;
+// a slice holds at most kHHElems elements (rows = kHHElems / hh) and is staged in shared memory
+// with one round of loads.  hh <= 16: thread = (output, row group), the row groups summed in a
+// fixed order; hh > 16: 16 x 16 threads with a TM x TM register tile each (rows ty + 16 i,
+// columns tx + 16 j).  A channel with one slice finishes X directly.  Otherwise each CTA writes
+// its partial P and the last CTA of the channel (atomic ticket) adds the partials in slice
+// order, so the result does not depend on scheduling.
 // ------------------------------------------------------------------------------------------
 constexpr int kHHThreads = 256;
-constexpr int kHHRows = 64;
-constexpr int kHHAcc = 21;  // (72*72)/256 rounded up
+constexpr int kHHElems = 2560;  // V (and T) elements of one slice
 
-__global__ void __launch_bounds__(kHHThreads)
+__host__ __device__ inline int hh_slice_rows(int hh) { return hh >= kHHElems ? 1 : kHHElems / hh; }
+
+// X, its X/2 operand tiles (FP64 and, for a mixed iteration, bf16 terms) and s from one
+// finished element P[kl][ij].
+__device__ __forceinline__ void hh_finish(const ChanInfo &ch, int kl, int ij, double p,
+                                          const double *__restrict__ v_hhhh, double *x_ref,
+                                          double *x_t, double *s_out, __nv_bfloat16 *xt_tc,
+                                          int64_t xt_tc_stride, int nt) {
+  const int hh = ch.hh, idx = kl * hh + ij;
+  const double x = v_hhhh[ch.x_off + idx] + 0.5 * p;
+  x_ref[ch.x_off + idx] = x;
+  x_t[ch.xt_base + (int64_t)(kl / kBK) * kBK * ch.nb + (kl % kBK) * ch.nb + ij] = 0.5 * x;
+  if (nt) {
+    __nv_bfloat16 hv[3];
+    split_bf16(0.5 * x, hv, nt);
+    const int64_t o =
+        ch.xt_tc_base + (int64_t)(kl >> 5) * (ch.nbt >> 3) * kTcGroup + tc_off(ij, kl & 31);
+    for (int q = 0; q < nt; ++q) xt_tc[q * xt_tc_stride + o] = hv[q];
+  }
+  if (kl == ij) s_out[ch.hh_off + ij] = p;
+}
+
+struct HHOut {
+  const HHTile &tt;
+  const ChanInfo &ch;
+  const double *v_hhhh;
+  double *part, *x_ref, *x_t, *s_out;
+  __nv_bfloat16 *xt_tc;
+  int64_t xt_tc_stride;
+  int nt;
+  // One slice's value of P[kl][ij]: final for single-slice channels, else a partial.
+  __device__ __forceinline__ void emit(int kl, int ij, double p) const {
+    if (ch.nhht == 1) hh_finish(ch, kl, ij, p, v_hhhh, x_ref, x_t, s_out, xt_tc, xt_tc_stride, nt);
+    else part[ch.part_off + (int64_t)tt.idx * ch.hh * ch.hh + kl * ch.hh + ij] = p;
+  }
+};
+
+template <int TM>
+__device__ __forceinline__ void hh_tiled(const double *Vs, const double *Ts, int rows, int hh,
+                                         const HHOut &out) {
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  int ci[TM], cj[TM];  // column offsets clamped into the row; lanes past hh are not stored
+#pragma unroll
+  for (int i = 0; i < TM; ++i) {
+    ci[i] = min(ty + 16 * i, hh - 1);
+    cj[i] = min(tx + 16 * i, hh - 1);
+  }
+  double acc[TM][TM];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TM; ++j) acc[i][j] = 0.0;
+#pragma unroll 2
+  for (int k = 0; k < rows; ++k) {
+    double a[TM], b[TM];
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+      a[i] = Vs[k * hh + ci[i]];
+      b[i] = Ts[k * hh + cj[i]];
+    }
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TM; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+  }
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TM; ++j) {
+      const int kl = ty + 16 * i, ij = tx + 16 * j;
+      if (kl < hh && ij < hh) out.emit(kl, ij, acc[i][j]);
+    }
+}
+
+// SMALL: channels with hh <= 16 (few registers, high occupancy); else the register-tiled rest.
+template <bool SMALL>
+__global__ void __launch_bounds__(kHHThreads, SMALL ? 4 : 2)
 hh_ladder_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ chans,
                  const double *__restrict__ v_pphh, const double *__restrict__ v_hhhh,
                  const double *tbuf0, const double *tbuf1, double *part, int32_t *counters,
@@ -364,80 +443,98 @@ hh_ladder_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ 
                  double *__restrict__ r_out, __nv_bfloat16 *__restrict__ xt_tc,
                  int64_t xt_tc_stride, int nt, const Control *ctl, int gate) {
   if (skip_iteration(ctl, gate)) return;
-  extern __shared__ __align__(16) double hsm[];
+  __shared__ __align__(16) double Vs[kHHElems], Ts[kHHElems];
+  __shared__ double red[kHHThreads];
   __shared__ int last;
   const HHTile tt = tiles[blockIdx.x];
   const ChanInfo ch = chans[tt.ch];
   const double *t_old = ctl->parity ? tbuf1 : tbuf0;
-  const int hh = ch.hh, tid = threadIdx.x;
-  const int rows = min(kHHRows, ch.pp - tt.k0);
-  double *Vs = hsm, *Ts = hsm + kHHRows * hh;
+  const int hh = ch.hh, tid = threadIdx.x, rows = tt.rows, n = rows * hh;
   const double *vb = v_pphh + ch.t_off + (int64_t)tt.k0 * hh;
   const double *tb = t_old + ch.t_off + (int64_t)tt.k0 * hh;
-  for (int e = tid; e < rows * hh; e += kHHThreads) {
+  for (int e = tid; e < n; e += kHHThreads) {
     Vs[e] = vb[e];
     Ts[e] = tb[e];
   }
   __syncthreads();
-  const int nout = hh * hh;
-  double *mypart = part + ch.part_off + (int64_t)tt.idx * nout;
-#pragma unroll
-  for (int q = 0; q < kHHAcc; ++q) {
-    const int idx = tid + q * kHHThreads;
-    if (idx < nout) {
-      const int kl = idx / hh, ij = idx - kl * hh;
-      mypart[idx] = dot4(Vs + kl, hh, Ts + ij, hh, rows);
+  for (int r = tid; r < rows; r += kHHThreads)
+    r_out[ch.pp_off + tt.k0 + r] = dot4(Vs + r * hh, 1, Ts + r * hh, 1, hh);
+  const HHOut out{tt, ch, v_hhhh, part, x_ref, x_t, s_out, xt_tc, xt_tc_stride, nt};
+  if (SMALL) {
+    const int no = hh * hh, groups = kHHThreads / no;
+    const int o = tid % no, g = tid / no, kl = o / hh, ij = o - kl * hh;
+    double acc = 0.0;
+    if (g < groups)
+      for (int r = g; r < rows; r += groups) acc = fma(Vs[r * hh + kl], Ts[r * hh + ij], acc);
+    red[tid] = acc;
+    __syncthreads();
+    if (tid < no) {
+      double p = 0.0;
+      for (int q = 0; q < groups; ++q) p += red[q * no + tid];
+      out.emit(kl, ij, p);
+    }
+  } else {
+    switch ((hh + 15) / 16) {
+      case 2: hh_tiled<2>(Vs, Ts, rows, hh, out); break;
+      case 3: hh_tiled<3>(Vs, Ts, rows, hh, out); break;
+      case 4: hh_tiled<4>(Vs, Ts, rows, hh, out); break;
+      case 5: hh_tiled<5>(Vs, Ts, rows, hh, out); break;
+      default: break;
     }
   }
-  if (tid < rows) r_out[ch.pp_off + tt.k0 + tid] = dot4(Vs + tid * hh, 1, Ts + tid * hh, 1, hh);
+  if (ch.nhht == 1) return;
   __threadfence();
   __syncthreads();
   if (tid == 0) last = (atomicAdd(&counters[tt.ch], 1) == ch.nhht - 1);
   __syncthreads();
   if (!last) return;
   __threadfence();
-  const int nb = ch.nb;
+  const int nout = hh * hh;
   const double *pbase = part + ch.part_off;
   for (int idx = tid; idx < nout; idx += kHHThreads) {
     double p = 0.0;
     for (int t = 0; t < ch.nhht; ++t) p += __ldcg(pbase + (int64_t)t * nout + idx);
-    const int kl = idx / hh, ij = idx - kl * hh;
-    const double x = v_hhhh[ch.x_off + idx] + 0.5 * p;
-    x_ref[ch.x_off + idx] = x;
-    x_t[ch.xt_base + (int64_t)(kl / kBK) * kBK * nb + (kl % kBK) * nb + ij] = 0.5 * x;
-    if (nt) {
-      __nv_bfloat16 hv[3];
-      split_bf16(0.5 * x, hv, nt);
-      const int64_t o =
-          ch.xt_tc_base + (int64_t)(kl >> 5) * (ch.nbt >> 3) * kTcGroup + tc_off(ij, kl & 31);
-      for (int p = 0; p < nt; ++p) xt_tc[p * xt_tc_stride + o] = hv[p];
-    }
-    if (kl == ij) s_out[ch.hh_off + ij] = p;
+    hh_finish(ch, idx / hh, idx % hh, p, v_hhhh, x_ref, x_t, s_out, xt_tc, xt_tc_stride, nt);
   }
   if (tid == 0) counters[tt.ch] = 0;
 }
 
 // ------------------------------------------------------------------------------------------
 // Ring term: Y = V_hphp + 0.5 V_hpph T', R = T' Y per modified channel.
-// Channels with ph', hp' <= kRingSmall run one per warp; larger ones one per CTA.
+// Operand source and result layout:
+//   fused path (inv != null): T' is gathered from the pphh amplitudes, T'[p] = t[inv[p]], and
+//     R is scattered back to pphh order, out[inv[p]] = R[p] (inv = inverse of the ai_jb table),
+//     so the assembly reads R_ai,jb / R_aj,ib / R_bi,ja / R_bj,ia from the channel's own block;
+//   table path (inv == null): T' = t2Old_phhp and R = t2Diff_phhp in the phhp slab
+//     (calc.cpp:264-313), tbuf0 = tbuf1 = the slab.
+// Channels with ph', hp' <= kRingSmall run one per warp; larger ones one per CTA with register
+// tiles, in two classes (<= 32 and above) so each class has its own shared-memory size.
 // ------------------------------------------------------------------------------------------
 constexpr int kRingThreads = 256;
 constexpr int kRingSmall = 16;
+constexpr int kRingMid = 32;
+
+__device__ __forceinline__ const double *ring_t(const Control *ctl, const int32_t *inv,
+                                                const double *tbuf0, const double *tbuf1) {
+  return (inv && ctl->parity) ? tbuf1 : tbuf0;
+}
 
 __global__ void __launch_bounds__(256)
 ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restrict__ v_hpph,
-                  const double *__restrict__ v_hphp, const double *__restrict__ t_phhp,
-                  double *__restrict__ r_phhp, const Control *ctl, int gate) {
+                  const double *__restrict__ v_hphp, const double *tbuf0, const double *tbuf1,
+                  const int32_t *__restrict__ inv, double *__restrict__ out, const Control *ctl,
+                  int gate) {
   if (skip_iteration(ctl, gate)) return;
   __shared__ double buf[8][3 * kRingSmall * kRingSmall];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int mi = blockIdx.x * 8 + w;
   if (mi >= n) return;
   const ModInfo m = mods[mi];
+  const double *tsrc = ring_t(ctl, inv, tbuf0, tbuf1);
   const int ph = m.ph, hp = m.hp;
   double *Ts = buf[w], *Va = Ts + ph * hp, *Ys = Va + hp * ph;
   for (int e = lane; e < ph * hp; e += 32) {
-    Ts[e] = t_phhp[m.m_off + e];
+    Ts[e] = tsrc[inv ? (int64_t)inv[m.m_off + e] : m.m_off + e];
     Va[e] = v_hpph[m.m_off + e];
   }
   for (int e = lane; e < hp * hp; e += 32) Ys[e] = v_hphp[m.y_off + e];
@@ -449,35 +546,118 @@ ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restr
   __syncwarp();
   for (int e = lane; e < ph * hp; e += 32) {
     const int i = e / hp, j = e - i * hp;
-    r_phhp[m.m_off + e] = dot4(Ts + i * hp, 1, Ys + j, hp, hp);
+    const double r = dot4(Ts + i * hp, 1, Ys + j, hp, hp);
+    out[inv ? (int64_t)inv[m.m_off + e] : m.m_off + e] = r;
   }
 }
 
-__global__ void __launch_bounds__(kRingThreads)
-ring_kernel(const ModInfo *__restrict__ mods, const double *__restrict__ v_hpph,
-            const double *__restrict__ v_hphp, const double *__restrict__ t_phhp,
-            double *__restrict__ r_phhp, const Control *ctl, int gate) {
-  if (skip_iteration(ctl, gate)) return;
-  extern __shared__ __align__(16) double rs[];
-  const ModInfo m = mods[blockIdx.x];
-  const int ph = m.ph, hp = m.hp, tid = threadIdx.x;
+// Channels above kRingSmall: one CTA, 16 x 16 threads with a TM x TM register tile each
+// (rows ty + 16 i, columns tx + 16 j, TM = ceil(max(ph', hp') / 16)); operands in shared memory.
+template <int TM>
+__device__ __forceinline__ void ring_body(const ModInfo &m, const double *__restrict__ v_hpph,
+                                          const double *__restrict__ v_hphp,
+                                          const double *__restrict__ tsrc,
+                                          const int32_t *__restrict__ inv,
+                                          double *__restrict__ out, double *rs) {
+  const int ph = m.ph, hp = m.hp, tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   double *Ts = rs;             // ph x hp
   double *Va = Ts + ph * hp;   // hp x ph
   double *Ys = Va + hp * ph;   // hp x hp
   for (int e = tid; e < ph * hp; e += kRingThreads) {
-    Ts[e] = t_phhp[m.m_off + e];
+    Ts[e] = tsrc[inv ? (int64_t)inv[m.m_off + e] : m.m_off + e];
     Va[e] = v_hpph[m.m_off + e];
   }
   for (int e = tid; e < hp * hp; e += kRingThreads) Ys[e] = v_hphp[m.y_off + e];
   __syncthreads();
-  for (int e = tid; e < hp * hp; e += kRingThreads) {
-    const int i = e / hp, j = e - i * hp;
-    Ys[e] = 0.5 * dot4(Va + i * ph, 1, Ts + j, hp, ph) + Ys[e];
+  // Y = V_hphp + 0.5 V_hpph T'   (hp x hp, K = ph)
+  int ri[TM], cj[TM];
+#pragma unroll
+  for (int i = 0; i < TM; ++i) {
+    ri[i] = min(ty + 16 * i, hp - 1);
+    cj[i] = min(tx + 16 * i, hp - 1);
   }
+  double acc[TM][TM];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TM; ++j) acc[i][j] = 0.0;
+#pragma unroll 2
+  for (int k = 0; k < ph; ++k) {
+    double a[TM], b[TM];
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+      a[i] = Va[ri[i] * ph + k];
+      b[i] = Ts[k * hp + cj[i]];
+    }
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TM; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+  }
+  // Each Y element is read and written by the thread that owns it; Ts and Va stay intact.
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TM; ++j) {
+      const int r = ty + 16 * i, c = tx + 16 * j;
+      if (r < hp && c < hp) Ys[r * hp + c] = 0.5 * acc[i][j] + Ys[r * hp + c];
+    }
   __syncthreads();
-  for (int e = tid; e < ph * hp; e += kRingThreads) {
-    const int i = e / hp, j = e - i * hp;
-    r_phhp[m.m_off + e] = dot4(Ts + i * hp, 1, Ys + j, hp, hp);
+  // R = T' Y   (ph x hp, K = hp)
+#pragma unroll
+  for (int i = 0; i < TM; ++i) ri[i] = min(ty + 16 * i, ph - 1);
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TM; ++j) acc[i][j] = 0.0;
+#pragma unroll 2
+  for (int k = 0; k < hp; ++k) {
+    double a[TM], b[TM];
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+      a[i] = Ts[ri[i] * hp + k];
+      b[i] = Ys[k * hp + cj[i]];
+    }
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TM; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+  }
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TM; ++j) {
+      const int r = ty + 16 * i, c = tx + 16 * j;
+      if (r < ph && c < hp) {
+        const int64_t p = m.m_off + r * hp + c;
+        out[inv ? (int64_t)inv[p] : p] = acc[i][j];
+      }
+    }
+}
+
+// TMAX = 2: channels up to kRingMid; TMAX = 5: the rest (up to 80).
+template <int TMAX>
+__global__ void __launch_bounds__(kRingThreads, TMAX <= 2 ? 4 : 2)
+ring_kernel(const ModInfo *__restrict__ mods, const double *__restrict__ v_hpph,
+            const double *__restrict__ v_hphp, const double *tbuf0, const double *tbuf1,
+            const int32_t *__restrict__ inv, double *__restrict__ out, const Control *ctl,
+            int gate) {
+  if (skip_iteration(ctl, gate)) return;
+  extern __shared__ __align__(16) double rs[];
+  const ModInfo m = mods[blockIdx.x];
+  const double *tsrc = ring_t(ctl, inv, tbuf0, tbuf1);
+  const int tm = (max(m.ph, m.hp) + 15) / 16;
+  if (TMAX <= 2) {
+    if (tm <= 1) ring_body<1>(m, v_hpph, v_hphp, tsrc, inv, out, rs);
+    else ring_body<2>(m, v_hpph, v_hphp, tsrc, inv, out, rs);
+  } else {
+    switch (tm) {
+      case 1: case 2: ring_body<2>(m, v_hpph, v_hphp, tsrc, inv, out, rs); break;
+      case 3: ring_body<3>(m, v_hpph, v_hphp, tsrc, inv, out, rs); break;
+      case 4: ring_body<4>(m, v_hpph, v_hphp, tsrc, inv, out, rs); break;
+      case 5: ring_body<5>(m, v_hpph, v_hphp, tsrc, inv, out, rs); break;
+      default: break;
+    }
   }
 }
 
@@ -609,66 +789,100 @@ __device__ __forceinline__ void write_t_tiles_tc(const ChanInfo &ch,
 //         + 0.5 x_i t_ab,ji - 0.5 x_j t_ab,ij                       (h2pp_h1 gathers, algebraically)
 //         + (-0.5 y_b) t_ab,ij - (-0.5 y_a) t_ba,ij                 (p2_p1hh gathers, algebraically)
 //   t_new = mixing value/(e_i+e_j-e_a-e_b) + (1-mixing) t_old;  E += V t_new
-// and the next iteration's operands are written in the same pass: t_new into the phhp slab
-// (mapToDistributed ai_jb) and into the ladder operand tiles.
+// and the next iteration's ladder operand tiles are written in the same pass.  The fused path
+// keeps no phhp slab: the ring reads T' from the amplitudes directly (ring kernels).
 // ------------------------------------------------------------------------------------------
 constexpr int kAsmThreads = 256;
-constexpr int kAsmPerThread = 1;
+constexpr int kAsmPerThread = 2;  // elements per thread; a CTA covers one ElemRange
 __device__ __forceinline__ void energy_reduce(const double *epart, int n, Control *ctl, int flags,
                                               double *e_out);
 
-__global__ void __launch_bounds__(kAsmThreads)
-assemble_fused_kernel(const ElemRange *__restrict__ ranges, const ChanInfo *__restrict__ chans,
+// Work is organised over packed elements (u, j): packed row u (a <= b) of a channel and column
+// j, numbered q = u * hh + j per channel, kAsmPerCTA of them per CTA (ElemRange over q).  A
+// thread computes element (ab, j) and its mirror (ba, j) together: both need t and R at
+// (ab,j), (ab,ji), (ba,j), (ba,ji), which the thread reads once; the column-swapped reads fall
+// in the same rows as their neighbours' direct reads, so each array streams once.
+constexpr int kAsmPerCTA = 2 * kAsmThreads;
+
+// value of one element (calc.cpp:384-418) of row r with mirror row m (m = r for a = b):
+//   V + D + R_ai,jb - R_aj,ib - R_bi,ja + R_bj,ia + 0.5 x_i t_ab,ji - 0.5 x_j t_ab,ij
+//     + (-0.5 y_b) t_ab,ij - (-0.5 y_a) t_ba,ij          with (a, b) = pab of row r.
+__device__ __forceinline__ double asm_value(double v, double dm, double r_j, double r_js,
+                                            double rm_j, double rm_js, double t_j, double t_js,
+                                            double tm_j, double xi, double xj, double ya,
+                                            double yb, double den, double mixing) {
+  double value = v;
+  value += dm;
+  value += r_j;
+  value -= r_js;
+  value -= rm_j;
+  value += rm_js;
+  value += (0.5 * xi) * t_js;
+  value -= (0.5 * xj) * t_j;
+  value += (-0.5 * yb) * t_j;
+  value -= (-0.5 * ya) * tm_j;
+  value = value / den;
+  return mixing * value + (1. - mixing) * t_j;
+}
+
+__global__ void __launch_bounds__(kAsmThreads, 3)
+assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__restrict__ chans,
                       const int2 *__restrict__ pp_pairs, const int2 *__restrict__ hh_pairs,
-                      const int32_t *__restrict__ pp_swap, const int32_t *__restrict__ hh_swap,
-                      const int2 *__restrict__ pk_idx,
+                      const int32_t *__restrict__ hh_swap, const int32_t *__restrict__ rowmap,
+                      const int32_t *__restrict__ mirror, const int2 *__restrict__ pk_idx,
                       const double *__restrict__ v_pphh, const double *__restrict__ dmat,
-                      const double *__restrict__ r_phhp, const int32_t *__restrict__ g_ai_jb,
-                      const int32_t *__restrict__ g_aj_ib, const int32_t *__restrict__ g_bi_ja,
-                      const int32_t *__restrict__ g_bj_ia, const double *__restrict__ xh,
+                      const double *__restrict__ d_ring, const double *__restrict__ xh,
                       const double *__restrict__ yp, const double *__restrict__ eps, int np,
-                      double *tbuf0, double *tbuf1, double *__restrict__ old_phhp,
-                      double *__restrict__ t_kt, double *__restrict__ t_mt,
-                      double *__restrict__ epart, int32_t *ticket, Control *ctl,
-                      __nv_bfloat16 *__restrict__ tkt_tc, int64_t tkt_tc_stride,
+                      double *tbuf0, double *tbuf1, double *__restrict__ t_kt,
+                      double *__restrict__ t_mt, double *__restrict__ epart, int32_t *ticket,
+                      Control *ctl, __nv_bfloat16 *__restrict__ tkt_tc, int64_t tkt_tc_stride,
                       __nv_bfloat16 *__restrict__ tmt_tc, int64_t tmt_tc_stride, int nt,
                       int gate) {
   if (skip_iteration(ctl, gate)) return;
   __shared__ double scratch[32];
   __shared__ int last;
-  const ElemRange rg = ranges[blockIdx.x];
+  const ElemRange rg = pranges[blockIdx.x];
   const ChanInfo ch = chans[rg.ch];
-  const double *t_old = ctl->parity ? tbuf1 : tbuf0;
-  double *t_new = ctl->parity ? tbuf0 : tbuf1;
+  const double *__restrict__ t_old = ctl->parity ? tbuf1 : tbuf0;
+  double *__restrict__ t_new = ctl->parity ? tbuf0 : tbuf1;
   const double mixing = ctl->mixing;
   const int hh = ch.hh;
   double corr = 0.0;
-  for (int64_t e = rg.e0 + threadIdx.x; e < rg.e1; e += kAsmThreads) {
-    const int64_t loc = e - ch.t_off;
-    const int ab = (int)(loc / hh), ij = (int)(loc - (int64_t)ab * hh);
-    const int2 pab = pp_pairs[ch.pp_off + ab], pij = hh_pairs[ch.hh_off + ij];
-    const double v = v_pphh[e];
-    const double to = t_old[e];
-    const double t_ji = t_old[ch.t_off + (int64_t)ab * hh + hh_swap[ch.hh_off + ij]];
-    const double t_ba = t_old[ch.t_off + (int64_t)pp_swap[ch.pp_off + ab] * hh + ij];
-    double value = v;
-    value += dmat[e];
-    value += r_phhp[g_ai_jb[e]];
-    value -= r_phhp[g_aj_ib[e]];
-    value -= r_phhp[g_bi_ja[e]];
-    value += r_phhp[g_bj_ia[e]];
-    value += (0.5 * xh[pij.x]) * t_ji;
-    value -= (0.5 * xh[pij.y]) * to;
-    value += (-0.5 * yp[pab.y - np]) * to;
-    value -= (-0.5 * yp[pab.x - np]) * t_ba;
-    value = value / (eps[pij.x] + eps[pij.y] - eps[pab.x] - eps[pab.y]);
-    value = mixing * value + (1. - mixing) * to;
-    t_new[e] = value;
-    old_phhp[g_ai_jb[e]] = value;
-    write_t_tiles(ch, pk_idx, ab, ij, value, t_kt, t_mt);
-    if (nt) write_t_tiles_tc(ch, pk_idx, ab, ij, value, nt, tkt_tc, tkt_tc_stride, tmt_tc,
+#pragma unroll 2
+  for (int64_t q = rg.e0 + threadIdx.x; q < rg.e1; q += kAsmThreads) {
+    const int u = (int)(q / hh), j = (int)(q - (int64_t)u * hh);
+    const int ab = rowmap[ch.row_off + u], mi = mirror[ch.row_off + u];
+    const int ba = mi >= 0 ? mi : ab;
+    const int js = hh_swap[ch.hh_off + j];
+    const int2 pij = hh_pairs[ch.hh_off + j];
+    const int2 pab = pp_pairs[ch.pp_off + ab];
+    const int64_t o_ab = ch.t_off + (int64_t)ab * hh, o_ba = ch.t_off + (int64_t)ba * hh;
+    const double t_abj = t_old[o_ab + j], t_abs = t_old[o_ab + js];
+    const double t_baj = t_old[o_ba + j], t_bas = t_old[o_ba + js];
+    const double r_abj = d_ring[o_ab + j], r_abs = d_ring[o_ab + js];
+    const double r_baj = d_ring[o_ba + j], r_bas = d_ring[o_ba + js];
+    const double v1 = v_pphh[o_ab + j], d1 = dmat[o_ab + j];
+    const double xi = xh[pij.x], xj = xh[pij.y];
+    const double ya = yp[pab.x - np], yb = yp[pab.y - np];
+    const double ei = eps[pij.x], ej = eps[pij.y], ea = eps[pab.x], eb = eps[pab.y];
+    const double t1 = asm_value(v1, d1, r_abj, r_abs, r_baj, r_bas, t_abj, t_abs, t_baj, xi, xj,
+                                ya, yb, ei + ej - ea - eb, mixing);
+    t_new[o_ab + j] = t1;
+    write_t_tiles(ch, pk_idx, ab, j, t1, t_kt, t_mt);
+    if (nt) write_t_tiles_tc(ch, pk_idx, ab, j, t1, nt, tkt_tc, tkt_tc_stride, tmt_tc,
                              tmt_tc_stride);
-    corr += v * value;
+    corr += v1 * t1;
+    if (mi >= 0) {
+      // Row ba: the same formula with a and b exchanged.
+      const double v2 = v_pphh[o_ba + j], d2 = dmat[o_ba + j];
+      const double t2 = asm_value(v2, d2, r_baj, r_bas, r_abj, r_abs, t_baj, t_bas, t_abj, xi, xj,
+                                  yb, ya, ei + ej - eb - ea, mixing);
+      t_new[o_ba + j] = t2;
+      write_t_tiles(ch, pk_idx, ba, j, t2, t_kt, t_mt);
+      if (nt) write_t_tiles_tc(ch, pk_idx, ba, j, t2, nt, tkt_tc, tkt_tc_stride, tmt_tc,
+                               tmt_tc_stride);
+      corr += v2 * t2;
+    }
   }
   const double sum = block_sum<kAsmThreads>(corr, scratch);
   // The last CTA to finish sums the partials and applies the stop rule (no extra launch).

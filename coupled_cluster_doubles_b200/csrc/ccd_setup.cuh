@@ -108,6 +108,35 @@ __global__ void convert_tables_kernel(const ElemRange *__restrict__ ranges, cons
   }
 }
 
+// Fused-path ring tables.  inv[ai_jb(e)] = e turns the phhp slab position of every amplitude
+// back into its pphh element, so the ring can read T' from the amplitudes and write R in pphh
+// order.  The other three ring maps of loadMaps are ai_jb composed with the swaps i<->j and
+// a<->b (load.cpp:469-526 builds all four from the same (a,i),(j,b) pairing); this is checked
+// here, since the fused assembly reads R_aj,ib, R_bi,ja and R_bj,ia at (ab,ji), (ba,ij) and
+// (ba,ji) of the pphh-ordered R.
+__global__ void ring_maps_kernel(const ElemRange *__restrict__ ranges,
+                                 const ChanInfo *__restrict__ chans,
+                                 const int32_t *__restrict__ pp_swap,
+                                 const int32_t *__restrict__ hh_swap,
+                                 const int32_t *__restrict__ flat, int64_t n_t,
+                                 int32_t *__restrict__ inv, int32_t *err) {
+  const ElemRange rg = ranges[blockIdx.x];
+  const ChanInfo ch = chans[rg.ch];
+  for (int64_t e = rg.e0 + threadIdx.x; e < rg.e1; e += blockDim.x) {
+    const int64_t loc = e - ch.t_off;
+    const int ab = (int)(loc / ch.hh), ij = (int)(loc - (int64_t)ab * ch.hh);
+    const int ps = pp_swap[ch.pp_off + ab], hs = hh_swap[ch.hh_off + ij];
+    const int64_t e_ji = ch.t_off + (int64_t)ab * ch.hh + hs;
+    const int64_t e_ba = ch.t_off + (int64_t)ps * ch.hh + ij;
+    const int64_t e_baji = ch.t_off + (int64_t)ps * ch.hh + hs;
+    const int32_t f = flat[4 * n_t + e];
+    inv[f] = (int32_t)e;
+    if (flat[5 * n_t + e] != flat[4 * n_t + e_ji] || flat[6 * n_t + e] != flat[4 * n_t + e_ba] ||
+        flat[7 * n_t + e] != flat[4 * n_t + e_baji])
+      atomicOr(err, kErrRingMaps);
+  }
+}
+
 __global__ void check_counts_kernel(const int32_t *__restrict__ counts, int64_t n, int32_t *err) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)

@@ -43,21 +43,25 @@ struct ccdgpu_handle {
   cudaEvent_t ev[10] = {};
   uint64_t nch = 0, nsp = 0, np = 0, npart = 0;
   int64_t n_t = 0, n_m = 0, n_h = 0, n_p = 0;
-  int n_act = 0, n_mod = 0, n_mod_small = 0, n_tiles = 0, n_hh_tiles = 0, n_ranges = 0;
+  int n_hh_small = 0;  // hh-ladder tiles of channels with hh <= 16 (first in hh_tiles)
+  int n_act = 0, n_mod = 0, n_mod_small = 0, n_mod_mid = 0, n_tiles = 0, n_hh_tiles = 0;
+  int n_ranges = 0;
+  int n_asm_blocks = 0;  // fused assembly CTAs (packed-element ranges)
   int n_cls[3] = {0, 0, 0};  // pp-ladder tiles per column class (thin, mid, wide), in that order
   size_t ladder_smem_thin = 0;
-  size_t ladder_smem = 0, ring_smem = 0, hh_smem = 0;
+  size_t ladder_smem = 0, ring_smem = 0, ring_smem_mid = 0, hh_smem = 0;
   bool have_3body = false;
   std::vector<DevBuf> allocs;
 
   ChanInfo *chans = nullptr;
-  ModInfo *mods = nullptr;        // small channels first (n_mod_small), then the others
+  ModInfo *mods = nullptr;        // small (n_mod_small), mid (n_mod_mid), then large channels
   LadderTile *tiles = nullptr;
   HHTile *hh_tiles = nullptr;
   int32_t *rowmap = nullptr, *mirror = nullptr, *counters = nullptr, *lcounters = nullptr;
   int2 *pk_idx = nullptr;
   double *part = nullptr, *lpart = nullptr;
   ElemRange *ranges = nullptr;
+  ElemRange *pranges = nullptr;  // fused assembly: ranges of packed elements u * hh + j
   int2 *pp_pairs = nullptr, *hh_pairs = nullptr;
   int32_t *pp_swap = nullptr, *hh_swap = nullptr;
   int64_t *list_off = nullptr;
@@ -68,6 +72,8 @@ struct ccdgpu_handle {
   double *x = nullptr, *x_t = nullptr, *t_kt = nullptr, *t_mt = nullptr;
   double *s = nullptr, *r = nullptr, *xh = nullptr, *yp = nullptr, *epart = nullptr;
   int32_t *flat = nullptr;
+  int32_t *inv4 = nullptr;   // phhp position -> pphh element (inverse of the ai_jb table)
+  double *d_ring = nullptr;  // fused path: ring result R in pphh order
   int64_t *o_h = nullptr, *o_p = nullptr;
   double *v_h_hpp = nullptr, *v_phh_p = nullptr;
   double *old_h1pp_h2 = nullptr, *old_h2pp_h1 = nullptr, *diff_h2pp_h1 = nullptr;
@@ -279,7 +285,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     ci.nkc = (int)ceil_div(pk, kBK);
     ci.nkh = (int)ceil_div(hh, kBK);
     ci.nmt = (int)ceil_div(pr, ci.bm);
-    ci.nhht = (int)ceil_div(pp, kHHRows);
+    ci.nhht = (int)ceil_div(pp, hh_slice_rows((int)hh));
     ci.t_off = o_t[c];
     ci.tkt_base = tkt; ci.tmt_base = tmt; ci.xt_base = xt; ci.vkt_base = vt;
     ci.part_off = part_tot;
@@ -302,19 +308,29 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     vraw_off.push_back(vraw_tot);
     vraw_tot += pp * pp;
     maxhh = std::max<int>(maxhh, (int)hh);
-    for (int t = 0; t < ci.nhht; t++) hh_tiles.push_back({ai, t * kHHRows, t, 0});
+    const int hrows = hh_slice_rows((int)hh);
+    for (int t = 0; t < ci.nhht; t++)
+      hh_tiles.push_back({ai, t * hrows, t, (int)std::min<int64_t>(hrows, pp - (int64_t)t * hrows)});
     chans.push_back(ci);
     act_chan.push_back(c);
   }
   h->n_act = (int)chans.size();
   h->n_hh_tiles = (int)hh_tiles.size();
+  // Channels with hh <= 16 first (their own launch), then the tiled ones; largest slices
+  // (rows x hh^2) first within each, so the short ones fill in behind them.
+  std::stable_sort(hh_tiles.begin(), hh_tiles.end(), [&](const HHTile &x, const HHTile &y) {
+    const ChanInfo &a = chans[x.ch], &b = chans[y.ch];
+    if ((a.hh > 16) != (b.hh > 16)) return a.hh <= 16;
+    return (int64_t)x.rows * a.hh * a.hh > (int64_t)y.rows * b.hh * b.hh;
+  });
+  for (const HHTile &t : hh_tiles) h->n_hh_small += chans[t.ch].hh <= 16 ? 1 : 0;
   std::vector<int64_t> list_off(nsp + 1, 0);
   for (uint64_t w = 0; w < nsp; w++) list_off[w + 1] = list_off[w] + (int64_t)seg[w].size();
   std::vector<int32_t> list(list_off[nsp]);
   for (uint64_t w = 0; w < nsp; w++) std::copy(seg[w].begin(), seg[w].end(), list.begin() + list_off[w]);
 
-  // Modified channels: small ones (one warp each) first.
-  std::vector<ModInfo> mods, mods_big;
+  // Modified channels: small ones (one warp each) first, then mid and large ones.
+  std::vector<ModInfo> mods, mods_mid, mods_big;
   std::vector<int2> mod_dims(nch);
   int64_t y_tot = 0;
   size_t ring_smem = 0;
@@ -324,20 +340,27 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     const int64_t ph = MD[c].ph, hp = MD[c].hp;
     mod_dims[c] = make_int2((int)ph, (int)hp);
     if (!ph || !hp) continue;
+    if (ph > kTcMaxNB || hp > kTcMaxNB) return CCDGPU_ERR_UNSUPPORTED;  // ring register tiles
     if (!P->v_hpph_mod[c] || !P->v_hphp_mod[c]) return CCDGPU_ERR_INVALID_ARGUMENT;
     ModInfo m{};
     m.ph = (int)ph; m.hp = (int)hp; m.m_off = o_m[c]; m.y_off = y_tot;
     y_tot += hp * hp;
     src_hpph.push_back(P->v_hpph_mod[c]); cnt_hpph.push_back(ph * hp);
     src_hphp.push_back(P->v_hphp_mod[c]); cnt_hphp.push_back(hp * hp);
+    const size_t smem = (size_t)(2 * ph * hp + hp * hp) * 8;
     if (ph <= kRingSmall && hp <= kRingSmall) {
       mods.push_back(m);
+    } else if (ph <= kRingMid && hp <= kRingMid) {
+      h->ring_smem_mid = std::max(h->ring_smem_mid, smem);
+      mods_mid.push_back(m);
     } else {
-      ring_smem = std::max(ring_smem, (size_t)(2 * ph * hp + hp * hp) * 8);
+      ring_smem = std::max(ring_smem, smem);
       mods_big.push_back(m);
     }
   }
   h->n_mod_small = (int)mods.size();
+  h->n_mod_mid = (int)mods_mid.size();
+  mods.insert(mods.end(), mods_mid.begin(), mods_mid.end());
   mods.insert(mods.end(), mods_big.begin(), mods_big.end());
   h->n_mod = (int)mods.size();
   h->ring_smem = ring_smem;
@@ -449,6 +472,13 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     for (int64_t e = 0; e < n; e += per) ranges.push_back({ai, 0, a.t_off + e, a.t_off + std::min(n, e + per)});
   }
   h->n_ranges = (int)ranges.size();
+  std::vector<ElemRange> pranges;
+  for (int ai = 0; ai < h->n_act; ai++) {
+    const int64_t n = (int64_t)chans[ai].pr * chans[ai].hh;
+    for (int64_t q = 0; q < n; q += kAsmPerCTA)
+      pranges.push_back({ai, 0, q, std::min<int64_t>(n, q + kAsmPerCTA)});
+  }
+  h->n_asm_blocks = (int)pranges.size();
 
   // Work estimate (reference GEMM flops) for roofline reporting.
   double fl = 0, lf = 0, vb = 0, vbp = 0;
@@ -489,12 +519,13 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   ar.add(&h->eps, nsp);
   ar.add(&h->v_pphh, n_t); ar.add(&h->v_hhhh, x_tot); ar.add(&h->v_t, vt);
   ar.add(&h->v_hpph, h->n_m); ar.add(&h->v_hphp, y_tot);
-  ar.add(&h->flat, (size_t)8 * n_t); ar.add(&h->o_h, o_h.size()); ar.add(&h->o_p, o_p.size());
+  ar.add(&h->flat, (size_t)8 * n_t); ar.add(&h->inv4, n_t); ar.add(&h->d_ring, n_t); ar.add(&h->o_h, o_h.size()); ar.add(&h->o_p, o_p.size());
   ar.add(&h->t[0], n_t); ar.add(&h->t[1], n_t); ar.add(&h->dmat, n_t);
   ar.add(&h->old_phhp, h->n_m); ar.add(&h->r_phhp, h->n_m);
   ar.add(&h->x, x_tot); ar.add(&h->x_t, xt); ar.add(&h->t_kt, tkt); ar.add(&h->t_mt, tmt);
   ar.add(&h->s, hh_tot); ar.add(&h->r, pp_tot); ar.add(&h->xh, np); ar.add(&h->yp, h->npart);
-  ar.add(&h->epart, h->n_ranges); ar.add(&h->ctl, 1); ar.add(&h->e_out, 1); ar.add(&h->err, 1);
+  ar.add(&h->pranges, pranges.size());
+  ar.add(&h->epart, std::max(h->n_ranges, h->n_asm_blocks)); ar.add(&h->ctl, 1); ar.add(&h->e_out, 1); ar.add(&h->err, 1);
   ar.add(&h->ticket, 1);
   if (h->nt) {
     auto round_up = [](int64_t n) { return std::max<int64_t>(256, (n + 255) / 256 * 256); };
@@ -533,7 +564,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     return CCDGPU_OK;
   };
   TRY(put(h->chans, chans)); TRY(put(h->mods, mods)); TRY(put(h->tiles, tiles));
-  TRY(put(h->hh_tiles, hh_tiles)); TRY(put(h->ranges, ranges));
+  TRY(put(h->hh_tiles, hh_tiles)); TRY(put(h->ranges, ranges)); TRY(put(h->pranges, pranges));
   if (h->nt) TRY(put(h->tc_tiles, tc_tiles));
   TRY(put(h->pp_pairs, pp_pairs)); TRY(put(h->hh_pairs, hh_pairs));
   TRY(put(h->pp_swap, pp_swap)); TRY(put(h->hh_swap, hh_swap));
@@ -599,6 +630,9 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     const int nb = (int)std::min<int64_t>(ceil_div(5 * n_t, 256), 148 * 32);
     check_counts_kernel<<<std::max(nb, 1), 256, 0, h->s0>>>(counts, 5 * n_t, h->err);
     CK(cudaGetLastError());
+    ring_maps_kernel<<<h->n_ranges, 256, 0, h->s0>>>(h->ranges, h->chans, h->pp_swap, h->hh_swap,
+                                                     h->flat, n_t, h->inv4, h->err);
+    CK(cudaGetLastError());
   }
   if (!vrows.empty()) {
     tile_v_kernel<<<(unsigned)vrows.size(), 128, 0, h->s0>>>(h->chans, d_vrows, h->rowmap, d_kcol,
@@ -617,7 +651,10 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   for (size_t i = n_allocs; i < h->allocs.size(); i++) cudaFree(h->allocs[i].p);
   h->allocs.resize(n_allocs);
   if (e & kErrBadIndex) return CCDGPU_ERR_BAD_TABLE;
-  if (e) return CCDGPU_ERR_CUDA;
+  // The fused path relies on the structure of the ring tables; the table path does not.
+  if ((e & kErrRingMaps) && h->opt.path == CCDGPU_PATH_FUSED) return CCDGPU_ERR_BAD_TABLE;
+  if (e & ~kErrRingMaps) return CCDGPU_ERR_CUDA;
+  if (e) CK(cudaMemsetAsync(h->err, 0, sizeof(int32_t), h->s0));
 #undef TRY
   CK(cudaMallocHost(&h->h_ctl, sizeof(Control)));
   std::memset(h->h_ctl, 0, sizeof(Control));
@@ -633,10 +670,10 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   CK(cudaFuncSetAttribute(pp_ladder_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)h->ladder_smem));
   CK(cudaFuncSetAttribute(pp_ladder_kernel<2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-  h->hh_smem = (size_t)2 * kHHRows * maxhh * 8;
-  CK(cudaFuncSetAttribute(hh_ladder_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)h->hh_smem));
-  CK(cudaFuncSetAttribute(ring_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  h->hh_smem = 0;  // static shared memory only
+  CK(cudaFuncSetAttribute(ring_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)std::max<size_t>(h->ring_smem_mid, 16)));
+  CK(cudaFuncSetAttribute(ring_kernel<5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)std::max<size_t>(h->ring_smem, 16)));
   if (h->nt) {
     h->tc_smem = tc_smem_bytes(h->nt);
@@ -674,12 +711,21 @@ cudaError_t launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, 
 // gate: 0 = kernel of an FP64 iteration, 1 = of a mixed-precision iteration (which also writes
 // the bf16 operand images of the tensor-core ladder).
 int launch_hh_ladder(ccdgpu_handle *h, cudaStream_t st, int gate) {
-  if (!h->n_hh_tiles) return CCDGPU_OK;
-  h->launches++;
-  return cuda_status(launch_pdl(hh_ladder_kernel, h->n_hh_tiles, kHHThreads, h->hh_smem, st,
-                                h->hh_tiles, h->chans, h->v_pphh, h->v_hhhh, h->t[0], h->t[1],
-                                h->part, h->counters, h->x, h->x_t, h->s, h->r, h->xt_tc,
-                                h->n_xttc, gate ? h->nt : 0, h->ctl, gate));
+  const int nt = gate ? h->nt : 0;
+  if (h->n_hh_small) {
+    h->launches++;
+    CK(launch_pdl(hh_ladder_kernel<true>, h->n_hh_small, kHHThreads, 0, st, h->hh_tiles, h->chans,
+                  h->v_pphh, h->v_hhhh, h->t[0], h->t[1], h->part, h->counters, h->x, h->x_t,
+                  h->s, h->r, h->xt_tc, h->n_xttc, nt, h->ctl, gate));
+  }
+  const int nbig = h->n_hh_tiles - h->n_hh_small;
+  if (nbig) {
+    h->launches++;
+    CK(launch_pdl(hh_ladder_kernel<false>, nbig, kHHThreads, 0, st, h->hh_tiles + h->n_hh_small,
+                  h->chans, h->v_pphh, h->v_hhhh, h->t[0], h->t[1], h->part, h->counters, h->x,
+                  h->x_t, h->s, h->r, h->xt_tc, h->n_xttc, nt, h->ctl, gate));
+  }
+  return CCDGPU_OK;
 }
 int launch_pp_ladder_tc(ccdgpu_handle *h, cudaStream_t st) {
   if (!h->n_tc_tiles) return CCDGPU_OK;
@@ -729,17 +775,29 @@ int launch_pp_ladder(ccdgpu_handle *h, cudaStream_t st) {
   return CCDGPU_OK;
 }
 
-int launch_ring(ccdgpu_handle *h, cudaStream_t st, int gate) {
+// fused: the fused path's layout (T' gathered from the amplitudes, R in pphh order); else the
+// table path's phhp slabs (t2Old_phhp -> t2Diff_phhp).
+int launch_ring(ccdgpu_handle *h, cudaStream_t st, int gate, bool fused) {
+  const int32_t *inv = fused ? h->inv4 : nullptr;
+  const double *t0 = fused ? h->t[0] : h->old_phhp, *t1 = fused ? h->t[1] : h->old_phhp;
+  double *out = fused ? h->d_ring : h->r_phhp;
   if (h->n_mod_small) {
     ring_small_kernel<<<(int)ceil_div(h->n_mod_small, 8), 256, 0, st>>>(
-        h->mods, h->n_mod_small, h->v_hpph, h->v_hphp, h->old_phhp, h->r_phhp, h->ctl, gate);
+        h->mods, h->n_mod_small, h->v_hpph, h->v_hphp, t0, t1, inv, out, h->ctl, gate);
     h->launches++;
     CK(cudaGetLastError());
   }
-  const int nbig = h->n_mod - h->n_mod_small;
+  if (h->n_mod_mid) {
+    ring_kernel<2><<<h->n_mod_mid, kRingThreads, std::max<size_t>(h->ring_smem_mid, 16), st>>>(
+        h->mods + h->n_mod_small, h->v_hpph, h->v_hphp, t0, t1, inv, out, h->ctl, gate);
+    h->launches++;
+    CK(cudaGetLastError());
+  }
+  const int nbig = h->n_mod - h->n_mod_small - h->n_mod_mid;
   if (nbig) {
-    ring_kernel<<<nbig, kRingThreads, std::max<size_t>(h->ring_smem, 16), st>>>(
-        h->mods + h->n_mod_small, h->v_hpph, h->v_hphp, h->old_phhp, h->r_phhp, h->ctl, gate);
+    ring_kernel<5><<<nbig, kRingThreads, std::max<size_t>(h->ring_smem, 16), st>>>(
+        h->mods + h->n_mod_small + h->n_mod_mid, h->v_hpph, h->v_hphp, t0, t1, inv, out, h->ctl,
+        gate);
     h->launches++;
     CK(cudaGetLastError());
   }
@@ -754,15 +812,13 @@ int launch_onebody_fused(ccdgpu_handle *h, cudaStream_t st, int gate) {
                                 h->yp, h->ctl, gate));
 }
 int launch_assemble_fused(ccdgpu_handle *h, cudaStream_t st, int gate) {
-  if (!h->n_ranges) return CCDGPU_OK;
-  const int64_t n_t = h->n_t;
+  if (!h->n_asm_blocks) return CCDGPU_OK;
   h->launches++;
   return cuda_status(launch_pdl(
-      assemble_fused_kernel, h->n_ranges, kAsmThreads, 0, st, h->ranges, h->chans, h->pp_pairs,
-      h->hh_pairs, h->pp_swap, h->hh_swap, h->pk_idx, h->v_pphh, h->dmat, h->r_phhp,
-      h->flat + 4 * n_t, h->flat + 5 * n_t, h->flat + 6 * n_t, h->flat + 7 * n_t, h->xh, h->yp,
-      h->eps, (int)h->np, h->t[0], h->t[1], h->old_phhp, h->t_kt, h->t_mt, h->epart, h->ticket,
-      h->ctl, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc, gate ? h->nt : 0, gate));
+      assemble_fused_kernel, h->n_asm_blocks, kAsmThreads, 0, st, h->pranges, h->chans,
+      h->pp_pairs, h->hh_pairs, h->hh_swap, h->rowmap, h->mirror, h->pk_idx, h->v_pphh, h->dmat,
+      h->d_ring, h->xh, h->yp, h->eps, (int)h->np, h->t[0], h->t[1], h->t_kt, h->t_mt, h->epart,
+      h->ticket, h->ctl, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc, gate ? h->nt : 0, gate));
 }
 int launch_energy(ccdgpu_handle *h, cudaStream_t st, int flags) {
   energy_kernel<<<1, kEnergyThreads, 0, st>>>(h->epart, h->n_ranges, h->ctl, flags, h->e_out, 0);
@@ -794,7 +850,7 @@ int enqueue_fused_iteration(ccdgpu_handle *h, bool mixed) {
     CK(cudaEventRecord(h->ev[0], h->s0));
     CK(cudaStreamWaitEvent(h->s1, h->ev[0], 0));
     CK(cudaEventRecord(h->ev[4], h->s1));
-    if ((rc = launch_ring(h, h->s1, gate))) return rc;
+    if ((rc = launch_ring(h, h->s1, gate, true))) return rc;
     CK(cudaEventRecord(h->ev[5], h->s1));
     if ((rc = launch_hh_ladder(h, h->s0, gate))) return rc;
     CK(cudaEventRecord(h->ev[1], h->s0));
@@ -811,7 +867,7 @@ int enqueue_fused_iteration(ccdgpu_handle *h, bool mixed) {
   }
   CK(cudaEventRecord(h->ev_fork, h->s0));
   CK(cudaStreamWaitEvent(h->s1, h->ev_fork, 0));
-  if ((rc = launch_ring(h, h->s1, gate))) return rc;
+  if ((rc = launch_ring(h, h->s1, gate, true))) return rc;
   CK(cudaEventRecord(h->ev_join, h->s1));
   if ((rc = launch_hh_ladder(h, h->s0, gate))) return rc;
   if ((rc = launch_onebody_fused(h, h->s0, gate))) return rc;
@@ -913,7 +969,7 @@ int tables_iteration(ccdgpu_handle *h, double mixing, double *corr) {
   int rc;
   if ((rc = stage_onebody_tables(h, 0, 1))) return rc;     // calcT2Diff_p2_p1hh
   if ((rc = stage_onebody_tables(h, 1, 0))) return rc;     // calcT2Diff_h2pp_h1
-  if ((rc = launch_ring(h, h->s0, 0))) return rc;          // calcT2Diff_phhp
+  if ((rc = launch_ring(h, h->s0, 0, false))) return rc;   // calcT2Diff_phhp
   if ((rc = launch_hh_ladder(h, h->s0, 0))) return rc;     // calcT2Diff_pphh
   if ((rc = launch_pp_ladder(h, h->s0))) return rc;
   if ((rc = stage_gather(h))) return rc;                   // 8 x mapFromDistributed
@@ -1150,7 +1206,7 @@ int ccdgpu_calc_t2diff_h2pp_h1(ccdgpu_handle *h) {
 int ccdgpu_calc_t2diff_phhp(ccdgpu_handle *h) {
   if (!h) return CCDGPU_ERR_INVALID_ARGUMENT;
   int rc = set_ctl(h, 0, h->h_ctl->tol, h->h_ctl->max_iters, h->h_ctl->mixing, false);
-  if (rc || (rc = launch_ring(h, h->s0, 0))) return rc;
+  if (rc || (rc = launch_ring(h, h->s0, 0, false))) return rc;
   CK(cudaStreamSynchronize(h->s0));
   return CCDGPU_OK;
 }
