@@ -122,6 +122,12 @@ struct ElemRange {
   int64_t e0, e1;
 };
 
+// Kernel ids of the start-time trace (Control::trace_*).
+enum TraceKernel {
+  kTrRingSmall = 0, kTrRingMid, kTrRingLarge, kTrHHSmall, kTrHHTiled, kTrOneBody, kTrLadderThin,
+  kTrLadderMid, kTrLadderWide, kTrLadderTC, kTrAssemble, kTrLoopCtl, kTrEnergy, kTraceKernels
+};
+
 // Device control block: iteration state of the solve loop lives on the device so that a
 // captured iteration can be replayed without host round trips.
 struct Control {
@@ -140,6 +146,10 @@ struct Control {
   int32_t pad;
   double polish_rel;     // phase 1 -> 2 once |dE| <= max(tol, polish_rel * |E|)
   int64_t polish_iters;  // iterations run in phase 2
+  int64_t stop_at;       // device solve loop: one graph launch runs while iterations < stop_at
+  int64_t trace_iter;    // kernel trace: the iteration whose kernels record start times
+  uint64_t trace_first[kTraceKernels];  // %globaltimer of the first / last CTA start
+  uint64_t trace_last[kTraceKernels];
   double energies[128];  // corrCCD per iteration (first 128)
 };
 

@@ -97,8 +97,18 @@ __device__ __forceinline__ void pdl_enter() {
 // gate 0: kernel of an FP64 iteration, gate 1: kernel of a mixed-precision iteration.  During
 // a solve, an iteration whose precision does not match the phase is a no-op (a replayed batch
 // can straddle the switch to the FP64 polish).
-__device__ __forceinline__ bool skip_iteration(const Control *ctl, int gate) {
+// The kernel id `tr` records its first and last CTA start in the trace of the armed iteration.
+__device__ __forceinline__ void trace_start(const Control *ctl, int tr) {
+  if (threadIdx.x == 0 && ctl->trace_iter == ctl->iterations) {
+    Control *c = const_cast<Control *>(ctl);
+    const unsigned long long t = global_ns();
+    atomicMin(reinterpret_cast<unsigned long long *>(&c->trace_first[tr]), t);
+    atomicMax(reinterpret_cast<unsigned long long *>(&c->trace_last[tr]), t);
+  }
+}
+__device__ __forceinline__ bool skip_iteration(const Control *ctl, int gate, int tr) {
   pdl_enter();
+  trace_start(ctl, tr);
   if (!ctl->active) return false;
   return ctl->done || ((gate == 1) != (ctl->phase == 1));
 }
@@ -267,7 +277,7 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict_
                  const double *__restrict__ x_t, const int32_t *__restrict__ rowmap,
                  const int32_t *__restrict__ mirror, double *__restrict__ d, double *part,
                  int32_t *counters, const Control *ctl, int32_t *err, int gate) {
-  if (skip_iteration(ctl, gate)) return;
+  if (skip_iteration(ctl, gate, kTrLadderThin + CLS)) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double *As = reinterpret_cast<double *>(smem_raw);
   double *Bs = As + kStages * kMaxBM * kBK;
@@ -442,7 +452,7 @@ hh_ladder_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ 
                  double *__restrict__ x_ref, double *__restrict__ x_t, double *__restrict__ s_out,
                  double *__restrict__ r_out, __nv_bfloat16 *__restrict__ xt_tc,
                  int64_t xt_tc_stride, int nt, const Control *ctl, int gate) {
-  if (skip_iteration(ctl, gate)) return;
+  if (skip_iteration(ctl, gate, SMALL ? kTrHHSmall : kTrHHTiled)) return;
   __shared__ __align__(16) double Vs[kHHElems], Ts[kHHElems];
   __shared__ double red[kHHThreads];
   __shared__ int last;
@@ -524,7 +534,7 @@ ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restr
                   const double *__restrict__ v_hphp, const double *tbuf0, const double *tbuf1,
                   const int32_t *__restrict__ inv, double *__restrict__ out, const Control *ctl,
                   int gate) {
-  if (skip_iteration(ctl, gate)) return;
+  if (skip_iteration(ctl, gate, kTrRingSmall)) return;
   __shared__ double buf[8][3 * kRingSmall * kRingSmall];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int mi = blockIdx.x * 8 + w;
@@ -642,7 +652,7 @@ ring_kernel(const ModInfo *__restrict__ mods, const double *__restrict__ v_hpph,
             const double *__restrict__ v_hphp, const double *tbuf0, const double *tbuf1,
             const int32_t *__restrict__ inv, double *__restrict__ out, const Control *ctl,
             int gate) {
-  if (skip_iteration(ctl, gate)) return;
+  if (skip_iteration(ctl, gate, TMAX <= 2 ? kTrRingMid : kTrRingLarge)) return;
   extern __shared__ __align__(16) double rs[];
   const ModInfo m = mods[blockIdx.x];
   const double *tsrc = ring_t(ctl, inv, tbuf0, tbuf1);
@@ -718,7 +728,7 @@ __global__ void onebody_fused_kernel(int np, int nsp, const int64_t *__restrict_
                                      const int32_t *__restrict__ list, const double *__restrict__ s,
                                      const double *__restrict__ r, double *__restrict__ xh,
                                      double *__restrict__ yp, const Control *ctl, int gate) {
-  if (skip_iteration(ctl, gate)) return;
+  if (skip_iteration(ctl, gate, kTrOneBody)) return;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (w >= nsp) return;
   const bool hole = w < np;
@@ -838,7 +848,7 @@ assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__r
                       Control *ctl, __nv_bfloat16 *__restrict__ tkt_tc, int64_t tkt_tc_stride,
                       __nv_bfloat16 *__restrict__ tmt_tc, int64_t tmt_tc_stride, int nt,
                       int gate) {
-  if (skip_iteration(ctl, gate)) return;
+  if (skip_iteration(ctl, gate, kTrAssemble)) return;
   __shared__ double scratch[32];
   __shared__ int last;
   const ElemRange rg = pranges[blockIdx.x];
@@ -1037,10 +1047,25 @@ __device__ __forceinline__ void energy_reduce(const double *epart, int n, Contro
   }
 }
 
+// Last node of an iteration body of the device solve loop (a CUDA graph with WHILE conditional
+// nodes): decides from the control block whether the loop runs another iteration.  body_mixed:
+// the mixed-precision loop continues in phase 1 only; the FP64 loop never runs in phase 1.
+// Every body ends here, also when its kernels skipped, so no loop can spin without progress:
+// a body either advances `iterations` or clears its condition.
+__global__ void loop_ctl_kernel(const Control *ctl, cudaGraphConditionalHandle cond,
+                                int body_mixed) {
+  pdl_enter();
+  trace_start(ctl, kTrLoopCtl);
+  if (threadIdx.x != 0) return;
+  const bool more = !ctl->done && ctl->iterations < ctl->stop_at;
+  const bool mixed_phase = ctl->phase == 1;
+  cudaGraphSetConditional(cond, (more && (body_mixed ? mixed_phase : !mixed_phase)) ? 1u : 0u);
+}
+
 __global__ void __launch_bounds__(kEnergyThreads)
 energy_kernel(const double *__restrict__ epart, int n, Control *ctl, int flags, double *e_out,
               int gate) {
-  if (skip_iteration(ctl, gate)) return;
+  if (skip_iteration(ctl, gate, kTrEnergy)) return;
   energy_reduce(epart, n, ctl, flags, e_out);
 }
 

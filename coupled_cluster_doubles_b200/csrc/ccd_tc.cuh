@@ -127,7 +127,7 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const __nv_bfloat16 *_
                     const int32_t *__restrict__ rowmap, const int32_t *__restrict__ mirror,
                     double *__restrict__ d, double *part, int32_t *counters, const Control *ctl,
                     int32_t *err) {
-  if (skip_iteration(ctl, 1)) return;
+  if (skip_iteration(ctl, 1, kTrLadderTC)) return;
   constexpr int S = tc_stages(NT);
   constexpr uint32_t kStageBytes = (uint32_t)tc_stage_bytes(NT);
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];

@@ -105,6 +105,15 @@ struct ccdgpu_handle {
   double ladder_bytes_tc = 0;
   cudaGraphExec_t graph_tc = nullptr;
   int64_t kernels_per_graph_tc = 0;
+
+  // Device solve loop: graphs of WHILE conditional nodes whose bodies are one iteration each
+  // (loop64: FP64 iterations; loop_tc: mixed iterations, then FP64 ones).  loop_state: 0 not
+  // built yet, 1 built, -1 unavailable (the batched graph replay is used instead).
+  cudaGraphExec_t loop64 = nullptr, loop_tc = nullptr;
+  int loop_state = 0;
+  int loop_capture = 0;  // while capturing a loop body: 1 FP64 body, 2 mixed body
+  cudaGraphConditionalHandle loop_cond = 0;
+  int64_t kernels_per_body64 = 0, kernels_per_body_tc = 0;
 };
 
 namespace {
@@ -142,6 +151,8 @@ void release(ccdgpu_handle *h) {
   if (!h) return;
   if (h->graph) cudaGraphExecDestroy(h->graph);
   if (h->graph_tc) cudaGraphExecDestroy(h->graph_tc);
+  if (h->loop64) cudaGraphExecDestroy(h->loop64);
+  if (h->loop_tc) cudaGraphExecDestroy(h->loop_tc);
   for (auto &b : h->allocs) cudaFree(b.p);
   h->allocs.clear();
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
@@ -692,6 +703,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
 // Launch with the programmatic-stream-serialization attribute (PDL): the kernel may begin
 // launching while its stream predecessor drains; it waits in griddepcontrol.wait before
 // touching the predecessor's results (skip_iteration / pdl_enter in every kernel).
+thread_local bool t_pdl = true;  // cleared while retrying a loop-graph capture without PDL
+
 template <typename... KArgs, typename... Args>
 cudaError_t launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem,
                        cudaStream_t st, Args... args) {
@@ -704,7 +717,7 @@ cudaError_t launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, 
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = t_pdl ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
 }
 
@@ -873,7 +886,13 @@ int enqueue_fused_iteration(ccdgpu_handle *h, bool mixed) {
   if ((rc = launch_onebody_fused(h, h->s0, gate))) return rc;
   if ((rc = ladder(h->s0))) return rc;
   CK(cudaStreamWaitEvent(h->s0, h->ev_join, 0));
-  return launch_assemble_fused(h, h->s0, gate);  // includes the energy reduction and stop rule
+  if ((rc = launch_assemble_fused(h, h->s0, gate))) return rc;  // + energy and stop rule
+  if (h->loop_capture) {
+    h->launches++;
+    CK(launch_pdl(loop_ctl_kernel, 1, 32, 0, h->s0, (const Control *)h->ctl, h->loop_cond,
+                  h->loop_capture == 2 ? 1 : 0));
+  }
+  return CCDGPU_OK;
 }
 
 // Table path stages (mirrors main.cpp:591-665).
@@ -964,6 +983,80 @@ int fused_ready_graph(ccdgpu_handle *h, bool mixed) {
   return CCDGPU_OK;
 }
 
+// The device solve loop.  Graph: [WHILE c_mix { mixed iteration }] -> WHILE c64 { FP64
+// iteration }; each body ends with loop_ctl_kernel, which sets its own condition.  Both
+// conditions default to 1 at every launch; one launch runs until the stop rule fires or
+// ctl->stop_at is reached.
+int capture_loop_graph(ccdgpu_handle *h, bool mixed, cudaGraphExec_t *exec) {
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  cudaGraphNode_t prev = nullptr;
+  int rc = CCDGPU_OK;
+  const int64_t before = h->launches;
+  for (int pass = mixed ? 0 : 1; pass < 2 && !rc; pass++) {
+    const bool body_mixed = pass == 0;
+    cudaGraphConditionalHandle cond = 0;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = cond;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, prev ? &prev : nullptr, prev ? 1 : 0, &p);
+    if (e == cudaSuccess)
+      e = cudaStreamBeginCaptureToGraph(h->s0, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      rc = cuda_status(e);
+      break;
+    }
+    h->loop_capture = body_mixed ? 2 : 1;
+    h->loop_cond = cond;
+    const int64_t b0 = h->launches;
+    rc = enqueue_fused_iteration(h, body_mixed);
+    (body_mixed ? h->kernels_per_body_tc : h->kernels_per_body64) = h->launches - b0;
+    h->loop_capture = 0;
+    cudaGraph_t body = nullptr;
+    e = cudaStreamEndCapture(h->s0, &body);
+    if (!rc && e != cudaSuccess) rc = cuda_status(e);
+    (void)cudaGetLastError();
+    prev = node;
+  }
+  h->launches = before;
+  if (!rc) {
+    cudaError_t e = cudaGraphInstantiate(exec, g, 0);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      *exec = nullptr;
+      rc = cuda_status(e);
+    }
+  }
+  cudaGraphDestroy(g);
+  return rc;
+}
+
+// Builds both loop graphs once; any failure (for example a driver without conditional nodes,
+// or without programmatic launches inside them, retried without) leaves the batched replay.
+void ready_loop_graphs(ccdgpu_handle *h) {
+  if (h->loop_state) return;
+  for (int attempt = 0; attempt < 2 && h->loop_state == 0; attempt++) {
+    t_pdl = attempt == 0;
+    int rc = capture_loop_graph(h, false, &h->loop64);
+    if (!rc && h->nt) rc = capture_loop_graph(h, true, &h->loop_tc);
+    if (!rc) {
+      h->loop_state = 1;
+    } else {
+      if (h->loop64) cudaGraphExecDestroy(h->loop64);
+      if (h->loop_tc) cudaGraphExecDestroy(h->loop_tc);
+      h->loop64 = h->loop_tc = nullptr;
+    }
+  }
+  t_pdl = true;
+  if (h->loop_state == 0) h->loop_state = -1;
+}
+
 // One table-path iteration: exactly the reference loop body.
 int tables_iteration(ccdgpu_handle *h, double mixing, double *corr) {
   int rc;
@@ -1044,6 +1137,7 @@ int ccdgpu_create(const ccdgpu_problem *prob, const ccdgpu_options *opt, ccdgpu_
   for (int i = 0; i < 10 && !rc; i++) rc = cuda_status(cudaEventCreate(&h->ev[i]));
   if (!rc) rc = build(h, prob);
   if (!rc) rc = set_ctl(h, 0, 0.0, 100, 0.5, true);
+  if (!rc) rc = ccdgpu_trace_arm(h, -1);
   if (rc) { release(h); delete h; return rc; }
   *out = h;
   return CCDGPU_OK;
@@ -1123,12 +1217,28 @@ int ccdgpu_solve(ccdgpu_handle *h, double tol, int64_t max_iters, double mixing,
   int rc = set_ctl(h, 1, tol, max_iters, mixing, true, -1, mixed ? 1 : 0);
   if (rc) return rc;
   const bool graph = fused && h->opt.use_graph && !h->profiling;
-  if (graph && (rc = fused_ready_graph(h, false))) return rc;
-  if (graph && mixed && (rc = fused_ready_graph(h, true))) return rc;
+  if (graph) ready_loop_graphs(h);
+  const bool device_loop = graph && h->loop_state == 1;
+  if (graph && !device_loop && (rc = fused_ready_graph(h, false))) return rc;
+  if (graph && !device_loop && mixed && (rc = fused_ready_graph(h, true))) return rc;
   auto t0 = std::chrono::steady_clock::now();
   int64_t launched = 0;
   const int64_t cap = max_iters + 1;
-  while (true) {
+  // Device loop: each launch runs up to kLoopChunk iterations without the host.
+  constexpr int64_t kLoopChunk = 128;
+  while (device_loop) {
+    Control &c = *h->h_ctl;
+    const int64_t it0 = c.iterations, pol0 = c.polish_iters;
+    c.stop_at = it0 + kLoopChunk;
+    CK(cudaMemcpyAsync(&h->ctl->stop_at, &c.stop_at, sizeof(int64_t), cudaMemcpyHostToDevice,
+                       h->s0));
+    CK(cudaGraphLaunch(mixed && c.phase == 1 ? h->loop_tc : h->loop64, h->s0));
+    if ((rc = sync_ctl(h))) return rc;
+    const int64_t fp = (c.polish_iters - pol0) + (mixed ? 0 : c.iterations - it0);
+    h->launches += (c.iterations - it0 - fp) * h->kernels_per_body_tc + fp * h->kernels_per_body64;
+    if (c.done || c.iterations >= cap || c.iterations == it0) break;
+  }
+  while (!device_loop) {
     // Iterations are launched in batches; once the device-side stop rule fires the remaining
     // launches of the batch return immediately.
     const int64_t batch =
@@ -1286,6 +1396,34 @@ int ccdgpu_enable_profiling(ccdgpu_handle *h, int32_t on) {
   return CCDGPU_OK;
 }
 void *ccdgpu_stream(ccdgpu_handle *h) { return h ? (void *)h->s0 : nullptr; }
+
+int ccdgpu_trace_arm(ccdgpu_handle *h, int64_t iteration) {
+  if (!h) return CCDGPU_ERR_INVALID_ARGUMENT;
+  CK(cudaSetDevice(h->opt.device));
+  int rc = sync_ctl(h);
+  if (rc) return rc;
+  Control &c = *h->h_ctl;
+  c.trace_iter = iteration;
+  for (int k = 0; k < kTraceKernels; k++) {
+    c.trace_first[k] = ~0ull;
+    c.trace_last[k] = 0;
+  }
+  CK(cudaMemcpyAsync(h->ctl, h->h_ctl, sizeof(Control), cudaMemcpyHostToDevice, h->s0));
+  CK(cudaStreamSynchronize(h->s0));
+  return CCDGPU_OK;
+}
+
+int ccdgpu_trace_read(ccdgpu_handle *h, uint64_t *first, uint64_t *last, int32_t n) {
+  if (!h || !first || !last || n < 0) return CCDGPU_ERR_INVALID_ARGUMENT;
+  CK(cudaSetDevice(h->opt.device));
+  int rc = sync_ctl(h);
+  if (rc) return rc;
+  for (int k = 0; k < n && k < kTraceKernels; k++) {
+    first[k] = h->h_ctl->trace_first[k];
+    last[k] = h->h_ctl->trace_last[k];
+  }
+  return CCDGPU_OK;
+}
 int ccdgpu_work_per_iteration(const ccdgpu_handle *h, double *flops, double *v_pppp_bytes,
                               double *ladder_flops) {
   if (!h) return CCDGPU_ERR_INVALID_ARGUMENT;

@@ -152,6 +152,27 @@ class CCDSolver:
         _check(_native.gpu_lib().ccdgpu_get_profile(self._h, ctypes.byref(p)), "profile")
         return {k: getattr(p, k) for k, _ in p._fields_}
 
+    TRACE_KERNELS = ["ring_small", "ring_mid", "ring_large", "hh_small", "hh_tiled", "onebody",
+                     "ladder_thin", "ladder_mid", "ladder_wide", "ladder_tc", "assemble",
+                     "loop_ctl", "energy"]
+
+    def trace_arm(self, iteration):
+        """Record kernel start times of iteration `iteration` of the next solve (-1 disarms)."""
+        _check(_native.gpu_lib().ccdgpu_trace_arm(self._h, int(iteration)), "ccdgpu_trace_arm")
+
+    def trace_read(self):
+        """{kernel: (first CTA start, last CTA start)} in ns, relative to the earliest start;
+        kernels that did not run in the traced iteration are left out."""
+        n = len(self.TRACE_KERNELS)
+        first = (ctypes.c_uint64 * n)()
+        last = (ctypes.c_uint64 * n)()
+        _check(_native.gpu_lib().ccdgpu_trace_read(self._h, first, last, n), "ccdgpu_trace_read")
+        ran = [k for k in range(n) if first[k] != 2**64 - 1]
+        if not ran:
+            return {}
+        t0 = min(first[k] for k in ran)
+        return {self.TRACE_KERNELS[k]: (first[k] - t0, last[k] - t0) for k in ran}
+
     def stream_ptr(self):
         """The handle's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
         return _native.gpu_lib().ccdgpu_stream(self._h)

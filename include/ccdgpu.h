@@ -225,6 +225,14 @@ void *ccdgpu_stream(ccdgpu_handle *h);
 int ccdgpu_work_per_iteration(const ccdgpu_handle *h, double *flops, double *ladder_bytes,
                               double *ladder_flops);
 
+/* Kernel start-time trace (diagnostics; no counterpart in the reference).  Arm with the index
+ * of an iteration of the next solve (-1 disarms); every kernel of that iteration then records
+ * the %globaltimer time (ns) at which its first and its last CTA started.  Kernel ids, in this
+ * order: ring small, ring mid, ring large, hh ladder small, hh ladder tiled, one-body, pp
+ * ladder thin, mid, wide, tensor-core pp ladder, assembly, loop control, energy (13). */
+int ccdgpu_trace_arm(ccdgpu_handle *h, int64_t iteration);
+int ccdgpu_trace_read(ccdgpu_handle *h, uint64_t *first, uint64_t *last, int32_t n);
+
 /* No counterpart in the reference.  The ladder term of one regular channel,
  * D = 0.5 T X + 0.5 V_pppp T with X = V_hhhh + 0.5 V_hhpp T (the arithmetic of
  * calcChannelT2Diff_pphh), for callers that cannot allocate device memory, such as a host
