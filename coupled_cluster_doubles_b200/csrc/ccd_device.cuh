@@ -57,9 +57,16 @@ constexpr int kTcGroup = 8 * kTcKC;          // bf16 elements of one 8-row group
 
 // Padded UMMA N for hh columns.
 __host__ __device__ inline int tc_nb(int hh) { return 16 * ((hh + 15) / 16); }
-// Offset of element (r, k) inside a chunk image (bf16 units), 0 <= k < kTcKC.
+// Offset of element (r, k) inside a chunk image (bf16 units), 0 <= k < kTcKC: K-major core
+// matrices (8 rows of 8 consecutive k), used for the A operands.
 __host__ __device__ inline int tc_off(int r, int k) {
   return (r >> 3) * kTcGroup + (k >> 3) * 64 + (r & 7) * 8 + (k & 7);
+}
+// The B operands (N = hh columns) in MN-major core matrices (8 k-rows of 8 consecutive n):
+// neighbouring columns are neighbouring bytes, as the assembly and hh ladder write them.  Same
+// 8 x 8 block positions as tc_off, so the shared-memory descriptors are the same.
+__host__ __device__ inline int tc_off_mn(int n, int k) {
+  return (n >> 3) * kTcGroup + (k >> 3) * 64 + (k & 7) * 8 + (n & 7);
 }
 // x -> nt bf16 terms, each the round-to-nearest of what the previous ones leave (the
 // remainders are exact in double).
@@ -125,7 +132,8 @@ struct ElemRange {
 // Kernel ids of the start-time trace (Control::trace_*).
 enum TraceKernel {
   kTrRingSmall = 0, kTrRingMid, kTrRingLarge, kTrHHSmall, kTrHHTiled, kTrOneBody, kTrLadderThin,
-  kTrLadderMid, kTrLadderWide, kTrLadderTC, kTrAssemble, kTrLoopCtl, kTrEnergy, kTraceKernels
+  kTrLadderMid, kTrLadderWide, kTrLadderTC, kTrAssemble, kTrLoopCtl, kTrEnergy, kTrRetile,
+  kTraceKernels
 };
 
 // Device control block: iteration state of the solve loop lives on the device so that a
@@ -143,7 +151,7 @@ struct Control {
   int32_t error;         // bit flags, see kErr*
   int32_t active;        // 1 while a solve is running (0: kernels run unconditionally)
   int32_t phase;         // mixed-precision solve: 1 = split-bf16 ladder, 2 = FP64 polish
-  int32_t pad;
+  int32_t retile;        // the FP64 ladder operand tiles are stale (a mixed iteration ran)
   double polish_rel;     // phase 1 -> 2 once |dE| <= max(tol, polish_rel * |E|)
   int64_t polish_iters;  // iterations run in phase 2
   int64_t stop_at;       // device solve loop: one graph launch runs while iterations < stop_at

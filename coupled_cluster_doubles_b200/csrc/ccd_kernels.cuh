@@ -354,6 +354,48 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict_
 }
 
 // ------------------------------------------------------------------------------------------
+// Register-tiled outer-product micro-GEMM for the small per-channel FP64 products:
+//   acc[i][j] += sum_k A[k*lda + r0 + i] * B[k*ldb + c0 + j],   i, j < TM.
+// Both operands are k-row major in shared memory, so a thread reads its TM-wide slices with
+// 16-byte loads (TM even: lda, ldb and r0, c0 even).  Slices may run past the valid rows or
+// columns (and past the last row into padding); those accumulators are never stored.
+// ------------------------------------------------------------------------------------------
+template <int TM>
+__device__ __forceinline__ void opgemm(const double *__restrict__ A, int lda,
+                                       const double *__restrict__ B, int ldb, int K, int r0,
+                                       int c0, double (&acc)[TM][TM]) {
+  const double *a = A + r0, *b = B + c0;
+#pragma unroll 2
+  for (int k = 0; k < K; ++k) {
+    double av[TM], bv[TM];
+    if constexpr (TM % 2 == 0) {
+#pragma unroll
+      for (int i = 0; i < TM / 2; ++i) {
+        const double2 x = *reinterpret_cast<const double2 *>(a + 2 * i);
+        const double2 y = *reinterpret_cast<const double2 *>(b + 2 * i);
+        av[2 * i] = x.x;
+        av[2 * i + 1] = x.y;
+        bv[2 * i] = y.x;
+        bv[2 * i + 1] = y.y;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < TM; ++i) {
+        av[i] = a[i];
+        bv[i] = b[i];
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TM; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+    a += lda;
+    b += ldb;
+  }
+}
+__host__ __device__ inline int even_up(int n) { return (n + 1) & ~1; }
+
+// ------------------------------------------------------------------------------------------
 // hh ladder intermediate, split into K slices of each channel:
 //   P = V_hhpp T (K = pp),  X = V_hhhh + 0.5 P  (reference layout, and X/2 as B tiles),
 //   s[IJ] = P[IJ][IJ]            (x_k = sum over IJ with first hole k, calc.cpp:82-84),
@@ -368,6 +410,7 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict_
 // ------------------------------------------------------------------------------------------
 constexpr int kHHThreads = 256;
 constexpr int kHHElems = 2560;  // V (and T) elements of one slice
+constexpr int kHHStagePad = 256 + 96;  // odd-hh row padding (<= 2560/17 rows) + slice overrun
 
 __host__ __device__ inline int hh_slice_rows(int hh) { return hh >= kHHElems ? 1 : kHHElems / hh; }
 
@@ -385,7 +428,7 @@ __device__ __forceinline__ void hh_finish(const ChanInfo &ch, int kl, int ij, do
     __nv_bfloat16 hv[3];
     split_bf16(0.5 * x, hv, nt);
     const int64_t o =
-        ch.xt_tc_base + (int64_t)(kl >> 5) * (ch.nbt >> 3) * kTcGroup + tc_off(ij, kl & 31);
+        ch.xt_tc_base + (int64_t)(kl >> 5) * (ch.nbt >> 3) * kTcGroup + tc_off_mn(ij, kl & 31);
     for (int q = 0; q < nt; ++q) xt_tc[q * xt_tc_stride + o] = hv[q];
   }
   if (kl == ij) s_out[ch.hh_off + ij] = p;
@@ -406,39 +449,25 @@ struct HHOut {
   }
 };
 
+// hh > 16: thread (tx, ty) owns P rows 2*TH*ty.. and columns 2*TH*tx.. (contiguous blocks of
+// TM = 2*TH); the slice is staged with an even row stride ld.
 template <int TM>
 __device__ __forceinline__ void hh_tiled(const double *Vs, const double *Ts, int rows, int hh,
-                                         const HHOut &out) {
+                                         int ld, const HHOut &out) {
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  int ci[TM], cj[TM];  // column offsets clamped into the row; lanes past hh are not stored
-#pragma unroll
-  for (int i = 0; i < TM; ++i) {
-    ci[i] = min(ty + 16 * i, hh - 1);
-    cj[i] = min(tx + 16 * i, hh - 1);
-  }
+  const int r0 = ty * TM, c0 = tx * TM;
+  if (r0 >= hh || c0 >= hh) return;
   double acc[TM][TM];
 #pragma unroll
   for (int i = 0; i < TM; ++i)
 #pragma unroll
     for (int j = 0; j < TM; ++j) acc[i][j] = 0.0;
-#pragma unroll 2
-  for (int k = 0; k < rows; ++k) {
-    double a[TM], b[TM];
-#pragma unroll
-    for (int i = 0; i < TM; ++i) {
-      a[i] = Vs[k * hh + ci[i]];
-      b[i] = Ts[k * hh + cj[i]];
-    }
-#pragma unroll
-    for (int i = 0; i < TM; ++i)
-#pragma unroll
-      for (int j = 0; j < TM; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-  }
+  opgemm<TM>(Vs, ld, Ts, ld, rows, r0, c0, acc);
 #pragma unroll
   for (int i = 0; i < TM; ++i)
 #pragma unroll
     for (int j = 0; j < TM; ++j) {
-      const int kl = ty + 16 * i, ij = tx + 16 * j;
+      const int kl = r0 + i, ij = c0 + j;
       if (kl < hh && ij < hh) out.emit(kl, ij, acc[i][j]);
     }
 }
@@ -453,22 +482,26 @@ hh_ladder_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ 
                  double *__restrict__ r_out, __nv_bfloat16 *__restrict__ xt_tc,
                  int64_t xt_tc_stride, int nt, const Control *ctl, int gate) {
   if (skip_iteration(ctl, gate, SMALL ? kTrHHSmall : kTrHHTiled)) return;
-  __shared__ __align__(16) double Vs[kHHElems], Ts[kHHElems];
+  // Even-stride staging: rows * even_up(hh) <= kHHElems + rows, plus room for slices that run
+  // past the last row.
+  __shared__ __align__(16) double Vs[kHHElems + kHHStagePad], Ts[kHHElems + kHHStagePad];
   __shared__ double red[kHHThreads];
   __shared__ int last;
   const HHTile tt = tiles[blockIdx.x];
   const ChanInfo ch = chans[tt.ch];
   const double *t_old = ctl->parity ? tbuf1 : tbuf0;
   const int hh = ch.hh, tid = threadIdx.x, rows = tt.rows, n = rows * hh;
+  const int ld = SMALL ? hh : even_up(hh);  // staged row stride (even for 16-byte loads)
   const double *vb = v_pphh + ch.t_off + (int64_t)tt.k0 * hh;
   const double *tb = t_old + ch.t_off + (int64_t)tt.k0 * hh;
   for (int e = tid; e < n; e += kHHThreads) {
-    Vs[e] = vb[e];
-    Ts[e] = tb[e];
+    const int r = e / hh, c = e - r * hh;
+    Vs[r * ld + c] = vb[e];
+    Ts[r * ld + c] = tb[e];
   }
   __syncthreads();
   for (int r = tid; r < rows; r += kHHThreads)
-    r_out[ch.pp_off + tt.k0 + r] = dot4(Vs + r * hh, 1, Ts + r * hh, 1, hh);
+    r_out[ch.pp_off + tt.k0 + r] = dot4(Vs + r * ld, 1, Ts + r * ld, 1, hh);
   const HHOut out{tt, ch, v_hhhh, part, x_ref, x_t, s_out, xt_tc, xt_tc_stride, nt};
   if (SMALL) {
     const int no = hh * hh, groups = kHHThreads / no;
@@ -484,12 +517,10 @@ hh_ladder_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ 
       out.emit(kl, ij, p);
     }
   } else {
-    switch ((hh + 15) / 16) {
-      case 2: hh_tiled<2>(Vs, Ts, rows, hh, out); break;
-      case 3: hh_tiled<3>(Vs, Ts, rows, hh, out); break;
-      case 4: hh_tiled<4>(Vs, Ts, rows, hh, out); break;
-      case 5: hh_tiled<5>(Vs, Ts, rows, hh, out); break;
-      default: break;
+    switch ((hh + 31) / 32) {  // blocks of TM = 2, 4, 6 cover 32, 64, 96 columns
+      case 1: hh_tiled<2>(Vs, Ts, rows, hh, ld, out); break;
+      case 2: hh_tiled<4>(Vs, Ts, rows, hh, ld, out); break;
+      default: hh_tiled<6>(Vs, Ts, rows, hh, ld, out); break;
     }
   }
   if (ch.nhht == 1) return;
@@ -510,28 +541,40 @@ hh_ladder_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ 
 }
 
 // ------------------------------------------------------------------------------------------
-// Ring term: Y = V_hphp + 0.5 V_hpph T', R = T' Y per modified channel.
-// Operand source and result layout:
-//   fused path (inv != null): T' is gathered from the pphh amplitudes, T'[p] = t[inv[p]], and
-//     R is scattered back to pphh order, out[inv[p]] = R[p] (inv = inverse of the ai_jb table),
-//     so the assembly reads R_ai,jb / R_aj,ib / R_bi,ja / R_bj,ia from the channel's own block;
-//   table path (inv == null): T' = t2Old_phhp and R = t2Diff_phhp in the phhp slab
-//     (calc.cpp:264-313), tbuf0 = tbuf1 = the slab.
-// Channels with ph', hp' <= kRingSmall run one per warp; larger ones one per CTA with register
-// tiles, in two classes (<= 32 and above) so each class has its own shared-memory size.
+// Ring term: Y = V_hphp + 0.5 V_hpph T', R = T' Y per modified channel (calc.cpp:264-313).
+// T' is read from the phhp slab (t2Old_phhp; the fused assembly keeps it current); V_hpph is
+// held transposed per channel (Vt[k][i] = V_hpph[i][k], k < ph', i < hp').  Result
+// layout: fused path (inv != null) scatters R into pphh order, out[inv[p]] = R[p] (inv =
+// inverse of the ai_jb table), so the assembly reads R_ai,jb / R_aj,ib / R_bi,ja / R_bj,ia from
+// the channel's own block; table path (inv == null) writes t2Diff_phhp, out[p] = R[p].
+// Channels with ph', hp' <= kRingSmall run one per warp; larger ones on resident CTAs that loop
+// over their channels with cp.async double buffering (the next channel's operands load while
+// the current one computes), in two classes (<= kRingMid and above) with their own shared
+// memory sizes.
 // ------------------------------------------------------------------------------------------
 constexpr int kRingThreads = 256;
 constexpr int kRingSmall = 16;
 constexpr int kRingMid = 32;
 
-__device__ __forceinline__ const double *ring_t(const Control *ctl, const int32_t *inv,
-                                                const double *tbuf0, const double *tbuf1) {
-  return (inv && ctl->parity) ? tbuf1 : tbuf0;
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 __global__ void __launch_bounds__(256)
 ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restrict__ v_hpph,
-                  const double *__restrict__ v_hphp, const double *tbuf0, const double *tbuf1,
+                  const double *__restrict__ v_hphp, const double *__restrict__ t_phhp,
                   const int32_t *__restrict__ inv, double *__restrict__ out, const Control *ctl,
                   int gate) {
   if (skip_iteration(ctl, gate, kTrRingSmall)) return;
@@ -540,18 +583,17 @@ ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restr
   const int mi = blockIdx.x * 8 + w;
   if (mi >= n) return;
   const ModInfo m = mods[mi];
-  const double *tsrc = ring_t(ctl, inv, tbuf0, tbuf1);
   const int ph = m.ph, hp = m.hp;
-  double *Ts = buf[w], *Va = Ts + ph * hp, *Ys = Va + hp * ph;
+  double *Ts = buf[w], *Vt = Ts + ph * hp, *Ys = Vt + hp * ph;
   for (int e = lane; e < ph * hp; e += 32) {
-    Ts[e] = tsrc[inv ? (int64_t)inv[m.m_off + e] : m.m_off + e];
-    Va[e] = v_hpph[m.m_off + e];
+    Ts[e] = t_phhp[m.m_off + e];
+    Vt[e] = v_hpph[m.m_off + e];
   }
   for (int e = lane; e < hp * hp; e += 32) Ys[e] = v_hphp[m.y_off + e];
   __syncwarp();
   for (int e = lane; e < hp * hp; e += 32) {
     const int i = e / hp, j = e - i * hp;
-    Ys[e] = 0.5 * dot4(Va + i * ph, 1, Ts + j, hp, ph) + Ys[e];
+    Ys[e] = 0.5 * dot4(Vt + i, hp, Ts + j, hp, ph) + Ys[e];
   }
   __syncwarp();
   for (int e = lane; e < ph * hp; e += 32) {
@@ -561,114 +603,122 @@ ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restr
   }
 }
 
-// Channels above kRingSmall: one CTA, 16 x 16 threads with a TM x TM register tile each
-// (rows ty + 16 i, columns tx + 16 j, TM = ceil(max(ph', hp') / 16)); operands in shared memory.
-template <int TM>
-__device__ __forceinline__ void ring_body(const ModInfo &m, const double *__restrict__ v_hpph,
-                                          const double *__restrict__ v_hphp,
-                                          const double *__restrict__ tsrc,
-                                          const int32_t *__restrict__ inv,
-                                          double *__restrict__ out, double *rs) {
-  const int ph = m.ph, hp = m.hp, tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  double *Ts = rs;             // ph x hp
-  double *Va = Ts + ph * hp;   // hp x ph
-  double *Ys = Va + hp * ph;   // hp x hp
-  for (int e = tid; e < ph * hp; e += kRingThreads) {
-    Ts[e] = tsrc[inv ? (int64_t)inv[m.m_off + e] : m.m_off + e];
-    Va[e] = v_hpph[m.m_off + e];
-  }
-  for (int e = tid; e < hp * hp; e += kRingThreads) Ys[e] = v_hphp[m.y_off + e];
-  __syncthreads();
-  // Y = V_hphp + 0.5 V_hpph T'   (hp x hp, K = ph)
-  int ri[TM], cj[TM];
-#pragma unroll
-  for (int i = 0; i < TM; ++i) {
-    ri[i] = min(ty + 16 * i, hp - 1);
-    cj[i] = min(tx + 16 * i, hp - 1);
-  }
-  double acc[TM][TM];
-#pragma unroll
-  for (int i = 0; i < TM; ++i)
-#pragma unroll
-    for (int j = 0; j < TM; ++j) acc[i][j] = 0.0;
-#pragma unroll 2
-  for (int k = 0; k < ph; ++k) {
-    double a[TM], b[TM];
-#pragma unroll
-    for (int i = 0; i < TM; ++i) {
-      a[i] = Va[ri[i] * ph + k];
-      b[i] = Ts[k * hp + cj[i]];
-    }
-#pragma unroll
-    for (int i = 0; i < TM; ++i)
-#pragma unroll
-      for (int j = 0; j < TM; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-  }
-  // Each Y element is read and written by the thread that owns it; Ts and Va stay intact.
-#pragma unroll
-  for (int i = 0; i < TM; ++i)
-#pragma unroll
-    for (int j = 0; j < TM; ++j) {
-      const int r = ty + 16 * i, c = tx + 16 * j;
-      if (r < hp && c < hp) Ys[r * hp + c] = 0.5 * acc[i][j] + Ys[r * hp + c];
-    }
-  __syncthreads();
-  // R = T' Y   (ph x hp, K = hp)
-#pragma unroll
-  for (int i = 0; i < TM; ++i) ri[i] = min(ty + 16 * i, ph - 1);
-#pragma unroll
-  for (int i = 0; i < TM; ++i)
-#pragma unroll
-    for (int j = 0; j < TM; ++j) acc[i][j] = 0.0;
-#pragma unroll 2
-  for (int k = 0; k < hp; ++k) {
-    double a[TM], b[TM];
-#pragma unroll
-    for (int i = 0; i < TM; ++i) {
-      a[i] = Ts[ri[i] * hp + k];
-      b[i] = Ys[k * hp + cj[i]];
-    }
-#pragma unroll
-    for (int i = 0; i < TM; ++i)
-#pragma unroll
-      for (int j = 0; j < TM; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-  }
-#pragma unroll
-  for (int i = 0; i < TM; ++i)
-#pragma unroll
-    for (int j = 0; j < TM; ++j) {
-      const int r = ty + 16 * i, c = tx + 16 * j;
-      if (r < ph && c < hp) {
-        const int64_t p = m.m_off + r * hp + c;
-        out[inv ? (int64_t)inv[p] : p] = acc[i][j];
-      }
-    }
+// Shared-memory stage of one channel, rows padded to even strides (ldh = even(hp'),
+// ldp = even(ph')): T' [ph'][ldh], T'^T [hp'][ldp], Vt [ph'][ldh], Y [hp'][ldh] (V_hphp on
+// arrival), the ph' x hp' scatter indices (int32, fused path), then padding for slices that run
+// past the last row.
+__host__ __device__ inline int ring_stage_doubles(int ph, int hp) {
+  const int ldh = even_up(hp), ldp = even_up(ph);
+  return even_up(2 * ph * ldh + hp * ldp + hp * ldh + (ph * hp + 1) / 2 + 16);  // 16-byte steps
 }
 
-// TMAX = 2: channels up to kRingMid; TMAX = 5: the rest (up to 80).
+// Thread (tx, ty) owns rows ty*TM.. and columns tx*TM.. of Y and of R.
+template <int TM>
+__device__ __forceinline__ void ring_compute(const ModInfo &m, double *st,
+                                             const int32_t *__restrict__ inv,
+                                             double *__restrict__ out) {
+  const int ph = m.ph, hp = m.hp, tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int ldh = even_up(hp), ldp = even_up(ph);
+  double *Ts = st, *TT = Ts + ph * ldh, *Vt = TT + hp * ldp, *Ys = Vt + ph * ldh;
+  const int32_t *Is = reinterpret_cast<const int32_t *>(Ys + hp * ldh);
+  // T'^T for the second product.
+  for (int e = tid; e < ph * hp; e += kRingThreads) {
+    const int i = e / hp, k = e - i * hp;
+    TT[k * ldp + i] = Ts[i * ldh + k];
+  }
+  const int r0 = ty * TM, c0 = tx * TM;
+  double acc[TM][TM];
+  // Y = V_hphp + 0.5 V_hpph T'   (hp x hp, K = ph)
+  if (r0 < hp && c0 < hp) {
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TM; ++j) acc[i][j] = 0.0;
+    opgemm<TM>(Vt, ldh, Ts, ldh, ph, r0, c0, acc);
+    // Each Y element is read and written by the thread that owns it.
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TM; ++j)
+        if (r0 + i < hp && c0 + j < hp)
+          Ys[(r0 + i) * ldh + c0 + j] = 0.5 * acc[i][j] + Ys[(r0 + i) * ldh + c0 + j];
+  }
+  __syncthreads();
+  // R = T' Y   (ph x hp, K = hp)
+  if (r0 < ph && c0 < hp) {
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TM; ++j) acc[i][j] = 0.0;
+    opgemm<TM>(TT, ldp, Ys, ldh, hp, r0, c0, acc);
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TM; ++j) {
+        const int r = r0 + i, c = c0 + j;
+        if (r < ph && c < hp) {
+          const int p = r * hp + c;
+          out[inv ? (int64_t)Is[p] : m.m_off + p] = acc[i][j];
+        }
+      }
+  }
+}
+
+// Resident CTAs: CTA b handles channels b, b + gridDim.x, ...  stage = doubles per buffer;
+// nbuf = 2 (prefetch the next channel) or 1 (largest channels, when two stages do not fit).
+// TMAX = 2: channels up to kRingMid; TMAX = 6: the rest (up to 96).
 template <int TMAX>
-__global__ void __launch_bounds__(kRingThreads, TMAX <= 2 ? 4 : 2)
-ring_kernel(const ModInfo *__restrict__ mods, const double *__restrict__ v_hpph,
-            const double *__restrict__ v_hphp, const double *tbuf0, const double *tbuf1,
-            const int32_t *__restrict__ inv, double *__restrict__ out, const Control *ctl,
-            int gate) {
+__global__ void __launch_bounds__(kRingThreads, TMAX <= 2 ? 3 : 1)
+ring_kernel(const ModInfo *__restrict__ mods, int n, const double *__restrict__ v_hpph,
+            const double *__restrict__ v_hphp, const double *__restrict__ t_phhp,
+            const int32_t *__restrict__ inv, double *__restrict__ out, int stage, int nbuf,
+            const Control *ctl, int gate) {
   if (skip_iteration(ctl, gate, TMAX <= 2 ? kTrRingMid : kTrRingLarge)) return;
   extern __shared__ __align__(16) double rs[];
-  const ModInfo m = mods[blockIdx.x];
-  const double *tsrc = ring_t(ctl, inv, tbuf0, tbuf1);
-  const int tm = (max(m.ph, m.hp) + 15) / 16;
-  if (TMAX <= 2) {
-    if (tm <= 1) ring_body<1>(m, v_hpph, v_hphp, tsrc, inv, out, rs);
-    else ring_body<2>(m, v_hpph, v_hphp, tsrc, inv, out, rs);
-  } else {
-    switch (tm) {
-      case 1: case 2: ring_body<2>(m, v_hpph, v_hphp, tsrc, inv, out, rs); break;
-      case 3: ring_body<3>(m, v_hpph, v_hphp, tsrc, inv, out, rs); break;
-      case 4: ring_body<4>(m, v_hpph, v_hphp, tsrc, inv, out, rs); break;
-      case 5: ring_body<5>(m, v_hpph, v_hphp, tsrc, inv, out, rs); break;
-      default: break;
+  const int tid = threadIdx.x;
+  auto issue = [&](int ci, double *st) {
+    const ModInfo m = mods[ci];
+    const int ph = m.ph, hp = m.hp, ldh = even_up(hp), ldp = even_up(ph);
+    double *Ts = st, *Vt = Ts + ph * ldh + hp * ldp, *Ys = Vt + ph * ldh;
+    int32_t *Is = reinterpret_cast<int32_t *>(Ys + hp * ldh);
+    for (int e = tid; e < ph * hp; e += kRingThreads) {
+      const int r = e / hp, c = e - r * hp;
+      cp_async8(Ts + r * ldh + c, t_phhp + m.m_off + e);
+      cp_async8(Vt + r * ldh + c, v_hpph + m.m_off + e);
+      if (inv) cp_async4(Is + e, inv + m.m_off + e);
+    }
+    for (int e = tid; e < hp * hp; e += kRingThreads) {
+      const int r = e / hp, c = e - r * hp;
+      cp_async8(Ys + r * ldh + c, v_hphp + m.y_off + e);
+    }
+  };
+  int ci = blockIdx.x;
+  if (ci < n) issue(ci, rs);
+  cp_async_commit();
+  for (int k = 0; ci < n; ++k, ci += gridDim.x) {
+    double *st = rs + (nbuf == 2 ? (k & 1) * stage : 0);
+    const int nxt = ci + gridDim.x;
+    if (nbuf == 2 && nxt < n) issue(nxt, rs + ((k + 1) & 1) * stage);
+    cp_async_commit();
+    if (nbuf == 2) cp_async_wait<1>();
+    else cp_async_wait<0>();
+    __syncthreads();
+    const ModInfo m = mods[ci];
+    const int tmb = (max(m.ph, m.hp) + 31) / 32;  // 32-wide blocks: TM = 2, 4, 6
+    if (TMAX <= 2) {
+      ring_compute<2>(m, st, inv, out);
+    } else {
+      if (tmb <= 1) ring_compute<2>(m, st, inv, out);
+      else if (tmb == 2) ring_compute<4>(m, st, inv, out);
+      else ring_compute<6>(m, st, inv, out);
+    }
+    __syncthreads();
+    if (nbuf == 1 && nxt < n) {
+      issue(nxt, rs);
+      cp_async_commit();
     }
   }
+  cp_async_wait<0>();
 }
 
 // Deterministic block reduction (fixed tree) of one double; result valid in thread 0.
@@ -781,7 +831,7 @@ __device__ __forceinline__ void write_t_tiles_tc(const ChanInfo &ch,
   split_bf16(t, hv, nt);
   if (q.x >= 0) {
     const int64_t o =
-        ch.tkt_tc_base + (int64_t)(q.x >> 5) * (ch.nbt >> 3) * kTcGroup + tc_off(ij, q.x & 31);
+        ch.tkt_tc_base + (int64_t)(q.x >> 5) * (ch.nbt >> 3) * kTcGroup + tc_off_mn(ij, q.x & 31);
     for (int p = 0; p < nt; ++p) tkt_tc[p * tkt_stride + o] = hv[p];
   }
   if (q.y >= 0) {
@@ -799,20 +849,26 @@ __device__ __forceinline__ void write_t_tiles_tc(const ChanInfo &ch,
 //         + 0.5 x_i t_ab,ji - 0.5 x_j t_ab,ij                       (h2pp_h1 gathers, algebraically)
 //         + (-0.5 y_b) t_ab,ij - (-0.5 y_a) t_ba,ij                 (p2_p1hh gathers, algebraically)
 //   t_new = mixing value/(e_i+e_j-e_a-e_b) + (1-mixing) t_old;  E += V t_new
-// and the next iteration's ladder operand tiles are written in the same pass.  The fused path
-// keeps no phhp slab: the ring reads T' from the amplitudes directly (ring kernels).
+// and the next iteration's operands are written in the same pass: t_new into the phhp slab
+// (mapToDistributed ai_jb, a scattered write) and into the ladder operand tiles.
 // ------------------------------------------------------------------------------------------
 constexpr int kAsmThreads = 256;
 constexpr int kAsmPerThread = 2;  // elements per thread; a CTA covers one ElemRange
 __device__ __forceinline__ void energy_reduce(const double *epart, int n, Control *ctl, int flags,
                                               double *e_out);
 
+// In a mixed iteration (nt > 0) the assembly writes only the bf16 ladder operand images;
+// retile_kernel rebuilds the FP64 tiles if FP64 iterations follow.
 // Work is organised over packed elements (u, j): packed row u (a <= b) of a channel and column
-// j, numbered q = u * hh + j per channel, kAsmPerCTA of them per CTA (ElemRange over q).  A
-// thread computes element (ab, j) and its mirror (ba, j) together: both need t and R at
-// (ab,j), (ab,ji), (ba,j), (ba,ji), which the thread reads once; the column-swapped reads fall
-// in the same rows as their neighbours' direct reads, so each array streams once.
+// j.  A CTA owns whole packed rows [u0, u1) of one channel (ElemRange over q = u * hh + j, row
+// aligned, about kAsmPerCTA elements) and first stages the small tables of those rows and of
+// the channel's columns in shared memory (row offsets of ab and ba, y_a, y_b, e_a, e_b; column
+// swap j -> ji, x_i, x_j, e_i + e_j), so that every element then needs a single round of
+// independent global loads.  A thread computes element (ab, j) and its mirror (ba, j)
+// together: both need t and R at (ab,j), (ab,ji), (ba,j), (ba,ji), read once.
 constexpr int kAsmPerCTA = 2 * kAsmThreads;
+constexpr int kAsmMaxRows = kAsmPerCTA;  // rows of a CTA (hh >= 1)
+constexpr int kAsmMaxCols = 96;
 
 // value of one element (calc.cpp:384-418) of row r with mirror row m (m = r for a = b):
 //   V + D + R_ai,jb - R_aj,ib - R_bi,ja + R_bj,ia + 0.5 x_i t_ab,ji - 0.5 x_j t_ab,ij
@@ -835,13 +891,24 @@ __device__ __forceinline__ double asm_value(double v, double dm, double r_j, dou
   return mixing * value + (1. - mixing) * t_j;
 }
 
+struct AsmRowInfo {
+  int32_t o_ab, o_ba;  // row offsets inside the channel block (ab * hh, ba * hh)
+  int32_t ab, mirrored;
+  double ya, yb, ea, eb;
+};
+struct AsmColInfo {
+  int32_t js, pad;
+  double xi, xj, eij;
+};
+
 __global__ void __launch_bounds__(kAsmThreads, 3)
 assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__restrict__ chans,
                       const int2 *__restrict__ pp_pairs, const int2 *__restrict__ hh_pairs,
                       const int32_t *__restrict__ hh_swap, const int32_t *__restrict__ rowmap,
                       const int32_t *__restrict__ mirror, const int2 *__restrict__ pk_idx,
                       const double *__restrict__ v_pphh, const double *__restrict__ dmat,
-                      const double *__restrict__ d_ring, const double *__restrict__ xh,
+                      const double *__restrict__ d_ring, const int32_t *__restrict__ g_ai_jb,
+                      double *__restrict__ old_phhp, const double *__restrict__ xh,
                       const double *__restrict__ yp, const double *__restrict__ eps, int np,
                       double *tbuf0, double *tbuf1, double *__restrict__ t_kt,
                       double *__restrict__ t_mt, double *__restrict__ epart, int32_t *ticket,
@@ -849,6 +916,8 @@ assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__r
                       __nv_bfloat16 *__restrict__ tmt_tc, int64_t tmt_tc_stride, int nt,
                       int gate) {
   if (skip_iteration(ctl, gate, kTrAssemble)) return;
+  __shared__ AsmRowInfo rows[kAsmMaxRows];
+  __shared__ AsmColInfo cols[kAsmMaxCols];
   __shared__ double scratch[32];
   __shared__ int last;
   const ElemRange rg = pranges[blockIdx.x];
@@ -857,40 +926,65 @@ assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__r
   double *__restrict__ t_new = ctl->parity ? tbuf0 : tbuf1;
   const double mixing = ctl->mixing;
   const int hh = ch.hh;
+  const int u0 = (int)(rg.e0 / hh), nrows = (int)(rg.e1 / hh) - u0;
+  for (int r = threadIdx.x; r < nrows; r += kAsmThreads) {
+    const int ab = rowmap[ch.row_off + u0 + r], mi = mirror[ch.row_off + u0 + r];
+    const int2 pab = pp_pairs[ch.pp_off + ab];
+    AsmRowInfo ri;
+    ri.ab = ab;
+    ri.mirrored = mi >= 0;
+    ri.o_ab = ab * hh;
+    ri.o_ba = (mi >= 0 ? mi : ab) * hh;
+    ri.ya = yp[pab.x - np];
+    ri.yb = yp[pab.y - np];
+    ri.ea = eps[pab.x];
+    ri.eb = eps[pab.y];
+    rows[r] = ri;
+  }
+  for (int j = threadIdx.x; j < hh; j += kAsmThreads) {
+    const int2 pij = hh_pairs[ch.hh_off + j];
+    AsmColInfo ci;
+    ci.js = hh_swap[ch.hh_off + j];
+    ci.pad = 0;
+    ci.xi = xh[pij.x];
+    ci.xj = xh[pij.y];
+    ci.eij = eps[pij.x] + eps[pij.y];
+    cols[j] = ci;
+  }
+  __syncthreads();
+  const double *tb = t_old + ch.t_off, *rb = d_ring + ch.t_off, *vb = v_pphh + ch.t_off;
+  const double *db = dmat + ch.t_off;
+  const int32_t *gb = g_ai_jb + ch.t_off;
+  double *nb = t_new + ch.t_off;
+  const int n = nrows * hh;
   double corr = 0.0;
 #pragma unroll 2
-  for (int64_t q = rg.e0 + threadIdx.x; q < rg.e1; q += kAsmThreads) {
-    const int u = (int)(q / hh), j = (int)(q - (int64_t)u * hh);
-    const int ab = rowmap[ch.row_off + u], mi = mirror[ch.row_off + u];
-    const int ba = mi >= 0 ? mi : ab;
-    const int js = hh_swap[ch.hh_off + j];
-    const int2 pij = hh_pairs[ch.hh_off + j];
-    const int2 pab = pp_pairs[ch.pp_off + ab];
-    const int64_t o_ab = ch.t_off + (int64_t)ab * hh, o_ba = ch.t_off + (int64_t)ba * hh;
-    const double t_abj = t_old[o_ab + j], t_abs = t_old[o_ab + js];
-    const double t_baj = t_old[o_ba + j], t_bas = t_old[o_ba + js];
-    const double r_abj = d_ring[o_ab + j], r_abs = d_ring[o_ab + js];
-    const double r_baj = d_ring[o_ba + j], r_bas = d_ring[o_ba + js];
-    const double v1 = v_pphh[o_ab + j], d1 = dmat[o_ab + j];
-    const double xi = xh[pij.x], xj = xh[pij.y];
-    const double ya = yp[pab.x - np], yb = yp[pab.y - np];
-    const double ei = eps[pij.x], ej = eps[pij.y], ea = eps[pab.x], eb = eps[pab.y];
-    const double t1 = asm_value(v1, d1, r_abj, r_abs, r_baj, r_bas, t_abj, t_abs, t_baj, xi, xj,
-                                ya, yb, ei + ej - ea - eb, mixing);
-    t_new[o_ab + j] = t1;
-    write_t_tiles(ch, pk_idx, ab, j, t1, t_kt, t_mt);
-    if (nt) write_t_tiles_tc(ch, pk_idx, ab, j, t1, nt, tkt_tc, tkt_tc_stride, tmt_tc,
+  for (int q = threadIdx.x; q < n; q += kAsmThreads) {
+    const int r = q / hh, j = q - r * hh;
+    const AsmRowInfo ri = rows[r];
+    const AsmColInfo ci = cols[j];
+    const int a1 = ri.o_ab + j, as = ri.o_ab + ci.js, b1 = ri.o_ba + j, bs = ri.o_ba + ci.js;
+    const double t_abj = tb[a1], t_abs = tb[as], t_baj = tb[b1], t_bas = tb[bs];
+    const double r_abj = rb[a1], r_abs = rb[as], r_baj = rb[b1], r_bas = rb[bs];
+    const double v1 = vb[a1], d1 = db[a1], v2 = vb[b1], d2 = db[b1];
+    const int32_t g1 = gb[a1], g2 = gb[b1];
+    const double t1 = asm_value(v1, d1, r_abj, r_abs, r_baj, r_bas, t_abj, t_abs, t_baj, ci.xi,
+                                ci.xj, ri.ya, ri.yb, ci.eij - ri.ea - ri.eb, mixing);
+    nb[a1] = t1;
+    old_phhp[g1] = t1;
+    if (nt) write_t_tiles_tc(ch, pk_idx, ri.ab, j, t1, nt, tkt_tc, tkt_tc_stride, tmt_tc,
                              tmt_tc_stride);
+    else write_t_tiles(ch, pk_idx, ri.ab, j, t1, t_kt, t_mt);
     corr += v1 * t1;
-    if (mi >= 0) {
+    if (ri.mirrored) {
       // Row ba: the same formula with a and b exchanged.
-      const double v2 = v_pphh[o_ba + j], d2 = dmat[o_ba + j];
-      const double t2 = asm_value(v2, d2, r_baj, r_bas, r_abj, r_abs, t_baj, t_bas, t_abj, xi, xj,
-                                  yb, ya, ei + ej - eb - ea, mixing);
-      t_new[o_ba + j] = t2;
-      write_t_tiles(ch, pk_idx, ba, j, t2, t_kt, t_mt);
-      if (nt) write_t_tiles_tc(ch, pk_idx, ba, j, t2, nt, tkt_tc, tkt_tc_stride, tmt_tc,
+      const double t2 = asm_value(v2, d2, r_baj, r_bas, r_abj, r_abs, t_baj, t_bas, t_abj, ci.xi,
+                                  ci.xj, ri.yb, ri.ya, ci.eij - ri.eb - ri.ea, mixing);
+      nb[b1] = t2;
+      old_phhp[g2] = t2;
+      if (nt) write_t_tiles_tc(ch, pk_idx, ri.o_ba / hh, j, t2, nt, tkt_tc, tkt_tc_stride, tmt_tc,
                                tmt_tc_stride);
+      else write_t_tiles(ch, pk_idx, ri.o_ba / hh, j, t2, t_kt, t_mt);
       corr += v2 * t2;
     }
   }
@@ -905,7 +999,34 @@ assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__r
   if (!last) return;
   __threadfence();
   energy_reduce(epart, gridDim.x, ctl, 3, nullptr);
-  if (threadIdx.x == 0) *ticket = 0;
+  if (threadIdx.x == 0) {
+    *ticket = 0;
+    if (nt) ctl->retile = 1;  // the FP64 ladder tiles were not written this iteration
+  }
+}
+
+// Rebuilds the FP64 ladder operand tiles from the current amplitudes after mixed iterations
+// (they write only the bf16 images); a no-op unless ctl->retile is set.  First kernel of every
+// FP64 iteration of the fused path and of the FP64 ladder stage.
+__global__ void __launch_bounds__(256)
+retile_kernel(const ElemRange *__restrict__ ranges, const ChanInfo *__restrict__ chans,
+              const int2 *__restrict__ pk_idx, const double *tbuf0, const double *tbuf1,
+              double *__restrict__ t_kt, double *__restrict__ t_mt, Control *ctl, int gate) {
+  if (skip_iteration(ctl, gate, kTrRetile) || !ctl->retile) return;
+  const ElemRange rg = ranges[blockIdx.x];
+  const ChanInfo ch = chans[rg.ch];
+  const double *t = ctl->parity ? tbuf1 : tbuf0;
+  for (int64_t e = rg.e0 + threadIdx.x; e < rg.e1; e += blockDim.x) {
+    const int64_t loc = e - ch.t_off;
+    const int ab = (int)(loc / ch.hh), ij = (int)(loc - (int64_t)ab * ch.hh);
+    write_t_tiles(ch, pk_idx, ab, ij, t[e], t_kt, t_mt);
+  }
+}
+
+// Clears the retile flag once every retile CTA has read it (single thread, after retile).
+__global__ void retile_done_kernel(Control *ctl) {
+  pdl_enter();
+  if (threadIdx.x == 0) ctl->retile = 0;
 }
 
 // Table path assembly: exactly calcChannelT2_pphh over the eight gathered chains.

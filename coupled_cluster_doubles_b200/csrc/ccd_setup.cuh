@@ -108,6 +108,17 @@ __global__ void convert_tables_kernel(const ElemRange *__restrict__ ranges, cons
   }
 }
 
+// V_hpph' blocks (hp' x ph', load.cpp:275-296) -> transposed (ph' x hp') for the ring kernels'
+// outer-product loops; one CTA per modified channel.
+__global__ void transpose_hpph_kernel(const ModInfo *__restrict__ mods,
+                                      const double *__restrict__ raw, double *__restrict__ out) {
+  const ModInfo m = mods[blockIdx.x];
+  for (int e = threadIdx.x; e < m.ph * m.hp; e += blockDim.x) {
+    const int i = e / m.ph, k = e - i * m.ph;
+    out[m.m_off + (int64_t)k * m.hp + i] = raw[m.m_off + e];
+  }
+}
+
 // Fused-path ring tables.  inv[ai_jb(e)] = e turns the phhp slab position of every amplitude
 // back into its pphh element, so the ring can read T' from the amplitudes and write R in pphh
 // order.  The other three ring maps of loadMaps are ai_jb composed with the swaps i<->j and

@@ -11,12 +11,13 @@
 // iterations (the fixed point does not depend on how D was rounded on the way).
 //
 // Operand images.  A 128-row x 32-deep K chunk of one term is stored in HBM exactly as the
-// tensor core reads it from shared memory: the K-major, non-swizzled canonical layout made of
-// 8 x 8 "core matrices" (8 rows of 16 bytes, 128 contiguous bytes):
+// tensor core reads it from shared memory: non-swizzled canonical layouts made of 8 x 8 "core
+// matrices" (128 contiguous bytes), K-major for A (V, and T rows for T X):
 //   element (r, k) of a chunk -> (r / 8) * 256 + (k / 8) * 64 + (r % 8) * 8 + k % 8   (bf16)
-// (tc_off in ccd_device.cuh), so one 1-D bulk copy per term moves a stage, and the smem
-// descriptors use LBO = 128 bytes (next core matrix along K) and SBO = 512 bytes (next 8-row
-// group).  The last row tile of a channel is compact (only its ceil(rows/8) row groups are
+// and MN-major for B (T for V T, X/2): element (n, k) -> (n / 8) * 256 + (k / 8) * 64 +
+// (k % 8) * 8 + n % 8 (tc_off / tc_off_mn in ccd_device.cuh).  One 1-D bulk copy per term moves
+// a stage, and both smem descriptors use LBO = 128 bytes (next core matrix along K) and
+// SBO = 512 bytes (next 8-row / 8-column group).  The last row tile of a channel is compact (only its ceil(rows/8) row groups are
 // stored); the rows beyond it in shared memory are stale and only reach accumulator rows that
 // the epilogue never reads.  K padding is zero in both operands.
 //
@@ -52,9 +53,9 @@ __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
   return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) |
          ((uint64_t)(512 >> 4) << 32) | (1ull << 46);
 }
-// Instruction descriptor: bf16 x bf16 -> f32, both K-major, M = 128, N = n.
+// Instruction descriptor: bf16 x bf16 -> f32, A K-major, B MN-major (bit 16), M = 128, N = n.
 __host__ __device__ constexpr uint32_t tc_idesc(int n) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+  return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) | ((uint32_t)(n >> 3) << 17) |
          ((uint32_t)(kTcBM >> 4) << 24);
 }
 __device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t adesc, uint64_t bdesc,

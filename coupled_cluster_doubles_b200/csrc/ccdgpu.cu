@@ -50,6 +50,8 @@ struct ccdgpu_handle {
   int n_cls[3] = {0, 0, 0};  // pp-ladder tiles per column class (thin, mid, wide), in that order
   size_t ladder_smem_thin = 0;
   size_t ladder_smem = 0, ring_smem = 0, ring_smem_mid = 0, hh_smem = 0;
+  int ring_stage_mid = 0, ring_stage_large = 0, ring_nbuf_large = 2;
+  int ring_grid_mid = 0, ring_grid_large = 0;
   bool have_3body = false;
   std::vector<DevBuf> allocs;
 
@@ -97,6 +99,7 @@ struct ccdgpu_handle {
   int nt = 0;
   int n_tc_tiles = 0;
   LadderTile *tc_tiles = nullptr;
+  int32_t *kcol = nullptr;  // pp index of the w-th c<d pair of each channel (pk_off + w)
   int32_t *tc_counters = nullptr;
   double *tc_part = nullptr;
   __nv_bfloat16 *v_tc = nullptr, *tkt_tc = nullptr, *tmt_tc = nullptr, *xt_tc = nullptr;
@@ -358,19 +361,30 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     y_tot += hp * hp;
     src_hpph.push_back(P->v_hpph_mod[c]); cnt_hpph.push_back(ph * hp);
     src_hphp.push_back(P->v_hphp_mod[c]); cnt_hphp.push_back(hp * hp);
-    const size_t smem = (size_t)(2 * ph * hp + hp * hp) * 8;
+    const int stage = ring_stage_doubles((int)ph, (int)hp);
     if (ph <= kRingSmall && hp <= kRingSmall) {
       mods.push_back(m);
     } else if (ph <= kRingMid && hp <= kRingMid) {
-      h->ring_smem_mid = std::max(h->ring_smem_mid, smem);
+      h->ring_stage_mid = std::max(h->ring_stage_mid, stage);
       mods_mid.push_back(m);
     } else {
-      ring_smem = std::max(ring_smem, smem);
+      h->ring_stage_large = std::max(h->ring_stage_large, stage);
       mods_big.push_back(m);
     }
   }
+  // Resident ring CTAs stride over their class: largest channels first for balance.
+  auto by_work = [](const ModInfo &x, const ModInfo &y) {
+    return (int64_t)x.ph * x.hp * x.hp > (int64_t)y.ph * y.hp * y.hp;
+  };
+  std::stable_sort(mods_mid.begin(), mods_mid.end(), by_work);
+  std::stable_sort(mods_big.begin(), mods_big.end(), by_work);
   h->n_mod_small = (int)mods.size();
   h->n_mod_mid = (int)mods_mid.size();
+  h->ring_smem_mid = (size_t)2 * h->ring_stage_mid * 8;
+  h->ring_nbuf_large = (size_t)2 * h->ring_stage_large * 8 <= 200 * 1024 ? 2 : 1;
+  ring_smem = (size_t)h->ring_nbuf_large * h->ring_stage_large * 8;
+  h->ring_grid_mid = (int)std::min<int64_t>(h->n_mod_mid, 3 * 148);
+  h->ring_grid_large = (int)std::min<int64_t>((int64_t)mods_big.size(), 148);
   mods.insert(mods.end(), mods_mid.begin(), mods_mid.end());
   mods.insert(mods.end(), mods_big.begin(), mods_big.end());
   h->n_mod = (int)mods.size();
@@ -475,6 +489,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     });
   }
   h->n_tc_tiles = (int)tc_tiles.size();
+
   std::vector<ElemRange> ranges;
   const int64_t per = (int64_t)kAsmThreads * kAsmPerThread;
   for (int ai = 0; ai < h->n_act; ai++) {
@@ -483,11 +498,13 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     for (int64_t e = 0; e < n; e += per) ranges.push_back({ai, 0, a.t_off + e, a.t_off + std::min(n, e + per)});
   }
   h->n_ranges = (int)ranges.size();
+  // Fused assembly: row-aligned ranges of packed elements, about kAsmPerCTA per CTA.
   std::vector<ElemRange> pranges;
   for (int ai = 0; ai < h->n_act; ai++) {
-    const int64_t n = (int64_t)chans[ai].pr * chans[ai].hh;
-    for (int64_t q = 0; q < n; q += kAsmPerCTA)
-      pranges.push_back({ai, 0, q, std::min<int64_t>(n, q + kAsmPerCTA)});
+    const int hh = chans[ai].hh, pr = chans[ai].pr;
+    const int rows = std::max(1, std::min(kAsmMaxRows, kAsmPerCTA / hh));
+    for (int u = 0; u < pr; u += rows)
+      pranges.push_back({ai, 0, (int64_t)u * hh, (int64_t)std::min(pr, u + rows) * hh});
   }
   h->n_asm_blocks = (int)pranges.size();
 
@@ -536,6 +553,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   ar.add(&h->x, x_tot); ar.add(&h->x_t, xt); ar.add(&h->t_kt, tkt); ar.add(&h->t_mt, tmt);
   ar.add(&h->s, hh_tot); ar.add(&h->r, pp_tot); ar.add(&h->xh, np); ar.add(&h->yp, h->npart);
   ar.add(&h->pranges, pranges.size());
+  ar.add(&h->kcol, kcol.size());  // V tiling at create
   ar.add(&h->epart, std::max(h->n_ranges, h->n_asm_blocks)); ar.add(&h->ctl, 1); ar.add(&h->e_out, 1); ar.add(&h->err, 1);
   ar.add(&h->ticket, 1);
   if (h->nt) {
@@ -558,14 +576,13 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   TRY(ar.commit(h));
   // Scratch for the raw inputs, released at the end of create.
   Arena sc;
-  double *vraw = nullptr, *hhpp_raw = nullptr;
+  double *vraw = nullptr, *hhpp_raw = nullptr, *hpph_raw = nullptr;
   RawIndex *raw_idx = nullptr;
   int32_t *counts = nullptr;
   int2 *d_vrows = nullptr, *d_mod_dims = nullptr;
-  int32_t *d_kcol = nullptr;
   int64_t *d_vraw_off = nullptr, *d_o_m = nullptr;
-  sc.add(&vraw, vraw_tot); sc.add(&hhpp_raw, n_t); sc.add(&raw_idx, (size_t)8 * n_t);
-  sc.add(&counts, (size_t)5 * n_t); sc.add(&d_vrows, vrows.size()); sc.add(&d_kcol, kcol.size());
+  sc.add(&vraw, vraw_tot); sc.add(&hhpp_raw, n_t); sc.add(&hpph_raw, h->n_m); sc.add(&raw_idx, (size_t)8 * n_t);
+  sc.add(&counts, (size_t)5 * n_t); sc.add(&d_vrows, vrows.size()); 
   sc.add(&d_vraw_off, vraw_off.size()); sc.add(&d_mod_dims, mod_dims.size()); sc.add(&d_o_m, o_m.size());
   const size_t n_allocs = h->allocs.size();
   TRY(sc.commit(h));
@@ -576,13 +593,16 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   };
   TRY(put(h->chans, chans)); TRY(put(h->mods, mods)); TRY(put(h->tiles, tiles));
   TRY(put(h->hh_tiles, hh_tiles)); TRY(put(h->ranges, ranges)); TRY(put(h->pranges, pranges));
-  if (h->nt) TRY(put(h->tc_tiles, tc_tiles));
+  if (h->nt) {
+    TRY(put(h->tc_tiles, tc_tiles));
+  }
+  TRY(put(h->kcol, kcol));
   TRY(put(h->pp_pairs, pp_pairs)); TRY(put(h->hh_pairs, hh_pairs));
   TRY(put(h->pp_swap, pp_swap)); TRY(put(h->hh_swap, hh_swap));
   TRY(put(h->list_off, list_off)); TRY(put(h->list, list));
   TRY(put(h->rowmap, rowmap)); TRY(put(h->mirror, mirror)); TRY(put(h->pk_idx, pk_idx));
   TRY(put(h->o_h, o_h)); TRY(put(h->o_p, o_p));
-  TRY(put(d_vrows, vrows)); TRY(put(d_kcol, kcol)); TRY(put(d_vraw_off, vraw_off));
+  TRY(put(d_vrows, vrows)); TRY(put(d_vraw_off, vraw_off));
   TRY(put(d_mod_dims, mod_dims)); TRY(put(d_o_m, o_m));
   CK(cudaMemcpyAsync(h->eps, P->sp_energy, nsp * 8, cudaMemcpyHostToDevice, h->s0));
 
@@ -611,7 +631,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     static_assert(sizeof(RawIndex) == sizeof(ccdgpu_chain_index), "ChainIndex layout");
     for (int k = 0; k < 8; k++)
       TRY(upload_runs(h, reinterpret_cast<ccdgpu_chain_index *>(raw_idx) + (size_t)k * n_t, sm[k], nm));
-    TRY(upload_runs(h, h->v_hpph, src_hpph, cnt_hpph));
+    TRY(upload_runs(h, hpph_raw, src_hpph, cnt_hpph));
     TRY(upload_runs(h, h->v_hphp, src_hphp, cnt_hphp));
     if (h->have_3body) {
       std::vector<const double *> s5, s6;
@@ -631,6 +651,10 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     }
   }
   // Device layout transforms.
+  if (h->n_mod) {
+    transpose_hpph_kernel<<<h->n_mod, 256, 0, h->s0>>>(h->mods, hpph_raw, h->v_hpph);
+    CK(cudaGetLastError());
+  }
   if (h->n_ranges) {
     transpose_hhpp_kernel<<<h->n_ranges, 256, 0, h->s0>>>(h->ranges, h->chans, hhpp_raw, h->v_pphh);
     CK(cudaGetLastError());
@@ -646,12 +670,12 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     CK(cudaGetLastError());
   }
   if (!vrows.empty()) {
-    tile_v_kernel<<<(unsigned)vrows.size(), 128, 0, h->s0>>>(h->chans, d_vrows, h->rowmap, d_kcol,
+    tile_v_kernel<<<(unsigned)vrows.size(), 128, 0, h->s0>>>(h->chans, d_vrows, h->rowmap, h->kcol,
                                                              d_vraw_off, vraw, h->v_t);
     CK(cudaGetLastError());
     if (h->nt) {
       tile_v_tc_kernel<<<(unsigned)vrows.size(), 128, 0, h->s0>>>(
-          h->chans, d_vrows, h->rowmap, d_kcol, d_vraw_off, vraw, h->v_tc, h->n_vtc, h->nt);
+          h->chans, d_vrows, h->rowmap, h->kcol, d_vraw_off, vraw, h->v_tc, h->n_vtc, h->nt);
       CK(cudaGetLastError());
     }
   }
@@ -684,7 +708,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   h->hh_smem = 0;  // static shared memory only
   CK(cudaFuncSetAttribute(ring_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)std::max<size_t>(h->ring_smem_mid, 16)));
-  CK(cudaFuncSetAttribute(ring_kernel<5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  CK(cudaFuncSetAttribute(ring_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)std::max<size_t>(h->ring_smem, 16)));
   if (h->nt) {
     h->tc_smem = tc_smem_bytes(h->nt);
@@ -756,6 +780,14 @@ int launch_pp_ladder_tc(ccdgpu_handle *h, cudaStream_t st) {
 // The three column classes run concurrently: mid and wide go to stream s2 (wide first, they
 // are the longest tiles), thin to `st`; s2 is joined back into `st` before returning.
 int launch_pp_ladder(ccdgpu_handle *h, cudaStream_t st) {
+  if (h->nt && h->n_ranges) {
+    // A mixed handle's FP64 ladder first refreshes its operand tiles if mixed iterations ran.
+    CK(launch_pdl(retile_kernel, h->n_ranges, 256, 0, st, (const ElemRange *)h->ranges,
+                  (const ChanInfo *)h->chans, (const int2 *)h->pk_idx, (const double *)h->t[0],
+                  (const double *)h->t[1], h->t_kt, h->t_mt, h->ctl, 0));
+    CK(launch_pdl(retile_done_kernel, 1, 32, 0, st, h->ctl));
+    h->launches += 2;
+  }
   const LadderTile *t_thin = h->tiles, *t_mid = h->tiles + h->n_cls[0];
   const LadderTile *t_wide = t_mid + h->n_cls[1];
   const bool side = h->n_cls[1] || h->n_cls[2];
@@ -788,29 +820,29 @@ int launch_pp_ladder(ccdgpu_handle *h, cudaStream_t st) {
   return CCDGPU_OK;
 }
 
-// fused: the fused path's layout (T' gathered from the amplitudes, R in pphh order); else the
-// table path's phhp slabs (t2Old_phhp -> t2Diff_phhp).
+// T' from the phhp slab in both paths.  fused: R scattered into pphh order for the fused
+// assembly; else the table path's t2Diff_phhp slab.
 int launch_ring(ccdgpu_handle *h, cudaStream_t st, int gate, bool fused) {
   const int32_t *inv = fused ? h->inv4 : nullptr;
-  const double *t0 = fused ? h->t[0] : h->old_phhp, *t1 = fused ? h->t[1] : h->old_phhp;
   double *out = fused ? h->d_ring : h->r_phhp;
   if (h->n_mod_small) {
     ring_small_kernel<<<(int)ceil_div(h->n_mod_small, 8), 256, 0, st>>>(
-        h->mods, h->n_mod_small, h->v_hpph, h->v_hphp, t0, t1, inv, out, h->ctl, gate);
+        h->mods, h->n_mod_small, h->v_hpph, h->v_hphp, h->old_phhp, inv, out, h->ctl, gate);
     h->launches++;
     CK(cudaGetLastError());
   }
   if (h->n_mod_mid) {
-    ring_kernel<2><<<h->n_mod_mid, kRingThreads, std::max<size_t>(h->ring_smem_mid, 16), st>>>(
-        h->mods + h->n_mod_small, h->v_hpph, h->v_hphp, t0, t1, inv, out, h->ctl, gate);
+    ring_kernel<2><<<h->ring_grid_mid, kRingThreads, h->ring_smem_mid, st>>>(
+        h->mods + h->n_mod_small, h->n_mod_mid, h->v_hpph, h->v_hphp, h->old_phhp, inv, out,
+        h->ring_stage_mid, 2, h->ctl, gate);
     h->launches++;
     CK(cudaGetLastError());
   }
   const int nbig = h->n_mod - h->n_mod_small - h->n_mod_mid;
   if (nbig) {
-    ring_kernel<5><<<nbig, kRingThreads, std::max<size_t>(h->ring_smem, 16), st>>>(
-        h->mods + h->n_mod_small + h->n_mod_mid, h->v_hpph, h->v_hphp, t0, t1, inv, out, h->ctl,
-        gate);
+    ring_kernel<6><<<h->ring_grid_large, kRingThreads, h->ring_smem, st>>>(
+        h->mods + h->n_mod_small + h->n_mod_mid, nbig, h->v_hpph, h->v_hphp, h->old_phhp, inv,
+        out, h->ring_stage_large, h->ring_nbuf_large, h->ctl, gate);
     h->launches++;
     CK(cudaGetLastError());
   }
@@ -830,7 +862,8 @@ int launch_assemble_fused(ccdgpu_handle *h, cudaStream_t st, int gate) {
   return cuda_status(launch_pdl(
       assemble_fused_kernel, h->n_asm_blocks, kAsmThreads, 0, st, h->pranges, h->chans,
       h->pp_pairs, h->hh_pairs, h->hh_swap, h->rowmap, h->mirror, h->pk_idx, h->v_pphh, h->dmat,
-      h->d_ring, h->xh, h->yp, h->eps, (int)h->np, h->t[0], h->t[1], h->t_kt, h->t_mt, h->epart,
+      h->d_ring, h->flat + 4 * h->n_t, h->old_phhp, h->xh, h->yp, h->eps, (int)h->np, h->t[0],
+      h->t[1], h->t_kt, h->t_mt, h->epart,
       h->ticket, h->ctl, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc, gate ? h->nt : 0, gate));
 }
 int launch_energy(ccdgpu_handle *h, cudaStream_t st, int flags) {

@@ -229,7 +229,8 @@ int ccdgpu_work_per_iteration(const ccdgpu_handle *h, double *flops, double *lad
  * of an iteration of the next solve (-1 disarms); every kernel of that iteration then records
  * the %globaltimer time (ns) at which its first and its last CTA started.  Kernel ids, in this
  * order: ring small, ring mid, ring large, hh ladder small, hh ladder tiled, one-body, pp
- * ladder thin, mid, wide, tensor-core pp ladder, assembly, loop control, energy (13). */
+ * ladder thin, mid, wide, tensor-core pp ladder, assembly, loop control, energy, FP64 tile
+ * refresh (14). */
 int ccdgpu_trace_arm(ccdgpu_handle *h, int64_t iteration);
 int ccdgpu_trace_read(ccdgpu_handle *h, uint64_t *first, uint64_t *last, int32_t n);
 
