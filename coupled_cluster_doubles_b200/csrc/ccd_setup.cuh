@@ -5,6 +5,7 @@
 #include <cstdint>
 
 #include "ccd_device.cuh"
+#include "ccdgpu.h"
 
 namespace ccd {
 
@@ -62,6 +63,103 @@ __global__ void tile_v_tc_kernel(const ChanInfo *__restrict__ chans, const int2 
     split_bf16(src[kcol[ch.pk_off + w]], hv, nt);
     const int64_t o = tb + (int64_t)(w >> 5) * rg * kTcGroup + tc_off(r, w & 31);
     for (int p = 0; p < nt; ++p) v_tc[p * stride + o] = hv[p];
+  }
+}
+
+// ---- V_pppp generated on the device from the model (CCDGPU_V_ON_THE_FLY) ----------------
+// The antisymmetrised <ab|v|cd> of SPBasis::calcTBME, evaluated for every packed element of the
+// pp ladder (rows a <= b, columns c < d) and written straight into its operand images, so the
+// host never builds or uploads V_pppp.
+struct ModelDev {
+  int32_t kind, stride;
+  const int32_t *qn;   // [n_sp * stride] quantum numbers (SPBasis::indexMap)
+  // Electron gas: direct Coulomb term by momentum transfer n_a - n_c in [-R, R]^3,
+  // vq[((dx + R) * W + dy + R) * W + dz + R], W = 2R + 1, built on the host with the reference's
+  // own expression (ElectronGasSPBasis.cpp:424-448), so generated elements are bit-identical.
+  const double *vq;
+  int32_t R, W;
+  double g;            // pairing strength
+  double Lb;           // PNM box length, (N / rho)^(1/3)
+};
+
+__device__ __forceinline__ double direct_pnm_dev(const int32_t *qi, const int32_t *qj,
+                                                 const int32_t *qk, const int32_t *ql,
+                                                 double Lb) {
+  // InfMatterSPBasis.cpp:361-437 (Minnesota), same expression order; exp from CUDA, so the
+  // element may differ from the reference's by an ulp.
+  const double v0r = 200, v0t = 178, v0s = 91.85;
+  const double kr = 1.487, kt = 0.639, ks = 0.465;
+  double q2 = 0.;
+  for (int i = 0; i < 3; i++) {
+    const double ki = 2 * M_PI * qi[i] / Lb, kj = 2 * M_PI * qj[i] / Lb;
+    const double kk = 2 * M_PI * qk[i] / Lb, kl = 2 * M_PI * ql[i] / Lb;
+    const double bra = __dmul_rn(0.5, ki - kj), ket = __dmul_rn(0.5, kk - kl);
+    const double tr = bra - ket;
+    q2 = __dadd_rn(q2, __dmul_rn(tr, tr));
+  }
+  const double L3 = Lb * Lb * Lb;
+  const double vr = v0r / L3 * pow(M_PI / kr, 1.5) * exp(-q2 / (4 * kr));
+  const double vt = -v0t / L3 * pow(M_PI / kt, 1.5) * exp(-q2 / (4 * kt));
+  const double vs = -v0s / L3 * pow(M_PI / ks, 1.5) * exp(-q2 / (4 * ks));
+  const double spin_ex = (qi[3] == ql[3] && qj[3] == qk[3]) ? 1 : 0;
+  const double iso_ex = (qi[4] == ql[4] && qj[4] == qk[4]) ? 1 : 0;
+  const int d_s = (qi[3] == qk[3]) * (qj[3] == ql[3]);
+  const int d_t = (qi[4] == qk[4]) * (qj[4] == ql[4]);
+  const double is_it = d_s * d_t, ps_it = spin_ex * d_t, ps_pt = spin_ex * iso_ex;
+  const double is_pt = d_s * iso_ex;
+  return 0.5 * (vr + 0.5 * vt + 0.5 * vs) * is_it + 0.25 * (vt - vs) * ps_it -
+         0.5 * (vr + 0.5 * vt + 0.5 * vs) * ps_pt - 0.25 * (vt - vs) * is_pt;
+}
+
+// <ab|v|cd> for orbitals a, b, c, d of one regular channel (momentum is conserved).
+__device__ __forceinline__ double tbme_dev(const ModelDev &m, int a, int b, int c, int d) {
+  const int32_t *qa = m.qn + (int64_t)a * m.stride, *qb = m.qn + (int64_t)b * m.stride;
+  const int32_t *qc = m.qn + (int64_t)c * m.stride, *qd = m.qn + (int64_t)d * m.stride;
+  if (m.kind == CCDGPU_MODEL_PAIRING) {  // PairingSPBasis.cpp:127-141
+    double vout = 0.;
+    if (qa[0] == qb[0] && qc[0] == qd[0] && qa[1] == -qb[1] && -qc[1] == qd[1]) {
+      vout = -0.5 * m.g;
+      if (qa[1] == -qc[1]) vout = -vout;
+    }
+    return vout;
+  }
+  if (m.kind == CCDGPU_MODEL_ELECTRON_GAS) {  // direct - exchange, spin diagonal
+    auto vq = [&](const int32_t *x, const int32_t *y) {
+      return m.vq[((x[0] - y[0] + m.R) * m.W + (x[1] - y[1] + m.R)) * m.W + (x[2] - y[2] + m.R)];
+    };
+    const double dir = (qa[3] == qc[3] && qb[3] == qd[3]) ? vq(qa, qc) : 0.;
+    const double exc = (qa[3] == qd[3] && qb[3] == qc[3]) ? vq(qa, qd) : 0.;
+    return dir - exc;
+  }
+  return direct_pnm_dev(qa, qb, qc, qd, m.Lb) - direct_pnm_dev(qa, qb, qd, qc, m.Lb);
+}
+
+// One CTA per packed row u of a channel (items as for tile_v_kernel): the FP64 ladder tile
+// element and, for a mixed handle (nt > 0), its nt bf16 terms.
+__global__ void gen_v_kernel(const ChanInfo *__restrict__ chans, const int2 *__restrict__ items,
+                             const int32_t *__restrict__ rowmap, const int32_t *__restrict__ kcol,
+                             const int2 *__restrict__ pp_pairs, ModelDev m,
+                             double *__restrict__ v_t, __nv_bfloat16 *__restrict__ v_tc,
+                             int64_t tc_stride, int nt) {
+  const int2 it = items[blockIdx.x];
+  const ChanInfo ch = chans[it.x];
+  const int u = it.y;
+  const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + u]];
+  const int mt = u / ch.bm, rows = min(ch.bm, ch.pr - mt * ch.bm);
+  const int64_t tb = ch.vkt_base + (int64_t)mt * ch.bm * ch.nkc * kBK;
+  const int mtc = u >> 7, r = u & 127;
+  const int rg = (min(kTcBM, ch.pr - mtc * kTcBM) + 7) >> 3;
+  const int64_t tbc = ch.vtc_base + (int64_t)mtc * kTcBM * ch.nkct * kTcKC;
+  for (int w = threadIdx.x; w < ch.pk; w += blockDim.x) {
+    const int2 cd = pp_pairs[ch.pp_off + kcol[ch.pk_off + w]];
+    const double v = tbme_dev(m, ab.x, ab.y, cd.x, cd.y);
+    v_t[tb + (int64_t)(w / kBK) * rows * kBK + swzA(u - mt * ch.bm, w % kBK)] = v;
+    if (nt) {
+      __nv_bfloat16 hv[3];
+      split_bf16(v, hv, nt);
+      const int64_t o = tbc + (int64_t)(w >> 5) * rg * kTcGroup + tc_off(r, w & 31);
+      for (int p = 0; p < nt; ++p) v_tc[p * tc_stride + o] = hv[p];
+    }
   }
 }
 

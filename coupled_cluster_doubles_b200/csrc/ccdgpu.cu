@@ -222,9 +222,15 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   const uint64_t nch = P->n_channels, nsp = P->n_sp, np = P->n_particles;
   h->nch = nch; h->nsp = nsp; h->np = np; h->npart = nsp - np;
   const ccdgpu_channel_dims *D = P->chan_dims, *MD = P->chan_mod_dims;
+  // V_ON_THE_FLY: V_pppp is generated on the device from the model, P->v_pppp is not read.
   const bool on_the_fly = h->opt.v_mode == CCDGPU_V_ON_THE_FLY;
-  if (on_the_fly) return CCDGPU_ERR_UNSUPPORTED;  // generated V_pppp: not built yet
-  if (!P->v_pppp || !P->v_hhpp || !P->v_hhhh || !P->v_hpph_mod || !P->v_hphp_mod)
+  const ccdgpu_model *M = P->model;
+  if (on_the_fly && (!M || !M->qn || M->kind < CCDGPU_MODEL_PAIRING ||
+                     M->kind > CCDGPU_MODEL_ELECTRON_GAS ||
+                     M->qn_stride < (M->kind == CCDGPU_MODEL_PAIRING ? 2 : 5)))
+    return CCDGPU_ERR_INVALID_ARGUMENT;
+  if ((!on_the_fly && !P->v_pppp) || !P->v_hhpp || !P->v_hhhh || !P->v_hpph_mod ||
+      !P->v_hphp_mod)
     return CCDGPU_ERR_INVALID_ARGUMENT;
   for (int k = 0; k < 8; k++)
     if (!P->maps[k]) return CCDGPU_ERR_INVALID_ARGUMENT;
@@ -320,7 +326,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     vt += (int64_t)ci.nkc * ci.pr * kBK;
     part_tot += (int64_t)ci.nhht * hh * hh;
     vraw_off.push_back(vraw_tot);
-    vraw_tot += pp * pp;
+    if (!on_the_fly) vraw_tot += pp * pp;
     maxhh = std::max<int>(maxhh, (int)hh);
     const int hrows = hh_slice_rows((int)hh);
     for (int t = 0; t < ci.nhht; t++)
@@ -584,8 +590,52 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   sc.add(&vraw, vraw_tot); sc.add(&hhpp_raw, n_t); sc.add(&hpph_raw, h->n_m); sc.add(&raw_idx, (size_t)8 * n_t);
   sc.add(&counts, (size_t)5 * n_t); sc.add(&d_vrows, vrows.size()); 
   sc.add(&d_vraw_off, vraw_off.size()); sc.add(&d_mod_dims, mod_dims.size()); sc.add(&d_o_m, o_m.size());
+  // On-the-fly V: quantum numbers and (electron gas) the direct Coulomb term by momentum
+  // transfer, computed here with the reference's expression (ElectronGasSPBasis.cpp:424-448).
+  ModelDev md{};
+  std::vector<double> vq;
+  int32_t *d_qn = nullptr;
+  double *d_vq = nullptr;
+  if (on_the_fly) {
+    md.kind = M->kind;
+    md.stride = M->qn_stride;
+    md.g = M->params[0];
+    md.Lb = M->params[0];
+    if (M->kind == CCDGPU_MODEL_ELECTRON_GAS) {
+      int nmax = 0;
+      for (uint64_t o = 0; o < nsp; o++)
+        for (int i = 0; i < 3; i++) nmax = std::max(nmax, std::abs(M->qn[o * M->qn_stride + i]));
+      md.R = 2 * nmax;
+      md.W = 2 * md.R + 1;
+      const double L = M->params[0], e_sq = M->params[1];
+      vq.assign((size_t)md.W * md.W * md.W, 0.0);
+      for (int dx = -md.R; dx <= md.R; dx++)
+        for (int dy = -md.R; dy <= md.R; dy++)
+          for (int dz = -md.R; dz <= md.R; dz++) {
+            const int d[3] = {dx, dy, dz};
+            const double prefactor = e_sq / (L * L * L);
+            double rel = 0.0, mu = 0.0;
+            for (int i = 0; i < 3; i++) {
+              const double term = 2 * M_PI * d[i] / L;
+              rel += term * term;
+            }
+            const double v = rel < 1.e-5 ? 0.0 : prefactor * 4 * M_PI / (rel + mu * mu);
+            vq[((size_t)(dx + md.R) * md.W + (dy + md.R)) * md.W + (dz + md.R)] = v;
+          }
+    }
+    sc.add(&d_qn, (size_t)nsp * M->qn_stride);
+    sc.add(&d_vq, vq.size());
+  }
   const size_t n_allocs = h->allocs.size();
   TRY(sc.commit(h));
+  if (on_the_fly) {
+    CK(cudaMemcpyAsync(d_qn, M->qn, (size_t)nsp * M->qn_stride * sizeof(int32_t),
+                       cudaMemcpyHostToDevice, h->s0));
+    if (!vq.empty())
+      CK(cudaMemcpyAsync(d_vq, vq.data(), vq.size() * 8, cudaMemcpyHostToDevice, h->s0));
+    md.qn = d_qn;
+    md.vq = d_vq;
+  }
 
   auto put = [&](auto *dst, const auto &v) -> int {
     if (!v.empty()) CK(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice, h->s0));
@@ -615,8 +665,9 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     for (size_t ai = 0; ai < chans.size(); ai++) {
       const uint64_t c = act_chan[ai];
       const ChanInfo &a = chans[ai];
-      if (!P->v_pppp[c] || !P->v_hhpp[c] || !P->v_hhhh[c]) return CCDGPU_ERR_INVALID_ARGUMENT;
-      sp.push_back(P->v_pppp[c]); np2.push_back((int64_t)a.pp * a.pp);
+      if ((!on_the_fly && !P->v_pppp[c]) || !P->v_hhpp[c] || !P->v_hhhh[c])
+        return CCDGPU_ERR_INVALID_ARGUMENT;
+      if (!on_the_fly) { sp.push_back(P->v_pppp[c]); np2.push_back((int64_t)a.pp * a.pp); }
       sx.push_back(P->v_hhpp[c]); nx.push_back((int64_t)a.pp * a.hh);
       sh.push_back(P->v_hhhh[c]); nh.push_back((int64_t)a.hh * a.hh);
       for (int k = 0; k < 8; k++) {
@@ -670,10 +721,16 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     CK(cudaGetLastError());
   }
   if (!vrows.empty()) {
-    tile_v_kernel<<<(unsigned)vrows.size(), 128, 0, h->s0>>>(h->chans, d_vrows, h->rowmap, h->kcol,
-                                                             d_vraw_off, vraw, h->v_t);
+    if (on_the_fly) {
+      gen_v_kernel<<<(unsigned)vrows.size(), 128, 0, h->s0>>>(h->chans, d_vrows, h->rowmap,
+                                                              h->kcol, h->pp_pairs, md, h->v_t,
+                                                              h->v_tc, h->n_vtc, h->nt);
+    } else {
+      tile_v_kernel<<<(unsigned)vrows.size(), 128, 0, h->s0>>>(h->chans, d_vrows, h->rowmap,
+                                                               h->kcol, d_vraw_off, vraw, h->v_t);
+    }
     CK(cudaGetLastError());
-    if (h->nt) {
+    if (h->nt && !on_the_fly) {
       tile_v_tc_kernel<<<(unsigned)vrows.size(), 128, 0, h->s0>>>(
           h->chans, d_vrows, h->rowmap, h->kcol, d_vraw_off, vraw, h->v_tc, h->n_vtc, h->nt);
       CK(cudaGetLastError());
