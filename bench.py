@@ -38,6 +38,9 @@ CONFIGS = {
     "eg54c36": ("3D electron gas, N=54, r_s=2.0, |n|^2<=36 (1850 spin-orbitals)", "electron_gas",
                 dict(r_s=2.0, n_shells=32, n_particle_shells=4),
                 ["--electronGas", "-r", "2.0", "-s", "32", "-p", "4"], 1e-12),
+    "eg54c36r05": ("3D electron gas, N=54, r_s=0.5, |n|^2<=36 (1850 spin-orbitals)",
+                   "electron_gas", dict(r_s=0.5, n_shells=32, n_particle_shells=4),
+                   ["--electronGas", "-r", "0.5", "-s", "32", "-p", "4"], 1e-12),
     "pnm66": ("pure neutron matter, N=66, rho=0.08 fm^-3, |n|^2<=36 (1850 spin-orbitals)",
               "inf_matter", dict(density=0.08, tz_max=1, n_shells=32, n_particle_shells=5),
               ["--infMatter", "-d", "0.08", "-z", "1", "-s", "32", "-p", "5"], 1e-12),
@@ -179,11 +182,14 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="eg14", choices=list(CONFIGS))
+    ap.add_argument("--config", default="eg14", choices=list(CONFIGS) + ["batch24"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--path", default="fused", choices=["fused", "tables"])
     ap.add_argument("--precision", default="mixed", choices=list(PRECISIONS),
                     help="headline arm; the other precision is timed beside it")
+    ap.add_argument("--v-mode", default="stored", choices=["stored", "on_the_fly"],
+                    help="on_the_fly: V_pppp generated on the device from the model (the host "
+                         "builds and uploads none)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--single-arm", action="store_true",
                     help="time only the headline precision (for profiler launch lists)")
@@ -192,6 +198,9 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference_arm(args)
+        return
+    if args.config == "batch24":
+        run_batch(args)
         return
 
     import numpy as np
@@ -205,14 +214,15 @@ def main():
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     desc, kind, params, cli, _ = CONFIGS[args.config]
-    system = getattr(System, kind)(**params)
+    system = getattr(System, kind)(**params, load_v_pppp=args.v_mode == "stored")
     n_part = system.n_particles
     tol = stop_tol(n_part)
     if args.path == "tables" and args.precision == "mixed":
         args.precision = "fp64"  # the table path is FP64 only
     arms = [args.precision] + ([p for p in PRECISIONS if p != args.precision]
                                if args.path == "fused" and not args.single_arm else [])
-    solvers = {a: CCDSolver(system, device=local, path=args.path, precision=PRECISIONS[a])
+    solvers = {a: CCDSolver(system, device=local, path=args.path, precision=PRECISIONS[a],
+                            v_mode=args.v_mode)
                for a in arms}
     stream = {a: torch.cuda.ExternalStream(solvers[a].stream_ptr(), device=local) for a in arms}
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
@@ -220,7 +230,8 @@ def main():
     # Fully converged FP64 energy (untimed) for the |dE/N| check.
     e_conv = float("nan")
     if not args.single_arm:
-        ref_solver = solvers.get("fp64") or CCDSolver(system, device=local, path=args.path)
+        ref_solver = solvers.get("fp64") or CCDSolver(system, device=local, path=args.path,
+                                                      v_mode=args.v_mode)
         ref_solver.reset()
         e_conv = ref_solver.solve(tol=1e-12, max_iters=100, mixing=0.5).e_corr
 
@@ -288,10 +299,11 @@ def main():
     # + solve + T2 read-back.
     host_t2 = np.empty(n_t2)
     e2e_secs, e2e_iters = 0.0, 0
-    h2d = _problem_bytes(system)
+    h2d = _problem_bytes(system, with_v_pppp=args.v_mode == "stored")
     for k in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        s2 = CCDSolver(system, device=local, path=args.path, precision=PRECISIONS[arms[0]])
+        s2 = CCDSolver(system, device=local, path=args.path, precision=PRECISIONS[arms[0]],
+                       v_mode=args.v_mode)
         r2 = s2.solve(tol=tol, max_iters=100, mixing=0.5)
         s2.t2(host_t2)
         s2.close()
@@ -360,6 +372,8 @@ def main():
                       if head == "mixed" else "f64"),
             "data": "synthetic",
             "config": {"workload": desc, "precision": PRECISIONS[head], "path": args.path,
+                       "v_pppp": ("generated on the device from the model"
+                                  if args.v_mode == "on_the_fly" else "uploaded from the host"),
                        "stop_rule": f"|dE| <= 1e-8 N = {tol:g} (guarantees |dE/N| <= 1e-7)",
                        "iterations_per_solve": t["iters_per_solve"],
                        "polish_iterations_per_solve": t["polish_per_solve"],
@@ -392,7 +406,106 @@ def main():
         torch.distributed.destroy_process_group()
 
 
-def _problem_bytes(system):
+BATCH_SEED = 20261203
+
+
+def batch_specs():
+    """The batched electron-gas sweep: N in {14, 38, 54} x r_s in {0.5, 1, 2, 3, 4, 5, 6, 8},
+    each with a cutoff |n|^2 in {16, 20, 24} (n_shells 15 / 19 / 22) drawn from a fixed seed."""
+    import numpy as np
+    rng = np.random.default_rng(BATCH_SEED)
+    return [dict(r_s=rs, n_shells=int(rng.choice([15, 19, 22])), n_particle_shells=p)
+            for p in (2, 3, 4) for rs in (0.5, 1.0, 2.0, 3.0, 4.0, 5.0, 6.0, 8.0)]
+
+
+def run_batch(args):
+    """Config 4: 24 independent systems solved together (ccdgpu_solve_batch), mixed precision
+    with V_pppp generated on the device; timed against the same 24 solved one after another.
+    value = systems solved per second; each system stops at |dE| <= 1e-8 N."""
+    import numpy as np
+    import torch
+
+    from coupled_cluster_doubles_b200 import CCDSolver, System, solve_batch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    specs = batch_specs()
+    systems = [System.electron_gas(**sp, load_v_pppp=False) for sp in specs]
+    ns = [s.n_particles for s in systems]
+    tol = min(stop_tol(n) for n in ns)  # one stop threshold for the batch: the strictest
+    mixed = [CCDSolver(s, device=local, precision="mixed_bf16", v_mode="on_the_fly") for s in systems]
+    ref = [CCDSolver(s, device=local, v_mode="on_the_fly") for s in systems]
+    # Low-density members of the sweep do not converge under the reference's iteration (capped
+    # at 101 iterations or diverging to non-finite amplitudes); they are run and counted, and
+    # errors are compared on the systems that converge in both precisions.
+    e_conv = [r.e_corr for r in solve_batch(ref, tol=1e-12, check=False)]
+    streams = [torch.cuda.ExternalStream(m.stream_ptr(), device=local) for m in mixed]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    def timed(run):
+        for m in mixed:
+            m.reset()
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e0.record(streams[0])
+        res = run()
+        ends = []
+        for st in streams:
+            e1 = torch.cuda.Event(enable_timing=True)
+            e1.record(st)
+            ends.append(e1)
+        torch.cuda.synchronize()
+        return max(e0.elapsed_time(e1) for e1 in ends), res
+
+    for _ in range(args.warmup):
+        timed(lambda: solve_batch(mixed, tol=tol, check=False))
+    batch_ms, seq_ms, res = [], [], None
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            ms, res = timed(lambda: solve_batch(mixed, tol=tol, check=False))
+            batch_ms.append(ms)
+        for _ in range(args.steps):
+            ms, _ = timed(lambda: [solve_batch([m], tol=tol, check=False) for m in mixed])
+            seq_ms.append(ms)
+    b_ms = sum(batch_ms) / len(batch_ms)
+    s_ms = sum(seq_ms) / len(seq_ms)
+    import math
+    iters = sum(r.iterations for r in res)
+    status = ["diverged" if not math.isfinite(r.e_corr) else
+              ("converged" if r.converged else "capped") for r in res]
+    de = [abs(r.e_corr - e) / n for r, e, n, st in zip(res, e_conv, ns, status)
+          if st == "converged" and math.isfinite(e)]
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": len(systems) / (b_ms / 1000.0), "unit": "systems/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": b_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 2-term split operands, f32 accumulate (pp ladder) + f64",
+            "data": "synthetic",
+            "config": {"workload": "24 electron-gas systems, N in {14,38,54} x r_s in "
+                                   "{0.5,1,2,3,4,5,6,8}, cutoff |n|^2 in {16,20,24} drawn with "
+                                   f"numpy default_rng({BATCH_SEED})",
+                       "systems": [dict(sp, N=n, status=st, iterations=r.iterations)
+                                   for sp, n, st, r in zip(specs, ns, status, res)],
+                       "converged": status.count("converged"), "capped": status.count("capped"),
+                       "diverged": status.count("diverged"),
+                       "precision": "mixed_bf16", "v_pppp": "generated on the device",
+                       "stop_rule": f"|dE| <= {tol:g}", "iterations_total": iters,
+                       "iter_per_s": iters / (b_ms / 1000.0),
+                       "sequential_ms": s_ms, "batch_speedup_vs_sequential": s_ms / b_ms,
+                       "max_abs_de_per_particle_vs_fp64_converged": max(de) if de else None,
+                       "l2": "flushed (256 MiB write) before every step"},
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line))
+    for m in mixed + ref:
+        m.close()
+    for s in systems:
+        s.close()
+
+
+def _problem_bytes(system, with_v_pppp=True):
     """Bytes ccdgpu_create copies host -> device for this system: V blocks in their reference
     layouts (V_pppp, V_hhpp, V_hhhh of amplitude-carrying channels, both modified-channel V,
     the three-body V), the eight ChainIndex tables (24 bytes per entry), the energies and the
@@ -406,7 +519,8 @@ def _problem_bytes(system):
     hp = md[:, 2].astype(np.int64)
     ph = md[:, 3].astype(np.int64)
     n_t = int((pp * hh).sum())
-    v = 8 * int((pp * pp).sum() + n_t + (hh * hh).sum() + (ph * hp).sum() + (hp * hp).sum())
+    v = 8 * int((pp * pp).sum() * (1 if with_v_pppp else 0) + n_t + (hh * hh).sum() +
+                (ph * hp).sum() + (hp * hp).sum())
     v += 8 * 2 * n_t
     meta = 24 * int(pp.sum()) + 16 * int(hh.sum()) + 8 * system.n_sp
     return v + 24 * 8 * n_t + meta

@@ -4,4 +4,4 @@ System      host-side problem (basis, channels, V blocks, remap tables): libccdh
 CCDSolver   the CUDA iteration behind the C ABI of include/ccdgpu.h: libccdgpu.so
 """
 from .system import System  # noqa: F401
-from .solver import CCDSolver, CCDGPUError, Result  # noqa: F401
+from .solver import CCDSolver, CCDGPUError, Result, solve_batch  # noqa: F401

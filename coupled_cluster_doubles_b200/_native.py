@@ -114,7 +114,7 @@ GPU_SYMBOLS = [
     "ccdgpu_calc_t2_pphh", "ccdgpu_map_to_distributed", "ccdgpu_read_chain",
     "ccdgpu_get_profile", "ccdgpu_enable_profiling", "ccdgpu_work_per_iteration",
     "ccdgpu_energy_history", "ccdgpu_stream", "ccdgpu_calc_channel_t2diff_pphh_noalloc",
-    "ccdgpu_trace_arm", "ccdgpu_trace_read",
+    "ccdgpu_trace_arm", "ccdgpu_trace_read", "ccdgpu_solve_batch",
 ]
 
 
@@ -156,6 +156,7 @@ def gpu_lib():
         lib.ccdgpu_calc_channel_t2diff_pphh_noalloc.argtypes = [vp, vp, vp, vp, vp, c_i64, c_i64, vp]
         lib.ccdgpu_calc_channel_t2diff_pphh_noalloc.restype = ctypes.c_int
         lib.ccdgpu_trace_arm.argtypes = [vp, c_i64]
+        lib.ccdgpu_solve_batch.argtypes = [P(vp), c_i32, c_dbl, c_i64, c_dbl, P(Result)]
         lib.ccdgpu_trace_read.argtypes = [vp, P(c_u64), P(c_u64), c_i32]
         _gpu = lib
     return _gpu

@@ -1298,55 +1298,85 @@ int ccdgpu_step(ccdgpu_handle *h, double mixing, double *e_corr) {
   return std::isfinite(h->h_ctl->e_corr) ? CCDGPU_OK : CCDGPU_ERR_NONFINITE;
 }
 
-int ccdgpu_solve(ccdgpu_handle *h, double tol, int64_t max_iters, double mixing, ccdgpu_result *res) {
+}  // extern "C"
+
+namespace {
+
+// A solve in two halves, so that a batch can put every handle's device loop in flight before
+// waiting for any of them.
+struct SolveState {
+  bool fused = false, mixed = false, graph = false, device_loop = false;
+  double tol = 0;
+  int64_t cap = 0, it0 = 0, pol0 = 0;
+  std::chrono::steady_clock::time_point t0;
+};
+constexpr int64_t kLoopChunk = 128;  // iterations one device-loop launch may run
+
+// Device loop: launch up to kLoopChunk iterations without the host (no synchronisation).
+int loop_launch(ccdgpu_handle *h, SolveState &st) {
+  Control &c = *h->h_ctl;
+  st.it0 = c.iterations;
+  st.pol0 = c.polish_iters;
+  c.stop_at = c.iterations + kLoopChunk;
+  CK(cudaMemcpyAsync(&h->ctl->stop_at, &c.stop_at, sizeof(int64_t), cudaMemcpyHostToDevice,
+                     h->s0));
+  CK(cudaGraphLaunch(st.mixed && c.phase == 1 ? h->loop_tc : h->loop64, h->s0));
+  return CCDGPU_OK;
+}
+
+int solve_begin(ccdgpu_handle *h, double tol, int64_t max_iters, double mixing, SolveState &st) {
   if (!h || max_iters < 0 || !(tol >= 0)) return CCDGPU_ERR_INVALID_ARGUMENT;
   CK(cudaSetDevice(h->opt.device));
-  const bool fused = h->opt.path == CCDGPU_PATH_FUSED;
-  const bool mixed = fused && h->nt > 0;
+  st.fused = h->opt.path == CCDGPU_PATH_FUSED;
+  st.mixed = st.fused && h->nt > 0;
+  st.tol = tol;
+  st.cap = max_iters + 1;
   // A mixed solve starts in phase 1 (tensor-core ladder) and finishes in phase 2 (FP64).
-  int rc = set_ctl(h, 1, tol, max_iters, mixing, true, -1, mixed ? 1 : 0);
+  int rc = set_ctl(h, 1, tol, max_iters, mixing, true, -1, st.mixed ? 1 : 0);
   if (rc) return rc;
-  const bool graph = fused && h->opt.use_graph && !h->profiling;
-  if (graph) ready_loop_graphs(h);
-  const bool device_loop = graph && h->loop_state == 1;
-  if (graph && !device_loop && (rc = fused_ready_graph(h, false))) return rc;
-  if (graph && !device_loop && mixed && (rc = fused_ready_graph(h, true))) return rc;
-  auto t0 = std::chrono::steady_clock::now();
+  st.graph = st.fused && h->opt.use_graph && !h->profiling;
+  if (st.graph) ready_loop_graphs(h);
+  st.device_loop = st.graph && h->loop_state == 1;
+  if (st.graph && !st.device_loop && (rc = fused_ready_graph(h, false))) return rc;
+  if (st.graph && !st.device_loop && st.mixed && (rc = fused_ready_graph(h, true))) return rc;
+  st.t0 = std::chrono::steady_clock::now();
+  if (st.device_loop) return loop_launch(h, st);
+  return CCDGPU_OK;
+}
+
+int solve_finish(ccdgpu_handle *h, SolveState &st, double mixing, ccdgpu_result *res) {
+  CK(cudaSetDevice(h->opt.device));
+  int rc;
   int64_t launched = 0;
-  const int64_t cap = max_iters + 1;
-  // Device loop: each launch runs up to kLoopChunk iterations without the host.
-  constexpr int64_t kLoopChunk = 128;
-  while (device_loop) {
-    Control &c = *h->h_ctl;
-    const int64_t it0 = c.iterations, pol0 = c.polish_iters;
-    c.stop_at = it0 + kLoopChunk;
-    CK(cudaMemcpyAsync(&h->ctl->stop_at, &c.stop_at, sizeof(int64_t), cudaMemcpyHostToDevice,
-                       h->s0));
-    CK(cudaGraphLaunch(mixed && c.phase == 1 ? h->loop_tc : h->loop64, h->s0));
+  while (st.device_loop) {
     if ((rc = sync_ctl(h))) return rc;
-    const int64_t fp = (c.polish_iters - pol0) + (mixed ? 0 : c.iterations - it0);
-    h->launches += (c.iterations - it0 - fp) * h->kernels_per_body_tc + fp * h->kernels_per_body64;
-    if (c.done || c.iterations >= cap || c.iterations == it0) break;
+    Control &c = *h->h_ctl;
+    const int64_t fp = (c.polish_iters - st.pol0) + (st.mixed ? 0 : c.iterations - st.it0);
+    h->launches += (c.iterations - st.it0 - fp) * h->kernels_per_body_tc + fp * h->kernels_per_body64;
+    if (c.done || c.iterations >= st.cap || c.iterations == st.it0) break;
+    if ((rc = loop_launch(h, st))) return rc;
   }
-  while (!device_loop) {
+  while (!st.device_loop) {
     // Iterations are launched in batches; once the device-side stop rule fires the remaining
     // launches of the batch return immediately.
-    const int64_t batch =
-        (fused && !h->profiling) ? std::min<int64_t>(launched < 8 ? 4 : 8, cap - launched) : 1;
+    const int64_t batch = (st.fused && !h->profiling)
+                              ? std::min<int64_t>(launched < 8 ? 4 : 8, st.cap - launched)
+                              : 1;
     // The phase can only change inside a batch from 1 to 2; mixed iterations that follow
     // the switch in the same batch are no-ops on the device.
-    const bool mphase = mixed && h->h_ctl->phase == 1;
+    const bool mphase = st.mixed && h->h_ctl->phase == 1;
     for (int64_t b = 0; b < batch; b++) {
-      if (graph) CK(cudaGraphLaunch(mphase ? h->graph_tc : h->graph, h->s0));
-      else if (fused) { if ((rc = enqueue_fused_iteration(h, mphase))) return rc; }
+      if (st.graph) CK(cudaGraphLaunch(mphase ? h->graph_tc : h->graph, h->s0));
+      else if (st.fused) { if ((rc = enqueue_fused_iteration(h, mphase))) return rc; }
       else {
         if ((rc = tables_iteration(h, mixing, nullptr))) return rc;
       }
     }
     launched += batch;
-    if (graph) h->launches += batch * (mphase ? h->kernels_per_graph_tc : h->kernels_per_graph);
+    if (st.graph)
+      h->launches += batch * (mphase ? h->kernels_per_graph_tc : h->kernels_per_graph);
     if ((rc = sync_ctl(h))) return rc;
-    if (h->profiling && fused && !graph) {
+    if (h->profiling && st.fused && !st.graph) {
       float a = 0, b = 0, c = 0, d = 0, e = 0, f = 0;
       cudaEventElapsedTime(&a, h->ev[0], h->ev[1]);
       cudaEventElapsedTime(&b, h->ev[1], h->ev[2]);
@@ -1362,20 +1392,55 @@ int ccdgpu_solve(ccdgpu_handle *h, double tol, int64_t max_iters, double mixing,
       h->prof.ms_total += f;
       h->prof.iterations += 1;
     }
-    if (h->h_ctl->done || launched >= cap) break;
+    if (h->h_ctl->done || launched >= st.cap) break;
   }
   auto t1 = std::chrono::steady_clock::now();
-  if ((rc = check_errors(h))) return rc;
+  // The result reflects the control block also when the solve failed (for example non-finite
+  // amplitudes of a diverging iteration); the status says so.
   const Control &c = *h->h_ctl;
   if (res) {
     res->e_corr = c.e_corr;
     res->e_diff = c.e_diff;
     res->iterations = c.iterations;
-    res->converged = std::fabs(c.e_diff) <= tol ? 1 : 0;
+    res->converged = std::fabs(c.e_diff) <= st.tol ? 1 : 0;
     res->polish_iterations = (int32_t)c.polish_iters;
-    res->seconds = std::chrono::duration<double>(t1 - t0).count();
+    res->seconds = std::chrono::duration<double>(t1 - st.t0).count();
   }
-  return CCDGPU_OK;
+  return check_errors(h);
+}
+
+}  // namespace
+
+extern "C" {
+
+int ccdgpu_solve(ccdgpu_handle *h, double tol, int64_t max_iters, double mixing, ccdgpu_result *res) {
+  SolveState st;
+  int rc = solve_begin(h, tol, max_iters, mixing, st);
+  if (rc) return rc;
+  return solve_finish(h, st, mixing, res);
+}
+
+int ccdgpu_solve_batch(ccdgpu_handle *const *hs, int32_t n, double tol, int64_t max_iters,
+                       double mixing, ccdgpu_result *res) {
+  if (!hs || n < 0) return CCDGPU_ERR_INVALID_ARGUMENT;
+  for (int32_t i = 0; i < n; i++)
+    for (int32_t j = 0; j < i; j++)
+      if (!hs[i] || hs[i] == hs[j]) return CCDGPU_ERR_INVALID_ARGUMENT;
+  std::vector<SolveState> st(n);
+  int first_rc = CCDGPU_OK;
+  std::vector<int> begun(n, 0);
+  // Every handle's device loop goes in flight on its own streams before any is waited for.
+  for (int32_t i = 0; i < n; i++) {
+    const int rc = solve_begin(hs[i], tol, max_iters, mixing, st[i]);
+    if (rc && !first_rc) first_rc = rc;
+    begun[i] = rc == CCDGPU_OK;
+  }
+  for (int32_t i = 0; i < n; i++) {
+    if (!begun[i]) continue;
+    const int rc = solve_finish(hs[i], st[i], mixing, res ? &res[i] : nullptr);
+    if (rc && !first_rc) first_rc = rc;
+  }
+  return first_rc;
 }
 
 int ccdgpu_energy_history(ccdgpu_handle *h, double *out, int64_t cap, int64_t *n_out) {

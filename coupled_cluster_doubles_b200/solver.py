@@ -61,6 +61,19 @@ class Result:
                 f"converged={self.converged}, seconds={self.seconds:.6f})")
 
 
+def solve_batch(solvers, tol=1e-8, max_iters=100, mixing=0.5, check=True):
+    """Solve several independent systems together (ccdgpu_solve_batch): every solver's device
+    loop is in flight at once.  Returns one Result per solver; with check=False a failed solve
+    (for example a diverging iteration, e_corr non-finite) does not raise."""
+    n = len(solvers)
+    hs = (ctypes.c_void_p * n)(*[s._h for s in solvers])
+    rs = (_native.Result * n)()
+    rc = _native.gpu_lib().ccdgpu_solve_batch(hs, n, tol, max_iters, mixing, rs)
+    if check:
+        _check(rc, "ccdgpu_solve_batch")
+    return [Result(r) for r in rs]
+
+
 class CCDSolver:
     def __init__(self, system, precision="fp64", path="fused", v_mode="stored", device=0,
                  use_graph=True, polish_threshold=1e-6):

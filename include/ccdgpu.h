@@ -169,6 +169,15 @@ int ccdgpu_step(ccdgpu_handle *h, double mixing, double *e_corr);
 int ccdgpu_solve(ccdgpu_handle *h, double tol, int64_t max_iters, double mixing,
                  ccdgpu_result *res);
 
+/* No counterpart in the reference (its runs are one system per process).  Solves n
+ * independent systems together: each handle's iteration loop runs on its own device streams
+ * and all of them are in flight at once, so the kernels of small systems share the GPU.  Same
+ * stop rule and results as n calls of ccdgpu_solve; res[i] is handle i's result, filled also
+ * for a handle whose solve failed (e_corr non-finite for a diverging iteration).  Handles must
+ * be distinct; returns the first error, after finishing the solves that started. */
+int ccdgpu_solve_batch(ccdgpu_handle *const *handles, int32_t n, double tol, int64_t max_iters,
+                       double mixing, ccdgpu_result *res);
+
 /* corrCCD after each iteration of the last ccdgpu_solve (first 128 iterations); *n_out gets
  * the number of iterations stored.  The per-iteration printout of main.cpp:672-680. */
 int ccdgpu_energy_history(ccdgpu_handle *h, double *out, int64_t cap, int64_t *n_out);

@@ -76,3 +76,30 @@ def test_mixed_stops_within_1e7_per_particle():
                 res = sol.solve(tol=1e-8 * n, max_iters=100, mixing=0.5)
             assert res.converged
             assert abs(res.e_corr - e_ref) / n <= 1e-7
+
+
+def test_batch_solve_matches_individual_solves():
+    """ccdgpu_solve_batch: several systems (different N, r_s, cutoff, precision) in flight at
+    once give exactly the results of separate solves."""
+    from coupled_cluster_doubles_b200 import System, solve_batch
+    specs = [dict(r_s=1.0, n_shells=19, n_particle_shells=2), dict(r_s=2.0, n_shells=15, n_particle_shells=3),
+             dict(r_s=0.5, n_shells=19, n_particle_shells=4)]
+    systems = [System.electron_gas(**p, load_v_pppp=False) for p in specs]
+    try:
+        precs = ["mixed_bf16", "fp64", "mixed_bf16"]
+        solos = []
+        for s, pr in zip(systems, precs):
+            with CCDSolver(s, v_mode="on_the_fly", precision=pr) as sol:
+                solos.append((sol.solve(tol=1e-10), sol.t2()))
+        sols = [CCDSolver(s, v_mode="on_the_fly", precision=pr) for s, pr in zip(systems, precs)]
+        try:
+            res = solve_batch(sols, tol=1e-10)
+            for (r0, t0), r, sol in zip(solos, res, sols):
+                assert r.iterations == r0.iterations and r.e_corr == r0.e_corr
+                np.testing.assert_array_equal(sol.t2(), t0)
+        finally:
+            for sol in sols:
+                sol.close()
+    finally:
+        for s in systems:
+            s.close()
