@@ -190,6 +190,8 @@ def main():
     ap.add_argument("--v-mode", default="stored", choices=["stored", "on_the_fly"],
                     help="on_the_fly: V_pppp generated on the device from the model (the host "
                          "builds and uploads none)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default pp-ladder schedule instead of autotuning it")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--single-arm", action="store_true",
                     help="time only the headline precision (for profiler launch lists)")
@@ -225,6 +227,9 @@ def main():
                             v_mode=args.v_mode)
                for a in arms}
     stream = {a: torch.cuda.ExternalStream(solvers[a].stream_ptr(), device=local) for a in arms}
+    # Autotuner: each arm's pp-ladder schedule picked by timing the candidates (untimed setup).
+    tuned = {a: (solvers[a].autotune(reps=3) if not args.no_autotune else
+                 (solvers[a].schedule(), None, None)) for a in arms}
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
 
     # Fully converged FP64 energy (untimed) for the |dE/N| check.
@@ -352,6 +357,8 @@ def main():
                 "pp_ladder_tflops_algorithmic": work[a]["ladder_flops"] / (lms / 1000.0) / 1e12,
                 "pp_ladder_gbs": work[a]["ladder_bytes"] / (lms / 1000.0) / 1e9,
                 "gpu_launches": int(ta["launches"]),
+                "schedule": tuned[a][0],
+                "schedule_source": "autotuned" if not args.no_autotune else "default",
             }
         if "fp64" in arms_out:
             # Executed FP64 rate: the antisymmetry-packed ladder runs about a quarter of the

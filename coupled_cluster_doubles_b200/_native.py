@@ -63,6 +63,11 @@ class Options(ctypes.Structure):
                 ("polish_threshold", c_dbl), ("use_graph", c_i32), ("reserved", c_i32 * 7)]
 
 
+class Schedule(ctypes.Structure):
+    _fields_ = [("thin_split_mul", c_i32), ("wide_split_mul", c_i32), ("tc_split_mul", c_i32),
+                ("reserved", c_i32 * 5)]
+
+
 class Result(ctypes.Structure):
     _fields_ = [("e_corr", c_dbl), ("e_diff", c_dbl), ("iterations", c_i64),
                 ("converged", c_i32), ("polish_iterations", c_i32), ("seconds", c_dbl)]
@@ -114,7 +119,8 @@ GPU_SYMBOLS = [
     "ccdgpu_calc_t2_pphh", "ccdgpu_map_to_distributed", "ccdgpu_read_chain",
     "ccdgpu_get_profile", "ccdgpu_enable_profiling", "ccdgpu_work_per_iteration",
     "ccdgpu_energy_history", "ccdgpu_stream", "ccdgpu_calc_channel_t2diff_pphh_noalloc",
-    "ccdgpu_trace_arm", "ccdgpu_trace_read", "ccdgpu_solve_batch",
+    "ccdgpu_trace_arm", "ccdgpu_trace_read", "ccdgpu_solve_batch", "ccdgpu_set_schedule",
+    "ccdgpu_get_schedule", "ccdgpu_autotune",
 ]
 
 
@@ -157,6 +163,9 @@ def gpu_lib():
         lib.ccdgpu_calc_channel_t2diff_pphh_noalloc.restype = ctypes.c_int
         lib.ccdgpu_trace_arm.argtypes = [vp, c_i64]
         lib.ccdgpu_solve_batch.argtypes = [P(vp), c_i32, c_dbl, c_i64, c_dbl, P(Result)]
+        lib.ccdgpu_set_schedule.argtypes = [vp, P(Schedule)]
+        lib.ccdgpu_get_schedule.argtypes = [vp, P(Schedule)]
+        lib.ccdgpu_autotune.argtypes = [vp, c_i32, P(Schedule), P(c_dbl), P(c_dbl)]
         lib.ccdgpu_trace_read.argtypes = [vp, P(c_u64), P(c_u64), c_i32]
         _gpu = lib
     return _gpu

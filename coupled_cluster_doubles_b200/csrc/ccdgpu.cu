@@ -95,6 +95,12 @@ struct ccdgpu_handle {
   int64_t n_tkt = 0, n_tmt = 0;
   int64_t launches = 0;
 
+  // pp-ladder work lists (make_ladder_tiles), in their own allocation so the autotuner can
+  // rebuild them.
+  std::vector<ChanInfo> host_chans;
+  ccdgpu_schedule schedule{};
+  void *tile_mem = nullptr;
+
   // Mixed precision (nt bf16 terms per operand; 0 for an FP64 handle).
   int nt = 0;
   int n_tc_tiles = 0;
@@ -158,6 +164,8 @@ void release(ccdgpu_handle *h) {
   if (h->loop_tc) cudaGraphExecDestroy(h->loop_tc);
   for (auto &b : h->allocs) cudaFree(b.p);
   h->allocs.clear();
+  if (h->tile_mem) cudaFree(h->tile_mem);
+  h->tile_mem = nullptr;
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
   for (auto &e : h->ev)
     if (e) cudaEventDestroy(e);
@@ -216,6 +224,126 @@ int upload_runs(ccdgpu_handle *h, T *dst, const std::vector<const T *> &src,
     pos += count[k];
   }
   return flush();
+}
+
+// pp-ladder work tiles for a schedule (split factors of K per column class), in their own
+// device allocation; drops captured graphs, which hold the old lists.
+//   FP64 ladder: thin row blocks stream at full bandwidth on their own, so K is split only when
+//   there are fewer of them than SMs (up to thin_split_mul tiles per SM); mid/wide tiles are
+//   compute-latency bound per CTA, so K is split into segments of at least four chunks until
+//   the class has about wide_split_mul tiles per SM.
+//   Tensor-core ladder: each CTA is bandwidth bound, so K is split until there are about
+//   tc_split_mul tiles per SM.
+// Split tiles are reduced deterministically (ladder_reduce).
+int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
+  const std::vector<ChanInfo> &chans = h->host_chans;
+  auto cls_of = [](int nb) { return nb <= 8 ? 0 : nb <= 32 ? 1 : 2; };
+  int64_t blocks_thin = 0, blocks_wide = 0;
+  for (const ChanInfo &a : chans) (a.nb <= 8 ? blocks_thin : blocks_wide) += a.nmt;
+  const int64_t kSMs = 148;
+  const int want_thin = blocks_thin >= kSMs ? 1 : (int)std::min<int64_t>(8, ceil_div(sch.thin_split_mul * kSMs, std::max<int64_t>(blocks_thin, 1)));
+  const int want_wide = (int)std::min<int64_t>(64, std::max<int64_t>(1, ceil_div(sch.wide_split_mul * kSMs, std::max<int64_t>(blocks_wide, 1))));
+  std::vector<LadderTile> tiles;
+  int64_t lpart_tot = 0;
+  int32_t groups = 0;
+  for (int ai = 0; ai < h->n_act; ai++) {
+    const ChanInfo &a = chans[ai];
+    const int want = a.nb <= 8 ? want_thin : want_wide;
+    const int min_chunks = 4;
+    const int nseg = std::max(1, std::min(want, a.nkc / min_chunks));
+    for (int mt = 0; mt < a.nmt; mt++) {
+      const int rows = std::min(a.bm, a.pr - mt * a.bm);
+      const int64_t pbase = lpart_tot;
+      if (nseg > 1) lpart_tot += (int64_t)nseg * a.bm * a.nb;
+      for (int sg = 0; sg < nseg; sg++) {
+        LadderTile tl{};
+        tl.ch = ai; tl.mt = mt;
+        tl.kc0 = (int)((int64_t)a.nkc * sg / nseg);
+        tl.nks = (int)((int64_t)a.nkc * (sg + 1) / nseg) - tl.kc0;
+        tl.nkc = a.nkc;
+        tl.nkh = (sg == nseg - 1) ? a.nkh : 0;
+        tl.nb = a.nb; tl.bm = a.bm; tl.rows = rows; tl.pr = a.pr; tl.hh = a.hh;
+        tl.seg = sg; tl.nseg = nseg; tl.group = groups;
+        tl.v_base = a.vkt_base; tl.tkt_base = a.tkt_base; tl.tmt_base = a.tmt_base;
+        tl.xt_base = a.xt_base; tl.t_off = a.t_off; tl.row_off = a.row_off;
+        tl.part_base = pbase;
+        tiles.push_back(tl);
+      }
+      groups++;
+    }
+  }
+  // Thin channels first, then wide ones; within each class the longest K streams first so
+  // the hardware block scheduler fills in the short ones.
+  std::stable_sort(tiles.begin(), tiles.end(), [&](const LadderTile &x, const LadderTile &y) {
+    const int cx = cls_of(x.nb), cy = cls_of(y.nb);
+    if (cx != cy) return cx < cy;
+    return (int64_t)(x.nks + x.nkh) * (x.rows + x.nb) > (int64_t)(y.nks + y.nkh) * (y.rows + y.nb);
+  });
+  std::vector<LadderTile> tc_tiles;
+  int64_t tcpart_tot = 0;
+  int32_t tc_groups = 0;
+  if (h->nt) {
+    int64_t blocks = 0;
+    for (const ChanInfo &a : chans) blocks += ceil_div(a.pr, kTcBM);
+    const int want = (int)std::min<int64_t>(32, std::max<int64_t>(1, ceil_div(sch.tc_split_mul * kSMs, blocks)));
+    for (int ai = 0; ai < h->n_act; ai++) {
+      const ChanInfo &a = chans[ai];
+      const int nmt = (int)ceil_div(a.pr, kTcBM);
+      const int nseg = std::max(1, std::min(want, a.nkct / 4));
+      for (int mt = 0; mt < nmt; mt++) {
+        const int rows = std::min(kTcBM, a.pr - mt * kTcBM);
+        const int64_t pbase = tcpart_tot;
+        if (nseg > 1) tcpart_tot += (int64_t)nseg * kTcBM * a.nbt;
+        for (int sg = 0; sg < nseg; sg++) {
+          LadderTile tl{};
+          tl.ch = ai; tl.mt = mt;
+          tl.kc0 = (int)((int64_t)a.nkct * sg / nseg);
+          tl.nks = (int)((int64_t)a.nkct * (sg + 1) / nseg) - tl.kc0;
+          tl.nkc = a.nkct;
+          tl.nkh = (sg == nseg - 1) ? a.nkht : 0;
+          tl.nb = a.nbt; tl.bm = kTcBM; tl.rows = rows; tl.pr = a.pr; tl.hh = a.hh;
+          tl.seg = sg; tl.nseg = nseg; tl.group = tc_groups;
+          tl.v_base = a.vtc_base; tl.tkt_base = a.tkt_tc_base; tl.tmt_base = a.tmt_tc_base;
+          tl.xt_base = a.xt_tc_base; tl.t_off = a.t_off; tl.row_off = a.row_off;
+          tl.part_base = pbase;
+          tc_tiles.push_back(tl);
+        }
+        tc_groups++;
+      }
+    }
+    // Largest byte streams first.
+    std::stable_sort(tc_tiles.begin(), tc_tiles.end(), [](const LadderTile &x, const LadderTile &y) {
+      return (int64_t)(x.nks + x.nkh) * (x.rows + x.nb) > (int64_t)(y.nks + y.nkh) * (y.rows + y.nb);
+    });
+  }
+  // Device copies: one allocation, counters zeroed.
+  CK(cudaStreamSynchronize(h->s0));
+  if (h->tile_mem) CK(cudaFree(h->tile_mem));
+  h->tile_mem = nullptr;
+  Arena ar;
+  ar.add(&h->tiles, tiles.size()); ar.add(&h->lcounters, groups); ar.add(&h->lpart, lpart_tot);
+  ar.add(&h->tc_tiles, tc_tiles.size()); ar.add(&h->tc_counters, tc_groups);
+  ar.add(&h->tc_part, tcpart_tot);
+  CK(cudaMalloc(&h->tile_mem, ar.used));
+  CK(cudaMemsetAsync(h->tile_mem, 0, ar.used, h->s0));
+  for (auto &r : ar.reqs) *r.first = static_cast<char *>(h->tile_mem) + r.second;
+  if (!tiles.empty())
+    CK(cudaMemcpyAsync(h->tiles, tiles.data(), tiles.size() * sizeof(LadderTile),
+                       cudaMemcpyHostToDevice, h->s0));
+  if (!tc_tiles.empty())
+    CK(cudaMemcpyAsync(h->tc_tiles, tc_tiles.data(), tc_tiles.size() * sizeof(LadderTile),
+                       cudaMemcpyHostToDevice, h->s0));
+  CK(cudaStreamSynchronize(h->s0));
+  h->n_tiles = (int)tiles.size();
+  h->n_cls[0] = h->n_cls[1] = h->n_cls[2] = 0;
+  for (const LadderTile &t : tiles) h->n_cls[cls_of(t.nb)]++;
+  h->n_tc_tiles = (int)tc_tiles.size();
+  h->schedule = sch;
+  // Captured graphs hold the previous lists.
+  for (cudaGraphExec_t *g : {&h->graph, &h->graph_tc, &h->loop64, &h->loop_tc})
+    if (*g) { cudaGraphExecDestroy(*g); *g = nullptr; }
+  h->loop_state = 0;
+  return CCDGPU_OK;
 }
 
 int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
@@ -405,96 +533,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   if (h->n_h != n_t || h->n_p != n_t) return CCDGPU_ERR_BAD_TABLE;
   h->have_3body = P->v_h_hpp && P->v_phh_p;
 
-  // pp-ladder work tiles.  Thin row blocks stream at full bandwidth on their own, so K is
-  // split only when there are fewer of them than SMs.  Mid/wide tiles are compute-latency
-  // bound per CTA, so their K is split into segments of at least four chunks until the class
-  // has about three tiles per SM.  Split tiles are reduced deterministically (ladder_reduce).
-  auto cls_of = [](int nb) { return nb <= 8 ? 0 : nb <= 32 ? 1 : 2; };
-  int64_t blocks_thin = 0, blocks_wide = 0;
-  for (const ChanInfo &a : chans) (a.nb <= 8 ? blocks_thin : blocks_wide) += a.nmt;
-  const int64_t kSMs = 148;
-  const int want_thin = blocks_thin >= kSMs ? 1 : (int)std::min<int64_t>(8, ceil_div(kSMs, std::max<int64_t>(blocks_thin, 1)));
-  const int want_wide = (int)std::min<int64_t>(32, std::max<int64_t>(1, ceil_div(3 * kSMs, std::max<int64_t>(blocks_wide, 1))));
-  std::vector<LadderTile> tiles;
-  int64_t lpart_tot = 0;
-  int32_t groups = 0;
-  for (int ai = 0; ai < h->n_act; ai++) {
-    const ChanInfo &a = chans[ai];
-    const int want = a.nb <= 8 ? want_thin : want_wide;
-    const int min_chunks = 4;
-    const int nseg = std::max(1, std::min(want, a.nkc / min_chunks));
-    for (int mt = 0; mt < a.nmt; mt++) {
-      const int rows = std::min(a.bm, a.pr - mt * a.bm);
-      const int64_t pbase = lpart_tot;
-      if (nseg > 1) lpart_tot += (int64_t)nseg * a.bm * a.nb;
-      for (int sg = 0; sg < nseg; sg++) {
-        LadderTile tl{};
-        tl.ch = ai; tl.mt = mt;
-        tl.kc0 = (int)((int64_t)a.nkc * sg / nseg);
-        tl.nks = (int)((int64_t)a.nkc * (sg + 1) / nseg) - tl.kc0;
-        tl.nkc = a.nkc;
-        tl.nkh = (sg == nseg - 1) ? a.nkh : 0;
-        tl.nb = a.nb; tl.bm = a.bm; tl.rows = rows; tl.pr = a.pr; tl.hh = a.hh;
-        tl.seg = sg; tl.nseg = nseg; tl.group = groups;
-        tl.v_base = a.vkt_base; tl.tkt_base = a.tkt_base; tl.tmt_base = a.tmt_base;
-        tl.xt_base = a.xt_base; tl.t_off = a.t_off; tl.row_off = a.row_off;
-        tl.part_base = pbase;
-        tiles.push_back(tl);
-      }
-      groups++;
-    }
-  }
-  // Thin channels first, then wide ones; within each class the longest K streams first so
-  // the hardware block scheduler fills in the short ones.
-  std::stable_sort(tiles.begin(), tiles.end(), [&](const LadderTile &x, const LadderTile &y) {
-    const int cx = cls_of(x.nb), cy = cls_of(y.nb);
-    if (cx != cy) return cx < cy;
-    return (int64_t)(x.nks + x.nkh) * (x.rows + x.nb) > (int64_t)(y.nks + y.nkh) * (y.rows + y.nb);
-  });
-  h->n_tiles = (int)tiles.size();
-  for (const LadderTile &t : tiles) h->n_cls[cls_of(t.nb)]++;
-
-  // Mixed-precision ladder tiles: 128-row tiles of every channel in one launch.  The tensor
-  // cores leave each CTA bandwidth bound, so K is split (deterministic reduction) until there
-  // are about two tiles per SM.
-  std::vector<LadderTile> tc_tiles;
-  int64_t tcpart_tot = 0;
-  int32_t tc_groups = 0;
-  if (h->nt) {
-    int64_t blocks = 0;
-    for (const ChanInfo &a : chans) blocks += ceil_div(a.pr, kTcBM);
-    const int want = (int)std::min<int64_t>(16, std::max<int64_t>(1, ceil_div(2 * kSMs, blocks)));
-    for (int ai = 0; ai < h->n_act; ai++) {
-      const ChanInfo &a = chans[ai];
-      const int nmt = (int)ceil_div(a.pr, kTcBM);
-      const int nseg = std::max(1, std::min(want, a.nkct / 4));
-      for (int mt = 0; mt < nmt; mt++) {
-        const int rows = std::min(kTcBM, a.pr - mt * kTcBM);
-        const int64_t pbase = tcpart_tot;
-        if (nseg > 1) tcpart_tot += (int64_t)nseg * kTcBM * a.nbt;
-        for (int sg = 0; sg < nseg; sg++) {
-          LadderTile tl{};
-          tl.ch = ai; tl.mt = mt;
-          tl.kc0 = (int)((int64_t)a.nkct * sg / nseg);
-          tl.nks = (int)((int64_t)a.nkct * (sg + 1) / nseg) - tl.kc0;
-          tl.nkc = a.nkct;
-          tl.nkh = (sg == nseg - 1) ? a.nkht : 0;
-          tl.nb = a.nbt; tl.bm = kTcBM; tl.rows = rows; tl.pr = a.pr; tl.hh = a.hh;
-          tl.seg = sg; tl.nseg = nseg; tl.group = tc_groups;
-          tl.v_base = a.vtc_base; tl.tkt_base = a.tkt_tc_base; tl.tmt_base = a.tmt_tc_base;
-          tl.xt_base = a.xt_tc_base; tl.t_off = a.t_off; tl.row_off = a.row_off;
-          tl.part_base = pbase;
-          tc_tiles.push_back(tl);
-        }
-        tc_groups++;
-      }
-    }
-    // Largest byte streams first.
-    std::stable_sort(tc_tiles.begin(), tc_tiles.end(), [](const LadderTile &x, const LadderTile &y) {
-      return (int64_t)(x.nks + x.nkh) * (x.rows + x.nb) > (int64_t)(y.nks + y.nkh) * (y.rows + y.nb);
-    });
-  }
-  h->n_tc_tiles = (int)tc_tiles.size();
+  h->host_chans = chans;
 
   std::vector<ElemRange> ranges;
   const int64_t per = (int64_t)kAsmThreads * kAsmPerThread;
@@ -541,7 +580,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   // ---- one device allocation ----
   Arena ar;
   ar.add(&h->chans, chans.size()); ar.add(&h->mods, mods.size());
-  ar.add(&h->tiles, tiles.size()); ar.add(&h->hh_tiles, hh_tiles.size());
+  ar.add(&h->hh_tiles, hh_tiles.size());
   ar.add(&h->ranges, ranges.size());
   ar.add(&h->pp_pairs, pp_pairs.size()); ar.add(&h->hh_pairs, hh_pairs.size());
   ar.add(&h->pp_swap, pp_swap.size()); ar.add(&h->hh_swap, hh_swap.size());
@@ -549,7 +588,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   ar.add(&h->rowmap, rowmap.size()); ar.add(&h->mirror, mirror.size());
   ar.add(&h->pk_idx, pk_idx.size());
   ar.add(&h->counters, h->n_act); ar.add(&h->part, part_tot);
-  ar.add(&h->lcounters, groups); ar.add(&h->lpart, lpart_tot);
+
   ar.add(&h->eps, nsp);
   ar.add(&h->v_pphh, n_t); ar.add(&h->v_hhhh, x_tot); ar.add(&h->v_t, vt);
   ar.add(&h->v_hpph, h->n_m); ar.add(&h->v_hphp, y_tot);
@@ -566,8 +605,6 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     auto round_up = [](int64_t n) { return std::max<int64_t>(256, (n + 255) / 256 * 256); };
     h->n_vtc = round_up(vtc); h->n_tkttc = round_up(tkttc);
     h->n_tmttc = round_up(tmttc); h->n_xttc = round_up(xttc);
-    ar.add(&h->tc_tiles, tc_tiles.size()); ar.add(&h->tc_counters, tc_groups);
-    ar.add(&h->tc_part, tcpart_tot);
     ar.add(&h->v_tc, (size_t)h->nt * h->n_vtc); ar.add(&h->tkt_tc, (size_t)h->nt * h->n_tkttc);
     ar.add(&h->tmt_tc, (size_t)h->nt * h->n_tmttc); ar.add(&h->xt_tc, (size_t)h->nt * h->n_xttc);
   }
@@ -641,11 +678,9 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     if (!v.empty()) CK(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice, h->s0));
     return CCDGPU_OK;
   };
-  TRY(put(h->chans, chans)); TRY(put(h->mods, mods)); TRY(put(h->tiles, tiles));
+  TRY(put(h->chans, chans)); TRY(put(h->mods, mods));
   TRY(put(h->hh_tiles, hh_tiles)); TRY(put(h->ranges, ranges)); TRY(put(h->pranges, pranges));
-  if (h->nt) {
-    TRY(put(h->tc_tiles, tc_tiles));
-  }
+
   TRY(put(h->kcol, kcol));
   TRY(put(h->pp_pairs, pp_pairs)); TRY(put(h->hh_pairs, hh_pairs));
   TRY(put(h->pp_swap, pp_swap)); TRY(put(h->hh_swap, hh_swap));
@@ -767,6 +802,11 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
                           (int)std::max<size_t>(h->ring_smem_mid, 16)));
   CK(cudaFuncSetAttribute(ring_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)std::max<size_t>(h->ring_smem, 16)));
+  ccdgpu_schedule sch{};
+  sch.thin_split_mul = 1;
+  sch.wide_split_mul = 3;
+  sch.tc_split_mul = 2;
+  if (int rc2 = make_ladder_tiles(h, sch)) return rc2;
   if (h->nt) {
     h->tc_smem = tc_smem_bytes(h->nt);
     if (h->nt == 2)
@@ -1551,6 +1591,77 @@ int ccdgpu_enable_profiling(ccdgpu_handle *h, int32_t on) {
   return CCDGPU_OK;
 }
 void *ccdgpu_stream(ccdgpu_handle *h) { return h ? (void *)h->s0 : nullptr; }
+
+int ccdgpu_set_schedule(ccdgpu_handle *h, const ccdgpu_schedule *sch) {
+  if (!h || !sch || sch->thin_split_mul < 1 || sch->wide_split_mul < 1 || sch->tc_split_mul < 1)
+    return CCDGPU_ERR_INVALID_ARGUMENT;
+  CK(cudaSetDevice(h->opt.device));
+  return make_ladder_tiles(h, *sch);
+}
+
+int ccdgpu_get_schedule(const ccdgpu_handle *h, ccdgpu_schedule *sch) {
+  if (!h || !sch) return CCDGPU_ERR_INVALID_ARGUMENT;
+  *sch = h->schedule;
+  return CCDGPU_OK;
+}
+
+// Times `reps` launches of the handle's pp ladders for each candidate schedule (CUDA events on
+// the handle's stream; the ladders only overwrite the iteration's D) and keeps the fastest.
+int ccdgpu_autotune(ccdgpu_handle *h, int32_t reps, ccdgpu_schedule *chosen, double *ms_fp64,
+                    double *ms_tc) {
+  if (!h || reps < 1) return CCDGPU_ERR_INVALID_ARGUMENT;
+  CK(cudaSetDevice(h->opt.device));
+  int rc = set_ctl(h, 0, h->h_ctl->tol, h->h_ctl->max_iters, h->h_ctl->mixing, false);
+  if (rc) return rc;
+  auto time_ladder = [&](bool tc, double *ms) -> int {
+    int r = tc ? launch_pp_ladder_tc(h, h->s0) : launch_pp_ladder(h, h->s0);  // warm-up
+    if (r) return r;
+    CK(cudaEventRecord(h->ev[0], h->s0));
+    for (int i = 0; i < reps && !r; i++) r = tc ? launch_pp_ladder_tc(h, h->s0) : launch_pp_ladder(h, h->s0);
+    if (r) return r;
+    CK(cudaEventRecord(h->ev[1], h->s0));
+    CK(cudaEventSynchronize(h->ev[1]));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, h->ev[0], h->ev[1]));
+    *ms = t / reps;
+    return check_errors(h);
+  };
+  ccdgpu_schedule best = h->schedule;
+  double best64 = 0, besttc = 0;
+  // FP64 ladder: split factors of the thin and the mid/wide classes.
+  const int thin_c[] = {1, 2, 4}, wide_c[] = {1, 3, 6, 12, 24, 48};
+  bool first = true;
+  for (int tm : thin_c)
+    for (int wm : wide_c) {
+      ccdgpu_schedule c = best;
+      c.thin_split_mul = tm;
+      c.wide_split_mul = wm;
+      if ((rc = make_ladder_tiles(h, c))) return rc;
+      double ms = 0;
+      if ((rc = time_ladder(false, &ms))) return rc;
+      if (first || ms < best64) { best64 = ms; best.thin_split_mul = tm; best.wide_split_mul = wm; }
+      first = false;
+    }
+  // Tensor-core ladder: split factor.
+  if (h->nt) {
+    first = true;
+    const int tc_c[] = {1, 2, 4, 8, 16};
+    for (int tm : tc_c) {
+      ccdgpu_schedule c = best;
+      c.tc_split_mul = tm;
+      if ((rc = make_ladder_tiles(h, c))) return rc;
+      double ms = 0;
+      if ((rc = time_ladder(true, &ms))) return rc;
+      if (first || ms < besttc) { besttc = ms; best.tc_split_mul = tm; }
+      first = false;
+    }
+  }
+  if ((rc = make_ladder_tiles(h, best))) return rc;
+  if (chosen) *chosen = best;
+  if (ms_fp64) *ms_fp64 = best64;
+  if (ms_tc) *ms_tc = besttc;
+  return CCDGPU_OK;
+}
 
 int ccdgpu_trace_arm(ccdgpu_handle *h, int64_t iteration) {
   if (!h) return CCDGPU_ERR_INVALID_ARGUMENT;

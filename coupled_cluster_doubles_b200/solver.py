@@ -165,6 +165,25 @@ class CCDSolver:
         _check(_native.gpu_lib().ccdgpu_get_profile(self._h, ctypes.byref(p)), "profile")
         return {k: getattr(p, k) for k, _ in p._fields_}
 
+    def schedule(self):
+        sch = _native.Schedule()
+        _check(_native.gpu_lib().ccdgpu_get_schedule(self._h, ctypes.byref(sch)), "schedule")
+        return {"thin_split_mul": sch.thin_split_mul, "wide_split_mul": sch.wide_split_mul,
+                "tc_split_mul": sch.tc_split_mul}
+
+    def set_schedule(self, thin_split_mul=1, wide_split_mul=3, tc_split_mul=2):
+        sch = _native.Schedule(thin_split_mul, wide_split_mul, tc_split_mul)
+        _check(_native.gpu_lib().ccdgpu_set_schedule(self._h, ctypes.byref(sch)), "set_schedule")
+
+    def autotune(self, reps=5):
+        """Pick the pp-ladder schedule by timing the candidates on this GPU (ccdgpu_autotune).
+        Returns (schedule dict, ms per FP64 ladder, ms per tensor-core ladder)."""
+        sch = _native.Schedule()
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(_native.gpu_lib().ccdgpu_autotune(self._h, reps, ctypes.byref(sch), ctypes.byref(a),
+                                                 ctypes.byref(b)), "ccdgpu_autotune")
+        return self.schedule(), a.value, b.value
+
     TRACE_KERNELS = ["ring_small", "ring_mid", "ring_large", "hh_small", "hh_tiled", "onebody",
                      "ladder_thin", "ladder_mid", "ladder_wide", "ladder_tc", "assemble",
                      "loop_ctl", "energy", "retile"]

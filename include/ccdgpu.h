@@ -234,6 +234,23 @@ void *ccdgpu_stream(ccdgpu_handle *h);
 int ccdgpu_work_per_iteration(const ccdgpu_handle *h, double *flops, double *ladder_bytes,
                               double *ladder_flops);
 
+/* pp-ladder schedule (no counterpart in the reference): how far the K dimension of each
+ * channel block is split into deterministic partial sums, as a target of tiles per SM for the
+ * FP64 thin class (hh <= 8), the FP64 mid/wide classes, and the tensor-core ladder. */
+typedef struct ccdgpu_schedule {
+  int32_t thin_split_mul;      /* default 1 */
+  int32_t wide_split_mul;      /* default 3 */
+  int32_t tc_split_mul;        /* default 2 */
+  int32_t reserved[5];
+} ccdgpu_schedule;
+int ccdgpu_set_schedule(ccdgpu_handle *h, const ccdgpu_schedule *sch);
+int ccdgpu_get_schedule(const ccdgpu_handle *h, ccdgpu_schedule *sch);
+/* Autotuner: times `reps` launches of the pp ladders for every candidate schedule on this GPU
+ * and this problem (CUDA events), keeps the fastest and returns it with its times (ms per
+ * ladder launch, FP64 and tensor-core).  Amplitudes are not changed. */
+int ccdgpu_autotune(ccdgpu_handle *h, int32_t reps, ccdgpu_schedule *chosen, double *ms_fp64,
+                    double *ms_tc);
+
 /* Kernel start-time trace (diagnostics; no counterpart in the reference).  Arm with the index
  * of an iteration of the next solve (-1 disarms); every kernel of that iteration then records
  * the %globaltimer time (ns) at which its first and its last CTA started.  Kernel ids, in this

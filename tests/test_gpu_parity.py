@@ -165,3 +165,22 @@ def test_bad_table_is_rejected_before_any_launch():
         entry.row = saved
         with CCDSolver(s) as sol:
             assert sol.n_t2 == s.t2_size()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed_bf16"])
+def test_autotune_and_schedules_keep_results(precision):
+    """Every pp-ladder schedule reduces its split-K partial sums deterministically, so the
+    solve agrees with the reference whatever schedule the autotuner picks."""
+    g = golden("eg14_s19")
+    with system_for(g) as s, CCDSolver(s, precision=precision) as sol:
+        sch, ms64, mstc = sol.autotune(reps=2)
+        assert ms64 > 0 and (mstc > 0 or precision == "fp64")
+        assert sol.schedule() == sch
+        res = sol.solve(tol=g["tol"])
+        assert abs(res.e_corr - g["energies"][-1]) <= 1e-10 * abs(g["energies"][-1])
+        for sch2 in [dict(thin_split_mul=4, wide_split_mul=12, tc_split_mul=8),
+                     dict(thin_split_mul=1, wide_split_mul=1, tc_split_mul=1)]:
+            sol.set_schedule(**sch2)
+            sol.reset()
+            r2 = sol.solve(tol=g["tol"])
+            assert abs(r2.e_corr - g["energies"][-1]) <= 1e-10 * abs(g["energies"][-1])
