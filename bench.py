@@ -190,6 +190,9 @@ def main():
     ap.add_argument("--v-mode", default="stored", choices=["stored", "on_the_fly"],
                     help="on_the_fly: V_pppp generated on the device from the model (the host "
                          "builds and uploads none)")
+    ap.add_argument("--no-device-loop", action="store_true",
+                    help="replay per-iteration graphs instead of the device solve loop (for "
+                         "profilers, which cannot see kernels inside graph WHILE nodes)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default pp-ladder schedule instead of autotuning it")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -224,7 +227,7 @@ def main():
     arms = [args.precision] + ([p for p in PRECISIONS if p != args.precision]
                                if args.path == "fused" and not args.single_arm else [])
     solvers = {a: CCDSolver(system, device=local, path=args.path, precision=PRECISIONS[a],
-                            v_mode=args.v_mode)
+                            v_mode=args.v_mode, device_loop=not args.no_device_loop)
                for a in arms}
     stream = {a: torch.cuda.ExternalStream(solvers[a].stream_ptr(), device=local) for a in arms}
     # Autotuner: each arm's pp-ladder schedule picked by timing the candidates (untimed setup).
@@ -267,7 +270,9 @@ def main():
                 e0 = torch.cuda.Event(enable_timing=True)
                 e1 = torch.cuda.Event(enable_timing=True)
                 e0.record(st)
+                torch.cuda.nvtx.range_push("timed_solve")  # profilers: ncu --nvtx-include
                 last = sol.solve(tol=tol, max_iters=100, mixing=0.5)
+                torch.cuda.nvtx.range_pop()
                 e1.record(st)
                 e1.synchronize()
                 dev_ms += e0.elapsed_time(e1)
@@ -308,7 +313,7 @@ def main():
     for k in range(args.warmup + args.steps):
         t0 = time.perf_counter()
         s2 = CCDSolver(system, device=local, path=args.path, precision=PRECISIONS[arms[0]],
-                       v_mode=args.v_mode)
+                       v_mode=args.v_mode, device_loop=not args.no_device_loop)
         r2 = s2.solve(tol=tol, max_iters=100, mixing=0.5)
         s2.t2(host_t2)
         s2.close()
@@ -388,6 +393,8 @@ def main():
                        "abs_de_per_particle_vs_fp64_converged": t["de_per_particle"],
                        "time_to_converge_ms": t["max_ms"] / args.steps,
                        "l2": "flushed (256 MiB write) before every step",
+                       "solve_loop": ("batched graph replay" if args.no_device_loop else
+                                      "device (graph WHILE nodes)"),
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "arms": arms_out,
             "e2e": {"value": e2e_i.item() / e2e_t.item(), "unit": "iter/s",

@@ -60,7 +60,8 @@ class Problem(ctypes.Structure):
 
 class Options(ctypes.Structure):
     _fields_ = [("device", c_i32), ("precision", c_i32), ("v_mode", c_i32), ("path", c_i32),
-                ("polish_threshold", c_dbl), ("use_graph", c_i32), ("reserved", c_i32 * 7)]
+                ("polish_threshold", c_dbl), ("use_graph", c_i32), ("device_loop", c_i32),
+                ("reserved", c_i32 * 6)]
 
 
 class Schedule(ctypes.Structure):

@@ -1216,6 +1216,7 @@ void ccdgpu_default_options(ccdgpu_options *opt) {
   opt->path = CCDGPU_PATH_FUSED;
   opt->polish_threshold = 1e-6;
   opt->use_graph = 1;
+  opt->device_loop = 1;
 }
 
 const char *ccdgpu_strerror(int status) {
@@ -1375,8 +1376,8 @@ int solve_begin(ccdgpu_handle *h, double tol, int64_t max_iters, double mixing, 
   int rc = set_ctl(h, 1, tol, max_iters, mixing, true, -1, st.mixed ? 1 : 0);
   if (rc) return rc;
   st.graph = st.fused && h->opt.use_graph && !h->profiling;
-  if (st.graph) ready_loop_graphs(h);
-  st.device_loop = st.graph && h->loop_state == 1;
+  if (st.graph && h->opt.device_loop) ready_loop_graphs(h);
+  st.device_loop = st.graph && h->opt.device_loop && h->loop_state == 1;
   if (st.graph && !st.device_loop && (rc = fused_ready_graph(h, false))) return rc;
   if (st.graph && !st.device_loop && st.mixed && (rc = fused_ready_graph(h, true))) return rc;
   st.t0 = std::chrono::steady_clock::now();

@@ -76,7 +76,7 @@ def solve_batch(solvers, tol=1e-8, max_iters=100, mixing=0.5, check=True):
 
 class CCDSolver:
     def __init__(self, system, precision="fp64", path="fused", v_mode="stored", device=0,
-                 use_graph=True, polish_threshold=1e-6):
+                 use_graph=True, polish_threshold=1e-6, device_loop=True):
         lib = _native.gpu_lib()
         self.system = system  # keeps the host problem alive during create
         opt = _native.Options()
@@ -86,6 +86,7 @@ class CCDSolver:
         opt.path = PATH[path]
         opt.v_mode = VMODE[v_mode]
         opt.use_graph = int(bool(use_graph))
+        opt.device_loop = int(bool(device_loop))
         opt.polish_threshold = polish_threshold
         self._h = ctypes.c_void_p()
         _check(lib.ccdgpu_create(system.problem, ctypes.byref(opt), ctypes.byref(self._h)),

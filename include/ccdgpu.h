@@ -127,7 +127,10 @@ typedef struct ccdgpu_options {
   double polish_threshold;     /* mixed: switch to FP64 iterations once |dE| <= max(tol,
                                   polish_threshold * |E|) or |dE| stops decreasing */
   int32_t use_graph;           /* capture one iteration as a CUDA graph (fused path) */
-  int32_t reserved[7];
+  int32_t device_loop;         /* with use_graph: run the whole solve loop on the device (graph
+                                  WHILE nodes, default 1); 0 replays per-iteration graphs in
+                                  batches (profilers cannot see kernels inside WHILE nodes) */
+  int32_t reserved[6];
 } ccdgpu_options;
 
 typedef struct ccdgpu_result {
