@@ -20,7 +20,7 @@ namespace ccd {
 //                         tile of a channel is stored compact (only its real rows).
 //   B tiles  [kBK][nb]    k-major, nb = padded hh columns, read as warp broadcasts.
 // Column classes: thin channels (hh <= 8) use nb in {2, 4, 8} with one row per consumer
-// thread; wide channels use nb = 8*cg with cg rows x 8 columns per consumer thread.
+// thread; the others nb = 8*C with 8 rows x C columns per consumer thread (k-major A).
 constexpr int kBK = 16;        // K depth of one pipeline stage
 constexpr int kStages = 4;     // bulk-copy pipeline depth
 constexpr int kMaxCG = 9;      // column groups of 8 -> up to 72 hh columns
@@ -34,14 +34,18 @@ __host__ __device__ inline int swzA(int row, int k) { return row * kBK + (k ^ (r
 __host__ __device__ inline int ladder_nb(int hh) {
   return hh <= 2 ? 2 : hh <= 4 ? 4 : 8 * ((hh + 7) / 8);
 }
-// Rows per consumer thread for a wide channel with cg column groups of 8.
-__host__ __device__ constexpr int ladder_tm(int cg) { return cg <= 4 ? cg : 4; }
-// Rows per tile: thin channels one row per consumer thread; wide ones ladder_tm(cg) rows x 8
-// columns per thread, 128/cg row groups.
-__host__ __device__ inline int ladder_bm(int nb) {
-  if (nb <= 8) return kLadderConsumers;
-  const int cg = nb / 8;
-  return (kLadderConsumers / cg) * ladder_tm(cg);
+// Rows per tile: thin channels one row per consumer thread; mid and wide ones (nb >= 16)
+// 8 rows x nb/8 columns per thread, 16 row groups.
+__host__ __device__ inline int ladder_bm(int nb) { return kLadderConsumers; }
+// A chunks of mid and wide channels are k-major with the rows padded to a multiple of 8 (a
+// thread reads its 8 consecutive rows as 16-byte vectors); thin ones are row-major and
+// XOR-swizzled (one row per thread).
+__host__ __device__ inline bool ladder_kmajor(int nb) { return nb >= 16; }
+__host__ __device__ inline int ladder_arows(int nb, int rows) {
+  return ladder_kmajor(nb) ? ((rows + 7) & ~7) : rows;
+}
+__host__ __device__ inline int ladder_aoff(int nb, int arows, int r, int k) {
+  return ladder_kmajor(nb) ? k * arows + r : swzA(r, k);
 }
 
 // Mixed-precision pp-ladder images (tensor-core operands, ccd_tc.cuh).  A K chunk of a
@@ -83,7 +87,7 @@ __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16 *out, int nt)
 // nseg-1 also runs the T X chunks.
 struct LadderTile {
   int32_t ch, mt, kc0, nks, nkc, nkh, nb, bm, rows, pr, hh, seg, nseg, group;
-  int64_t v_base;    // A tiles of V:  tile base + kc * rows*kBK (tile base = mt*bm*nkc*kBK)
+  int64_t v_base;    // A tiles of V:  tile base + kc * arows*kBK (tile base = mt*bm*nkc*kBK)
   int64_t tkt_base;  // B tiles of T:  + kc * kBK*nb
   int64_t tmt_base;  // A tiles of T (rows a<=b, K = hh): + mt*bm*nkh*kBK + kh * rows*kBK
   int64_t xt_base;   // B tiles of X/2: + kh * kBK*nb

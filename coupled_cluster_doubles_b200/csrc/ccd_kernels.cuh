@@ -214,21 +214,22 @@ __device__ __forceinline__ bool consume_thin(const LadderTile &tile, const doubl
   return true;
 }
 
-// Wide channels (nb = 8*CG): consumer thread = ladder_tm(CG) rows (strided by the row-group
-// count) x 8 columns; V values are reused across the CG column groups, T values across rows.
-template <int CG>
-__device__ __forceinline__ bool consume_wide(const LadderTile &tile, const double *As,
-                                             const double *Bs, int bstage, uint64_t *bars,
-                                             int tid, const LadderOut &out, int32_t *err) {
-  constexpr int TM = ladder_tm(CG), RG = kLadderConsumers / CG, NB = 8 * CG;
-  const int rg = tid / CG, cg = tid - rg * CG;
-  const bool worker = rg < RG;
-  const int lane = tid & 31;
-  double acc[TM][8];
+// Mid and wide channels (nb = 8*C, C = 2..9): 16 row groups of 8 consecutive rows x 8 column groups of
+// C columns; A is k-major in shared memory (ladder_aoff), so a thread reads its 8 rows with four
+// 16-byte loads and runs 8*C independent FMAs per k.
+template <int C>
+__device__ __forceinline__ bool consume_wide8(const LadderTile &tile, const double *As,
+                                              const double *Bs, int bstage, uint64_t *bars,
+                                              int tid, const LadderOut &out, int32_t *err) {
+  constexpr int NB = 8 * C;
+  const int r0 = (tid >> 3) * 8, c0 = (tid & 7) * C, lane = tid & 31;
+  const int ar = ladder_arows(NB, tile.rows);
+  const bool worker = r0 < ar;
+  double acc[8][C];
 #pragma unroll
-  for (int i = 0; i < TM; ++i)
+  for (int i = 0; i < 8; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < C; ++j) acc[i][j] = 0.0;
   const int nchunks = tile.nks + tile.nkh;
   for (int c = 0; c < nchunks; ++c) {
     const int s = c % kStages;
@@ -236,26 +237,24 @@ __device__ __forceinline__ bool consume_wide(const LadderTile &tile, const doubl
       atomicOr(err, kErrTimeout);
       return false;
     }
-    const double *A = As + s * (kMaxBM * kBK);
-    const double *B = Bs + s * bstage;
+    const double *A = As + s * (kMaxBM * kBK) + r0;
+    const double *B = Bs + s * bstage + c0;
     if (worker) {
-#pragma unroll 4
+#pragma unroll 2
       for (int k = 0; k < kBK; ++k) {
-        double a[TM];
+        double a[8], b[C];
 #pragma unroll
-        for (int i = 0; i < TM; ++i) a[i] = A[swzA(rg + i * RG, k)];
-        const double2 *bp = reinterpret_cast<const double2 *>(B + k * NB + cg * 8);
-        double b[8];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const double2 v = bp[j];
-          b[2 * j] = v.x;
-          b[2 * j + 1] = v.y;
+        for (int i = 0; i < 4; ++i) {
+          const double2 v = *reinterpret_cast<const double2 *>(A + k * ar + 2 * i);
+          a[2 * i] = v.x;
+          a[2 * i + 1] = v.y;
         }
 #pragma unroll
-        for (int i = 0; i < TM; ++i)
+        for (int j = 0; j < C; ++j) b[j] = B[k * NB + j];
 #pragma unroll
-          for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int j = 0; j < C; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
       }
     }
     __syncwarp();
@@ -263,7 +262,7 @@ __device__ __forceinline__ bool consume_wide(const LadderTile &tile, const doubl
   }
   if (worker) {
 #pragma unroll
-    for (int i = 0; i < TM; ++i) out.row(rg + i * RG, cg * 8, acc[i], 8);
+    for (int i = 0; i < 8; ++i) out.row(r0 + i, c0, acc[i], C);
   }
   return true;
 }
@@ -271,7 +270,7 @@ __device__ __forceinline__ bool consume_wide(const LadderTile &tile, const doubl
 // Column classes: CLS 0 = thin (nb <= 8), 1 = mid (nb 16..32), 2 = wide (nb 40..72).  Separate
 // instantiations keep the register budget of narrow channels independent of the 72-column case.
 template <int CLS>
-__global__ void __launch_bounds__(kLadderThreads, CLS == 0 ? 3 : 2)
+__global__ void __launch_bounds__(kLadderThreads, CLS == 0 ? 3 : CLS == 1 ? 2 : 1)
 pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict__ v_t,
                  const double *__restrict__ t_kt, const double *__restrict__ t_mt,
                  const double *__restrict__ x_t, const int32_t *__restrict__ rowmap,
@@ -297,7 +296,8 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict_
 
   if (warp == kLadderConsumers / 32) {
     if (lane == 0) {
-      const uint32_t abytes = tile.rows * kBK * 8, bbytes = kBK * tile.nb * 8;
+      const int ar = ladder_arows(tile.nb, tile.rows);
+      const uint32_t abytes = ar * kBK * 8, bbytes = kBK * tile.nb * 8;
       const int nchunks = tile.nks + tile.nkh;
       const int64_t vtile = tile.v_base + (int64_t)tile.mt * tile.bm * tile.nkc * kBK;
       const int64_t ttile = tile.tmt_base + (int64_t)tile.mt * tile.bm * tile.nkh * kBK;
@@ -310,11 +310,11 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict_
         const double *asrc, *bsrc;
         if (c < tile.nks) {
           const int kc = tile.kc0 + c;
-          asrc = v_t + vtile + (int64_t)kc * tile.rows * kBK;
+          asrc = v_t + vtile + (int64_t)kc * ar * kBK;
           bsrc = t_kt + tile.tkt_base + (int64_t)kc * kBK * tile.nb;
         } else {
           const int kh = c - tile.nks;
-          asrc = t_mt + ttile + (int64_t)kh * tile.rows * kBK;
+          asrc = t_mt + ttile + (int64_t)kh * ar * kBK;
           bsrc = x_t + tile.xt_base + (int64_t)kh * kBK * tile.nb;
         }
         const uint32_t full = smem_u32(&bars[s]);
@@ -335,17 +335,17 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict_
       default: ok = consume_thin<8>(tile, As, Bs, bstage, bars, tid, out, err); break;
     }
   } else {
-#define CCD_WIDE_CASE(n) \
-  case n: ok = consume_wide<n>(tile, As, Bs, bstage, bars, tid, out, err); break;
+#define CCD_WIDE8_CASE(n) \
+  case n: ok = consume_wide8<n>(tile, As, Bs, bstage, bars, tid, out, err); break;
     if (CLS == 1) {
-      switch (tile.nb / 8) { CCD_WIDE_CASE(2) CCD_WIDE_CASE(3) CCD_WIDE_CASE(4) default: break; }
+      switch (tile.nb / 8) { CCD_WIDE8_CASE(2) CCD_WIDE8_CASE(3) CCD_WIDE8_CASE(4) default: break; }
     } else {
       switch (tile.nb / 8) {
-        CCD_WIDE_CASE(5) CCD_WIDE_CASE(6) CCD_WIDE_CASE(7) CCD_WIDE_CASE(8) CCD_WIDE_CASE(9)
+        CCD_WIDE8_CASE(5) CCD_WIDE8_CASE(6) CCD_WIDE8_CASE(7) CCD_WIDE8_CASE(8) CCD_WIDE8_CASE(9)
         default: break;
       }
     }
-#undef CCD_WIDE_CASE
+#undef CCD_WIDE8_CASE
   }
   if (tile.nseg > 1) {
     if (!ok) return;  // a timed-out tile leaves its row block unfinished (error already set)
@@ -813,8 +813,9 @@ __device__ __forceinline__ void write_t_tiles(const ChanInfo &ch, const int2 *__
   if (q.x >= 0) t_kt[ch.tkt_base + (int64_t)(q.x / kBK) * kBK * ch.nb + (q.x % kBK) * ch.nb + ij] = t;
   if (q.y >= 0) {
     const int mt = q.y / ch.bm, rows = min(ch.bm, ch.pr - mt * ch.bm);
-    t_mt[ch.tmt_base + (int64_t)mt * ch.bm * ch.nkh * kBK + (int64_t)(ij / kBK) * rows * kBK +
-         swzA(q.y - mt * ch.bm, ij % kBK)] = t;
+    const int ar = ladder_arows(ch.nb, rows);
+    t_mt[ch.tmt_base + (int64_t)mt * ch.bm * ch.nkh * kBK + (int64_t)(ij / kBK) * ar * kBK +
+         ladder_aoff(ch.nb, ar, q.y - mt * ch.bm, ij % kBK)] = t;
   }
 }
 

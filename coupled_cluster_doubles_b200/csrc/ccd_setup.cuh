@@ -39,9 +39,11 @@ __global__ void tile_v_kernel(const ChanInfo *__restrict__ chans, const int2 *__
   const int ab = rowmap[ch.row_off + u];
   const double *src = vraw + vraw_off[it.x] + (int64_t)ab * ch.pp;
   const int mt = u / ch.bm, rows = min(ch.bm, ch.pr - mt * ch.bm);
+  const int ar = ladder_arows(ch.nb, rows);
   const int64_t tb = ch.vkt_base + (int64_t)mt * ch.bm * ch.nkc * kBK;
   for (int w = threadIdx.x; w < ch.pk; w += blockDim.x)
-    v_t[tb + (int64_t)(w / kBK) * rows * kBK + swzA(u - mt * ch.bm, w % kBK)] = src[kcol[ch.pk_off + w]];
+    v_t[tb + (int64_t)(w / kBK) * ar * kBK + ladder_aoff(ch.nb, ar, u - mt * ch.bm, w % kBK)] =
+        src[kcol[ch.pk_off + w]];
 }
 
 // Packed V_pppp as nt bf16 terms in the tensor-core chunk images of the mixed-precision
@@ -146,6 +148,7 @@ __global__ void gen_v_kernel(const ChanInfo *__restrict__ chans, const int2 *__r
   const int u = it.y;
   const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + u]];
   const int mt = u / ch.bm, rows = min(ch.bm, ch.pr - mt * ch.bm);
+  const int ar = ladder_arows(ch.nb, rows);
   const int64_t tb = ch.vkt_base + (int64_t)mt * ch.bm * ch.nkc * kBK;
   const int mtc = u >> 7, r = u & 127;
   const int rg = (min(kTcBM, ch.pr - mtc * kTcBM) + 7) >> 3;
@@ -153,7 +156,7 @@ __global__ void gen_v_kernel(const ChanInfo *__restrict__ chans, const int2 *__r
   for (int w = threadIdx.x; w < ch.pk; w += blockDim.x) {
     const int2 cd = pp_pairs[ch.pp_off + kcol[ch.pk_off + w]];
     const double v = tbme_dev(m, ab.x, ab.y, cd.x, cd.y);
-    v_t[tb + (int64_t)(w / kBK) * rows * kBK + swzA(u - mt * ch.bm, w % kBK)] = v;
+    v_t[tb + (int64_t)(w / kBK) * ar * kBK + ladder_aoff(ch.nb, ar, u - mt * ch.bm, w % kBK)] = v;
     if (nt) {
       __nv_bfloat16 hv[3];
       split_bf16(v, hv, nt);

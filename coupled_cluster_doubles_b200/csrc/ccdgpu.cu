@@ -449,9 +449,12 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     const int nb = ci.nb;
     pp_tot += pp; hh_tot += hh; x_tot += hh * hh;
     tkt += (int64_t)ci.nkc * kBK * nb;
-    tmt += (int64_t)ci.nkh * ci.pr * kBK;  // compact row tiles
+    // Compact last row tile (rows padded to 8 for k-major wide channels).
+    const int64_t arows_tot = (int64_t)(ci.nmt - 1) * ci.bm +
+                              ladder_arows(ci.nb, ci.pr - (ci.nmt - 1) * ci.bm);
+    tmt += (int64_t)ci.nkh * arows_tot * kBK;
     xt += (int64_t)ci.nkh * kBK * nb;
-    vt += (int64_t)ci.nkc * ci.pr * kBK;
+    vt += (int64_t)ci.nkc * arows_tot * kBK;
     part_tot += (int64_t)ci.nhht * hh * hh;
     vraw_off.push_back(vraw_tot);
     if (!on_the_fly) vraw_tot += pp * pp;
