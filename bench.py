@@ -303,6 +303,7 @@ def main():
         prof[a] = sol.profile()
         sol.enable_profiling(False)
         work[a] = sol.work_per_iteration()
+    ladder_cls = {a: solvers[a].ladder_profile(reps=5) for a in arms}
     n_t2 = solvers[arms[0]].n_t2
 
     # e2e (headline arm): the public API from host buffers, every step: create (H2D upload)
@@ -365,12 +366,20 @@ def main():
                 "schedule": tuned[a][0],
                 "schedule_source": "autotuned" if not args.no_autotune else "default",
             }
+        for a in arms:
+            # Each ladder class alone: executed rate (packed rows a<=b, K over c<d and hh) and
+            # bandwidth; the FP64 wide class holds the largest channels (hh 36..72).
+            cls = {}
+            for name, (ms, fl, by) in ladder_cls[a].items():
+                cls[name] = {"ms": ms, "tflops_executed": fl / (ms / 1000.0) / 1e12,
+                             "gbs": by / (ms / 1000.0) / 1e9}
+                if name.startswith("fp64"):
+                    cls[name]["frac_of_fp64_peak"] = cls[name]["tflops_executed"] / FP64_PEAK_TFLOPS
+                else:
+                    cls[name]["frac_of_hbm_peak"] = cls[name]["gbs"] / peaks["hbm_gbs"]
+            arms_out[a]["pp_ladder_classes_alone"] = cls
         if "fp64" in arms_out:
-            # Executed FP64 rate: the antisymmetry-packed ladder runs about a quarter of the
-            # reference's 2 pp^2 hh flops (rows a<=b, K over c<d).
             f = arms_out["fp64"]
-            f["pp_ladder_tflops_executed_approx"] = f["pp_ladder_tflops_algorithmic"] / 4
-            f["pp_ladder_frac_of_fp64_peak"] = f["pp_ladder_tflops_executed_approx"] / FP64_PEAK_TFLOPS
             f["fp64_peak_tflops"] = FP64_PEAK_TFLOPS
         cpu = None
         if not args.no_cpu_baseline:

@@ -122,7 +122,7 @@ __device__ __forceinline__ bool skip_iteration(const Control *ctl, int gate, int
 // threads run register-blocked DFMAs: V rows come from shared memory conflict-free (XOR
 // swizzle), T / X columns are warp broadcasts.  K runs over the c<d pairs (V T) and then over
 // hh (T X) with the same pipeline.  Row blocks whose K is split over several tiles write
-// partial sums that the last tile to finish adds in segment order (deterministic).
+// partial sums that ladder_reduce_kernel adds in segment order (deterministic).
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ void consumers_sync() {
   asm volatile("bar.sync 1, %0;" ::"n"(kLadderConsumers) : "memory");
@@ -151,30 +151,35 @@ struct LadderOut {
   }
 };
 
-// After partial sums are written: the last tile of the row block adds them in order.
-__device__ __forceinline__ void ladder_reduce(const LadderTile &tile, int tid, int32_t *counters,
-                                              const int32_t *rowmap, const int32_t *mirror,
-                                              double *d, const double *part) {
-  __shared__ int last;
-  __threadfence();
-  consumers_sync();
-  if (tid == 0) last = (atomicAdd(&counters[tile.group], 1) == tile.nseg - 1);
-  consumers_sync();
-  if (!last) return;
-  __threadfence();
-  const int n = tile.rows * tile.nb;
-  for (int e = tid; e < n; e += kLadderConsumers) {
-    const int u_local = e / tile.nb, col = e - u_local * tile.nb;
+// Split-K partial sums of a row block, added in segment order by ladder_reduce_kernel after the
+// ladder: item = (first tile of the row block, first row of a kRedRows-row chunk).
+struct RedItem {
+  int32_t tile, r0;
+};
+constexpr int kRedRows = 16;
+
+// D rows of split row blocks: sum of the segments' partials in segment order (deterministic),
+// written to row ab and negated to its mirror ba.  Fully parallel over (row block, row chunk).
+__global__ void __launch_bounds__(256)
+ladder_reduce_kernel(const RedItem *__restrict__ items, const LadderTile *__restrict__ tiles,
+                     const int32_t *__restrict__ rowmap, const int32_t *__restrict__ mirror,
+                     double *__restrict__ d, const double *__restrict__ part, const Control *ctl,
+                     int gate) {
+  if (skip_iteration(ctl, gate, kTrReduce)) return;
+  const RedItem it = items[blockIdx.x];
+  const LadderTile tile = tiles[it.tile];
+  const int nr = min(kRedRows, tile.rows - it.r0), n = nr * tile.nb;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    const int u_local = it.r0 + e / tile.nb, col = e % tile.nb;
     if (col >= tile.hh) continue;
     double v = 0.0;
     for (int sg = 0; sg < tile.nseg; ++sg)
-      v += __ldcg(part + tile.part_base + ((int64_t)sg * tile.bm + u_local) * tile.nb + col);
+      v += part[tile.part_base + ((int64_t)sg * tile.bm + u_local) * tile.nb + col];
     const int u = tile.mt * tile.bm + u_local;
     const int ab = rowmap[tile.row_off + u], mir = mirror[tile.row_off + u];
     d[tile.t_off + (int64_t)ab * tile.hh + col] = v;
     if (mir >= 0) d[tile.t_off + (int64_t)mir * tile.hh + col] = -v;
   }
-  if (tid == 0) counters[tile.group] = 0;
 }
 
 // Thin channels (nb in {2,4,8}): consumer thread = one packed row, all nb columns.
@@ -347,10 +352,7 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict_
     }
 #undef CCD_WIDE8_CASE
   }
-  if (tile.nseg > 1) {
-    if (!ok) return;  // a timed-out tile leaves its row block unfinished (error already set)
-    ladder_reduce(tile, tid, counters, rowmap, mirror, d, part);
-  }
+  (void)ok;  // a timed-out tile leaves its row block unfinished (error already set)
 }
 
 // ------------------------------------------------------------------------------------------

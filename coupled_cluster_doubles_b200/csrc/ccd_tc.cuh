@@ -239,7 +239,7 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const __nv_bfloat16 *_
     const int tid = threadIdx.x;
     const LadderOut out{tile, rowmap, mirror, d, part};
     if (!ok) atomicOr(err, kErrTimeout);
-    // One decision for all four warps (ladder_reduce synchronises them again).
+    // One decision for all four warps (tcgen05.ld is warp-collective).
     if (consumers_all(ok && !read_flag(&abort_flag) && nchunks > 0)) {
       const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
       for (int c0 = 0; c0 < tile.nb; c0 += 16) {
@@ -250,7 +250,6 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const __nv_bfloat16 *_
         for (int i = 0; i < 16; ++i) dv[i] = (double)v[i];
         out.row(tid, c0, dv, 16);
       }
-      if (tile.nseg > 1) ladder_reduce(tile, tid, counters, rowmap, mirror, d, part);
     }
   }
   tc_fence_before();

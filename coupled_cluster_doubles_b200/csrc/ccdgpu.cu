@@ -100,6 +100,8 @@ struct ccdgpu_handle {
   std::vector<ChanInfo> host_chans;
   ccdgpu_schedule schedule{};
   void *tile_mem = nullptr;
+  RedItem *red_fp = nullptr, *red_tc = nullptr;  // split-K reduction items
+  int n_red_fp = 0, n_red_tc = 0, n_red_cls[3] = {0, 0, 0};
 
   // Mixed precision (nt bf16 terms per operand; 0 for an FP64 handle).
   int nt = 0;
@@ -234,7 +236,8 @@ int upload_runs(ccdgpu_handle *h, T *dst, const std::vector<const T *> &src,
 //   the class has about wide_split_mul tiles per SM.
 //   Tensor-core ladder: each CTA is bandwidth bound, so K is split until there are about
 //   tc_split_mul tiles per SM.
-// Split tiles are reduced deterministically (ladder_reduce).
+// Split row blocks are reduced after the ladder by ladder_reduce_kernel (segment order, so
+// deterministic), one item per (row block, 16-row chunk), FP64 items grouped by class.
 int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
   const std::vector<ChanInfo> &chans = h->host_chans;
   auto cls_of = [](int nb) { return nb <= 8 ? 0 : nb <= 32 ? 1 : 2; };
@@ -316,6 +319,28 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
       return (int64_t)(x.nks + x.nkh) * (x.rows + x.nb) > (int64_t)(y.nks + y.nkh) * (y.rows + y.nb);
     });
   }
+  // Reduction items of split row blocks.
+  auto red_items = [](const std::vector<LadderTile> &tl, std::vector<RedItem> &out, int *per_cls,
+                      bool by_class, int (*cls)(int)) {
+    std::vector<std::vector<RedItem>> parts(by_class ? 3 : 1);
+    std::vector<char> seen;
+    for (size_t i = 0; i < tl.size(); i++) {
+      const LadderTile &t = tl[i];
+      if (t.nseg <= 1) continue;
+      if ((size_t)t.group >= seen.size()) seen.resize(t.group + 1, 0);
+      if (seen[t.group]) continue;
+      seen[t.group] = 1;
+      for (int r0 = 0; r0 < t.rows; r0 += kRedRows)
+        parts[by_class ? cls(t.nb) : 0].push_back({(int32_t)i, r0});
+    }
+    for (size_t k = 0; k < parts.size(); k++) {
+      if (per_cls) per_cls[k] = (int)parts[k].size();
+      out.insert(out.end(), parts[k].begin(), parts[k].end());
+    }
+  };
+  std::vector<RedItem> red_fp, red_tc;
+  red_items(tiles, red_fp, h->n_red_cls, true, [](int nb) { return nb <= 8 ? 0 : nb <= 32 ? 1 : 2; });
+  red_items(tc_tiles, red_tc, nullptr, false, nullptr);
   // Device copies: one allocation, counters zeroed.
   CK(cudaStreamSynchronize(h->s0));
   if (h->tile_mem) CK(cudaFree(h->tile_mem));
@@ -324,6 +349,7 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
   ar.add(&h->tiles, tiles.size()); ar.add(&h->lcounters, groups); ar.add(&h->lpart, lpart_tot);
   ar.add(&h->tc_tiles, tc_tiles.size()); ar.add(&h->tc_counters, tc_groups);
   ar.add(&h->tc_part, tcpart_tot);
+  ar.add(&h->red_fp, red_fp.size()); ar.add(&h->red_tc, red_tc.size());
   CK(cudaMalloc(&h->tile_mem, ar.used));
   CK(cudaMemsetAsync(h->tile_mem, 0, ar.used, h->s0));
   for (auto &r : ar.reqs) *r.first = static_cast<char *>(h->tile_mem) + r.second;
@@ -333,6 +359,14 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
   if (!tc_tiles.empty())
     CK(cudaMemcpyAsync(h->tc_tiles, tc_tiles.data(), tc_tiles.size() * sizeof(LadderTile),
                        cudaMemcpyHostToDevice, h->s0));
+  if (!red_fp.empty())
+    CK(cudaMemcpyAsync(h->red_fp, red_fp.data(), red_fp.size() * sizeof(RedItem),
+                       cudaMemcpyHostToDevice, h->s0));
+  if (!red_tc.empty())
+    CK(cudaMemcpyAsync(h->red_tc, red_tc.data(), red_tc.size() * sizeof(RedItem),
+                       cudaMemcpyHostToDevice, h->s0));
+  h->n_red_fp = (int)red_fp.size();
+  h->n_red_tc = (int)red_tc.size();
   CK(cudaStreamSynchronize(h->s0));
   h->n_tiles = (int)tiles.size();
   h->n_cls[0] = h->n_cls[1] = h->n_cls[2] = 0;
@@ -868,14 +902,23 @@ int launch_pp_ladder_tc(ccdgpu_handle *h, cudaStream_t st) {
   if (!h->n_tc_tiles) return CCDGPU_OK;
   h->launches++;
   if (h->nt == 2)
-    return cuda_status(launch_pdl(pp_ladder_tc_kernel<2>, h->n_tc_tiles, kTcThreads, h->tc_smem,
-                                  st, h->tc_tiles, h->v_tc, h->n_vtc, h->tkt_tc, h->n_tkttc,
-                                  h->tmt_tc, h->n_tmttc, h->xt_tc, h->n_xttc, h->rowmap,
-                                  h->mirror, h->dmat, h->tc_part, h->tc_counters, h->ctl, h->err));
-  return cuda_status(launch_pdl(pp_ladder_tc_kernel<3>, h->n_tc_tiles, kTcThreads, h->tc_smem,
-                                st, h->tc_tiles, h->v_tc, h->n_vtc, h->tkt_tc, h->n_tkttc,
-                                h->tmt_tc, h->n_tmttc, h->xt_tc, h->n_xttc, h->rowmap, h->mirror,
-                                h->dmat, h->tc_part, h->tc_counters, h->ctl, h->err));
+    CK(launch_pdl(pp_ladder_tc_kernel<2>, h->n_tc_tiles, kTcThreads, h->tc_smem, st,
+                  h->tc_tiles, h->v_tc, h->n_vtc, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc,
+                  h->xt_tc, h->n_xttc, h->rowmap, h->mirror, h->dmat, h->tc_part,
+                  h->tc_counters, h->ctl, h->err));
+  else
+    CK(launch_pdl(pp_ladder_tc_kernel<3>, h->n_tc_tiles, kTcThreads, h->tc_smem, st,
+                  h->tc_tiles, h->v_tc, h->n_vtc, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc,
+                  h->xt_tc, h->n_xttc, h->rowmap, h->mirror, h->dmat, h->tc_part,
+                  h->tc_counters, h->ctl, h->err));
+  if (h->n_red_tc) {
+    CK(launch_pdl(ladder_reduce_kernel, h->n_red_tc, 256, 0, st, (const RedItem *)h->red_tc,
+                  (const LadderTile *)h->tc_tiles, (const int32_t *)h->rowmap,
+                  (const int32_t *)h->mirror, h->dmat, (const double *)h->tc_part,
+                  (const Control *)h->ctl, 1));
+    h->launches++;
+  }
+  return CCDGPU_OK;
 }
 // The three column classes run concurrently: mid and wide go to stream s2 (wide first, they
 // are the longest tiles), thin to `st`; s2 is joined back into `st` before returning.
@@ -917,6 +960,13 @@ int launch_pp_ladder(ccdgpu_handle *h, cudaStream_t st) {
     h->launches++;
   }
   if (side) CK(cudaStreamWaitEvent(st, h->ev_join2, 0));
+  if (h->n_red_fp) {
+    CK(launch_pdl(ladder_reduce_kernel, h->n_red_fp, 256, 0, st, (const RedItem *)h->red_fp,
+                  (const LadderTile *)h->tiles, (const int32_t *)h->rowmap,
+                  (const int32_t *)h->mirror, h->dmat, (const double *)h->lpart,
+                  (const Control *)h->ctl, 0));
+    h->launches++;
+  }
   return CCDGPU_OK;
 }
 
@@ -1595,6 +1645,60 @@ int ccdgpu_enable_profiling(ccdgpu_handle *h, int32_t on) {
   return CCDGPU_OK;
 }
 void *ccdgpu_stream(ccdgpu_handle *h) { return h ? (void *)h->s0 : nullptr; }
+
+// Each pp-ladder class launched alone (FP64 thin, mid, wide; tensor-core ladder), `reps` times
+// between CUDA events on the handle's stream; with the executed flops (packed: rows a<=b, K over
+// c<d and hh) and the algorithmic bytes of each class.
+int ccdgpu_ladder_profile(ccdgpu_handle *h, int32_t reps, double *ms, double *flops,
+                          double *bytes) {
+  if (!h || reps < 1 || !ms || !flops || !bytes) return CCDGPU_ERR_INVALID_ARGUMENT;
+  CK(cudaSetDevice(h->opt.device));
+  int rc = set_ctl(h, 0, h->h_ctl->tol, h->h_ctl->max_iters, h->h_ctl->mixing, false);
+  if (rc) return rc;
+  for (int k = 0; k < 4; k++) ms[k] = flops[k] = bytes[k] = 0;
+  for (const ChanInfo &a : h->host_chans) {
+    const int k = a.nb <= 8 ? 0 : a.nb <= 32 ? 1 : 2;
+    const double f = 2.0 * a.pr * ((double)a.pk + a.hh) * a.hh;
+    const double b = (double)a.pr * a.pk + ((double)a.pk + a.pr) * a.hh + (double)a.hh * a.hh;
+    flops[k] += f;
+    bytes[k] += 8.0 * b + 8.0 * a.pp * a.hh;
+    if (h->nt) {
+      flops[3] += f;
+      bytes[3] += 2.0 * h->nt * b + 8.0 * a.pp * a.hh;
+    }
+  }
+  const LadderTile *start[3] = {h->tiles, h->tiles + h->n_cls[0], h->tiles + h->n_cls[0] + h->n_cls[1]};
+  for (int k = 0; k < 4; k++) {
+    if (k < 3 && !h->n_cls[k]) continue;
+    if (k == 3 && !h->n_tc_tiles) continue;
+    auto launch = [&]() -> int {
+      if (k == 3) return launch_pp_ladder_tc(h, h->s0);
+      const size_t smem = k == 0 ? h->ladder_smem_thin : h->ladder_smem;
+      auto kern = k == 0 ? pp_ladder_kernel<0> : k == 1 ? pp_ladder_kernel<1> : pp_ladder_kernel<2>;
+      kern<<<h->n_cls[k], kLadderThreads, smem, h->s0>>>(start[k], h->v_t, h->t_kt, h->t_mt, h->x_t,
+                                                        h->rowmap, h->mirror, h->dmat, h->lpart,
+                                                        h->lcounters, h->ctl, h->err, 0);
+      CK(cudaGetLastError());
+      if (h->n_red_cls[k]) {
+        const int off = k == 0 ? 0 : k == 1 ? h->n_red_cls[0] : h->n_red_cls[0] + h->n_red_cls[1];
+        ladder_reduce_kernel<<<h->n_red_cls[k], 256, 0, h->s0>>>(
+            h->red_fp + off, h->tiles, h->rowmap, h->mirror, h->dmat, h->lpart, h->ctl, 0);
+        CK(cudaGetLastError());
+      }
+      return CCDGPU_OK;
+    };
+    if ((rc = launch())) return rc;  // warm-up
+    CK(cudaEventRecord(h->ev[0], h->s0));
+    for (int i = 0; i < reps && !rc; i++) rc = launch();
+    if (rc) return rc;
+    CK(cudaEventRecord(h->ev[1], h->s0));
+    CK(cudaEventSynchronize(h->ev[1]));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, h->ev[0], h->ev[1]));
+    ms[k] = t / reps;
+  }
+  return check_errors(h);
+}
 
 int ccdgpu_set_schedule(ccdgpu_handle *h, const ccdgpu_schedule *sch) {
   if (!h || !sch || sch->thin_split_mul < 1 || sch->wide_split_mul < 1 || sch->tc_split_mul < 1)

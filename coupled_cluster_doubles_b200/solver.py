@@ -185,9 +185,17 @@ class CCDSolver:
                                                  ctypes.byref(b)), "ccdgpu_autotune")
         return self.schedule(), a.value, b.value
 
+    def ladder_profile(self, reps=5):
+        """Each pp-ladder class alone (ccdgpu_ladder_profile): {class: (ms, flops, bytes)}."""
+        ms, fl, by = (ctypes.c_double * 4)(), (ctypes.c_double * 4)(), (ctypes.c_double * 4)()
+        _check(_native.gpu_lib().ccdgpu_ladder_profile(self._h, reps, ms, fl, by),
+               "ccdgpu_ladder_profile")
+        names = ["fp64_thin", "fp64_mid", "fp64_wide", "tensor_core"]
+        return {n: (ms[k], fl[k], by[k]) for k, n in enumerate(names) if ms[k] > 0}
+
     TRACE_KERNELS = ["ring_small", "ring_mid", "ring_large", "hh_small", "hh_tiled", "onebody",
                      "ladder_thin", "ladder_mid", "ladder_wide", "ladder_tc", "assemble",
-                     "loop_ctl", "energy", "retile"]
+                     "loop_ctl", "energy", "retile", "ladder_reduce"]
 
     def trace_arm(self, iteration):
         """Record kernel start times of iteration `iteration` of the next solve (-1 disarms)."""

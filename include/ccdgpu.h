@@ -254,12 +254,19 @@ int ccdgpu_get_schedule(const ccdgpu_handle *h, ccdgpu_schedule *sch);
 int ccdgpu_autotune(ccdgpu_handle *h, int32_t reps, ccdgpu_schedule *chosen, double *ms_fp64,
                     double *ms_tc);
 
+/* Each pp-ladder class launched alone, reps times (CUDA events): ms, executed flops (packed:
+ * rows a<=b, K over c<d and hh) and algorithmic bytes per launch, indexed FP64 thin (hh <= 8),
+ * FP64 mid (nb 16..32), FP64 wide (nb 40..72, the largest channels), tensor-core ladder
+ * (mixed handles).  Amplitudes are not changed.  No counterpart in the reference. */
+int ccdgpu_ladder_profile(ccdgpu_handle *h, int32_t reps, double ms[4], double flops[4],
+                          double bytes[4]);
+
 /* Kernel start-time trace (diagnostics; no counterpart in the reference).  Arm with the index
  * of an iteration of the next solve (-1 disarms); every kernel of that iteration then records
  * the %globaltimer time (ns) at which its first and its last CTA started.  Kernel ids, in this
  * order: ring small, ring mid, ring large, hh ladder small, hh ladder tiled, one-body, pp
  * ladder thin, mid, wide, tensor-core pp ladder, assembly, loop control, energy, FP64 tile
- * refresh (14). */
+ * refresh, split-K reduction (15). */
 int ccdgpu_trace_arm(ccdgpu_handle *h, int64_t iteration);
 int ccdgpu_trace_read(ccdgpu_handle *h, uint64_t *first, uint64_t *last, int32_t n);
 

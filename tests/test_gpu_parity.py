@@ -184,3 +184,15 @@ def test_autotune_and_schedules_keep_results(precision):
             sol.reset()
             r2 = sol.solve(tol=g["tol"])
             assert abs(r2.e_corr - g["energies"][-1]) <= 1e-10 * abs(g["energies"][-1])
+
+
+def test_ladder_profile_reports_every_class():
+    g = golden("eg54_s19")
+    with system_for(g) as s, CCDSolver(s, precision="mixed_bf16") as sol:
+        prof = sol.ladder_profile(reps=2)
+        for name in ["fp64_thin", "fp64_mid", "fp64_wide", "tensor_core"]:
+            ms, fl, by = prof[name]
+            assert ms > 0 and fl > 0 and by > 0
+        # Timing the ladders alone leaves the solve unchanged.
+        res = sol.solve(tol=g["tol"])
+        assert abs(res.e_corr - g["energies"][-1]) <= 1e-10 * abs(g["energies"][-1])
