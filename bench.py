@@ -304,6 +304,7 @@ def main():
         sol.enable_profiling(False)
         work[a] = sol.work_per_iteration()
     ladder_cls = {a: solvers[a].ladder_profile(reps=5) for a in arms}
+    other_cls = solvers[arms[0]].kernel_profile(reps=5)  # shared by both arms
     n_t2 = solvers[arms[0]].n_t2
 
     # e2e (headline arm): the public API from host buffers, every step: create (H2D upload)
@@ -378,6 +379,14 @@ def main():
                 else:
                     cls[name]["frac_of_hbm_peak"] = cls[name]["gbs"] / peaks["hbm_gbs"]
             arms_out[a]["pp_ladder_classes_alone"] = cls
+        # Ring / hh ladder / one-body classes alone (the same kernels in both arms).
+        shared = {}
+        for name, (ms, fl, by) in other_cls.items():
+            shared[name] = {"ms": ms, "gbs": by / (ms / 1000.0) / 1e9,
+                            "frac_of_hbm_peak": by / (ms / 1000.0) / 1e9 / peaks["hbm_gbs"]}
+            if fl > 0:
+                shared[name]["tflops"] = fl / (ms / 1000.0) / 1e12
+                shared[name]["frac_of_fp64_peak"] = shared[name]["tflops"] / FP64_PEAK_TFLOPS
         if "fp64" in arms_out:
             f = arms_out["fp64"]
             f["fp64_peak_tflops"] = FP64_PEAK_TFLOPS
@@ -406,6 +415,7 @@ def main():
                                       "device (graph WHILE nodes)"),
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "arms": arms_out,
+            "shared_kernels_alone": shared,
             "e2e": {"value": e2e_i.item() / e2e_t.item(), "unit": "iter/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * n_t2,
                     "what": "ccdgpu_create from host buffers + ccdgpu_solve + ccdgpu_get_t2"},

@@ -121,7 +121,7 @@ GPU_SYMBOLS = [
     "ccdgpu_get_profile", "ccdgpu_enable_profiling", "ccdgpu_work_per_iteration",
     "ccdgpu_energy_history", "ccdgpu_stream", "ccdgpu_calc_channel_t2diff_pphh_noalloc",
     "ccdgpu_trace_arm", "ccdgpu_trace_read", "ccdgpu_solve_batch", "ccdgpu_set_schedule",
-    "ccdgpu_get_schedule", "ccdgpu_autotune", "ccdgpu_ladder_profile",
+    "ccdgpu_get_schedule", "ccdgpu_autotune", "ccdgpu_ladder_profile", "ccdgpu_kernel_profile",
 ]
 
 
@@ -168,6 +168,7 @@ def gpu_lib():
         lib.ccdgpu_get_schedule.argtypes = [vp, P(Schedule)]
         lib.ccdgpu_autotune.argtypes = [vp, c_i32, P(Schedule), P(c_dbl), P(c_dbl)]
         lib.ccdgpu_ladder_profile.argtypes = [vp, c_i32, P(c_dbl), P(c_dbl), P(c_dbl)]
+        lib.ccdgpu_kernel_profile.argtypes = [vp, c_i32, P(c_dbl), P(c_dbl), P(c_dbl)]
         lib.ccdgpu_trace_read.argtypes = [vp, P(c_u64), P(c_u64), c_i32]
         _gpu = lib
     return _gpu

@@ -114,9 +114,9 @@ struct ChanInfo {
   int64_t vtc_base, tkt_tc_base, tmt_tc_base, xt_tc_base;
 };
 
-// hh-ladder split-K tile: rows [k0, k0+rows) of channel ch.
+// hh-ladder unit: rows [k0, k0+rows) of channel ch (slice idx), a chunk of P rows.
 struct HHTile {
-  int32_t ch, k0, idx, rows;  // idx = tile index within the channel
+  int32_t ch, k0, idx, rows, chunk, pad;
 };
 
 // Per active modified channel.
@@ -137,7 +137,7 @@ struct ElemRange {
 enum TraceKernel {
   kTrRingSmall = 0, kTrRingMid, kTrRingLarge, kTrHHSmall, kTrHHTiled, kTrOneBody, kTrLadderThin,
   kTrLadderMid, kTrLadderWide, kTrLadderTC, kTrAssemble, kTrLoopCtl, kTrEnergy, kTrRetile,
-  kTrReduce, kTraceKernels
+  kTrReduce, kTrHHReduce, kTraceKernels
 };
 
 // Device control block: iteration state of the solve loop lives on the device so that a

@@ -3,7 +3,7 @@
 // Reference correspondence (calc.cpp / Chain.hpp of justinlietz/coupled_cluster_doubles):
 //   pp_ladder_kernel        D = 0.5 T X + 0.5 V_pppp T              calc.cpp:162-202
 //                           (antisymmetry-packed, FP64 FMA pipe)
-//   hh_ladder_kernel        X = V_hhhh + 0.5 V_hhpp T                calc.cpp:141-160
+//   hh_mma_kernel           X = V_hhhh + 0.5 V_hhpp T                calc.cpp:141-160
 //   ring_*_kernel           Y = V_hphp + 0.5 V_hpph T'; R = T' Y     calc.cpp:264-313
 //   onebody_tables_kernel   calcChannelT2Diff_h2pp_h1 / _p2_p1hh     calc.cpp:9-25, 73-89
 //   onebody_fused_kernel    the same dot products, read from the ladder intermediates
@@ -397,24 +397,29 @@ __device__ __forceinline__ void opgemm(const double *__restrict__ A, int lda,
 }
 __host__ __device__ inline int even_up(int n) { return (n + 1) & ~1; }
 
-// ------------------------------------------------------------------------------------------
-// hh ladder intermediate, split into K slices of each channel:
-//   P = V_hhpp T (K = pp),  X = V_hhhh + 0.5 P  (reference layout, and X/2 as B tiles),
-//   s[IJ] = P[IJ][IJ]            (x_k = sum over IJ with first hole k, calc.cpp:82-84),
-//   r[AB] = sum_IJ V[IJ][AB] T[AB][IJ]  (y_a = sum over AB with first particle a, calc.cpp:18-20).
-// V_hhpp is held transposed (pp x hh), so a slice of V and of T are both contiguous row ranges;
-// a slice holds at most kHHElems elements (rows = kHHElems / hh) and is staged in shared memory
-// with one round of loads.  hh <= 16: thread = (output, row group), the row groups summed in a
-// fixed order; hh > 16: 16 x 16 threads with a TM x TM register tile each (rows ty + 16 i,
-// columns tx + 16 j).  A channel with one slice finishes X directly.  Otherwise each CTA writes
-// its partial P and the last CTA of the channel (atomic ticket) adds the partials in slice
-// order, so the result does not depend on scheduling.
-// ------------------------------------------------------------------------------------------
-constexpr int kHHThreads = 256;
-constexpr int kHHElems = 2560;  // V (and T) elements of one slice
-constexpr int kHHStagePad = 256 + 96;  // odd-hh row padding (<= 2560/17 rows) + slice overrun
+// FP64 tensor-core MMA (mma.sync m8n8k4, the full-rate FP64 path of sm_100a): lane
+// (g = lane / 4, t = lane % 4) supplies A[g][t] and B[t][g] and accumulates C[g][2t] and
+// C[g][2t + 1].  One instruction does 256 multiply-adds, so the small channel GEMMs are no longer
+// bound by instruction issue and shared-memory loads.
+__device__ __forceinline__ void dmma_884(double (&c)[2], double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+      : "+d"(c[0]), "+d"(c[1])
+      : "d"(a), "d"(b));
+}
 
-__host__ __device__ inline int hh_slice_rows(int hh) { return hh >= kHHElems ? 1 : kHHElems / hh; }
+// ------------------------------------------------------------------------------------------
+// hh ladder intermediate (calc.cpp:141-160 and the one-body sums of calc.cpp:18-20, 82-84):
+//   P = V_hhpp T (K = pp),  X = V_hhhh + 0.5 P  (reference layout, and X/2 as B tiles),
+//   s[IJ] = P[IJ][IJ],  r[AB] = sum_IJ V[IJ][AB] T[AB][IJ].
+// V_hhpp is held transposed (pp x hh), so a K slice of V and of T are contiguous row ranges.
+// hh_mma_kernel: one warp per (slice of kHHRows pp rows, chunk of P rows) on the FP64 MMA,
+// fragments loaded straight from global memory (8 consecutive columns of 4 rows per load);
+// rows past the slice and columns past hh read as zero.  The warp of chunk 0 also forms the
+// row dots r from the same fragments.  Each slice writes its partial P; hh_reduce_kernel adds
+// the partials in slice order (deterministic) and finishes X, its operand tiles and s.
+// ------------------------------------------------------------------------------------------
+constexpr int kHHWarps = 8;
+constexpr int kHHRows = 32;  // pp rows of one K slice
 
 // X, its X/2 operand tiles (FP64 and, for a mixed iteration, bf16 terms) and s from one
 // finished element P[kl][ij].
@@ -436,110 +441,101 @@ __device__ __forceinline__ void hh_finish(const ChanInfo &ch, int kl, int ij, do
   if (kl == ij) s_out[ch.hh_off + ij] = p;
 }
 
-struct HHOut {
-  const HHTile &tt;
-  const ChanInfo &ch;
-  const double *v_hhhh;
-  double *part, *x_ref, *x_t, *s_out;
-  __nv_bfloat16 *xt_tc;
-  int64_t xt_tc_stride;
-  int nt;
-  // One slice's value of P[kl][ij]: final for single-slice channels, else a partial.
-  __device__ __forceinline__ void emit(int kl, int ij, double p) const {
-    if (ch.nhht == 1) hh_finish(ch, kl, ij, p, v_hhhh, x_ref, x_t, s_out, xt_tc, xt_tc_stride, nt);
-    else part[ch.part_off + (int64_t)tt.idx * ch.hh * ch.hh + kl * ch.hh + ij] = p;
+// NMAX = column tiles of 8 held per warp: 2 for hh <= 16 (MC = 2 row tiles per warp, the whole
+// P), kMaxCG for the rest (MC = 1 row tile per warp).
+template <int NMAX>
+__global__ void __launch_bounds__(kHHWarps * 32, NMAX <= 2 ? 4 : 2)
+hh_mma_kernel(const HHTile *__restrict__ tiles, int n, const ChanInfo *__restrict__ chans,
+              const double *__restrict__ v_pphh, const double *tbuf0, const double *tbuf1,
+              double *__restrict__ part, double *__restrict__ r_out, const Control *ctl,
+              int gate) {
+  if (skip_iteration(ctl, gate, NMAX <= 2 ? kTrHHSmall : kTrHHTiled)) return;
+  const int u = blockIdx.x * kHHWarps + (threadIdx.x >> 5);
+  if (u >= n) return;
+  const HHTile tt = tiles[u];
+  const ChanInfo ch = chans[tt.ch];
+  const double *t_old = ctl->parity ? tbuf1 : tbuf0;
+  const int hh = ch.hh, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  constexpr int MC = NMAX <= 2 ? 2 : 1;
+  const int h8 = (hh + 7) >> 3, mc0 = MC * tt.chunk, mc = min(MC, h8 - mc0);
+  const bool do_dot = tt.chunk == 0;
+  const double *vb = v_pphh + ch.t_off + (int64_t)tt.k0 * hh;
+  const double *tb = t_old + ch.t_off + (int64_t)tt.k0 * hh;
+  double acc[MC][NMAX][2];
+#pragma unroll
+  for (int m = 0; m < MC; ++m)
+#pragma unroll
+    for (int c = 0; c < NMAX; ++c) acc[m][c][0] = acc[m][c][1] = 0.0;
+  const int nk4 = (tt.rows + 3) >> 2;
+#pragma unroll 2
+  for (int k4 = 0; k4 < nk4; ++k4) {
+    const int k = 4 * k4 + t;
+    const bool kin = k < tt.rows;
+    const double *vr = vb + (int64_t)k * hh, *tr = tb + (int64_t)k * hh;
+    double a[MC], b[NMAX];
+#pragma unroll
+    for (int m = 0; m < MC; ++m) {
+      const int col = (mc0 + m) * 8 + g;
+      a[m] = (kin && col < hh) ? vr[col] : 0.0;
+    }
+#pragma unroll
+    for (int c = 0; c < NMAX; ++c) {
+      const int col = c * 8 + g;
+      b[c] = (kin && col < hh) ? tr[col] : 0.0;
+    }
+#pragma unroll
+    for (int m = 0; m < MC; ++m)
+#pragma unroll
+      for (int c = 0; c < NMAX; ++c)
+        if (m < mc && c < h8) dmma_884(acc[m][c], a[m], b[c]);
+    if (do_dot) {
+      // Row k: lane partial over columns 8c + g, then a fixed butterfly over g.
+      double d = 0.0;
+#pragma unroll
+      for (int c = 0; c < NMAX; ++c) {
+        const int col = c * 8 + g;
+        const double v = c < MC ? a[c] : ((kin && col < hh) ? vr[col] : 0.0);
+        d = fma(v, b[c], d);
+      }
+      d += __shfl_xor_sync(0xffffffffu, d, 4);
+      d += __shfl_xor_sync(0xffffffffu, d, 8);
+      d += __shfl_xor_sync(0xffffffffu, d, 16);
+      if (g == 0 && kin) r_out[ch.pp_off + tt.k0 + k] = d;
+    }
   }
-};
-
-// hh > 16: thread (tx, ty) owns P rows 2*TH*ty.. and columns 2*TH*tx.. (contiguous blocks of
-// TM = 2*TH); the slice is staged with an even row stride ld.
-template <int TM>
-__device__ __forceinline__ void hh_tiled(const double *Vs, const double *Ts, int rows, int hh,
-                                         int ld, const HHOut &out) {
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  const int r0 = ty * TM, c0 = tx * TM;
-  if (r0 >= hh || c0 >= hh) return;
-  double acc[TM][TM];
+  double *pb = part + ch.part_off + (int64_t)tt.idx * hh * hh;
 #pragma unroll
-  for (int i = 0; i < TM; ++i)
+  for (int m = 0; m < MC; ++m)
 #pragma unroll
-    for (int j = 0; j < TM; ++j) acc[i][j] = 0.0;
-  opgemm<TM>(Vs, ld, Ts, ld, rows, r0, c0, acc);
-#pragma unroll
-  for (int i = 0; i < TM; ++i)
-#pragma unroll
-    for (int j = 0; j < TM; ++j) {
-      const int kl = r0 + i, ij = c0 + j;
-      if (kl < hh && ij < hh) out.emit(kl, ij, acc[i][j]);
+    for (int c = 0; c < NMAX; ++c) {
+      const int kl = (mc0 + m) * 8 + g, ij = c * 8 + 2 * t;
+      if (m < mc && c < h8 && kl < hh) {
+        if (ij < hh) pb[kl * hh + ij] = acc[m][c][0];
+        if (ij + 1 < hh) pb[kl * hh + ij + 1] = acc[m][c][1];
+      }
     }
 }
 
-// SMALL: channels with hh <= 16 (few registers, high occupancy); else the register-tiled rest.
-template <bool SMALL>
-__global__ void __launch_bounds__(kHHThreads, SMALL ? 4 : 2)
-hh_ladder_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ chans,
-                 const double *__restrict__ v_pphh, const double *__restrict__ v_hhhh,
-                 const double *tbuf0, const double *tbuf1, double *part, int32_t *counters,
+// Item = 256 consecutive elements P[kl][ij] (row-major) of channel ch, from idx0.
+struct HHRed {
+  int32_t ch, idx0;
+};
+__global__ void __launch_bounds__(256)
+hh_reduce_kernel(const HHRed *__restrict__ items, const ChanInfo *__restrict__ chans,
+                 const double *__restrict__ v_hhhh, const double *__restrict__ part,
                  double *__restrict__ x_ref, double *__restrict__ x_t, double *__restrict__ s_out,
-                 double *__restrict__ r_out, __nv_bfloat16 *__restrict__ xt_tc,
-                 int64_t xt_tc_stride, int nt, const Control *ctl, int gate) {
-  if (skip_iteration(ctl, gate, SMALL ? kTrHHSmall : kTrHHTiled)) return;
-  // Even-stride staging: rows * even_up(hh) <= kHHElems + rows, plus room for slices that run
-  // past the last row.
-  __shared__ __align__(16) double Vs[kHHElems + kHHStagePad], Ts[kHHElems + kHHStagePad];
-  __shared__ double red[kHHThreads];
-  __shared__ int last;
-  const HHTile tt = tiles[blockIdx.x];
-  const ChanInfo ch = chans[tt.ch];
-  const double *t_old = ctl->parity ? tbuf1 : tbuf0;
-  const int hh = ch.hh, tid = threadIdx.x, rows = tt.rows, n = rows * hh;
-  const int ld = SMALL ? hh : even_up(hh);  // staged row stride (even for 16-byte loads)
-  const double *vb = v_pphh + ch.t_off + (int64_t)tt.k0 * hh;
-  const double *tb = t_old + ch.t_off + (int64_t)tt.k0 * hh;
-  for (int e = tid; e < n; e += kHHThreads) {
-    const int r = e / hh, c = e - r * hh;
-    Vs[r * ld + c] = vb[e];
-    Ts[r * ld + c] = tb[e];
-  }
-  __syncthreads();
-  for (int r = tid; r < rows; r += kHHThreads)
-    r_out[ch.pp_off + tt.k0 + r] = dot4(Vs + r * ld, 1, Ts + r * ld, 1, hh);
-  const HHOut out{tt, ch, v_hhhh, part, x_ref, x_t, s_out, xt_tc, xt_tc_stride, nt};
-  if (SMALL) {
-    const int no = hh * hh, groups = kHHThreads / no;
-    const int o = tid % no, g = tid / no, kl = o / hh, ij = o - kl * hh;
-    double acc = 0.0;
-    if (g < groups)
-      for (int r = g; r < rows; r += groups) acc = fma(Vs[r * hh + kl], Ts[r * hh + ij], acc);
-    red[tid] = acc;
-    __syncthreads();
-    if (tid < no) {
-      double p = 0.0;
-      for (int q = 0; q < groups; ++q) p += red[q * no + tid];
-      out.emit(kl, ij, p);
-    }
-  } else {
-    switch ((hh + 31) / 32) {  // blocks of TM = 2, 4, 6 cover 32, 64, 96 columns
-      case 1: hh_tiled<2>(Vs, Ts, rows, hh, ld, out); break;
-      case 2: hh_tiled<4>(Vs, Ts, rows, hh, ld, out); break;
-      default: hh_tiled<6>(Vs, Ts, rows, hh, ld, out); break;
-    }
-  }
-  if (ch.nhht == 1) return;
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) last = (atomicAdd(&counters[tt.ch], 1) == ch.nhht - 1);
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  const int nout = hh * hh;
-  const double *pbase = part + ch.part_off;
-  for (int idx = tid; idx < nout; idx += kHHThreads) {
-    double p = 0.0;
-    for (int t = 0; t < ch.nhht; ++t) p += __ldcg(pbase + (int64_t)t * nout + idx);
-    hh_finish(ch, idx / hh, idx % hh, p, v_hhhh, x_ref, x_t, s_out, xt_tc, xt_tc_stride, nt);
-  }
-  if (tid == 0) counters[tt.ch] = 0;
+                 __nv_bfloat16 *__restrict__ xt_tc, int64_t xt_tc_stride, int nt,
+                 const Control *ctl, int gate) {
+  if (skip_iteration(ctl, gate, kTrHHReduce)) return;
+  const HHRed it = items[blockIdx.x];
+  const ChanInfo ch = chans[it.ch];
+  const int hh = ch.hh, nout = hh * hh, idx = it.idx0 + threadIdx.x;
+  if (idx >= nout) return;
+  const double *pb = part + ch.part_off + idx;
+  double p = 0.0;
+  for (int sl = 0; sl < ch.nhht; ++sl) p += pb[(int64_t)sl * nout];
+  hh_finish(ch, idx / hh, idx - (idx / hh) * hh, p, v_hhhh, x_ref, x_t, s_out, xt_tc,
+            xt_tc_stride, nt);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -555,6 +551,7 @@ hh_ladder_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ 
 // memory sizes.
 // ------------------------------------------------------------------------------------------
 constexpr int kRingThreads = 256;
+__host__ __device__ constexpr int kRingThreadsOf(int nc) { return nc <= 2 ? 256 : 512; }
 constexpr int kRingSmall = 16;
 constexpr int kRingMid = 32;
 
@@ -605,93 +602,114 @@ ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restr
   }
 }
 
-// Shared-memory stage of one channel, rows padded to even strides (ldh = even(hp'),
-// ldp = even(ph')): T' [ph'][ldh], T'^T [hp'][ldp], Vt [ph'][ldh], Y [hp'][ldh] (V_hphp on
-// arrival), the ph' x hp' scatter indices (int32, fused path), then padding for slices that run
-// past the last row.
-__host__ __device__ inline int ring_stage_doubles(int ph, int hp) {
-  const int ldh = even_up(hp), ldp = even_up(ph);
-  return even_up(2 * ph * ldh + hp * ldp + hp * ldh + (ph * hp + 1) / 2 + 16);  // 16-byte steps
-}
-
-// Thread (tx, ty) owns rows ty*TM.. and columns tx*TM.. of Y and of R.
-template <int TM>
-__device__ __forceinline__ void ring_compute(const ModInfo &m, double *st,
-                                             const int32_t *__restrict__ inv,
-                                             double *__restrict__ out) {
-  const int ph = m.ph, hp = m.hp, tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  const int ldh = even_up(hp), ldp = even_up(ph);
-  double *Ts = st, *TT = Ts + ph * ldh, *Vt = TT + hp * ldp, *Ys = Vt + ph * ldh;
-  const int32_t *Is = reinterpret_cast<const int32_t *>(Ys + hp * ldh);
-  // T'^T for the second product.
-  for (int e = tid; e < ph * hp; e += kRingThreads) {
-    const int i = e / hp, k = e - i * hp;
-    TT[k * ldp + i] = Ts[i * ldh + k];
-  }
-  const int r0 = ty * TM, c0 = tx * TM;
-  double acc[TM][TM];
-  // Y = V_hphp + 0.5 V_hpph T'   (hp x hp, K = ph)
-  if (r0 < hp && c0 < hp) {
+// C (M8*8 x N8*8) = A B, K4*4 deep, on 8 x 8 tiles: warps warp, warp + nwarps, ... take items of
+// one 8-row tile by NC column tiles (the A fragment is reused NC times).  A[m][k] =
+// A[m * ars + k * aks], B[k][n] = B[k * ldb + n]; epi(row, col, value) stores each result.
+template <int NC, class Epi>
+__device__ __forceinline__ void warp_mma_gemm(const double *A, int ars, int aks, const double *B,
+                                              int ldb, int M8, int N8, int K4, int warp,
+                                              int nwarps, const Epi &epi) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int nch = (N8 + NC - 1) / NC;
+  for (int it = warp; it < M8 * nch; it += nwarps) {
+    const int mt = it / nch, n0 = (it - mt * nch) * NC, nn = min(NC, N8 - n0);
+    double acc[NC][2];
 #pragma unroll
-    for (int i = 0; i < TM; ++i)
+    for (int n = 0; n < NC; ++n) acc[n][0] = acc[n][1] = 0.0;
+    const double *ap = A + (mt * 8 + g) * ars + t * aks;
+    const double *bp = B + t * ldb + n0 * 8 + g;
+    const int astep = 4 * aks, bstep = 4 * ldb;
+#pragma unroll 2
+    for (int k4 = 0; k4 < K4; ++k4) {
+      const double a = ap[k4 * astep];
 #pragma unroll
-      for (int j = 0; j < TM; ++j) acc[i][j] = 0.0;
-    opgemm<TM>(Vt, ldh, Ts, ldh, ph, r0, c0, acc);
-    // Each Y element is read and written by the thread that owns it.
+      for (int n = 0; n < NC; ++n)
+        if (n < nn) dmma_884(acc[n], a, bp[k4 * bstep + n * 8]);
+    }
 #pragma unroll
-    for (int i = 0; i < TM; ++i)
-#pragma unroll
-      for (int j = 0; j < TM; ++j)
-        if (r0 + i < hp && c0 + j < hp)
-          Ys[(r0 + i) * ldh + c0 + j] = 0.5 * acc[i][j] + Ys[(r0 + i) * ldh + c0 + j];
-  }
-  __syncthreads();
-  // R = T' Y   (ph x hp, K = hp)
-  if (r0 < ph && c0 < hp) {
-#pragma unroll
-    for (int i = 0; i < TM; ++i)
-#pragma unroll
-      for (int j = 0; j < TM; ++j) acc[i][j] = 0.0;
-    opgemm<TM>(TT, ldp, Ys, ldh, hp, r0, c0, acc);
-#pragma unroll
-    for (int i = 0; i < TM; ++i)
-#pragma unroll
-      for (int j = 0; j < TM; ++j) {
-        const int r = r0 + i, c = c0 + j;
-        if (r < ph && c < hp) {
-          const int p = r * hp + c;
-          out[inv ? (int64_t)Is[p] : m.m_off + p] = acc[i][j];
-        }
+    for (int n = 0; n < NC; ++n)
+      if (n < nn) {
+        const int r = mt * 8 + g, c = (n0 + n) * 8 + 2 * t;
+        epi(r, c, acc[n][0]);
+        epi(r, c + 1, acc[n][1]);
       }
   }
 }
 
+// Shared-memory stage of one channel: ph' and hp' padded to multiples of 8 (P, H) with zeros,
+// row stride ld = H + 4 (ld = 4 mod 8 spreads the 4 k-rows of a fragment load over all banks):
+// T' [P][ld], Vt [P][ld], Y [H][ld] (V_hphp on arrival), then the ph' x hp' scatter indices
+// (int32, fused path).
+__host__ __device__ inline int ring_pad8(int n) { return (n + 7) & ~7; }
+__host__ __device__ inline int ring_stage_doubles(int ph, int hp) {
+  const int P = ring_pad8(ph), H = ring_pad8(hp), ld = H + 4;
+  return even_up((2 * P + H) * ld + (ph * hp + 1) / 2);  // 16-byte steps
+}
+
+// Y = V_hphp + 0.5 V_hpph T' (H x H, K = P), then R = T' Y (P x H, K = H) on the FP64 MMA;
+// R is stored (scattered through the inverse ai_jb table on the fused path) for r < ph', c < hp'.
+template <int NC, int THREADS>
+__device__ __forceinline__ void ring_compute(const ModInfo &m, double *st,
+                                             const int32_t *__restrict__ inv,
+                                             double *__restrict__ out) {
+  const int ph = m.ph, hp = m.hp, P = ring_pad8(ph), H = ring_pad8(hp), ld = H + 4;
+  double *Ts = st, *Vt = Ts + P * ld, *Ys = Vt + P * ld;
+  const int32_t *Is = reinterpret_cast<const int32_t *>(Ys + H * ld);
+  const int warp = threadIdx.x >> 5;
+  constexpr int kWarps = THREADS / 32;
+  // A[i][k] = V_hpph[i][k] = Vt[k][i].  Each Y element is read and written by its owner lane.
+  warp_mma_gemm<NC>(Vt, 1, ld, Ts, ld, H / 8, H / 8, P / 4, warp, kWarps,
+                    [&](int r, int c, double v) { Ys[r * ld + c] = 0.5 * v + Ys[r * ld + c]; });
+  __syncthreads();
+  warp_mma_gemm<NC>(Ts, ld, 1, Ys, ld, P / 8, H / 8, H / 4, warp, kWarps,
+                    [&](int r, int c, double v) {
+                      if (r < ph && c < hp) {
+                        const int p = r * hp + c;
+                        out[inv ? (int64_t)Is[p] : m.m_off + p] = v;
+                      }
+                    });
+}
+
 // Resident CTAs: CTA b handles channels b, b + gridDim.x, ...  stage = doubles per buffer;
 // nbuf = 2 (prefetch the next channel) or 1 (largest channels, when two stages do not fit).
-// TMAX = 2: channels up to kRingMid; TMAX = 6: the rest (up to 96).
-template <int TMAX>
-__global__ void __launch_bounds__(kRingThreads, TMAX <= 2 ? 3 : 1)
+// NC = 2: channels up to kRingMid (256 threads, 3 CTAs per SM); NC = 4: the rest (up to
+// kTcMaxNB; 512 threads, one CTA per SM, so that the 8 x 32 items of a channel run at once).
+template <int NC, int THREADS = kRingThreadsOf(NC)>
+__global__ void __launch_bounds__(THREADS, NC <= 2 ? 3 : 1)
 ring_kernel(const ModInfo *__restrict__ mods, int n, const double *__restrict__ v_hpph,
             const double *__restrict__ v_hphp, const double *__restrict__ t_phhp,
             const int32_t *__restrict__ inv, double *__restrict__ out, int stage, int nbuf,
             const Control *ctl, int gate) {
-  if (skip_iteration(ctl, gate, TMAX <= 2 ? kTrRingMid : kTrRingLarge)) return;
+  if (skip_iteration(ctl, gate, NC <= 2 ? kTrRingMid : kTrRingLarge)) return;
   extern __shared__ __align__(16) double rs[];
   const int tid = threadIdx.x;
+  // Operands of channel ci into stage st (cp.async), pad cells zeroed with plain stores; a
+  // warp per row, lanes over the columns.
+  const int warp = tid >> 5, lane = tid & 31;
   auto issue = [&](int ci, double *st) {
     const ModInfo m = mods[ci];
-    const int ph = m.ph, hp = m.hp, ldh = even_up(hp), ldp = even_up(ph);
-    double *Ts = st, *Vt = Ts + ph * ldh + hp * ldp, *Ys = Vt + ph * ldh;
-    int32_t *Is = reinterpret_cast<int32_t *>(Ys + hp * ldh);
-    for (int e = tid; e < ph * hp; e += kRingThreads) {
-      const int r = e / hp, c = e - r * hp;
-      cp_async8(Ts + r * ldh + c, t_phhp + m.m_off + e);
-      cp_async8(Vt + r * ldh + c, v_hpph + m.m_off + e);
-      if (inv) cp_async4(Is + e, inv + m.m_off + e);
+    const int ph = m.ph, hp = m.hp, P = ring_pad8(ph), H = ring_pad8(hp), ld = H + 4;
+    double *Ts = st, *Vt = Ts + P * ld, *Ys = Vt + P * ld;
+    int32_t *Is = reinterpret_cast<int32_t *>(Ys + H * ld);
+    for (int r = warp; r < P; r += THREADS / 32) {
+      const int64_t src = m.m_off + (int64_t)r * hp;
+      for (int c = lane; c < H; c += 32) {
+        if (r < ph && c < hp) {
+          cp_async8(Ts + r * ld + c, t_phhp + src + c);
+          cp_async8(Vt + r * ld + c, v_hpph + src + c);
+          if (inv) cp_async4(Is + r * hp + c, inv + src + c);
+        } else {
+          Ts[r * ld + c] = 0.0;
+          Vt[r * ld + c] = 0.0;
+        }
+      }
     }
-    for (int e = tid; e < hp * hp; e += kRingThreads) {
-      const int r = e / hp, c = e - r * hp;
-      cp_async8(Ys + r * ldh + c, v_hphp + m.y_off + e);
+    for (int r = warp; r < H; r += THREADS / 32) {
+      const int64_t src = m.y_off + (int64_t)r * hp;
+      for (int c = lane; c < H; c += 32) {
+        if (r < hp && c < hp) cp_async8(Ys + r * ld + c, v_hphp + src + c);
+        else Ys[r * ld + c] = 0.0;
+      }
     }
   };
   int ci = blockIdx.x;
@@ -705,15 +723,7 @@ ring_kernel(const ModInfo *__restrict__ mods, int n, const double *__restrict__ 
     if (nbuf == 2) cp_async_wait<1>();
     else cp_async_wait<0>();
     __syncthreads();
-    const ModInfo m = mods[ci];
-    const int tmb = (max(m.ph, m.hp) + 31) / 32;  // 32-wide blocks: TM = 2, 4, 6
-    if (TMAX <= 2) {
-      ring_compute<2>(m, st, inv, out);
-    } else {
-      if (tmb <= 1) ring_compute<2>(m, st, inv, out);
-      else if (tmb == 2) ring_compute<4>(m, st, inv, out);
-      else ring_compute<6>(m, st, inv, out);
-    }
+    ring_compute<NC, THREADS>(mods[ci], st, inv, out);
     __syncthreads();
     if (nbuf == 1 && nxt < n) {
       issue(nxt, rs);
@@ -961,34 +971,54 @@ assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__r
   double *nb = t_new + ch.t_off;
   const int n = nrows * hh;
   double corr = 0.0;
-#pragma unroll 2
-  for (int q = threadIdx.x; q < n; q += kAsmThreads) {
-    const int r = q / hh, j = q - r * hh;
-    const AsmRowInfo ri = rows[r];
-    const AsmColInfo ci = cols[j];
-    const int a1 = ri.o_ab + j, as = ri.o_ab + ci.js, b1 = ri.o_ba + j, bs = ri.o_ba + ci.js;
-    const double t_abj = tb[a1], t_abs = tb[as], t_baj = tb[b1], t_bas = tb[bs];
-    const double r_abj = rb[a1], r_abs = rb[as], r_baj = rb[b1], r_bas = rb[bs];
-    const double v1 = vb[a1], d1 = db[a1], v2 = vb[b1], d2 = db[b1];
-    const int32_t g1 = gb[a1], g2 = gb[b1];
-    const double t1 = asm_value(v1, d1, r_abj, r_abs, r_baj, r_bas, t_abj, t_abs, t_baj, ci.xi,
-                                ci.xj, ri.ya, ri.yb, ci.eij - ri.ea - ri.eb, mixing);
-    nb[a1] = t1;
-    old_phhp[g1] = t1;
-    if (nt) write_t_tiles_tc(ch, pk_idx, ri.ab, j, t1, nt, tkt_tc, tkt_tc_stride, tmt_tc,
-                             tmt_tc_stride);
-    else write_t_tiles(ch, pk_idx, ri.ab, j, t1, t_kt, t_mt);
-    corr += v1 * t1;
-    if (ri.mirrored) {
-      // Row ba: the same formula with a and b exchanged.
-      const double t2 = asm_value(v2, d2, r_baj, r_bas, r_abj, r_abs, t_baj, t_bas, t_abj, ci.xi,
-                                  ci.xj, ri.yb, ri.ya, ci.eij - ri.eb - ri.ea, mixing);
-      nb[b1] = t2;
-      old_phhp[g2] = t2;
-      if (nt) write_t_tiles_tc(ch, pk_idx, ri.o_ba / hh, j, t2, nt, tkt_tc, tkt_tc_stride, tmt_tc,
+  // kAsmPerThread elements per thread: every load of all of them is issued before the first
+  // store (t_new may alias t_old for the compiler, which would otherwise serialise them).
+  for (int q0 = threadIdx.x; q0 < n; q0 += kAsmPerThread * kAsmThreads) {
+    double tv[kAsmPerThread][4], rv[kAsmPerThread][4], vv[kAsmPerThread][2],
+        dv[kAsmPerThread][2];
+    int32_t gv[kAsmPerThread][2], a1[kAsmPerThread], b1[kAsmPerThread], jj[kAsmPerThread],
+        rr[kAsmPerThread];
+#pragma unroll
+    for (int u = 0; u < kAsmPerThread; ++u) {
+      const int q = q0 + u * kAsmThreads;
+      if (q >= n) continue;
+      const int r = q / hh, j = q - r * hh;
+      const int o_ab = rows[r].o_ab, o_ba = rows[r].o_ba, js = cols[j].js;
+      rr[u] = r; jj[u] = j;
+      a1[u] = o_ab + j; b1[u] = o_ba + j;
+      const int as = o_ab + js, bs = o_ba + js;
+      tv[u][0] = tb[a1[u]]; tv[u][1] = tb[as]; tv[u][2] = tb[b1[u]]; tv[u][3] = tb[bs];
+      rv[u][0] = rb[a1[u]]; rv[u][1] = rb[as]; rv[u][2] = rb[b1[u]]; rv[u][3] = rb[bs];
+      vv[u][0] = vb[a1[u]]; dv[u][0] = db[a1[u]]; vv[u][1] = vb[b1[u]]; dv[u][1] = db[b1[u]];
+      gv[u][0] = gb[a1[u]]; gv[u][1] = gb[b1[u]];
+    }
+#pragma unroll
+    for (int u = 0; u < kAsmPerThread; ++u) {
+      if (q0 + u * kAsmThreads >= n) continue;
+      const AsmRowInfo ri = rows[rr[u]];
+      const AsmColInfo ci = cols[jj[u]];
+      const int j = jj[u];
+      const double t1 = asm_value(vv[u][0], dv[u][0], rv[u][0], rv[u][1], rv[u][2], rv[u][3],
+                                  tv[u][0], tv[u][1], tv[u][2], ci.xi, ci.xj, ri.ya, ri.yb,
+                                  ci.eij - ri.ea - ri.eb, mixing);
+      nb[a1[u]] = t1;
+      old_phhp[gv[u][0]] = t1;
+      if (nt) write_t_tiles_tc(ch, pk_idx, ri.ab, j, t1, nt, tkt_tc, tkt_tc_stride, tmt_tc,
                                tmt_tc_stride);
-      else write_t_tiles(ch, pk_idx, ri.o_ba / hh, j, t2, t_kt, t_mt);
-      corr += v2 * t2;
+      else write_t_tiles(ch, pk_idx, ri.ab, j, t1, t_kt, t_mt);
+      corr += vv[u][0] * t1;
+      if (ri.mirrored) {
+        // Row ba: the same formula with a and b exchanged.
+        const double t2 = asm_value(vv[u][1], dv[u][1], rv[u][2], rv[u][3], rv[u][0], rv[u][1],
+                                    tv[u][2], tv[u][3], tv[u][0], ci.xi, ci.xj, ri.yb, ri.ya,
+                                    ci.eij - ri.eb - ri.ea, mixing);
+        nb[b1[u]] = t2;
+        old_phhp[gv[u][1]] = t2;
+        if (nt) write_t_tiles_tc(ch, pk_idx, ri.o_ba / hh, j, t2, nt, tkt_tc, tkt_tc_stride,
+                                 tmt_tc, tmt_tc_stride);
+        else write_t_tiles(ch, pk_idx, ri.o_ba / hh, j, t2, t_kt, t_mt);
+        corr += vv[u][1] * t2;
+      }
     }
   }
   const double sum = block_sum<kAsmThreads>(corr, scratch);

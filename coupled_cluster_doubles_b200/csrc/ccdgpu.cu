@@ -43,7 +43,8 @@ struct ccdgpu_handle {
   cudaEvent_t ev[10] = {};
   uint64_t nch = 0, nsp = 0, np = 0, npart = 0;
   int64_t n_t = 0, n_m = 0, n_h = 0, n_p = 0;
-  int n_hh_small = 0;  // hh-ladder tiles of channels with hh <= 16 (first in hh_tiles)
+  int n_hh_small = 0;  // hh-ladder units of channels with hh <= 16 (first in hh_tiles)
+  int n_hh_red = 0;    // hh-ladder reduction items
   int n_act = 0, n_mod = 0, n_mod_small = 0, n_mod_mid = 0, n_tiles = 0, n_hh_tiles = 0;
   int n_ranges = 0;
   int n_asm_blocks = 0;  // fused assembly CTAs (packed-element ranges)
@@ -59,7 +60,8 @@ struct ccdgpu_handle {
   ModInfo *mods = nullptr;        // small (n_mod_small), mid (n_mod_mid), then large channels
   LadderTile *tiles = nullptr;
   HHTile *hh_tiles = nullptr;
-  int32_t *rowmap = nullptr, *mirror = nullptr, *counters = nullptr, *lcounters = nullptr;
+  HHRed *hh_red = nullptr;
+  int32_t *rowmap = nullptr, *mirror = nullptr, *lcounters = nullptr;
   int2 *pk_idx = nullptr;
   double *part = nullptr, *lpart = nullptr;
   ElemRange *ranges = nullptr;
@@ -98,6 +100,8 @@ struct ccdgpu_handle {
   // pp-ladder work lists (make_ladder_tiles), in their own allocation so the autotuner can
   // rebuild them.
   std::vector<ChanInfo> host_chans;
+  std::vector<ModInfo> host_mods;
+  int64_t n_list = 0;  // entries of the one-body segment lists
   ccdgpu_schedule schedule{};
   void *tile_mem = nullptr;
   RedItem *red_fp = nullptr, *red_tc = nullptr;  // split-K reduction items
@@ -415,6 +419,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   std::vector<int2> pk_idx, pp_pairs, hh_pairs, vrows;
   std::vector<int32_t> pp_swap, hh_swap;
   std::vector<HHTile> hh_tiles;
+  std::vector<HHRed> hh_red;
   std::vector<std::vector<int32_t>> seg(nsp);
   int64_t pp_tot = 0, hh_tot = 0, x_tot = 0, tkt = 0, tmt = 0, xt = 0, vt = 0, part_tot = 0;
   int64_t vraw_tot = 0;
@@ -467,7 +472,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     ci.nkc = (int)ceil_div(pk, kBK);
     ci.nkh = (int)ceil_div(hh, kBK);
     ci.nmt = (int)ceil_div(pr, ci.bm);
-    ci.nhht = (int)ceil_div(pp, hh_slice_rows((int)hh));
+    ci.nhht = (int)ceil_div(pp, kHHRows);
     ci.t_off = o_t[c];
     ci.tkt_base = tkt; ci.tmt_base = tmt; ci.xt_base = xt; ci.vkt_base = vt;
     ci.part_off = part_tot;
@@ -493,15 +498,21 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     vraw_off.push_back(vraw_tot);
     if (!on_the_fly) vraw_tot += pp * pp;
     maxhh = std::max<int>(maxhh, (int)hh);
-    const int hrows = hh_slice_rows((int)hh);
+    // hh ladder: one unit per (K slice, chunk of P rows): hh <= 16 is a single chunk, larger
+    // hh one chunk per 8 rows of P.
+    const int nchunk = hh <= 16 ? 1 : (int)ceil_div(hh, 8);
     for (int t = 0; t < ci.nhht; t++)
-      hh_tiles.push_back({ai, t * hrows, t, (int)std::min<int64_t>(hrows, pp - (int64_t)t * hrows)});
+      for (int q = 0; q < nchunk; q++)
+        hh_tiles.push_back({ai, t * kHHRows, t,
+                            (int)std::min<int64_t>(kHHRows, pp - (int64_t)t * kHHRows), q, 0});
+    for (int64_t i0 = 0; i0 < hh * hh; i0 += 256) hh_red.push_back({ai, (int32_t)i0});
     chans.push_back(ci);
     act_chan.push_back(c);
   }
   h->n_act = (int)chans.size();
   h->n_hh_tiles = (int)hh_tiles.size();
-  // Channels with hh <= 16 first (their own launch), then the tiled ones; largest slices
+  h->n_hh_red = (int)hh_red.size();
+  // Channels with hh <= 16 first (their own launch), then the rest; largest units
   // (rows x hh^2) first within each, so the short ones fill in behind them.
   std::stable_sort(hh_tiles.begin(), hh_tiles.end(), [&](const HHTile &x, const HHTile &y) {
     const ChanInfo &a = chans[x.ch], &b = chans[y.ch];
@@ -512,6 +523,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   std::vector<int64_t> list_off(nsp + 1, 0);
   for (uint64_t w = 0; w < nsp; w++) list_off[w + 1] = list_off[w] + (int64_t)seg[w].size();
   std::vector<int32_t> list(list_off[nsp]);
+  h->n_list = list_off[nsp];
   for (uint64_t w = 0; w < nsp; w++) std::copy(seg[w].begin(), seg[w].end(), list.begin() + list_off[w]);
 
   // Modified channels: small ones (one warp each) first, then mid and large ones.
@@ -560,6 +572,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   mods.insert(mods.end(), mods_big.begin(), mods_big.end());
   h->n_mod = (int)mods.size();
   h->ring_smem = ring_smem;
+  h->host_mods = mods;
 
   std::vector<int64_t> o_h(np + 1, 0), o_p(h->npart + 1, 0);
   for (uint64_t k = 0; k < np; k++) o_h[k + 1] = o_h[k] + (int64_t)P->three_body_dims[k].hpp;
@@ -617,14 +630,14 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   // ---- one device allocation ----
   Arena ar;
   ar.add(&h->chans, chans.size()); ar.add(&h->mods, mods.size());
-  ar.add(&h->hh_tiles, hh_tiles.size());
+  ar.add(&h->hh_tiles, hh_tiles.size()); ar.add(&h->hh_red, hh_red.size());
   ar.add(&h->ranges, ranges.size());
   ar.add(&h->pp_pairs, pp_pairs.size()); ar.add(&h->hh_pairs, hh_pairs.size());
   ar.add(&h->pp_swap, pp_swap.size()); ar.add(&h->hh_swap, hh_swap.size());
   ar.add(&h->list_off, list_off.size()); ar.add(&h->list, list.size());
   ar.add(&h->rowmap, rowmap.size()); ar.add(&h->mirror, mirror.size());
   ar.add(&h->pk_idx, pk_idx.size());
-  ar.add(&h->counters, h->n_act); ar.add(&h->part, part_tot);
+  ar.add(&h->part, part_tot);
 
   ar.add(&h->eps, nsp);
   ar.add(&h->v_pphh, n_t); ar.add(&h->v_hhhh, x_tot); ar.add(&h->v_t, vt);
@@ -716,7 +729,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     return CCDGPU_OK;
   };
   TRY(put(h->chans, chans)); TRY(put(h->mods, mods));
-  TRY(put(h->hh_tiles, hh_tiles)); TRY(put(h->ranges, ranges)); TRY(put(h->pranges, pranges));
+  TRY(put(h->hh_tiles, hh_tiles)); TRY(put(h->hh_red, hh_red)); TRY(put(h->ranges, ranges)); TRY(put(h->pranges, pranges));
 
   TRY(put(h->kcol, kcol));
   TRY(put(h->pp_pairs, pp_pairs)); TRY(put(h->hh_pairs, hh_pairs));
@@ -837,7 +850,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   h->hh_smem = 0;  // static shared memory only
   CK(cudaFuncSetAttribute(ring_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)std::max<size_t>(h->ring_smem_mid, 16)));
-  CK(cudaFuncSetAttribute(ring_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  CK(cudaFuncSetAttribute(ring_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)std::max<size_t>(h->ring_smem, 16)));
   ccdgpu_schedule sch{};
   sch.thin_split_mul = 1;
@@ -881,20 +894,30 @@ cudaError_t launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, 
 
 // gate: 0 = kernel of an FP64 iteration, 1 = of a mixed-precision iteration (which also writes
 // the bf16 operand images of the tensor-core ladder).
-int launch_hh_ladder(ccdgpu_handle *h, cudaStream_t st, int gate) {
+// only: -1 everything, 0 units of hh <= 16, 1 the other units (2: neither); the reduction
+// runs when only < 0.
+int launch_hh_ladder(ccdgpu_handle *h, cudaStream_t st, int gate, int only = -1) {
   const int nt = gate ? h->nt : 0;
-  if (h->n_hh_small) {
+  if (h->n_hh_small && only <= 0) {
     h->launches++;
-    CK(launch_pdl(hh_ladder_kernel<true>, h->n_hh_small, kHHThreads, 0, st, h->hh_tiles, h->chans,
-                  h->v_pphh, h->v_hhhh, h->t[0], h->t[1], h->part, h->counters, h->x, h->x_t,
-                  h->s, h->r, h->xt_tc, h->n_xttc, nt, h->ctl, gate));
+    CK(launch_pdl(hh_mma_kernel<2>, (int)ceil_div(h->n_hh_small, kHHWarps), kHHWarps * 32, 0, st,
+                  (const HHTile *)h->hh_tiles, h->n_hh_small, (const ChanInfo *)h->chans,
+                  (const double *)h->v_pphh, (const double *)h->t[0], (const double *)h->t[1],
+                  h->part, h->r, (const Control *)h->ctl, gate));
   }
   const int nbig = h->n_hh_tiles - h->n_hh_small;
-  if (nbig) {
+  if (nbig && (only < 0 || only == 1)) {
     h->launches++;
-    CK(launch_pdl(hh_ladder_kernel<false>, nbig, kHHThreads, 0, st, h->hh_tiles + h->n_hh_small,
-                  h->chans, h->v_pphh, h->v_hhhh, h->t[0], h->t[1], h->part, h->counters, h->x,
-                  h->x_t, h->s, h->r, h->xt_tc, h->n_xttc, nt, h->ctl, gate));
+    CK(launch_pdl(hh_mma_kernel<kMaxCG>, (int)ceil_div(nbig, kHHWarps), kHHWarps * 32, 0, st,
+                  (const HHTile *)(h->hh_tiles + h->n_hh_small), nbig, (const ChanInfo *)h->chans,
+                  (const double *)h->v_pphh, (const double *)h->t[0], (const double *)h->t[1],
+                  h->part, h->r, (const Control *)h->ctl, gate));
+  }
+  if (h->n_hh_red && (only < 0 || only == 2)) {
+    h->launches++;
+    CK(launch_pdl(hh_reduce_kernel, h->n_hh_red, 256, 0, st, (const HHRed *)h->hh_red,
+                  (const ChanInfo *)h->chans, (const double *)h->v_hhhh, (const double *)h->part,
+                  h->x, h->x_t, h->s, h->xt_tc, h->n_xttc, nt, (const Control *)h->ctl, gate));
   }
   return CCDGPU_OK;
 }
@@ -972,16 +995,17 @@ int launch_pp_ladder(ccdgpu_handle *h, cudaStream_t st) {
 
 // T' from the phhp slab in both paths.  fused: R scattered into pphh order for the fused
 // assembly; else the table path's t2Diff_phhp slab.
-int launch_ring(ccdgpu_handle *h, cudaStream_t st, int gate, bool fused) {
+// only: -1 every class, else 0 small, 1 mid, 2 large.
+int launch_ring(ccdgpu_handle *h, cudaStream_t st, int gate, bool fused, int only = -1) {
   const int32_t *inv = fused ? h->inv4 : nullptr;
   double *out = fused ? h->d_ring : h->r_phhp;
-  if (h->n_mod_small) {
+  if (h->n_mod_small && (only < 0 || only == 0)) {
     ring_small_kernel<<<(int)ceil_div(h->n_mod_small, 8), 256, 0, st>>>(
         h->mods, h->n_mod_small, h->v_hpph, h->v_hphp, h->old_phhp, inv, out, h->ctl, gate);
     h->launches++;
     CK(cudaGetLastError());
   }
-  if (h->n_mod_mid) {
+  if (h->n_mod_mid && (only < 0 || only == 1)) {
     ring_kernel<2><<<h->ring_grid_mid, kRingThreads, h->ring_smem_mid, st>>>(
         h->mods + h->n_mod_small, h->n_mod_mid, h->v_hpph, h->v_hphp, h->old_phhp, inv, out,
         h->ring_stage_mid, 2, h->ctl, gate);
@@ -989,8 +1013,8 @@ int launch_ring(ccdgpu_handle *h, cudaStream_t st, int gate, bool fused) {
     CK(cudaGetLastError());
   }
   const int nbig = h->n_mod - h->n_mod_small - h->n_mod_mid;
-  if (nbig) {
-    ring_kernel<6><<<h->ring_grid_large, kRingThreads, h->ring_smem, st>>>(
+  if (nbig && (only < 0 || only == 2)) {
+    ring_kernel<4><<<h->ring_grid_large, kRingThreadsOf(4), h->ring_smem, st>>>(
         h->mods + h->n_mod_small + h->n_mod_mid, nbig, h->v_hpph, h->v_hphp, h->old_phhp, inv,
         out, h->ring_stage_large, h->ring_nbuf_large, h->ctl, gate);
     h->launches++;
@@ -1649,6 +1673,55 @@ void *ccdgpu_stream(ccdgpu_handle *h) { return h ? (void *)h->s0 : nullptr; }
 // Each pp-ladder class launched alone (FP64 thin, mid, wide; tensor-core ladder), `reps` times
 // between CUDA events on the handle's stream; with the executed flops (packed: rows a<=b, K over
 // c<d and hh) and the algorithmic bytes of each class.
+int ccdgpu_kernel_profile(ccdgpu_handle *h, int32_t reps, double *ms, double *flops,
+                          double *bytes) {
+  if (!h || reps < 1 || !ms || !flops || !bytes) return CCDGPU_ERR_INVALID_ARGUMENT;
+  CK(cudaSetDevice(h->opt.device));
+  int rc = set_ctl(h, 0, h->h_ctl->tol, h->h_ctl->max_iters, h->h_ctl->mixing, false);
+  if (rc) return rc;
+  for (int k = 0; k < 7; k++) ms[k] = flops[k] = bytes[k] = 0;
+  // Ring: Y = V_hphp + 0.5 V_hpph T' and R = T' Y; reads T', V_hpph, V_hphp and the inverse
+  // ai_jb table, writes R.
+  for (const ModInfo &m : h->host_mods) {
+    const int k = (m.ph <= kRingSmall && m.hp <= kRingSmall) ? 0
+                  : (m.ph <= kRingMid && m.hp <= kRingMid) ? 1 : 2;
+    flops[k] += 4.0 * m.ph * (double)m.hp * m.hp;
+    bytes[k] += 28.0 * m.ph * m.hp + 8.0 * m.hp * m.hp;
+  }
+  // hh ladder: P = V_hhpp T over the pp rows and r = row dots; reads V_pphh and T, writes the
+  // slice partials of P and r.  Reduction: reads the partials and V_hhhh, writes X (reference
+  // layout and FP64 operand tiles) and s.
+  for (const ChanInfo &a : h->host_chans) {
+    const int k = a.hh <= 16 ? 3 : 4;
+    const double hh2 = (double)a.hh * a.hh;
+    flops[k] += 2.0 * a.pp * a.hh * (a.hh + 1.0);
+    bytes[k] += 16.0 * a.pp * a.hh + 8.0 * a.nhht * hh2 + 8.0 * a.pp;
+    flops[6] += (double)a.nhht * hh2;
+    bytes[6] += 8.0 * a.nhht * hh2 + 24.0 * hh2 + 8.0 * a.hh;
+  }
+  // One-body: segmented sums of s and r (one value per pair) into x_k and y_a.
+  flops[5] = (double)h->n_t * 0;  // no arithmetic worth counting
+  bytes[5] = 16.0 * (double)(h->nsp) + 12.0 * (double)h->n_list;
+  for (int k = 0; k < 7; k++) {
+    auto launch = [&]() -> int {
+      if (k <= 2) return launch_ring(h, h->s0, 0, true, k);
+      if (k <= 4) return launch_hh_ladder(h, h->s0, 0, k - 3);
+      if (k == 6) return launch_hh_ladder(h, h->s0, 0, 2);
+      return launch_onebody_fused(h, h->s0, 0);
+    };
+    if ((rc = launch())) return rc;  // warm-up
+    CK(cudaEventRecord(h->ev[0], h->s0));
+    for (int i = 0; i < reps && !rc; i++) rc = launch();
+    if (rc) return rc;
+    CK(cudaEventRecord(h->ev[1], h->s0));
+    CK(cudaEventSynchronize(h->ev[1]));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, h->ev[0], h->ev[1]));
+    ms[k] = t / reps;
+  }
+  return check_errors(h);
+}
+
 int ccdgpu_ladder_profile(ccdgpu_handle *h, int32_t reps, double *ms, double *flops,
                           double *bytes) {
   if (!h || reps < 1 || !ms || !flops || !bytes) return CCDGPU_ERR_INVALID_ARGUMENT;

@@ -193,9 +193,19 @@ class CCDSolver:
         names = ["fp64_thin", "fp64_mid", "fp64_wide", "tensor_core"]
         return {n: (ms[k], fl[k], by[k]) for k, n in enumerate(names) if ms[k] > 0}
 
-    TRACE_KERNELS = ["ring_small", "ring_mid", "ring_large", "hh_small", "hh_tiled", "onebody",
+    def kernel_profile(self, reps=5):
+        """Ring, hh-ladder and one-body kernel classes alone (ccdgpu_kernel_profile):
+        {class: (ms, flops, bytes)}; classes without work are left out."""
+        ms, fl, by = (ctypes.c_double * 7)(), (ctypes.c_double * 7)(), (ctypes.c_double * 7)()
+        _check(_native.gpu_lib().ccdgpu_kernel_profile(self._h, reps, ms, fl, by),
+               "ccdgpu_kernel_profile")
+        names = ["ring_small", "ring_mid", "ring_large", "hh_small", "hh_large", "onebody",
+                 "hh_reduce"]
+        return {n: (ms[k], fl[k], by[k]) for k, n in enumerate(names) if by[k] > 0}
+
+    TRACE_KERNELS = ["ring_small", "ring_mid", "ring_large", "hh_small", "hh_large", "onebody",
                      "ladder_thin", "ladder_mid", "ladder_wide", "ladder_tc", "assemble",
-                     "loop_ctl", "energy", "retile", "ladder_reduce"]
+                     "loop_ctl", "energy", "retile", "ladder_reduce", "hh_reduce"]
 
     def trace_arm(self, iteration):
         """Record kernel start times of iteration `iteration` of the next solve (-1 disarms)."""

@@ -261,12 +261,20 @@ int ccdgpu_autotune(ccdgpu_handle *h, int32_t reps, ccdgpu_schedule *chosen, dou
 int ccdgpu_ladder_profile(ccdgpu_handle *h, int32_t reps, double ms[4], double flops[4],
                           double bytes[4]);
 
+/* The other kernels of an iteration, each class launched alone `reps` times on the handle's
+ * stream (after one warm-up launch): average ms per launch, FP64 flops and algorithmic bytes
+ * per launch, indexed ring small (ph', hp' <= 16), ring mid (<= 32), ring large, hh ladder
+ * small (hh <= 16), hh ladder rest, one-body sums, hh-ladder slice reduction.  Amplitudes are
+ * not changed (the kernels write only intermediates).  No counterpart in the reference. */
+int ccdgpu_kernel_profile(ccdgpu_handle *h, int32_t reps, double ms[7], double flops[7],
+                          double bytes[7]);
+
 /* Kernel start-time trace (diagnostics; no counterpart in the reference).  Arm with the index
  * of an iteration of the next solve (-1 disarms); every kernel of that iteration then records
  * the %globaltimer time (ns) at which its first and its last CTA started.  Kernel ids, in this
  * order: ring small, ring mid, ring large, hh ladder small, hh ladder tiled, one-body, pp
  * ladder thin, mid, wide, tensor-core pp ladder, assembly, loop control, energy, FP64 tile
- * refresh, split-K reduction (15). */
+ * refresh, split-K reduction, hh-ladder reduction (16). */
 int ccdgpu_trace_arm(ccdgpu_handle *h, int64_t iteration);
 int ccdgpu_trace_read(ccdgpu_handle *h, uint64_t *first, uint64_t *last, int32_t n);
 

@@ -196,3 +196,15 @@ def test_ladder_profile_reports_every_class():
         # Timing the ladders alone leaves the solve unchanged.
         res = sol.solve(tol=g["tol"])
         assert abs(res.e_corr - g["energies"][-1]) <= 1e-10 * abs(g["energies"][-1])
+
+
+def test_kernel_profile_reports_ring_hh_onebody():
+    g = golden("eg54_s19")
+    with system_for(g) as s, CCDSolver(s) as sol:
+        prof = sol.kernel_profile(reps=2)
+        assert {"ring_large", "hh_small", "hh_large", "onebody", "hh_reduce"} <= set(prof)
+        for name, (ms, fl, by) in prof.items():
+            assert ms > 0 and by > 0
+        # The ring and hh kernels write only intermediates: the solve is unchanged.
+        res = sol.solve(tol=g["tol"])
+        assert abs(res.e_corr - g["energies"][-1]) <= 1e-10 * abs(g["energies"][-1])
