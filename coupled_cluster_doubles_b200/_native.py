@@ -66,7 +66,7 @@ class Options(ctypes.Structure):
 
 class Schedule(ctypes.Structure):
     _fields_ = [("thin_split_mul", c_i32), ("wide_split_mul", c_i32), ("tc_split_mul", c_i32),
-                ("reserved", c_i32 * 5)]
+                ("mid_split_mul", c_i32), ("reserved", c_i32 * 4)]
 
 
 class Result(ctypes.Structure):

@@ -15,19 +15,29 @@ namespace ccd {
 //
 // Operand tiles are stored in HBM already in their shared-memory image so that one bulk copy
 // (TMA) moves a whole stage:
-//   A tiles  [rows][kBK]  row-major, column XOR-swizzled by (row & 15): a warp reading 16
-//                         consecutive rows at one k hits 16 distinct bank pairs.  The last row
-//                         tile of a channel is stored compact (only its real rows).
-//   B tiles  [kBK][nb]    k-major, nb = padded hh columns, read as warp broadcasts.
-// Column classes: thin channels (hh <= 8) use nb in {2, 4, 8} with one row per consumer
-// thread; the others nb = 8*C with 8 rows x C columns per consumer thread (k-major A).
+//   thin channels (hh <= 8, nb in {2, 4, 8}, one row per consumer thread):
+//     A tiles [rows][kBK] row-major, column XOR-swizzled by (row & 15): a warp reading 16
+//             consecutive rows at one k hits 16 distinct bank pairs;
+//     B tiles [kBK][nb] k-major, read as warp broadcasts;
+//   mid and wide channels (nb = 8*C, FP64 MMA fragments):
+//     A tiles [kBK][as] k-major, as = rows rounded up to 8, plus 4;
+//     B tiles [kBK][bs] k-major, bs = nb + 4;
+//     strides of 4 mod 8 doubles put the 4 k-rows of an m8n8k4 fragment load on distinct banks.
+// The last row tile of a channel is stored compact (only its real rows, rounded up to 8).
 constexpr int kBK = 16;        // K depth of one pipeline stage
 constexpr int kStages = 4;     // bulk-copy pipeline depth
 constexpr int kMaxCG = 9;      // column groups of 8 -> up to 72 hh columns
 constexpr int kLadderConsumers = 128;
 constexpr int kLadderThreads = kLadderConsumers + 32;  // + 1 producer warp
+// Mid and wide classes: 8 consumer warps of 16 rows each (two CTAs per SM).
+constexpr int kLadderConsumersMMA = 256;
+__host__ __device__ constexpr int ladder_threads(int cls) {
+  return (cls == 0 ? kLadderConsumers : kLadderConsumersMMA) + 32;
+}
 constexpr int kMaxBM = 128;
 constexpr int kMaxNB = 8 * kMaxCG;
+constexpr int kMaxAS = kMaxBM + 4;  // A stage row stride bound (doubles)
+constexpr int kMaxBS = kMaxNB + 4;  // B stage row stride bound (doubles)
 
 __host__ __device__ inline int swzA(int row, int k) { return row * kBK + (k ^ (row & 15)); }
 // Padded column count of a channel with hh hole pairs.
@@ -35,15 +45,19 @@ __host__ __device__ inline int ladder_nb(int hh) {
   return hh <= 2 ? 2 : hh <= 4 ? 4 : 8 * ((hh + 7) / 8);
 }
 // Rows per tile: thin channels one row per consumer thread; mid and wide ones (nb >= 16)
-// 8 rows x nb/8 columns per thread, 16 row groups.
+// 16 rows x nb columns per consumer warp.
 __host__ __device__ inline int ladder_bm(int nb) { return kLadderConsumers; }
-// A chunks of mid and wide channels are k-major with the rows padded to a multiple of 8 (a
-// thread reads its 8 consecutive rows as 16-byte vectors); thin ones are row-major and
-// XOR-swizzled (one row per thread).
+// A chunks of mid and wide channels are k-major (row stride `arows`, see above); thin ones are
+// row-major and XOR-swizzled (one row per thread).
 __host__ __device__ inline bool ladder_kmajor(int nb) { return nb >= 16; }
+// A row stride (doubles per k row of an A chunk) of a row tile with `rows` real rows.
 __host__ __device__ inline int ladder_arows(int nb, int rows) {
-  return ladder_kmajor(nb) ? ((rows + 7) & ~7) : rows;
+  return ladder_kmajor(nb) ? ((rows + 7) & ~7) + 4 : rows;
 }
+// A image of row tile mt starts at mt * ladder_arows(nb, kMaxBM) * nk * kBK (full tiles).
+__host__ __device__ inline int ladder_arows_full(int nb) { return ladder_arows(nb, kMaxBM); }
+// B row stride (doubles per k row of a B chunk).
+__host__ __device__ inline int ladder_bs(int nb) { return ladder_kmajor(nb) ? nb + 4 : nb; }
 __host__ __device__ inline int ladder_aoff(int nb, int arows, int r, int k) {
   return ladder_kmajor(nb) ? k * arows + r : swzA(r, k);
 }
@@ -87,10 +101,10 @@ __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16 *out, int nt)
 // nseg-1 also runs the T X chunks.
 struct LadderTile {
   int32_t ch, mt, kc0, nks, nkc, nkh, nb, bm, rows, pr, hh, seg, nseg, group;
-  int64_t v_base;    // A tiles of V:  tile base + kc * arows*kBK (tile base = mt*bm*nkc*kBK)
-  int64_t tkt_base;  // B tiles of T:  + kc * kBK*nb
+  int64_t v_base;    // A tiles of V:  + mt*arows_full*nkc*kBK + kc * arows*kBK
+  int64_t tkt_base;  // B tiles of T:  + kc * kBK*bs
   int64_t tmt_base;  // A tiles of T (rows a<=b, K = hh): + mt*bm*nkh*kBK + kh * rows*kBK
-  int64_t xt_base;   // B tiles of X/2: + kh * kBK*nb
+  int64_t xt_base;   // B tiles of X/2: + kh * kBK*bs
   int64_t t_off;     // offset of the channel's pp x hh block in the t2 layout
   int64_t row_off;   // offset into rowmap / mirror
   int64_t part_base; // partial sums of this row block: nseg * bm * nb doubles

@@ -114,19 +114,27 @@ __device__ __forceinline__ bool skip_iteration(const Control *ctl, int gate, int
 }
 
 // ------------------------------------------------------------------------------------------
-// pp ladder + hh-ladder output on the FP64 FMA pipe:
+// pp ladder + hh-ladder output in FP64 (FMA pipe for thin channels, FP64 MMA for the rest):
 //   D[ab,:] = sum_{c<d} V[ab,cd] T[cd,:] + T[ab,:] (X/2)     for packed rows a <= b,
 //   D[ba,:] = -D[ab,:]                                        (antisymmetry of V and T).
 // Warp 4 is the producer: one lane streams pre-tiled A/B stages with bulk copies (TMA, no
 // multicast) into a kStages-deep shared-memory ring guarded by mbarriers.  The 128 consumer
-// threads run register-blocked DFMAs: V rows come from shared memory conflict-free (XOR
-// swizzle), T / X columns are warp broadcasts.  K runs over the c<d pairs (V T) and then over
+// threads run register-blocked DFMAs (thin channels: V rows from shared memory conflict-free
+// by an XOR swizzle, T / X columns as warp broadcasts) or FP64 MMAs (mid and wide channels).  K runs over the c<d pairs (V T) and then over
 // hh (T X) with the same pipeline.  Row blocks whose K is split over several tiles write
 // partial sums that ladder_reduce_kernel adds in segment order (deterministic).
 // ------------------------------------------------------------------------------------------
-__device__ __forceinline__ void consumers_sync() {
-  asm volatile("bar.sync 1, %0;" ::"n"(kLadderConsumers) : "memory");
+
+// FP64 tensor-core MMA (mma.sync m8n8k4, the full-rate FP64 path of sm_100a): lane
+// (g = lane / 4, t = lane % 4) supplies A[g][t] and B[t][g] and accumulates C[g][2t] and
+// C[g][2t + 1].  One instruction does 256 multiply-adds, so the small channel GEMMs are no longer
+// bound by instruction issue and shared-memory loads.
+__device__ __forceinline__ void dmma_884(double (&c)[2], double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+      : "+d"(c[0]), "+d"(c[1])
+      : "d"(a), "d"(b));
 }
+
 
 // Stores the finished values of packed row u_local (cols [c0, c0+n)), or its partial sum.
 struct LadderOut {
@@ -199,7 +207,7 @@ __device__ __forceinline__ bool consume_thin(const LadderTile &tile, const doubl
       atomicOr(err, kErrTimeout);
       return false;
     }
-    const double *A = As + s * (kMaxBM * kBK);
+    const double *A = As + s * (kMaxAS * kBK);
     const double *B = Bs + s * bstage;
 #pragma unroll
     for (int k = 0; k < kBK; ++k) {
@@ -219,22 +227,24 @@ __device__ __forceinline__ bool consume_thin(const LadderTile &tile, const doubl
   return true;
 }
 
-// Mid and wide channels (nb = 8*C, C = 2..9): 16 row groups of 8 consecutive rows x 8 column groups of
-// C columns; A is k-major in shared memory (ladder_aoff), so a thread reads its 8 rows with four
-// 16-byte loads and runs 8*C independent FMAs per k.
+// Mid and wide channels (nb = 8*C, C = 2..9) on the FP64 MMA: consumer warp w owns tile rows
+// [16w, 16w + 16) as 2 row tiles x C column tiles of 8 x 8 (4*C accumulators per lane).  A
+// (k-major, row stride ar) and B (k-major, row stride bs) fragments come from the stage
+// conflict-free: both strides are 4 mod 8 doubles.
 template <int C>
-__device__ __forceinline__ bool consume_wide8(const LadderTile &tile, const double *As,
-                                              const double *Bs, int bstage, uint64_t *bars,
-                                              int tid, const LadderOut &out, int32_t *err) {
-  constexpr int NB = 8 * C;
-  const int r0 = (tid >> 3) * 8, c0 = (tid & 7) * C, lane = tid & 31;
+__device__ __forceinline__ bool consume_mma(const LadderTile &tile, const double *As,
+                                            const double *Bs, int bstage, uint64_t *bars,
+                                            int tid, const LadderOut &out, int32_t *err) {
+  constexpr int NB = 8 * C, BS = NB + 4;
+  const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
   const int ar = ladder_arows(NB, tile.rows);
-  const bool worker = r0 < ar;
-  double acc[8][C];
+  constexpr int MT = 2;
+  const int mtiles = min(MT, max(0, ((tile.rows + 7) >> 3) - MT * warp));  // row tiles with rows
+  double acc[MT][C][2];
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < MT; ++i)
 #pragma unroll
-    for (int j = 0; j < C; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < C; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   const int nchunks = tile.nks + tile.nkh;
   for (int c = 0; c < nchunks; ++c) {
     const int s = c % kStages;
@@ -242,40 +252,41 @@ __device__ __forceinline__ bool consume_wide8(const LadderTile &tile, const doub
       atomicOr(err, kErrTimeout);
       return false;
     }
-    const double *A = As + s * (kMaxBM * kBK) + r0;
-    const double *B = Bs + s * bstage + c0;
-    if (worker) {
-#pragma unroll 2
-      for (int k = 0; k < kBK; ++k) {
-        double a[8], b[C];
+    if (mtiles > 0) {
+      const double *A = As + s * (kMaxAS * kBK) + t * ar + 8 * MT * warp + g;
+      const double *B = Bs + s * bstage + t * BS + g;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const double2 v = *reinterpret_cast<const double2 *>(A + k * ar + 2 * i);
-          a[2 * i] = v.x;
-          a[2 * i + 1] = v.y;
-        }
+      for (int k4 = 0; k4 < kBK / 4; ++k4) {
+        double a[MT], b[C];
 #pragma unroll
-        for (int j = 0; j < C; ++j) b[j] = B[k * NB + j];
+        for (int i = 0; i < MT; ++i) a[i] = A[k4 * 4 * ar + 8 * i];
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
+        for (int j = 0; j < C; ++j) b[j] = B[k4 * 4 * BS + 8 * j];
 #pragma unroll
-          for (int j = 0; j < C; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        for (int i = 0; i < MT; ++i)
+          if (i < mtiles) {
+#pragma unroll
+            for (int j = 0; j < C; ++j) dmma_884(acc[i][j], a[i], b[j]);
+          }
       }
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(smem_u32(&bars[kStages + s]));
   }
-  if (worker) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) out.row(r0 + i, c0, acc[i], C);
-  }
+  for (int i = 0; i < MT; ++i)
+    if (i < mtiles) {
+#pragma unroll
+      for (int j = 0; j < C; ++j)
+        out.row(8 * MT * warp + 8 * i + g, 8 * j + 2 * t, acc[i][j], 2);
+    }
   return true;
 }
 
 // Column classes: CLS 0 = thin (nb <= 8), 1 = mid (nb 16..32), 2 = wide (nb 40..72).  Separate
 // instantiations keep the register budget of narrow channels independent of the 72-column case.
 template <int CLS>
-__global__ void __launch_bounds__(kLadderThreads, CLS == 0 ? 3 : CLS == 1 ? 2 : 1)
+__global__ void __launch_bounds__(ladder_threads(CLS), CLS == 0 ? 3 : CLS == 1 ? 2 : 1)
 pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict__ v_t,
                  const double *__restrict__ t_kt, const double *__restrict__ t_mt,
                  const double *__restrict__ x_t, const int32_t *__restrict__ rowmap,
@@ -284,28 +295,29 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict_
   if (skip_iteration(ctl, gate, kTrLadderThin + CLS)) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double *As = reinterpret_cast<double *>(smem_raw);
-  double *Bs = As + kStages * kMaxBM * kBK;
+  double *Bs = As + kStages * kMaxAS * kBK;
   constexpr bool WIDE = CLS > 0;
-  const int bstage = WIDE ? kBK * kMaxNB : kBK * 8;
+  const int bstage = WIDE ? kBK * kMaxBS : kBK * 8;
   uint64_t *bars = reinterpret_cast<uint64_t *>(Bs + kStages * bstage);
   const LadderTile tile = tiles[blockIdx.x];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(smem_u32(&bars[s]), 1);
-      mbar_init(smem_u32(&bars[kStages + s]), kLadderConsumers / 32);
+      mbar_init(smem_u32(&bars[kStages + s]), (ladder_threads(CLS) - 32) / 32);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
 
-  if (warp == kLadderConsumers / 32) {
+  if (warp == (ladder_threads(CLS) - 32) / 32) {
     if (lane == 0) {
       const int ar = ladder_arows(tile.nb, tile.rows);
-      const uint32_t abytes = ar * kBK * 8, bbytes = kBK * tile.nb * 8;
+      const int bs = ladder_bs(tile.nb), af = ladder_arows_full(tile.nb);
+      const uint32_t abytes = ar * kBK * 8, bbytes = kBK * bs * 8;
       const int nchunks = tile.nks + tile.nkh;
-      const int64_t vtile = tile.v_base + (int64_t)tile.mt * tile.bm * tile.nkc * kBK;
-      const int64_t ttile = tile.tmt_base + (int64_t)tile.mt * tile.bm * tile.nkh * kBK;
+      const int64_t vtile = tile.v_base + (int64_t)tile.mt * af * tile.nkc * kBK;
+      const int64_t ttile = tile.tmt_base + (int64_t)tile.mt * af * tile.nkh * kBK;
       for (int c = 0; c < nchunks; ++c) {
         const int s = c % kStages;
         if (c >= kStages && !mbar_wait(smem_u32(&bars[kStages + s]), ((c / kStages) - 1) & 1)) {
@@ -316,15 +328,15 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict_
         if (c < tile.nks) {
           const int kc = tile.kc0 + c;
           asrc = v_t + vtile + (int64_t)kc * ar * kBK;
-          bsrc = t_kt + tile.tkt_base + (int64_t)kc * kBK * tile.nb;
+          bsrc = t_kt + tile.tkt_base + (int64_t)kc * kBK * bs;
         } else {
           const int kh = c - tile.nks;
           asrc = t_mt + ttile + (int64_t)kh * ar * kBK;
-          bsrc = x_t + tile.xt_base + (int64_t)kh * kBK * tile.nb;
+          bsrc = x_t + tile.xt_base + (int64_t)kh * kBK * bs;
         }
         const uint32_t full = smem_u32(&bars[s]);
         mbar_expect_tx(full, abytes + bbytes);
-        bulk_g2s(smem_u32(As + s * kMaxBM * kBK), asrc, abytes, full);
+        bulk_g2s(smem_u32(As + s * kMaxAS * kBK), asrc, abytes, full);
         bulk_g2s(smem_u32(Bs + s * bstage), bsrc, bbytes, full);
       }
     }
@@ -341,7 +353,7 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict_
     }
   } else {
 #define CCD_WIDE8_CASE(n) \
-  case n: ok = consume_wide8<n>(tile, As, Bs, bstage, bars, tid, out, err); break;
+  case n: ok = consume_mma<n>(tile, As, Bs, bstage, bars, tid, out, err); break;
     if (CLS == 1) {
       switch (tile.nb / 8) { CCD_WIDE8_CASE(2) CCD_WIDE8_CASE(3) CCD_WIDE8_CASE(4) default: break; }
     } else {
@@ -397,16 +409,6 @@ __device__ __forceinline__ void opgemm(const double *__restrict__ A, int lda,
 }
 __host__ __device__ inline int even_up(int n) { return (n + 1) & ~1; }
 
-// FP64 tensor-core MMA (mma.sync m8n8k4, the full-rate FP64 path of sm_100a): lane
-// (g = lane / 4, t = lane % 4) supplies A[g][t] and B[t][g] and accumulates C[g][2t] and
-// C[g][2t + 1].  One instruction does 256 multiply-adds, so the small channel GEMMs are no longer
-// bound by instruction issue and shared-memory loads.
-__device__ __forceinline__ void dmma_884(double (&c)[2], double a, double b) {
-  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
-      : "+d"(c[0]), "+d"(c[1])
-      : "d"(a), "d"(b));
-}
-
 // ------------------------------------------------------------------------------------------
 // hh ladder intermediate (calc.cpp:141-160 and the one-body sums of calc.cpp:18-20, 82-84):
 //   P = V_hhpp T (K = pp),  X = V_hhhh + 0.5 P  (reference layout, and X/2 as B tiles),
@@ -430,7 +432,8 @@ __device__ __forceinline__ void hh_finish(const ChanInfo &ch, int kl, int ij, do
   const int hh = ch.hh, idx = kl * hh + ij;
   const double x = v_hhhh[ch.x_off + idx] + 0.5 * p;
   x_ref[ch.x_off + idx] = x;
-  x_t[ch.xt_base + (int64_t)(kl / kBK) * kBK * ch.nb + (kl % kBK) * ch.nb + ij] = 0.5 * x;
+  const int bs = ladder_bs(ch.nb);
+  x_t[ch.xt_base + (int64_t)(kl / kBK) * kBK * bs + (kl % kBK) * bs + ij] = 0.5 * x;
   if (nt) {
     __nv_bfloat16 hv[3];
     split_bf16(0.5 * x, hv, nt);
@@ -822,11 +825,13 @@ __device__ __forceinline__ void write_t_tiles(const ChanInfo &ch, const int2 *__
                                               int ab, int ij, double t, double *t_kt,
                                               double *t_mt) {
   const int2 q = pk_idx[ch.pp_off + ab];
-  if (q.x >= 0) t_kt[ch.tkt_base + (int64_t)(q.x / kBK) * kBK * ch.nb + (q.x % kBK) * ch.nb + ij] = t;
+  const int bs = ladder_bs(ch.nb);
+  if (q.x >= 0) t_kt[ch.tkt_base + (int64_t)(q.x / kBK) * kBK * bs + (q.x % kBK) * bs + ij] = t;
   if (q.y >= 0) {
     const int mt = q.y / ch.bm, rows = min(ch.bm, ch.pr - mt * ch.bm);
     const int ar = ladder_arows(ch.nb, rows);
-    t_mt[ch.tmt_base + (int64_t)mt * ch.bm * ch.nkh * kBK + (int64_t)(ij / kBK) * ar * kBK +
+    t_mt[ch.tmt_base + (int64_t)mt * ladder_arows_full(ch.nb) * ch.nkh * kBK +
+         (int64_t)(ij / kBK) * ar * kBK +
          ladder_aoff(ch.nb, ar, q.y - mt * ch.bm, ij % kBK)] = t;
   }
 }

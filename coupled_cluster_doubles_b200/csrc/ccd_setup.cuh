@@ -40,7 +40,7 @@ __global__ void tile_v_kernel(const ChanInfo *__restrict__ chans, const int2 *__
   const double *src = vraw + vraw_off[it.x] + (int64_t)ab * ch.pp;
   const int mt = u / ch.bm, rows = min(ch.bm, ch.pr - mt * ch.bm);
   const int ar = ladder_arows(ch.nb, rows);
-  const int64_t tb = ch.vkt_base + (int64_t)mt * ch.bm * ch.nkc * kBK;
+  const int64_t tb = ch.vkt_base + (int64_t)mt * ladder_arows_full(ch.nb) * ch.nkc * kBK;
   for (int w = threadIdx.x; w < ch.pk; w += blockDim.x)
     v_t[tb + (int64_t)(w / kBK) * ar * kBK + ladder_aoff(ch.nb, ar, u - mt * ch.bm, w % kBK)] =
         src[kcol[ch.pk_off + w]];
@@ -149,7 +149,7 @@ __global__ void gen_v_kernel(const ChanInfo *__restrict__ chans, const int2 *__r
   const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + u]];
   const int mt = u / ch.bm, rows = min(ch.bm, ch.pr - mt * ch.bm);
   const int ar = ladder_arows(ch.nb, rows);
-  const int64_t tb = ch.vkt_base + (int64_t)mt * ch.bm * ch.nkc * kBK;
+  const int64_t tb = ch.vkt_base + (int64_t)mt * ladder_arows_full(ch.nb) * ch.nkc * kBK;
   const int mtc = u >> 7, r = u & 127;
   const int rg = (min(kTcBM, ch.pr - mtc * kTcBM) + 7) >> 3;
   const int64_t tbc = ch.vtc_base + (int64_t)mtc * kTcBM * ch.nkct * kTcKC;

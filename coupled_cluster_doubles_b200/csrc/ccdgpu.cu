@@ -245,17 +245,22 @@ int upload_runs(ccdgpu_handle *h, T *dst, const std::vector<const T *> &src,
 int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
   const std::vector<ChanInfo> &chans = h->host_chans;
   auto cls_of = [](int nb) { return nb <= 8 ? 0 : nb <= 32 ? 1 : 2; };
-  int64_t blocks_thin = 0, blocks_wide = 0;
-  for (const ChanInfo &a : chans) (a.nb <= 8 ? blocks_thin : blocks_wide) += a.nmt;
+  int64_t blocks[3] = {0, 0, 0};
+  for (const ChanInfo &a : chans) blocks[cls_of(a.nb)] += a.nmt;
   const int64_t kSMs = 148;
-  const int want_thin = blocks_thin >= kSMs ? 1 : (int)std::min<int64_t>(8, ceil_div(sch.thin_split_mul * kSMs, std::max<int64_t>(blocks_thin, 1)));
-  const int want_wide = (int)std::min<int64_t>(64, std::max<int64_t>(1, ceil_div(sch.wide_split_mul * kSMs, std::max<int64_t>(blocks_wide, 1))));
+  const int mid_mul = sch.mid_split_mul > 0 ? sch.mid_split_mul : sch.wide_split_mul;
+  auto want_of = [&](int64_t mul, int64_t b) {
+    return (int)std::min<int64_t>(64, std::max<int64_t>(1, ceil_div(mul * kSMs, std::max<int64_t>(b, 1))));
+  };
+  const int want_cls[3] = {
+      blocks[0] >= kSMs ? 1 : (int)std::min<int64_t>(8, ceil_div(sch.thin_split_mul * kSMs, std::max<int64_t>(blocks[0], 1))),
+      want_of(mid_mul, blocks[1]), want_of(sch.wide_split_mul, blocks[2])};
   std::vector<LadderTile> tiles;
   int64_t lpart_tot = 0;
   int32_t groups = 0;
   for (int ai = 0; ai < h->n_act; ai++) {
     const ChanInfo &a = chans[ai];
-    const int want = a.nb <= 8 ? want_thin : want_wide;
+    const int want = want_cls[cls_of(a.nb)];
     const int min_chunks = 4;
     const int nseg = std::max(1, std::min(want, a.nkc / min_chunks));
     for (int mt = 0; mt < a.nmt; mt++) {
@@ -487,12 +492,12 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     xttc += (int64_t)ci.nkht * (ci.nbt / 8) * kTcGroup;
     const int nb = ci.nb;
     pp_tot += pp; hh_tot += hh; x_tot += hh * hh;
-    tkt += (int64_t)ci.nkc * kBK * nb;
-    // Compact last row tile (rows padded to 8 for k-major wide channels).
-    const int64_t arows_tot = (int64_t)(ci.nmt - 1) * ci.bm +
+    tkt += (int64_t)ci.nkc * kBK * ladder_bs(nb);
+    // Full row tiles at their A stride, then the compact last one.
+    const int64_t arows_tot = (int64_t)(ci.nmt - 1) * ladder_arows_full(ci.nb) +
                               ladder_arows(ci.nb, ci.pr - (ci.nmt - 1) * ci.bm);
     tmt += (int64_t)ci.nkh * arows_tot * kBK;
-    xt += (int64_t)ci.nkh * kBK * nb;
+    xt += (int64_t)ci.nkh * kBK * ladder_bs(nb);
     vt += (int64_t)ci.nkc * arows_tot * kBK;
     part_tot += (int64_t)ci.nhht * hh * hh;
     vraw_off.push_back(vraw_tot);
@@ -836,8 +841,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   CK(cudaMallocHost(&h->h_ctl, sizeof(Control)));
   std::memset(h->h_ctl, 0, sizeof(Control));
 
-  h->ladder_smem = (size_t)kStages * (kMaxBM * kBK + kBK * kMaxNB) * 8 + 2 * kStages * 8;
-  h->ladder_smem_thin = (size_t)kStages * (kMaxBM * kBK + kBK * 8) * 8 + 2 * kStages * 8;
+  h->ladder_smem = (size_t)kStages * (kMaxAS * kBK + kBK * kMaxBS) * 8 + 2 * kStages * 8;
+  h->ladder_smem_thin = (size_t)kStages * (kMaxAS * kBK + kBK * 8) * 8 + 2 * kStages * 8;
   CK(cudaFuncSetAttribute(pp_ladder_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)h->ladder_smem_thin));
   CK(cudaFuncSetAttribute(pp_ladder_kernel<0>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
@@ -961,14 +966,14 @@ int launch_pp_ladder(ccdgpu_handle *h, cudaStream_t st) {
     CK(cudaEventRecord(h->ev_fork2, st));
     CK(cudaStreamWaitEvent(h->s2, h->ev_fork2, 0));
     if (h->n_cls[2]) {
-      pp_ladder_kernel<2><<<h->n_cls[2], kLadderThreads, h->ladder_smem, h->s2>>>(
+      pp_ladder_kernel<2><<<h->n_cls[2], ladder_threads(2), h->ladder_smem, h->s2>>>(
           t_wide, h->v_t, h->t_kt, h->t_mt, h->x_t, h->rowmap, h->mirror, h->dmat, h->lpart,
           h->lcounters, h->ctl, h->err, 0);
       h->launches++;
       CK(cudaGetLastError());
     }
     if (h->n_cls[1]) {
-      pp_ladder_kernel<1><<<h->n_cls[1], kLadderThreads, h->ladder_smem, h->s2>>>(
+      pp_ladder_kernel<1><<<h->n_cls[1], ladder_threads(1), h->ladder_smem, h->s2>>>(
           t_mid, h->v_t, h->t_kt, h->t_mt, h->x_t, h->rowmap, h->mirror, h->dmat, h->lpart,
           h->lcounters, h->ctl, h->err, 0);
       h->launches++;
@@ -1748,7 +1753,7 @@ int ccdgpu_ladder_profile(ccdgpu_handle *h, int32_t reps, double *ms, double *fl
       if (k == 3) return launch_pp_ladder_tc(h, h->s0);
       const size_t smem = k == 0 ? h->ladder_smem_thin : h->ladder_smem;
       auto kern = k == 0 ? pp_ladder_kernel<0> : k == 1 ? pp_ladder_kernel<1> : pp_ladder_kernel<2>;
-      kern<<<h->n_cls[k], kLadderThreads, smem, h->s0>>>(start[k], h->v_t, h->t_kt, h->t_mt, h->x_t,
+      kern<<<h->n_cls[k], ladder_threads(k), smem, h->s0>>>(start[k], h->v_t, h->t_kt, h->t_mt, h->x_t,
                                                         h->rowmap, h->mirror, h->dmat, h->lpart,
                                                         h->lcounters, h->ctl, h->err, 0);
       CK(cudaGetLastError());
@@ -1774,7 +1779,8 @@ int ccdgpu_ladder_profile(ccdgpu_handle *h, int32_t reps, double *ms, double *fl
 }
 
 int ccdgpu_set_schedule(ccdgpu_handle *h, const ccdgpu_schedule *sch) {
-  if (!h || !sch || sch->thin_split_mul < 1 || sch->wide_split_mul < 1 || sch->tc_split_mul < 1)
+  if (!h || !sch || sch->thin_split_mul < 1 || sch->wide_split_mul < 1 || sch->tc_split_mul < 1 ||
+      sch->mid_split_mul < 0)
     return CCDGPU_ERR_INVALID_ARGUMENT;
   CK(cudaSetDevice(h->opt.device));
   return make_ladder_tiles(h, *sch);
@@ -1809,9 +1815,11 @@ int ccdgpu_autotune(ccdgpu_handle *h, int32_t reps, ccdgpu_schedule *chosen, dou
   };
   ccdgpu_schedule best = h->schedule;
   double best64 = 0, besttc = 0;
-  // FP64 ladder: split factors of the thin and the mid/wide classes.
-  const int thin_c[] = {1, 2, 4}, wide_c[] = {1, 3, 6, 12, 24, 48};
+  // FP64 ladder: split factors of the thin and the mid/wide classes (mid as wide), then the
+  // mid class's own.
+  const int thin_c[] = {1, 2, 4}, wide_c[] = {1, 2, 3, 6, 12, 24, 48};
   bool first = true;
+  best.mid_split_mul = 0;
   for (int tm : thin_c)
     for (int wm : wide_c) {
       ccdgpu_schedule c = best;
@@ -1823,6 +1831,14 @@ int ccdgpu_autotune(ccdgpu_handle *h, int32_t reps, ccdgpu_schedule *chosen, dou
       if (first || ms < best64) { best64 = ms; best.thin_split_mul = tm; best.wide_split_mul = wm; }
       first = false;
     }
+  for (int mm : wide_c) {
+    ccdgpu_schedule c = best;
+    c.mid_split_mul = mm;
+    if ((rc = make_ladder_tiles(h, c))) return rc;
+    double ms = 0;
+    if ((rc = time_ladder(false, &ms))) return rc;
+    if (ms < best64) { best64 = ms; best.mid_split_mul = mm; }
+  }
   // Tensor-core ladder: split factor.
   if (h->nt) {
     first = true;

@@ -170,10 +170,10 @@ class CCDSolver:
         sch = _native.Schedule()
         _check(_native.gpu_lib().ccdgpu_get_schedule(self._h, ctypes.byref(sch)), "schedule")
         return {"thin_split_mul": sch.thin_split_mul, "wide_split_mul": sch.wide_split_mul,
-                "tc_split_mul": sch.tc_split_mul}
+                "tc_split_mul": sch.tc_split_mul, "mid_split_mul": sch.mid_split_mul}
 
-    def set_schedule(self, thin_split_mul=1, wide_split_mul=3, tc_split_mul=2):
-        sch = _native.Schedule(thin_split_mul, wide_split_mul, tc_split_mul)
+    def set_schedule(self, thin_split_mul=1, wide_split_mul=3, tc_split_mul=2, mid_split_mul=0):
+        sch = _native.Schedule(thin_split_mul, wide_split_mul, tc_split_mul, mid_split_mul)
         _check(_native.gpu_lib().ccdgpu_set_schedule(self._h, ctypes.byref(sch)), "set_schedule")
 
     def autotune(self, reps=5):

@@ -242,9 +242,10 @@ int ccdgpu_work_per_iteration(const ccdgpu_handle *h, double *flops, double *lad
  * FP64 thin class (hh <= 8), the FP64 mid/wide classes, and the tensor-core ladder. */
 typedef struct ccdgpu_schedule {
   int32_t thin_split_mul;      /* default 1 */
-  int32_t wide_split_mul;      /* default 3 */
+  int32_t wide_split_mul;      /* default 3: FP64 wide class (nb > 32; also mid when mid is 0) */
   int32_t tc_split_mul;        /* default 2 */
-  int32_t reserved[5];
+  int32_t mid_split_mul;       /* default 0 = as wide_split_mul: FP64 mid class (nb 16..32) */
+  int32_t reserved[4];
 } ccdgpu_schedule;
 int ccdgpu_set_schedule(ccdgpu_handle *h, const ccdgpu_schedule *sch);
 int ccdgpu_get_schedule(const ccdgpu_handle *h, ccdgpu_schedule *sch);

@@ -179,7 +179,8 @@ def test_autotune_and_schedules_keep_results(precision):
         res = sol.solve(tol=g["tol"])
         assert abs(res.e_corr - g["energies"][-1]) <= 1e-10 * abs(g["energies"][-1])
         for sch2 in [dict(thin_split_mul=4, wide_split_mul=12, tc_split_mul=8),
-                     dict(thin_split_mul=1, wide_split_mul=1, tc_split_mul=1)]:
+                     dict(thin_split_mul=1, wide_split_mul=1, tc_split_mul=1),
+                     dict(thin_split_mul=2, wide_split_mul=2, tc_split_mul=4, mid_split_mul=24)]:
             sol.set_schedule(**sch2)
             sol.reset()
             r2 = sol.solve(tol=g["tol"])
