@@ -88,10 +88,33 @@ __host__ __device__ inline int tc_off_mn(int n, int k) {
 }
 // x -> nt bf16 terms, each the round-to-nearest of what the previous ones leave (the
 // remainders are exact in double).
+// bf16 bits of a double h that has at most 8 significant bits: sign, exponent rebased from
+// 1023 to 127, top 7 mantissa bits.  Zero and magnitudes below bf16's normal range (2^-126)
+// give a signed zero; NaN stays NaN.
+__device__ __forceinline__ __nv_bfloat16 bf16_of_short(double h) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(h);
+  const unsigned short sign = (unsigned short)((b >> 48) & 0x8000u);
+  const int e = (int)((b >> 52) & 0x7FF) - 1023 + 127;
+  unsigned short bits;
+  if (e <= 0) bits = sign;
+  else if (e >= 255) bits = (unsigned short)(sign | 0x7F80u | ((b << 12) ? 0x40u : 0u));
+  else bits = (unsigned short)(sign | (e << 7) | (unsigned)((b >> 45) & 0x7F));
+  return __ushort_as_bfloat16(bits);
+}
+
+// x = t_0 + t_1 (+ t_2) + remainder, each t_p a bf16 (nt terms): t_p is the remainder rounded
+// to 8 significant bits by Dekker's splitting (Dekker 1971: c = r (2^45 + 1), t = c - (c - r)),
+// which is exact in bf16, and the next remainder r - t_p is exact in FP64.  Only FP64 and
+// integer arithmetic, no conversion instructions.
 __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16 *out, int nt) {
   for (int p = 0; p < nt; ++p) {
-    out[p] = __double2bfloat16(x);
-    x -= (double)__bfloat162float(out[p]);
+    // Explicitly rounded operations: an FMA contraction of c - x would skip the rounding of c
+    // that the splitting relies on.
+    const double c = __dmul_rn(x, 35184372088833.0);  // 2^45 + 1
+    double hi = __dsub_rn(c, __dsub_rn(c, x));
+    if (fabs(hi) < 1.1754943508222875e-38) hi = 0.0;  // below bf16's normal range
+    out[p] = bf16_of_short(hi);
+    x = __dsub_rn(x, hi);
   }
 }
 
@@ -131,6 +154,21 @@ struct ChanInfo {
 // hh-ladder unit: rows [k0, k0+rows) of channel ch (slice idx), a chunk of P rows.
 struct HHTile {
   int32_t ch, k0, idx, rows, chunk, pad;
+};
+
+// Fused assembly, static data of packed row u of a channel (index row_off + u): rows ab and
+// ba = mirror (ba = ab when a = b) as offsets ab * hh, ba * hh in the channel block, their
+// ladder operand indices (pk_idx), the particle indices a - np, b - np and e_a, e_b.
+struct AsmRowStatic {
+  int32_t o_ab, o_ba;
+  int32_t qa_x, qa_y, qb_x, qb_y;
+  int32_t pa, pb;
+  double ea, eb;
+};
+// ... and of column j (index hh_off + j): ji, the hole indices i, j and e_i + e_j.
+struct AsmColStatic {
+  int32_t js, i, j, pad;
+  double eij;
 };
 
 // Per active modified channel.

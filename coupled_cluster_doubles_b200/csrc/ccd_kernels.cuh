@@ -821,10 +821,8 @@ __global__ void onebody_fused_kernel(int np, int nsp, const int64_t *__restrict_
 // Writes one amplitude into the ladder operand tiles: the B tiles of V T (rows c<d) and the A
 // tiles of T X (rows a<=b, compact last row tile).  pk_idx[AB] = (K index or -1, packed row
 // or -1).
-__device__ __forceinline__ void write_t_tiles(const ChanInfo &ch, const int2 *__restrict__ pk_idx,
-                                              int ab, int ij, double t, double *t_kt,
-                                              double *t_mt) {
-  const int2 q = pk_idx[ch.pp_off + ab];
+__device__ __forceinline__ void write_t_tiles_q(const ChanInfo &ch, int2 q, int ij, double t,
+                                                double *t_kt, double *t_mt) {
   const int bs = ladder_bs(ch.nb);
   if (q.x >= 0) t_kt[ch.tkt_base + (int64_t)(q.x / kBK) * kBK * bs + (q.x % kBK) * bs + ij] = t;
   if (q.y >= 0) {
@@ -835,16 +833,20 @@ __device__ __forceinline__ void write_t_tiles(const ChanInfo &ch, const int2 *__
          ladder_aoff(ch.nb, ar, q.y - mt * ch.bm, ij % kBK)] = t;
   }
 }
+__device__ __forceinline__ void write_t_tiles(const ChanInfo &ch, const int2 *__restrict__ pk_idx,
+                                              int ab, int ij, double t, double *t_kt,
+                                              double *t_mt) {
+  write_t_tiles_q(ch, pk_idx[ch.pp_off + ab], ij, t, t_kt, t_mt);
+}
 
 // The same amplitude into the mixed-precision operand images: nt bf16 terms of T in the
 // tensor-core chunk layout (tc_off), V T operand B (K = c<d pair) and T X operand A (rows a<=b,
 // compact last 128-row tile, K = hh).
-__device__ __forceinline__ void write_t_tiles_tc(const ChanInfo &ch,
-                                                 const int2 *__restrict__ pk_idx, int ab, int ij,
-                                                 double t, int nt, __nv_bfloat16 *tkt_tc,
+__device__ __forceinline__ void write_t_tiles_tc(const ChanInfo &ch, int2 q, int ij, double t,
+                                                 int nt, __nv_bfloat16 *tkt_tc,
                                                  int64_t tkt_stride, __nv_bfloat16 *tmt_tc,
                                                  int64_t tmt_stride) {
-  const int2 q = pk_idx[ch.pp_off + ab];
+  if (q.x < 0 && q.y < 0) return;  // row ba of a mirrored pair: in neither image
   __nv_bfloat16 hv[3];
   split_bf16(t, hv, nt);
   if (q.x >= 0) {
@@ -909,9 +911,12 @@ __device__ __forceinline__ double asm_value(double v, double dm, double r_j, dou
   return mixing * value + (1. - mixing) * t_j;
 }
 
+// Shared-memory tables of a CTA's rows and of its channel's columns: the static parts come from
+// AsmRowStatic / AsmColStatic (built at create), y_a, y_b, x_i, x_j are the current one-body sums.
 struct AsmRowInfo {
   int32_t o_ab, o_ba;  // row offsets inside the channel block (ab * hh, ba * hh)
-  int32_t ab, mirrored;
+  int2 qa, qb;         // ladder operand indices of rows ab and ba (pk_idx)
+  int32_t mirrored, pad;
   double ya, yb, ea, eb;
 };
 struct AsmColInfo {
@@ -921,16 +926,15 @@ struct AsmColInfo {
 
 __global__ void __launch_bounds__(kAsmThreads, 3)
 assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__restrict__ chans,
-                      const int2 *__restrict__ pp_pairs, const int2 *__restrict__ hh_pairs,
-                      const int32_t *__restrict__ hh_swap, const int32_t *__restrict__ rowmap,
-                      const int32_t *__restrict__ mirror, const int2 *__restrict__ pk_idx,
+                      const AsmRowStatic *__restrict__ asm_rows,
+                      const AsmColStatic *__restrict__ asm_cols,
                       const double *__restrict__ v_pphh, const double *__restrict__ dmat,
                       const double *__restrict__ d_ring, const int32_t *__restrict__ g_ai_jb,
                       double *__restrict__ old_phhp, const double *__restrict__ xh,
-                      const double *__restrict__ yp, const double *__restrict__ eps, int np,
-                      double *tbuf0, double *tbuf1, double *__restrict__ t_kt,
-                      double *__restrict__ t_mt, double *__restrict__ epart, int32_t *ticket,
-                      Control *ctl, __nv_bfloat16 *__restrict__ tkt_tc, int64_t tkt_tc_stride,
+                      const double *__restrict__ yp, double *tbuf0, double *tbuf1,
+                      double *__restrict__ t_kt, double *__restrict__ t_mt,
+                      double *__restrict__ epart, int32_t *ticket, Control *ctl,
+                      __nv_bfloat16 *__restrict__ tkt_tc, int64_t tkt_tc_stride,
                       __nv_bfloat16 *__restrict__ tmt_tc, int64_t tmt_tc_stride, int nt,
                       int gate) {
   if (skip_iteration(ctl, gate, kTrAssemble)) return;
@@ -946,27 +950,28 @@ assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__r
   const int hh = ch.hh;
   const int u0 = (int)(rg.e0 / hh), nrows = (int)(rg.e1 / hh) - u0;
   for (int r = threadIdx.x; r < nrows; r += kAsmThreads) {
-    const int ab = rowmap[ch.row_off + u0 + r], mi = mirror[ch.row_off + u0 + r];
-    const int2 pab = pp_pairs[ch.pp_off + ab];
+    const AsmRowStatic s = asm_rows[ch.row_off + u0 + r];
     AsmRowInfo ri;
-    ri.ab = ab;
-    ri.mirrored = mi >= 0;
-    ri.o_ab = ab * hh;
-    ri.o_ba = (mi >= 0 ? mi : ab) * hh;
-    ri.ya = yp[pab.x - np];
-    ri.yb = yp[pab.y - np];
-    ri.ea = eps[pab.x];
-    ri.eb = eps[pab.y];
+    ri.o_ab = s.o_ab;
+    ri.o_ba = s.o_ba;
+    ri.qa = make_int2(s.qa_x, s.qa_y);
+    ri.qb = make_int2(s.qb_x, s.qb_y);
+    ri.mirrored = s.o_ba != s.o_ab;
+    ri.pad = 0;
+    ri.ya = yp[s.pa];
+    ri.yb = yp[s.pb];
+    ri.ea = s.ea;
+    ri.eb = s.eb;
     rows[r] = ri;
   }
   for (int j = threadIdx.x; j < hh; j += kAsmThreads) {
-    const int2 pij = hh_pairs[ch.hh_off + j];
+    const AsmColStatic s = asm_cols[ch.hh_off + j];
     AsmColInfo ci;
-    ci.js = hh_swap[ch.hh_off + j];
+    ci.js = s.js;
     ci.pad = 0;
-    ci.xi = xh[pij.x];
-    ci.xj = xh[pij.y];
-    ci.eij = eps[pij.x] + eps[pij.y];
+    ci.xi = xh[s.i];
+    ci.xj = xh[s.j];
+    ci.eij = s.eij;
     cols[j] = ci;
   }
   __syncthreads();
@@ -975,6 +980,9 @@ assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__r
   const int32_t *gb = g_ai_jb + ch.t_off;
   double *nb = t_new + ch.t_off;
   const int n = nrows * hh;
+  // q / hh as a multiply-high by ceil(2^32 / hh) (Granlund-Montgomery): exact for
+  // q < 2^32 / hh (q < 2^11 here); hh = 1 has no 32-bit multiplier and divides trivially.
+  const uint32_t hh_magic = hh > 1 ? 0xFFFFFFFFu / (uint32_t)hh + 1u : 0u;
   double corr = 0.0;
   // kAsmPerThread elements per thread: every load of all of them is issued before the first
   // store (t_new may alias t_old for the compiler, which would otherwise serialise them).
@@ -987,7 +995,7 @@ assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__r
     for (int u = 0; u < kAsmPerThread; ++u) {
       const int q = q0 + u * kAsmThreads;
       if (q >= n) continue;
-      const int r = q / hh, j = q - r * hh;
+      const int r = hh > 1 ? (int)__umulhi((uint32_t)q, hh_magic) : q, j = q - r * hh;
       const int o_ab = rows[r].o_ab, o_ba = rows[r].o_ba, js = cols[j].js;
       rr[u] = r; jj[u] = j;
       a1[u] = o_ab + j; b1[u] = o_ba + j;
@@ -1008,9 +1016,9 @@ assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__r
                                   ci.eij - ri.ea - ri.eb, mixing);
       nb[a1[u]] = t1;
       old_phhp[gv[u][0]] = t1;
-      if (nt) write_t_tiles_tc(ch, pk_idx, ri.ab, j, t1, nt, tkt_tc, tkt_tc_stride, tmt_tc,
+      if (nt) write_t_tiles_tc(ch, ri.qa, j, t1, nt, tkt_tc, tkt_tc_stride, tmt_tc,
                                tmt_tc_stride);
-      else write_t_tiles(ch, pk_idx, ri.ab, j, t1, t_kt, t_mt);
+      else write_t_tiles_q(ch, ri.qa, j, t1, t_kt, t_mt);
       corr += vv[u][0] * t1;
       if (ri.mirrored) {
         // Row ba: the same formula with a and b exchanged.
@@ -1019,9 +1027,9 @@ assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__r
                                     ci.eij - ri.eb - ri.ea, mixing);
         nb[b1[u]] = t2;
         old_phhp[gv[u][1]] = t2;
-        if (nt) write_t_tiles_tc(ch, pk_idx, ri.o_ba / hh, j, t2, nt, tkt_tc, tkt_tc_stride,
-                                 tmt_tc, tmt_tc_stride);
-        else write_t_tiles(ch, pk_idx, ri.o_ba / hh, j, t2, t_kt, t_mt);
+        if (nt) write_t_tiles_tc(ch, ri.qb, j, t2, nt, tkt_tc, tkt_tc_stride, tmt_tc,
+                                 tmt_tc_stride);
+        else write_t_tiles_q(ch, ri.qb, j, t2, t_kt, t_mt);
         corr += vv[u][1] * t2;
       }
     }
@@ -1144,8 +1152,8 @@ __global__ void map_to_kernel(const ElemRange *__restrict__ ranges, const ChanIn
     const int64_t loc = e - ch.t_off;
     const int ab = (int)(loc / ch.hh), ij = (int)(loc - (int64_t)ab * ch.hh);
     write_t_tiles(ch, pk_idx, ab, ij, t, t_kt, t_mt);
-    if (nt) write_t_tiles_tc(ch, pk_idx, ab, ij, t, nt, tkt_tc, tkt_tc_stride, tmt_tc,
-                             tmt_tc_stride);
+    if (nt) write_t_tiles_tc(ch, pk_idx[ch.pp_off + ab], ij, t, nt, tkt_tc, tkt_tc_stride,
+                             tmt_tc, tmt_tc_stride);
   }
 }
 

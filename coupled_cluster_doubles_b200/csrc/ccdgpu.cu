@@ -66,6 +66,8 @@ struct ccdgpu_handle {
   double *part = nullptr, *lpart = nullptr;
   ElemRange *ranges = nullptr;
   ElemRange *pranges = nullptr;  // fused assembly: ranges of packed elements u * hh + j
+  AsmRowStatic *asm_rows = nullptr;  // fused assembly: per packed row / per hh column tables
+  AsmColStatic *asm_cols = nullptr;
   int2 *pp_pairs = nullptr, *hh_pairs = nullptr;
   int32_t *pp_swap = nullptr, *hh_swap = nullptr;
   int64_t *list_off = nullptr;
@@ -607,6 +609,29 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
       pranges.push_back({ai, 0, (int64_t)u * hh, (int64_t)std::min(pr, u + rows) * hh});
   }
   h->n_asm_blocks = (int)pranges.size();
+  // Static assembly tables (packed rows in rowmap order, columns in hh order).
+  std::vector<AsmRowStatic> asm_rows(rowmap.size());
+  std::vector<AsmColStatic> asm_cols(hh_pairs.size());
+  for (int ai = 0; ai < h->n_act; ai++) {
+    const ChanInfo &a = chans[ai];
+    for (int u = 0; u < a.pr; u++) {
+      const int ab = rowmap[a.row_off + u], mi = mirror[a.row_off + u];
+      const int ba = mi >= 0 ? mi : ab;
+      const int2 pab = pp_pairs[a.pp_off + ab];
+      const int2 qa = pk_idx[a.pp_off + ab], qb = pk_idx[a.pp_off + ba];
+      AsmRowStatic &r = asm_rows[a.row_off + u];
+      r.o_ab = ab * a.hh; r.o_ba = ba * a.hh;
+      r.qa_x = qa.x; r.qa_y = qa.y; r.qb_x = qb.x; r.qb_y = qb.y;
+      r.pa = pab.x - (int)np; r.pb = pab.y - (int)np;
+      r.ea = P->sp_energy[pab.x]; r.eb = P->sp_energy[pab.y];
+    }
+    for (int j = 0; j < a.hh; j++) {
+      const int2 pij = hh_pairs[a.hh_off + j];
+      AsmColStatic &c = asm_cols[a.hh_off + j];
+      c.js = hh_swap[a.hh_off + j]; c.i = pij.x; c.j = pij.y; c.pad = 0;
+      c.eij = P->sp_energy[pij.x] + P->sp_energy[pij.y];
+    }
+  }
 
   // Work estimate (reference GEMM flops) for roofline reporting.
   double fl = 0, lf = 0, vb = 0, vbp = 0;
@@ -653,6 +678,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   ar.add(&h->x, x_tot); ar.add(&h->x_t, xt); ar.add(&h->t_kt, tkt); ar.add(&h->t_mt, tmt);
   ar.add(&h->s, hh_tot); ar.add(&h->r, pp_tot); ar.add(&h->xh, np); ar.add(&h->yp, h->npart);
   ar.add(&h->pranges, pranges.size());
+  ar.add(&h->asm_rows, asm_rows.size()); ar.add(&h->asm_cols, asm_cols.size());
   ar.add(&h->kcol, kcol.size());  // V tiling at create
   ar.add(&h->epart, std::max(h->n_ranges, h->n_asm_blocks)); ar.add(&h->ctl, 1); ar.add(&h->e_out, 1); ar.add(&h->err, 1);
   ar.add(&h->ticket, 1);
@@ -735,6 +761,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   };
   TRY(put(h->chans, chans)); TRY(put(h->mods, mods));
   TRY(put(h->hh_tiles, hh_tiles)); TRY(put(h->hh_red, hh_red)); TRY(put(h->ranges, ranges)); TRY(put(h->pranges, pranges));
+  TRY(put(h->asm_rows, asm_rows)); TRY(put(h->asm_cols, asm_cols));
 
   TRY(put(h->kcol, kcol));
   TRY(put(h->pp_pairs, pp_pairs)); TRY(put(h->hh_pairs, hh_pairs));
@@ -1039,10 +1066,11 @@ int launch_assemble_fused(ccdgpu_handle *h, cudaStream_t st, int gate) {
   if (!h->n_asm_blocks) return CCDGPU_OK;
   h->launches++;
   return cuda_status(launch_pdl(
-      assemble_fused_kernel, h->n_asm_blocks, kAsmThreads, 0, st, h->pranges, h->chans,
-      h->pp_pairs, h->hh_pairs, h->hh_swap, h->rowmap, h->mirror, h->pk_idx, h->v_pphh, h->dmat,
-      h->d_ring, h->flat + 4 * h->n_t, h->old_phhp, h->xh, h->yp, h->eps, (int)h->np, h->t[0],
-      h->t[1], h->t_kt, h->t_mt, h->epart,
+      assemble_fused_kernel, h->n_asm_blocks, kAsmThreads, 0, st, (const ElemRange *)h->pranges,
+      (const ChanInfo *)h->chans, (const AsmRowStatic *)h->asm_rows,
+      (const AsmColStatic *)h->asm_cols, (const double *)h->v_pphh, (const double *)h->dmat,
+      (const double *)h->d_ring, (const int32_t *)(h->flat + 4 * h->n_t), h->old_phhp,
+      (const double *)h->xh, (const double *)h->yp, h->t[0], h->t[1], h->t_kt, h->t_mt, h->epart,
       h->ticket, h->ctl, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc, gate ? h->nt : 0, gate));
 }
 int launch_energy(ccdgpu_handle *h, cudaStream_t st, int flags) {
