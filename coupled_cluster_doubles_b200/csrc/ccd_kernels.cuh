@@ -195,15 +195,16 @@ ladder_reduce_kernel(const RedItem *__restrict__ items, const LadderTile *__rest
 template <int NB>
 __device__ __forceinline__ bool consume_thin(const LadderTile &tile, const double *As,
                                              const double *Bs, int bstage, uint64_t *bars,
-                                             int tid, const LadderOut &out, int32_t *err) {
+                                             int tid, const LadderOut &out, int32_t *err,
+                                             int gc0) {
   const int lane = tid & 31;
   double acc[NB];
 #pragma unroll
   for (int j = 0; j < NB; ++j) acc[j] = 0.0;
   const int nchunks = tile.nks + tile.nkh;
   for (int c = 0; c < nchunks; ++c) {
-    const int s = c % kStages;
-    if (!mbar_wait(smem_u32(&bars[s]), (c / kStages) & 1)) {
+    const int gch = gc0 + c, s = gch % kStages;  // chunk number gch of this CTA
+    if (!mbar_wait(smem_u32(&bars[s]), (gch / kStages) & 1)) {
       atomicOr(err, kErrTimeout);
       return false;
     }
@@ -234,7 +235,8 @@ __device__ __forceinline__ bool consume_thin(const LadderTile &tile, const doubl
 template <int C>
 __device__ __forceinline__ bool consume_mma(const LadderTile &tile, const double *As,
                                             const double *Bs, int bstage, uint64_t *bars,
-                                            int tid, const LadderOut &out, int32_t *err) {
+                                            int tid, const LadderOut &out, int32_t *err,
+                                            int gc0) {
   constexpr int NB = 8 * C, BS = NB + 4;
   const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
   const int ar = ladder_arows(NB, tile.rows);
@@ -247,8 +249,8 @@ __device__ __forceinline__ bool consume_mma(const LadderTile &tile, const double
     for (int j = 0; j < C; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   const int nchunks = tile.nks + tile.nkh;
   for (int c = 0; c < nchunks; ++c) {
-    const int s = c % kStages;
-    if (!mbar_wait(smem_u32(&bars[s]), (c / kStages) & 1)) {
+    const int gch = gc0 + c, s = gch % kStages;  // chunk number gch of this CTA
+    if (!mbar_wait(smem_u32(&bars[s]), (gch / kStages) & 1)) {
       atomicOr(err, kErrTimeout);
       return false;
     }
@@ -285,86 +287,103 @@ __device__ __forceinline__ bool consume_mma(const LadderTile &tile, const double
 
 // Column classes: CLS 0 = thin (nb <= 8), 1 = mid (nb 16..32), 2 = wide (nb 40..72).  Separate
 // instantiations keep the register budget of narrow channels independent of the 72-column case.
+// Persistent CTAs: CTA b runs tiles cta_off[b] .. cta_off[b+1] (a balanced assignment made on the
+// host); the producer streams K chunks through the stage ring across tile boundaries and the
+// consumers write each tile's rows when its last chunk is done.
 template <int CLS>
 __global__ void __launch_bounds__(ladder_threads(CLS), CLS == 0 ? 3 : CLS == 1 ? 2 : 1)
-pp_ladder_kernel(const LadderTile *__restrict__ tiles, const double *__restrict__ v_t,
-                 const double *__restrict__ t_kt, const double *__restrict__ t_mt,
-                 const double *__restrict__ x_t, const int32_t *__restrict__ rowmap,
-                 const int32_t *__restrict__ mirror, double *__restrict__ d, double *part,
-                 int32_t *counters, const Control *ctl, int32_t *err, int gate) {
+pp_ladder_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restrict__ cta_off,
+                 const double *__restrict__ v_t, const double *__restrict__ t_kt,
+                 const double *__restrict__ t_mt, const double *__restrict__ x_t,
+                 const int32_t *__restrict__ rowmap, const int32_t *__restrict__ mirror,
+                 double *__restrict__ d, double *part, const Control *ctl, int32_t *err,
+                 int gate) {
   if (skip_iteration(ctl, gate, kTrLadderThin + CLS)) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double *As = reinterpret_cast<double *>(smem_raw);
   double *Bs = As + kStages * kMaxAS * kBK;
   constexpr bool WIDE = CLS > 0;
+  constexpr int kConsumerWarps = (ladder_threads(CLS) - 32) / 32;
   const int bstage = WIDE ? kBK * kMaxBS : kBK * 8;
   uint64_t *bars = reinterpret_cast<uint64_t *>(Bs + kStages * bstage);
-  const LadderTile tile = tiles[blockIdx.x];
+  const int t_begin = cta_off[blockIdx.x], t_end = cta_off[blockIdx.x + 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(smem_u32(&bars[s]), 1);
-      mbar_init(smem_u32(&bars[kStages + s]), (ladder_threads(CLS) - 32) / 32);
+      mbar_init(smem_u32(&bars[kStages + s]), kConsumerWarps);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
 
-  if (warp == (ladder_threads(CLS) - 32) / 32) {
+  if (warp == kConsumerWarps) {
     if (lane == 0) {
-      const int ar = ladder_arows(tile.nb, tile.rows);
-      const int bs = ladder_bs(tile.nb), af = ladder_arows_full(tile.nb);
-      const uint32_t abytes = ar * kBK * 8, bbytes = kBK * bs * 8;
-      const int nchunks = tile.nks + tile.nkh;
-      const int64_t vtile = tile.v_base + (int64_t)tile.mt * af * tile.nkc * kBK;
-      const int64_t ttile = tile.tmt_base + (int64_t)tile.mt * af * tile.nkh * kBK;
-      for (int c = 0; c < nchunks; ++c) {
-        const int s = c % kStages;
-        if (c >= kStages && !mbar_wait(smem_u32(&bars[kStages + s]), ((c / kStages) - 1) & 1)) {
-          atomicOr(err, kErrTimeout);
-          break;
+      int gc = 0;  // chunks issued by this CTA
+      bool stop = false;
+      for (int ti = t_begin; ti < t_end && !stop; ++ti) {
+        const LadderTile tile = tiles[ti];
+        const int ar = ladder_arows(tile.nb, tile.rows);
+        const int bs = ladder_bs(tile.nb), af = ladder_arows_full(tile.nb);
+        const uint32_t abytes = ar * kBK * 8, bbytes = kBK * bs * 8;
+        const int nchunks = tile.nks + tile.nkh;
+        const int64_t vtile = tile.v_base + (int64_t)tile.mt * af * tile.nkc * kBK;
+        const int64_t ttile = tile.tmt_base + (int64_t)tile.mt * af * tile.nkh * kBK;
+        for (int c = 0; c < nchunks; ++c, ++gc) {
+          const int s = gc % kStages;
+          if (gc >= kStages &&
+              !mbar_wait(smem_u32(&bars[kStages + s]), ((gc / kStages) - 1) & 1)) {
+            atomicOr(err, kErrTimeout);
+            stop = true;
+            break;
+          }
+          const double *asrc, *bsrc;
+          if (c < tile.nks) {
+            const int kc = tile.kc0 + c;
+            asrc = v_t + vtile + (int64_t)kc * ar * kBK;
+            bsrc = t_kt + tile.tkt_base + (int64_t)kc * kBK * bs;
+          } else {
+            const int kh = c - tile.nks;
+            asrc = t_mt + ttile + (int64_t)kh * ar * kBK;
+            bsrc = x_t + tile.xt_base + (int64_t)kh * kBK * bs;
+          }
+          const uint32_t full = smem_u32(&bars[s]);
+          mbar_expect_tx(full, abytes + bbytes);
+          bulk_g2s(smem_u32(As + s * kMaxAS * kBK), asrc, abytes, full);
+          bulk_g2s(smem_u32(Bs + s * bstage), bsrc, bbytes, full);
         }
-        const double *asrc, *bsrc;
-        if (c < tile.nks) {
-          const int kc = tile.kc0 + c;
-          asrc = v_t + vtile + (int64_t)kc * ar * kBK;
-          bsrc = t_kt + tile.tkt_base + (int64_t)kc * kBK * bs;
-        } else {
-          const int kh = c - tile.nks;
-          asrc = t_mt + ttile + (int64_t)kh * ar * kBK;
-          bsrc = x_t + tile.xt_base + (int64_t)kh * kBK * bs;
-        }
-        const uint32_t full = smem_u32(&bars[s]);
-        mbar_expect_tx(full, abytes + bbytes);
-        bulk_g2s(smem_u32(As + s * kMaxAS * kBK), asrc, abytes, full);
-        bulk_g2s(smem_u32(Bs + s * bstage), bsrc, bbytes, full);
       }
     }
     return;
   }
   const int tid = threadIdx.x;
-  const LadderOut out{tile, rowmap, mirror, d, part};
-  bool ok = true;
-  if (!WIDE) {
-    switch (tile.nb) {
-      case 2: ok = consume_thin<2>(tile, As, Bs, bstage, bars, tid, out, err); break;
-      case 4: ok = consume_thin<4>(tile, As, Bs, bstage, bars, tid, out, err); break;
-      default: ok = consume_thin<8>(tile, As, Bs, bstage, bars, tid, out, err); break;
-    }
-  } else {
-#define CCD_WIDE8_CASE(n) \
-  case n: ok = consume_mma<n>(tile, As, Bs, bstage, bars, tid, out, err); break;
-    if (CLS == 1) {
-      switch (tile.nb / 8) { CCD_WIDE8_CASE(2) CCD_WIDE8_CASE(3) CCD_WIDE8_CASE(4) default: break; }
-    } else {
-      switch (tile.nb / 8) {
-        CCD_WIDE8_CASE(5) CCD_WIDE8_CASE(6) CCD_WIDE8_CASE(7) CCD_WIDE8_CASE(8) CCD_WIDE8_CASE(9)
-        default: break;
+  int gc = 0;
+  for (int ti = t_begin; ti < t_end; ++ti) {
+    const LadderTile tile = tiles[ti];
+    const LadderOut out{tile, rowmap, mirror, d, part};
+    bool ok = true;
+    if (!WIDE) {
+      switch (tile.nb) {
+        case 2: ok = consume_thin<2>(tile, As, Bs, bstage, bars, tid, out, err, gc); break;
+        case 4: ok = consume_thin<4>(tile, As, Bs, bstage, bars, tid, out, err, gc); break;
+        default: ok = consume_thin<8>(tile, As, Bs, bstage, bars, tid, out, err, gc); break;
       }
-    }
+    } else {
+#define CCD_WIDE8_CASE(n) \
+  case n: ok = consume_mma<n>(tile, As, Bs, bstage, bars, tid, out, err, gc); break;
+      if (CLS == 1) {
+        switch (tile.nb / 8) { CCD_WIDE8_CASE(2) CCD_WIDE8_CASE(3) CCD_WIDE8_CASE(4) default: break; }
+      } else {
+        switch (tile.nb / 8) {
+          CCD_WIDE8_CASE(5) CCD_WIDE8_CASE(6) CCD_WIDE8_CASE(7) CCD_WIDE8_CASE(8) CCD_WIDE8_CASE(9)
+          default: break;
+        }
+      }
 #undef CCD_WIDE8_CASE
+    }
+    if (!ok) break;  // a timed-out tile leaves its row block unfinished (error already set)
+    gc += tile.nks + tile.nkh;
   }
-  (void)ok;  // a timed-out tile leaves its row block unfinished (error already set)
 }
 
 // ------------------------------------------------------------------------------------------

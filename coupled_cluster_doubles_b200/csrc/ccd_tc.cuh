@@ -41,7 +41,8 @@ __host__ __device__ constexpr int tc_stages(int nt) { return nt == 2 ? 4 : 3; }
 __host__ __device__ constexpr size_t tc_stage_bytes(int nt) {
   return (size_t)nt * (kTcAPlane + kTcBPlane) * 2;
 }
-// Dynamic shared memory: 1024 bytes of alignment slack, the stages, then the barriers.
+// Dynamic shared memory: 1024 bytes of alignment slack, the stages, then the barriers
+// (2 S + 5 of them).
 __host__ __device__ constexpr size_t tc_smem_bytes(int nt) {
   return 1024 + tc_stages(nt) * tc_stage_bytes(nt) + 256;
 }
@@ -117,17 +118,26 @@ __device__ __forceinline__ void tc_drain(const uint64_t *full, int issued, int s
     (void)mbar_wait(smem_u32(&full[c % stages]), (c / stages) & 1);
 }
 
-// One CTA = one LadderTile (bm = 128, nb = UMMA N, K chunks of kTcKC).  Image arrays hold NT
-// planes each, plane p at base + p * stride.  A mixed-phase kernel (gate 1 of skip_iteration).
+// Persistent CTAs: CTA b runs tiles cta_off[b] .. cta_off[b+1] (a balanced assignment made on
+// the host).  The producer streams K chunks through the S-stage ring without a break at tile
+// boundaries; the MMA thread accumulates tile number lt of the CTA into tensor-memory buffer
+// lt & 1 (two 128-column accumulators), so that the epilogue warps read tile lt back while
+// tile lt + 1 is loaded and multiplied.  Barriers: full / empty per stage, acc_full / acc_empty
+// per accumulator (tcgen05.commit, and one arrival per epilogue warp).  Every wait is bounded
+// and checks the CTA's abort flag.  Tiles are bm = 128 rows, nb = UMMA N columns, K chunks of
+// kTcKC; image arrays hold NT planes each, plane p at base + p * stride.  A mixed-phase kernel
+// (gate 1 of skip_iteration).
+constexpr uint32_t kTcAccCols = 128;  // columns of one accumulator buffer (nb <= kTcMaxNB)
+constexpr int kTcGrid = 2 * 148;      // persistent grid: two CTAs on each of the 148 SMs
 template <int NT>
 __global__ void __launch_bounds__(kTcThreads, 1)
-pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const __nv_bfloat16 *__restrict__ v_tc,
-                    int64_t v_stride, const __nv_bfloat16 *__restrict__ tkt_tc, int64_t tkt_stride,
+pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restrict__ cta_off,
+                    const __nv_bfloat16 *__restrict__ v_tc, int64_t v_stride,
+                    const __nv_bfloat16 *__restrict__ tkt_tc, int64_t tkt_stride,
                     const __nv_bfloat16 *__restrict__ tmt_tc, int64_t tmt_stride,
                     const __nv_bfloat16 *__restrict__ xt_tc, int64_t xt_stride,
                     const int32_t *__restrict__ rowmap, const int32_t *__restrict__ mirror,
-                    double *__restrict__ d, double *part, int32_t *counters, const Control *ctl,
-                    int32_t *err) {
+                    double *__restrict__ d, double *part, const Control *ctl, int32_t *err) {
   if (skip_iteration(ctl, 1, kTrLadderTC)) return;
   constexpr int S = tc_stages(NT);
   constexpr uint32_t kStageBytes = (uint32_t)tc_stage_bytes(NT);
@@ -137,14 +147,17 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const __nv_bfloat16 *_
   const uint32_t raw = smem_u32(tc_smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;  // stage s at base + s * kStageBytes
   uint64_t *bars = reinterpret_cast<uint64_t *>(tc_smem_raw + (base - raw) + S * kStageBytes);
-  uint64_t *full = bars, *empty = bars + S, *done = bars + 2 * S;
-  const LadderTile tile = tiles[blockIdx.x];
+  uint64_t *full = bars, *empty = bars + S, *acc_full = bars + 2 * S,
+           *acc_empty = bars + 2 * S + 2, *done = bars + 2 * S + 4;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t ncols = tc_tmem_cols(tile.nb);
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(smem_u32(&full[s]), 1);
       mbar_init(smem_u32(&empty[s]), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&acc_full[b]), 1);
+      mbar_init(smem_u32(&acc_empty[b]), kLadderConsumers / 32);
     }
     mbar_init(smem_u32(done), 1);
     abort_flag = 0;
@@ -153,103 +166,137 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const __nv_bfloat16 *_
   }
   if (warp == 5) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                 ::"r"(smem_u32(&tmem_holder)), "r"(ncols) : "memory");
+                 ::"r"(smem_u32(&tmem_holder)), "r"(2 * kTcAccCols) : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_holder;
-  const int nchunks = tile.nks + tile.nkh;
-  const int rg = (tile.rows + 7) >> 3;   // stored row groups of this row tile's A chunks
-  const int ng = tile.nb >> 3;           // row groups of a B chunk
-  const uint32_t abytes = (uint32_t)rg * kTcGroup * 2, bbytes = (uint32_t)ng * kTcGroup * 2;
+  const int t_begin = cta_off[blockIdx.x], t_end = cta_off[blockIdx.x + 1];
+  auto fail = [&]() {
+    atomicOr(err, kErrTimeout);
+    atomicExch(&abort_flag, 1);
+  };
 
   if (warp == 4) {
     // ---- producer ----
     if (lane == 0) {
-      const int64_t vtile = tile.v_base + (int64_t)tile.mt * kTcBM * tile.nkc * kTcKC;
-      const int64_t ttile = tile.tmt_base + (int64_t)tile.mt * kTcBM * tile.nkh * kTcKC;
-      int issued = 0;
-      for (int c = 0; c < nchunks; ++c) {
-        const int s = c % S;
-        if (c >= S && !mbar_wait(smem_u32(&empty[s]), ((c / S) - 1) & 1)) {
-          atomicOr(err, kErrTimeout);
-          atomicExch(&abort_flag, 1);
-          break;
-        }
-        const __nv_bfloat16 *asrc, *bsrc;
-        int64_t as, bs;
-        if (c < tile.nks) {
-          const int kc = tile.kc0 + c;
-          asrc = v_tc + vtile + (int64_t)kc * rg * kTcGroup;
-          bsrc = tkt_tc + tile.tkt_base + (int64_t)kc * ng * kTcGroup;
-          as = v_stride;
-          bs = tkt_stride;
-        } else {
-          const int kh = c - tile.nks;
-          asrc = tmt_tc + ttile + (int64_t)kh * rg * kTcGroup;
-          bsrc = xt_tc + tile.xt_base + (int64_t)kh * ng * kTcGroup;
-          as = tmt_stride;
-          bs = xt_stride;
-        }
-        const uint32_t fb = smem_u32(&full[s]);
-        const uint32_t sa = base + s * kStageBytes, sb = sa + NT * kTcAPlane * 2;
-        mbar_expect_tx(fb, NT * (abytes + bbytes));
+      int gc = 0;  // chunks issued by this CTA (all its tiles)
+      bool stop = false;
+      for (int ti = t_begin; ti < t_end && !stop; ++ti) {
+        const LadderTile tile = tiles[ti];
+        const int nchunks = tile.nks + tile.nkh;
+        const int rg = (tile.rows + 7) >> 3;  // stored row groups of the A chunks
+        const int ng = tile.nb >> 3;          // row groups of a B chunk
+        const uint32_t abytes = (uint32_t)rg * kTcGroup * 2, bbytes = (uint32_t)ng * kTcGroup * 2;
+        const int64_t vtile = tile.v_base + (int64_t)tile.mt * kTcBM * tile.nkc * kTcKC;
+        const int64_t ttile = tile.tmt_base + (int64_t)tile.mt * kTcBM * tile.nkh * kTcKC;
+        for (int c = 0; c < nchunks; ++c, ++gc) {
+          const int s = gc % S;
+          if (read_flag(&abort_flag) ||
+              (gc >= S && !mbar_wait(smem_u32(&empty[s]), ((gc / S) - 1) & 1))) {
+            fail();
+            stop = true;
+            break;
+          }
+          const __nv_bfloat16 *asrc, *bsrc;
+          int64_t as, bs;
+          if (c < tile.nks) {
+            const int kc = tile.kc0 + c;
+            asrc = v_tc + vtile + (int64_t)kc * rg * kTcGroup;
+            bsrc = tkt_tc + tile.tkt_base + (int64_t)kc * ng * kTcGroup;
+            as = v_stride;
+            bs = tkt_stride;
+          } else {
+            const int kh = c - tile.nks;
+            asrc = tmt_tc + ttile + (int64_t)kh * rg * kTcGroup;
+            bsrc = xt_tc + tile.xt_base + (int64_t)kh * ng * kTcGroup;
+            as = tmt_stride;
+            bs = xt_stride;
+          }
+          const uint32_t fb = smem_u32(&full[s]);
+          const uint32_t sa = base + s * kStageBytes, sb = sa + NT * kTcAPlane * 2;
+          mbar_expect_tx(fb, NT * (abytes + bbytes));
 #pragma unroll
-        for (int p = 0; p < NT; ++p) {
-          bulk_g2s(sa + p * kTcAPlane * 2, asrc + p * as, abytes, fb);
-          bulk_g2s(sb + p * kTcBPlane * 2, bsrc + p * bs, bbytes, fb);
+          for (int p = 0; p < NT; ++p) {
+            bulk_g2s(sa + p * kTcAPlane * 2, asrc + p * as, abytes, fb);
+            bulk_g2s(sb + p * kTcBPlane * 2, bsrc + p * bs, bbytes, fb);
+          }
         }
-        ++issued;
       }
-      issued_chunks = issued;
+      issued_chunks = gc;
     }
   } else if (warp == 5) {
     // ---- MMA issuer ----
     if (lane == 0) {
-      const uint32_t idesc = tc_idesc(tile.nb);
-      for (int c = 0; c < nchunks; ++c) {
-        const int s = c % S;
-        if (read_flag(&abort_flag) || !mbar_wait(smem_u32(&full[s]), (c / S) & 1)) {
-          atomicOr(err, kErrTimeout);
-          atomicExch(&abort_flag, 1);
+      int gc = 0, lt = 0;
+      for (int ti = t_begin; ti < t_end; ++ti, ++lt) {
+        const LadderTile tile = tiles[ti];
+        const int buf = lt & 1, use = lt >> 1;
+        if (read_flag(&abort_flag) ||
+            (use > 0 && !mbar_wait(smem_u32(&acc_empty[buf]), (use - 1) & 1))) {
+          fail();
           break;
         }
         tc_fence_after();
-        const uint32_t sa = base + s * kStageBytes, sb = sa + NT * kTcAPlane * 2;
+        const uint32_t acc = tmem + buf * kTcAccCols;
+        const uint32_t idesc = tc_idesc(tile.nb);
+        const int nchunks = tile.nks + tile.nkh;
+        bool ok = true;
+        for (int c = 0; c < nchunks; ++c, ++gc) {
+          const int s = gc % S;
+          if (read_flag(&abort_flag) || !mbar_wait(smem_u32(&full[s]), (gc / S) & 1)) {
+            fail();
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sa = base + s * kStageBytes, sb = sa + NT * kTcAPlane * 2;
 #pragma unroll
-        for (int j = 0; j < kTcKC / 16; ++j) {
+          for (int j = 0; j < kTcKC / 16; ++j) {
 #pragma unroll
-          for (int pa = 0; pa < NT; ++pa)
+            for (int pa = 0; pa < NT; ++pa)
 #pragma unroll
-            for (int pb = 0; pb < NT - pa; ++pb)
-              tc_mma(tmem, tc_desc(sa + pa * kTcAPlane * 2 + j * 256),
-                     tc_desc(sb + pb * kTcBPlane * 2 + j * 256), idesc,
-                     (c | j | pa | pb) != 0 ? 1u : 0u);
+              for (int pb = 0; pb < NT - pa; ++pb)
+                tc_mma(acc, tc_desc(sa + pa * kTcAPlane * 2 + j * 256),
+                       tc_desc(sb + pb * kTcBPlane * 2 + j * 256), idesc,
+                       (c | j | pa | pb) != 0 ? 1u : 0u);
+          }
+          tc_commit(smem_u32(&empty[s]));
         }
-        tc_commit(smem_u32(&empty[s]));
+        tc_commit(smem_u32(&acc_full[buf]));  // also after an abort: the epilogue's wait ends
+        if (!ok) break;
       }
-      tc_commit(smem_u32(done));  // also after an abort: the epilogue waits for issued MMAs
+      tc_commit(smem_u32(done));
     }
   } else {
     // ---- epilogue: accumulator rows -> D (or split-K partials) ----
-    const bool ok = mbar_wait(smem_u32(done), 0);
-    tc_fence_after();
     const int tid = threadIdx.x;
-    const LadderOut out{tile, rowmap, mirror, d, part};
-    if (!ok) atomicOr(err, kErrTimeout);
-    // One decision for all four warps (tcgen05.ld is warp-collective).
-    if (consumers_all(ok && !read_flag(&abort_flag) && nchunks > 0)) {
-      const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
-      for (int c0 = 0; c0 < tile.nb; c0 += 16) {
-        float v[16];
-        tc_ld16(lane_addr + c0, v);
-        double dv[16];
+    int lt = 0;
+    for (int ti = t_begin; ti < t_end; ++ti, ++lt) {
+      const LadderTile tile = tiles[ti];
+      const int buf = lt & 1, use = lt >> 1;
+      const bool ok = mbar_wait(smem_u32(&acc_full[buf]), use & 1);
+      tc_fence_after();
+      if (!ok) fail();
+      // One decision for all four warps (tcgen05.ld is warp-collective).
+      if (!consumers_all(ok && !read_flag(&abort_flag))) break;
+      if (tile.nks + tile.nkh > 0) {
+        const LadderOut out{tile, rowmap, mirror, d, part};
+        const uint32_t lane_addr = tmem + buf * kTcAccCols + ((uint32_t)(warp * 32) << 16);
+        for (int c0 = 0; c0 < tile.nb; c0 += 16) {
+          float v[16];
+          tc_ld16(lane_addr + c0, v);
+          double dv[16];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) dv[i] = (double)v[i];
-        out.row(tid, c0, dv, 16);
+          for (int i = 0; i < 16; ++i) dv[i] = (double)v[i];
+          out.row(tid, c0, dv, 16);
+        }
       }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&acc_empty[buf]));
     }
   }
   tc_fence_before();
@@ -262,8 +309,8 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const __nv_bfloat16 *_
     // path); only then is the accumulator released.
     (void)mbar_wait(smem_u32(done), 0);
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols)
-                 : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                 ::"r"(tmem), "r"(2 * kTcAccCols) : "memory");
   }
 }
 

@@ -13,6 +13,7 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <queue>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -61,7 +62,7 @@ struct ccdgpu_handle {
   LadderTile *tiles = nullptr;
   HHTile *hh_tiles = nullptr;
   HHRed *hh_red = nullptr;
-  int32_t *rowmap = nullptr, *mirror = nullptr, *lcounters = nullptr;
+  int32_t *rowmap = nullptr, *mirror = nullptr;
   int2 *pk_idx = nullptr;
   double *part = nullptr, *lpart = nullptr;
   ElemRange *ranges = nullptr;
@@ -107,6 +108,10 @@ struct ccdgpu_handle {
   ccdgpu_schedule schedule{};
   void *tile_mem = nullptr;
   RedItem *red_fp = nullptr, *red_tc = nullptr;  // split-K reduction items
+  int32_t *tc_cta_off = nullptr;  // tensor-core ladder: tile range of each persistent CTA
+  int tc_grid = 0;
+  int32_t *fp_cta_off = nullptr;  // FP64 ladder classes: tile ranges of their persistent CTAs
+  int fp_grid[3] = {0, 0, 0}, fp_off_base[3] = {0, 0, 0};
   int n_red_fp = 0, n_red_tc = 0, n_red_cls[3] = {0, 0, 0};
 
   // Mixed precision (nt bf16 terms per operand; 0 for an FP64 handle).
@@ -114,7 +119,6 @@ struct ccdgpu_handle {
   int n_tc_tiles = 0;
   LadderTile *tc_tiles = nullptr;
   int32_t *kcol = nullptr;  // pp index of the w-th c<d pair of each channel (pk_off + w)
-  int32_t *tc_counters = nullptr;
   double *tc_part = nullptr;
   __nv_bfloat16 *v_tc = nullptr, *tkt_tc = nullptr, *tmt_tc = nullptr, *xt_tc = nullptr;
   int64_t n_vtc = 0, n_tkttc = 0, n_tmttc = 0, n_xttc = 0;  // plane strides (elements)
@@ -244,6 +248,32 @@ int upload_runs(ccdgpu_handle *h, T *dst, const std::vector<const T *> &src,
 //   tc_split_mul tiles per SM.
 // Split row blocks are reduced after the ladder by ladder_reduce_kernel (segment order, so
 // deterministic), one item per (row block, 16-row chunk), FP64 items grouped by class.
+// Longest-processing-time assignment of tiles[lo, hi) to G persistent CTAs: sorted by cost,
+// largest first, each tile goes to the CTA with the least work so far; the range is rewritten
+// grouped by CTA and the CTAs' ranges are appended to `off` (absolute indices, G + 1 entries).
+template <class Cost>
+void lpt_group(std::vector<LadderTile> &tiles, size_t lo, size_t hi, int G, Cost cost,
+               std::vector<int32_t> &off) {
+  std::stable_sort(tiles.begin() + lo, tiles.begin() + hi,
+                   [&](const LadderTile &x, const LadderTile &y) { return cost(x) > cost(y); });
+  std::vector<std::vector<LadderTile>> per(G);
+  std::priority_queue<std::pair<int64_t, int>, std::vector<std::pair<int64_t, int>>,
+                      std::greater<std::pair<int64_t, int>>> load;
+  for (int b = 0; b < G; b++) load.push({0, b});
+  for (size_t i = lo; i < hi; i++) {
+    auto [w, b] = load.top();
+    load.pop();
+    per[b].push_back(tiles[i]);
+    load.push({w + cost(tiles[i]), b});
+  }
+  size_t pos = lo;
+  off.push_back((int32_t)pos);
+  for (int b = 0; b < G; b++) {
+    for (const LadderTile &t : per[b]) tiles[pos++] = t;
+    off.push_back((int32_t)pos);
+  }
+}
+
 int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
   const std::vector<ChanInfo> &chans = h->host_chans;
   auto cls_of = [](int nb) { return nb <= 8 ? 0 : nb <= 32 ? 1 : 2; };
@@ -286,14 +316,30 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
       groups++;
     }
   }
-  // Thin channels first, then wide ones; within each class the longest K streams first so
-  // the hardware block scheduler fills in the short ones.
+  // Thin channels first, then mid and wide ones; each class runs on persistent CTAs (3, 2 and
+  // 1 per SM) with a balanced (LPT) assignment.  Cost = bytes per 16-deep chunk x chunks, plus
+  // two chunks' worth for the pipeline fill and the epilogue.
   std::stable_sort(tiles.begin(), tiles.end(), [&](const LadderTile &x, const LadderTile &y) {
-    const int cx = cls_of(x.nb), cy = cls_of(y.nb);
-    if (cx != cy) return cx < cy;
-    return (int64_t)(x.nks + x.nkh) * (x.rows + x.nb) > (int64_t)(y.nks + y.nkh) * (y.rows + y.nb);
+    return cls_of(x.nb) < cls_of(y.nb);
   });
+  std::vector<int32_t> fp_cta_off;
+  {
+    auto fp_cost = [](const LadderTile &x) {
+      return (int64_t)(x.nks + x.nkh + 2) * (ladder_arows(x.nb, x.rows) + ladder_bs(x.nb));
+    };
+    size_t lo = 0;
+    const int slots[3] = {3 * 148, 2 * 148, 148};
+    for (int k = 0; k < 3; k++) {
+      size_t hi = lo;
+      while (hi < tiles.size() && cls_of(tiles[hi].nb) == k) hi++;
+      h->fp_off_base[k] = (int)fp_cta_off.size();
+      h->fp_grid[k] = (int)std::min<size_t>(hi - lo, slots[k]);
+      if (hi > lo) lpt_group(tiles, lo, hi, h->fp_grid[k], fp_cost, fp_cta_off);
+      lo = hi;
+    }
+  }
   std::vector<LadderTile> tc_tiles;
+  std::vector<int32_t> tc_cta_off;
   int64_t tcpart_tot = 0;
   int32_t tc_groups = 0;
   if (h->nt) {
@@ -325,10 +371,15 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
         tc_groups++;
       }
     }
-    // Largest byte streams first.
-    std::stable_sort(tc_tiles.begin(), tc_tiles.end(), [](const LadderTile &x, const LadderTile &y) {
-      return (int64_t)(x.nks + x.nkh) * (x.rows + x.nb) > (int64_t)(y.nks + y.nkh) * (y.rows + y.nb);
-    });
+    // Persistent CTAs (CTA b runs entries tc_cta_off[b] .. tc_cta_off[b+1]), LPT-balanced.
+    // Cost = bytes streamed per 32-deep chunk x chunks, plus two chunks' worth for the pipeline
+    // fill and the epilogue.
+    auto tc_cost = [](const LadderTile &x) {
+      return (int64_t)(x.nks + x.nkh + 2) * (((x.rows + 7) & ~7) + x.nb);
+    };
+    if (!tc_tiles.empty())
+      lpt_group(tc_tiles, 0, tc_tiles.size(), (int)std::min<size_t>(tc_tiles.size(), kTcGrid),
+                tc_cost, tc_cta_off);
   }
   // Reduction items of split row blocks.
   auto red_items = [](const std::vector<LadderTile> &tl, std::vector<RedItem> &out, int *per_cls,
@@ -357,8 +408,9 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
   if (h->tile_mem) CK(cudaFree(h->tile_mem));
   h->tile_mem = nullptr;
   Arena ar;
-  ar.add(&h->tiles, tiles.size()); ar.add(&h->lcounters, groups); ar.add(&h->lpart, lpart_tot);
-  ar.add(&h->tc_tiles, tc_tiles.size()); ar.add(&h->tc_counters, tc_groups);
+  ar.add(&h->tiles, tiles.size()); ar.add(&h->lpart, lpart_tot);
+  ar.add(&h->tc_tiles, tc_tiles.size());
+  ar.add(&h->fp_cta_off, fp_cta_off.size()); ar.add(&h->tc_cta_off, tc_cta_off.size());
   ar.add(&h->tc_part, tcpart_tot);
   ar.add(&h->red_fp, red_fp.size()); ar.add(&h->red_tc, red_tc.size());
   CK(cudaMalloc(&h->tile_mem, ar.used));
@@ -370,6 +422,13 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
   if (!tc_tiles.empty())
     CK(cudaMemcpyAsync(h->tc_tiles, tc_tiles.data(), tc_tiles.size() * sizeof(LadderTile),
                        cudaMemcpyHostToDevice, h->s0));
+  if (!fp_cta_off.empty())
+    CK(cudaMemcpyAsync(h->fp_cta_off, fp_cta_off.data(), fp_cta_off.size() * sizeof(int32_t),
+                       cudaMemcpyHostToDevice, h->s0));
+  if (!tc_cta_off.empty())
+    CK(cudaMemcpyAsync(h->tc_cta_off, tc_cta_off.data(), tc_cta_off.size() * sizeof(int32_t),
+                       cudaMemcpyHostToDevice, h->s0));
+  h->tc_grid = tc_cta_off.empty() ? 0 : (int)tc_cta_off.size() - 1;
   if (!red_fp.empty())
     CK(cudaMemcpyAsync(h->red_fp, red_fp.data(), red_fp.size() * sizeof(RedItem),
                        cudaMemcpyHostToDevice, h->s0));
@@ -956,16 +1015,17 @@ int launch_hh_ladder(ccdgpu_handle *h, cudaStream_t st, int gate, int only = -1)
 int launch_pp_ladder_tc(ccdgpu_handle *h, cudaStream_t st) {
   if (!h->n_tc_tiles) return CCDGPU_OK;
   h->launches++;
+  // Persistent: two CTAs per SM (shared memory and 2 x 128 tensor-memory columns each).
   if (h->nt == 2)
-    CK(launch_pdl(pp_ladder_tc_kernel<2>, h->n_tc_tiles, kTcThreads, h->tc_smem, st,
-                  h->tc_tiles, h->v_tc, h->n_vtc, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc,
-                  h->xt_tc, h->n_xttc, h->rowmap, h->mirror, h->dmat, h->tc_part,
-                  h->tc_counters, h->ctl, h->err));
+    CK(launch_pdl(pp_ladder_tc_kernel<2>, h->tc_grid, kTcThreads, h->tc_smem, st,
+                  (const LadderTile *)h->tc_tiles, (const int32_t *)h->tc_cta_off, h->v_tc,
+                  h->n_vtc, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc, h->xt_tc, h->n_xttc,
+                  h->rowmap, h->mirror, h->dmat, h->tc_part, h->ctl, h->err));
   else
-    CK(launch_pdl(pp_ladder_tc_kernel<3>, h->n_tc_tiles, kTcThreads, h->tc_smem, st,
-                  h->tc_tiles, h->v_tc, h->n_vtc, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc,
-                  h->xt_tc, h->n_xttc, h->rowmap, h->mirror, h->dmat, h->tc_part,
-                  h->tc_counters, h->ctl, h->err));
+    CK(launch_pdl(pp_ladder_tc_kernel<3>, h->tc_grid, kTcThreads, h->tc_smem, st,
+                  (const LadderTile *)h->tc_tiles, (const int32_t *)h->tc_cta_off, h->v_tc,
+                  h->n_vtc, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc, h->xt_tc, h->n_xttc,
+                  h->rowmap, h->mirror, h->dmat, h->tc_part, h->ctl, h->err));
   if (h->n_red_tc) {
     CK(launch_pdl(ladder_reduce_kernel, h->n_red_tc, 256, 0, st, (const RedItem *)h->red_tc,
                   (const LadderTile *)h->tc_tiles, (const int32_t *)h->rowmap,
@@ -986,32 +1046,32 @@ int launch_pp_ladder(ccdgpu_handle *h, cudaStream_t st) {
     CK(launch_pdl(retile_done_kernel, 1, 32, 0, st, h->ctl));
     h->launches += 2;
   }
-  const LadderTile *t_thin = h->tiles, *t_mid = h->tiles + h->n_cls[0];
-  const LadderTile *t_wide = t_mid + h->n_cls[1];
   const bool side = h->n_cls[1] || h->n_cls[2];
   if (side) {
     CK(cudaEventRecord(h->ev_fork2, st));
     CK(cudaStreamWaitEvent(h->s2, h->ev_fork2, 0));
     if (h->n_cls[2]) {
-      pp_ladder_kernel<2><<<h->n_cls[2], ladder_threads(2), h->ladder_smem, h->s2>>>(
-          t_wide, h->v_t, h->t_kt, h->t_mt, h->x_t, h->rowmap, h->mirror, h->dmat, h->lpart,
-          h->lcounters, h->ctl, h->err, 0);
+      pp_ladder_kernel<2><<<h->fp_grid[2], ladder_threads(2), h->ladder_smem, h->s2>>>(
+          h->tiles, h->fp_cta_off + h->fp_off_base[2], h->v_t, h->t_kt, h->t_mt, h->x_t,
+          h->rowmap, h->mirror, h->dmat, h->lpart, h->ctl, h->err, 0);
       h->launches++;
       CK(cudaGetLastError());
     }
     if (h->n_cls[1]) {
-      pp_ladder_kernel<1><<<h->n_cls[1], ladder_threads(1), h->ladder_smem, h->s2>>>(
-          t_mid, h->v_t, h->t_kt, h->t_mt, h->x_t, h->rowmap, h->mirror, h->dmat, h->lpart,
-          h->lcounters, h->ctl, h->err, 0);
+      pp_ladder_kernel<1><<<h->fp_grid[1], ladder_threads(1), h->ladder_smem, h->s2>>>(
+          h->tiles, h->fp_cta_off + h->fp_off_base[1], h->v_t, h->t_kt, h->t_mt, h->x_t,
+          h->rowmap, h->mirror, h->dmat, h->lpart, h->ctl, h->err, 0);
       h->launches++;
       CK(cudaGetLastError());
     }
     CK(cudaEventRecord(h->ev_join2, h->s2));
   }
   if (h->n_cls[0]) {
-    CK(launch_pdl(pp_ladder_kernel<0>, h->n_cls[0], kLadderThreads, h->ladder_smem_thin, st,
-                  t_thin, h->v_t, h->t_kt, h->t_mt, h->x_t, h->rowmap, h->mirror, h->dmat,
-                  h->lpart, h->lcounters, h->ctl, h->err, 0));
+    CK(launch_pdl(pp_ladder_kernel<0>, h->fp_grid[0], kLadderThreads, h->ladder_smem_thin, st,
+                  (const LadderTile *)h->tiles, (const int32_t *)(h->fp_cta_off + h->fp_off_base[0]),
+                  (const double *)h->v_t, (const double *)h->t_kt, (const double *)h->t_mt,
+                  (const double *)h->x_t, (const int32_t *)h->rowmap, (const int32_t *)h->mirror,
+                  h->dmat, h->lpart, (const Control *)h->ctl, h->err, 0));
     h->launches++;
   }
   if (side) CK(cudaStreamWaitEvent(st, h->ev_join2, 0));
@@ -1773,7 +1833,6 @@ int ccdgpu_ladder_profile(ccdgpu_handle *h, int32_t reps, double *ms, double *fl
       bytes[3] += 2.0 * h->nt * b + 8.0 * a.pp * a.hh;
     }
   }
-  const LadderTile *start[3] = {h->tiles, h->tiles + h->n_cls[0], h->tiles + h->n_cls[0] + h->n_cls[1]};
   for (int k = 0; k < 4; k++) {
     if (k < 3 && !h->n_cls[k]) continue;
     if (k == 3 && !h->n_tc_tiles) continue;
@@ -1781,9 +1840,9 @@ int ccdgpu_ladder_profile(ccdgpu_handle *h, int32_t reps, double *ms, double *fl
       if (k == 3) return launch_pp_ladder_tc(h, h->s0);
       const size_t smem = k == 0 ? h->ladder_smem_thin : h->ladder_smem;
       auto kern = k == 0 ? pp_ladder_kernel<0> : k == 1 ? pp_ladder_kernel<1> : pp_ladder_kernel<2>;
-      kern<<<h->n_cls[k], ladder_threads(k), smem, h->s0>>>(start[k], h->v_t, h->t_kt, h->t_mt, h->x_t,
-                                                        h->rowmap, h->mirror, h->dmat, h->lpart,
-                                                        h->lcounters, h->ctl, h->err, 0);
+      kern<<<h->fp_grid[k], ladder_threads(k), smem, h->s0>>>(
+          h->tiles, h->fp_cta_off + h->fp_off_base[k], h->v_t, h->t_kt, h->t_mt, h->x_t,
+          h->rowmap, h->mirror, h->dmat, h->lpart, h->ctl, h->err, 0);
       CK(cudaGetLastError());
       if (h->n_red_cls[k]) {
         const int off = k == 0 ? 0 : k == 1 ? h->n_red_cls[0] : h->n_red_cls[0] + h->n_red_cls[1];
