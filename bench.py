@@ -55,6 +55,14 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the headline
+# kernel, from the ncu captures summarised in profiles/ (workload, kernel): bytes, source.
+NCU_TRAFFIC = {
+    ("eg14", "pp_ladder_tc_kernel<2>"): (16.13e6, "profiles/pp_ladder_tc_eg14_mixed_traffic.md"),
+    ("eg54c36", "pp_ladder_tc_kernel<2>"): (360.76e6, "profiles/pp_ladder_tc_eg54c36_mixed.md"),
+}
+
+
 def measured_peaks():
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -422,7 +430,11 @@ def main():
             "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved,
                          "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "peak_source": peak_kind,
-                         "traffic": None, "algorithmic_bytes_per_launch": ladder_bytes,
+                         "traffic": NCU_TRAFFIC.get((args.config, kname), (None, None))[0]
+                         if args.v_mode == "stored" else None,
+                         "traffic_source": NCU_TRAFFIC.get((args.config, kname), (None, None))[1]
+                         if args.v_mode == "stored" else None,
+                         "algorithmic_bytes_per_launch": ladder_bytes,
                          "avg_launch_ms": ladder_ms},
             "gpu_launches": int(t["launches"]),
             "clocks": clocks.summary(),
