@@ -939,10 +939,14 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
                           (int)h->ladder_smem));
   CK(cudaFuncSetAttribute(pp_ladder_kernel<2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   h->hh_smem = 0;  // static shared memory only
-  CK(cudaFuncSetAttribute(ring_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)std::max<size_t>(h->ring_smem_mid, 16)));
-  CK(cudaFuncSetAttribute(ring_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)std::max<size_t>(h->ring_smem, 16)));
+  // The attribute belongs to the kernel, not to this handle: set the device's opt-in maximum
+  // (the same value for every handle), so that handles of different channel sizes coexist.
+  int smem_optin = 0;
+  CK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->opt.device));
+  if (h->ring_smem_mid > (size_t)smem_optin || h->ring_smem > (size_t)smem_optin)
+    return CCDGPU_ERR_UNSUPPORTED;
+  CK(cudaFuncSetAttribute(ring_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin));
+  CK(cudaFuncSetAttribute(ring_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin));
   ccdgpu_schedule sch{};
   sch.thin_split_mul = 1;
   sch.wide_split_mul = 3;

@@ -209,3 +209,15 @@ def test_kernel_profile_reports_ring_hh_onebody():
         # The ring and hh kernels write only intermediates: the solve is unchanged.
         res = sol.solve(tol=g["tol"])
         assert abs(res.e_corr - g["energies"][-1]) <= 1e-10 * abs(g["energies"][-1])
+
+
+def test_handles_of_different_sizes_coexist():
+    """Launch attributes belong to the kernels, not to a handle: a solver created before one
+    with smaller channels (smaller ring stages) still runs, and both match the reference."""
+    big, small = golden("eg54_s19"), golden("eg14_s19")
+    with system_for(big) as sb, system_for(small) as ss:
+        with CCDSolver(sb) as s1, CCDSolver(ss) as s2:
+            r1 = s1.solve(tol=big["tol"])
+            check_against_golden(big, s1, r1)
+            r2 = s2.solve(tol=small["tol"])
+            check_against_golden(small, s2, r2)
