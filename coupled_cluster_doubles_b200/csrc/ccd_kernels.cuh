@@ -895,6 +895,16 @@ constexpr int kAsmThreads = 256;
 constexpr int kAsmPerThread = 2;  // elements per thread; a CTA covers one ElemRange
 __device__ __forceinline__ void energy_reduce(const double *epart, int n, Control *ctl, int flags,
                                               double *e_out);
+// Condition of the device solve loop's WHILE node after an iteration: another iteration while
+// the stop rule has not fired, below the launch's iteration limit, and (body_mixed) in the
+// mixed phase or (FP64 body) past it.
+__device__ __forceinline__ void loop_set_condition(const Control *ctl,
+                                                   cudaGraphConditionalHandle cond,
+                                                   bool body_mixed) {
+  const bool more = !ctl->done && ctl->iterations < ctl->stop_at;
+  const bool mixed_phase = ctl->phase == 1;
+  cudaGraphSetConditional(cond, (more && (body_mixed ? mixed_phase : !mixed_phase)) ? 1u : 0u);
+}
 
 // In a mixed iteration (nt > 0) the assembly writes only the bf16 ladder operand images;
 // retile_kernel rebuilds the FP64 tiles if FP64 iterations follow.
@@ -955,8 +965,14 @@ assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__r
                       double *__restrict__ epart, int32_t *ticket, Control *ctl,
                       __nv_bfloat16 *__restrict__ tkt_tc, int64_t tkt_tc_stride,
                       __nv_bfloat16 *__restrict__ tmt_tc, int64_t tmt_tc_stride, int nt,
-                      int gate) {
-  if (skip_iteration(ctl, gate, kTrAssemble)) return;
+                      cudaGraphConditionalHandle cond, int loop_body, int gate) {
+  // loop_body: 0 outside the device solve loop, 1 / 2 last kernel of its FP64 / mixed body,
+  // where the CTA that applies the stop rule also sets the loop condition.  A skipped body
+  // (stop rule fired, or the other precision's phase) ends its loop.
+  if (skip_iteration(ctl, gate, kTrAssemble)) {
+    if (loop_body && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0u);
+    return;
+  }
   __shared__ AsmRowInfo rows[kAsmMaxRows];
   __shared__ AsmColInfo cols[kAsmMaxCols];
   __shared__ double scratch[32];
@@ -1067,6 +1083,7 @@ assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__r
   if (threadIdx.x == 0) {
     *ticket = 0;
     if (nt) ctl->retile = 1;  // the FP64 ladder tiles were not written this iteration
+    if (loop_body) loop_set_condition(ctl, cond, loop_body == 2);
   }
 }
 
@@ -1234,18 +1251,17 @@ __device__ __forceinline__ void energy_reduce(const double *epart, int n, Contro
 }
 
 // Last node of an iteration body of the device solve loop (a CUDA graph with WHILE conditional
-// nodes): decides from the control block whether the loop runs another iteration.  body_mixed:
-// the mixed-precision loop continues in phase 1 only; the FP64 loop never runs in phase 1.
-// Every body ends here, also when its kernels skipped, so no loop can spin without progress:
-// a body either advances `iterations` or clears its condition.
+// nodes) when the system has no assembly blocks: decides from the control block whether the
+// loop runs another iteration.  body_mixed: the mixed-precision loop continues in phase 1 only;
+// the FP64 loop never runs in phase 1.  Otherwise the fused assembly, the last kernel of every
+// body, sets the condition (also when it skipped), so no loop can spin without progress: a
+// body either advances `iterations` or clears its condition.
 __global__ void loop_ctl_kernel(const Control *ctl, cudaGraphConditionalHandle cond,
                                 int body_mixed) {
   pdl_enter();
   trace_start(ctl, kTrLoopCtl);
   if (threadIdx.x != 0) return;
-  const bool more = !ctl->done && ctl->iterations < ctl->stop_at;
-  const bool mixed_phase = ctl->phase == 1;
-  cudaGraphSetConditional(cond, (more && (body_mixed ? mixed_phase : !mixed_phase)) ? 1u : 0u);
+  loop_set_condition(ctl, cond, body_mixed != 0);
 }
 
 __global__ void __launch_bounds__(kEnergyThreads)

@@ -1135,7 +1135,8 @@ int launch_assemble_fused(ccdgpu_handle *h, cudaStream_t st, int gate) {
       (const AsmColStatic *)h->asm_cols, (const double *)h->v_pphh, (const double *)h->dmat,
       (const double *)h->d_ring, (const int32_t *)(h->flat + 4 * h->n_t), h->old_phhp,
       (const double *)h->xh, (const double *)h->yp, h->t[0], h->t[1], h->t_kt, h->t_mt, h->epart,
-      h->ticket, h->ctl, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc, gate ? h->nt : 0, gate));
+      h->ticket, h->ctl, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc, gate ? h->nt : 0,
+      (cudaGraphConditionalHandle)(h->loop_capture ? h->loop_cond : 0), h->loop_capture, gate));
 }
 int launch_energy(ccdgpu_handle *h, cudaStream_t st, int flags) {
   energy_kernel<<<1, kEnergyThreads, 0, st>>>(h->epart, h->n_ranges, h->ctl, flags, h->e_out, 0);
@@ -1191,7 +1192,7 @@ int enqueue_fused_iteration(ccdgpu_handle *h, bool mixed) {
   if ((rc = ladder(h->s0))) return rc;
   CK(cudaStreamWaitEvent(h->s0, h->ev_join, 0));
   if ((rc = launch_assemble_fused(h, h->s0, gate))) return rc;  // + energy and stop rule
-  if (h->loop_capture) {
+  if (h->loop_capture && !h->n_asm_blocks) {  // else the assembly set the loop condition
     h->launches++;
     CK(launch_pdl(loop_ctl_kernel, 1, 32, 0, h->s0, (const Control *)h->ctl, h->loop_cond,
                   h->loop_capture == 2 ? 1 : 0));
@@ -1288,7 +1289,8 @@ int fused_ready_graph(ccdgpu_handle *h, bool mixed) {
 }
 
 // The device solve loop.  Graph: [WHILE c_mix { mixed iteration }] -> WHILE c64 { FP64
-// iteration }; each body ends with loop_ctl_kernel, which sets its own condition.  Both
+// iteration }; each body ends with the fused assembly, whose stop-rule CTA sets the body's
+// condition (loop_ctl_kernel when a system has no assembly blocks).  Both
 // conditions default to 1 at every launch; one launch runs until the stop rule fires or
 // ctl->stop_at is reached.
 int capture_loop_graph(ccdgpu_handle *h, bool mixed, cudaGraphExec_t *exec) {
