@@ -593,37 +593,6 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-__global__ void __launch_bounds__(256)
-ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restrict__ v_hpph,
-                  const double *__restrict__ v_hphp, const double *__restrict__ t_phhp,
-                  const int32_t *__restrict__ inv, double *__restrict__ out, const Control *ctl,
-                  int gate) {
-  if (skip_iteration(ctl, gate, kTrRingSmall)) return;
-  __shared__ double buf[8][3 * kRingSmall * kRingSmall];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int mi = blockIdx.x * 8 + w;
-  if (mi >= n) return;
-  const ModInfo m = mods[mi];
-  const int ph = m.ph, hp = m.hp;
-  double *Ts = buf[w], *Vt = Ts + ph * hp, *Ys = Vt + hp * ph;
-  for (int e = lane; e < ph * hp; e += 32) {
-    Ts[e] = t_phhp[m.m_off + e];
-    Vt[e] = v_hpph[m.m_off + e];
-  }
-  for (int e = lane; e < hp * hp; e += 32) Ys[e] = v_hphp[m.y_off + e];
-  __syncwarp();
-  for (int e = lane; e < hp * hp; e += 32) {
-    const int i = e / hp, j = e - i * hp;
-    Ys[e] = 0.5 * dot4(Vt + i, hp, Ts + j, hp, ph) + Ys[e];
-  }
-  __syncwarp();
-  for (int e = lane; e < ph * hp; e += 32) {
-    const int i = e / hp, j = e - i * hp;
-    const double r = dot4(Ts + i * hp, 1, Ys + j, hp, hp);
-    out[inv ? (int64_t)inv[m.m_off + e] : m.m_off + e] = r;
-  }
-}
-
 // C (M8*8 x N8*8) = A B, K4*4 deep, on 8 x 8 tiles: warps warp, warp + nwarps, ... take items of
 // one 8-row tile by NC column tiles (the A fragment is reused NC times).  A[m][k] =
 // A[m * ars + k * aks], B[k][n] = B[k * ldb + n]; epi(row, col, value) stores each result.
@@ -666,6 +635,50 @@ __host__ __device__ inline int ring_pad8(int n) { return (n + 7) & ~7; }
 __host__ __device__ inline int ring_stage_doubles(int ph, int hp) {
   const int P = ring_pad8(ph), H = ring_pad8(hp), ld = H + 4;
   return even_up((2 * P + H) * ld + (ph * hp + 1) / 2);  // 16-byte steps
+}
+
+// Channels with ph', hp' <= kRingSmall, one per warp (kRingSmallWarps per CTA), the same two
+// products on the FP64 MMA: the warp's stage is padded to P, H in {8, 16} with zeros and a row
+// stride of 20 doubles (4 mod 8: conflict-free fragment loads); R goes straight to global
+// memory (scattered through the inverse ai_jb table on the fused path).
+constexpr int kRingSmallWarps = 4;
+constexpr int kRingSmallLd = kRingSmall + 4;
+__global__ void __launch_bounds__(kRingSmallWarps * 32)
+ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restrict__ v_hpph,
+                  const double *__restrict__ v_hphp, const double *__restrict__ t_phhp,
+                  const int32_t *__restrict__ inv, double *__restrict__ out, const Control *ctl,
+                  int gate) {
+  if (skip_iteration(ctl, gate, kTrRingSmall)) return;
+  __shared__ __align__(16) double buf[kRingSmallWarps][3 * kRingSmall * kRingSmallLd];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int mi = blockIdx.x * kRingSmallWarps + w;
+  if (mi >= n) return;  // whole warps: the MMAs below are warp-collective
+  const ModInfo m = mods[mi];
+  const int ph = m.ph, hp = m.hp, P = ring_pad8(ph), H = ring_pad8(hp), ld = kRingSmallLd;
+  const int hs = H == 8 ? 3 : 4;  // log2 H
+  double *Ts = buf[w], *Vt = Ts + kRingSmall * ld, *Ys = Vt + kRingSmall * ld;
+  for (int e = lane; e < P * H; e += 32) {
+    const int r = e >> hs, c = e & (H - 1);
+    const bool in = r < ph && c < hp;
+    const int64_t src = m.m_off + r * hp + c;
+    Ts[r * ld + c] = in ? t_phhp[src] : 0.0;
+    Vt[r * ld + c] = in ? v_hpph[src] : 0.0;
+  }
+  for (int e = lane; e < H * H; e += 32) {
+    const int r = e >> hs, c = e & (H - 1);
+    Ys[r * ld + c] = (r < hp && c < hp) ? v_hphp[m.y_off + r * hp + c] : 0.0;
+  }
+  __syncwarp();
+  // A[i][k] = V_hpph[i][k] = Vt[k][i]; each Y element is read and written by its owner lane.
+  warp_mma_gemm<2>(Vt, 1, ld, Ts, ld, H / 8, H / 8, P / 4, 0, 1,
+                   [&](int r, int c, double v) { Ys[r * ld + c] = 0.5 * v + Ys[r * ld + c]; });
+  __syncwarp();
+  warp_mma_gemm<2>(Ts, ld, 1, Ys, ld, P / 8, H / 8, H / 4, 0, 1, [&](int r, int c, double v) {
+    if (r < ph && c < hp) {
+      const int p = r * hp + c;
+      out[inv ? (int64_t)inv[m.m_off + p] : m.m_off + p] = v;
+    }
+  });
 }
 
 // Y = V_hphp + 0.5 V_hpph T' (H x H, K = P), then R = T' Y (P x H, K = H) on the FP64 MMA;
@@ -953,6 +966,9 @@ struct AsmColInfo {
   double xi, xj, eij;
 };
 
+// LOOP: launched as the last kernel of a device-solve-loop body (sets the WHILE condition);
+// the variant without it is the one profilers can replay.
+template <bool LOOP>
 __global__ void __launch_bounds__(kAsmThreads, 3)
 assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__restrict__ chans,
                       const AsmRowStatic *__restrict__ asm_rows,
@@ -970,7 +986,8 @@ assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__r
   // where the CTA that applies the stop rule also sets the loop condition.  A skipped body
   // (stop rule fired, or the other precision's phase) ends its loop.
   if (skip_iteration(ctl, gate, kTrAssemble)) {
-    if (loop_body && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0u);
+    if constexpr (LOOP)
+      if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0u);
     return;
   }
   __shared__ AsmRowInfo rows[kAsmMaxRows];
@@ -1083,7 +1100,7 @@ assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__r
   if (threadIdx.x == 0) {
     *ticket = 0;
     if (nt) ctl->retile = 1;  // the FP64 ladder tiles were not written this iteration
-    if (loop_body) loop_set_condition(ctl, cond, loop_body == 2);
+    if constexpr (LOOP) loop_set_condition(ctl, cond, loop_body == 2);
   }
 }
 

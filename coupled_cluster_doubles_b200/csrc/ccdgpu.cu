@@ -1096,7 +1096,8 @@ int launch_ring(ccdgpu_handle *h, cudaStream_t st, int gate, bool fused, int onl
   const int32_t *inv = fused ? h->inv4 : nullptr;
   double *out = fused ? h->d_ring : h->r_phhp;
   if (h->n_mod_small && (only < 0 || only == 0)) {
-    ring_small_kernel<<<(int)ceil_div(h->n_mod_small, 8), 256, 0, st>>>(
+    ring_small_kernel<<<(int)ceil_div(h->n_mod_small, kRingSmallWarps), kRingSmallWarps * 32, 0,
+                        st>>>(
         h->mods, h->n_mod_small, h->v_hpph, h->v_hphp, h->old_phhp, inv, out, h->ctl, gate);
     h->launches++;
     CK(cudaGetLastError());
@@ -1130,7 +1131,8 @@ int launch_assemble_fused(ccdgpu_handle *h, cudaStream_t st, int gate) {
   if (!h->n_asm_blocks) return CCDGPU_OK;
   h->launches++;
   return cuda_status(launch_pdl(
-      assemble_fused_kernel, h->n_asm_blocks, kAsmThreads, 0, st, (const ElemRange *)h->pranges,
+      h->loop_capture ? assemble_fused_kernel<true> : assemble_fused_kernel<false>,
+      h->n_asm_blocks, kAsmThreads, 0, st, (const ElemRange *)h->pranges,
       (const ChanInfo *)h->chans, (const AsmRowStatic *)h->asm_rows,
       (const AsmColStatic *)h->asm_cols, (const double *)h->v_pphh, (const double *)h->dmat,
       (const double *)h->d_ring, (const int32_t *)(h->flat + 4 * h->n_t), h->old_phhp,
