@@ -39,8 +39,9 @@ struct DevBuf {
 
 struct ccdgpu_handle {
   ccdgpu_options opt{};
-  cudaStream_t s0 = nullptr, s1 = nullptr, s2 = nullptr;
+  cudaStream_t s0 = nullptr, s1 = nullptr, s2 = nullptr, s3 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork2 = nullptr, ev_join2 = nullptr;
+  cudaEvent_t ev_fork3 = nullptr, ev_join3 = nullptr;  // one-body sums beside the pp ladder
   cudaEvent_t ev[10] = {};
   uint64_t nch = 0, nsp = 0, np = 0, npart = 0;
   int64_t n_t = 0, n_m = 0, n_h = 0, n_p = 0;
@@ -186,6 +187,9 @@ void release(ccdgpu_handle *h) {
   if (h->ev_fork2) cudaEventDestroy(h->ev_fork2);
   if (h->ev_join2) cudaEventDestroy(h->ev_join2);
   if (h->s2) cudaStreamDestroy(h->s2);
+  if (h->ev_fork3) cudaEventDestroy(h->ev_fork3);
+  if (h->ev_join3) cudaEventDestroy(h->ev_join3);
+  if (h->s3) cudaStreamDestroy(h->s3);
   if (h->s1) cudaStreamDestroy(h->s1);
   if (h->s0) cudaStreamDestroy(h->s0);
 }
@@ -1156,7 +1160,8 @@ int launch_map_to(ccdgpu_handle *h, cudaStream_t st, const double *src, double *
   return cuda_status(cudaGetLastError());
 }
 
-// One fused iteration: hh ladder and ring concurrently, then one-body, pp ladder, assembly.
+// One fused iteration: ring (s1) beside hh ladder, then pp ladder beside the one-body sums (s3),
+// then the assembly.
 // mixed: the pp ladder runs on the tensor cores (split bf16) instead of the FP64 pipe.
 int enqueue_fused_iteration(ccdgpu_handle *h, bool mixed) {
   int rc;
@@ -1190,9 +1195,14 @@ int enqueue_fused_iteration(ccdgpu_handle *h, bool mixed) {
   if ((rc = launch_ring(h, h->s1, gate, true))) return rc;
   CK(cudaEventRecord(h->ev_join, h->s1));
   if ((rc = launch_hh_ladder(h, h->s0, gate))) return rc;
-  if ((rc = launch_onebody_fused(h, h->s0, gate))) return rc;
+  // The one-body sums feed only the assembly: they run on s3 beside the pp ladder.
+  CK(cudaEventRecord(h->ev_fork3, h->s0));
+  CK(cudaStreamWaitEvent(h->s3, h->ev_fork3, 0));
+  if ((rc = launch_onebody_fused(h, h->s3, gate))) return rc;
+  CK(cudaEventRecord(h->ev_join3, h->s3));
   if ((rc = ladder(h->s0))) return rc;
   CK(cudaStreamWaitEvent(h->s0, h->ev_join, 0));
+  CK(cudaStreamWaitEvent(h->s0, h->ev_join3, 0));
   if ((rc = launch_assemble_fused(h, h->s0, gate))) return rc;  // + energy and stop rule
   if (h->loop_capture && !h->n_asm_blocks) {  // else the assembly set the loop condition
     h->launches++;
@@ -1443,6 +1453,9 @@ int ccdgpu_create(const ccdgpu_problem *prob, const ccdgpu_options *opt, ccdgpu_
   if (!rc) rc = cuda_status(cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking));
   if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->ev_fork2, cudaEventDisableTiming));
   if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->ev_join2, cudaEventDisableTiming));
+  if (!rc) rc = cuda_status(cudaStreamCreateWithFlags(&h->s3, cudaStreamNonBlocking));
+  if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->ev_fork3, cudaEventDisableTiming));
+  if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->ev_join3, cudaEventDisableTiming));
   for (int i = 0; i < 10 && !rc; i++) rc = cuda_status(cudaEventCreate(&h->ev[i]));
   if (!rc) rc = build(h, prob);
   if (!rc) rc = set_ctl(h, 0, 0.0, 100, 0.5, true);
