@@ -956,13 +956,13 @@ __device__ __forceinline__ double asm_value(double v, double dm, double r_j, dou
 // Shared-memory tables of a CTA's rows and of its channel's columns: the static parts come from
 // AsmRowStatic / AsmColStatic (built at create), y_a, y_b, x_i, x_j are the current one-body sums.
 struct AsmRowInfo {
-  int32_t o_ab, o_ba;  // row offsets inside the channel block (ab * hh, ba * hh)
+  int32_t o_ab, o_ba;  // row offsets inside the channel block (ab * hh, ba * hh; equal if a = b)
   int2 qa, qb;         // ladder operand indices of rows ab and ba (pk_idx)
-  int32_t mirrored, pad;
+  int32_t pa, pb;      // particle indices a - np, b - np
   double ya, yb, ea, eb;
 };
 struct AsmColInfo {
-  int32_t js, pad;
+  int32_t js, i, j, pad;
   double xi, xj, eij;
 };
 
@@ -985,46 +985,55 @@ assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__r
   // loop_body: 0 outside the device solve loop, 1 / 2 last kernel of its FP64 / mixed body,
   // where the CTA that applies the stop rule also sets the loop condition.  A skipped body
   // (stop rule fired, or the other precision's phase) ends its loop.
+  __shared__ AsmRowInfo rows[kAsmMaxRows];
+  __shared__ AsmColInfo cols[kAsmMaxCols];
+  __shared__ double scratch[32];
+  __shared__ int last;
+  // The CTA's range, channel and static tables are written only at create: they are read
+  // before waiting for this iteration's earlier kernels (skip_iteration), so that their load
+  // latency overlaps those kernels' tail.  A thread later completes the rows and columns it
+  // staged itself.
+  const ElemRange rg = pranges[blockIdx.x];
+  const ChanInfo ch = chans[rg.ch];
+  const int hh = ch.hh;
+  const int u0 = (int)(rg.e0 / hh), nrows = (int)(rg.e1 / hh) - u0;
+  for (int r = threadIdx.x; r < nrows; r += kAsmThreads) {
+    const AsmRowStatic s = asm_rows[ch.row_off + u0 + r];
+    AsmRowInfo &ri = rows[r];
+    ri.o_ab = s.o_ab;
+    ri.o_ba = s.o_ba;
+    ri.qa = make_int2(s.qa_x, s.qa_y);
+    ri.qb = make_int2(s.qb_x, s.qb_y);
+    ri.pa = s.pa;
+    ri.pb = s.pb;
+    ri.ea = s.ea;
+    ri.eb = s.eb;
+  }
+  for (int j = threadIdx.x; j < hh; j += kAsmThreads) {
+    const AsmColStatic s = asm_cols[ch.hh_off + j];
+    AsmColInfo &ci = cols[j];
+    ci.js = s.js;
+    ci.i = s.i;
+    ci.j = s.j;
+    ci.pad = 0;
+    ci.eij = s.eij;
+  }
   if (skip_iteration(ctl, gate, kTrAssemble)) {
     if constexpr (LOOP)
       if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0u);
     return;
   }
-  __shared__ AsmRowInfo rows[kAsmMaxRows];
-  __shared__ AsmColInfo cols[kAsmMaxCols];
-  __shared__ double scratch[32];
-  __shared__ int last;
-  const ElemRange rg = pranges[blockIdx.x];
-  const ChanInfo ch = chans[rg.ch];
   const double *__restrict__ t_old = ctl->parity ? tbuf1 : tbuf0;
   double *__restrict__ t_new = ctl->parity ? tbuf0 : tbuf1;
   const double mixing = ctl->mixing;
-  const int hh = ch.hh;
-  const int u0 = (int)(rg.e0 / hh), nrows = (int)(rg.e1 / hh) - u0;
+  // The current one-body sums y_a, y_b, x_i, x_j (same thread, same entries as above).
   for (int r = threadIdx.x; r < nrows; r += kAsmThreads) {
-    const AsmRowStatic s = asm_rows[ch.row_off + u0 + r];
-    AsmRowInfo ri;
-    ri.o_ab = s.o_ab;
-    ri.o_ba = s.o_ba;
-    ri.qa = make_int2(s.qa_x, s.qa_y);
-    ri.qb = make_int2(s.qb_x, s.qb_y);
-    ri.mirrored = s.o_ba != s.o_ab;
-    ri.pad = 0;
-    ri.ya = yp[s.pa];
-    ri.yb = yp[s.pb];
-    ri.ea = s.ea;
-    ri.eb = s.eb;
-    rows[r] = ri;
+    rows[r].ya = yp[rows[r].pa];
+    rows[r].yb = yp[rows[r].pb];
   }
   for (int j = threadIdx.x; j < hh; j += kAsmThreads) {
-    const AsmColStatic s = asm_cols[ch.hh_off + j];
-    AsmColInfo ci;
-    ci.js = s.js;
-    ci.pad = 0;
-    ci.xi = xh[s.i];
-    ci.xj = xh[s.j];
-    ci.eij = s.eij;
-    cols[j] = ci;
+    cols[j].xi = xh[cols[j].i];
+    cols[j].xj = xh[cols[j].j];
   }
   __syncthreads();
   const double *tb = t_old + ch.t_off, *rb = d_ring + ch.t_off, *vb = v_pphh + ch.t_off;
@@ -1072,7 +1081,7 @@ assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__r
                                tmt_tc_stride);
       else write_t_tiles_q(ch, ri.qa, j, t1, t_kt, t_mt);
       corr += vv[u][0] * t1;
-      if (ri.mirrored) {
+      if (ri.o_ba != ri.o_ab) {
         // Row ba: the same formula with a and b exchanged.
         const double t2 = asm_value(vv[u][1], dv[u][1], rv[u][2], rv[u][3], rv[u][0], rv[u][1],
                                     tv[u][2], tv[u][3], tv[u][0], ci.xi, ci.xj, ri.yb, ri.ya,
