@@ -3,8 +3,8 @@
 Tolerances.  One ladder evaluation with 2-term bf16 operands (about 17 significant bits each,
 FP32 accumulation) agrees with the FP64 ladder to 2e-4 of the largest |D| of the chain; with
 3-term operands to 2e-6.  A mixed solve ends with FP64 iterations, so its converged energy
-per particle agrees with the reference's to 1e-7 relative and its T2
-with the reference's to 1e-7 max-abs; both are usually far closer.
+per particle agrees with the reference's to 1e-7 relative (the accuracy bound of the mixed
+mode) and its T2 with the reference's to 1e-7 max-abs; both are usually far closer.
 """
 import numpy as np
 import pytest
