@@ -1290,6 +1290,31 @@ __global__ void loop_ctl_kernel(const Control *ctl, cudaGraphConditionalHandle c
   loop_set_condition(ctl, cond, body_mixed != 0);
 }
 
+// MBPT2 (MBPT2Corr.cpp:6-38) over the elements of the active channels, one CTA per range:
+// epart[range] = sum <ij|v|ab>^2 / (e_i + e_j - e_a - e_b) (energy_reduce applies the 1/4), and
+// with t_out the first-order amplitudes t_ab,ij = <ab|v|ij> / (e_i + e_j - e_a - e_b).
+__global__ void __launch_bounds__(256)
+mbpt2_kernel(const ElemRange *__restrict__ ranges, const ChanInfo *__restrict__ chans,
+             const int2 *__restrict__ pp_pairs, const int2 *__restrict__ hh_pairs,
+             const double *__restrict__ v_pphh, const double *__restrict__ eps,
+             double *__restrict__ t_out, double *__restrict__ epart) {
+  __shared__ double scratch[32];
+  const ElemRange rg = ranges[blockIdx.x];
+  const ChanInfo ch = chans[rg.ch];
+  double acc = 0.0;
+  for (int64_t e = rg.e0 + threadIdx.x; e < rg.e1; e += blockDim.x) {
+    const int64_t loc = e - ch.t_off;
+    const int ab = (int)(loc / ch.hh), ij = (int)(loc - (int64_t)ab * ch.hh);
+    const int2 pab = pp_pairs[ch.pp_off + ab], pij = hh_pairs[ch.hh_off + ij];
+    const double den = eps[pij.x] + eps[pij.y] - eps[pab.x] - eps[pab.y];
+    const double v = v_pphh[e];
+    acc += v * v / den;
+    if (t_out) t_out[e] = v / den;
+  }
+  const double sum = block_sum<256>(acc, scratch);
+  if (threadIdx.x == 0) epart[blockIdx.x] = sum;
+}
+
 __global__ void __launch_bounds__(kEnergyThreads)
 energy_kernel(const double *__restrict__ epart, int n, Control *ctl, int flags, double *e_out,
               int gate) {

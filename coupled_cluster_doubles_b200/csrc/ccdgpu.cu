@@ -1504,6 +1504,31 @@ int ccdgpu_set_t2(ccdgpu_handle *h, const double *t2, uint64_t n) {
   return CCDGPU_OK;
 }
 
+int ccdgpu_mbpt2(ccdgpu_handle *h, int32_t init_t2, double *e_mbpt2) {
+  if (!h) return CCDGPU_ERR_INVALID_ARGUMENT;
+  CK(cudaSetDevice(h->opt.device));
+  int rc = set_ctl(h, 0, h->h_ctl->tol, h->h_ctl->max_iters, h->h_ctl->mixing, false);
+  if (rc) return rc;
+  if (init_t2) {
+    // The amplitudes become the current ones (parity 0, as after ccdgpu_set_t2).
+    h->h_ctl->parity = 0;
+    CK(cudaMemcpyAsync(h->ctl, h->h_ctl, sizeof(Control), cudaMemcpyHostToDevice, h->s0));
+  }
+  if (h->n_ranges) {
+    mbpt2_kernel<<<h->n_ranges, 256, 0, h->s0>>>(h->ranges, h->chans, h->pp_pairs, h->hh_pairs,
+                                                  h->v_pphh, h->eps, init_t2 ? h->t[1] : nullptr,
+                                                  h->epart);
+    CK(cudaGetLastError());
+  }
+  if ((rc = launch_energy(h, h->s0, 0))) return rc;
+  if (init_t2 && (rc = launch_map_to(h, h->s0, h->t[1], h->t[0]))) return rc;
+  double e = 0.0;
+  CK(cudaMemcpyAsync(&e, h->e_out, 8, cudaMemcpyDeviceToHost, h->s0));
+  CK(cudaStreamSynchronize(h->s0));
+  if (e_mbpt2) *e_mbpt2 = h->n_ranges ? e : 0.0;
+  return check_errors(h);
+}
+
 int ccdgpu_get_t2(ccdgpu_handle *h, double *t2, uint64_t n) {
   if (!h || !t2 || n != (uint64_t)h->n_t) return CCDGPU_ERR_INVALID_ARGUMENT;
   CK(cudaSetDevice(h->opt.device));

@@ -193,6 +193,14 @@ class CCDSolver:
         names = ["fp64_thin", "fp64_mid", "fp64_wide", "tensor_core"]
         return {n: (ms[k], fl[k], by[k]) for k, n in enumerate(names) if ms[k] > 0}
 
+    def mbpt2(self, init_t2=False):
+        """E_MBPT2 computed on the device (ccdgpu_mbpt2); init_t2=True also starts T2 from the
+        first-order amplitudes instead of zero."""
+        e = ctypes.c_double()
+        _check(_native.gpu_lib().ccdgpu_mbpt2(self._h, int(bool(init_t2)), ctypes.byref(e)),
+               "ccdgpu_mbpt2")
+        return e.value
+
     def kernel_profile(self, reps=5):
         """Ring, hh-ladder and one-body kernel classes alone (ccdgpu_kernel_profile):
         {class: (ms, flops, bytes)}; classes without work are left out."""

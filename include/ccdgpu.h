@@ -160,6 +160,12 @@ int ccdgpu_reset(ccdgpu_handle *h);
  * the scattered layouts, as main.cpp:660-665 would after an iteration. */
 int ccdgpu_set_t2(ccdgpu_handle *h, const double *t2_pphh, uint64_t n);
 int ccdgpu_get_t2(ccdgpu_handle *h, double *t2_pphh, uint64_t n);
+/* Second-order energy on the device, the reference's MBPT2 (MBPT2Corr.cpp:6-38):
+ * E_MBPT2 = 1/4 sum_{abij} |<ij|v|ab>|^2 / (e_i + e_j - e_a - e_b) from the handle's V_hhpp and
+ * single-particle energies (deterministic compensated sum).  init_t2 != 0 also makes the
+ * first-order amplitudes t_ab,ij = <ab|v|ij> / (e_i + e_j - e_a - e_b) the current T2 (an
+ * alternative start to the reference's T2 = 0, main.cpp:497-503). */
+int ccdgpu_mbpt2(ccdgpu_handle *h, int32_t init_t2, double *e_mbpt2);
 uint64_t ccdgpu_t2_size(const ccdgpu_handle *h);
 
 /* One CCD iteration (main.cpp:589-670) with the path and precision chosen at create time.

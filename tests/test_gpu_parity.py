@@ -221,3 +221,46 @@ def test_handles_of_different_sizes_coexist():
             check_against_golden(big, s1, r1)
             r2 = s2.solve(tol=small["tol"])
             check_against_golden(small, s2, r2)
+
+
+@pytest.mark.parametrize("name", SMALL + ["eg54_s19"])
+def test_device_mbpt2_matches_reference(name):
+    """E_MBPT2 on the device against the reference's own value (MBPT2Corr.cpp:6-38)."""
+    g = golden(name)
+    with system_for(g) as s, CCDSolver(s) as sol:
+        e2 = sol.mbpt2()
+    ref = float(g["scalars"][1])
+    assert abs(e2 - ref) <= 1e-12 * abs(ref) + 1e-15, (e2, ref)
+
+
+@pytest.mark.parametrize("path", ["fused", "tables"])
+def test_mbpt2_start_reaches_the_same_fixed_point(path):
+    """Starting from the first-order amplitudes: T2 = V / D, and the solve converges to the
+    reference's energy (the fixed point does not depend on the start)."""
+    g = golden("eg14_s19")
+    with system_for(g) as s, CCDSolver(s, path=path) as sol:
+        e2 = sol.mbpt2(init_t2=True)
+        assert abs(e2 - float(g["scalars"][1])) <= 1e-12 * abs(e2)
+        t2 = sol.t2()
+        # Expected amplitudes from the host's V_hhpp blocks (hh x pp per channel) and energies.
+        d = s.chan_dims()
+        v = s.array("v_hhpp")
+        eps = s.array("sp_energy")
+        pp_map = s.array("pp_map").reshape(-1, 2)
+        hh_map = s.array("hh_map").reshape(-1, 2)
+        expect = np.zeros_like(t2)
+        off = po = ho = 0
+        for c in range(s.n_channels):
+            pp, hh = int(d[c, 0]), int(d[c, 1])
+            if pp and hh:
+                vb = v[off:off + pp * hh].reshape(hh, pp).T
+                P, H = pp_map[po:po + pp], hh_map[ho:ho + hh]
+                den = (eps[H[:, 0]] + eps[H[:, 1]])[None, :] - (eps[P[:, 0]] + eps[P[:, 1]])[:, None]
+                expect[off:off + pp * hh] = (vb / den).ravel()
+            off += pp * hh
+            po += pp
+            ho += hh
+        np.testing.assert_allclose(t2, expect, rtol=1e-14, atol=0)
+        res = sol.solve(tol=1e-12)
+        assert res.converged
+        assert abs(res.e_corr - g["energies"][-1]) <= 1e-10 * abs(g["energies"][-1])
