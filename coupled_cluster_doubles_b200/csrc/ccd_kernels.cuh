@@ -488,9 +488,11 @@ hh_mma_kernel(const HHTile *__restrict__ tiles, int n, const ChanInfo *__restric
   for (int m = 0; m < MC; ++m)
 #pragma unroll
     for (int c = 0; c < NMAX; ++c) acc[m][c][0] = acc[m][c][1] = 0.0;
-  const int nk4 = (tt.rows + 3) >> 2;
-#pragma unroll 2
-  for (int k4 = 0; k4 < nk4; ++k4) {
+  // hh <= 16: all kHHRows / 4 steps unrolled, so that every fragment load of the slice is issued
+  // at once (rows past the slice read as zero); wider hh: two steps at a time (registers).
+  constexpr int kSteps = kHHRows / 4;
+#pragma unroll(NMAX <= 2 ? kSteps : 2)
+  for (int k4 = 0; k4 < kSteps; ++k4) {
     const int k = 4 * k4 + t;
     const bool kin = k < tt.rows;
     const double *vr = vb + (int64_t)k * hh, *tr = tb + (int64_t)k * hh;
