@@ -55,6 +55,18 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def combine_ranks(dev_ms, iters, device, world):
+    """Replicas: the job's time is the slowest rank's device time (MAX) and its work the
+    iterations of all ranks (SUM); returns (max_ms, total_iterations)."""
+    import torch
+    ms = torch.tensor([float(dev_ms)], dtype=torch.float64, device=device)
+    it = torch.tensor([float(iters)], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(ms, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(it, op=torch.distributed.ReduceOp.SUM)
+    return float(ms.item()), float(it.item())
+
+
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the headline
 # kernel, from the ncu captures summarised in profiles/ (workload, kernel): bytes, source.
 NCU_TRAFFIC = {
@@ -287,12 +299,8 @@ def main():
                 iters += last.iterations
             torch.cuda.synchronize()
             barrier()
-            ms = torch.tensor([dev_ms], dtype=torch.float64, device=f"cuda:{local}")
-            it_t = torch.tensor([float(iters)], dtype=torch.float64, device=f"cuda:{local}")
-            if world > 1:
-                torch.distributed.all_reduce(ms, op=torch.distributed.ReduceOp.MAX)
-                torch.distributed.all_reduce(it_t, op=torch.distributed.ReduceOp.SUM)
-            timing[a] = {"max_ms": float(ms.item()), "iters": float(it_t.item()),
+            max_ms, total_it = combine_ranks(dev_ms, iters, f"cuda:{local}", world)
+            timing[a] = {"max_ms": max_ms, "iters": total_it,
                          "iters_per_solve": last.iterations,
                          "polish_per_solve": last.polish_iterations,
                          "e_corr": last.e_corr,
@@ -331,11 +339,7 @@ def main():
         if k >= args.warmup:
             e2e_secs += t1 - t0
             e2e_iters += r2.iterations
-    e2e_t = torch.tensor([e2e_secs], dtype=torch.float64, device=f"cuda:{local}")
-    e2e_i = torch.tensor([float(e2e_iters)], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(e2e_i, op=torch.distributed.ReduceOp.SUM)
+    e2e_secs_max, e2e_iters_all = combine_ranks(e2e_secs, e2e_iters, f"cuda:{local}", world)
 
     if rank == 0:
         peaks, peak_kind = measured_peaks()
@@ -424,7 +428,7 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "arms": arms_out,
             "shared_kernels_alone": shared,
-            "e2e": {"value": e2e_i.item() / e2e_t.item(), "unit": "iter/s",
+            "e2e": {"value": e2e_iters_all / e2e_secs_max, "unit": "iter/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * n_t2,
                     "what": "ccdgpu_create from host buffers + ccdgpu_solve + ccdgpu_get_t2"},
             "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved,
