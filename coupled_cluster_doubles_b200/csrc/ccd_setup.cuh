@@ -136,6 +136,26 @@ __device__ __forceinline__ double tbme_dev(const ModelDev &m, int a, int b, int 
   return direct_pnm_dev(qa, qb, qc, qd, m.Lb) - direct_pnm_dev(qa, qb, qd, qc, m.Lb);
 }
 
+// E_ref and the normal-ordered single-particle energies from the bare ones (SPBasis.cpp:7-40).
+// Thread p < nsp: e_p + sum_{j < nh} <pj|v|pj>, summed in the reference's order.  Thread nsp:
+// E_ref = sum_{i,j < nh} 0.5 <ij|v|ij> + sum_{i < nh} e_i, one running sum in the reference's
+// order, so its rounding matches.  out holds nsp energies, then E_ref.
+__global__ void normal_order_kernel(ModelDev m, const double *__restrict__ bare, int nsp, int nh,
+                                    double *__restrict__ out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < nsp) {
+    double e = bare[p];
+    for (int j = 0; j < nh; ++j) e += tbme_dev(m, p, j, p, j);
+    out[p] = e;
+  } else if (p == nsp) {
+    double eref = 0.;
+    for (int i = 0; i < nh; ++i)
+      for (int j = 0; j < nh; ++j) eref += 0.5 * tbme_dev(m, i, j, i, j);
+    for (int i = 0; i < nh; ++i) eref += bare[i];
+    out[nsp] = eref;
+  }
+}
+
 // One CTA per packed row u of a channel (items as for tile_v_kernel): the FP64 ladder tile
 // element and, for a mixed handle (nt > 0), its nt bf16 terms.
 __global__ void gen_v_kernel(const ChanInfo *__restrict__ chans, const int2 *__restrict__ items,

@@ -92,6 +92,11 @@ struct ccdgpu_handle {
   int32_t *ticket = nullptr;  // assembly's last-CTA ticket
   double *e_out = nullptr;
   int32_t *err = nullptr;
+  // The interaction model on the device (present when the problem carries one), and the
+  // buffer of ccdgpu_reference_energy: n_sp bare energies in, n_sp normal-ordered + E_ref out.
+  ModelDev md{};
+  bool has_model = false;
+  double *eps_io = nullptr;
 
   cudaGraphExec_t graph = nullptr;
   int64_t kernels_per_graph = 0;
@@ -461,10 +466,10 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   // V_ON_THE_FLY: V_pppp is generated on the device from the model, P->v_pppp is not read.
   const bool on_the_fly = h->opt.v_mode == CCDGPU_V_ON_THE_FLY;
   const ccdgpu_model *M = P->model;
-  if (on_the_fly && (!M || !M->qn || M->kind < CCDGPU_MODEL_PAIRING ||
-                     M->kind > CCDGPU_MODEL_ELECTRON_GAS ||
-                     M->qn_stride < (M->kind == CCDGPU_MODEL_PAIRING ? 2 : 5)))
-    return CCDGPU_ERR_INVALID_ARGUMENT;
+  const bool model_ok = M && M->qn && M->kind >= CCDGPU_MODEL_PAIRING &&
+                        M->kind <= CCDGPU_MODEL_ELECTRON_GAS &&
+                        M->qn_stride >= (M->kind == CCDGPU_MODEL_PAIRING ? 2 : 5);
+  if (on_the_fly && !model_ok) return CCDGPU_ERR_INVALID_ARGUMENT;
   if ((!on_the_fly && !P->v_pppp) || !P->v_hhpp || !P->v_hhhh || !P->v_hpph_mod ||
       !P->v_hphp_mod)
     return CCDGPU_ERR_INVALID_ARGUMENT;
@@ -771,13 +776,14 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   sc.add(&vraw, vraw_tot); sc.add(&hhpp_raw, n_t); sc.add(&hpph_raw, h->n_m); sc.add(&raw_idx, (size_t)8 * n_t);
   sc.add(&counts, (size_t)5 * n_t); sc.add(&d_vrows, vrows.size()); 
   sc.add(&d_vraw_off, vraw_off.size()); sc.add(&d_mod_dims, mod_dims.size()); sc.add(&d_o_m, o_m.size());
-  // On-the-fly V: quantum numbers and (electron gas) the direct Coulomb term by momentum
-  // transfer, computed here with the reference's expression (ElectronGasSPBasis.cpp:424-448).
+  // The model on the device (on-the-fly V, E_ref and normal ordering): quantum numbers and
+  // (electron gas) the direct Coulomb term by momentum transfer, computed here with the
+  // reference's expression (ElectronGasSPBasis.cpp:424-448).  Kept for the handle's lifetime.
   ModelDev md{};
   std::vector<double> vq;
   int32_t *d_qn = nullptr;
   double *d_vq = nullptr;
-  if (on_the_fly) {
+  if (model_ok) {
     md.kind = M->kind;
     md.stride = M->qn_stride;
     md.g = M->params[0];
@@ -804,19 +810,22 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
             vq[((size_t)(dx + md.R) * md.W + (dy + md.R)) * md.W + (dz + md.R)] = v;
           }
     }
-    sc.add(&d_qn, (size_t)nsp * M->qn_stride);
-    sc.add(&d_vq, vq.size());
-  }
-  const size_t n_allocs = h->allocs.size();
-  TRY(sc.commit(h));
-  if (on_the_fly) {
+    Arena mr;
+    mr.add(&d_qn, (size_t)nsp * M->qn_stride);
+    mr.add(&d_vq, vq.size());
+    mr.add(&h->eps_io, 2 * nsp + 1);
+    TRY(mr.commit(h));
     CK(cudaMemcpyAsync(d_qn, M->qn, (size_t)nsp * M->qn_stride * sizeof(int32_t),
                        cudaMemcpyHostToDevice, h->s0));
     if (!vq.empty())
       CK(cudaMemcpyAsync(d_vq, vq.data(), vq.size() * 8, cudaMemcpyHostToDevice, h->s0));
     md.qn = d_qn;
     md.vq = d_vq;
+    h->md = md;
+    h->has_model = true;
   }
+  const size_t n_allocs = h->allocs.size();
+  TRY(sc.commit(h));
 
   auto put = [&](auto *dst, const auto &v) -> int {
     if (!v.empty()) CK(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice, h->s0));
@@ -1527,6 +1536,24 @@ int ccdgpu_mbpt2(ccdgpu_handle *h, int32_t init_t2, double *e_mbpt2) {
   CK(cudaStreamSynchronize(h->s0));
   if (e_mbpt2) *e_mbpt2 = h->n_ranges ? e : 0.0;
   return check_errors(h);
+}
+
+int ccdgpu_reference_energy(ccdgpu_handle *h, const double *sp_energy_bare, double *e_ref,
+                            double *sp_energy_normal) {
+  if (!h || !sp_energy_bare || !e_ref) return CCDGPU_ERR_INVALID_ARGUMENT;
+  if (!h->has_model) return CCDGPU_ERR_UNSUPPORTED;
+  CK(cudaSetDevice(h->opt.device));
+  const int nsp = (int)h->nsp;
+  std::vector<double> out((size_t)nsp + 1);
+  CK(cudaMemcpyAsync(h->eps_io, sp_energy_bare, (size_t)nsp * 8, cudaMemcpyHostToDevice, h->s0));
+  normal_order_kernel<<<(nsp + 128) / 128, 128, 0, h->s0>>>(h->md, h->eps_io, nsp, (int)h->np,
+                                                            h->eps_io + nsp);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out.data(), h->eps_io + nsp, out.size() * 8, cudaMemcpyDeviceToHost, h->s0));
+  CK(cudaStreamSynchronize(h->s0));
+  *e_ref = out[nsp];
+  if (sp_energy_normal) std::copy(out.begin(), out.begin() + nsp, sp_energy_normal);
+  return CCDGPU_OK;
 }
 
 int ccdgpu_get_t2(ccdgpu_handle *h, double *t2, uint64_t n) {

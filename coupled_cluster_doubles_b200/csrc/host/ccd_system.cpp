@@ -633,6 +633,10 @@ int ccdhost_array(const ccdhost_system *cs, const char *name, const void **data,
     *data = s->eps.data(); *count = s->eps.size(); *dtype = 1;
     return CCDGPU_OK;
   }
+  if (n == "sp_energy_bare") {
+    *data = s->m.eps.data(); *count = s->m.eps.size(); *dtype = 1;
+    return CCDGPU_OK;
+  }
   static const char *tnames[8] = {"map_iab_j", "map_jab_i", "map_a_bij", "map_b_aij",
                                   "map_ai_jb", "map_aj_ib", "map_bi_ja", "map_bj_ia"};
   for (int k = 0; k < 8; k++)

@@ -201,6 +201,18 @@ class CCDSolver:
                "ccdgpu_mbpt2")
         return e.value
 
+    def reference_energy(self, sp_energy_bare):
+        """E_ref and the normal-ordered single-particle energies computed on the device from
+        the bare ones and the system's model (ccdgpu_reference_energy): (e_ref, energies)."""
+        bare = np.ascontiguousarray(sp_energy_bare, dtype=np.float64)
+        out = np.zeros_like(bare)
+        e = ctypes.c_double()
+        dp = ctypes.POINTER(ctypes.c_double)
+        _check(_native.gpu_lib().ccdgpu_reference_energy(
+            self._h, bare.ctypes.data_as(dp), ctypes.byref(e), out.ctypes.data_as(dp)),
+            "ccdgpu_reference_energy")
+        return e.value, out
+
     def kernel_profile(self, reps=5):
         """Ring, hh-ladder and one-body kernel classes alone (ccdgpu_kernel_profile):
         {class: (ms, flops, bytes)}; classes without work are left out."""

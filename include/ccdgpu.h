@@ -166,6 +166,15 @@ int ccdgpu_get_t2(ccdgpu_handle *h, double *t2_pphh, uint64_t n);
  * first-order amplitudes t_ab,ij = <ab|v|ij> / (e_i + e_j - e_a - e_b) the current T2 (an
  * alternative start to the reference's T2 = 0, main.cpp:497-503). */
 int ccdgpu_mbpt2(ccdgpu_handle *h, int32_t init_t2, double *e_mbpt2);
+/* Reference energy and normal ordering on the device (SPBasis.cpp:7-40, referenceEnergy and
+ * rotateSpEnergiesToNormalOrdered, called at main.cpp:64-67): from the bare single-particle
+ * energies sp_energy_bare[n_sp] and the problem's interaction model,
+ *   E_ref = sum_{i,j<A} 1/2 <ij|v|ij> + sum_{i<A} e_i,   e'_p = e_p + sum_{j<A} <pj|v|pj>,
+ * each summed in the reference's order.  Writes E_ref to *e_ref and, when sp_energy_normal is
+ * not NULL, the n_sp normal-ordered energies.  Needs ccdgpu_problem.model at create
+ * (CCDGPU_ERR_UNSUPPORTED without it); the handle's own energies are not changed. */
+int ccdgpu_reference_energy(ccdgpu_handle *h, const double *sp_energy_bare, double *e_ref,
+                            double *sp_energy_normal);
 uint64_t ccdgpu_t2_size(const ccdgpu_handle *h);
 
 /* One CCD iteration (main.cpp:589-670) with the path and precision chosen at create time.

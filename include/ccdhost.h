@@ -49,7 +49,8 @@ double ccdhost_mbpt2(const ccdhost_system *s);            /* MBPT2Corr over all 
 /* Named flat arrays for tests: "chan_dims", "chan_mod_dims", "three_body_dims", "pp_map",
  * "hh_map", "ph_mod_map", "hp_mod_map", "hpp_map", "phh_map" (u64), "map_<name>" (u64
  * channel,row,column triples in pphh order, <name> as in ccdgpu_map_id), "v_<kind>" (f64, the
- * active-channel blocks concatenated), "sp_energy" (f64), "qn" (i32 SPBasis::indexMap rows).  dtype: 1 = f64, 2 = u64, 4 = i32. */
+ * active-channel blocks concatenated), "sp_energy" (f64, normal ordered), "sp_energy_bare" (f64,
+ * before normal ordering), "qn" (i32 SPBasis::indexMap rows).  dtype: 1 = f64, 2 = u64, 4 = i32. */
 int ccdhost_array(const ccdhost_system *s, const char *name, const void **data,
                   uint64_t *count, int32_t *dtype);
 

@@ -4,12 +4,14 @@ Tolerances (FP64 path): correlation energy per particle within 1e-10 relative of
 reference, T2 within 1e-9 max-abs; stage intermediates within 1e-12 of the oracle relative to
 the chain's largest element.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
-from coupled_cluster_doubles_b200 import CCDGPUError, CCDSolver, solver as solver_mod
-from helpers import SMALL, golden, system_for, t2_sample
-from oracle.oracle import Oracle
+from coupled_cluster_doubles_b200 import CCDGPUError, CCDSolver, _native, solver as solver_mod
+from helpers import SMALL, STRUCT, golden, system_for, t2_sample
+from oracle.oracle import Oracle, fnv1a
 
 pytestmark = pytest.mark.gpu
 
@@ -231,6 +233,41 @@ def test_device_mbpt2_matches_reference(name):
         e2 = sol.mbpt2()
     ref = float(g["scalars"][1])
     assert abs(e2 - ref) <= 1e-12 * abs(ref) + 1e-15, (e2, ref)
+
+
+@pytest.mark.parametrize("name", SMALL + ["eg54_s19"])
+def test_device_reference_energy_and_normal_order(name):
+    """E_ref and the normal-ordered energies computed on the device from the bare energies
+    (SPBasis.cpp:7-40) against the reference's own E_ref and energy dump: bit-exact where the
+    matrix elements are (pairing, electron gas: table lookups and products); within 1e-13 for
+    the Minnesota potential, whose exp/pow come from CUDA and may differ by an ulp."""
+    g = golden(name)
+    with system_for(g) as s, CCDSolver(s) as sol:
+        e_ref, eps = sol.reference_energy(s.array("sp_energy_bare"))
+        host_eps = s.array("sp_energy")
+    ref = float(g["scalars"][0])
+    if g["kind"] == "inf_matter":
+        assert abs(e_ref - ref) <= 1e-13 * abs(ref), (e_ref, ref)
+        np.testing.assert_allclose(eps, host_eps, rtol=0, atol=1e-13 * np.max(np.abs(host_eps)))
+    else:
+        assert e_ref == ref, (e_ref, ref)
+        assert fnv1a(eps) == int(g["struct_hashes"][STRUCT.index("sp_energy")])
+
+
+def test_reference_energy_needs_the_model():
+    """Without ccdgpu_problem.model the call reports UNSUPPORTED instead of guessing."""
+    g = golden("pairing_gp0.5")
+    with system_for(g) as s:
+        class NoModel:
+            pass
+        nm = NoModel()
+        nm.prob = _native.Problem.from_buffer_copy(s.problem.contents)
+        nm.prob.model = None
+        nm.problem = ctypes.pointer(nm.prob)
+        with CCDSolver(nm) as sol:
+            with pytest.raises(CCDGPUError) as ei:
+                sol.reference_energy(s.array("sp_energy_bare"))
+            assert ei.value.status == -7
 
 
 @pytest.mark.parametrize("path", ["fused", "tables"])
