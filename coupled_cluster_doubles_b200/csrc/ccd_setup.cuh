@@ -229,6 +229,128 @@ __global__ void convert_tables_kernel(const ElemRange *__restrict__ ranges, cons
   }
 }
 
+// ---- Remap tables derived on the device (problem without loadMaps tables) ----------------
+// loadMaps (load.cpp:389-532) builds the eight tables from the channel maps alone; the same
+// derivation here needs only the pair lists the solver already holds.  Block sizes first:
+// hsz[k * np + j] = pp of the channel of hole pair (k, j), psz[(a - np) * npart + (b - np)] =
+// hh of the channel of particle pair (a, b) (zero for pairs of channels without amplitudes).
+// One CTA per active channel.
+__global__ void pair_sizes_kernel(const ChanInfo *__restrict__ chans, const int2 *__restrict__ pp_pairs,
+                                  const int2 *__restrict__ hh_pairs, int np, int npart,
+                                  int32_t *__restrict__ hsz, int32_t *__restrict__ psz) {
+  const ChanInfo ch = chans[blockIdx.x];
+  for (int t = threadIdx.x; t < ch.pp; t += blockDim.x) {
+    const int2 ab = pp_pairs[ch.pp_off + t];
+    psz[(int64_t)(ab.x - np) * npart + (ab.y - np)] = ch.hh;
+  }
+  for (int t = threadIdx.x; t < ch.hh; t += blockDim.x) {
+    const int2 ij = hh_pairs[ch.hh_off + t];
+    hsz[(int64_t)ij.x * np + ij.y] = ch.pp;
+  }
+}
+
+// In-place exclusive prefix sum of each row (one CTA of 256 threads per row): block sizes ->
+// offsets of the blocks inside the three-body chains hpp(k) (SPBasis.cpp:181-256) and phh(a)
+// (SPBasis.cpp:443-563), whose blocks follow the partner index in ascending order.
+__global__ void __launch_bounds__(256) row_scan_kernel(int32_t *__restrict__ x, int len) {
+  __shared__ int32_t warp_tot[8];
+  int32_t *row = x + (int64_t)blockIdx.x * len;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int32_t carry = 0;
+  for (int base = 0; base < len; base += 256) {
+    const int k = base + threadIdx.x;
+    const int32_t v = k < len ? row[k] : 0;
+    int32_t sum = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t y = __shfl_up_sync(0xffffffffu, sum, o);
+      if (lane >= o) sum += y;
+    }
+    if (lane == 31) warp_tot[w] = sum;
+    __syncthreads();
+    int32_t before = 0, tile = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      before += q < w ? warp_tot[q] : 0;
+      tile += warp_tot[q];
+    }
+    if (k < len) row[k] = carry + before + sum - v;
+    carry += tile;
+    __syncthreads();
+  }
+}
+
+struct DeriveGeometry {
+  const int64_t *o_h;      // [np+1] hpp chain offsets
+  const int64_t *o_p;      // [npart+1] phh chain offsets
+  const int64_t *o_m;      // [nch+1] phhp chain offsets
+  const int2 *mod_dims;    // [nch] (ph', hp')
+  const int32_t *hblk;     // [np * np] offset of the block of hole j inside hpp(k)
+  const int32_t *pblk;     // [npart * npart] offset of the block of particle b inside phh(a)
+  const int4 *mlook;       // [npart * np] of (particle a, hole i): x, y = modified channel and
+                           // row of (a, i) in its ph' map; z, w = channel and column of (i, a)
+                           // in its hp' map (-1 where the pair is in no active channel)
+  int32_t np, npart;
+};
+
+// The eight tables as int32 flat offsets, from the pair lists (load.cpp:469-526):
+//   iab_j -> hpp(j) at block i, row ab;     jab_i -> hpp(i) at block j, row ab;
+//   a_bij -> phh(a) at block b, column ij;  b_aij -> phh(b) at block a, column ij;
+//   ai_jb, aj_ib, bi_ja, bj_ia -> phhp block of the modified channel of the ph' pair, at
+//   (row of the ph' pair, column of the hp' pair).
+// Range checks and hit counts as for convert_tables_kernel.
+__global__ void derive_tables_kernel(const ElemRange *__restrict__ ranges,
+                                     const ChanInfo *__restrict__ chans,
+                                     const int2 *__restrict__ pp_pairs,
+                                     const int2 *__restrict__ hh_pairs, DeriveGeometry g,
+                                     int64_t n_t, int32_t *__restrict__ flat,
+                                     int32_t *__restrict__ counts, int32_t *err) {
+  const ElemRange rg = ranges[blockIdx.x];
+  const ChanInfo ch = chans[rg.ch];
+  const int np = g.np, npart = g.npart;
+  auto hole_chain = [&](int k, int j, int ab) -> int64_t {
+    const int64_t f = g.o_h[k] + g.hblk[(int64_t)k * np + j] + ab;
+    return f < g.o_h[k + 1] ? f : -1;
+  };
+  auto part_chain = [&](int a, int b, int ij) -> int64_t {
+    const int64_t f = g.o_p[a] + g.pblk[(int64_t)a * npart + b] + ij;
+    return f < g.o_p[a + 1] ? f : -1;
+  };
+  // (x, y): particle-hole pair of the ph' map; (u, v): hole-particle pair of the hp' map.
+  auto ring = [&](int x, int y, int u, int v) -> int64_t {
+    const int4 r = g.mlook[(int64_t)(x - np) * np + y], c = g.mlook[(int64_t)(v - np) * np + u];
+    if (r.x < 0 || r.x != c.z) return -1;
+    const int2 md = g.mod_dims[r.x];
+    if (r.y >= md.x || c.w < 0 || c.w >= md.y) return -1;
+    return g.o_m[r.x] + (int64_t)r.y * md.y + c.w;
+  };
+  for (int64_t e = rg.e0 + threadIdx.x; e < rg.e1; e += blockDim.x) {
+    const int64_t loc = e - ch.t_off;
+    const int ab = (int)(loc / ch.hh), ij = (int)(loc - (int64_t)ab * ch.hh);
+    const int2 pab = pp_pairs[ch.pp_off + ab], pij = hh_pairs[ch.hh_off + ij];
+    const int a = pab.x, b = pab.y, i = pij.x, j = pij.y;
+    int64_t f[8];
+    f[0] = hole_chain(j, i, ab);
+    f[1] = hole_chain(i, j, ab);
+    f[2] = part_chain(a - np, b - np, ij);
+    f[3] = part_chain(b - np, a - np, ij);
+    f[4] = ring(a, i, j, b);
+    f[5] = ring(a, j, i, b);
+    f[6] = ring(b, i, j, a);
+    f[7] = ring(b, j, i, a);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      int64_t x = f[k];
+      if (x < 0 || x >= n_t) {
+        atomicOr(err, kErrBadIndex);
+        x = 0;
+      }
+      flat[(int64_t)k * n_t + e] = (int32_t)x;
+      if (k <= 4) atomicAdd(&counts[(int64_t)k * n_t + x], 1);
+    }
+  }
+}
+
 // V_hpph' blocks (hp' x ph', load.cpp:275-296) -> transposed (ph' x hp') for the ring kernels'
 // outer-product loops; one CTA per modified channel.
 __global__ void transpose_hpph_kernel(const ModInfo *__restrict__ mods,

@@ -473,8 +473,11 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   if ((!on_the_fly && !P->v_pppp) || !P->v_hhpp || !P->v_hhhh || !P->v_hpph_mod ||
       !P->v_hphp_mod)
     return CCDGPU_ERR_INVALID_ARGUMENT;
-  for (int k = 0; k < 8; k++)
-    if (!P->maps[k]) return CCDGPU_ERR_INVALID_ARGUMENT;
+  // No loadMaps tables at all: the library derives them on the device from the channel maps.
+  int n_maps = 0;
+  for (int k = 0; k < 8; k++) n_maps += P->maps[k] ? 1 : 0;
+  if (n_maps != 0 && n_maps != 8) return CCDGPU_ERR_INVALID_ARGUMENT;
+  const bool derive_tables = n_maps == 0;
 
   std::vector<int64_t> o_t(nch + 1, 0), o_m(nch + 1, 0);
   for (uint64_t c = 0; c < nch; c++) {
@@ -773,7 +776,41 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   int32_t *counts = nullptr;
   int2 *d_vrows = nullptr, *d_mod_dims = nullptr;
   int64_t *d_vraw_off = nullptr, *d_o_m = nullptr;
-  sc.add(&vraw, vraw_tot); sc.add(&hhpp_raw, n_t); sc.add(&hpph_raw, h->n_m); sc.add(&raw_idx, (size_t)8 * n_t);
+  // Derived tables: per-pair block offsets and the modified-channel lookup of (particle, hole)
+  // pairs, built here from the ph' / hp' maps (O(npart * np)).
+  int32_t *d_hblk = nullptr, *d_pblk = nullptr;
+  int4 *d_mlook = nullptr;
+  std::vector<int4> mlook;
+  if (derive_tables) {
+    const uint64_t npart = nsp - np;
+    mlook.assign(npart * np, make_int4(-1, -1, -1, -1));
+    for (uint64_t c = 0; c < nch; c++) {
+      const uint64_t ph = MD[c].ph, hp = MD[c].hp;
+      if (!ph || !hp) continue;
+      const ccdgpu_pair *phm = P->chan_mod_maps[c].ph, *hpm = P->chan_mod_maps[c].hp;
+      if (!phm || !hpm) return CCDGPU_ERR_INVALID_ARGUMENT;
+      for (uint64_t k = 0; k < ph; k++) {
+        const uint64_t a = phm[k].p, i = phm[k].q;
+        if (a < np || a >= nsp || i >= np) return CCDGPU_ERR_BAD_TABLE;
+        int4 &m = mlook[(a - np) * np + i];
+        if (m.x >= 0) return CCDGPU_ERR_BAD_TABLE;
+        m.x = (int)c; m.y = (int)k;
+      }
+      for (uint64_t k = 0; k < hp; k++) {
+        const uint64_t i = hpm[k].p, a = hpm[k].q;
+        if (i >= np || a < np || a >= nsp) return CCDGPU_ERR_BAD_TABLE;
+        int4 &m = mlook[(a - np) * np + i];
+        if (m.z >= 0) return CCDGPU_ERR_BAD_TABLE;
+        m.z = (int)c; m.w = (int)k;
+      }
+    }
+    sc.add(&d_hblk, np * np);
+    sc.add(&d_pblk, npart * npart);
+    sc.add(&d_mlook, mlook.size());
+  } else {
+    sc.add(&raw_idx, (size_t)8 * n_t);
+  }
+  sc.add(&vraw, vraw_tot); sc.add(&hhpp_raw, n_t); sc.add(&hpph_raw, h->n_m);
   sc.add(&counts, (size_t)5 * n_t); sc.add(&d_vrows, vrows.size()); 
   sc.add(&d_vraw_off, vraw_off.size()); sc.add(&d_mod_dims, mod_dims.size()); sc.add(&d_o_m, o_m.size());
   // The model on the device (on-the-fly V, E_ref and normal ordering): quantum numbers and
@@ -859,7 +896,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
       if (!on_the_fly) { sp.push_back(P->v_pppp[c]); np2.push_back((int64_t)a.pp * a.pp); }
       sx.push_back(P->v_hhpp[c]); nx.push_back((int64_t)a.pp * a.hh);
       sh.push_back(P->v_hhhh[c]); nh.push_back((int64_t)a.hh * a.hh);
-      for (int k = 0; k < 8; k++) {
+      for (int k = 0; k < 8 && !derive_tables; k++) {
         if (!P->maps[k][c]) return CCDGPU_ERR_INVALID_ARGUMENT;
         sm[k].push_back(P->maps[k][c]);
       }
@@ -869,8 +906,9 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     TRY(upload_runs(h, hhpp_raw, sx, nx));
     TRY(upload_runs(h, h->v_hhhh, sh, nh));
     static_assert(sizeof(RawIndex) == sizeof(ccdgpu_chain_index), "ChainIndex layout");
-    for (int k = 0; k < 8; k++)
+    for (int k = 0; k < 8 && !derive_tables; k++)
       TRY(upload_runs(h, reinterpret_cast<ccdgpu_chain_index *>(raw_idx) + (size_t)k * n_t, sm[k], nm));
+    if (derive_tables) TRY(put(d_mlook, mlook));
     TRY(upload_runs(h, hpph_raw, src_hpph, cnt_hpph));
     TRY(upload_runs(h, h->v_hphp, src_hphp, cnt_hphp));
     if (h->have_3body) {
@@ -898,9 +936,24 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   if (h->n_ranges) {
     transpose_hhpp_kernel<<<h->n_ranges, 256, 0, h->s0>>>(h->ranges, h->chans, hhpp_raw, h->v_pphh);
     CK(cudaGetLastError());
-    TableGeometry geo{h->o_h, h->o_p, d_o_m, d_mod_dims, nch, np, h->npart};
-    convert_tables_kernel<<<h->n_ranges, 256, 0, h->s0>>>(h->ranges, raw_idx, n_t, geo, h->flat,
-                                                          counts, h->err);
+    if (derive_tables) {
+      pair_sizes_kernel<<<(unsigned)chans.size(), 256, 0, h->s0>>>(
+          h->chans, h->pp_pairs, h->hh_pairs, (int)np, (int)h->npart, d_hblk, d_pblk);
+      CK(cudaGetLastError());
+      row_scan_kernel<<<(unsigned)np, 256, 0, h->s0>>>(d_hblk, (int)np);
+      CK(cudaGetLastError());
+      row_scan_kernel<<<(unsigned)h->npart, 256, 0, h->s0>>>(d_pblk, (int)h->npart);
+      CK(cudaGetLastError());
+      DeriveGeometry dg{h->o_h, h->o_p, d_o_m, d_mod_dims, d_hblk, d_pblk, d_mlook,
+                        (int32_t)np, (int32_t)h->npart};
+      derive_tables_kernel<<<h->n_ranges, 256, 0, h->s0>>>(h->ranges, h->chans, h->pp_pairs,
+                                                           h->hh_pairs, dg, n_t, h->flat, counts,
+                                                           h->err);
+    } else {
+      TableGeometry geo{h->o_h, h->o_p, d_o_m, d_mod_dims, nch, np, h->npart};
+      convert_tables_kernel<<<h->n_ranges, 256, 0, h->s0>>>(h->ranges, raw_idx, n_t, geo,
+                                                            h->flat, counts, h->err);
+    }
     CK(cudaGetLastError());
     const int nb = (int)std::min<int64_t>(ceil_div(5 * n_t, 256), 148 * 32);
     check_counts_kernel<<<std::max(nb, 1), 256, 0, h->s0>>>(counts, 5 * n_t, h->err);

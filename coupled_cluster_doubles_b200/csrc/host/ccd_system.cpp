@@ -216,7 +216,9 @@ struct ccdhost_system {
 
 namespace {
 
-int finish(ccdhost_system *s, int32_t load_v_pppp) {
+int finish(ccdhost_system *s, int32_t flags) {
+  const bool load_v_pppp = flags & CCDHOST_LOAD_V_PPPP;
+  const bool tables = !(flags & CCDHOST_NO_TABLES);
   Model &m = s->m;
   const uint64_t nsp = m.nsp, np = m.np, nch = m.nchan;
 
@@ -327,7 +329,8 @@ int finish(ccdhost_system *s, int32_t load_v_pppp) {
   // Three-body maps (SPBasis.cpp:181-256, 443-563): hpp(k) = {(j,a,b): (a,b) in pp(ch(k,j))},
   // phh(a) = {(b,i,j): (i,j) in hh(ch(a,b))}, both sorted lexicographically.
   s->tdims.assign(nsp, ccdgpu_three_body_dims{0, 0});
-  std::vector<uint64_t> hpp_blk(np * np), phh_blk((nsp - np) * (nsp - np));
+  // Block offsets inside hpp(k) / phh(a), kept for the remap tables.
+  std::vector<uint64_t> hpp_blk(np * np), phh_blk(tables ? (nsp - np) * (nsp - np) : 0);
   s->hpp_off_map.assign(np + 1, 0);
   for (uint64_t k = 0; k < np; k++) {
     uint64_t n = 0;
@@ -343,7 +346,7 @@ int finish(ccdhost_system *s, int32_t load_v_pppp) {
   for (uint64_t a = np; a < nsp; a++) {
     uint64_t n = 0;
     for (uint64_t b = np; b < nsp; b++) {
-      phh_blk[(a - np) * npart + (b - np)] = n;
+      if (tables) phh_blk[(a - np) * npart + (b - np)] = n;
       n += s->dims[chan[a * nsp + b]].hh;
     }
     s->tdims[a].phh = n;
@@ -447,15 +450,16 @@ int finish(ccdhost_system *s, int32_t load_v_pppp) {
   for (uint64_t a = 0; a < npart; a++)
     if (s->tdims[a + np].phh) s->vptr[6][a] = &s->v[6][s->phh_off_map[a]];
 
-  // Remap tables (load.cpp:469-526), from block offsets instead of hash tables.
+  // Remap tables (load.cpp:469-526), from block offsets instead of hash tables; skipped with
+  // CCDHOST_NO_TABLES (the solver library then derives them on the device).
   std::vector<uint64_t> o_t(nch + 1, 0);
   for (uint64_t c = 0; c < nch; c++) o_t[c + 1] = o_t[c] + s->dims[c].pp * s->dims[c].hh;
   for (int k = 0; k < 8; k++) {
-    s->tab[k].resize(o_t[nch]);
+    s->tab[k].resize(tables ? o_t[nch] : 0);
     s->tabptr[k].assign(nch, nullptr);
   }
 #pragma omp parallel for schedule(dynamic)
-  for (int64_t ci = 0; ci < (int64_t)nch; ci++) {
+  for (int64_t ci = 0; ci < (tables ? (int64_t)nch : 0); ci++) {
     const uint64_t c = ci, pp = s->dims[c].pp, hh = s->dims[c].hh;
     for (uint64_t AB = 0; AB < pp; AB++)
       for (uint64_t IJ = 0; IJ < hh; IJ++) {
@@ -472,7 +476,7 @@ int finish(ccdhost_system *s, int32_t load_v_pppp) {
         s->tab[7][e] = {mchan[b * nsp + j], mpos[b * nsp + j], mpos[i * nsp + a]};
       }
   }
-  for (int k = 0; k < 8; k++)
+  for (int k = 0; k < 8 && tables; k++)
     for (uint64_t c = 0; c < nch; c++)
       if (o_t[c + 1] > o_t[c]) s->tabptr[k][c] = &s->tab[k][o_t[c]];
 
@@ -516,7 +520,7 @@ int finish(ccdhost_system *s, int32_t load_v_pppp) {
   P.v_pppp = load_v_pppp ? s->vptr[2].data() : nullptr;
   P.v_hpph_mod = s->vptr[3].data(); P.v_hphp_mod = s->vptr[4].data();
   P.v_h_hpp = s->vptr[5].data(); P.v_phh_p = s->vptr[6].data();
-  for (int k = 0; k < 8; k++) P.maps[k] = s->tabptr[k].data();
+  for (int k = 0; k < 8; k++) P.maps[k] = tables ? s->tabptr[k].data() : nullptr;
   P.model = &s->model;
   return CCDGPU_OK;
 }
@@ -526,7 +530,7 @@ int finish(ccdhost_system *s, int32_t load_v_pppp) {
 extern "C" {
 
 int ccdhost_build_pairing(double xi, double g, uint64_t n_pair_states, uint64_t n_particles,
-                          int32_t load_v_pppp, ccdhost_system **out) {
+                          int32_t flags, ccdhost_system **out) {
   if (!out || n_pair_states == 0 || n_particles == 0 || n_particles >= 2 * n_pair_states)
     return CCDGPU_ERR_INVALID_ARGUMENT;
   ccdhost_system *s = new (std::nothrow) ccdhost_system();
@@ -542,14 +546,14 @@ int ccdhost_build_pairing(double xi, double g, uint64_t n_pair_states, uint64_t 
   }
   m.eps.resize(m.nsp);
   for (uint64_t i = 0; i < m.nsp; i++) m.eps[i] = (m.qn[i * 2] - 1.0) * xi;
-  int rc = finish(s, load_v_pppp);
+  int rc = finish(s, flags);
   if (rc) { delete s; return rc; }
   *out = s;
   return CCDGPU_OK;
 }
 
 int ccdhost_build_inf_matter(double density, int32_t tz_max, uint64_t n_shells,
-                             uint64_t n_particle_shells, int32_t load_v_pppp,
+                             uint64_t n_particle_shells, int32_t flags,
                              ccdhost_system **out) {
   if (!out || density <= 0 || (tz_max != 1 && tz_max != 2) || n_shells == 0 ||
       n_particle_shells == 0 || n_particle_shells >= n_shells)
@@ -571,14 +575,14 @@ int ccdhost_build_inf_matter(double density, int32_t tz_max, uint64_t n_shells,
     const int32_t *r = m.q(i);
     m.eps[i] = (prefactor * 4 * M_PI * M_PI / (box * box)) * (r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
   }
-  int rc = finish(s, load_v_pppp);
+  int rc = finish(s, flags);
   if (rc) { delete s; return rc; }
   *out = s;
   return CCDGPU_OK;
 }
 
 int ccdhost_build_electron_gas(double r_s, uint64_t n_shells, uint64_t n_particle_shells,
-                               int32_t load_v_pppp, ccdhost_system **out) {
+                               int32_t flags, ccdhost_system **out) {
   if (!out || r_s <= 0 || n_shells == 0 || n_particle_shells == 0 ||
       n_particle_shells >= n_shells)
     return CCDGPU_ERR_INVALID_ARGUMENT;
@@ -605,7 +609,7 @@ int ccdhost_build_electron_gas(double r_s, uint64_t n_shells, uint64_t n_particl
     const int32_t *r = m.q(i);
     m.eps[i] = (prefactor * 4 * M_PI * M_PI / (m.L * m.L)) * (r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
   }
-  int rc = finish(s, load_v_pppp);
+  int rc = finish(s, flags);
   if (rc) { delete s; return rc; }
   *out = s;
   return CCDGPU_OK;

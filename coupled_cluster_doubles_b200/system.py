@@ -3,7 +3,8 @@
 `System` wraps one ccdhost_system built by libccdhost.so.  Its `.problem` pointer is the
 `ccdgpu_problem` that the solver consumes; `.array(name)` exposes the builder's flat arrays
 (channel dims, maps, remap tables, V slabs) for tests.  Constructors mirror the reference CLI
-(parse.cpp:131-244):
+(parse.cpp:131-244); `tables=False` leaves the eight remap tables to the
+device (ccdgpu_create derives them):
 
     System.pairing(xi=1.0, g=0.5, n_pair_states=4, n_particles=4)      # --pairing -x -g -l -n
     System.inf_matter(density=0.08, tz_max=1, n_shells=4, n_particle_shells=2)  # --infMatter
@@ -20,6 +21,15 @@ _DT = {1: np.float64, 2: np.uint64, 4: np.int32}
 
 class BuildError(RuntimeError):
     pass
+
+
+LOAD_V_PPPP, NO_TABLES = 1, 2  # ccdhost_flags
+
+
+def _flags(load_v_pppp, tables):
+    """Builder flags: V_pppp built on the host or not; remap tables built on the host, or left
+    to ccdgpu_create, which then derives them on the device."""
+    return (LOAD_V_PPPP if load_v_pppp else 0) | (0 if tables else NO_TABLES)
 
 
 class System:
@@ -46,25 +56,28 @@ class System:
         return System(h, kind, params)
 
     @classmethod
-    def pairing(cls, xi=1.0, g=0.5, n_pair_states=4, n_particles=4, load_v_pppp=True):
+    def pairing(cls, xi=1.0, g=0.5, n_pair_states=4, n_particles=4, load_v_pppp=True,
+                tables=True):
         return cls._build("ccdhost_build_pairing", float(xi), float(g), int(n_pair_states),
-                          int(n_particles), int(bool(load_v_pppp)), kind="pairing",
+                          int(n_particles), _flags(load_v_pppp, tables), kind="pairing",
                           params=dict(xi=xi, g=g, n_pair_states=n_pair_states,
                                       n_particles=n_particles))
 
     @classmethod
     def inf_matter(cls, density=0.08, tz_max=1, n_shells=4, n_particle_shells=2,
-                   load_v_pppp=True):
+                   load_v_pppp=True, tables=True):
         return cls._build("ccdhost_build_inf_matter", float(density), int(tz_max),
-                          int(n_shells), int(n_particle_shells), int(bool(load_v_pppp)),
+                          int(n_shells), int(n_particle_shells), _flags(load_v_pppp, tables),
                           kind="inf_matter",
                           params=dict(density=density, tz_max=tz_max, n_shells=n_shells,
                                       n_particle_shells=n_particle_shells))
 
     @classmethod
-    def electron_gas(cls, r_s=0.5, n_shells=4, n_particle_shells=2, load_v_pppp=True):
+    def electron_gas(cls, r_s=0.5, n_shells=4, n_particle_shells=2, load_v_pppp=True,
+                     tables=True):
         return cls._build("ccdhost_build_electron_gas", float(r_s), int(n_shells),
-                          int(n_particle_shells), int(bool(load_v_pppp)), kind="electron_gas",
+                          int(n_particle_shells), _flags(load_v_pppp, tables),
+                          kind="electron_gas",
                           params=dict(r_s=r_s, n_shells=n_shells,
                                       n_particle_shells=n_particle_shells))
 

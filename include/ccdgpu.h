@@ -85,7 +85,10 @@ typedef struct ccdgpu_problem {
   const double *const *v_hphp_mod;  /* [n_channels] hp' x hp' (vnn_hpph_hphp_mod) */
   const double *const *v_h_hpp;     /* [n_particles] 1 x hpp  (vnn_h_hpp); NULL allowed (fused path) */
   const double *const *v_phh_p;     /* [n_sp - n_particles] phh x 1 (vnn_phh_p); NULL allowed */
-  const ccdgpu_chain_index *const *maps[8]; /* [n_channels] pp x hh blocks, ccdgpu_map_id order */
+  const ccdgpu_chain_index *const *maps[8]; /* [n_channels] pp x hh blocks, ccdgpu_map_id order
+                                               (loadMaps, load.cpp:389-532); all eight NULL:
+                                               derived on the device from chan_maps (pp, hh),
+                                               chan_mod_maps (ph, hp) and three_body_dims */
   const ccdgpu_model *model;        /* optional, required for CCDGPU_V_ON_THE_FLY */
 } ccdgpu_problem;
 

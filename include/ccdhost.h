@@ -30,16 +30,23 @@ extern "C" {
 
 typedef struct ccdhost_system ccdhost_system;
 
+/* Build flags (the last int32 argument of the ccdhost_build_* functions). */
+enum ccdhost_flags {
+  CCDHOST_LOAD_V_PPPP = 1, /* build and pass V_pppp (off: the solver generates it, saveMemory) */
+  CCDHOST_NO_TABLES = 2    /* build no loadMaps remap tables: ccdgpu_problem.maps[] are NULL
+                              and ccdgpu_create derives the tables on the device */
+};
+
 /* --pairing -l n_pair_states -n n_particles -x xi -g g  (parse.cpp:232-234) */
 int ccdhost_build_pairing(double xi, double g, uint64_t n_pair_states, uint64_t n_particles,
-                          int32_t load_v_pppp, ccdhost_system **out);
+                          int32_t flags, ccdhost_system **out);
 /* --infMatter -d density -z tz_max -s n_shells -p n_particle_shells  (parse.cpp:235-237) */
 int ccdhost_build_inf_matter(double density, int32_t tz_max, uint64_t n_shells,
-                             uint64_t n_particle_shells, int32_t load_v_pppp,
+                             uint64_t n_particle_shells, int32_t flags,
                              ccdhost_system **out);
 /* --electronGas -r r_s -s n_shells -p n_particle_shells  (parse.cpp:238-240) */
 int ccdhost_build_electron_gas(double r_s, uint64_t n_shells, uint64_t n_particle_shells,
-                               int32_t load_v_pppp, ccdhost_system **out);
+                               int32_t flags, ccdhost_system **out);
 void ccdhost_free(ccdhost_system *s);
 
 const ccdgpu_problem *ccdhost_problem(const ccdhost_system *s);

@@ -37,6 +37,24 @@ def test_builder_without_v_pppp_keeps_everything_else():
             assert fnv1a(s.array(n)) == int(g["map_hashes"][k]), n
 
 
+@pytest.mark.parametrize("name", ["pairing_gp0.5", "pnm14_s4", "eg14_s19"])
+def test_builder_without_tables_keeps_everything_else(name):
+    """CCDHOST_NO_TABLES: no remap tables and NULL ccdgpu_problem.maps (the solver derives
+    them on the device); every other input stays bit-identical to the reference's."""
+    from coupled_cluster_doubles_b200 import System
+    g = golden(name)
+    with getattr(System, g["kind"])(**g["params"], tables=False) as s:
+        p = s.problem.contents
+        assert all(not p.maps[k] for k in range(8))
+        assert s.reference_energy == float(g["scalars"][0])
+        for n in MAPS:
+            assert s.array(n).size == 0, n
+        for k, n in enumerate(STRUCT):
+            assert fnv1a(s.array(n)) == int(g["struct_hashes"][k]), n
+        for k, n in enumerate(VKINDS):
+            assert fnv1a(s.array(n)) == int(g["v_hashes"][k]), n
+
+
 @pytest.mark.parametrize("args", [dict(xi=1.0, g=0.5, n_pair_states=4, n_particles=8),
                                   dict(xi=1.0, g=0.5, n_pair_states=0, n_particles=0)])
 def test_builder_rejects_bad_pairing_input(args):

@@ -1,0 +1,48 @@
+"""Remap tables derived on the device.
+
+A problem built without the eight loadMaps tables (load.cpp:389-532; ccdgpu_problem.maps all
+NULL) makes ccdgpu_create derive them from the channel maps, as loadMaps does.  The flat
+tables must equal the converted host tables entry for entry, so every solve through them is
+bit-identical to the solve through the host's tables: same iteration count, same energy
+history, same amplitudes.
+"""
+import numpy as np
+import pytest
+
+from coupled_cluster_doubles_b200 import CCDSolver, System
+from helpers import SMALL, golden, system_for
+
+pytestmark = pytest.mark.gpu
+
+
+def _no_tables(g, load_v_pppp=True):
+    return getattr(System, g["kind"])(**g["params"], load_v_pppp=load_v_pppp, tables=False)
+
+
+def _same_solve(a, b, g):
+    ra = a.solve(tol=g["tol"], max_iters=100, mixing=0.5)
+    rb = b.solve(tol=g["tol"], max_iters=100, mixing=0.5)
+    assert ra.iterations == rb.iterations
+    np.testing.assert_array_equal(a.energy_history(), b.energy_history())
+    np.testing.assert_array_equal(a.t2(), b.t2())
+    return ra
+
+
+@pytest.mark.parametrize("path", ["fused", "tables"])
+@pytest.mark.parametrize("name", SMALL + ["eg54_s19"])
+def test_derived_tables_solve_bit_identical(name, path):
+    g = golden(name)
+    with system_for(g) as s1, _no_tables(g) as s2, \
+            CCDSolver(s1, path=path) as a, CCDSolver(s2, path=path) as b:
+        r = _same_solve(a, b, g)
+        assert abs(r.e_corr - g["energies"][-1]) <= 1e-10 * abs(g["energies"][-1]) + 1e-14
+
+
+def test_derived_tables_mixed_precision_on_the_fly_v():
+    """Nothing but the channel maps, dimensions, energies and model from the host: V_pppp is
+    generated and the tables derived on the device."""
+    g = golden("eg14_s19")
+    with system_for(g, load_v_pppp=False) as s1, _no_tables(g, load_v_pppp=False) as s2, \
+            CCDSolver(s1, precision="mixed_bf16", v_mode="on_the_fly") as a, \
+            CCDSolver(s2, precision="mixed_bf16", v_mode="on_the_fly") as b:
+        _same_solve(a, b, g)
