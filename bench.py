@@ -324,21 +324,30 @@ def main():
     n_t2 = solvers[arms[0]].n_t2
 
     # e2e (headline arm): the public API from host buffers, every step: create (H2D upload)
-    # + solve + T2 read-back.
+    # + solve + T2 read-back.  The problem carries no loadMaps tables: create derives them on
+    # the device, as a caller that skips loadMaps would have it.
     host_t2 = np.empty(n_t2)
     e2e_secs, e2e_iters = 0.0, 0
-    h2d = _problem_bytes(system, with_v_pppp=args.v_mode == "stored")
+    system_e2e = getattr(System, kind)(**params, load_v_pppp=args.v_mode == "stored",
+                                       tables=False)
+    h2d = _problem_bytes(system_e2e, with_v_pppp=args.v_mode == "stored", with_tables=False)
+    phase_s = np.zeros(4)  # create, solve (graph capture included), T2 read-back, destroy
     for k in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        s2 = CCDSolver(system, device=local, path=args.path, precision=PRECISIONS[arms[0]],
+        s2 = CCDSolver(system_e2e, device=local, path=args.path, precision=PRECISIONS[arms[0]],
                        v_mode=args.v_mode, device_loop=not args.no_device_loop)
+        ta = time.perf_counter()
         r2 = s2.solve(tol=tol, max_iters=100, mixing=0.5)
+        tb = time.perf_counter()
         s2.t2(host_t2)
+        tc = time.perf_counter()
         s2.close()
         t1 = time.perf_counter()
         if k >= args.warmup:
             e2e_secs += t1 - t0
             e2e_iters += r2.iterations
+            phase_s += np.array([ta - t0, tb - ta, tc - tb, t1 - tc])
+    system_e2e.close()
     e2e_secs_max, e2e_iters_all = combine_ranks(e2e_secs, e2e_iters, f"cuda:{local}", world)
 
     if rank == 0:
@@ -430,7 +439,10 @@ def main():
             "shared_kernels_alone": shared,
             "e2e": {"value": e2e_iters_all / e2e_secs_max, "unit": "iter/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * n_t2,
-                    "what": "ccdgpu_create from host buffers + ccdgpu_solve + ccdgpu_get_t2"},
+                    "what": "ccdgpu_create from host buffers (remap tables derived on the "
+                            "device) + ccdgpu_solve + ccdgpu_get_t2",
+                    "rank0_ms_per_step": dict(zip(["create", "solve", "get_t2", "destroy"],
+                                                  (1e3 * phase_s / args.steps).round(3).tolist()))},
             "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved,
                          "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "peak_source": peak_kind,
@@ -554,11 +566,12 @@ def run_batch(args):
         s.close()
 
 
-def _problem_bytes(system, with_v_pppp=True):
+def _problem_bytes(system, with_v_pppp=True, with_tables=True):
     """Bytes ccdgpu_create copies host -> device for this system: V blocks in their reference
     layouts (V_pppp, V_hhpp, V_hhhh of amplitude-carrying channels, both modified-channel V,
-    the three-body V), the eight ChainIndex tables (24 bytes per entry), the energies and the
-    O(sum pp) pair metadata."""
+    the three-body V), the eight ChainIndex tables (24 bytes per entry) or, without them, the
+    16-byte modified-pair lookup per (particle, hole), the energies and the O(sum pp) pair
+    metadata."""
     import numpy as np
     d = system.chan_dims()
     act = (d[:, 0] > 0) & (d[:, 1] > 0)
@@ -572,7 +585,9 @@ def _problem_bytes(system, with_v_pppp=True):
                 (ph * hp).sum() + (hp * hp).sum())
     v += 8 * 2 * n_t
     meta = 24 * int(pp.sum()) + 16 * int(hh.sum()) + 8 * system.n_sp
-    return v + 24 * 8 * n_t + meta
+    npart = system.n_sp - system.n_particles
+    tables = 24 * 8 * n_t if with_tables else 16 * npart * system.n_particles
+    return v + tables + meta
 
 
 def _cpu_baseline(cfg):

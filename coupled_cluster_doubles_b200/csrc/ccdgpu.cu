@@ -17,6 +17,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -219,17 +220,88 @@ struct Arena {
   }
 };
 
+// Process-wide pinned staging for large host -> device uploads: two page-locked buffers of
+// kStageChunk bytes, allocated on first use and kept until the process exits.  A copy from
+// pageable memory is bounced by the driver through small internal buffers at a fraction of
+// the link bandwidth; here host threads fill one pinned buffer while the copy engine drains
+// the other.  Creates on other threads that find the buffers busy copy directly.
+constexpr size_t kStageChunk = size_t(16) << 20;
+constexpr size_t kStageMin = size_t(1) << 20;  // smaller copies go direct
+
+struct Staging {
+  std::mutex mu;
+  char *buf = nullptr;  // 2 * kStageChunk, cudaHostAllocPortable
+  bool failed = false;
+};
+
+Staging &staging() {
+  static Staging s;
+  return s;
+}
+
+int copy_to_device(ccdgpu_handle *h, void *dst, const void *src, size_t bytes) {
+  Staging &S = staging();
+  std::unique_lock<std::mutex> lock(S.mu, std::defer_lock);
+  if (bytes >= kStageMin && lock.try_lock()) {
+    if (!S.buf && !S.failed &&
+        cudaHostAlloc(reinterpret_cast<void **>(&S.buf), 2 * kStageChunk,
+                      cudaHostAllocPortable) != cudaSuccess) {
+      (void)cudaGetLastError();
+      S.buf = nullptr;
+      S.failed = true;
+    }
+    if (S.buf) {
+      cudaEvent_t ev[2] = {nullptr, nullptr};
+      bool pending[2] = {false, false};
+      cudaError_t e = cudaSuccess;
+      for (int k = 0; k < 2 && e == cudaSuccess; k++)
+        e = cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming);
+      const char *in = static_cast<const char *>(src);
+      char *out = static_cast<char *>(dst);
+      for (size_t off = 0, k = 0; off < bytes && e == cudaSuccess; off += kStageChunk, k ^= 1) {
+        const size_t n = std::min(kStageChunk, bytes - off);
+        char *stage = S.buf + k * kStageChunk;
+        if (pending[k] && (e = cudaEventSynchronize(ev[k])) != cudaSuccess) break;
+        const int parts = std::max(1, std::min(omp_get_max_threads(), 16));
+        const size_t part = (n + parts - 1) / parts;
+#pragma omp parallel for num_threads(parts) schedule(static)
+        for (int t = 0; t < parts; t++) {
+          const size_t b = std::min(n, (size_t)t * part), l = std::min(n - b, part);
+          if (l) std::memcpy(stage + b, in + off + b, l);
+        }
+        e = cudaMemcpyAsync(out + off, stage, n, cudaMemcpyHostToDevice, h->s0);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[k], h->s0);
+        pending[k] = e == cudaSuccess;
+      }
+      // The buffers are free for the next upload only once their copies have completed.
+      for (int k = 0; k < 2; k++) {
+        if (pending[k]) {
+          const cudaError_t w = cudaEventSynchronize(ev[k]);
+          if (e == cudaSuccess) e = w;
+        }
+        if (ev[k]) cudaEventDestroy(ev[k]);
+      }
+      if (e != cudaSuccess) {
+        (void)cudaStreamSynchronize(h->s0);
+        (void)cudaGetLastError();
+        return e == cudaErrorMemoryAllocation ? CCDGPU_ERR_OUT_OF_MEMORY : CCDGPU_ERR_CUDA;
+      }
+      return CCDGPU_OK;
+    }
+  }
+  CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->s0));
+  return CCDGPU_OK;
+}
+
 // Copies per-channel host blocks (block k of `count[k]` elements at src[k]) to consecutive
-// device positions, one cudaMemcpy per run of blocks that are adjacent in host memory.
+// device positions, one copy per run of blocks that are adjacent in host memory.
 template <typename T>
 int upload_runs(ccdgpu_handle *h, T *dst, const std::vector<const T *> &src,
                 const std::vector<int64_t> &count) {
   const T *run_src = nullptr;
   int64_t run_len = 0, pos = 0, run_dst = 0;
   auto flush = [&]() -> int {
-    if (run_len) CK(cudaMemcpyAsync(dst + run_dst, run_src, run_len * sizeof(T),
-                                    cudaMemcpyHostToDevice, h->s0));
-    return CCDGPU_OK;
+    return run_len ? copy_to_device(h, dst + run_dst, run_src, run_len * sizeof(T)) : CCDGPU_OK;
   };
   for (size_t k = 0; k < src.size(); k++) {
     if (!count[k]) continue;
@@ -865,8 +937,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   TRY(sc.commit(h));
 
   auto put = [&](auto *dst, const auto &v) -> int {
-    if (!v.empty()) CK(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice, h->s0));
-    return CCDGPU_OK;
+    return v.empty() ? CCDGPU_OK : copy_to_device(h, dst, v.data(), v.size() * sizeof(v[0]));
   };
   TRY(put(h->chans, chans)); TRY(put(h->mods, mods));
   TRY(put(h->hh_tiles, hh_tiles)); TRY(put(h->hh_red, hh_red)); TRY(put(h->ranges, ranges)); TRY(put(h->pranges, pranges));
