@@ -122,7 +122,7 @@ GPU_SYMBOLS = [
     "ccdgpu_energy_history", "ccdgpu_stream", "ccdgpu_calc_channel_t2diff_pphh_noalloc",
     "ccdgpu_trace_arm", "ccdgpu_trace_read", "ccdgpu_solve_batch", "ccdgpu_set_schedule",
     "ccdgpu_get_schedule", "ccdgpu_autotune", "ccdgpu_ladder_profile", "ccdgpu_kernel_profile",
-    "ccdgpu_mbpt2", "ccdgpu_reference_energy",
+    "ccdgpu_mbpt2", "ccdgpu_reference_energy", "ccdgpu_release_cached_memory",
 ]
 
 
@@ -172,6 +172,8 @@ def gpu_lib():
         lib.ccdgpu_kernel_profile.argtypes = [vp, c_i32, P(c_dbl), P(c_dbl), P(c_dbl)]
         lib.ccdgpu_mbpt2.argtypes = [vp, c_i32, P(c_dbl)]
         lib.ccdgpu_reference_energy.argtypes = [vp, P(c_dbl), P(c_dbl), P(c_dbl)]
+        lib.ccdgpu_release_cached_memory.argtypes = []
+        lib.ccdgpu_release_cached_memory.restype = None
         lib.ccdgpu_trace_read.argtypes = [vp, P(c_u64), P(c_u64), c_i32]
         _gpu = lib
     return _gpu

@@ -114,6 +114,7 @@ struct ccdgpu_handle {
   int64_t n_list = 0;  // entries of the one-body segment lists
   ccdgpu_schedule schedule{};
   void *tile_mem = nullptr;
+  size_t tile_bytes = 0;
   RedItem *red_fp = nullptr, *red_tc = nullptr;  // split-K reduction items
   int32_t *tc_cta_off = nullptr;  // tensor-core ladder: tile range of each persistent CTA
   int tc_grid = 0;
@@ -175,17 +176,151 @@ int find_pair(const ccdgpu_pair *list, int64_t n, uint64_t p, uint64_t q) {
   return -1;
 }
 
+// Process-wide cache of device blocks given back by destroyed handles, by create's scratch
+// and by schedule changes, reused by later allocations on the same device instead of
+// cudaMalloc / cudaFree (hundreds of microseconds each; cudaFree also waits for the whole
+// device).  Holds at most kCacheMax bytes; ccdgpu_release_cached_memory returns them.
+constexpr size_t kCacheMax = size_t(16) << 30;
+
+struct CachedBlock {
+  int dev;
+  void *p;
+  size_t bytes;
+};
+
+struct BlockCache {
+  std::mutex mu;
+  std::vector<CachedBlock> blocks;
+  size_t total = 0;
+};
+
+BlockCache &block_cache() {
+  static BlockCache c;
+  return c;
+}
+
+// Frees the cached blocks of device `dev` (all devices for dev < 0).
+void release_cache(int dev) {
+  BlockCache &C = block_cache();
+  std::vector<CachedBlock> drop;
+  {
+    std::lock_guard<std::mutex> lock(C.mu);
+    std::vector<CachedBlock> keep;
+    for (const CachedBlock &b : C.blocks) (dev < 0 || b.dev == dev ? drop : keep).push_back(b);
+    C.blocks.swap(keep);
+    for (const CachedBlock &b : drop) C.total -= b.bytes;
+  }
+  int cur = 0;
+  if (cudaGetDevice(&cur) != cudaSuccess) cur = -1;
+  for (const CachedBlock &b : drop) {
+    cudaSetDevice(b.dev);
+    cudaFree(b.p);
+  }
+  if (cur >= 0) cudaSetDevice(cur);
+  (void)cudaGetLastError();
+}
+
+// A block of at least `bytes` on the current device: the smallest cached one that is at most
+// twice as large (plus 64 MiB), else a new allocation, retried once after this device's cache
+// has been freed.  *got receives the block's size.
+cudaError_t dev_alloc(size_t bytes, void **p, size_t *got) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  BlockCache &C = block_cache();
+  {
+    std::lock_guard<std::mutex> lock(C.mu);
+    int best = -1;
+    for (int i = 0; i < (int)C.blocks.size(); i++) {
+      const CachedBlock &b = C.blocks[i];
+      if (b.dev == dev && b.bytes >= bytes && b.bytes <= 2 * bytes + (size_t(64) << 20) &&
+          (best < 0 || b.bytes < C.blocks[best].bytes))
+        best = i;
+    }
+    if (best >= 0) {
+      *p = C.blocks[best].p;
+      *got = C.blocks[best].bytes;
+      C.total -= *got;
+      C.blocks.erase(C.blocks.begin() + best);
+      return cudaSuccess;
+    }
+  }
+  e = cudaMalloc(p, bytes);
+  if (e == cudaErrorMemoryAllocation) {
+    (void)cudaGetLastError();
+    release_cache(dev);
+    e = cudaMalloc(p, bytes);
+  }
+  *got = bytes;
+  return e;
+}
+
+// Gives a block back (to the cache while it has room).  The caller has waited for every use.
+void dev_free(void *p, size_t bytes) {
+  if (!p) return;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) {
+    BlockCache &C = block_cache();
+    std::lock_guard<std::mutex> lock(C.mu);
+    if (C.total + bytes <= kCacheMax) {
+      C.blocks.push_back({dev, p, bytes});
+      C.total += bytes;
+      return;
+    }
+  }
+  cudaFree(p);
+}
+
+// Page-locked Control mirrors, handed out from slabs of 64 that live for the process:
+// cudaMallocHost / cudaFreeHost per handle cost more than a small create's own work.
+struct CtlPool {
+  std::mutex mu;
+  std::vector<Control *> free;
+};
+
+CtlPool &ctl_pool() {
+  static CtlPool p;
+  return p;
+}
+
+Control *ctl_acquire() {
+  CtlPool &pool = ctl_pool();
+  std::lock_guard<std::mutex> lock(pool.mu);
+  if (pool.free.empty()) {
+    Control *slab = nullptr;
+    if (cudaMallocHost(reinterpret_cast<void **>(&slab), 64 * sizeof(Control)) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return nullptr;
+    }
+    for (int i = 63; i >= 0; i--) pool.free.push_back(slab + i);
+  }
+  Control *c = pool.free.back();
+  pool.free.pop_back();
+  std::memset(c, 0, sizeof(Control));
+  return c;
+}
+
+void ctl_release(Control *c) {
+  CtlPool &pool = ctl_pool();
+  std::lock_guard<std::mutex> lock(pool.mu);
+  pool.free.push_back(c);
+}
+
 void release(ccdgpu_handle *h) {
   if (!h) return;
+  // Cached blocks are handed to other handles: nothing of this one may still run on them.
+  for (cudaStream_t st : {h->s0, h->s1, h->s2, h->s3})
+    if (st) cudaStreamSynchronize(st);
   if (h->graph) cudaGraphExecDestroy(h->graph);
   if (h->graph_tc) cudaGraphExecDestroy(h->graph_tc);
   if (h->loop64) cudaGraphExecDestroy(h->loop64);
   if (h->loop_tc) cudaGraphExecDestroy(h->loop_tc);
-  for (auto &b : h->allocs) cudaFree(b.p);
+  for (auto &b : h->allocs) dev_free(b.p, b.bytes);
   h->allocs.clear();
-  if (h->tile_mem) cudaFree(h->tile_mem);
+  dev_free(h->tile_mem, h->tile_bytes);
   h->tile_mem = nullptr;
-  if (h->h_ctl) cudaFreeHost(h->h_ctl);
+  if (h->h_ctl) ctl_release(h->h_ctl);
+  h->h_ctl = nullptr;
   for (auto &e : h->ev)
     if (e) cudaEventDestroy(e);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
@@ -212,8 +347,9 @@ struct Arena {
   }
   int commit(ccdgpu_handle *h) {
     void *base = nullptr;
-    CK(cudaMalloc(&base, used));
-    h->allocs.push_back({base, used});
+    size_t got = 0;
+    CK(dev_alloc(used, &base, &got));
+    h->allocs.push_back({base, got});
     CK(cudaMemsetAsync(base, 0, used, h->s0));
     for (auto &r : reqs) *r.first = static_cast<char *>(base) + r.second;
     return CCDGPU_OK;
@@ -486,15 +622,26 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
   red_items(tc_tiles, red_tc, nullptr, false, nullptr);
   // Device copies: one allocation, counters zeroed.
   CK(cudaStreamSynchronize(h->s0));
-  if (h->tile_mem) CK(cudaFree(h->tile_mem));
+  CK(cudaStreamSynchronize(h->s2));
+  // Captured graphs hold the previous lists; they go before the block they point into.
+  for (cudaGraphExec_t *g : {&h->graph, &h->graph_tc, &h->loop64, &h->loop_tc})
+    if (*g) { cudaGraphExecDestroy(*g); *g = nullptr; }
+  h->loop_state = 0;
+  dev_free(h->tile_mem, h->tile_bytes);
   h->tile_mem = nullptr;
+  h->tile_bytes = 0;
+  h->tiles = h->tc_tiles = nullptr;
+  h->lpart = h->tc_part = nullptr;
+  h->fp_cta_off = h->tc_cta_off = nullptr;
+  h->red_fp = h->red_tc = nullptr;
+  h->n_tiles = h->n_tc_tiles = 0;
   Arena ar;
   ar.add(&h->tiles, tiles.size()); ar.add(&h->lpart, lpart_tot);
   ar.add(&h->tc_tiles, tc_tiles.size());
   ar.add(&h->fp_cta_off, fp_cta_off.size()); ar.add(&h->tc_cta_off, tc_cta_off.size());
   ar.add(&h->tc_part, tcpart_tot);
   ar.add(&h->red_fp, red_fp.size()); ar.add(&h->red_tc, red_tc.size());
-  CK(cudaMalloc(&h->tile_mem, ar.used));
+  CK(dev_alloc(ar.used, &h->tile_mem, &h->tile_bytes));
   CK(cudaMemsetAsync(h->tile_mem, 0, ar.used, h->s0));
   for (auto &r : ar.reqs) *r.first = static_cast<char *>(h->tile_mem) + r.second;
   if (!tiles.empty())
@@ -524,10 +671,6 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
   for (const LadderTile &t : tiles) h->n_cls[cls_of(t.nb)]++;
   h->n_tc_tiles = (int)tc_tiles.size();
   h->schedule = sch;
-  // Captured graphs hold the previous lists.
-  for (cudaGraphExec_t *g : {&h->graph, &h->graph_tc, &h->loop64, &h->loop_tc})
-    if (*g) { cudaGraphExecDestroy(*g); *g = nullptr; }
-  h->loop_state = 0;
   return CCDGPU_OK;
 }
 
@@ -1053,7 +1196,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   CK(cudaMemcpyAsync(&e, h->err, sizeof(e), cudaMemcpyDeviceToHost, h->s0));
   CK(cudaStreamSynchronize(h->s0));
   // Release the scratch allocation.
-  for (size_t i = n_allocs; i < h->allocs.size(); i++) cudaFree(h->allocs[i].p);
+  for (size_t i = n_allocs; i < h->allocs.size(); i++) dev_free(h->allocs[i].p, h->allocs[i].bytes);
   h->allocs.resize(n_allocs);
   if (e & kErrBadIndex) return CCDGPU_ERR_BAD_TABLE;
   // The fused path relies on the structure of the ring tables; the table path does not.
@@ -1061,8 +1204,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   if (e & ~kErrRingMaps) return CCDGPU_ERR_CUDA;
   if (e) CK(cudaMemsetAsync(h->err, 0, sizeof(int32_t), h->s0));
 #undef TRY
-  CK(cudaMallocHost(&h->h_ctl, sizeof(Control)));
-  std::memset(h->h_ctl, 0, sizeof(Control));
+  h->h_ctl = ctl_acquire();
+  if (!h->h_ctl) return CCDGPU_ERR_OUT_OF_MEMORY;
 
   h->ladder_smem = (size_t)kStages * (kMaxAS * kBK + kBK * kMaxBS) * 8 + 2 * kStages * 8;
   h->ladder_smem_thin = (size_t)kStages * (kMaxAS * kBK + kBK * 8) * 8 + 2 * kStages * 8;
@@ -1597,6 +1740,8 @@ int ccdgpu_create(const ccdgpu_problem *prob, const ccdgpu_options *opt, ccdgpu_
   *out = h;
   return CCDGPU_OK;
 }
+
+void ccdgpu_release_cached_memory(void) { release_cache(-1); }
 
 void ccdgpu_destroy(ccdgpu_handle *h) {
   if (!h) return;

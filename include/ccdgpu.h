@@ -155,6 +155,10 @@ void ccdgpu_default_options(ccdgpu_options *opt);
  * concerned; the host data may be freed afterwards.  T2 starts at zero (main.cpp:497-503). */
 int ccdgpu_create(const ccdgpu_problem *prob, const ccdgpu_options *opt, ccdgpu_handle **out);
 void ccdgpu_destroy(ccdgpu_handle *h);
+/* Device memory of destroyed handles stays in a process-wide cache (at most 16 GiB) and is
+ * reused by later handles on the same device, so that repeated create/destroy cycles do not
+ * call cudaMalloc/cudaFree.  This returns the cached memory to the device. */
+void ccdgpu_release_cached_memory(void);
 const char *ccdgpu_strerror(int status);
 
 /* Zero every amplitude chain (main.cpp:497-503). */
