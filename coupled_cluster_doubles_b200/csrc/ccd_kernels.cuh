@@ -135,6 +135,18 @@ __device__ __forceinline__ void dmma_884(double (&c)[2], double a, double b) {
       : "d"(a), "d"(b));
 }
 
+// C (16 x 8) += A (16 x 16) B (16 x 8) in FP64, lane layout (g = lane / 4, t = lane % 4):
+// a[i] = A[g + 8 (i % 2)][t + 4 (i / 2)], b[i] = B[t + 4 i][g],
+// c = {C[g][2t], C[g][2t + 1], C[g + 8][2t], C[g + 8][2t + 1]}.
+__device__ __forceinline__ void dmma_16816(double (&c)[4], const double (&a)[8],
+                                           const double (&b)[4]) {
+  asm("mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+      "{%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]),
+        "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
 
 // Stores the finished values of packed row u_local (cols [c0, c0+n)), or its partial sum.
 struct LadderOut {
@@ -229,24 +241,23 @@ __device__ __forceinline__ bool consume_thin(const LadderTile &tile, const doubl
 }
 
 // Mid and wide channels (nb = 8*C, C = 2..9) on the FP64 MMA: consumer warp w owns tile rows
-// [16w, 16w + 16) as 2 row tiles x C column tiles of 8 x 8 (4*C accumulators per lane).  A
-// (k-major, row stride ar) and B (k-major, row stride bs) fragments come from the stage
-// conflict-free: both strides are 4 mod 8 doubles.
+// [16w, 16w + 16), one m16n8k16 per 8-column tile and stage (kBK = 16), 4*C accumulators per
+// lane.  A (k-major, row stride ar) and B (k-major, row stride bs) fragments come from the
+// stage conflict-free: both strides are 4 mod 8 doubles.  A warp whose lower 8-row half has
+// no rows feeds zeros there instead of reading past the tile.
 template <int C>
 __device__ __forceinline__ bool consume_mma(const LadderTile &tile, const double *As,
                                             const double *Bs, int bstage, uint64_t *bars,
                                             int tid, const LadderOut &out, int32_t *err,
                                             int gc0) {
+  static_assert(kBK == 16, "one m16n8k16 K step per stage");
   constexpr int NB = 8 * C, BS = NB + 4;
   const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
   const int ar = ladder_arows(NB, tile.rows);
-  constexpr int MT = 2;
-  const int mtiles = min(MT, max(0, ((tile.rows + 7) >> 3) - MT * warp));  // row tiles with rows
-  double acc[MT][C][2];
+  const int halves = min(2, max(0, ((tile.rows + 7) >> 3) - 2 * warp));  // 8-row halves with rows
+  double acc[C][4];
 #pragma unroll
-  for (int i = 0; i < MT; ++i)
-#pragma unroll
-    for (int j = 0; j < C; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  for (int j = 0; j < C; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
   const int nchunks = tile.nks + tile.nkh;
   for (int c = 0; c < nchunks; ++c) {
     const int gch = gc0 + c, s = gch % kStages;  // chunk number gch of this CTA
@@ -254,34 +265,31 @@ __device__ __forceinline__ bool consume_mma(const LadderTile &tile, const double
       atomicOr(err, kErrTimeout);
       return false;
     }
-    if (mtiles > 0) {
-      const double *A = As + s * (kMaxAS * kBK) + t * ar + 8 * MT * warp + g;
+    if (halves > 0) {
+      const double *A = As + s * (kMaxAS * kBK) + t * ar + 16 * warp + g;
       const double *B = Bs + s * bstage + t * BS + g;
+      double a[8];
 #pragma unroll
-      for (int k4 = 0; k4 < kBK / 4; ++k4) {
-        double a[MT], b[C];
+      for (int i = 0; i < 8; ++i)
+        a[i] = (i % 2 == 0 || halves > 1) ? A[4 * (i / 2) * ar + 8 * (i % 2)] : 0.0;
 #pragma unroll
-        for (int i = 0; i < MT; ++i) a[i] = A[k4 * 4 * ar + 8 * i];
+      for (int j = 0; j < C; ++j) {
+        double b[4];
 #pragma unroll
-        for (int j = 0; j < C; ++j) b[j] = B[k4 * 4 * BS + 8 * j];
-#pragma unroll
-        for (int i = 0; i < MT; ++i)
-          if (i < mtiles) {
-#pragma unroll
-            for (int j = 0; j < C; ++j) dmma_884(acc[i][j], a[i], b[j]);
-          }
+        for (int q = 0; q < 4; ++q) b[q] = B[4 * q * BS + 8 * j];
+        dmma_16816(acc[j], a, b);
       }
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(smem_u32(&bars[kStages + s]));
   }
+  if (halves > 0) {
 #pragma unroll
-  for (int i = 0; i < MT; ++i)
-    if (i < mtiles) {
-#pragma unroll
-      for (int j = 0; j < C; ++j)
-        out.row(8 * MT * warp + 8 * i + g, 8 * j + 2 * t, acc[i][j], 2);
+    for (int j = 0; j < C; ++j) {
+      out.row(16 * warp + g, 8 * j + 2 * t, acc[j], 2);
+      if (halves > 1) out.row(16 * warp + 8 + g, 8 * j + 2 * t, acc[j] + 2, 2);
     }
+  }
   return true;
 }
 
