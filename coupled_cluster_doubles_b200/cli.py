@@ -91,6 +91,7 @@ def system_spec(opts):
         kw = dict(r_s=opts["r_s"], n_shells=opts["nShells"],
                   n_particle_shells=opts["nParticleShells"])
     kw["load_v_pppp"] = not opts["saveMemory"]
+    kw["tables"] = False  # the remap tables are derived on the device at create
     return opts["basis"], kw
 
 
