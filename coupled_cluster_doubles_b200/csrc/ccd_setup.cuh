@@ -136,6 +136,62 @@ __device__ __forceinline__ double tbme_dev(const ModelDev &m, int a, int b, int 
   return direct_pnm_dev(qa, qb, qc, qd, m.Lb) - direct_pnm_dev(qa, qb, qd, qc, m.Lb);
 }
 
+// ---- The other V blocks generated on the device (problem without V blocks) ---------------
+// The reference's loaders with SPBasis::calcTBME (load.cpp:112-130, 155-172, 275-318), written
+// straight into the solver's layouts.  V_hhhh[ij][kl] = <ij|v|kl>, one CTA per active channel.
+__global__ void gen_v_hhhh_kernel(const ChanInfo *__restrict__ chans,
+                                  const int2 *__restrict__ hh_pairs, ModelDev m,
+                                  double *__restrict__ v_hhhh) {
+  const ChanInfo ch = chans[blockIdx.x];
+  for (int e = threadIdx.x; e < ch.hh * ch.hh; e += blockDim.x) {
+    const int2 ij = hh_pairs[ch.hh_off + e / ch.hh], kl = hh_pairs[ch.hh_off + e % ch.hh];
+    v_hhhh[ch.x_off + e] = tbme_dev(m, ij.x, ij.y, kl.x, kl.y);
+  }
+}
+
+// V_pphh[ab][ij] = V_hhpp[ij][ab] = <ij|v|ab>, over the element ranges of the amplitudes.
+__global__ void gen_v_pphh_kernel(const ElemRange *__restrict__ ranges,
+                                  const ChanInfo *__restrict__ chans,
+                                  const int2 *__restrict__ pp_pairs,
+                                  const int2 *__restrict__ hh_pairs, ModelDev m,
+                                  double *__restrict__ v_pphh) {
+  const ElemRange rg = ranges[blockIdx.x];
+  const ChanInfo ch = chans[rg.ch];
+  for (int64_t e = rg.e0 + threadIdx.x; e < rg.e1; e += blockDim.x) {
+    const int64_t loc = e - ch.t_off;
+    const int ab = (int)(loc / ch.hh), ij = (int)(loc - (int64_t)ab * ch.hh);
+    const int2 pab = pp_pairs[ch.pp_off + ab], pij = hh_pairs[ch.hh_off + ij];
+    v_pphh[e] = tbme_dev(m, pij.x, pij.y, pab.x, pab.y);
+  }
+}
+
+// Per active modified channel (channel order): its block offsets and where its ph' pairs (b, j)
+// and hp' pairs (i, a) start in the pair arrays.
+struct ModGen {
+  int32_t ph, hp;
+  int64_t m_off, y_off, ph_off, hp_off;
+};
+
+// One CTA per active modified channel:
+//   V_hpph' (load.cpp:275-296): [(i,a)][(b,j)] = <ij|v|ab>, stored transposed (ph' x hp') as the
+//     ring reads it;
+//   V_hphp' (load.cpp:298-318): [(i,b)][(j,a)] = <ia|v|bj>.
+__global__ void gen_v_mod_kernel(const ModGen *__restrict__ mods, const int2 *__restrict__ ph_pairs,
+                                 const int2 *__restrict__ hp_pairs, ModelDev m,
+                                 double *__restrict__ v_hpph_t, double *__restrict__ v_hphp) {
+  const ModGen g = mods[blockIdx.x];
+  for (int e = threadIdx.x; e < g.ph * g.hp; e += blockDim.x) {
+    const int k = e / g.hp, x = e - k * g.hp;  // ph' row k, hp' column x
+    const int2 bj = ph_pairs[g.ph_off + k], ia = hp_pairs[g.hp_off + x];
+    v_hpph_t[g.m_off + e] = tbme_dev(m, ia.x, bj.y, ia.y, bj.x);
+  }
+  for (int e = threadIdx.x; e < g.hp * g.hp; e += blockDim.x) {
+    const int x = e / g.hp, y = e - x * g.hp;
+    const int2 ib = hp_pairs[g.hp_off + x], ja = hp_pairs[g.hp_off + y];
+    v_hphp[g.y_off + e] = tbme_dev(m, ib.x, ja.y, ib.y, ja.x);
+  }
+}
+
 // E_ref and the normal-ordered single-particle energies from the bare ones (SPBasis.cpp:7-40).
 // Thread p < nsp: e_p + sum_{j < nh} <pj|v|pj>, summed in the reference's order.  Thread nsp:
 // E_ref = sum_{i,j < nh} 0.5 <ij|v|ij> + sum_{i < nh} e_i, one running sum in the reference's

@@ -685,9 +685,14 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
                         M->kind <= CCDGPU_MODEL_ELECTRON_GAS &&
                         M->qn_stride >= (M->kind == CCDGPU_MODEL_PAIRING ? 2 : 5);
   if (on_the_fly && !model_ok) return CCDGPU_ERR_INVALID_ARGUMENT;
-  if ((!on_the_fly && !P->v_pppp) || !P->v_hhpp || !P->v_hhhh || !P->v_hpph_mod ||
-      !P->v_hphp_mod)
-    return CCDGPU_ERR_INVALID_ARGUMENT;
+  if (!on_the_fly && !P->v_pppp) return CCDGPU_ERR_INVALID_ARGUMENT;
+  // No V_hhhh, V_hhpp and modified-channel V at all (all four NULL): generated on the device
+  // from the model, like V_pppp in the on-the-fly mode.
+  const int n_vblocks = (P->v_hhhh ? 1 : 0) + (P->v_hhpp ? 1 : 0) + (P->v_hpph_mod ? 1 : 0) +
+                        (P->v_hphp_mod ? 1 : 0);
+  if (n_vblocks != 0 && n_vblocks != 4) return CCDGPU_ERR_INVALID_ARGUMENT;
+  const bool gen_v = n_vblocks == 0;
+  if (gen_v && !model_ok) return CCDGPU_ERR_INVALID_ARGUMENT;
   // No loadMaps tables at all: the library derives them on the device from the channel maps.
   int n_maps = 0;
   for (int k = 0; k < 8; k++) n_maps += P->maps[k] ? 1 : 0;
@@ -826,17 +831,34 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   size_t ring_smem = 0;
   std::vector<const double *> src_hpph, src_hphp;
   std::vector<int64_t> cnt_hpph, cnt_hphp;
+  std::vector<ModGen> mod_gen;        // generated V: modified channels in channel order
+  std::vector<int2> mod_ph, mod_hp;   // ... and their ph' (b, j) and hp' (i, a) pairs
   for (uint64_t c = 0; c < nch; c++) {
     const int64_t ph = MD[c].ph, hp = MD[c].hp;
     mod_dims[c] = make_int2((int)ph, (int)hp);
     if (!ph || !hp) continue;
     if (ph > kTcMaxNB || hp > kTcMaxNB) return CCDGPU_ERR_UNSUPPORTED;  // ring register tiles
-    if (!P->v_hpph_mod[c] || !P->v_hphp_mod[c]) return CCDGPU_ERR_INVALID_ARGUMENT;
     ModInfo m{};
     m.ph = (int)ph; m.hp = (int)hp; m.m_off = o_m[c]; m.y_off = y_tot;
+    if (gen_v) {
+      const ccdgpu_pair *phm = P->chan_mod_maps[c].ph, *hpm = P->chan_mod_maps[c].hp;
+      if (!phm || !hpm) return CCDGPU_ERR_INVALID_ARGUMENT;
+      mod_gen.push_back(ModGen{(int)ph, (int)hp, m.m_off, m.y_off, (int64_t)mod_ph.size(),
+                               (int64_t)mod_hp.size()});
+      for (int64_t k = 0; k < ph; k++) {
+        if (phm[k].p < np || phm[k].p >= nsp || phm[k].q >= np) return CCDGPU_ERR_BAD_TABLE;
+        mod_ph.push_back(make_int2((int)phm[k].p, (int)phm[k].q));
+      }
+      for (int64_t k = 0; k < hp; k++) {
+        if (hpm[k].p >= np || hpm[k].q < np || hpm[k].q >= nsp) return CCDGPU_ERR_BAD_TABLE;
+        mod_hp.push_back(make_int2((int)hpm[k].p, (int)hpm[k].q));
+      }
+    } else {
+      if (!P->v_hpph_mod[c] || !P->v_hphp_mod[c]) return CCDGPU_ERR_INVALID_ARGUMENT;
+      src_hpph.push_back(P->v_hpph_mod[c]); cnt_hpph.push_back(ph * hp);
+      src_hphp.push_back(P->v_hphp_mod[c]); cnt_hphp.push_back(hp * hp);
+    }
     y_tot += hp * hp;
-    src_hpph.push_back(P->v_hpph_mod[c]); cnt_hpph.push_back(ph * hp);
-    src_hphp.push_back(P->v_hphp_mod[c]); cnt_hphp.push_back(hp * hp);
     const int stage = ring_stage_doubles((int)ph, (int)hp);
     if (ph <= kRingSmall && hp <= kRingSmall) {
       mods.push_back(m);
@@ -1025,7 +1047,14 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   } else {
     sc.add(&raw_idx, (size_t)8 * n_t);
   }
-  sc.add(&vraw, vraw_tot); sc.add(&hhpp_raw, n_t); sc.add(&hpph_raw, h->n_m);
+  ModGen *d_mod_gen = nullptr;
+  int2 *d_mod_ph = nullptr, *d_mod_hp = nullptr;
+  if (gen_v) {
+    sc.add(&d_mod_gen, mod_gen.size()); sc.add(&d_mod_ph, mod_ph.size());
+    sc.add(&d_mod_hp, mod_hp.size());
+  }
+  sc.add(&vraw, vraw_tot); sc.add(&hhpp_raw, gen_v ? 0 : n_t);
+  sc.add(&hpph_raw, gen_v ? 0 : h->n_m);
   sc.add(&counts, (size_t)5 * n_t); sc.add(&d_vrows, vrows.size()); 
   sc.add(&d_vraw_off, vraw_off.size()); sc.add(&d_mod_dims, mod_dims.size()); sc.add(&d_o_m, o_m.size());
   // The model on the device (on-the-fly V, E_ref and normal ordering): quantum numbers and
@@ -1105,11 +1134,13 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     for (size_t ai = 0; ai < chans.size(); ai++) {
       const uint64_t c = act_chan[ai];
       const ChanInfo &a = chans[ai];
-      if ((!on_the_fly && !P->v_pppp[c]) || !P->v_hhpp[c] || !P->v_hhhh[c])
+      if ((!on_the_fly && !P->v_pppp[c]) || (!gen_v && (!P->v_hhpp[c] || !P->v_hhhh[c])))
         return CCDGPU_ERR_INVALID_ARGUMENT;
       if (!on_the_fly) { sp.push_back(P->v_pppp[c]); np2.push_back((int64_t)a.pp * a.pp); }
-      sx.push_back(P->v_hhpp[c]); nx.push_back((int64_t)a.pp * a.hh);
-      sh.push_back(P->v_hhhh[c]); nh.push_back((int64_t)a.hh * a.hh);
+      if (!gen_v) {
+        sx.push_back(P->v_hhpp[c]); nx.push_back((int64_t)a.pp * a.hh);
+        sh.push_back(P->v_hhhh[c]); nh.push_back((int64_t)a.hh * a.hh);
+      }
       for (int k = 0; k < 8 && !derive_tables; k++) {
         if (!P->maps[k][c]) return CCDGPU_ERR_INVALID_ARGUMENT;
         sm[k].push_back(P->maps[k][c]);
@@ -1123,6 +1154,11 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     for (int k = 0; k < 8 && !derive_tables; k++)
       TRY(upload_runs(h, reinterpret_cast<ccdgpu_chain_index *>(raw_idx) + (size_t)k * n_t, sm[k], nm));
     if (derive_tables) TRY(put(d_mlook, mlook));
+    if (gen_v) {
+      TRY(put(d_mod_gen, mod_gen));
+      TRY(put(d_mod_ph, mod_ph));
+      TRY(put(d_mod_hp, mod_hp));
+    }
     TRY(upload_runs(h, hpph_raw, src_hpph, cnt_hpph));
     TRY(upload_runs(h, h->v_hphp, src_hphp, cnt_hphp));
     if (h->have_3body) {
@@ -1143,12 +1179,25 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     }
   }
   // Device layout transforms.
-  if (h->n_mod) {
+  if (gen_v && !mod_gen.empty()) {
+    gen_v_mod_kernel<<<(unsigned)mod_gen.size(), 256, 0, h->s0>>>(d_mod_gen, d_mod_ph, d_mod_hp,
+                                                                 md, h->v_hpph, h->v_hphp);
+    CK(cudaGetLastError());
+  } else if (h->n_mod) {
     transpose_hpph_kernel<<<h->n_mod, 256, 0, h->s0>>>(h->mods, hpph_raw, h->v_hpph);
     CK(cudaGetLastError());
   }
   if (h->n_ranges) {
-    transpose_hhpp_kernel<<<h->n_ranges, 256, 0, h->s0>>>(h->ranges, h->chans, hhpp_raw, h->v_pphh);
+    if (gen_v) {
+      gen_v_pphh_kernel<<<h->n_ranges, 256, 0, h->s0>>>(h->ranges, h->chans, h->pp_pairs,
+                                                        h->hh_pairs, md, h->v_pphh);
+      CK(cudaGetLastError());
+      gen_v_hhhh_kernel<<<(unsigned)chans.size(), 256, 0, h->s0>>>(h->chans, h->hh_pairs, md,
+                                                                   h->v_hhhh);
+    } else {
+      transpose_hhpp_kernel<<<h->n_ranges, 256, 0, h->s0>>>(h->ranges, h->chans, hhpp_raw,
+                                                            h->v_pphh);
+    }
     CK(cudaGetLastError());
     if (derive_tables) {
       pair_sizes_kernel<<<(unsigned)chans.size(), 256, 0, h->s0>>>(

@@ -217,7 +217,8 @@ struct ccdhost_system {
 namespace {
 
 int finish(ccdhost_system *s, int32_t flags) {
-  const bool load_v_pppp = flags & CCDHOST_LOAD_V_PPPP;
+  const bool vblocks = !(flags & CCDHOST_NO_V);
+  const bool load_v_pppp = vblocks && (flags & CCDHOST_LOAD_V_PPPP);
   const bool tables = !(flags & CCDHOST_NO_TABLES);
   Model &m = s->m;
   const uint64_t nsp = m.nsp, np = m.np, nch = m.nchan;
@@ -373,9 +374,10 @@ int finish(ccdhost_system *s, int32_t flags) {
     }
   }
 
-  // V blocks for amplitude-carrying channels (load.cpp:112-318).
-  auto active = [&](uint64_t c) { return s->dims[c].pp && s->dims[c].hh; };
-  auto mactive = [&](uint64_t c) { return s->mdims[c].ph && s->mdims[c].hp; };
+  // V blocks for amplitude-carrying channels (load.cpp:112-318); none with CCDHOST_NO_V (the
+  // solver library then generates them on the device from the model).
+  auto active = [&](uint64_t c) { return vblocks && s->dims[c].pp && s->dims[c].hh; };
+  auto mactive = [&](uint64_t c) { return vblocks && s->mdims[c].ph && s->mdims[c].hp; };
   std::vector<uint64_t> o_hhhh(nch + 1, 0), o_hhpp(nch + 1, 0), o_pppp(nch + 1, 0),
       o_hpph(nch + 1, 0), o_hphp(nch + 1, 0);
   for (uint64_t c = 0; c < nch; c++) {
@@ -390,7 +392,8 @@ int finish(ccdhost_system *s, int32_t flags) {
   try {
     s->v[0].resize(o_hhhh[nch]); s->v[1].resize(o_hhpp[nch]); s->v[2].resize(o_pppp[nch]);
     s->v[3].resize(o_hpph[nch]); s->v[4].resize(o_hphp[nch]);
-    s->v[5].resize(s->hpp_off_map[np]); s->v[6].resize(s->phh_off_map[npart]);
+    s->v[5].resize(vblocks ? s->hpp_off_map[np] : 0);
+    s->v[6].resize(vblocks ? s->phh_off_map[npart] : 0);
   } catch (const std::bad_alloc &) {
     return CCDGPU_ERR_OUT_OF_MEMORY;
   }
@@ -438,16 +441,16 @@ int finish(ccdhost_system *s, int32_t flags) {
     }
   }
 #pragma omp parallel for schedule(dynamic)
-  for (int64_t k = 0; k < (int64_t)np; k++)  // vnn_h_hpp[k][(j,a,b)] = <kj|v|ab> (load.cpp:258-273)
+  for (int64_t k = 0; k < (vblocks ? (int64_t)np : 0); k++)  // vnn_h_hpp[k][(j,a,b)] = <kj|v|ab> (load.cpp:258-273)
     for (uint64_t t = s->hpp_off_map[k]; t < s->hpp_off_map[k + 1]; t++)
       s->v[5][t] = s->m.tbme(k, s->hpp_all[t].p, s->hpp_all[t].q, s->hpp_all[t].r);
 #pragma omp parallel for schedule(dynamic)
-  for (int64_t a = 0; a < (int64_t)npart; a++)  // vnn_phh_p[a][(b,i,j)] = <ij|v|ab> (load.cpp:241-256)
+  for (int64_t a = 0; a < (vblocks ? (int64_t)npart : 0); a++)  // vnn_phh_p[a][(b,i,j)] = <ij|v|ab> (load.cpp:241-256)
     for (uint64_t t = s->phh_off_map[a]; t < s->phh_off_map[a + 1]; t++)
       s->v[6][t] = s->m.tbme(s->phh_all[t].q, s->phh_all[t].r, a + np, s->phh_all[t].p);
-  for (uint64_t k = 0; k < np; k++)
+  for (uint64_t k = 0; k < np && vblocks; k++)
     if (s->tdims[k].hpp) s->vptr[5][k] = &s->v[5][s->hpp_off_map[k]];
-  for (uint64_t a = 0; a < npart; a++)
+  for (uint64_t a = 0; a < npart && vblocks; a++)
     if (s->tdims[a + np].phh) s->vptr[6][a] = &s->v[6][s->phh_off_map[a]];
 
   // Remap tables (load.cpp:469-526), from block offsets instead of hash tables; skipped with
@@ -483,15 +486,15 @@ int finish(ccdhost_system *s, int32_t flags) {
   // MBPT2 (MBPT2Corr.cpp:6-38), channel order, normal-ordered energies.
   double e2 = 0.;
   for (uint64_t c = 0; c < nch; c++) {
-    if (!active(c)) continue;
+    if (!s->dims[c].pp || !s->dims[c].hh) continue;
     const uint64_t pp = s->dims[c].pp, hh = s->dims[c].hh;
-    const double *vx = s->vptr[1][c];
+    const double *vx = s->vptr[1][c];  // NULL with CCDHOST_NO_V: the same elements, evaluated
     double corr = 0.;
     for (uint64_t x = 0; x < hh; x++)
       for (uint64_t y = 0; y < pp; y++) {
         const ccdgpu_pair H = s->maps[c].hh[x], P = s->maps[c].pp[y];
         double den = s->eps[H.p] + s->eps[H.q] - s->eps[P.p] - s->eps[P.q];
-        double v = vx[x * pp + y];
+        double v = vx ? vx[x * pp + y] : s->m.tbme(H.p, H.q, P.p, P.q);
         corr += v * v / den;
       }
     e2 += 0.25 * corr;
@@ -516,10 +519,13 @@ int finish(ccdhost_system *s, int32_t flags) {
   P.chan_dims = s->dims.data(); P.chan_mod_dims = s->mdims.data();
   P.chan_maps = s->maps.data(); P.chan_mod_maps = s->mmaps.data();
   P.three_body_dims = s->tdims.data();
-  P.v_hhhh = s->vptr[0].data(); P.v_hhpp = s->vptr[1].data();
+  P.v_hhhh = vblocks ? s->vptr[0].data() : nullptr;
+  P.v_hhpp = vblocks ? s->vptr[1].data() : nullptr;
   P.v_pppp = load_v_pppp ? s->vptr[2].data() : nullptr;
-  P.v_hpph_mod = s->vptr[3].data(); P.v_hphp_mod = s->vptr[4].data();
-  P.v_h_hpp = s->vptr[5].data(); P.v_phh_p = s->vptr[6].data();
+  P.v_hpph_mod = vblocks ? s->vptr[3].data() : nullptr;
+  P.v_hphp_mod = vblocks ? s->vptr[4].data() : nullptr;
+  P.v_h_hpp = vblocks ? s->vptr[5].data() : nullptr;
+  P.v_phh_p = vblocks ? s->vptr[6].data() : nullptr;
   for (int k = 0; k < 8; k++) P.maps[k] = tables ? s->tabptr[k].data() : nullptr;
   P.model = &s->model;
   return CCDGPU_OK;

@@ -78,6 +78,8 @@ typedef struct ccdgpu_problem {
   const ccdgpu_channel_maps *chan_maps;        /* [n_channels] pp and hh maps are read */
   const ccdgpu_channel_maps *chan_mod_maps;    /* [n_channels] ph and hp maps are read */
   const ccdgpu_three_body_dims *three_body_dims; /* [n_sp] hpp for holes, phh for particles */
+  /* V blocks.  v_hhhh, v_hhpp, v_hpph_mod and v_hphp_mod may be NULL together when a model is
+   * given: ccdgpu_create then generates them on the device (load.cpp:112-318 elements). */
   const double *const *v_hhhh;      /* [n_channels] hh x hh  (vnn_hhhh) */
   const double *const *v_hhpp;      /* [n_channels] hh x pp  (vnn_hhpp) */
   const double *const *v_pppp;      /* [n_channels] pp x pp  (vnn_pppp); may be NULL if model given */

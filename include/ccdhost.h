@@ -33,8 +33,12 @@ typedef struct ccdhost_system ccdhost_system;
 /* Build flags (the last int32 argument of the ccdhost_build_* functions). */
 enum ccdhost_flags {
   CCDHOST_LOAD_V_PPPP = 1, /* build and pass V_pppp (off: the solver generates it, saveMemory) */
-  CCDHOST_NO_TABLES = 2    /* build no loadMaps remap tables: ccdgpu_problem.maps[] are NULL
+  CCDHOST_NO_TABLES = 2,   /* build no loadMaps remap tables: ccdgpu_problem.maps[] are NULL
                               and ccdgpu_create derives the tables on the device */
+  CCDHOST_NO_V = 4         /* build no V blocks at all (CCDHOST_LOAD_V_PPPP is ignored): every
+                              ccdgpu_problem.v_* is NULL and ccdgpu_create generates them on
+                              the device from the model (V_pppp needs CCDGPU_V_ON_THE_FLY;
+                              without the three-body V only the fused path runs) */
 };
 
 /* --pairing -l n_pair_states -n n_particles -x xi -g g  (parse.cpp:232-234) */

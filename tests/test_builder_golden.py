@@ -55,6 +55,25 @@ def test_builder_without_tables_keeps_everything_else(name):
             assert fnv1a(s.array(n)) == int(g["v_hashes"][k]), n
 
 
+@pytest.mark.parametrize("name", ["pairing_gp0.5", "pnm14_s4", "eg14_s19"])
+def test_builder_without_v_blocks(name):
+    """CCDHOST_NO_V: every ccdgpu_problem.v_* is NULL (the solver generates the blocks on the
+    device); E_ref, E_MBPT2 (evaluated element by element) and the structure stay bit-identical
+    to the reference's."""
+    from coupled_cluster_doubles_b200 import System
+    g = golden(name)
+    with getattr(System, g["kind"])(**g["params"], tables=False, v_blocks=False) as s:
+        p = s.problem.contents
+        assert not any([p.v_hhhh, p.v_hhpp, p.v_pppp, p.v_hpph_mod, p.v_hphp_mod, p.v_h_hpp,
+                        p.v_phh_p])
+        assert s.reference_energy == float(g["scalars"][0])
+        assert s.mbpt2 == float(g["scalars"][1])
+        for n in VKINDS:
+            assert s.array(n).size == 0, n
+        for k, n in enumerate(STRUCT):
+            assert fnv1a(s.array(n)) == int(g["struct_hashes"][k]), n
+
+
 @pytest.mark.parametrize("args", [dict(xi=1.0, g=0.5, n_pair_states=4, n_particles=8),
                                   dict(xi=1.0, g=0.5, n_pair_states=0, n_particles=0)])
 def test_builder_rejects_bad_pairing_input(args):

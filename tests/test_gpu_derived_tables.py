@@ -46,3 +46,25 @@ def test_derived_tables_mixed_precision_on_the_fly_v():
             CCDSolver(s1, precision="mixed_bf16", v_mode="on_the_fly") as a, \
             CCDSolver(s2, precision="mixed_bf16", v_mode="on_the_fly") as b:
         _same_solve(a, b, g)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed_bf16"])
+@pytest.mark.parametrize("name", SMALL + ["eg54_s19"])
+def test_nothing_but_structure_from_the_host(name, precision):
+    """No V block and no remap table from the host: ccdgpu_create generates every V block from
+    the model (load.cpp:112-318 elements) and derives the tables.  Pairing and electron-gas
+    elements are bit-identical to the host's, so the solve is too; the Minnesota elements use
+    CUDA's exp/pow and may differ by an ulp, so the PNM solve is held to the reference energy."""
+    g = golden(name)
+    with system_for(g) as s1, \
+            getattr(System, g["kind"])(**g["params"], tables=False, v_blocks=False) as s2, \
+            CCDSolver(s1, precision=precision) as a, \
+            CCDSolver(s2, precision=precision, v_mode="on_the_fly") as b:
+        if g["kind"] == "inf_matter":
+            rb = b.solve(tol=g["tol"], max_iters=100, mixing=0.5)
+            ref = g["energies"][-1]
+            rtol = 1e-10 if precision == "fp64" else 1e-6
+            assert abs(rb.e_corr - ref) <= rtol * abs(ref) + 1e-14
+        else:
+            _same_solve(a, b, g)
+        assert b.mbpt2() == pytest.approx(float(g["scalars"][1]), rel=1e-12, abs=1e-15)
