@@ -328,9 +328,11 @@ def main():
     # the device, as a caller that skips loadMaps would have it.
     host_t2 = np.empty(n_t2)
     e2e_secs, e2e_iters = 0.0, 0
-    system_e2e = getattr(System, kind)(**params, load_v_pppp=args.v_mode == "stored",
-                                       tables=False)
-    h2d = _problem_bytes(system_e2e, with_v_pppp=args.v_mode == "stored", with_tables=False)
+    # With V generated on the device (on_the_fly) the problem carries no V block either.
+    stored = args.v_mode == "stored"
+    system_e2e = getattr(System, kind)(**params, load_v_pppp=stored, tables=False,
+                                       v_blocks=stored)
+    h2d = _problem_bytes(system_e2e, with_v_pppp=stored, with_tables=False, with_v=stored)
     phase_s = np.zeros(4)  # create, solve (graph capture included), T2 read-back, destroy
     for k in range(args.warmup + args.steps):
         t0 = time.perf_counter()
@@ -439,8 +441,9 @@ def main():
             "shared_kernels_alone": shared,
             "e2e": {"value": e2e_iters_all / e2e_secs_max, "unit": "iter/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * n_t2,
-                    "what": "ccdgpu_create from host buffers (remap tables derived on the "
-                            "device) + ccdgpu_solve + ccdgpu_get_t2",
+                    "what": "ccdgpu_create from host buffers (remap tables"
+                            + ("" if args.v_mode == "stored" else " and every V block")
+                            + " made on the device) + ccdgpu_solve + ccdgpu_get_t2",
                     "rank0_ms_per_step": dict(zip(["create", "solve", "get_t2", "destroy"],
                                                   (1e3 * phase_s / args.steps).round(3).tolist()))},
             "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved,
@@ -566,12 +569,13 @@ def run_batch(args):
         s.close()
 
 
-def _problem_bytes(system, with_v_pppp=True, with_tables=True):
+def _problem_bytes(system, with_v_pppp=True, with_tables=True, with_v=True):
     """Bytes ccdgpu_create copies host -> device for this system: V blocks in their reference
     layouts (V_pppp, V_hhpp, V_hhhh of amplitude-carrying channels, both modified-channel V,
     the three-body V), the eight ChainIndex tables (24 bytes per entry) or, without them, the
     16-byte modified-pair lookup per (particle, hole), the energies and the O(sum pp) pair
-    metadata."""
+    metadata.  with_v=False: no V block; the modified channels' pair lists (8 bytes a pair)
+    instead, from which the device generates them."""
     import numpy as np
     d = system.chan_dims()
     act = (d[:, 0] > 0) & (d[:, 1] > 0)
@@ -584,6 +588,9 @@ def _problem_bytes(system, with_v_pppp=True, with_tables=True):
     v = 8 * int((pp * pp).sum() * (1 if with_v_pppp else 0) + n_t + (hh * hh).sum() +
                 (ph * hp).sum() + (hp * hp).sum())
     v += 8 * 2 * n_t
+    if not with_v:
+        act_m = (ph > 0) & (hp > 0)
+        v = 8 * int(ph[act_m].sum() + hp[act_m].sum()) + 40 * int(act_m.sum())
     meta = 24 * int(pp.sum()) + 16 * int(hh.sum()) + 8 * system.n_sp
     npart = system.n_sp - system.n_particles
     tables = 24 * 8 * n_t if with_tables else 16 * npart * system.n_particles
