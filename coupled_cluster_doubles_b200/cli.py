@@ -7,7 +7,7 @@ Reference options and defaults (parse.cpp:128-196, main.cpp:34-39):
   --pairing | --infMatter (default) | --electronGas     basis
   -d/--density 0.08  -g/--g 0.5  -p/--nParticleShells 2  -n/--nParticles 4
   -l/--nPairStates 4  -r/--r_s 0.5  -s/--nShells 4  -t/--tolerance 1e-8  -z/--tzMax 1
-  -x/--xi 1.0  -m/--saveMemory 0 (1: V_pppp generated on the device)  -v/--verbose 0
+  -x/--xi 1.0  -m/--saveMemory 0 (1: every V block generated on the device)  -v/--verbose 0
   -c/--config FILE   whitespace-separated options read first; the command line overrides them
 The reference's load-balancer timing options (-T, -W, -M) have no counterpart (one GPU per
 system).  Additions: --precision (fp64, mixed_bf16, mixed_bf16x3), --device, --max-iters,
@@ -92,6 +92,8 @@ def system_spec(opts):
                   n_particle_shells=opts["nParticleShells"])
     kw["load_v_pppp"] = not opts["saveMemory"]
     kw["tables"] = False  # the remap tables are derived on the device at create
+    # saveMemory: every V block is generated on the device from the model, none on the host.
+    kw["v_blocks"] = not opts["saveMemory"]
     return opts["basis"], kw
 
 

@@ -35,13 +35,14 @@ def test_system_spec_per_basis():
     kind, kw = cli.system_spec(cli.parse_args("--infMatter -d 0.08 -z 1 -s 4 -p 2".split()))
     assert kind == "inf_matter"
     assert kw == dict(density=0.08, tz_max=1, n_shells=4, n_particle_shells=2, load_v_pppp=True,
-                      tables=False)
+                      tables=False, v_blocks=True)
     kind, kw = cli.system_spec(cli.parse_args("--pairing -l 8 -n 8 -x 1.0 -g 0.5".split()))
     assert kind == "pairing"
     assert kw == dict(xi=1.0, g=0.5, n_pair_states=8, n_particles=8, load_v_pppp=True,
-                      tables=False)
+                      tables=False, v_blocks=True)
     kind, kw = cli.system_spec(cli.parse_args("--electronGas -r 1 -s 19 -p 2 -m 1".split()))
     assert kind == "electron_gas" and kw["load_v_pppp"] is False  # saveMemory: V on the device
+    assert kw["v_blocks"] is False
 
 
 def test_batch_file_lines_on_top_of_command_line(tmp_path):

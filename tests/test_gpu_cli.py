@@ -32,6 +32,18 @@ def test_cli_reproduces_reference_energy(name):
     assert abs(v["iterations"][0] - len(g["energies"])) <= 1
 
 
+@pytest.mark.parametrize("name", ["eg14_s19", "pairing_gp0.5"])
+def test_cli_save_memory_mode(name):
+    """-m 1 (saveMemory): no V block from the host, every one generated on the device."""
+    g = golden(name)
+    buf = io.StringIO()
+    assert cli.main(str(g["cli"]).split() + ["-m", "1", "-v", "1"], out=buf) == 0
+    v = _values(buf.getvalue())
+    ref = float(g["energies"][-1])
+    assert abs(v["CCDCorr"][0] - ref) <= 1e-10 * abs(ref)
+    assert abs(v["MBPT2Corr"][0] - float(g["scalars"][1])) <= 1e-12 * abs(g["scalars"][1])
+
+
 def test_cli_batch_and_restart(tmp_path):
     eg, pnm = golden("eg14_s19"), golden("pnm14_s4")
     bf = tmp_path / "sweep.txt"
