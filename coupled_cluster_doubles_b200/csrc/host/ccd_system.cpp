@@ -239,12 +239,22 @@ int finish(ccdhost_system *s, int32_t flags) {
   // Channel dimensions in unpermuted order (SPBasis.cpp:80-179).
   std::vector<ccdgpu_channel_dims> d0(nch, ccdgpu_channel_dims{0, 0, 0, 0}), md0 = d0;
   std::vector<uint32_t> c0(nsp * nsp), mc0(nsp * nsp);
-  for (uint64_t p = 0; p < nsp; p++)
+  int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+  for (int64_t p = 0; p < (int64_t)nsp; p++)
     for (uint64_t q = 0; q < nsp; q++) {
-      uint64_t c = m.chan0(p, q), mc = m.mod0(p, q);
-      if (c >= nch || mc >= nch) return CCDGPU_ERR_INVALID_ARGUMENT;
+      const uint64_t c = m.chan0(p, q), mc = m.mod0(p, q);
+      if (c >= nch || mc >= nch) {
+        bad = 1;
+        continue;
+      }
       c0[p * nsp + q] = (uint32_t)c;
       mc0[p * nsp + q] = (uint32_t)mc;
+    }
+  if (bad) return CCDGPU_ERR_INVALID_ARGUMENT;
+  for (uint64_t p = 0; p < nsp; p++)
+    for (uint64_t q = 0; q < nsp; q++) {
+      const uint64_t c = c0[p * nsp + q], mc = mc0[p * nsp + q];
       bool ph = p < np, qh = q < np;
       if (ph && qh) { d0[c].hh++; md0[mc].hh++; }
       else if (ph) { d0[c].hp++; md0[mc].hp++; }
@@ -292,32 +302,56 @@ int finish(ccdhost_system *s, int32_t flags) {
   s->ph_all.resize(off_ph[nch]); s->hp_all.resize(off_hp[nch]);
   s->mpp_all.resize(moff_pp[nch]); s->mhh_all.resize(moff_hh[nch]);
   s->mph_all.resize(moff_ph[nch]); s->mhp_all.resize(moff_hp[nch]);
-  std::vector<uint64_t> fill(nch * 4, 0), mfill(nch * 4, 0);
+  // Kind of a pair: 0 pp, 1 hh, 2 hp, 3 ph.  The lists are filled in parallel over contiguous
+  // ranges of p: pass 1 counts each range's pairs per (channel, kind), exclusive sums over the
+  // ranges give each range its start inside every list, pass 2 places the pairs.  Ranges in
+  // ascending p keep every list in (p, q) order, as the sequential scan would.
+  auto kind_of = [&](uint64_t p, uint64_t q) { return p < np ? (q < np ? 1 : 2) : (q < np ? 3 : 0); };
+  ccdgpu_pair *lists[4] = {s->pp_all.data(), s->hh_all.data(), s->hp_all.data(), s->ph_all.data()};
+  ccdgpu_pair *mlists[4] = {s->mpp_all.data(), s->mhh_all.data(), s->mhp_all.data(), s->mph_all.data()};
+  const uint64_t *offs[4] = {off_pp.data(), off_hh.data(), off_hp.data(), off_ph.data()};
+  const uint64_t *moffs[4] = {moff_pp.data(), moff_hh.data(), moff_hp.data(), moff_ph.data()};
   std::vector<uint32_t> pos(nsp * nsp), mpos(nsp * nsp), chan(nsp * nsp), mchan(nsp * nsp);
-  for (uint64_t p = 0; p < nsp; p++)
-    for (uint64_t q = 0; q < nsp; q++) {
-      uint64_t c = inv[c0[p * nsp + q]], mc = inv[mc0[p * nsp + q]];
-      chan[p * nsp + q] = (uint32_t)c;
-      mchan[p * nsp + q] = (uint32_t)mc;
-      bool ph = p < np, qh = q < np;
-      ccdgpu_pair pr{p, q};
-      uint64_t k, mk;
-      if (ph && qh) {
-        k = fill[c * 4 + 1]++; s->hh_all[off_hh[c] + k] = pr;
-        mk = mfill[mc * 4 + 1]++; s->mhh_all[moff_hh[mc] + mk] = pr;
-      } else if (ph) {
-        k = fill[c * 4 + 2]++; s->hp_all[off_hp[c] + k] = pr;
-        mk = mfill[mc * 4 + 2]++; s->mhp_all[moff_hp[mc] + mk] = pr;
-      } else if (qh) {
-        k = fill[c * 4 + 3]++; s->ph_all[off_ph[c] + k] = pr;
-        mk = mfill[mc * 4 + 3]++; s->mph_all[moff_ph[mc] + mk] = pr;
-      } else {
-        k = fill[c * 4 + 0]++; s->pp_all[off_pp[c] + k] = pr;
-        mk = mfill[mc * 4 + 0]++; s->mpp_all[moff_pp[mc] + mk] = pr;
+  const int nrange = (int)std::max<uint64_t>(1, std::min<uint64_t>(nsp, omp_get_max_threads()));
+  std::vector<uint32_t> cnt((size_t)nrange * nch * 4, 0), mcnt((size_t)nrange * nch * 4, 0);
+  auto p_begin = [&](int r) { return nsp * (uint64_t)r / (uint64_t)nrange; };
+#pragma omp parallel for schedule(static)
+  for (int r = 0; r < nrange; r++) {
+    uint32_t *ct = &cnt[(size_t)r * nch * 4], *mct = &mcnt[(size_t)r * nch * 4];
+    for (uint64_t p = p_begin(r); p < p_begin(r + 1); p++)
+      for (uint64_t q = 0; q < nsp; q++) {
+        const int k = kind_of(p, q);
+        ct[inv[c0[p * nsp + q]] * 4 + k]++;
+        mct[inv[mc0[p * nsp + q]] * 4 + k]++;
       }
-      pos[p * nsp + q] = (uint32_t)k;
-      mpos[p * nsp + q] = (uint32_t)mk;
+  }
+#pragma omp parallel for schedule(static)
+  for (int64_t e = 0; e < (int64_t)(nch * 4); e++) {
+    uint32_t a = 0, b = 0;
+    for (int r = 0; r < nrange; r++) {
+      const uint32_t x = cnt[(size_t)r * nch * 4 + e], y = mcnt[(size_t)r * nch * 4 + e];
+      cnt[(size_t)r * nch * 4 + e] = a;
+      mcnt[(size_t)r * nch * 4 + e] = b;
+      a += x;
+      b += y;
     }
+  }
+#pragma omp parallel for schedule(static)
+  for (int r = 0; r < nrange; r++) {
+    uint32_t *ct = &cnt[(size_t)r * nch * 4], *mct = &mcnt[(size_t)r * nch * 4];
+    for (uint64_t p = p_begin(r); p < p_begin(r + 1); p++)
+      for (uint64_t q = 0; q < nsp; q++) {
+        const uint64_t c = inv[c0[p * nsp + q]], mc = inv[mc0[p * nsp + q]];
+        const int kd = kind_of(p, q);
+        const uint32_t k = ct[c * 4 + kd]++, mk = mct[mc * 4 + kd]++;
+        lists[kd][offs[kd][c] + k] = ccdgpu_pair{p, q};
+        mlists[kd][moffs[kd][mc] + mk] = ccdgpu_pair{p, q};
+        chan[p * nsp + q] = (uint32_t)c;
+        mchan[p * nsp + q] = (uint32_t)mc;
+        pos[p * nsp + q] = k;
+        mpos[p * nsp + q] = mk;
+      }
+  }
   s->maps.resize(nch);
   s->mmaps.resize(nch);
   for (uint64_t c = 0; c < nch; c++) {
@@ -483,9 +517,12 @@ int finish(ccdhost_system *s, int32_t flags) {
     for (uint64_t c = 0; c < nch; c++)
       if (o_t[c + 1] > o_t[c]) s->tabptr[k][c] = &s->tab[k][o_t[c]];
 
-  // MBPT2 (MBPT2Corr.cpp:6-38), channel order, normal-ordered energies.
-  double e2 = 0.;
-  for (uint64_t c = 0; c < nch; c++) {
+  // MBPT2 (MBPT2Corr.cpp:6-38), normal-ordered energies: each channel's sum as the reference
+  // forms it (in parallel over channels), then the channel sums added in channel order.
+  std::vector<double> corr_c(nch, 0.0);
+#pragma omp parallel for schedule(dynamic)
+  for (int64_t ci = 0; ci < (int64_t)nch; ci++) {
+    const uint64_t c = ci;
     if (!s->dims[c].pp || !s->dims[c].hh) continue;
     const uint64_t pp = s->dims[c].pp, hh = s->dims[c].hh;
     const double *vx = s->vptr[1][c];  // NULL with CCDHOST_NO_V: the same elements, evaluated
@@ -497,8 +534,11 @@ int finish(ccdhost_system *s, int32_t flags) {
         double v = vx ? vx[x * pp + y] : s->m.tbme(H.p, H.q, P.p, P.q);
         corr += v * v / den;
       }
-    e2 += 0.25 * corr;
+    corr_c[c] = corr;
   }
+  double e2 = 0.;
+  for (uint64_t c = 0; c < nch; c++)
+    if (s->dims[c].pp && s->dims[c].hh) e2 += 0.25 * corr_c[c];
   s->mbpt2 = e2;
 
   // Model description for on-the-fly V.
