@@ -123,6 +123,7 @@ GPU_SYMBOLS = [
     "ccdgpu_trace_arm", "ccdgpu_trace_read", "ccdgpu_solve_batch", "ccdgpu_set_schedule",
     "ccdgpu_get_schedule", "ccdgpu_autotune", "ccdgpu_ladder_profile", "ccdgpu_kernel_profile",
     "ccdgpu_mbpt2", "ccdgpu_reference_energy", "ccdgpu_release_cached_memory",
+    "ccdgpu_build_channels",
 ]
 
 

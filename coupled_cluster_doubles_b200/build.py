@@ -32,20 +32,25 @@ def _sources(d, exts):
 
 
 def build_host(force=False):
+    """Links against libccdgpu.so (device channel construction), found next to it at run time."""
     out = os.path.join(HERE, "libccdhost.so")
     src = os.path.join(CSRC, "host", "ccd_system.cpp")
-    deps = [src, os.path.join(INC, "ccdhost.h"), os.path.join(INC, "ccdgpu.h")]
+    gpu = os.path.join(HERE, "libccdgpu.so")
+    deps = [src, gpu, os.path.join(CSRC, "host", "channel_order.h"),
+            os.path.join(INC, "ccdhost.h"), os.path.join(INC, "ccdgpu.h")]
     if not force and _newer(out, deps):
         return out
     subprocess.run([GXX, "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-Wall",
-                    "-I" + INC, src, "-o", out], check=True)
+                    "-I" + INC, "-I" + os.path.join(CSRC, "host"), src, "-o", out,
+                    "-L" + HERE, "-lccdgpu", "-Wl,-rpath,$ORIGIN"], check=True)
     return out
 
 
 def build_gpu(force=False, verbose=False):
     out = os.path.join(HERE, "libccdgpu.so")
     srcs = [os.path.join(CSRC, "ccdgpu.cu"), os.path.join(CSRC, "ccd_noalloc.cu")]
-    deps = _sources(CSRC, (".cu", ".cuh")) + [os.path.join(INC, "ccdgpu.h")]
+    deps = _sources(CSRC, (".cu", ".cuh")) + [os.path.join(INC, "ccdgpu.h"),
+                                              os.path.join(CSRC, "host", "channel_order.h")]
     if not force and _newer(out, deps):
         return out
     cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
@@ -63,10 +68,11 @@ def build_gpu(force=False, verbose=False):
 
 
 def build_all(force=False):
-    return build_host(force), build_gpu(force)
+    gpu = build_gpu(force)
+    return build_host(force), gpu
 
 
 if __name__ == "__main__":
     import sys
-    print(build_host(force=True))
     print(build_gpu(force=True, verbose="-v" in sys.argv))
+    print(build_host(force=True))

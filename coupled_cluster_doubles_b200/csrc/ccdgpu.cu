@@ -21,11 +21,13 @@
 #include <new>
 #include <vector>
 
+#include "ccd_channels.cuh"
 #include "ccd_device.cuh"
 #include "ccd_kernels.cuh"
 #include "ccd_setup.cuh"
 #include "ccd_tc.cuh"
 #include "ccdgpu.h"
+#include "host/channel_order.h"
 
 using namespace ccd;
 
@@ -1872,6 +1874,139 @@ int ccdgpu_reference_energy(ccdgpu_handle *h, const double *sp_energy_bare, doub
   *e_ref = out[nsp];
   if (sp_energy_normal) std::copy(out.begin(), out.begin() + nsp, sp_energy_normal);
   return CCDGPU_OK;
+}
+
+int ccdgpu_build_channels(const ccdgpu_channel_rule *rule, ccdgpu_channel_dims *dims,
+                          ccdgpu_channel_dims *mod_dims, ccdgpu_pair *const lists[4],
+                          ccdgpu_pair *const mod_lists[4], uint32_t *chan, uint32_t *mod_chan,
+                          uint32_t *pos, uint32_t *mod_pos) {
+  if (!rule || !rule->qn || !dims || !mod_dims || !lists || !mod_lists) return CCDGPU_ERR_INVALID_ARGUMENT;
+  const uint64_t nsp = rule->n_sp, np = rule->n_particles, nch = rule->n_channels;
+  if (np == 0 || np >= nsp || nch == 0 || rule->kind < CCDGPU_MODEL_PAIRING ||
+      rule->kind > CCDGPU_MODEL_ELECTRON_GAS ||
+      rule->qn_stride < (rule->kind == CCDGPU_MODEL_PAIRING ? 2 : 5) || rule->nmax < 0)
+    return CCDGPU_ERR_INVALID_ARGUMENT;
+  if (nsp > 65535 || nch * 4 >= (uint64_t(1) << 31)) return CCDGPU_ERR_UNSUPPORTED;
+  const uint64_t npart = nsp - np, n = nsp * nsp;
+  const uint64_t tot[4] = {npart * npart, np * np, np * npart, npart * np};  // pp, hh, hp, ph
+  for (int k = 0; k < 4; k++)
+    if (!lists[k] || !mod_lists[k]) return CCDGPU_ERR_INVALID_ARGUMENT;
+  if (rule->device >= 0) CK(cudaSetDevice(rule->device));
+  cudaStream_t st = nullptr;
+  CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  // One device block: qn, the per-pair arrays and the per-(channel, kind) arrays.
+  size_t used = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = used;
+    used += (bytes + 255) & ~size_t(255);
+    return o;
+  };
+  const size_t o_qn = take(nsp * rule->qn_stride * 4), o_c0 = take(n * 4), o_mc0 = take(n * 4),
+               o_codes = take(n * 4), o_mcodes = take(n * 4), o_chan = take(n * 4),
+               o_mchan = take(n * 4), o_pos = take(n * 4), o_mpos = take(n * 4),
+               o_cnt = take(nch * 16), o_mcnt = take(nch * 16), o_fill = take(nch * 16),
+               o_mfill = take(nch * 16), o_err = take(4), o_zero_end = used,
+               o_inv = take(nch * 4), o_seg = take(nch * 16), o_mseg = take(nch * 16),
+               o_segs = take(nch * 8 * sizeof(PairSegment));
+  void *base = nullptr;
+  size_t got = 0;
+  int rc = CCDGPU_OK;
+  std::vector<uint32_t> cnt(nch * 4), mcnt(nch * 4);
+  std::vector<uint32_t> inv(nch), seg(nch * 4), mseg(nch * 4), codes(n), mcodes(n);
+  std::vector<PairSegment> segs;
+  int32_t err = 0;
+  auto at = [&](size_t o) { return static_cast<char *>(base) + o; };
+  auto run = [&]() -> int {
+    CK(dev_alloc(used, &base, &got));
+    CK(cudaMemsetAsync(at(o_cnt), 0, o_zero_end - o_cnt, st));
+    CK(cudaMemcpyAsync(at(o_qn), rule->qn, nsp * rule->qn_stride * 4, cudaMemcpyHostToDevice, st));
+    ChannelRuleDev r{reinterpret_cast<const int32_t *>(at(o_qn)), rule->kind, rule->qn_stride,
+                     rule->nmax, rule->chan_tz_max, rule->mod_chan_tz_max, nsp, np, nch};
+    const unsigned grid = (unsigned)std::min<uint64_t>((n + 255) / 256, 148 * 16);
+    uint32_t *c0 = reinterpret_cast<uint32_t *>(at(o_c0)), *mc0 = reinterpret_cast<uint32_t *>(at(o_mc0));
+    pair_channel_kernel<<<grid, 256, 0, st>>>(r, c0, mc0, reinterpret_cast<uint32_t *>(at(o_cnt)),
+                                               reinterpret_cast<uint32_t *>(at(o_mcnt)),
+                                               reinterpret_cast<int32_t *>(at(o_err)));
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(cnt.data(), at(o_cnt), nch * 16, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(mcnt.data(), at(o_mcnt), nch * 16, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&err, at(o_err), 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (err) return CCDGPU_ERR_INVALID_ARGUMENT;  // a pair outside the channel slots
+    // Channel order, dimensions and segment starts (kinds one after another).
+    std::vector<ccdgpu_channel_dims> d0(nch), md0(nch);
+    for (uint64_t c = 0; c < nch; c++) {
+      d0[c] = {cnt[c * 4 + 0], cnt[c * 4 + 1], cnt[c * 4 + 2], cnt[c * 4 + 3]};
+      md0[c] = {mcnt[c * 4 + 0], mcnt[c * 4 + 1], mcnt[c * 4 + 2], mcnt[c * 4 + 3]};
+    }
+    const std::vector<uint64_t> order = ffd_channel_order(d0);
+    for (uint64_t i = 0; i < nch; i++) {
+      inv[order[i]] = (uint32_t)i;
+      dims[i] = d0[order[i]];
+      mod_dims[i] = md0[order[i]];
+    }
+    uint64_t base_k = 0;
+    for (int k = 0; k < 4; k++) {
+      uint64_t o = base_k, mo = base_k;
+      for (uint64_t i = 0; i < nch; i++) {
+        const uint64_t len = (&dims[i].pp)[k], mlen = (&mod_dims[i].pp)[k];
+        if (len > (uint64_t)kMaxSegment || mlen > (uint64_t)kMaxSegment) return CCDGPU_ERR_UNSUPPORTED;
+        seg[i * 4 + k] = (uint32_t)o;
+        mseg[i * 4 + k] = (uint32_t)mo;
+        if (len) segs.push_back(PairSegment{(uint32_t)o, (uint32_t)len, 0, 0});
+        if (mlen) segs.push_back(PairSegment{(uint32_t)mo, (uint32_t)mlen, 1, 0});
+        o += len;
+        mo += mlen;
+      }
+      if (o - base_k != tot[k] || mo - base_k != tot[k]) return CCDGPU_ERR_INVALID_ARGUMENT;
+      base_k += tot[k];
+    }
+    if (segs.size() > nch * 8) return CCDGPU_ERR_INVALID_ARGUMENT;
+    CK(cudaMemcpyAsync(at(o_inv), inv.data(), nch * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(at(o_seg), seg.data(), nch * 16, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(at(o_mseg), mseg.data(), nch * 16, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(at(o_segs), segs.data(), segs.size() * sizeof(PairSegment),
+                       cudaMemcpyHostToDevice, st));
+    uint32_t *codes_d = reinterpret_cast<uint32_t *>(at(o_codes));
+    uint32_t *mcodes_d = reinterpret_cast<uint32_t *>(at(o_mcodes));
+    place_pairs_kernel<<<grid, 256, 0, st>>>(
+        nsp, np, c0, mc0, reinterpret_cast<const uint32_t *>(at(o_inv)),
+        reinterpret_cast<const uint32_t *>(at(o_seg)), reinterpret_cast<const uint32_t *>(at(o_mseg)),
+        reinterpret_cast<uint32_t *>(at(o_fill)), reinterpret_cast<uint32_t *>(at(o_mfill)),
+        codes_d, mcodes_d, reinterpret_cast<uint32_t *>(at(o_chan)),
+        reinterpret_cast<uint32_t *>(at(o_mchan)));
+    CK(cudaGetLastError());
+    if (!segs.empty()) {
+      sort_segments_kernel<<<(unsigned)segs.size(), 512, 0, st>>>(
+          reinterpret_cast<const PairSegment *>(at(o_segs)), codes_d, mcodes_d,
+          reinterpret_cast<uint32_t *>(at(o_pos)), reinterpret_cast<uint32_t *>(at(o_mpos)));
+      CK(cudaGetLastError());
+    }
+    CK(cudaMemcpyAsync(codes.data(), codes_d, n * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(mcodes.data(), mcodes_d, n * 4, cudaMemcpyDeviceToHost, st));
+    if (chan) CK(cudaMemcpyAsync(chan, at(o_chan), n * 4, cudaMemcpyDeviceToHost, st));
+    if (mod_chan) CK(cudaMemcpyAsync(mod_chan, at(o_mchan), n * 4, cudaMemcpyDeviceToHost, st));
+    if (pos) CK(cudaMemcpyAsync(pos, at(o_pos), n * 4, cudaMemcpyDeviceToHost, st));
+    if (mod_pos) CK(cudaMemcpyAsync(mod_pos, at(o_mpos), n * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // Codes -> pairs.
+    uint64_t kb[4] = {0, tot[0], tot[0] + tot[1], tot[0] + tot[1] + tot[2]};
+    for (int k = 0; k < 4; k++) {
+#pragma omp parallel for schedule(static)
+      for (int64_t j = 0; j < (int64_t)tot[k]; j++) {
+        const uint32_t x = codes[kb[k] + j], y = mcodes[kb[k] + j];
+        lists[k][j] = ccdgpu_pair{x / nsp, x % nsp};
+        mod_lists[k][j] = ccdgpu_pair{y / nsp, y % nsp};
+      }
+    }
+    return CCDGPU_OK;
+  };
+  rc = run();
+  (void)cudaStreamSynchronize(st);
+  if (base) dev_free(base, got);
+  cudaStreamDestroy(st);
+  if (rc) (void)cudaGetLastError();
+  return rc;
 }
 
 int ccdgpu_get_t2(ccdgpu_handle *h, double *t2, uint64_t n) {

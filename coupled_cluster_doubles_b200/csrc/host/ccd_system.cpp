@@ -8,6 +8,7 @@
 // every matrix element is evaluated with the same floating-point expression as the reference,
 // so the blocks are bit-identical.
 #include "ccdhost.h"
+#include "channel_order.h"
 
 #include <omp.h>
 
@@ -236,121 +237,135 @@ int finish(ccdhost_system *s, int32_t flags) {
     s->eps[p] = e;
   }
 
-  // Channel dimensions in unpermuted order (SPBasis.cpp:80-179).
-  std::vector<ccdgpu_channel_dims> d0(nch, ccdgpu_channel_dims{0, 0, 0, 0}), md0 = d0;
-  std::vector<uint32_t> c0(nsp * nsp), mc0(nsp * nsp);
-  int bad = 0;
-#pragma omp parallel for schedule(static) reduction(| : bad)
-  for (int64_t p = 0; p < (int64_t)nsp; p++)
-    for (uint64_t q = 0; q < nsp; q++) {
-      const uint64_t c = m.chan0(p, q), mc = m.mod0(p, q);
-      if (c >= nch || mc >= nch) {
-        bad = 1;
-        continue;
-      }
-      c0[p * nsp + q] = (uint32_t)c;
-      mc0[p * nsp + q] = (uint32_t)mc;
-    }
-  if (bad) return CCDGPU_ERR_INVALID_ARGUMENT;
-  for (uint64_t p = 0; p < nsp; p++)
-    for (uint64_t q = 0; q < nsp; q++) {
-      const uint64_t c = c0[p * nsp + q], mc = mc0[p * nsp + q];
-      bool ph = p < np, qh = q < np;
-      if (ph && qh) { d0[c].hh++; md0[mc].hh++; }
-      else if (ph) { d0[c].hp++; md0[mc].hp++; }
-      else if (qh) { d0[c].ph++; md0[mc].ph++; }
-      else { d0[c].pp++; md0[mc].pp++; }
-    }
-
-  // 1-rank first-fit-decreasing order: cost descending, index ascending (main.cpp:94-115,
-  // balance.cpp:11-24,91-140).  Regular and modified channels share the permutation.
-  std::vector<std::pair<double, uint64_t>> load(nch);
-  for (uint64_t c = 0; c < nch; c++) {
-    double pp = d0[c].pp, hh = d0[c].hh, ph = d0[c].ph, hp = d0[c].hp;
-    double cost = 0;
-    cost += hh * hh; cost += hh * hp; cost += hh * pp; cost += hp * ph;
-    cost += hp * pp; cost += pp * pp; cost += hp * ph; cost += hp * hp;
-    load[c] = {cost, c};
-  }
-  std::sort(load.begin(), load.end(), [](const std::pair<double, uint64_t> &a,
-                                         const std::pair<double, uint64_t> &b) {
-    if (a.first != b.first) return a.first > b.first;
-    return a.second < b.second;
-  });
-  std::vector<uint32_t> inv(nch);
+  // Channels and their sorted maps (SPBasis.cpp:80-441), in the 1-rank first-fit-decreasing
+  // order: on the device with CCDHOST_DEVICE_CHANNELS (ccdgpu_build_channels), else here.
+  // pos[] = index of (p, q) inside its own list, chan[] = its permuted channel.
+  const uint64_t npart = nsp - np;
+  std::vector<uint32_t> pos(nsp * nsp), mpos(nsp * nsp), chan(nsp * nsp), mchan(nsp * nsp);
   s->dims.resize(nch);
   s->mdims.resize(nch);
-  for (uint64_t i = 0; i < nch; i++) {
-    inv[load[i].second] = (uint32_t)i;
-    s->dims[i] = d0[load[i].second];
-    s->mdims[i] = md0[load[i].second];
-  }
-
-  // Sorted channel maps (SPBasis.cpp:307-441): scanning p then q ascending appends each
-  // channel's pairs already in (p, q) order.  pos[] = index of (p, q) inside its own list.
+  // List offsets of every channel from the (permuted) dimensions; the lists sized to match.
   std::vector<uint64_t> off_pp(nch + 1, 0), off_hh(nch + 1, 0), off_ph(nch + 1, 0),
       off_hp(nch + 1, 0);
   std::vector<uint64_t> moff_pp(nch + 1, 0), moff_hh(nch + 1, 0), moff_ph(nch + 1, 0),
       moff_hp(nch + 1, 0);
-  for (uint64_t c = 0; c < nch; c++) {
-    off_pp[c + 1] = off_pp[c] + s->dims[c].pp; off_hh[c + 1] = off_hh[c] + s->dims[c].hh;
-    off_ph[c + 1] = off_ph[c] + s->dims[c].ph; off_hp[c + 1] = off_hp[c] + s->dims[c].hp;
-    moff_pp[c + 1] = moff_pp[c] + s->mdims[c].pp; moff_hh[c + 1] = moff_hh[c] + s->mdims[c].hh;
-    moff_ph[c + 1] = moff_ph[c] + s->mdims[c].ph; moff_hp[c + 1] = moff_hp[c] + s->mdims[c].hp;
-  }
-  s->pp_all.resize(off_pp[nch]); s->hh_all.resize(off_hh[nch]);
-  s->ph_all.resize(off_ph[nch]); s->hp_all.resize(off_hp[nch]);
-  s->mpp_all.resize(moff_pp[nch]); s->mhh_all.resize(moff_hh[nch]);
-  s->mph_all.resize(moff_ph[nch]); s->mhp_all.resize(moff_hp[nch]);
-  // Kind of a pair: 0 pp, 1 hh, 2 hp, 3 ph.  The lists are filled in parallel over contiguous
-  // ranges of p: pass 1 counts each range's pairs per (channel, kind), exclusive sums over the
-  // ranges give each range its start inside every list, pass 2 places the pairs.  Ranges in
-  // ascending p keep every list in (p, q) order, as the sequential scan would.
-  auto kind_of = [&](uint64_t p, uint64_t q) { return p < np ? (q < np ? 1 : 2) : (q < np ? 3 : 0); };
-  ccdgpu_pair *lists[4] = {s->pp_all.data(), s->hh_all.data(), s->hp_all.data(), s->ph_all.data()};
-  ccdgpu_pair *mlists[4] = {s->mpp_all.data(), s->mhh_all.data(), s->mhp_all.data(), s->mph_all.data()};
-  const uint64_t *offs[4] = {off_pp.data(), off_hh.data(), off_hp.data(), off_ph.data()};
-  const uint64_t *moffs[4] = {moff_pp.data(), moff_hh.data(), moff_hp.data(), moff_ph.data()};
-  std::vector<uint32_t> pos(nsp * nsp), mpos(nsp * nsp), chan(nsp * nsp), mchan(nsp * nsp);
-  const int nrange = (int)std::max<uint64_t>(1, std::min<uint64_t>(nsp, omp_get_max_threads()));
-  std::vector<uint32_t> cnt((size_t)nrange * nch * 4, 0), mcnt((size_t)nrange * nch * 4, 0);
-  auto p_begin = [&](int r) { return nsp * (uint64_t)r / (uint64_t)nrange; };
-#pragma omp parallel for schedule(static)
-  for (int r = 0; r < nrange; r++) {
-    uint32_t *ct = &cnt[(size_t)r * nch * 4], *mct = &mcnt[(size_t)r * nch * 4];
-    for (uint64_t p = p_begin(r); p < p_begin(r + 1); p++)
-      for (uint64_t q = 0; q < nsp; q++) {
-        const int k = kind_of(p, q);
-        ct[inv[c0[p * nsp + q]] * 4 + k]++;
-        mct[inv[mc0[p * nsp + q]] * 4 + k]++;
-      }
-  }
-#pragma omp parallel for schedule(static)
-  for (int64_t e = 0; e < (int64_t)(nch * 4); e++) {
-    uint32_t a = 0, b = 0;
-    for (int r = 0; r < nrange; r++) {
-      const uint32_t x = cnt[(size_t)r * nch * 4 + e], y = mcnt[(size_t)r * nch * 4 + e];
-      cnt[(size_t)r * nch * 4 + e] = a;
-      mcnt[(size_t)r * nch * 4 + e] = b;
-      a += x;
-      b += y;
+  auto set_offsets = [&]() {
+    for (uint64_t c = 0; c < nch; c++) {
+      off_pp[c + 1] = off_pp[c] + s->dims[c].pp; off_hh[c + 1] = off_hh[c] + s->dims[c].hh;
+      off_ph[c + 1] = off_ph[c] + s->dims[c].ph; off_hp[c + 1] = off_hp[c] + s->dims[c].hp;
+      moff_pp[c + 1] = moff_pp[c] + s->mdims[c].pp; moff_hh[c + 1] = moff_hh[c] + s->mdims[c].hh;
+      moff_ph[c + 1] = moff_ph[c] + s->mdims[c].ph; moff_hp[c + 1] = moff_hp[c] + s->mdims[c].hp;
     }
-  }
-#pragma omp parallel for schedule(static)
-  for (int r = 0; r < nrange; r++) {
-    uint32_t *ct = &cnt[(size_t)r * nch * 4], *mct = &mcnt[(size_t)r * nch * 4];
-    for (uint64_t p = p_begin(r); p < p_begin(r + 1); p++)
+    s->pp_all.resize(off_pp[nch]); s->hh_all.resize(off_hh[nch]);
+    s->ph_all.resize(off_ph[nch]); s->hp_all.resize(off_hp[nch]);
+    s->mpp_all.resize(moff_pp[nch]); s->mhh_all.resize(moff_hh[nch]);
+    s->mph_all.resize(moff_ph[nch]); s->mhp_all.resize(moff_hp[nch]);
+  };
+  if (flags & CCDHOST_DEVICE_CHANNELS) {
+    for (auto *v : {&s->pp_all, &s->mpp_all}) v->resize(npart * npart);
+    for (auto *v : {&s->hh_all, &s->mhh_all}) v->resize(np * np);
+    for (auto *v : {&s->hp_all, &s->mhp_all, &s->ph_all, &s->mph_all}) v->resize(np * npart);
+    ccdgpu_channel_rule rule{};
+    rule.kind = m.kind == kPairing ? CCDGPU_MODEL_PAIRING
+                : m.kind == kInfMatter ? CCDGPU_MODEL_INF_MATTER
+                                       : CCDGPU_MODEL_ELECTRON_GAS;
+    rule.qn_stride = m.stride;
+    rule.qn = m.qn.data();
+    rule.n_sp = nsp; rule.n_particles = np; rule.n_channels = nch;
+    rule.nmax = m.nmax; rule.chan_tz_max = m.chan_tz_max; rule.mod_chan_tz_max = m.mod_chan_tz_max;
+    rule.device = -1;  // the calling thread's current CUDA device
+    ccdgpu_pair *const dl[4] = {s->pp_all.data(), s->hh_all.data(), s->hp_all.data(), s->ph_all.data()};
+    ccdgpu_pair *const dml[4] = {s->mpp_all.data(), s->mhh_all.data(), s->mhp_all.data(), s->mph_all.data()};
+    const int rc = ccdgpu_build_channels(&rule, s->dims.data(), s->mdims.data(), dl, dml,
+                                         chan.data(), mchan.data(), pos.data(), mpos.data());
+    if (rc) return rc;
+    set_offsets();
+  } else {
+    // Channel dimensions in unpermuted order (SPBasis.cpp:80-179).
+    std::vector<ccdgpu_channel_dims> d0(nch, ccdgpu_channel_dims{0, 0, 0, 0}), md0 = d0;
+    std::vector<uint32_t> c0(nsp * nsp), mc0(nsp * nsp);
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (int64_t p = 0; p < (int64_t)nsp; p++)
       for (uint64_t q = 0; q < nsp; q++) {
-        const uint64_t c = inv[c0[p * nsp + q]], mc = inv[mc0[p * nsp + q]];
-        const int kd = kind_of(p, q);
-        const uint32_t k = ct[c * 4 + kd]++, mk = mct[mc * 4 + kd]++;
-        lists[kd][offs[kd][c] + k] = ccdgpu_pair{p, q};
-        mlists[kd][moffs[kd][mc] + mk] = ccdgpu_pair{p, q};
-        chan[p * nsp + q] = (uint32_t)c;
-        mchan[p * nsp + q] = (uint32_t)mc;
-        pos[p * nsp + q] = k;
-        mpos[p * nsp + q] = mk;
+        const uint64_t c = m.chan0(p, q), mc = m.mod0(p, q);
+        if (c >= nch || mc >= nch) {
+          bad = 1;
+          continue;
+        }
+        c0[p * nsp + q] = (uint32_t)c;
+        mc0[p * nsp + q] = (uint32_t)mc;
       }
+    if (bad) return CCDGPU_ERR_INVALID_ARGUMENT;
+    for (uint64_t p = 0; p < nsp; p++)
+      for (uint64_t q = 0; q < nsp; q++) {
+        const uint64_t c = c0[p * nsp + q], mc = mc0[p * nsp + q];
+        bool ph = p < np, qh = q < np;
+        if (ph && qh) { d0[c].hh++; md0[mc].hh++; }
+        else if (ph) { d0[c].hp++; md0[mc].hp++; }
+        else if (qh) { d0[c].ph++; md0[mc].ph++; }
+        else { d0[c].pp++; md0[mc].pp++; }
+      }
+
+    // 1-rank first-fit-decreasing order (shared with the device construction).
+    const std::vector<uint64_t> order = ffd_channel_order(d0);
+    std::vector<uint32_t> inv(nch);
+    for (uint64_t i = 0; i < nch; i++) {
+      inv[order[i]] = (uint32_t)i;
+      s->dims[i] = d0[order[i]];
+      s->mdims[i] = md0[order[i]];
+    }
+
+    set_offsets();
+    // Kind of a pair: 0 pp, 1 hh, 2 hp, 3 ph.  The lists are filled in parallel over contiguous
+    // ranges of p: pass 1 counts each range's pairs per (channel, kind), exclusive sums over the
+    // ranges give each range its start inside every list, pass 2 places the pairs.  Ranges in
+    // ascending p keep every list in (p, q) order, as the sequential scan would.
+    auto kind_of = [&](uint64_t p, uint64_t q) { return p < np ? (q < np ? 1 : 2) : (q < np ? 3 : 0); };
+    ccdgpu_pair *lists[4] = {s->pp_all.data(), s->hh_all.data(), s->hp_all.data(), s->ph_all.data()};
+    ccdgpu_pair *mlists[4] = {s->mpp_all.data(), s->mhh_all.data(), s->mhp_all.data(), s->mph_all.data()};
+    const uint64_t *offs[4] = {off_pp.data(), off_hh.data(), off_hp.data(), off_ph.data()};
+    const uint64_t *moffs[4] = {moff_pp.data(), moff_hh.data(), moff_hp.data(), moff_ph.data()};
+    const int nrange = (int)std::max<uint64_t>(1, std::min<uint64_t>(nsp, omp_get_max_threads()));
+    std::vector<uint32_t> cnt((size_t)nrange * nch * 4, 0), mcnt((size_t)nrange * nch * 4, 0);
+    auto p_begin = [&](int r) { return nsp * (uint64_t)r / (uint64_t)nrange; };
+#pragma omp parallel for schedule(static)
+    for (int r = 0; r < nrange; r++) {
+      uint32_t *ct = &cnt[(size_t)r * nch * 4], *mct = &mcnt[(size_t)r * nch * 4];
+      for (uint64_t p = p_begin(r); p < p_begin(r + 1); p++)
+        for (uint64_t q = 0; q < nsp; q++) {
+          const int k = kind_of(p, q);
+          ct[inv[c0[p * nsp + q]] * 4 + k]++;
+          mct[inv[mc0[p * nsp + q]] * 4 + k]++;
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < (int64_t)(nch * 4); e++) {
+      uint32_t a = 0, b = 0;
+      for (int r = 0; r < nrange; r++) {
+        const uint32_t x = cnt[(size_t)r * nch * 4 + e], y = mcnt[(size_t)r * nch * 4 + e];
+        cnt[(size_t)r * nch * 4 + e] = a;
+        mcnt[(size_t)r * nch * 4 + e] = b;
+        a += x;
+        b += y;
+      }
+    }
+#pragma omp parallel for schedule(static)
+    for (int r = 0; r < nrange; r++) {
+      uint32_t *ct = &cnt[(size_t)r * nch * 4], *mct = &mcnt[(size_t)r * nch * 4];
+      for (uint64_t p = p_begin(r); p < p_begin(r + 1); p++)
+        for (uint64_t q = 0; q < nsp; q++) {
+          const uint64_t c = inv[c0[p * nsp + q]], mc = inv[mc0[p * nsp + q]];
+          const int kd = kind_of(p, q);
+          const uint32_t k = ct[c * 4 + kd]++, mk = mct[mc * 4 + kd]++;
+          lists[kd][offs[kd][c] + k] = ccdgpu_pair{p, q};
+          mlists[kd][moffs[kd][mc] + mk] = ccdgpu_pair{p, q};
+          chan[p * nsp + q] = (uint32_t)c;
+          mchan[p * nsp + q] = (uint32_t)mc;
+          pos[p * nsp + q] = k;
+          mpos[p * nsp + q] = mk;
+        }
+    }
   }
   s->maps.resize(nch);
   s->mmaps.resize(nch);
@@ -376,7 +391,6 @@ int finish(ccdhost_system *s, int32_t flags) {
     s->tdims[k].hpp = n;
     s->hpp_off_map[k + 1] = s->hpp_off_map[k] + n;
   }
-  const uint64_t npart = nsp - np;
   s->phh_off_map.assign(npart + 1, 0);
   for (uint64_t a = np; a < nsp; a++) {
     uint64_t n = 0;

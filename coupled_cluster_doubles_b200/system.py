@@ -23,15 +23,16 @@ class BuildError(RuntimeError):
     pass
 
 
-LOAD_V_PPPP, NO_TABLES, NO_V = 1, 2, 4  # ccdhost_flags
+LOAD_V_PPPP, NO_TABLES, NO_V, DEVICE_CHANNELS = 1, 2, 4, 8  # ccdhost_flags
 
 
-def _flags(load_v_pppp, tables, v_blocks=True):
+def _flags(load_v_pppp, tables, v_blocks=True, device_channels=False):
     """Builder flags: V_pppp built on the host or not; remap tables built on the host, or left
     to ccdgpu_create, which then derives them on the device; with v_blocks=False no V block at
-    all (ccdgpu_create generates them on the device; the solver needs v_mode="on_the_fly")."""
+    all (ccdgpu_create generates them on the device; the solver needs v_mode="on_the_fly");
+    device_channels=True builds the channel dimensions and maps on the current CUDA device."""
     return ((LOAD_V_PPPP if load_v_pppp else 0) | (0 if tables else NO_TABLES) |
-            (0 if v_blocks else NO_V))
+            (0 if v_blocks else NO_V) | (DEVICE_CHANNELS if device_channels else 0))
 
 
 class System:
@@ -59,28 +60,30 @@ class System:
 
     @classmethod
     def pairing(cls, xi=1.0, g=0.5, n_pair_states=4, n_particles=4, load_v_pppp=True,
-                tables=True, v_blocks=True):
+                tables=True, v_blocks=True, device_channels=False):
         return cls._build("ccdhost_build_pairing", float(xi), float(g), int(n_pair_states),
-                          int(n_particles), _flags(load_v_pppp, tables, v_blocks),
+                          int(n_particles),
+                          _flags(load_v_pppp, tables, v_blocks, device_channels),
                           kind="pairing",
                           params=dict(xi=xi, g=g, n_pair_states=n_pair_states,
                                       n_particles=n_particles))
 
     @classmethod
     def inf_matter(cls, density=0.08, tz_max=1, n_shells=4, n_particle_shells=2,
-                   load_v_pppp=True, tables=True, v_blocks=True):
+                   load_v_pppp=True, tables=True, v_blocks=True, device_channels=False):
         return cls._build("ccdhost_build_inf_matter", float(density), int(tz_max),
                           int(n_shells), int(n_particle_shells),
-                          _flags(load_v_pppp, tables, v_blocks),
+                          _flags(load_v_pppp, tables, v_blocks, device_channels),
                           kind="inf_matter",
                           params=dict(density=density, tz_max=tz_max, n_shells=n_shells,
                                       n_particle_shells=n_particle_shells))
 
     @classmethod
     def electron_gas(cls, r_s=0.5, n_shells=4, n_particle_shells=2, load_v_pppp=True,
-                     tables=True, v_blocks=True):
+                     tables=True, v_blocks=True, device_channels=False):
         return cls._build("ccdhost_build_electron_gas", float(r_s), int(n_shells),
-                          int(n_particle_shells), _flags(load_v_pppp, tables, v_blocks),
+                          int(n_particle_shells),
+                          _flags(load_v_pppp, tables, v_blocks, device_channels),
                           kind="electron_gas",
                           params=dict(r_s=r_s, n_shells=n_shells,
                                       n_particle_shells=n_particle_shells))

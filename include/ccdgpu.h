@@ -68,6 +68,20 @@ typedef struct ccdgpu_model {
   double params[8];             /* EG: {L, e_sq}; PNM: {L}; pairing: {g} */
 } ccdgpu_model;
 
+/* Channel numbering of a basis (the inputs of SPBasis::setUpChannelDims / setUpChannelMaps,
+ * SPBasis.cpp:80-441): orbital quantum numbers and the channel index rule of the model. */
+typedef struct ccdgpu_channel_rule {
+  int32_t kind;                 /* ccdgpu_model_kind */
+  int32_t qn_stride;            /* ints per orbital in qn (5 for plane waves, 2 for pairing) */
+  const int32_t *qn;            /* [n_sp * qn_stride]: SPBasis::indexMap rows */
+  uint64_t n_sp, n_particles;   /* orbitals; the first n_particles are holes */
+  uint64_t n_channels;          /* channel slots (SPBasis::nChannels) */
+  int32_t nmax;                 /* largest |n_x|, |n_y|, |n_z| of the basis (plane waves) */
+  int32_t chan_tz_max;          /* T_z rule of regular channels (-2: one T_z, 2: three) */
+  int32_t mod_chan_tz_max;      /* T_z rule of modified channels (0: one T_z, 2: three) */
+  int32_t device;               /* CUDA device, < 0: the calling thread's current device */
+} ccdgpu_channel_rule;
+
 typedef struct ccdgpu_problem {
   uint64_t n_sp;                /* SPBasis::nSpstates; orbitals < n_particles are holes */
   uint64_t n_particles;         /* SPBasis::nParticles */
@@ -184,6 +198,19 @@ int ccdgpu_mbpt2(ccdgpu_handle *h, int32_t init_t2, double *e_mbpt2);
  * (CCDGPU_ERR_UNSUPPORTED without it); the handle's own energies are not changed. */
 int ccdgpu_reference_energy(ccdgpu_handle *h, const double *sp_energy_bare, double *e_ref,
                             double *sp_energy_normal);
+/* Channel construction on the device (SPBasis.cpp:80-441 with the one-rank ffdBalance order of
+ * main.cpp:94-115 and balance.cpp:91-144): the regular and modified channel dimensions in
+ * permuted order and their pair lists, each sorted by (p, q), for every ordered orbital pair.
+ * lists[k] / mod_lists[k] hold kind k = pp, hh, hp, ph for all channels one after another in
+ * permuted order: npart^2, A^2, A*npart and npart*A pairs (A = n_particles, npart = n_sp - A).
+ * chan / mod_chan / pos / mod_pos (optional, n_sp^2 each, index p * n_sp + q) receive the
+ * permuted channel of every pair and its index inside its channel's list.  Returns
+ * CCDGPU_ERR_UNSUPPORTED when one channel holds more than 8192 pairs of one kind or n_sp^2
+ * does not fit 32 bits. */
+int ccdgpu_build_channels(const ccdgpu_channel_rule *rule, ccdgpu_channel_dims *dims,
+                          ccdgpu_channel_dims *mod_dims, ccdgpu_pair *const lists[4],
+                          ccdgpu_pair *const mod_lists[4], uint32_t *chan, uint32_t *mod_chan,
+                          uint32_t *pos, uint32_t *mod_pos);
 uint64_t ccdgpu_t2_size(const ccdgpu_handle *h);
 
 /* One CCD iteration (main.cpp:589-670) with the path and precision chosen at create time.

@@ -35,10 +35,12 @@ enum ccdhost_flags {
   CCDHOST_LOAD_V_PPPP = 1, /* build and pass V_pppp (off: the solver generates it, saveMemory) */
   CCDHOST_NO_TABLES = 2,   /* build no loadMaps remap tables: ccdgpu_problem.maps[] are NULL
                               and ccdgpu_create derives the tables on the device */
-  CCDHOST_NO_V = 4         /* build no V blocks at all (CCDHOST_LOAD_V_PPPP is ignored): every
+  CCDHOST_NO_V = 4,        /* build no V blocks at all (CCDHOST_LOAD_V_PPPP is ignored): every
                               ccdgpu_problem.v_* is NULL and ccdgpu_create generates them on
                               the device from the model (V_pppp needs CCDGPU_V_ON_THE_FLY;
                               without the three-body V only the fused path runs) */
+  CCDHOST_DEVICE_CHANNELS = 8 /* channel dimensions and maps built on the current CUDA device
+                              (ccdgpu_build_channels) instead of on the host */
 };
 
 /* --pairing -l n_pair_states -n n_particles -x xi -g g  (parse.cpp:232-234) */
