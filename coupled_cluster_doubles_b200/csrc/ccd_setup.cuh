@@ -165,6 +165,37 @@ __global__ void gen_v_pphh_kernel(const ElemRange *__restrict__ ranges,
   }
 }
 
+// The three-body V of the table path (load.cpp:241-273): vnn_h_hpp[k][(j,a,b)] = <kj|v|ab>
+// over (a, b) in pp(ch(k, j)), vnn_phh_p[a][(b,i,j)] = <ij|v|ab> over (i, j) in hh(ch(a, b)),
+// the blocks of hpp(k) and phh(a) ordered by j and b (offsets hblk, pblk of the table
+// derivation).  One CTA per active channel: its hh pairs (k, j) with its pp pairs, and its pp
+// pairs (a, b) with its hh pairs.  A position outside its chain (three-body dimensions that do
+// not match the channel maps) is not written and sets kErrBadIndex.
+__global__ void gen_v3_kernel(const ChanInfo *__restrict__ chans, const int2 *__restrict__ pp_pairs,
+                              const int2 *__restrict__ hh_pairs, ModelDev m,
+                              const int64_t *__restrict__ o_h, const int64_t *__restrict__ o_p,
+                              const int32_t *__restrict__ hblk, const int32_t *__restrict__ pblk,
+                              int np, int npart, double *__restrict__ v_h_hpp,
+                              double *__restrict__ v_phh_p, int32_t *err) {
+  const ChanInfo ch = chans[blockIdx.x];
+  const int n1 = ch.hh * ch.pp;
+  for (int e = threadIdx.x; e < n1; e += blockDim.x) {
+    const int x = e / ch.pp, ab = e - x * ch.pp;
+    const int2 kj = hh_pairs[ch.hh_off + x], pab = pp_pairs[ch.pp_off + ab];
+    const int64_t f = o_h[kj.x] + hblk[(int64_t)kj.x * np + kj.y] + ab;
+    if (f < o_h[kj.x + 1]) v_h_hpp[f] = tbme_dev(m, kj.x, kj.y, pab.x, pab.y);
+    else atomicOr(err, kErrBadIndex);
+  }
+  for (int e = threadIdx.x; e < n1; e += blockDim.x) {
+    const int y = e / ch.hh, ij = e - y * ch.hh;
+    const int2 pab = pp_pairs[ch.pp_off + y], pij = hh_pairs[ch.hh_off + ij];
+    const int a = pab.x - np, b = pab.y - np;
+    const int64_t f = o_p[a] + pblk[(int64_t)a * npart + b] + ij;
+    if (f < o_p[a + 1]) v_phh_p[f] = tbme_dev(m, pij.x, pij.y, pab.x, pab.y);
+    else atomicOr(err, kErrBadIndex);
+  }
+}
+
 // Per active modified channel (channel order): its block offsets and where its ph' pairs (b, j)
 // and hp' pairs (i, a) start in the pair arrays.
 struct ModGen {

@@ -898,7 +898,10 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   h->n_h = o_h[np];
   h->n_p = o_p[h->npart];
   if (h->n_h != n_t || h->n_p != n_t) return CCDGPU_ERR_BAD_TABLE;
-  h->have_3body = P->v_h_hpp && P->v_phh_p;
+  // Three-body V of the table path: from the host, or generated with the other V blocks when
+  // the problem carries none of them.
+  const bool gen_v3 = gen_v && !P->v_h_hpp && !P->v_phh_p;
+  h->have_3body = (P->v_h_hpp && P->v_phh_p) || gen_v3;
 
   h->host_chans = chans;
 
@@ -1043,11 +1046,13 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
         m.z = (int)c; m.w = (int)k;
       }
     }
-    sc.add(&d_hblk, np * np);
-    sc.add(&d_pblk, npart * npart);
     sc.add(&d_mlook, mlook.size());
   } else {
     sc.add(&raw_idx, (size_t)8 * n_t);
+  }
+  if (derive_tables || gen_v3) {  // block offsets inside hpp(k) and phh(a)
+    sc.add(&d_hblk, np * np);
+    sc.add(&d_pblk, (nsp - np) * (nsp - np));
   }
   ModGen *d_mod_gen = nullptr;
   int2 *d_mod_ph = nullptr, *d_mod_hp = nullptr;
@@ -1163,7 +1168,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     }
     TRY(upload_runs(h, hpph_raw, src_hpph, cnt_hpph));
     TRY(upload_runs(h, h->v_hphp, src_hphp, cnt_hphp));
-    if (h->have_3body) {
+    if (h->have_3body && !gen_v3) {
       std::vector<const double *> s5, s6;
       std::vector<int64_t> n5, n6;
       for (uint64_t k = 0; k < np; k++) {
@@ -1201,7 +1206,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
                                                             h->v_pphh);
     }
     CK(cudaGetLastError());
-    if (derive_tables) {
+    if (derive_tables || gen_v3) {
       pair_sizes_kernel<<<(unsigned)chans.size(), 256, 0, h->s0>>>(
           h->chans, h->pp_pairs, h->hh_pairs, (int)np, (int)h->npart, d_hblk, d_pblk);
       CK(cudaGetLastError());
@@ -1209,6 +1214,14 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
       CK(cudaGetLastError());
       row_scan_kernel<<<(unsigned)h->npart, 256, 0, h->s0>>>(d_pblk, (int)h->npart);
       CK(cudaGetLastError());
+    }
+    if (gen_v3) {
+      gen_v3_kernel<<<(unsigned)chans.size(), 256, 0, h->s0>>>(
+          h->chans, h->pp_pairs, h->hh_pairs, md, h->o_h, h->o_p, d_hblk, d_pblk, (int)np,
+          (int)h->npart, h->v_h_hpp, h->v_phh_p, h->err);
+      CK(cudaGetLastError());
+    }
+    if (derive_tables) {
       DeriveGeometry dg{h->o_h, h->o_p, d_o_m, d_mod_dims, d_hblk, d_pblk, d_mlook,
                         (int32_t)np, (int32_t)h->npart};
       derive_tables_kernel<<<h->n_ranges, 256, 0, h->s0>>>(h->ranges, h->chans, h->pp_pairs,

@@ -68,3 +68,20 @@ def test_nothing_but_structure_from_the_host(name, precision):
         else:
             _same_solve(a, b, g)
         assert b.mbpt2() == pytest.approx(float(g["scalars"][1]), rel=1e-12, abs=1e-15)
+
+
+@pytest.mark.parametrize("name", SMALL + ["eg54_s19"])
+def test_table_path_on_generated_v(name):
+    """The table path (the reference's stage structure) with every V block, the three-body V
+    included, generated on the device and the tables derived there."""
+    g = golden(name)
+    with system_for(g) as s1, \
+            getattr(System, g["kind"])(**g["params"], tables=False, v_blocks=False) as s2, \
+            CCDSolver(s1, path="tables") as a, \
+            CCDSolver(s2, path="tables", v_mode="on_the_fly") as b:
+        if g["kind"] == "inf_matter":
+            rb = b.solve(tol=g["tol"], max_iters=100, mixing=0.5)
+            ref = g["energies"][-1]
+            assert abs(rb.e_corr - ref) <= 1e-10 * abs(ref) + 1e-14
+        else:
+            _same_solve(a, b, g)
