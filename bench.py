@@ -571,7 +571,7 @@ def run_batch(args):
 
 def _problem_bytes(system, with_v_pppp=True, with_tables=True, with_v=True):
     """Bytes ccdgpu_create copies host -> device for this system: V blocks in their reference
-    layouts (V_pppp, V_hhpp, V_hhhh of amplitude-carrying channels, both modified-channel V,
+    layouts (the a <= b rows of V_pppp, V_hhpp, V_hhhh of amplitude-carrying channels, both modified-channel V,
     the three-body V), the eight ChainIndex tables (24 bytes per entry) or, without them, the
     16-byte modified-pair lookup per (particle, hole), the energies and the O(sum pp) pair
     metadata.  with_v=False: no V block; the modified channels' pair lists (8 bytes a pair)
@@ -585,7 +585,13 @@ def _problem_bytes(system, with_v_pppp=True, with_tables=True, with_v=True):
     hp = md[:, 2].astype(np.int64)
     ph = md[:, 3].astype(np.int64)
     n_t = int((pp * hh).sum())
-    v = 8 * int((pp * pp).sum() * (1 if with_v_pppp else 0) + n_t + (hh * hh).sum() +
+    # V_pppp: only the rows a <= b of each block cross (pr rows of pp values).
+    pm = system.array("pp_map").reshape(-1, 2)
+    starts = np.concatenate([[0], np.cumsum(d[:, 0])[:-1]]).astype(np.int64)
+    keep = (pm[:, 0] <= pm[:, 1]).astype(np.int64)
+    pr_all = np.add.reduceat(keep, starts[d[:, 0] > 0]) if len(keep) else np.zeros(0, np.int64)
+    pr = pr_all[(d[d[:, 0] > 0, 1] > 0)]
+    v = 8 * int((pr * pp).sum() * (1 if with_v_pppp else 0) + n_t + (hh * hh).sum() +
                 (ph * hp).sum() + (hp * hp).sum())
     v += 8 * 2 * n_t
     if not with_v:

@@ -27,7 +27,8 @@ __global__ void transpose_hhpp_kernel(const ElemRange *__restrict__ ranges,
   }
 }
 
-// Packed, tiled V_pppp: one CTA per packed row u of one channel.
+// Packed, tiled V_pppp: one CTA per packed row u of one channel.  vraw holds each channel's
+// packed rows (a <= b) in u order, pp values each, from vraw_off[channel].
 // items[i] = (active channel, packed row); kcol[pk_off + w] = pp index of the w-th c<d pair.
 __global__ void tile_v_kernel(const ChanInfo *__restrict__ chans, const int2 *__restrict__ items,
                               const int32_t *__restrict__ rowmap, const int32_t *__restrict__ kcol,
@@ -36,8 +37,7 @@ __global__ void tile_v_kernel(const ChanInfo *__restrict__ chans, const int2 *__
   const int2 it = items[blockIdx.x];
   const ChanInfo ch = chans[it.x];
   const int u = it.y;
-  const int ab = rowmap[ch.row_off + u];
-  const double *src = vraw + vraw_off[it.x] + (int64_t)ab * ch.pp;
+  const double *src = vraw + vraw_off[it.x] + (int64_t)u * ch.pp;  // packed row u
   const int mt = u / ch.bm, rows = min(ch.bm, ch.pr - mt * ch.bm);
   const int ar = ladder_arows(ch.nb, rows);
   const int64_t tb = ch.vkt_base + (int64_t)mt * ladder_arows_full(ch.nb) * ch.nkc * kBK;
@@ -55,8 +55,7 @@ __global__ void tile_v_tc_kernel(const ChanInfo *__restrict__ chans, const int2 
   const int2 it = items[blockIdx.x];
   const ChanInfo ch = chans[it.x];
   const int u = it.y;
-  const int ab = rowmap[ch.row_off + u];
-  const double *src = vraw + vraw_off[it.x] + (int64_t)ab * ch.pp;
+  const double *src = vraw + vraw_off[it.x] + (int64_t)u * ch.pp;  // packed row u
   const int mt = u >> 7, r = u & 127;
   const int rg = (min(kTcBM, ch.pr - mt * kTcBM) + 7) >> 3;
   const int64_t tb = ch.vtc_base + (int64_t)mt * kTcBM * ch.nkct * kTcKC;

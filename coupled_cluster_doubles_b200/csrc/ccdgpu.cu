@@ -377,10 +377,21 @@ Staging &staging() {
   return s;
 }
 
-int copy_to_device(ccdgpu_handle *h, void *dst, const void *src, size_t bytes) {
+// Host runs (src[i], bytes[i]) to consecutive device bytes from dst.  Large totals go through
+// the staging buffers: each chunk is filled by host threads from pieces of the runs (a run may
+// span chunks, a chunk may hold many runs) and moved by one device copy.
+int copy_runs_to_device(ccdgpu_handle *h, char *dst, const std::vector<const char *> &src,
+                        const std::vector<size_t> &bytes) {
+  size_t total = 0;
+  std::vector<size_t> at(src.size());
+  for (size_t i = 0; i < src.size(); i++) {
+    at[i] = total;
+    total += bytes[i];
+  }
+  if (!total) return CCDGPU_OK;
   Staging &S = staging();
   std::unique_lock<std::mutex> lock(S.mu, std::defer_lock);
-  if (bytes >= kStageMin && lock.try_lock()) {
+  if (total >= kStageMin && lock.try_lock()) {
     if (!S.buf && !S.failed &&
         cudaHostAlloc(reinterpret_cast<void **>(&S.buf), 2 * kStageChunk,
                       cudaHostAllocPortable) != cudaSuccess) {
@@ -394,20 +405,31 @@ int copy_to_device(ccdgpu_handle *h, void *dst, const void *src, size_t bytes) {
       cudaError_t e = cudaSuccess;
       for (int k = 0; k < 2 && e == cudaSuccess; k++)
         e = cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming);
-      const char *in = static_cast<const char *>(src);
-      char *out = static_cast<char *>(dst);
-      for (size_t off = 0, k = 0; off < bytes && e == cudaSuccess; off += kStageChunk, k ^= 1) {
-        const size_t n = std::min(kStageChunk, bytes - off);
+      const int threads = std::max(1, std::min(omp_get_max_threads(), 16));
+      size_t r0 = 0;  // first run that reaches into the current chunk
+      struct Piece {
+        size_t to;
+        const char *from;
+        size_t n;
+      };
+      std::vector<Piece> pieces;
+      for (size_t off = 0, k = 0; off < total && e == cudaSuccess; off += kStageChunk, k ^= 1) {
+        const size_t n = std::min(kStageChunk, total - off), end = off + n;
         char *stage = S.buf + k * kStageChunk;
         if (pending[k] && (e = cudaEventSynchronize(ev[k])) != cudaSuccess) break;
-        const int parts = std::max(1, std::min(omp_get_max_threads(), 16));
-        const size_t part = (n + parts - 1) / parts;
-#pragma omp parallel for num_threads(parts) schedule(static)
-        for (int t = 0; t < parts; t++) {
-          const size_t b = std::min(n, (size_t)t * part), l = std::min(n - b, part);
-          if (l) std::memcpy(stage + b, in + off + b, l);
+        // Pieces of at most n / threads bytes, so that one large run is copied in parallel too.
+        const size_t piece = std::max<size_t>(size_t(64) << 10, (n + threads - 1) / threads);
+        pieces.clear();
+        while (at[r0] + bytes[r0] <= off) r0++;
+        for (size_t i = r0; i < src.size() && at[i] < end; i++) {
+          const size_t lo = std::max(at[i], off), hi = std::min(at[i] + bytes[i], end);
+          for (size_t x = lo; x < hi; x += piece)
+            pieces.push_back(Piece{x - off, src[i] + (x - at[i]), std::min(piece, hi - x)});
         }
-        e = cudaMemcpyAsync(out + off, stage, n, cudaMemcpyHostToDevice, h->s0);
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 8)
+        for (int64_t j = 0; j < (int64_t)pieces.size(); j++)
+          std::memcpy(stage + pieces[j].to, pieces[j].from, pieces[j].n);
+        e = cudaMemcpyAsync(dst + off, stage, n, cudaMemcpyHostToDevice, h->s0);
         if (e == cudaSuccess) e = cudaEventRecord(ev[k], h->s0);
         pending[k] = e == cudaSuccess;
       }
@@ -427,34 +449,35 @@ int copy_to_device(ccdgpu_handle *h, void *dst, const void *src, size_t bytes) {
       return CCDGPU_OK;
     }
   }
-  CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->s0));
+  for (size_t i = 0; i < src.size(); i++)
+    if (bytes[i]) CK(cudaMemcpyAsync(dst + at[i], src[i], bytes[i], cudaMemcpyHostToDevice, h->s0));
   return CCDGPU_OK;
 }
 
+int copy_to_device(ccdgpu_handle *h, void *dst, const void *src, size_t bytes) {
+  return copy_runs_to_device(h, static_cast<char *>(dst), {static_cast<const char *>(src)},
+                             {bytes});
+}
+
 // Copies per-channel host blocks (block k of `count[k]` elements at src[k]) to consecutive
-// device positions, one copy per run of blocks that are adjacent in host memory.
+// device positions; blocks adjacent in host memory form one run.
 template <typename T>
 int upload_runs(ccdgpu_handle *h, T *dst, const std::vector<const T *> &src,
                 const std::vector<int64_t> &count) {
-  const T *run_src = nullptr;
-  int64_t run_len = 0, pos = 0, run_dst = 0;
-  auto flush = [&]() -> int {
-    return run_len ? copy_to_device(h, dst + run_dst, run_src, run_len * sizeof(T)) : CCDGPU_OK;
-  };
+  std::vector<const char *> rs;
+  std::vector<size_t> rl;
   for (size_t k = 0; k < src.size(); k++) {
     if (!count[k]) continue;
-    if (run_len && src[k] == run_src + run_len) {
-      run_len += count[k];
+    const char *p = reinterpret_cast<const char *>(src[k]);
+    const size_t n = (size_t)count[k] * sizeof(T);
+    if (!rs.empty() && rs.back() + rl.back() == p) {
+      rl.back() += n;
     } else {
-      int rc = flush();
-      if (rc) return rc;
-      run_src = src[k];
-      run_len = count[k];
-      run_dst = pos;
+      rs.push_back(p);
+      rl.push_back(n);
     }
-    pos += count[k];
   }
-  return flush();
+  return copy_runs_to_device(h, reinterpret_cast<char *>(dst), rs, rl);
 }
 
 // pp-ladder work tiles for a schedule (split factors of K per column class), in their own
@@ -796,7 +819,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     vt += (int64_t)ci.nkc * arows_tot * kBK;
     part_tot += (int64_t)ci.nhht * hh * hh;
     vraw_off.push_back(vraw_tot);
-    if (!on_the_fly) vraw_tot += pp * pp;
+    if (!on_the_fly) vraw_tot += (int64_t)ci.pr * pp;  // packed rows (a <= b) only
     maxhh = std::max<int>(maxhh, (int)hh);
     // hh ladder: one unit per (K slice, chunk of P rows): hh <= 16 is a single chunk, larger
     // hh one chunk per 8 rows of P.
@@ -1143,7 +1166,11 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
       const ChanInfo &a = chans[ai];
       if ((!on_the_fly && !P->v_pppp[c]) || (!gen_v && (!P->v_hhpp[c] || !P->v_hhhh[c])))
         return CCDGPU_ERR_INVALID_ARGUMENT;
-      if (!on_the_fly) { sp.push_back(P->v_pppp[c]); np2.push_back((int64_t)a.pp * a.pp); }
+      if (!on_the_fly)  // the rows a <= b of V_pppp, the only ones the ladder reads
+        for (int u = 0; u < a.pr; u++) {
+          sp.push_back(P->v_pppp[c] + (int64_t)rowmap[a.row_off + u] * a.pp);
+          np2.push_back(a.pp);
+        }
       if (!gen_v) {
         sx.push_back(P->v_hhpp[c]); nx.push_back((int64_t)a.pp * a.hh);
         sh.push_back(P->v_hhhh[c]); nh.push_back((int64_t)a.hh * a.hh);
