@@ -38,6 +38,10 @@ CONFIGS = {
                       "pairing", dict(xi=1.0, g=1.0, n_pair_states=8, n_particles=8), True),
     "pnm14_s4": (["--infMatter", "-d", "0.08", "-z", "1", "-s", "4", "-p", "2", "-t", "1e-8"],
                  "inf_matter", dict(density=0.08, tz_max=1, n_shells=4, n_particle_shells=2), True),
+    # Symmetric nuclear matter (both isospins): one particle shell, which converges (with two
+    # the reference's iteration runs to its cap or to NaN at these densities).
+    "snm4_s4": (["--infMatter", "-d", "0.16", "-z", "2", "-s", "4", "-p", "1", "-t", "1e-8"],
+                "inf_matter", dict(density=0.16, tz_max=2, n_shells=4, n_particle_shells=1), True),
     "eg14_s19": (["--electronGas", "-r", "1.0", "-s", "19", "-p", "2", "-t", "1e-12"],
                  "electron_gas", dict(r_s=1.0, n_shells=19, n_particle_shells=2), True),
     "eg54_s19": (["--electronGas", "-r", "1.0", "-s", "19", "-p", "4", "-t", "1e-12"],

@@ -7,7 +7,8 @@ import numpy as np
 from coupled_cluster_doubles_b200 import System
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-SMALL = ["pairing_gm1.0", "pairing_gm0.5", "pairing_gp0.5", "pairing_gp1.0", "pnm14_s4", "eg14_s19"]
+SMALL = ["pairing_gm1.0", "pairing_gm0.5", "pairing_gp0.5", "pairing_gp1.0", "pnm14_s4",
+         "snm4_s4", "eg14_s19"]
 STRUCT = ["chan_dims", "chan_mod_dims", "three_body_dims", "pp_map", "hh_map", "ph_mod_map",
           "hp_mod_map", "hpp_map", "phh_map", "sp_energy"]
 MAPS = ["map_iab_j", "map_jab_i", "map_a_bij", "map_b_aij", "map_ai_jb", "map_aj_ib",
