@@ -46,6 +46,18 @@ CONFIGS = {
                  "electron_gas", dict(r_s=1.0, n_shells=19, n_particle_shells=2), True),
     "eg54_s19": (["--electronGas", "-r", "1.0", "-s", "19", "-p", "4", "-t", "1e-12"],
                  "electron_gas", dict(r_s=1.0, n_shells=19, n_particle_shells=4), False),
+    # More pins of the builder and the oracle (CPU tests).
+    "eg14_r05": (["--electronGas", "-r", "0.5", "-s", "19", "-p", "2", "-t", "1e-12"],
+                 "electron_gas", dict(r_s=0.5, n_shells=19, n_particle_shells=2), True),
+    "eg14_r2": (["--electronGas", "-r", "2.0", "-s", "19", "-p", "2", "-t", "1e-12"],
+                "electron_gas", dict(r_s=2.0, n_shells=19, n_particle_shells=2), True),
+    "pnm14_d016": (["--infMatter", "-d", "0.16", "-z", "1", "-s", "4", "-p", "2", "-t", "1e-10"],
+                   "inf_matter", dict(density=0.16, tz_max=1, n_shells=4, n_particle_shells=2),
+                   True),
+    "pairing_l6n4": (["--pairing", "-l", "6", "-n", "4", "-x", "1.0", "-g", "0.3", "-t", "1e-12"],
+                     "pairing", dict(xi=1.0, g=0.3, n_pair_states=6, n_particles=4), True),
+    "eg38_s16": (["--electronGas", "-r", "1.0", "-s", "16", "-p", "3", "-t", "1e-10"],
+                 "electron_gas", dict(r_s=1.0, n_shells=16, n_particle_shells=3), False),
 }
 
 STRUCT = ["chan_dims", "chan_mod_dims", "three_body_dims", "pp_map", "hh_map", "ph_mod_map",

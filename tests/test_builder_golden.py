@@ -7,11 +7,11 @@ exact equality.
 """
 import pytest
 
-from helpers import MAPS, SMALL, STRUCT, VKINDS, golden, system_for
+from helpers import EXTRA, MAPS, SMALL, STRUCT, VKINDS, golden, system_for
 from oracle.oracle import fnv1a
 
 
-@pytest.mark.parametrize("name", SMALL + ["eg54_s19"])
+@pytest.mark.parametrize("name", SMALL + ["eg54_s19"] + EXTRA)
 def test_builder_matches_reference(name):
     g = golden(name)
     with system_for(g) as s:
