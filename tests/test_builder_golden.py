@@ -90,3 +90,15 @@ def test_builder_rejects_bad_plane_wave_input():
         System.electron_gas(r_s=1.0, n_shells=2, n_particle_shells=4)
     with pytest.raises(BuildError):
         System.inf_matter(density=0.08, tz_max=3, n_shells=4, n_particle_shells=2)
+
+
+def test_device_channels_without_a_gpu_is_an_error():
+    """CCDHOST_DEVICE_CHANNELS has no host fallback: without a GPU the build fails with
+    CCDGPU_ERR_NO_DEVICE (-6)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    from coupled_cluster_doubles_b200 import System
+    from coupled_cluster_doubles_b200.system import BuildError
+    with pytest.raises(BuildError, match="status -6"):
+        System.pairing(xi=1.0, g=0.5, n_pair_states=4, n_particles=4, device_channels=True)
