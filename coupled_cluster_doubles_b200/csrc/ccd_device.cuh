@@ -22,7 +22,8 @@ namespace ccd {
 //   mid and wide channels (nb = 8*C, FP64 MMA fragments):
 //     A tiles [kBK][as] k-major, as = rows rounded up to 8, plus 4;
 //     B tiles [kBK][bs] k-major, bs = nb + 4;
-//     strides of 4 mod 8 doubles put the 4 k-rows of an m8n8k4 fragment load on distinct banks.
+//     strides of 4 mod 8 doubles put the 4 k-rows of an FP64 MMA fragment load (m16n8k16 in
+//     the ladder) on distinct banks.
 // The last row tile of a channel is stored compact (only its real rows, rounded up to 8).
 constexpr int kBK = 16;        // K depth of one pipeline stage
 constexpr int kStages = 4;     // bulk-copy pipeline depth
