@@ -100,3 +100,21 @@ def test_generator_mappings_reproduce_reference_v(name):
             v3p[o_p[a] + pblk[a, b] + ij] = v(H[ij, 0], H[ij, 1], P[y, 0], P[y, 1])
         np.testing.assert_allclose(v3h, s.array("v_h_hpp"), rtol=1e-14, atol=0)
         np.testing.assert_allclose(v3p, s.array("v_phh_p"), rtol=1e-14, atol=0)
+
+
+@pytest.mark.parametrize("name", ["pairing_gp0.5", "eg14_s19"])
+def test_normal_order_formula_reproduces_reference(name):
+    """normal_order_kernel (SPBasis.cpp:7-40): e'_p = e_p + sum_{j<A} <pj|v|pj> and
+    E_ref = sum_{i,j<A} 1/2 <ij|v|ij> + sum_{i<A} e_i, from the bare energies."""
+    g = golden(name)
+    with system_for(g) as s:
+        v = tbme_fn(s, g["kind"])
+        nh, nsp = s.n_particles, s.n_sp
+        bare = s.array("sp_energy_bare")
+        p, j = np.meshgrid(np.arange(nsp), np.arange(nh), indexing="ij")
+        corr = v(p.ravel(), j.ravel(), p.ravel(), j.ravel()).reshape(nsp, nh)
+        np.testing.assert_allclose(bare + corr.sum(axis=1), s.array("sp_energy"), rtol=1e-13,
+                                   atol=1e-14)
+        i, jj = np.meshgrid(np.arange(nh), np.arange(nh), indexing="ij")
+        e_ref = 0.5 * v(i.ravel(), jj.ravel(), i.ravel(), jj.ravel()).sum() + bare[:nh].sum()
+        assert e_ref == pytest.approx(float(g["scalars"][0]), rel=1e-13)
