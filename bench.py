@@ -1,12 +1,21 @@
 """Benchmark: CCD iterations/s and time-to-converge of the B200 solver.
 
 One "step" is one complete CCD solve of the workload from T2 = 0 with the reference's stop
-rule (|dE| <= tol on the total correlation energy, at most 101 iterations, mixing 0.5).
+rule (|dE| <= tol on the total correlation energy, at most 101 iterations, mixing 0.5) and
+tol = 1e-8 N, which keeps the energy within 1e-7 per particle of the converged value.
 `value` = iterations of all timed steps / their device time (inputs resident in HBM, L2
 flushed before every step).  `e2e` runs the same solve through the C ABI from host buffers:
-create (upload of V, maps, energies) + solve + read-back of T2, every step.
+create (upload of the problem) + solve + read-back of T2 + destroy, every step.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--config eg14] [--impl reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config eg54c36] [--impl reference]
+
+Default workload: the 3D electron gas with N=54, r_s=2.0, |n|^2 <= 36 (1850 spin-orbitals),
+V_pppp generated on the device from the model, mixed precision (split-bf16 tensor-core pp
+ladder, FP64 polish) as the headline arm beside the plain FP64 solver.
+
+--impl reference times the reference's own loop (oracle/_ref/ref_harness: the unmodified
+reference sources, one MPI rank, all host cores as OpenMP threads) on the same workload, stop
+rule and `config`: one set-up, then each step is a bounded sample of the solve.
 
 With --gpus N under torchrun every rank solves its own replica of the workload (the CCD
 iteration of one system is not sharded); value sums the iterations of all ranks over the
@@ -27,27 +36,57 @@ sys.path.insert(0, REPO)
 
 METRIC = "CCD iter/s & time-to-converge, mixed vs FP64 on 1 B200 at |ΔE/N|≤1e-7; %peak"
 
-# name -> (description, builder kind, builder params, reference CLI, tol)
+# name -> description, builder kind, builder params, reference CLI, particles, golden fixture
+# (tests/golden, a reference run at tol 1e-12), V_pppp mode of the GPU arm, iterations per
+# reference-arm step (a bounded sample: one step stays around a second of host time).
 CONFIGS = {
-    "eg14": ("3D electron gas, N=14, r_s=1.0, |n|^2<=20 (778 spin-orbitals)", "electron_gas",
-             dict(r_s=1.0, n_shells=19, n_particle_shells=2),
-             ["--electronGas", "-r", "1.0", "-s", "19", "-p", "2"], 1e-12),
-    "eg54c20": ("3D electron gas, N=54, r_s=1.0, |n|^2<=20 (778 spin-orbitals)", "electron_gas",
-                dict(r_s=1.0, n_shells=19, n_particle_shells=4),
-                ["--electronGas", "-r", "1.0", "-s", "19", "-p", "4"], 1e-12),
-    "eg54c36": ("3D electron gas, N=54, r_s=2.0, |n|^2<=36 (1850 spin-orbitals)", "electron_gas",
-                dict(r_s=2.0, n_shells=32, n_particle_shells=4),
-                ["--electronGas", "-r", "2.0", "-s", "32", "-p", "4"], 1e-12),
-    "eg54c36r05": ("3D electron gas, N=54, r_s=0.5, |n|^2<=36 (1850 spin-orbitals)",
-                   "electron_gas", dict(r_s=0.5, n_shells=32, n_particle_shells=4),
-                   ["--electronGas", "-r", "0.5", "-s", "32", "-p", "4"], 1e-12),
-    "pnm66": ("pure neutron matter, N=66, rho=0.08 fm^-3, |n|^2<=36 (1850 spin-orbitals)",
-              "inf_matter", dict(density=0.08, tz_max=1, n_shells=32, n_particle_shells=5),
-              ["--infMatter", "-d", "0.08", "-z", "1", "-s", "32", "-p", "5"], 1e-12),
-    "pairing": ("pairing model, 8 levels, 4 pairs, g=-1.0", "pairing",
-                dict(xi=1.0, g=-1.0, n_pair_states=8, n_particles=8),
-                ["--pairing", "-l", "8", "-n", "8", "-x", "1.0", "-g", "-1.0"], 1e-12),
+    "eg54c36": dict(desc="3D electron gas, N=54, r_s=2.0, |n|^2<=36 (1850 spin-orbitals)",
+                    kind="electron_gas", params=dict(r_s=2.0, n_shells=32, n_particle_shells=4),
+                    cli=["--electronGas", "-r", "2.0", "-s", "32", "-p", "4"], n=54,
+                    golden="eg54c36_r2", v_mode="on_the_fly", ref_iters=3),
+    "eg54c36r05": dict(desc="3D electron gas, N=54, r_s=0.5, |n|^2<=36 (1850 spin-orbitals)",
+                       kind="electron_gas",
+                       params=dict(r_s=0.5, n_shells=32, n_particle_shells=4),
+                       cli=["--electronGas", "-r", "0.5", "-s", "32", "-p", "4"], n=54,
+                       golden="eg54c36_r05", v_mode="on_the_fly", ref_iters=3),
+    "pnm66": dict(desc="pure neutron matter, N=66, rho=0.08 fm^-3, |n|^2<=36 (1850 "
+                       "spin-orbitals)", kind="inf_matter",
+                  params=dict(density=0.08, tz_max=1, n_shells=32, n_particle_shells=5),
+                  cli=["--infMatter", "-d", "0.08", "-z", "1", "-s", "32", "-p", "5"], n=66,
+                  golden="pnm66_s32", v_mode="stored", ref_iters=3),
+    "eg14": dict(desc="3D electron gas, N=14, r_s=1.0, |n|^2<=20 (778 spin-orbitals)",
+                 kind="electron_gas", params=dict(r_s=1.0, n_shells=19, n_particle_shells=2),
+                 cli=["--electronGas", "-r", "1.0", "-s", "19", "-p", "2"], n=14,
+                 golden="eg14_s19", v_mode="stored", ref_iters=101),
+    "eg54c20": dict(desc="3D electron gas, N=54, r_s=1.0, |n|^2<=20 (778 spin-orbitals)",
+                    kind="electron_gas", params=dict(r_s=1.0, n_shells=19, n_particle_shells=4),
+                    cli=["--electronGas", "-r", "1.0", "-s", "19", "-p", "4"], n=54,
+                    golden="eg54_s19", v_mode="stored", ref_iters=10),
+    "pairing": dict(desc="pairing model, 8 levels, 4 pairs, g=-1.0", kind="pairing",
+                    params=dict(xi=1.0, g=-1.0, n_pair_states=8, n_particles=8),
+                    cli=["--pairing", "-l", "8", "-n", "8", "-x", "1.0", "-g", "-1.0"], n=8,
+                    golden="pairing_gm1.0", v_mode="stored", ref_iters=101),
 }
+DEFAULT_CONFIG = "eg54c36"
+MIXING = 0.5
+MAX_ITERS = 100  # the reference's cap: at most 101 iterations (main.cpp:509-519)
+
+
+def stop_tol(n_particles):
+    """|dE| bound of the stop rule that keeps the converged energy within 1e-7 per particle
+    of the fully converged value (a factor-10 margin over the linear convergence tail;
+    the achieved error is measured against the reference and reported)."""
+    return 1e-8 * n_particles
+
+
+def config_dict(name):
+    """The workload description, identical in the GPU arm's and the reference arm's lines."""
+    c = CONFIGS[name]
+    return {"workload": c["desc"], "reference_cli": " ".join(c["cli"]),
+            "stop_rule": f"|dE| <= 1e-8 N = {stop_tol(c['n']):g} on the total correlation "
+                         "energy (keeps |dE/N| <= 1e-7)",
+            "start": "T2 = 0", "mixing": MIXING, "max_iterations": MAX_ITERS + 1,
+            "l2": "GPU arm: flushed (256 MiB write) before every step"}
 
 
 def dist_env():
@@ -67,12 +106,14 @@ def combine_ranks(dev_ms, iters, device, world):
     return float(ms.item()), float(it.item())
 
 
-# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the headline
-# kernel, from the ncu captures summarised in profiles/ (workload, kernel): bytes, source.
-NCU_TRAFFIC = {
-    ("eg14", "pp_ladder_tc_kernel<2>"): (16.13e6, "profiles/pp_ladder_tc_eg14_mixed_traffic.md"),
-    ("eg54c36", "pp_ladder_tc_kernel<2>"): (360.76e6, "profiles/pp_ladder_tc_eg54c36_mixed.md"),
-}
+def dram_traffic():
+    """DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch per (workload,
+    kernel), from ncu captures (bench_dram_traffic.json beside this file)."""
+    try:
+        with open(os.path.join(REPO, "bench_dram_traffic.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
 
 
 def measured_peaks():
@@ -81,6 +122,26 @@ def measured_peaks():
             return json.load(f), "measured"
     except OSError:
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def fp64_gemm_peak(device, n=8192, reps=3):
+    """FP64 GEMM throughput of this GPU (cuBLAS DGEMM n^3 through torch), TF/s: the FP64
+    denominator of the ladder rooflines, measured in the run."""
+    import torch
+    a = torch.rand(n, n, dtype=torch.float64, device=device)
+    b = torch.rand(n, n, dtype=torch.float64, device=device)
+    torch.matmul(a, b)
+    torch.cuda.synchronize(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        torch.matmul(a, b)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (ms / 1e3) / 1e12
 
 
 class ClockSampler:
@@ -138,63 +199,88 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def reference_run(cfg, cores, timeout=600):
-    """Runs the reference executable (oracle/_ref/ccd.exe) once; returns (iterations, loop s)."""
-    exe = os.path.join(REPO, "oracle", "_ref", "ccd.exe")
-    _, kind, _, cli, tol = CONFIGS[cfg]
-    env = dict(os.environ, OMP_NUM_THREADS=str(1 if kind == "pairing" else cores),
-               OPENBLAS_NUM_THREADS="1")
-    out = subprocess.run([exe, *cli, "-t", repr(tol)], env=env, capture_output=True, text=True,
+def reference_threads(name):
+    # The reference's pairing basis builds its three-body maps correctly only single-threaded
+    # (SPBasis.cpp:227-255 appends inside an omp parallel region without omp for).
+    return 1 if CONFIGS[name]["kind"] == "pairing" else (os.cpu_count() or 1)
+
+
+def reference_bench(name, steps, timeout):
+    """The reference's own loop (oracle/_ref/ref_harness, bench mode) on this host: one
+    set-up, then `steps` solves from T2 = 0, each a bounded sample of at most ref_iters
+    iterations at the GPU arm's stop rule.  Returns ([(iterations, seconds, e_corr)],
+    setup seconds, threads) or raises."""
+    c = CONFIGS[name]
+    exe = os.path.join(REPO, "oracle", "_ref", "ref_harness")
+    threads = reference_threads(name)
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS="1",
+               CCD_BENCH=f"{steps},{c['ref_iters']},{stop_tol(c['n'])!r}")
+    out = subprocess.run([exe, *c["cli"]], env=env, capture_output=True, text=True,
                          timeout=timeout, check=True).stdout
-    it = int(re.findall(r"^iterations: (\d+)", out, re.M)[-1])
-    secs = float(re.findall(r"cc_diagrams_time: ([0-9.eE+-]+)", out)[-1])
-    return it, secs, out
+    rows = [(int(a), float(b), float(e)) for a, b, e in
+            re.findall(r"^bench_step: (\d+) ([0-9.eE+-]+) (\S+)", out, re.M)]
+    setup = sum(float(x) for x in re.findall(r"^(?:setup|load)_time: ([0-9.eE+-]+)", out, re.M))
+    if len(rows) != steps:
+        raise RuntimeError("reference harness printed %d of %d steps" % (len(rows), steps))
+    return rows, setup, threads
 
 
 def run_reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    desc, kind, _, cli, tol = CONFIGS[args.config]
-    exe = os.path.join(REPO, "oracle", "_ref", "ccd.exe")
-    if not os.path.exists(exe):
+    c = CONFIGS[args.config]
+    if not os.path.exists(os.path.join(REPO, "oracle", "_ref", "ref_harness")):
         print(json.dumps({"impl": "reference", "unavailable":
-                          "reference build oracle/_ref/ccd.exe missing (built from the reference "
-                          "sources by oracle/build.py)"}))
+                          "reference build oracle/_ref/ref_harness missing (built from the "
+                          "reference sources by oracle/build.py)"}))
         return
-    cores = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        reference_run(args.config, cores)
-    its, secs = 0, 0.0
-    for _ in range(args.steps):
-        i, s, _ = reference_run(args.config, cores)
-        its += i
-        secs += s
+    rows, setup, threads = reference_bench(args.config, args.warmup + args.steps, timeout=3000)
+    timed = rows[args.warmup:]
+    its = sum(r[0] for r in timed)
+    secs = sum(r[1] for r in timed)
     value = its / secs
-    used = 1 if kind == "pairing" else cores
+    sample = (f"{args.steps} timed steps after {args.warmup} warm-up steps in one process "
+              f"after one set-up ({setup:.1f} s, untimed); each step a solve from T2 = 0 "
+              f"capped at {c['ref_iters']} iterations of the reference loop "
+              f"({its} iterations timed)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "iter/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * secs / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": desc, "tol": tol, "cli": " ".join(cli),
-                   "time": "reference cc_diagrams_time (CCD loop only), 1 MPI rank"},
-        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": used, "kind": "reference",
-                         "sample": f"{args.steps} full solves ({its} iterations) of the workload"},
-        "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": config_dict(args.config),
+        "time": "per step: wall time of the reference loop (its cc_diagrams_time span), "
+                "1 MPI rank, OMP threads = host cores, OpenBLAS single-threaded",
+        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
 
 
-FP64_PEAK_TFLOPS = 35.47  # cuBLAS DGEMM 8192^3 measured on this pool's B200 (FP64 pipe)
 PRECISIONS = {"mixed": "mixed_bf16", "fp64": "fp64"}
+FP64_PEAK_FALLBACK = 35.47  # cuBLAS DGEMM 8192^3 measured on this pool's B200 (FP64 pipe)
 
 
-def stop_tol(n_particles):
-    """|dE| bound of the stop rule that keeps the converged energy within 1e-7 per particle
-    of the fully converged FP64 value (a factor-10 margin over the linear convergence tail;
-    the achieved error is measured and reported)."""
-    return 1e-8 * n_particles
+def golden_reference(name):
+    """The reference's converged energy and sampled T2 (every 97th element) for a workload,
+    from the committed fixture of a reference run at tol 1e-12; None if there is none."""
+    import numpy as np
+    path = os.path.join(REPO, "tests", "golden", CONFIGS[name]["golden"] + ".npz")
+    if not os.path.exists(path):
+        return None
+    g = np.load(path)
+    return {"e_corr": float(g["energies"][-1]), "t2": g["t2"], "full": bool(g["t2_full"][0])}
+
+
+def assemble_bytes(n_t2, nt):
+    """Algorithmic bytes of one fused assembly launch: per amplitude, read t_old, R (the ring
+    term in pphh order), V, D and the int32 phhp index, write t_new and its phhp copy (52 B),
+    plus the next iteration's ladder operands: nt bf16 terms (mixed) or one FP64 value in the
+    operand image that holds its row (each amplitude is in one of them)."""
+    return n_t2 * (52.0 + (2.0 * nt if nt else 8.0))
 
 
 def main():
@@ -202,14 +288,14 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="eg14", choices=list(CONFIGS) + ["batch24"])
+    ap.add_argument("--config", default=DEFAULT_CONFIG, choices=list(CONFIGS) + ["batch24"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--path", default="fused", choices=["fused", "tables"])
     ap.add_argument("--precision", default="mixed", choices=list(PRECISIONS),
                     help="headline arm; the other precision is timed beside it")
-    ap.add_argument("--v-mode", default="stored", choices=["stored", "on_the_fly"],
-                    help="on_the_fly: V_pppp generated on the device from the model (the host "
-                         "builds and uploads none)")
+    ap.add_argument("--v-mode", default=None, choices=["stored", "on_the_fly"],
+                    help="stored: V_pppp built on the host and uploaded; on_the_fly: generated "
+                         "on the device from the model (default: the workload's own setting)")
     ap.add_argument("--no-device-loop", action="store_true",
                     help="replay per-iteration graphs instead of the device solve loop (for "
                          "profilers, which cannot see kernels inside graph WHILE nodes)")
@@ -238,8 +324,10 @@ def main():
     if world > 1:
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    desc, kind, params, cli, _ = CONFIGS[args.config]
-    system = getattr(System, kind)(**params, load_v_pppp=args.v_mode == "stored")
+    cfg = CONFIGS[args.config]
+    v_mode = args.v_mode or cfg["v_mode"]
+    kind, params = cfg["kind"], cfg["params"]
+    system = getattr(System, kind)(**params, load_v_pppp=v_mode == "stored")
     n_part = system.n_particles
     tol = stop_tol(n_part)
     if args.path == "tables" and args.precision == "mixed":
@@ -247,26 +335,19 @@ def main():
     arms = [args.precision] + ([p for p in PRECISIONS if p != args.precision]
                                if args.path == "fused" and not args.single_arm else [])
     solvers = {a: CCDSolver(system, device=local, path=args.path, precision=PRECISIONS[a],
-                            v_mode=args.v_mode, device_loop=not args.no_device_loop)
+                            v_mode=v_mode, device_loop=not args.no_device_loop)
                for a in arms}
     stream = {a: torch.cuda.ExternalStream(solvers[a].stream_ptr(), device=local) for a in arms}
     # Autotuner: each arm's pp-ladder schedule picked by timing the candidates (untimed setup).
     tuned = {a: (solvers[a].autotune(reps=3) if not args.no_autotune else
                  (solvers[a].schedule(), None, None)) for a in arms}
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
-
-    # Fully converged FP64 energy (untimed) for the |dE/N| check.
-    e_conv = float("nan")
-    if not args.single_arm:
-        ref_solver = solvers.get("fp64") or CCDSolver(system, device=local, path=args.path,
-                                                      v_mode=args.v_mode)
-        ref_solver.reset()
-        e_conv = ref_solver.solve(tol=1e-12, max_iters=100, mixing=0.5).e_corr
+    gold = golden_reference(args.config)
 
     for a in arms:
         for _ in range(args.warmup):
             solvers[a].reset()
-            solvers[a].solve(tol=tol, max_iters=100, mixing=0.5)
+            solvers[a].solve(tol=tol, max_iters=MAX_ITERS, mixing=MIXING)
     torch.cuda.synchronize()
 
     def barrier():
@@ -291,7 +372,7 @@ def main():
                 e1 = torch.cuda.Event(enable_timing=True)
                 e0.record(st)
                 torch.cuda.nvtx.range_push("timed_solve")  # profilers: ncu --nvtx-include
-                last = sol.solve(tol=tol, max_iters=100, mixing=0.5)
+                last = sol.solve(tol=tol, max_iters=MAX_ITERS, mixing=MIXING)
                 torch.cuda.nvtx.range_pop()
                 e1.record(st)
                 e1.synchronize()
@@ -300,11 +381,17 @@ def main():
             torch.cuda.synchronize()
             barrier()
             max_ms, total_it = combine_ranks(dev_ms, iters, f"cuda:{local}", world)
+            t2 = sol.t2()
+            acc = {}
+            if gold is not None:
+                t2s = t2 if gold["full"] else t2[::97]
+                acc = {"abs_de_per_particle_vs_reference":
+                       abs(last.e_corr - gold["e_corr"]) / n_part,
+                       "t2_max_abs_vs_reference": float(np.max(np.abs(t2s - gold["t2"])))}
             timing[a] = {"max_ms": max_ms, "iters": total_it,
                          "iters_per_solve": last.iterations,
                          "polish_per_solve": last.polish_iterations,
-                         "e_corr": last.e_corr,
-                         "de_per_particle": abs(last.e_corr - e_conv) / n_part,
+                         "e_corr": last.e_corr, **acc,
                          "launches": solvers[a].profile()["launches"] - launches0[a]}
 
     # Kernel-level pass per arm: one solve with CUDA events around every kernel family.
@@ -315,21 +402,22 @@ def main():
         sol.enable_profiling(True)
         flush.fill_(1.0)
         torch.cuda.synchronize()
-        sol.solve(tol=tol, max_iters=100, mixing=0.5)
+        sol.solve(tol=tol, max_iters=MAX_ITERS, mixing=MIXING)
         prof[a] = sol.profile()
         sol.enable_profiling(False)
         work[a] = sol.work_per_iteration()
     ladder_cls = {a: solvers[a].ladder_profile(reps=5) for a in arms}
     other_cls = solvers[arms[0]].kernel_profile(reps=5)  # shared by both arms
     n_t2 = solvers[arms[0]].n_t2
+    nt_of = {"mixed": 2, "fp64": 0}
 
     # e2e (headline arm): the public API from host buffers, every step: create (H2D upload)
-    # + solve + T2 read-back.  The problem carries no loadMaps tables: create derives them on
-    # the device, as a caller that skips loadMaps would have it.
+    # + solve + T2 read-back + destroy.  The problem carries no loadMaps tables: create derives
+    # them on the device, as a caller that skips loadMaps would have it; with V generated on
+    # the device it carries no V block either.
     host_t2 = np.empty(n_t2)
     e2e_secs, e2e_iters = 0.0, 0
-    # With V generated on the device (on_the_fly) the problem carries no V block either.
-    stored = args.v_mode == "stored"
+    stored = v_mode == "stored"
     system_e2e = getattr(System, kind)(**params, load_v_pppp=stored, tables=False,
                                        v_blocks=stored)
     h2d = _problem_bytes(system_e2e, with_v_pppp=stored, with_tables=False, with_v=stored)
@@ -337,9 +425,9 @@ def main():
     for k in range(args.warmup + args.steps):
         t0 = time.perf_counter()
         s2 = CCDSolver(system_e2e, device=local, path=args.path, precision=PRECISIONS[arms[0]],
-                       v_mode=args.v_mode, device_loop=not args.no_device_loop)
+                       v_mode=v_mode, device_loop=not args.no_device_loop)
         ta = time.perf_counter()
-        r2 = s2.solve(tol=tol, max_iters=100, mixing=0.5)
+        r2 = s2.solve(tol=tol, max_iters=MAX_ITERS, mixing=MIXING)
         tb = time.perf_counter()
         s2.t2(host_t2)
         tc = time.perf_counter()
@@ -351,9 +439,17 @@ def main():
             phase_s += np.array([ta - t0, tb - ta, tc - tb, t1 - tc])
     system_e2e.close()
     e2e_secs_max, e2e_iters_all = combine_ranks(e2e_secs, e2e_iters, f"cuda:{local}", world)
+    fp64_peak, fp64_peak_src = FP64_PEAK_FALLBACK, "fallback (cuBLAS DGEMM measured earlier)"
+    try:
+        fp64_peak = fp64_gemm_peak(torch.device(f"cuda:{local}"))
+        fp64_peak_src = "cuBLAS DGEMM 8192^3 measured in this run"
+    except RuntimeError:
+        pass
 
     if rank == 0:
         peaks, peak_kind = measured_peaks()
+        hbm = peaks["hbm_gbs"]
+        traffic = dram_traffic()
         per_it = {}
         for a in arms:
             p = prof[a]
@@ -365,13 +461,45 @@ def main():
         head = arms[0]
         t = timing[head]
         value = t["iters"] / (t["max_ms"] / 1000.0)
-        # Roofline of the dominant kernel of the headline arm, the pp ladder: algorithmic
-        # bytes of one launch (antisymmetry-packed V_pppp, T and X operands at the arm's
-        # precision, D written in full) over its average device time.
-        ladder_ms = per_it[head]["pp_ladder"]
-        ladder_bytes = work[head]["ladder_bytes"]
-        achieved = ladder_bytes / (ladder_ms / 1000.0) / 1e9
-        kname = "pp_ladder_tc_kernel<2>" if head == "mixed" else "pp_ladder_kernel<0,1,2>"
+
+        def cls_bytes(*names):
+            return sum(other_cls[n][2] for n in names if n in other_cls)
+
+        def cls_flops(*names):
+            return sum(other_cls[n][1] for n in names if n in other_cls)
+
+        # Per kernel family of one iteration: algorithmic bytes (and flops) per launch over its
+        # average device time in the profiled solve (events around each family on its stream).
+        def kernel_rooflines(a):
+            nt = nt_of[a]
+            lad = "pp_ladder_tc_kernel<2>" if a == "mixed" else "pp_ladder_kernel<0,1,2>"
+            fams = [
+                ("pp_ladder", lad, work[a]["ladder_bytes"], work[a]["ladder_flops"]),
+                ("assemble_energy", "assemble_fused_kernel", assemble_bytes(n_t2, nt), 0.0),
+                ("ring", "ring_small_kernel + ring_kernel<2/4>",
+                 cls_bytes("ring_small", "ring_mid", "ring_large"),
+                 cls_flops("ring_small", "ring_mid", "ring_large")),
+                ("hh_ladder", "hh_mma_kernel<2/9> + hh_reduce_kernel",
+                 cls_bytes("hh_small", "hh_large", "hh_reduce"),
+                 cls_flops("hh_small", "hh_large")),
+                ("onebody", "onebody_fused_kernel", cls_bytes("onebody"), 0.0),
+            ]
+            out = {}
+            for fam, kname, by, fl in fams:
+                ms = per_it[a][fam]
+                if ms <= 0 or by <= 0:
+                    continue
+                gbs = by / (ms / 1e3) / 1e9
+                tr = traffic.get(f"{args.config}|{v_mode}|{kname}")
+                out[fam] = {"kernel": kname, "bound": "hbm", "achieved": gbs, "peak": hbm,
+                            "unit": "GB/s", "frac": gbs / hbm, "traffic": tr,
+                            "algorithmic_bytes_per_launch": by, "avg_launch_ms": ms}
+                if fl > 0:
+                    out[fam]["fp64_tflops"] = fl / (ms / 1e3) / 1e12
+            return out
+
+        roof = {a: kernel_rooflines(a) for a in arms}
+        dominant = max(roof[head], key=lambda f: roof[head][f]["avg_launch_ms"])
         arms_out = {}
         for a in arms:
             ta = timing[a]
@@ -382,15 +510,15 @@ def main():
                 "iterations_per_solve": ta["iters_per_solve"],
                 "polish_iterations_per_solve": ta["polish_per_solve"],
                 "e_corr": ta["e_corr"],
-                "abs_de_per_particle_vs_fp64_converged": ta["de_per_particle"],
+                "abs_de_per_particle_vs_reference": ta.get("abs_de_per_particle_vs_reference"),
+                "t2_max_abs_vs_reference": ta.get("t2_max_abs_vs_reference"),
                 "kernel_ms_per_iteration": per_it[a],
+                "kernel_rooflines": roof[a],
                 "pp_ladder_tflops_algorithmic": work[a]["ladder_flops"] / (lms / 1000.0) / 1e12,
-                "pp_ladder_gbs": work[a]["ladder_bytes"] / (lms / 1000.0) / 1e9,
                 "gpu_launches": int(ta["launches"]),
                 "schedule": tuned[a][0],
                 "schedule_source": "autotuned" if not args.no_autotune else "default",
             }
-        for a in arms:
             # Each ladder class alone: executed rate (packed rows a<=b, K over c<d and hh) and
             # bandwidth; the FP64 wide class holds the largest channels (hh 36..72).
             cls = {}
@@ -398,24 +526,39 @@ def main():
                 cls[name] = {"ms": ms, "tflops_executed": fl / (ms / 1000.0) / 1e12,
                              "gbs": by / (ms / 1000.0) / 1e9}
                 if name.startswith("fp64"):
-                    cls[name]["frac_of_fp64_peak"] = cls[name]["tflops_executed"] / FP64_PEAK_TFLOPS
+                    cls[name]["frac_of_fp64_peak"] = cls[name]["tflops_executed"] / fp64_peak
                 else:
-                    cls[name]["frac_of_hbm_peak"] = cls[name]["gbs"] / peaks["hbm_gbs"]
+                    cls[name]["frac_of_hbm_peak"] = cls[name]["gbs"] / hbm
             arms_out[a]["pp_ladder_classes_alone"] = cls
         # Ring / hh ladder / one-body classes alone (the same kernels in both arms).
         shared = {}
         for name, (ms, fl, by) in other_cls.items():
             shared[name] = {"ms": ms, "gbs": by / (ms / 1000.0) / 1e9,
-                            "frac_of_hbm_peak": by / (ms / 1000.0) / 1e9 / peaks["hbm_gbs"]}
+                            "frac_of_hbm_peak": by / (ms / 1000.0) / 1e9 / hbm}
             if fl > 0:
                 shared[name]["tflops"] = fl / (ms / 1000.0) / 1e12
-                shared[name]["frac_of_fp64_peak"] = shared[name]["tflops"] / FP64_PEAK_TFLOPS
-        if "fp64" in arms_out:
-            f = arms_out["fp64"]
-            f["fp64_peak_tflops"] = FP64_PEAK_TFLOPS
+                shared[name]["frac_of_fp64_peak"] = shared[name]["tflops"] / fp64_peak
         cpu = None
         if not args.no_cpu_baseline:
             cpu = _cpu_baseline(args.config)
+        result = {"precision": PRECISIONS[head], "path": args.path,
+                  "v_pppp": ("generated on the device from the model" if v_mode == "on_the_fly"
+                             else "uploaded from the host"),
+                  "solve_loop": ("batched graph replay" if args.no_device_loop else
+                                 "device (graph WHILE nodes)"),
+                  "iterations_per_solve": t["iters_per_solve"],
+                  "polish_iterations_per_solve": t["polish_per_solve"],
+                  "time_to_converge_ms": t["max_ms"] / args.steps,
+                  "e_corr_per_particle": t["e_corr"] / n_part,
+                  "abs_de_per_particle_vs_reference": t.get("abs_de_per_particle_vs_reference"),
+                  "t2_max_abs_vs_reference": t.get("t2_max_abs_vs_reference"),
+                  "reference_golden": ("tests/golden/%s.npz (reference at tol 1e-12; T2 every "
+                                       "97th element)" % cfg["golden"]) if gold else None,
+                  "fp64_peak_tflops": fp64_peak, "fp64_peak_source": fp64_peak_src,
+                  "parallelism": "replicas" if world > 1 else "single GPU"}
+        if "fp64" in arms_out and head != "fp64":
+            result["speedup_time_to_converge_vs_fp64"] = (
+                arms_out["fp64"]["time_to_converge_ms"] / arms_out[head]["time_to_converge_ms"])
         line = {
             "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -424,43 +567,22 @@ def main():
             "dtype": ("bf16 2-term split operands, f32 accumulate (pp ladder) + f64"
                       if head == "mixed" else "f64"),
             "data": "synthetic",
-            "config": {"workload": desc, "precision": PRECISIONS[head], "path": args.path,
-                       "v_pppp": ("generated on the device from the model"
-                                  if args.v_mode == "on_the_fly" else "uploaded from the host"),
-                       "stop_rule": f"|dE| <= 1e-8 N = {tol:g} (guarantees |dE/N| <= 1e-7)",
-                       "iterations_per_solve": t["iters_per_solve"],
-                       "polish_iterations_per_solve": t["polish_per_solve"],
-                       "e_corr_per_particle": t["e_corr"] / n_part,
-                       "abs_de_per_particle_vs_fp64_converged": t["de_per_particle"],
-                       "time_to_converge_ms": t["max_ms"] / args.steps,
-                       "l2": "flushed (256 MiB write) before every step",
-                       "solve_loop": ("batched graph replay" if args.no_device_loop else
-                                      "device (graph WHILE nodes)"),
-                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "config": config_dict(args.config),
+            "result": result,
             "arms": arms_out,
             "shared_kernels_alone": shared,
             "e2e": {"value": e2e_iters_all / e2e_secs_max, "unit": "iter/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * n_t2,
                     "what": "ccdgpu_create from host buffers (remap tables"
-                            + ("" if args.v_mode == "stored" else " and every V block")
-                            + " made on the device) + ccdgpu_solve + ccdgpu_get_t2",
+                            + ("" if stored else " and every V block")
+                            + " made on the device) + ccdgpu_solve + ccdgpu_get_t2 + "
+                              "ccdgpu_destroy",
                     "rank0_ms_per_step": dict(zip(["create", "solve", "get_t2", "destroy"],
                                                   (1e3 * phase_s / args.steps).round(3).tolist()))},
-            "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved,
-                         "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / peaks["hbm_gbs"], "peak_source": peak_kind,
-                         "traffic": NCU_TRAFFIC.get((args.config, kname), (None, None))[0]
-                         if args.v_mode == "stored" else None,
-                         "traffic_source": NCU_TRAFFIC.get((args.config, kname), (None, None))[1]
-                         if args.v_mode == "stored" else None,
-                         "algorithmic_bytes_per_launch": ladder_bytes,
-                         "avg_launch_ms": ladder_ms},
+            "roofline": {**roof[head][dominant], "family": dominant, "peak_source": peak_kind},
             "gpu_launches": int(t["launches"]),
             "clocks": clocks.summary(),
         }
-        if "fp64" in arms_out and head != "fp64":
-            line["config"]["speedup_time_to_converge_vs_fp64"] = (
-                arms_out["fp64"]["time_to_converge_ms"] / arms_out[head]["time_to_converge_ms"])
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line))
@@ -603,20 +725,23 @@ def _problem_bytes(system, with_v_pppp=True, with_tables=True, with_v=True):
     return v + tables + meta
 
 
-def _cpu_baseline(cfg):
-    exe = os.path.join(REPO, "oracle", "_ref", "ccd.exe")
-    if not os.path.exists(exe):
+def _cpu_baseline(name, steps=2):
+    """The reference's loop on this host's cores (oracle/_ref, bench mode): one set-up, then
+    `steps` bounded samples of the workload's solve; None when the reference build is
+    missing or fails."""
+    if not os.path.exists(os.path.join(REPO, "oracle", "_ref", "ref_harness")):
         return None
-    cores = os.cpu_count() or 1
-    kind = CONFIGS[cfg][1]
     try:
-        it, secs, _ = reference_run(cfg, cores, timeout=120)
-    except (subprocess.SubprocessError, IndexError, OSError):
+        rows, setup, threads = reference_bench(name, steps, timeout=900)
+    except (subprocess.SubprocessError, RuntimeError, OSError, ValueError):
         return None
-    return {"value": it / secs, "unit": "iter/s", "cores": 1 if kind == "pairing" else cores,
-            "kind": "reference",
-            "sample": f"one full solve of the workload by the reference build ({it} iterations, "
-                      f"cc_diagrams_time {secs:.3f} s, OMP threads = cores, 1 MPI rank)"}
+    it = sum(r[0] for r in rows)
+    secs = sum(r[1] for r in rows)
+    return {"value": it / secs, "unit": "iter/s", "cores": threads, "kind": "reference",
+            "sample": f"{steps} solves from T2 = 0 of the workload, each capped at "
+                      f"{CONFIGS[name]['ref_iters']} iterations ({it} iterations, {secs:.3f} s "
+                      f"of loop time) by the reference build after one set-up ({setup:.1f} s, "
+                      f"untimed); OMP threads = {threads}, 1 MPI rank"}
 
 
 if __name__ == "__main__":

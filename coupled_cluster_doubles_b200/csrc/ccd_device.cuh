@@ -209,6 +209,9 @@ struct Control {
   int32_t active;        // 1 while a solve is running (0: kernels run unconditionally)
   int32_t phase;         // mixed-precision solve: 1 = split-bf16 ladder, 2 = FP64 polish
   int32_t retile;        // the FP64 ladder operand tiles are stale (a mixed iteration ran)
+  int32_t inject;        // test-only fault: 1 = the first FP64 pp-ladder CTA of each class
+                         // withholds its first stage (its bounded waits run out)
+  int32_t pad0;
   double polish_rel;     // phase 1 -> 2 once |dE| <= max(tol, polish_rel * |E|)
   int64_t polish_iters;  // iterations run in phase 2
   int64_t stop_at;       // device solve loop: one graph launch runs while iterations < stop_at

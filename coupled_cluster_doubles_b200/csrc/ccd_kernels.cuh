@@ -329,6 +329,9 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restrict
     if (lane == 0) {
       int gc = 0;  // chunks issued by this CTA
       bool stop = false;
+      // Test-only fault (ccdgpu_inject_wait_timeout): CTA 0 never fills its first stage, so
+      // its consumers' bounded waits run out, then this producer's wait for that stage does.
+      const bool withhold = ctl->inject != 0 && blockIdx.x == 0;
       for (int ti = t_begin; ti < t_end && !stop; ++ti) {
         const LadderTile tile = tiles[ti];
         const int ar = ladder_arows(tile.nb, tile.rows);
@@ -345,6 +348,7 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restrict
             stop = true;
             break;
           }
+          if (withhold && gc == 0) continue;
           const double *asrc, *bsrc;
           if (c < tile.nks) {
             const int kc = tile.kc0 + c;

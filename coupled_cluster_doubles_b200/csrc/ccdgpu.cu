@@ -104,6 +104,7 @@ struct ccdgpu_handle {
   cudaGraphExec_t graph = nullptr;
   int64_t kernels_per_graph = 0;
   bool profiling = false;
+  bool inject_next_step = false;  // ccdgpu_inject_wait_timeout armed for the next step
   ccdgpu_profile prof{};
   double flops = 0, v_bytes = 0, v_packed_bytes = 0, ladder_flops = 0, ladder_bytes = 0;
   int64_t n_tkt = 0, n_tmt = 0;
@@ -1618,7 +1619,12 @@ int sync_ctl(ccdgpu_handle *h) {
 int check_errors(ccdgpu_handle *h) {
   int32_t e = 0;
   CK(cudaMemcpy(&e, h->err, sizeof(int32_t), cudaMemcpyDeviceToHost));
-  if (e & kErrTimeout) return CCDGPU_ERR_TIMEOUT;
+  if (e & kErrTimeout) {
+    // Reported once: the handle stays usable (the timed-out iteration's amplitudes are
+    // incomplete; ccdgpu_reset or ccdgpu_set_t2 starts over).
+    CK(cudaMemset(h->err, 0, sizeof(int32_t)));
+    return CCDGPU_ERR_TIMEOUT;
+  }
   if (h->h_ctl->error & kErrNonFinite) return CCDGPU_ERR_NONFINITE;
   return CCDGPU_OK;
 }
@@ -2064,10 +2070,20 @@ int ccdgpu_get_t2(ccdgpu_handle *h, double *t2, uint64_t n) {
 int ccdgpu_step(ccdgpu_handle *h, double mixing, double *e_corr) {
   if (!h) return CCDGPU_ERR_INVALID_ARGUMENT;
   CK(cudaSetDevice(h->opt.device));
+  const bool inject = h->inject_next_step;
+  h->inject_next_step = false;
   int rc = set_ctl(h, 0, h->h_ctl->tol, INT64_MAX / 2, mixing, false);
   if (rc) return rc;
+  if (inject) {
+    const int32_t one = 1;
+    CK(cudaMemcpyAsync(&h->ctl->inject, &one, sizeof(one), cudaMemcpyHostToDevice, h->s0));
+  }
   if (h->opt.path == CCDGPU_PATH_TABLES) rc = tables_iteration(h, mixing, nullptr);
   else rc = enqueue_fused_iteration(h, h->nt > 0);
+  if (inject) {  // the fault applies to this iteration only
+    const int32_t zero = 0;
+    CK(cudaMemcpyAsync(&h->ctl->inject, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->s0));
+  }
   if (rc) return rc;
   if ((rc = sync_ctl(h))) return rc;
   if ((rc = check_errors(h))) return rc;
@@ -2328,6 +2344,12 @@ int ccdgpu_enable_profiling(ccdgpu_handle *h, int32_t on) {
   return CCDGPU_OK;
 }
 void *ccdgpu_stream(ccdgpu_handle *h) { return h ? (void *)h->s0 : nullptr; }
+
+int ccdgpu_inject_wait_timeout(ccdgpu_handle *h) {
+  if (!h) return CCDGPU_ERR_INVALID_ARGUMENT;
+  h->inject_next_step = true;
+  return CCDGPU_OK;
+}
 
 // Each pp-ladder class launched alone (FP64 thin, mid, wide; tensor-core ladder), `reps` times
 // between CUDA events on the handle's stream; with the executed flops (packed: rows a<=b, K over

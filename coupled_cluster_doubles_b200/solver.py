@@ -244,6 +244,11 @@ class CCDSolver:
         t0 = min(first[k] for k in ran)
         return {self.TRACE_KERNELS[k]: (first[k] - t0, last[k] - t0) for k in ran}
 
+    def inject_wait_timeout(self):
+        """Failure-path test hook (ccdgpu_inject_wait_timeout): the next step() makes a bounded
+        device wait of the FP64 pp ladder run out and raises CCDGPUError(CCDGPU_ERR_TIMEOUT)."""
+        _check(_native.gpu_lib().ccdgpu_inject_wait_timeout(self._h), "inject_wait_timeout")
+
     def stream_ptr(self):
         """The handle's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
         return _native.gpu_lib().ccdgpu_stream(self._h)

@@ -118,18 +118,26 @@ enum ccdgpu_status {
   CCDGPU_ERR_NO_DEVICE = -6,
   CCDGPU_ERR_UNSUPPORTED = -7,
   CCDGPU_ERR_NOT_CONVERGED = -8,   /* only from ccdgpu_solve when require_convergence is set */
-  CCDGPU_ERR_TIMEOUT = -9          /* wall-clock limit of ccdgpu_solve reached */
+  CCDGPU_ERR_TIMEOUT = -9          /* a bounded device-side wait (an mbarrier of a pipelined
+                                      kernel) ran out (1 s of %globaltimer); the kernel stopped
+                                      cleanly and the handle stays usable */
 };
 
 enum ccdgpu_precision {
-  CCDGPU_PREC_FP64 = 0,        /* FP64 throughout (FP64 FMA-pipe contractions) */
+  CCDGPU_PREC_FP64 = 0,        /* FP64 throughout: FP64 tensor-core MMA (mma.sync f64) for
+                                  the mid/wide pp-ladder classes, the hh ladder and the ring,
+                                  FP64 FMA for the thinnest pp-ladder channels */
   CCDGPU_PREC_MIXED_BF16 = 1,  /* pp ladder on tensor cores with 2-term bf16 split operands,
                                   FP32 accumulation; FP64 polish iterations at the end */
   CCDGPU_PREC_MIXED_BF16X3 = 2 /* the same with 3-term bf16 split operands */
 };
 enum ccdgpu_v_mode {
   CCDGPU_V_STORED = 0,         /* V_pppp uploaded from the host blocks */
-  CCDGPU_V_ON_THE_FLY = 1      /* V_pppp regenerated inside the pp-ladder kernel from the model */
+  CCDGPU_V_ON_THE_FLY = 1      /* V_pppp generated on the device from the model
+                                  (ccdgpu_problem.model) instead of uploaded: at create, into
+                                  the FP64 ladder tiles and bf16 images; electron gas with the
+                                  tensor-core ladder: regenerated inside the ladder kernel
+                                  every iteration and never stored */
 };
 enum ccdgpu_path {
   CCDGPU_PATH_FUSED = 0,       /* fused kernels: one-body terms from the ladder intermediates,
@@ -280,6 +288,14 @@ int ccdgpu_enable_profiling(ccdgpu_handle *h, int32_t on);
 /* The handle's main CUDA stream (cudaStream_t), for callers that time or order work on it. */
 void *ccdgpu_stream(ccdgpu_handle *h);
 
+/* Failure-path test hook; no counterpart in the reference.  Arms a fault for the next
+ * ccdgpu_step only: in that iteration the first CTA of every FP64 pp-ladder class withholds
+ * its first shared-memory stage, so its bounded mbarrier waits run out after 1 s; the kernel
+ * stops cleanly and ccdgpu_step returns CCDGPU_ERR_TIMEOUT.  The handle stays usable (the
+ * error is reported once), but that iteration's amplitudes are incomplete: call ccdgpu_reset
+ * or ccdgpu_set_t2 before iterating on.  Affects only iterations that run the FP64 ladder. */
+int ccdgpu_inject_wait_timeout(ccdgpu_handle *h);
+
 /* Work of one iteration for roofline reporting: *flops = reference GEMM flops (sum over
  * channels of 2 pp^2 hh + 4 pp hh^2 + 4 ph' hp'^2); *ladder_bytes = bytes one pp-ladder launch
  * moves (antisymmetry-packed V_pppp, the T and X operands, D) at the handle's precision (FP64
@@ -331,20 +347,20 @@ int ccdgpu_trace_arm(ccdgpu_handle *h, int64_t iteration);
 int ccdgpu_trace_read(ccdgpu_handle *h, uint64_t *first, uint64_t *last, int32_t n);
 
 /* No counterpart in the reference.  The ladder term of one regular channel,
- * D = 0.5 T X + 0.5 V_pppp T with X = V_hhhh + 0.5 V_hhpp T (the arithmetic of
- * calcChannelT2Diff_pphh), for callers that cannot allocate device memory, such as a host
- * that owns all device memory through its own pool or budget.  Nothing is allocated: every
- * argument is a caller-provided device buffer (reference row-major layouts: v_pppp pp x pp,
- * v_hhpp hh x pp, v_hhhh hh x hh, t2 pp x hh, d pp x hh), and the intermediate X with its
- * split-K partial sums lives in a fixed 2 MiB scratch array built into the library (one per
- * GPU that loads it, kept until the process exits).  Limits: hh <= 72 and
- * 32 + (ceil(pp/64) + 1) * hh^2 <= 262144 doubles; larger sizes return
- * CCDGPU_ERR_UNSUPPORTED without launching anything.  Work is enqueued on `stream`
+ *   D = 0.5 T X + 0.5 V_pppp T   with   X = V_hhhh + 0.5 V_hhpp T,
+ * for callers that cannot allocate device memory, such as a host that owns all device memory
+ * through its own pool or budget.  Nothing is allocated: every argument is a caller-provided
+ * device buffer (row-major: v_pppp pp x pp, v_hhpp hh x pp, v_hhhh hh x hh, t2 pp x hh,
+ * d pp x hh), and the intermediate X with its split-K partial sums lives in a fixed 2 MiB
+ * scratch array built into the library (one per GPU that loads it, kept until the process
+ * exits).  Limits: hh <= 72 and 32 + (ceil(pp/64) + 1) * hh^2 <= 262144 doubles; larger sizes
+ * return CCDGPU_ERR_UNSUPPORTED without launching anything.  Work is enqueued on `stream`
  * (a cudaStream_t; NULL = legacy default stream) for the current device.  The first call on a
  * device looks up the scratch address (cudaGetSymbolAddress) and sets a kernel attribute; make
- * that first call before any stream capture.  Every call shares the one scratch array, which
- * keeps the last call's contents: calls whose work overlaps on the GPU (different streams
- * without ordering) race and must not be issued. */
+ * that first call before any stream capture.  Both are remembered for the life of the process,
+ * so cudaDeviceReset after the first call is not supported.  Every call shares the one scratch
+ * array, which keeps the last call's contents: calls whose work overlaps on the GPU (different
+ * streams without ordering) race and must not be issued. */
 int ccdgpu_calc_channel_t2diff_pphh_noalloc(const double *v_pppp, const double *v_hhpp,
                                             const double *v_hhhh, const double *t2, double *d,
                                             int64_t pp, int64_t hh, void *stream);

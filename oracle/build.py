@@ -10,7 +10,8 @@ import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
-REF_SRC = "/root/reference/src"
+# The reference sources; CCD_REF_SRC overrides the default location.
+REF_SRC = os.environ.get("CCD_REF_SRC", "/root/reference/src")
 GXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 GCC = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
 
@@ -39,7 +40,8 @@ def build_ref():
     previous build are available."""
     out = os.path.join(HERE, "_ref")
     if os.path.isdir(REF_SRC):
-        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "ref"), "-j8"], check=True)
+        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "ref"), "-j8", "REF_SRC=" + REF_SRC],
+                       check=True)
     if os.path.exists(os.path.join(out, "ccd.exe")):
         return out
     return None

@@ -10,6 +10,7 @@
 //   when CCD_DUMP_V=1).
 //
 // Usage: CCD_DUMP=out.bin [CCD_DUMP_V=1] ref_harness <ccd.exe options>
+//        CCD_BENCH=steps,iterations,tol ref_harness <ccd.exe options>   (timing only)
 // The dump format is read by oracle/refdump.py.
 #include <cstdio>
 #include <cstdlib>
@@ -199,45 +200,73 @@ int main(int argc, char *argv[]) {
   MapDistributedData *t_ai_jb = m_ai_jb.mapToDistributedCreate(0, nch, s0, e_ch, MPI_COMM_WORLD);
   double t_load1 = omp_get_wtime();
 
-  double mbpt2 = MBPT2Corr(0, nch, v_hhpp, basis);
-
-  t2.zero(); t2Old.zero(); t2Old_h2pp_h1.zero(); t2Old_h1pp_h2.zero();
-  t2Old_p1_p2hh.zero(); t2Old_p2_p1hh.zero(); t2Old_phhp.zero();
+  // Bench mode (CCD_BENCH="steps,iterations,tol"): after the one set-up above, `steps`
+  // solves from T2 = 0, each a bounded sample of at most `iterations` iterations of the loop
+  // below (stopping earlier at |dE| <= tol), timed like cc_diagrams_time; one line per step.
+  const char *bench = getenv("CCD_BENCH");
+  long bench_steps = 0, bench_iters = 0;
+  double bench_tol = 0;
+  if (bench && sscanf(bench, "%ld,%ld,%lf", &bench_steps, &bench_iters, &bench_tol) != 3) {
+    fprintf(stderr, "CCD_BENCH must be steps,iterations,tol\n");
+    return 2;
+  }
+  double mbpt2 = bench ? 0.0 : MBPT2Corr(0, nch, v_hhpp, basis);
 
   // Iteration loop: same stop rule, cap and mixing as main.cpp:491-519.
   double energyDiff = 1.0, corrCCD = 100.0, corrPrev = 100.0, mixing = 0.5;
   unsigned long iterations = 0;
   int max_iters = 100;
   std::vector<double> energies;
-  double cc0 = omp_get_wtime();
-  while (std::abs(energyDiff) > tolerance) {
-    if (iterations > (unsigned long)max_iters) break;
-    calcT2Diff_p2_p1hh(0, nsp - np, v_phh_p, t2Old_p1_p2hh, t2Old_p2_p1hh, t2Diff_p2_p1hh, basis);
-    calcT2Diff_h2pp_h1(0, np, v_h_hpp, t2Old_h1pp_h2, t2Old_h2pp_h1, t2Diff_h2pp_h1, basis);
-    calcT2Diff_phhp(0, nch, v_hpph_mod, v_hphp_mod, t2Old_phhp, t2Diff_phhp, basis);
-    calcT2Diff_pphh(0, nch, v_hhhh, v_hhpp, v_pppp, t2Old, t2Diff, basis);
-    d_iab_j.mapFromDistributed(&t2Diff_h2pp_h1, f_iab_j);
-    d_jab_i.mapFromDistributed(&t2Diff_h2pp_h1, f_jab_i);
-    d_a_bij.mapFromDistributed(&t2Diff_p2_p1hh, f_a_bij);
-    d_b_aij.mapFromDistributed(&t2Diff_p2_p1hh, f_b_aij);
-    d_ai_jb.mapFromDistributed(&t2Diff_phhp, f_ai_jb);
-    d_aj_ib.mapFromDistributed(&t2Diff_phhp, f_aj_ib);
-    d_bi_ja.mapFromDistributed(&t2Diff_phhp, f_bi_ja);
-    d_bj_ia.mapFromDistributed(&t2Diff_phhp, f_bj_ia);
-    double corr = calcT2_pphh(0, nch, v_hhpp, t2, t2Diff, t2Old, d_iab_j, d_jab_i, d_a_bij,
-                              d_b_aij, d_ai_jb, d_aj_ib, d_bi_ja, d_bj_ia, basis, mixing);
-    t2Old.set(&t2);
-    t2.mapToDistributed(&t2Old_h2pp_h1, t_jab_i);
-    t2.mapToDistributed(&t2Old_h1pp_h2, t_iab_j);
-    t2.mapToDistributed(&t2Old_p1_p2hh, t_a_bij);
-    t2.mapToDistributed(&t2Old_p2_p1hh, t_b_aij);
-    t2.mapToDistributed(&t2Old_phhp, t_ai_jb);
-    corrCCD = corr;
-    energyDiff = corrCCD - corrPrev;
-    corrPrev = corrCCD;
-    energies.push_back(corrCCD);
-    iterations++;
+  auto solve = [&](double tol, unsigned long cap) {
+    t2.zero(); t2Old.zero(); t2Old_h2pp_h1.zero(); t2Old_h1pp_h2.zero();
+    t2Old_p1_p2hh.zero(); t2Old_p2_p1hh.zero(); t2Old_phhp.zero();
+    energyDiff = 1.0; corrCCD = 100.0; corrPrev = 100.0;
+    iterations = 0;
+    energies.clear();
+    while (std::abs(energyDiff) > tol) {
+      if (iterations > (unsigned long)max_iters || iterations >= cap) break;
+      calcT2Diff_p2_p1hh(0, nsp - np, v_phh_p, t2Old_p1_p2hh, t2Old_p2_p1hh, t2Diff_p2_p1hh, basis);
+      calcT2Diff_h2pp_h1(0, np, v_h_hpp, t2Old_h1pp_h2, t2Old_h2pp_h1, t2Diff_h2pp_h1, basis);
+      calcT2Diff_phhp(0, nch, v_hpph_mod, v_hphp_mod, t2Old_phhp, t2Diff_phhp, basis);
+      calcT2Diff_pphh(0, nch, v_hhhh, v_hhpp, v_pppp, t2Old, t2Diff, basis);
+      d_iab_j.mapFromDistributed(&t2Diff_h2pp_h1, f_iab_j);
+      d_jab_i.mapFromDistributed(&t2Diff_h2pp_h1, f_jab_i);
+      d_a_bij.mapFromDistributed(&t2Diff_p2_p1hh, f_a_bij);
+      d_b_aij.mapFromDistributed(&t2Diff_p2_p1hh, f_b_aij);
+      d_ai_jb.mapFromDistributed(&t2Diff_phhp, f_ai_jb);
+      d_aj_ib.mapFromDistributed(&t2Diff_phhp, f_aj_ib);
+      d_bi_ja.mapFromDistributed(&t2Diff_phhp, f_bi_ja);
+      d_bj_ia.mapFromDistributed(&t2Diff_phhp, f_bj_ia);
+      double corr = calcT2_pphh(0, nch, v_hhpp, t2, t2Diff, t2Old, d_iab_j, d_jab_i, d_a_bij,
+                                d_b_aij, d_ai_jb, d_aj_ib, d_bi_ja, d_bj_ia, basis, mixing);
+      t2Old.set(&t2);
+      t2.mapToDistributed(&t2Old_h2pp_h1, t_jab_i);
+      t2.mapToDistributed(&t2Old_h1pp_h2, t_iab_j);
+      t2.mapToDistributed(&t2Old_p1_p2hh, t_a_bij);
+      t2.mapToDistributed(&t2Old_p2_p1hh, t_b_aij);
+      t2.mapToDistributed(&t2Old_phhp, t_ai_jb);
+      corrCCD = corr;
+      energyDiff = corrCCD - corrPrev;
+      corrPrev = corrCCD;
+      energies.push_back(corrCCD);
+      iterations++;
+    }
+  };
+  if (bench) {
+    printf("setup_time: %f\nload_time: %f\n", t_setup1 - t_setup0, t_load1 - t_setup1);
+    for (long k = 0; k < bench_steps; k++) {
+      double b0 = omp_get_wtime();
+      solve(bench_tol, (unsigned long)bench_iters);
+      double b1 = omp_get_wtime();
+      printf("bench_step: %lu %.9f %.17g\n", iterations, b1 - b0, corrCCD);
+      fflush(stdout);
+    }
+    parseFree(parseMem);
+    MPI_Finalize();
+    return 0;
   }
+  double cc0 = omp_get_wtime();
+  solve(tolerance, ~0ul);
   double cc1 = omp_get_wtime();
 
   printf("iterations: %lu\n", iterations);

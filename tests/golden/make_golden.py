@@ -58,6 +58,14 @@ CONFIGS = {
                      "pairing", dict(xi=1.0, g=0.3, n_pair_states=6, n_particles=4), True),
     "eg38_s16": (["--electronGas", "-r", "1.0", "-s", "16", "-p", "3", "-t", "1e-10"],
                  "electron_gas", dict(r_s=1.0, n_shells=16, n_particle_shells=3), False),
+    # The large workloads: 1850 spin-orbitals (|n|^2 <= 36), hh up to 54 / 66.
+    "eg54c36_r2": (["--electronGas", "-r", "2.0", "-s", "32", "-p", "4", "-t", "1e-12"],
+                   "electron_gas", dict(r_s=2.0, n_shells=32, n_particle_shells=4), False),
+    "eg54c36_r05": (["--electronGas", "-r", "0.5", "-s", "32", "-p", "4", "-t", "1e-12"],
+                    "electron_gas", dict(r_s=0.5, n_shells=32, n_particle_shells=4), False),
+    "pnm66_s32": (["--infMatter", "-d", "0.08", "-z", "1", "-s", "32", "-p", "5", "-t", "1e-12"],
+                  "inf_matter", dict(density=0.08, tz_max=1, n_shells=32, n_particle_shells=5),
+                  False),
 }
 
 STRUCT = ["chan_dims", "chan_mod_dims", "three_body_dims", "pp_map", "hh_map", "ph_mod_map",
