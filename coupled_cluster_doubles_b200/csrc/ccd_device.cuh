@@ -150,6 +150,10 @@ struct ChanInfo {
   // nbt = UMMA N, nkct / nkht = 32-deep K chunks of V T / T X.
   int32_t nbt, nkct, nkht, pad_tc;
   int64_t vtc_base, tkt_tc_base, tmt_tc_base, xt_tc_base;
+  // Fused assembly: hk = strict hole pairs (i < j); quad tables from qrow_off (pk strict
+  // packed rows a < b) and qcol_off (hk entries).
+  int32_t hk, pad_q;
+  int64_t qrow_off, qcol_off;
 };
 
 // hh-ladder unit: rows [k0, k0+rows) of channel ch (slice idx), a chunk of P rows.
@@ -157,19 +161,25 @@ struct HHTile {
   int32_t ch, k0, idx, rows, chunk, pad;
 };
 
-// Fused assembly, static data of packed row u of a channel (index row_off + u): rows ab and
-// ba = mirror (ba = ab when a = b) as offsets ab * hh, ba * hh in the channel block, their
-// ladder operand indices (pk_idx), the particle indices a - np, b - np and e_a, e_b.
-struct AsmRowStatic {
+// Fused assembly, static data of strict packed row u (a < b) of a channel (index
+// qrow_off + u): offsets of rows ab and ba inside the channel block (ab * hh, ba * hh), the
+// operand-image indices of row ab (pk_idx: K index, packed row), particle indices a - np,
+// b - np, and e_a, e_b ...
+struct QuadRow {
   int32_t o_ab, o_ba;
-  int32_t qa_x, qa_y, qb_x, qb_y;
+  int32_t qx, qy;
   int32_t pa, pb;
   double ea, eb;
 };
-// ... and of column j (index hh_off + j): ji, the hole indices i, j and e_i + e_j.
-struct AsmColStatic {
-  int32_t js, i, j, pad;
+// ... and of strict hole pair w (i < j, index qcol_off + w): the columns ij and ji, the hole
+// indices i, j and e_i + e_j.
+struct QuadCol {
+  int32_t c_ij, c_ji, i, j;
   double eij;
+};
+// Work item of the fused assembly: quads [q0, q1) (q = u * hk + w) of active channel ch.
+struct QuadItem {
+  int32_t ch, q0, q1, pad;
 };
 
 // Per active modified channel.

@@ -919,7 +919,7 @@ __device__ __forceinline__ void write_t_tiles_tc(const ChanInfo &ch, int2 q, int
 // (mapToDistributed ai_jb, a scattered write) and into the ladder operand tiles.
 // ------------------------------------------------------------------------------------------
 constexpr int kAsmThreads = 256;
-constexpr int kAsmPerThread = 2;  // elements per thread; a CTA covers one ElemRange
+constexpr int kAsmPerThread = 2;  // table path: elements per thread of an ElemRange
 __device__ __forceinline__ void energy_reduce(const double *epart, int n, Control *ctl, int flags,
                                               double *e_out);
 // Condition of the device solve loop's WHILE node after an iteration: another iteration while
@@ -933,105 +933,62 @@ __device__ __forceinline__ void loop_set_condition(const Control *ctl,
   cudaGraphSetConditional(cond, (more && (body_mixed ? mixed_phase : !mixed_phase)) ? 1u : 0u);
 }
 
-// In a mixed iteration (nt > 0) the assembly writes only the bf16 ladder operand images;
-// retile_kernel rebuilds the FP64 tiles if FP64 iterations follow.
-// Work is organised over packed elements (u, j): packed row u (a <= b) of a channel and column
-// j.  A CTA owns whole packed rows [u0, u1) of one channel (ElemRange over q = u * hh + j, row
-// aligned, about kAsmPerCTA elements) and first stages the small tables of those rows and of
-// the channel's columns in shared memory (row offsets of ab and ba, y_a, y_b, e_a, e_b; column
-// swap j -> ji, x_i, x_j, e_i + e_j), so that every element then needs a single round of
-// independent global loads.  A thread computes element (ab, j) and its mirror (ba, j)
-// together: both need t and R at (ab,j), (ab,ji), (ba,j), (ba,ji), read once.
-constexpr int kAsmPerCTA = 2 * kAsmThreads;
-constexpr int kAsmMaxRows = kAsmPerCTA;  // rows of a CTA (hh >= 1)
-constexpr int kAsmMaxCols = 96;
+// Work is organised over quads (u, w): strict packed row u (a < b) of a channel and strict hole
+// pair w (i < j).  The amplitudes are antisymmetric, t_ab,ij = -t_ab,ji = -t_ba,ij = t_ba,ji,
+// and so are V, D and the combination of the four R terms; the fused path keeps them exactly
+// so (the ladders write D[ba] = -D[ab]; a quad writes its four elements as +t, -t, -t, +t), and
+// rows a = b or columns i = j hold zeros that no iteration changes.  One thread computes the
+// quad's element (ab, ij) from V, D, t at (ab, ij) and R at the four positions, and writes all
+// four elements, their phhp copies and the operand-image entries of rows ab (row ba is in
+// neither image).  The energy gains 4 V t_new per quad.
+// Persistent CTAs stride over work items of up to kQuadPerItem quads of one channel; a thread
+// takes kQuadPerThread quads of an item and issues all their loads before the first store.
+// In a mixed iteration (nt > 0) only the bf16 operand images are written; retile_kernel
+// rebuilds the FP64 tiles if FP64 iterations follow.
+constexpr int kQuadPerThread = 1;
+constexpr int kQuadPerItem = kQuadPerThread * kAsmThreads;
+constexpr int kAsmCTAsPerSM = 4;
 
-// value of one element (calc.cpp:384-418) of row r with mirror row m (m = r for a = b):
+// value of element (ab, ij) (calc.cpp:384-418) with t_ab,ji = -t and t_ba,ij = -t:
 //   V + D + R_ai,jb - R_aj,ib - R_bi,ja + R_bj,ia + 0.5 x_i t_ab,ji - 0.5 x_j t_ab,ij
-//     + (-0.5 y_b) t_ab,ij - (-0.5 y_a) t_ba,ij          with (a, b) = pab of row r.
-__device__ __forceinline__ double asm_value(double v, double dm, double r_j, double r_js,
-                                            double rm_j, double rm_js, double t_j, double t_js,
-                                            double tm_j, double xi, double xj, double ya,
-                                            double yb, double den, double mixing) {
+//     + (-0.5 y_b) t_ab,ij - (-0.5 y_a) t_ba,ij
+__device__ __forceinline__ double quad_value(double v, double dm, double r1, double r2, double r3,
+                                             double r4, double t, double xi, double xj,
+                                             double ya, double yb, double den, double mixing) {
   double value = v;
   value += dm;
-  value += r_j;
-  value -= r_js;
-  value -= rm_j;
-  value += rm_js;
-  value += (0.5 * xi) * t_js;
-  value -= (0.5 * xj) * t_j;
-  value += (-0.5 * yb) * t_j;
-  value -= (-0.5 * ya) * tm_j;
+  value += r1;
+  value -= r2;
+  value -= r3;
+  value += r4;
+  value += (0.5 * xi) * (-t);
+  value -= (0.5 * xj) * t;
+  value += (-0.5 * yb) * t;
+  value -= (-0.5 * ya) * (-t);
   value = value / den;
-  return mixing * value + (1. - mixing) * t_j;
+  return mixing * value + (1. - mixing) * t;
 }
-
-// Shared-memory tables of a CTA's rows and of its channel's columns: the static parts come from
-// AsmRowStatic / AsmColStatic (built at create), y_a, y_b, x_i, x_j are the current one-body sums.
-struct AsmRowInfo {
-  int32_t o_ab, o_ba;  // row offsets inside the channel block (ab * hh, ba * hh; equal if a = b)
-  int2 qa, qb;         // ladder operand indices of rows ab and ba (pk_idx)
-  int32_t pa, pb;      // particle indices a - np, b - np
-  double ya, yb, ea, eb;
-};
-struct AsmColInfo {
-  int32_t js, i, j, pad;
-  double xi, xj, eij;
-};
 
 // LOOP: launched as the last kernel of a device-solve-loop body (sets the WHILE condition);
 // the variant without it is the one profilers can replay.
 template <bool LOOP>
-__global__ void __launch_bounds__(kAsmThreads, 3)
-assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__restrict__ chans,
-                      const AsmRowStatic *__restrict__ asm_rows,
-                      const AsmColStatic *__restrict__ asm_cols,
-                      const double *__restrict__ v_pphh, const double *__restrict__ dmat,
-                      const double *__restrict__ d_ring, const int32_t *__restrict__ g_ai_jb,
-                      double *__restrict__ old_phhp, const double *__restrict__ xh,
-                      const double *__restrict__ yp, double *tbuf0, double *tbuf1,
-                      double *__restrict__ t_kt, double *__restrict__ t_mt,
-                      double *__restrict__ epart, int32_t *ticket, Control *ctl,
-                      __nv_bfloat16 *__restrict__ tkt_tc, int64_t tkt_tc_stride,
+__global__ void __launch_bounds__(kAsmThreads, kAsmCTAsPerSM)
+assemble_fused_kernel(const QuadItem *__restrict__ items, int n_items,
+                      const ChanInfo *__restrict__ chans, const QuadRow *__restrict__ qrows,
+                      const QuadCol *__restrict__ qcols, const double *__restrict__ v_pphh,
+                      const double *__restrict__ dmat, const double *__restrict__ d_ring,
+                      const int32_t *__restrict__ g_ai_jb, double *__restrict__ old_phhp,
+                      const double *__restrict__ xh, const double *__restrict__ yp,
+                      double *tbuf0, double *tbuf1, double *__restrict__ t_kt,
+                      double *__restrict__ t_mt, double *__restrict__ epart, int32_t *ticket,
+                      Control *ctl, __nv_bfloat16 *__restrict__ tkt_tc, int64_t tkt_tc_stride,
                       __nv_bfloat16 *__restrict__ tmt_tc, int64_t tmt_tc_stride, int nt,
                       cudaGraphConditionalHandle cond, int loop_body, int gate) {
   // loop_body: 0 outside the device solve loop, 1 / 2 last kernel of its FP64 / mixed body,
   // where the CTA that applies the stop rule also sets the loop condition.  A skipped body
   // (stop rule fired, or the other precision's phase) ends its loop.
-  __shared__ AsmRowInfo rows[kAsmMaxRows];
-  __shared__ AsmColInfo cols[kAsmMaxCols];
   __shared__ double scratch[32];
   __shared__ int last;
-  // The CTA's range, channel and static tables are written only at create: they are read
-  // before waiting for this iteration's earlier kernels (skip_iteration), so that their load
-  // latency overlaps those kernels' tail.  A thread later completes the rows and columns it
-  // staged itself.
-  const ElemRange rg = pranges[blockIdx.x];
-  const ChanInfo ch = chans[rg.ch];
-  const int hh = ch.hh;
-  const int u0 = (int)(rg.e0 / hh), nrows = (int)(rg.e1 / hh) - u0;
-  for (int r = threadIdx.x; r < nrows; r += kAsmThreads) {
-    const AsmRowStatic s = asm_rows[ch.row_off + u0 + r];
-    AsmRowInfo &ri = rows[r];
-    ri.o_ab = s.o_ab;
-    ri.o_ba = s.o_ba;
-    ri.qa = make_int2(s.qa_x, s.qa_y);
-    ri.qb = make_int2(s.qb_x, s.qb_y);
-    ri.pa = s.pa;
-    ri.pb = s.pb;
-    ri.ea = s.ea;
-    ri.eb = s.eb;
-  }
-  for (int j = threadIdx.x; j < hh; j += kAsmThreads) {
-    const AsmColStatic s = asm_cols[ch.hh_off + j];
-    AsmColInfo &ci = cols[j];
-    ci.js = s.js;
-    ci.i = s.i;
-    ci.j = s.j;
-    ci.pad = 0;
-    ci.eij = s.eij;
-  }
   if (skip_iteration(ctl, gate, kTrAssemble)) {
     if constexpr (LOOP)
       if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0u);
@@ -1040,73 +997,72 @@ assemble_fused_kernel(const ElemRange *__restrict__ pranges, const ChanInfo *__r
   const double *__restrict__ t_old = ctl->parity ? tbuf1 : tbuf0;
   double *__restrict__ t_new = ctl->parity ? tbuf0 : tbuf1;
   const double mixing = ctl->mixing;
-  // The current one-body sums y_a, y_b, x_i, x_j (same thread, same entries as above).
-  for (int r = threadIdx.x; r < nrows; r += kAsmThreads) {
-    rows[r].ya = yp[rows[r].pa];
-    rows[r].yb = yp[rows[r].pb];
-  }
-  for (int j = threadIdx.x; j < hh; j += kAsmThreads) {
-    cols[j].xi = xh[cols[j].i];
-    cols[j].xj = xh[cols[j].j];
-  }
-  __syncthreads();
-  const double *tb = t_old + ch.t_off, *rb = d_ring + ch.t_off, *vb = v_pphh + ch.t_off;
-  const double *db = dmat + ch.t_off;
-  const int32_t *gb = g_ai_jb + ch.t_off;
-  double *nb = t_new + ch.t_off;
-  const int n = nrows * hh;
-  // q / hh as a multiply-high by ceil(2^32 / hh) (Granlund-Montgomery): exact for
-  // q < 2^32 / hh (q < 2^11 here); hh = 1 has no 32-bit multiplier and divides trivially.
-  const uint32_t hh_magic = hh > 1 ? 0xFFFFFFFFu / (uint32_t)hh + 1u : 0u;
   double corr = 0.0;
-  // kAsmPerThread elements per thread: every load of all of them is issued before the first
-  // store (t_new may alias t_old for the compiler, which would otherwise serialise them).
-  for (int q0 = threadIdx.x; q0 < n; q0 += kAsmPerThread * kAsmThreads) {
-    double tv[kAsmPerThread][4], rv[kAsmPerThread][4], vv[kAsmPerThread][2],
-        dv[kAsmPerThread][2];
-    int32_t gv[kAsmPerThread][2], a1[kAsmPerThread], b1[kAsmPerThread], jj[kAsmPerThread],
-        rr[kAsmPerThread];
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const QuadItem item = items[it];
+    const ChanInfo &ch = chans[item.ch];
+    const int hk = ch.hk, q1 = item.q1;
+    const int64_t t_off = ch.t_off;
+    const QuadRow *__restrict__ rtab = qrows + ch.qrow_off;
+    const QuadCol *__restrict__ ctab = qcols + ch.qcol_off;
+    // q / hk as a multiply-high by ceil(2^32 / hk) (Granlund-Montgomery): exact for
+    // q < 2^32 / hk (q < 2^21, hk < 2^11 here); hk = 1 has no 32-bit multiplier.
+    const uint32_t magic = hk > 1 ? 0xFFFFFFFFu / (uint32_t)hk + 1u : 0u;
+    double tv[kQuadPerThread], vv[kQuadPerThread], dv[kQuadPerThread], rv[kQuadPerThread][4];
+    double den[kQuadPerThread], xs[kQuadPerThread][2], ys[kQuadPerThread][2];
+    int32_t gv[kQuadPerThread][4], pos[kQuadPerThread][4], qx[kQuadPerThread],
+        qy[kQuadPerThread], cij[kQuadPerThread], cji[kQuadPerThread];
 #pragma unroll
-    for (int u = 0; u < kAsmPerThread; ++u) {
-      const int q = q0 + u * kAsmThreads;
-      if (q >= n) continue;
-      const int r = hh > 1 ? (int)__umulhi((uint32_t)q, hh_magic) : q, j = q - r * hh;
-      const int o_ab = rows[r].o_ab, o_ba = rows[r].o_ba, js = cols[j].js;
-      rr[u] = r; jj[u] = j;
-      a1[u] = o_ab + j; b1[u] = o_ba + j;
-      const int as = o_ab + js, bs = o_ba + js;
-      tv[u][0] = tb[a1[u]]; tv[u][1] = tb[as]; tv[u][2] = tb[b1[u]]; tv[u][3] = tb[bs];
-      rv[u][0] = rb[a1[u]]; rv[u][1] = rb[as]; rv[u][2] = rb[b1[u]]; rv[u][3] = rb[bs];
-      vv[u][0] = vb[a1[u]]; dv[u][0] = db[a1[u]]; vv[u][1] = vb[b1[u]]; dv[u][1] = db[b1[u]];
-      gv[u][0] = gb[a1[u]]; gv[u][1] = gb[b1[u]];
+    for (int k = 0; k < kQuadPerThread; ++k) {
+      const int q = item.q0 + threadIdx.x + k * kAsmThreads;
+      if (q >= q1) continue;
+      const int u = hk > 1 ? (int)__umulhi((uint32_t)q, magic) : q, w = q - u * hk;
+      const QuadRow rw = rtab[u];
+      const QuadCol cl = ctab[w];
+      pos[k][0] = rw.o_ab + cl.c_ij;
+      pos[k][1] = rw.o_ab + cl.c_ji;
+      pos[k][2] = rw.o_ba + cl.c_ij;
+      pos[k][3] = rw.o_ba + cl.c_ji;
+      qx[k] = rw.qx;
+      qy[k] = rw.qy;
+      cij[k] = cl.c_ij;
+      cji[k] = cl.c_ji;
+      den[k] = cl.eij - rw.ea - rw.eb;
+      const int64_t p0 = t_off + pos[k][0];
+      tv[k] = t_old[p0];
+      vv[k] = __ldg(v_pphh + p0);
+      dv[k] = __ldcg(dmat + p0);
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        rv[k][m] = __ldcg(d_ring + t_off + pos[k][m]);
+        gv[k][m] = __ldg(g_ai_jb + t_off + pos[k][m]);
+      }
+      xs[k][0] = __ldcg(xh + cl.i);
+      xs[k][1] = __ldcg(xh + cl.j);
+      ys[k][0] = __ldcg(yp + rw.pa);
+      ys[k][1] = __ldcg(yp + rw.pb);
     }
 #pragma unroll
-    for (int u = 0; u < kAsmPerThread; ++u) {
-      if (q0 + u * kAsmThreads >= n) continue;
-      const AsmRowInfo ri = rows[rr[u]];
-      const AsmColInfo ci = cols[jj[u]];
-      const int j = jj[u];
-      const double t1 = asm_value(vv[u][0], dv[u][0], rv[u][0], rv[u][1], rv[u][2], rv[u][3],
-                                  tv[u][0], tv[u][1], tv[u][2], ci.xi, ci.xj, ri.ya, ri.yb,
-                                  ci.eij - ri.ea - ri.eb, mixing);
-      nb[a1[u]] = t1;
-      old_phhp[gv[u][0]] = t1;
-      if (nt) write_t_tiles_tc(ch, ri.qa, j, t1, nt, tkt_tc, tkt_tc_stride, tmt_tc,
-                               tmt_tc_stride);
-      else write_t_tiles_q(ch, ri.qa, j, t1, t_kt, t_mt);
-      corr += vv[u][0] * t1;
-      if (ri.o_ba != ri.o_ab) {
-        // Row ba: the same formula with a and b exchanged.
-        const double t2 = asm_value(vv[u][1], dv[u][1], rv[u][2], rv[u][3], rv[u][0], rv[u][1],
-                                    tv[u][2], tv[u][3], tv[u][0], ci.xi, ci.xj, ri.yb, ri.ya,
-                                    ci.eij - ri.eb - ri.ea, mixing);
-        nb[b1[u]] = t2;
-        old_phhp[gv[u][1]] = t2;
-        if (nt) write_t_tiles_tc(ch, ri.qb, j, t2, nt, tkt_tc, tkt_tc_stride, tmt_tc,
-                                 tmt_tc_stride);
-        else write_t_tiles_q(ch, ri.qb, j, t2, t_kt, t_mt);
-        corr += vv[u][1] * t2;
+    for (int k = 0; k < kQuadPerThread; ++k) {
+      const int q = item.q0 + threadIdx.x + k * kAsmThreads;
+      if (q >= q1) continue;
+      const double t1 = quad_value(vv[k], dv[k], rv[k][0], rv[k][1], rv[k][2], rv[k][3], tv[k],
+                                   xs[k][0], xs[k][1], ys[k][0], ys[k][1], den[k], mixing);
+      const double sg[4] = {t1, -t1, -t1, t1};
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        t_new[t_off + pos[k][m]] = sg[m];
+        old_phhp[gv[k][m]] = sg[m];
       }
+      const int2 qa = make_int2(qx[k], qy[k]);
+      if (nt) {
+        write_t_tiles_tc(ch, qa, cij[k], t1, nt, tkt_tc, tkt_tc_stride, tmt_tc, tmt_tc_stride);
+        write_t_tiles_tc(ch, qa, cji[k], -t1, nt, tkt_tc, tkt_tc_stride, tmt_tc, tmt_tc_stride);
+      } else {
+        write_t_tiles_q(ch, qa, cij[k], t1, t_kt, t_mt);
+        write_t_tiles_q(ch, qa, cji[k], -t1, t_kt, t_mt);
+      }
+      corr += 4.0 * (vv[k] * t1);
     }
   }
   const double sum = block_sum<kAsmThreads>(corr, scratch);

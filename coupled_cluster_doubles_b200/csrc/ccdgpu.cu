@@ -52,7 +52,7 @@ struct ccdgpu_handle {
   int n_hh_red = 0;    // hh-ladder reduction items
   int n_act = 0, n_mod = 0, n_mod_small = 0, n_mod_mid = 0, n_tiles = 0, n_hh_tiles = 0;
   int n_ranges = 0;
-  int n_asm_blocks = 0;  // fused assembly CTAs (packed-element ranges)
+  int n_asm_blocks = 0;  // fused assembly CTAs (persistent, striding over quad_items)
   int n_cls[3] = {0, 0, 0};  // pp-ladder tiles per column class (thin, mid, wide), in that order
   size_t ladder_smem_thin = 0;
   size_t ladder_smem = 0, ring_smem = 0, ring_smem_mid = 0, hh_smem = 0;
@@ -70,9 +70,10 @@ struct ccdgpu_handle {
   int2 *pk_idx = nullptr;
   double *part = nullptr, *lpart = nullptr;
   ElemRange *ranges = nullptr;
-  ElemRange *pranges = nullptr;  // fused assembly: ranges of packed elements u * hh + j
-  AsmRowStatic *asm_rows = nullptr;  // fused assembly: per packed row / per hh column tables
-  AsmColStatic *asm_cols = nullptr;
+  QuadItem *quad_items = nullptr;  // fused assembly: work items of quads (u, w)
+  QuadRow *quad_rows = nullptr;    // fused assembly: per strict packed row / hole pair tables
+  QuadCol *quad_cols = nullptr;
+  int n_quad_items = 0;
   int2 *pp_pairs = nullptr, *hh_pairs = nullptr;
   int32_t *pp_swap = nullptr, *hh_swap = nullptr;
   int64_t *list_off = nullptr;
@@ -937,38 +938,47 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     for (int64_t e = 0; e < n; e += per) ranges.push_back({ai, 0, a.t_off + e, a.t_off + std::min(n, e + per)});
   }
   h->n_ranges = (int)ranges.size();
-  // Fused assembly: row-aligned ranges of packed elements, about kAsmPerCTA per CTA.
-  std::vector<ElemRange> pranges;
+  // Fused assembly: quads (strict packed row a < b, strict hole pair i < j) per channel, their
+  // static tables, and work items of up to kQuadPerItem quads of one channel.
+  std::vector<QuadRow> quad_rows;
+  std::vector<QuadCol> quad_cols;
+  std::vector<QuadItem> quad_items;
   for (int ai = 0; ai < h->n_act; ai++) {
-    const int hh = chans[ai].hh, pr = chans[ai].pr;
-    const int rows = std::max(1, std::min(kAsmMaxRows, kAsmPerCTA / hh));
-    for (int u = 0; u < pr; u += rows)
-      pranges.push_back({ai, 0, (int64_t)u * hh, (int64_t)std::min(pr, u + rows) * hh});
-  }
-  h->n_asm_blocks = (int)pranges.size();
-  // Static assembly tables (packed rows in rowmap order, columns in hh order).
-  std::vector<AsmRowStatic> asm_rows(rowmap.size());
-  std::vector<AsmColStatic> asm_cols(hh_pairs.size());
-  for (int ai = 0; ai < h->n_act; ai++) {
-    const ChanInfo &a = chans[ai];
+    ChanInfo &a = chans[ai];
+    a.qrow_off = (int64_t)quad_rows.size();
+    a.qcol_off = (int64_t)quad_cols.size();
     for (int u = 0; u < a.pr; u++) {
-      const int ab = rowmap[a.row_off + u], mi = mirror[a.row_off + u];
-      const int ba = mi >= 0 ? mi : ab;
+      const int ab = rowmap[a.row_off + u], ba = mirror[a.row_off + u];
+      if (ba < 0) continue;  // a = b: zero row
       const int2 pab = pp_pairs[a.pp_off + ab];
-      const int2 qa = pk_idx[a.pp_off + ab], qb = pk_idx[a.pp_off + ba];
-      AsmRowStatic &r = asm_rows[a.row_off + u];
+      const int2 qa = pk_idx[a.pp_off + ab];
+      QuadRow r{};
       r.o_ab = ab * a.hh; r.o_ba = ba * a.hh;
-      r.qa_x = qa.x; r.qa_y = qa.y; r.qb_x = qb.x; r.qb_y = qb.y;
+      r.qx = qa.x; r.qy = qa.y;
       r.pa = pab.x - (int)np; r.pb = pab.y - (int)np;
       r.ea = P->sp_energy[pab.x]; r.eb = P->sp_energy[pab.y];
+      quad_rows.push_back(r);
     }
     for (int j = 0; j < a.hh; j++) {
       const int2 pij = hh_pairs[a.hh_off + j];
-      AsmColStatic &c = asm_cols[a.hh_off + j];
-      c.js = hh_swap[a.hh_off + j]; c.i = pij.x; c.j = pij.y; c.pad = 0;
+      if (pij.x >= pij.y) continue;  // i = j: zero column; i > j: the mirror of (j, i)
+      QuadCol c{};
+      c.c_ij = j; c.c_ji = hh_swap[a.hh_off + j]; c.i = pij.x; c.j = pij.y;
       c.eij = P->sp_energy[pij.x] + P->sp_energy[pij.y];
+      quad_cols.push_back(c);
     }
+    const int64_t rows_q = (int64_t)quad_rows.size() - a.qrow_off;
+    a.hk = (int)((int64_t)quad_cols.size() - a.qcol_off);
+    const int64_t nq = rows_q * a.hk;
+    if (nq >= ((int64_t)1 << 31) / 2) return CCDGPU_ERR_UNSUPPORTED;
+    for (int64_t q = 0; q < nq; q += kQuadPerItem)
+      quad_items.push_back({ai, (int32_t)q, (int32_t)std::min<int64_t>(nq, q + kQuadPerItem), 0});
   }
+  h->host_chans = chans;
+  h->n_quad_items = (int)quad_items.size();
+  // Persistent assembly grid: kAsmCTAsPerSM resident CTAs per SM at most (one CTA if there is no quad,
+  // for the energy and the stop rule).
+  h->n_asm_blocks = h->n_act ? std::max(1, std::min(h->n_quad_items, kAsmCTAsPerSM * 148)) : 0;
 
   // Work estimate (reference GEMM flops) for roofline reporting.
   double fl = 0, lf = 0, vb = 0, vbp = 0;
@@ -1014,8 +1024,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   ar.add(&h->old_phhp, h->n_m); ar.add(&h->r_phhp, h->n_m);
   ar.add(&h->x, x_tot); ar.add(&h->x_t, xt); ar.add(&h->t_kt, tkt); ar.add(&h->t_mt, tmt);
   ar.add(&h->s, hh_tot); ar.add(&h->r, pp_tot); ar.add(&h->xh, np); ar.add(&h->yp, h->npart);
-  ar.add(&h->pranges, pranges.size());
-  ar.add(&h->asm_rows, asm_rows.size()); ar.add(&h->asm_cols, asm_cols.size());
+  ar.add(&h->quad_items, quad_items.size());
+  ar.add(&h->quad_rows, quad_rows.size()); ar.add(&h->quad_cols, quad_cols.size());
   ar.add(&h->kcol, kcol.size());  // V tiling at create
   ar.add(&h->epart, std::max(h->n_ranges, h->n_asm_blocks)); ar.add(&h->ctl, 1); ar.add(&h->e_out, 1); ar.add(&h->err, 1);
   ar.add(&h->ticket, 1);
@@ -1143,8 +1153,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     return v.empty() ? CCDGPU_OK : copy_to_device(h, dst, v.data(), v.size() * sizeof(v[0]));
   };
   TRY(put(h->chans, chans)); TRY(put(h->mods, mods));
-  TRY(put(h->hh_tiles, hh_tiles)); TRY(put(h->hh_red, hh_red)); TRY(put(h->ranges, ranges)); TRY(put(h->pranges, pranges));
-  TRY(put(h->asm_rows, asm_rows)); TRY(put(h->asm_cols, asm_cols));
+  TRY(put(h->hh_tiles, hh_tiles)); TRY(put(h->hh_red, hh_red)); TRY(put(h->ranges, ranges)); TRY(put(h->quad_items, quad_items));
+  TRY(put(h->quad_rows, quad_rows)); TRY(put(h->quad_cols, quad_cols));
 
   TRY(put(h->kcol, kcol));
   TRY(put(h->pp_pairs, pp_pairs)); TRY(put(h->hh_pairs, hh_pairs));
@@ -1504,9 +1514,9 @@ int launch_assemble_fused(ccdgpu_handle *h, cudaStream_t st, int gate) {
   h->launches++;
   return cuda_status(launch_pdl(
       h->loop_capture ? assemble_fused_kernel<true> : assemble_fused_kernel<false>,
-      h->n_asm_blocks, kAsmThreads, 0, st, (const ElemRange *)h->pranges,
-      (const ChanInfo *)h->chans, (const AsmRowStatic *)h->asm_rows,
-      (const AsmColStatic *)h->asm_cols, (const double *)h->v_pphh, (const double *)h->dmat,
+      h->n_asm_blocks, kAsmThreads, 0, st, (const QuadItem *)h->quad_items, h->n_quad_items,
+      (const ChanInfo *)h->chans, (const QuadRow *)h->quad_rows,
+      (const QuadCol *)h->quad_cols, (const double *)h->v_pphh, (const double *)h->dmat,
       (const double *)h->d_ring, (const int32_t *)(h->flat + 4 * h->n_t), h->old_phhp,
       (const double *)h->xh, (const double *)h->yp, h->t[0], h->t[1], h->t_kt, h->t_mt, h->epart,
       h->ticket, h->ctl, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc, gate ? h->nt : 0,
