@@ -41,10 +41,40 @@ __host__ __device__ constexpr int tc_stages(int nt) { return nt == 2 ? 4 : 3; }
 __host__ __device__ constexpr size_t tc_stage_bytes(int nt) {
   return (size_t)nt * (kTcAPlane + kTcBPlane) * 2;
 }
+// V_pppp generated inside the ladder (electron gas): generator warps, and the size of the
+// direct-term table by squared momentum transfer q^2 (|n| <= 6 per axis: q^2 <= 432).
+constexpr int kTcGenWarps = 4;
+constexpr int kTcGenTab = 512;
+__host__ __device__ constexpr int tc_threads(bool gen) {
+  return kTcThreads + (gen ? 32 * kTcGenWarps : 0);
+}
 // Dynamic shared memory: 1024 bytes of alignment slack, the stages, then the barriers
-// (2 S + 5 of them).
-__host__ __device__ constexpr size_t tc_smem_bytes(int nt) {
-  return 1024 + tc_stages(nt) * tc_stage_bytes(nt) + 256;
+// (2 S + 5 of them), then (gen) the q^2 table.
+__host__ __device__ constexpr size_t tc_smem_bytes(int nt, bool gen = false) {
+  return 1024 + tc_stages(nt) * tc_stage_bytes(nt) + 256 + (gen ? kTcGenTab * 4 : 0);
+}
+
+// ---- V_pppp of the electron gas generated in the ladder ----------------------------------
+// <ab|v|cd> = [s_a = s_c, s_b = s_d] w(|n_a - n_c|^2) - [s_a = s_d, s_b = s_c] w(|n_a - n_d|^2)
+// (ElectronGasSPBasis.cpp:418-471: direct minus exchange, spin-diagonal Coulomb term that
+// depends only on the momentum transfer, zero at q = 0), with n_a - n_d = n_c - n_b inside a
+// channel (n_a + n_b = n_c + n_d).  Momenta are stored as three bytes biased by 64, so one
+// vabsdiffu4 gives |dx|, |dy|, |dz| and one dp4a gives q^2; the spin keys are 2 s_a + s_b
+// (rows) and 2 s_c + s_d, 2 s_d + s_c (columns).  w is a float table by q^2, so an element is
+// exact to FP32 before its bf16 split (the split keeps about 16 bits).
+struct VGenRow {
+  uint32_t na, nb, key, pad;
+};
+struct VGenCol {
+  uint32_t nc, keys;  // keys: key | swapped key << 8
+};
+__device__ __forceinline__ float vgen_elem(const VGenRow &r, uint32_t nc, uint32_t keys,
+                                           const float *tab) {
+  const uint32_t d1 = __vabsdiffu4(r.na, nc), d2 = __vabsdiffu4(r.nb, nc);
+  const uint32_t q1 = __dp4a(d1, d1, 0u), q2 = __dp4a(d2, d2, 0u);
+  const float dir = r.key == (keys & 0xFFu) ? tab[q1] : 0.f;
+  const float exc = r.key == (keys >> 8) ? tab[q2] : 0.f;
+  return dir - exc;
 }
 
 // --- tcgen05 / descriptor helpers --------------------------------------------------------
@@ -129,15 +159,21 @@ __device__ __forceinline__ void tc_drain(const uint64_t *full, int issued, int s
 // (gate 1 of skip_iteration).
 constexpr uint32_t kTcAccCols = 128;  // columns of one accumulator buffer (nb <= kTcMaxNB)
 constexpr int kTcGrid = 2 * 148;      // persistent grid: two CTAs on each of the 148 SMs
-template <int NT>
-__global__ void __launch_bounds__(kTcThreads, 1)
+// GEN (electron gas, V generated in the ladder): warps 6 .. 6 + kTcGenWarps - 1 write the V
+// operand planes of every V T chunk into the stage (fence.proxy.async, then one arrival per
+// warp on the stage's full barrier, for every chunk); the producer copies only the B planes of
+// those chunks.  No V image is read from HBM.
+template <int NT, bool GEN>
+__global__ void __launch_bounds__(tc_threads(GEN), GEN ? 2 : 1)
 pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restrict__ cta_off,
                     const __nv_bfloat16 *__restrict__ v_tc, int64_t v_stride,
                     const __nv_bfloat16 *__restrict__ tkt_tc, int64_t tkt_stride,
                     const __nv_bfloat16 *__restrict__ tmt_tc, int64_t tmt_stride,
                     const __nv_bfloat16 *__restrict__ xt_tc, int64_t xt_stride,
                     const int32_t *__restrict__ rowmap, const int32_t *__restrict__ mirror,
-                    double *__restrict__ d, double *part, const Control *ctl, int32_t *err) {
+                    double *__restrict__ d, double *part, const Control *ctl, int32_t *err,
+                    const ChanInfo *__restrict__ chans, const VGenRow *__restrict__ vg_rows,
+                    const VGenCol *__restrict__ vg_cols, const float *__restrict__ vg_tab) {
   if (skip_iteration(ctl, 1, kTrLadderTC)) return;
   constexpr int S = tc_stages(NT);
   constexpr uint32_t kStageBytes = (uint32_t)tc_stage_bytes(NT);
@@ -149,10 +185,15 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
   uint64_t *bars = reinterpret_cast<uint64_t *>(tc_smem_raw + (base - raw) + S * kStageBytes);
   uint64_t *full = bars, *empty = bars + S, *acc_full = bars + 2 * S,
            *acc_empty = bars + 2 * S + 2, *done = bars + 2 * S + 4;
+  float *gtab = reinterpret_cast<float *>(tc_smem_raw + (base - raw) + S * kStageBytes + 256);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if constexpr (GEN) {
+    if (warp >= 6)
+      for (int i = threadIdx.x - 192; i < kTcGenTab; i += 32 * kTcGenWarps) gtab[i] = vg_tab[i];
+  }
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
-      mbar_init(smem_u32(&full[s]), 1);
+      mbar_init(smem_u32(&full[s]), GEN ? 1 + kTcGenWarps : 1);
       mbar_init(smem_u32(&empty[s]), 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -217,10 +258,11 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
           }
           const uint32_t fb = smem_u32(&full[s]);
           const uint32_t sa = base + s * kStageBytes, sb = sa + NT * kTcAPlane * 2;
-          mbar_expect_tx(fb, NT * (abytes + bbytes));
+          const bool copy_a = !GEN || c >= tile.nks;  // GEN: the generator warps write V
+          mbar_expect_tx(fb, NT * ((copy_a ? abytes : 0u) + bbytes));
 #pragma unroll
           for (int p = 0; p < NT; ++p) {
-            bulk_g2s(sa + p * kTcAPlane * 2, asrc + p * as, abytes, fb);
+            if (copy_a) bulk_g2s(sa + p * kTcAPlane * 2, asrc + p * as, abytes, fb);
             bulk_g2s(sb + p * kTcBPlane * 2, bsrc + p * bs, bbytes, fb);
           }
         }
@@ -269,6 +311,71 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
         if (!ok) break;
       }
       tc_commit(smem_u32(done));
+    }
+  } else if (GEN && warp >= 6) {
+    // ---- V generators: warp gw owns row groups gw, gw + G, ... of each tile; a lane writes
+    // row 8 rg + lane / 4, K columns 8 kg + 2 (lane % 4) + {0, 1} of every core matrix (one
+    // 32-bit word per plane: conflict-free) ----
+    const int gw = warp - 6;
+    constexpr int RG = (kTcBM / 8) / kTcGenWarps;  // row groups per generator warp
+    int gc = 0;
+    bool stop = false;
+    for (int ti = t_begin; ti < t_end && !stop; ++ti) {
+      const LadderTile tile = tiles[ti];
+      const int nchunks = tile.nks + tile.nkh;
+      const int64_t pk_off = chans[tile.ch].pk_off;
+      const int pk = chans[tile.ch].pk;
+      VGenRow rw[RG];
+#pragma unroll
+      for (int i = 0; i < RG; ++i) {
+        const int r = 8 * (gw + i * kTcGenWarps) + (lane >> 2);
+        rw[i] = r < tile.rows ? vg_rows[tile.row_off + (int64_t)tile.mt * kTcBM + r]
+                              : VGenRow{0u, 0u, 0xFFu, 0u};
+      }
+      for (int c = 0; c < nchunks; ++c, ++gc) {
+        const int s = gc % S;
+        if (read_flag(&abort_flag) ||
+            (gc >= S && !mbar_wait(smem_u32(&empty[s]), ((gc / S) - 1) & 1))) {
+          fail();
+          stop = true;
+          break;
+        }
+        if (c < tile.nks) {
+          const int kc = tile.kc0 + c;
+          uint32_t cn[8], ck[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {  // columns 8 (j / 2) + 2 (lane % 4) + j % 2
+            const int w = kc * kTcKC + 8 * (j >> 1) + 2 * (lane & 3) + (j & 1);
+            const VGenCol cl = w < pk ? vg_cols[pk_off + w] : VGenCol{0u, 0xFEFEu};
+            cn[j] = cl.nc;
+            ck[j] = cl.keys;
+          }
+          const uint32_t sa = base + s * kStageBytes;
+#pragma unroll
+          for (int i = 0; i < RG; ++i) {
+            const int rg = gw + i * kTcGenWarps;
+            if (8 * rg >= tile.rows) continue;
+#pragma unroll
+            for (int kg = 0; kg < 4; ++kg) {
+              float v[2];
+#pragma unroll
+              for (int e = 0; e < 2; ++e) v[e] = vgen_elem(rw[i], cn[2 * kg + e], ck[2 * kg + e], gtab);
+              const uint32_t off = (uint32_t)(rg * kTcGroup + kg * 64 + (lane >> 2) * 8 + 2 * (lane & 3)) * 2;
+#pragma unroll
+              for (int p = 0; p < NT; ++p) {
+                const __nv_bfloat162 t = __floats2bfloat162_rn(v[0], v[1]);
+                asm volatile("st.shared.b32 [%0], %1;" ::"r"(sa + p * kTcAPlane * 2 + off),
+                             "r"(*reinterpret_cast<const uint32_t *>(&t)) : "memory");
+                v[0] -= __low2float(t);
+                v[1] -= __high2float(t);
+              }
+            }
+          }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&full[s]));
+      }
     }
   } else {
     // ---- epilogue: accumulator rows -> D (or split-K partials) ----

@@ -133,6 +133,12 @@ struct ccdgpu_handle {
   int32_t *kcol = nullptr;  // pp index of the w-th c<d pair of each channel (pk_off + w)
   double *tc_part = nullptr;
   __nv_bfloat16 *v_tc = nullptr, *tkt_tc = nullptr, *tmt_tc = nullptr, *xt_tc = nullptr;
+  // Electron gas with V generated on the device: the tensor-core ladder generates its V
+  // planes itself (no v_tc images) from these per-row / per-K-column codes and the q^2 table.
+  bool tc_gen = false;
+  VGenRow *vg_rows = nullptr;
+  VGenCol *vg_cols = nullptr;
+  float *vg_tab = nullptr;
   int64_t n_vtc = 0, n_tkttc = 0, n_tmttc = 0, n_xttc = 0;  // plane strides (elements)
   size_t tc_smem = 0;
   double ladder_bytes_tc = 0;
@@ -701,6 +707,16 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
   return CCDGPU_OK;
 }
 
+using TcKernel = void (*)(const LadderTile *, const int32_t *, const __nv_bfloat16 *, int64_t,
+                         const __nv_bfloat16 *, int64_t, const __nv_bfloat16 *, int64_t,
+                         const __nv_bfloat16 *, int64_t, const int32_t *, const int32_t *,
+                         double *, double *, const Control *, int32_t *, const ChanInfo *,
+                         const VGenRow *, const VGenCol *, const float *);
+TcKernel tc_kernel_of(int nt, bool gen) {
+  if (nt == 2) return gen ? pp_ladder_tc_kernel<2, true> : pp_ladder_tc_kernel<2, false>;
+  return gen ? pp_ladder_tc_kernel<3, true> : pp_ladder_tc_kernel<3, false>;
+}
+
 int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   const uint64_t nch = P->n_channels, nsp = P->n_sp, np = P->n_particles;
   h->nch = nch; h->nsp = nsp; h->np = np; h->npart = nsp - np;
@@ -1004,6 +1020,54 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   h->n_tkt = tkt;
   h->n_tmt = tmt;
 
+  // Tensor-core ladder with V generated in the kernel (electron gas, on-the-fly V, momenta
+  // |n_i| <= 6 so that q^2 fits the kTcGenTab table): per packed row u (rowmap order) the
+  // momenta of a and b and the spin key, per K index w (kcol order) the momentum of c and the
+  // keys of (c, d) and (d, c); the direct term by q^2.
+  std::vector<VGenRow> vg_rows;
+  std::vector<VGenCol> vg_cols;
+  std::vector<float> vg_tab;
+  if (on_the_fly && h->nt && model_ok && M->kind == CCDGPU_MODEL_ELECTRON_GAS) {
+    int nmax = 0;
+    for (uint64_t o = 0; o < nsp; o++)
+      for (int i = 0; i < 3; i++) nmax = std::max(nmax, std::abs(M->qn[o * M->qn_stride + i]));
+    if (3 * (2 * nmax) * (2 * nmax) < kTcGenTab) {
+      h->tc_gen = true;
+      auto mom = [&](int o) {
+        const int32_t *q = M->qn + (int64_t)o * M->qn_stride;
+        return (uint32_t)(q[0] + 64) | ((uint32_t)(q[1] + 64) << 8) | ((uint32_t)(q[2] + 64) << 16);
+      };
+      auto up = [&](int o) { return M->qn[(int64_t)o * M->qn_stride + 3] > 0 ? 1u : 0u; };
+      vg_rows.resize(rowmap.size());
+      vg_cols.resize(kcol.size());
+      for (const ChanInfo &a : chans) {
+        for (int u = 0; u < a.pr; u++) {
+          const int2 ab = pp_pairs[a.pp_off + rowmap[a.row_off + u]];
+          vg_rows[a.row_off + u] = VGenRow{mom(ab.x), mom(ab.y), 2 * up(ab.x) + up(ab.y), 0u};
+        }
+        for (int w = 0; w < a.pk; w++) {
+          const int2 cd = pp_pairs[a.pp_off + kcol[a.pk_off + w]];
+          vg_cols[a.pk_off + w] =
+              VGenCol{mom(cd.x), (2 * up(cd.x) + up(cd.y)) | ((2 * up(cd.y) + up(cd.x)) << 8)};
+        }
+      }
+      // w(q^2) = e^2 / L^3 * 4 pi / (2 pi / L)^2 q^2, zero for q = 0 (ElectronGasSPBasis.cpp:
+      // 453-466 as a function of q^2).
+      const double L = M->params[0], e_sq = M->params[1];
+      vg_tab.assign(kTcGenTab, 0.f);
+      for (int q2 = 1; q2 < kTcGenTab; q2++) {
+        const double rel = (2 * M_PI / L) * (2 * M_PI / L) * q2;
+        vg_tab[q2] = (float)(e_sq / (L * L * L) * 4 * M_PI / rel);
+      }
+      // The ladder then moves no V bytes: the T and X operand images and D.
+      double lbg = 0;
+      for (const ChanInfo &a : chans)
+        lbg += 2.0 * h->nt * ((double)a.pk * a.hh + (double)a.pr * a.hh + (double)a.hh * a.hh) +
+               8.0 * a.pp * (double)a.hh;
+      h->ladder_bytes_tc = lbg;
+    }
+  }
+
   // ---- one device allocation ----
   Arena ar;
   ar.add(&h->chans, chans.size()); ar.add(&h->mods, mods.size());
@@ -1033,7 +1097,14 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     auto round_up = [](int64_t n) { return std::max<int64_t>(256, (n + 255) / 256 * 256); };
     h->n_vtc = round_up(vtc); h->n_tkttc = round_up(tkttc);
     h->n_tmttc = round_up(tmttc); h->n_xttc = round_up(xttc);
-    ar.add(&h->v_tc, (size_t)h->nt * h->n_vtc); ar.add(&h->tkt_tc, (size_t)h->nt * h->n_tkttc);
+    if (h->tc_gen) {
+      h->n_vtc = 0;  // V planes generated in the ladder
+      ar.add(&h->vg_rows, vg_rows.size()); ar.add(&h->vg_cols, vg_cols.size());
+      ar.add(&h->vg_tab, vg_tab.size());
+    } else {
+      ar.add(&h->v_tc, (size_t)h->nt * h->n_vtc);
+    }
+    ar.add(&h->tkt_tc, (size_t)h->nt * h->n_tkttc);
     ar.add(&h->tmt_tc, (size_t)h->nt * h->n_tmttc); ar.add(&h->xt_tc, (size_t)h->nt * h->n_xttc);
   }
   if (h->have_3body) {
@@ -1157,6 +1228,9 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   TRY(put(h->quad_rows, quad_rows)); TRY(put(h->quad_cols, quad_cols));
 
   TRY(put(h->kcol, kcol));
+  if (h->tc_gen) {
+    TRY(put(h->vg_rows, vg_rows)); TRY(put(h->vg_cols, vg_cols)); TRY(put(h->vg_tab, vg_tab));
+  }
   TRY(put(h->pp_pairs, pp_pairs)); TRY(put(h->hh_pairs, hh_pairs));
   TRY(put(h->pp_swap, pp_swap)); TRY(put(h->hh_swap, hh_swap));
   TRY(put(h->list_off, list_off)); TRY(put(h->list, list));
@@ -1280,9 +1354,11 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   }
   if (!vrows.empty()) {
     if (on_the_fly) {
+      // FP64 tiles, and the bf16 images unless the tensor-core ladder generates its own V.
       gen_v_kernel<<<(unsigned)vrows.size(), 128, 0, h->s0>>>(h->chans, d_vrows, h->rowmap,
                                                               h->kcol, h->pp_pairs, md, h->v_t,
-                                                              h->v_tc, h->n_vtc, h->nt);
+                                                              h->v_tc, h->n_vtc,
+                                                              h->tc_gen ? 0 : h->nt);
     } else {
       tile_v_kernel<<<(unsigned)vrows.size(), 128, 0, h->s0>>>(h->chans, d_vrows, h->rowmap,
                                                                h->kcol, d_vraw_off, vraw, h->v_t);
@@ -1335,13 +1411,9 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   sch.tc_split_mul = 2;
   if (int rc2 = make_ladder_tiles(h, sch)) return rc2;
   if (h->nt) {
-    h->tc_smem = tc_smem_bytes(h->nt);
-    if (h->nt == 2)
-      CK(cudaFuncSetAttribute(pp_ladder_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)h->tc_smem));
-    else
-      CK(cudaFuncSetAttribute(pp_ladder_tc_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)h->tc_smem));
+    h->tc_smem = tc_smem_bytes(h->nt, h->tc_gen);
+    CK(cudaFuncSetAttribute(tc_kernel_of(h->nt, h->tc_gen),
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->tc_smem));
   }
   return CCDGPU_OK;
 }
@@ -1402,16 +1474,14 @@ int launch_pp_ladder_tc(ccdgpu_handle *h, cudaStream_t st) {
   if (!h->n_tc_tiles) return CCDGPU_OK;
   h->launches++;
   // Persistent: two CTAs per SM (shared memory and 2 x 128 tensor-memory columns each).
-  if (h->nt == 2)
-    CK(launch_pdl(pp_ladder_tc_kernel<2>, h->tc_grid, kTcThreads, h->tc_smem, st,
-                  (const LadderTile *)h->tc_tiles, (const int32_t *)h->tc_cta_off, h->v_tc,
-                  h->n_vtc, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc, h->xt_tc, h->n_xttc,
-                  h->rowmap, h->mirror, h->dmat, h->tc_part, h->ctl, h->err));
-  else
-    CK(launch_pdl(pp_ladder_tc_kernel<3>, h->tc_grid, kTcThreads, h->tc_smem, st,
-                  (const LadderTile *)h->tc_tiles, (const int32_t *)h->tc_cta_off, h->v_tc,
-                  h->n_vtc, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc, h->xt_tc, h->n_xttc,
-                  h->rowmap, h->mirror, h->dmat, h->tc_part, h->ctl, h->err));
+  CK(launch_pdl(tc_kernel_of(h->nt, h->tc_gen), h->tc_grid, tc_threads(h->tc_gen), h->tc_smem,
+                st, (const LadderTile *)h->tc_tiles, (const int32_t *)h->tc_cta_off,
+                (const __nv_bfloat16 *)h->v_tc, h->n_vtc, (const __nv_bfloat16 *)h->tkt_tc,
+                h->n_tkttc, (const __nv_bfloat16 *)h->tmt_tc, h->n_tmttc,
+                (const __nv_bfloat16 *)h->xt_tc, h->n_xttc, (const int32_t *)h->rowmap,
+                (const int32_t *)h->mirror, h->dmat, h->tc_part, (const Control *)h->ctl, h->err,
+                (const ChanInfo *)h->chans, (const VGenRow *)h->vg_rows,
+                (const VGenCol *)h->vg_cols, (const float *)h->vg_tab));
   if (h->n_red_tc) {
     CK(launch_pdl(ladder_reduce_kernel, h->n_red_tc, 256, 0, st, (const RedItem *)h->red_tc,
                   (const LadderTile *)h->tc_tiles, (const int32_t *)h->rowmap,
@@ -2428,7 +2498,7 @@ int ccdgpu_ladder_profile(ccdgpu_handle *h, int32_t reps, double *ms, double *fl
     bytes[k] += 8.0 * b + 8.0 * a.pp * a.hh;
     if (h->nt) {
       flops[3] += f;
-      bytes[3] += 2.0 * h->nt * b + 8.0 * a.pp * a.hh;
+      bytes[3] += 2.0 * h->nt * (h->tc_gen ? b - (double)a.pr * a.pk : b) + 8.0 * a.pp * a.hh;
     }
   }
   for (int k = 0; k < 4; k++) {
