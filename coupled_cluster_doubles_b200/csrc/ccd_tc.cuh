@@ -65,6 +65,7 @@ __host__ __device__ constexpr size_t tc_smem_bytes(int nt, bool gen = false) {
 struct VGenRow {
   uint32_t na, nb, key, pad;
 };
+constexpr uint32_t kVGenZero = 0x404040u;  // momentum (0, 0, 0), biased
 struct VGenCol {
   uint32_t nc, keys;  // keys: key | swapped key << 8
 };
@@ -329,8 +330,10 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
 #pragma unroll
       for (int i = 0; i < RG; ++i) {
         const int r = 8 * (gw + i * kTcGenWarps) + (lane >> 2);
+        // Rows past the tile: zero momenta (so q^2 stays inside the table) and a spin key that
+        // matches no column, so the element is 0.
         rw[i] = r < tile.rows ? vg_rows[tile.row_off + (int64_t)tile.mt * kTcBM + r]
-                              : VGenRow{0u, 0u, 0xFFu, 0u};
+                              : VGenRow{kVGenZero, kVGenZero, 0xFFu, 0u};
       }
       for (int c = 0; c < nchunks; ++c, ++gc) {
         const int s = gc % S;
@@ -346,7 +349,7 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
 #pragma unroll
           for (int j = 0; j < 8; ++j) {  // columns 8 (j / 2) + 2 (lane % 4) + j % 2
             const int w = kc * kTcKC + 8 * (j >> 1) + 2 * (lane & 3) + (j & 1);
-            const VGenCol cl = w < pk ? vg_cols[pk_off + w] : VGenCol{0u, 0xFEFEu};
+            const VGenCol cl = w < pk ? vg_cols[pk_off + w] : VGenCol{kVGenZero, 0xFEFEu};
             cn[j] = cl.nc;
             ck[j] = cl.keys;
           }
