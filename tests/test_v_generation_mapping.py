@@ -118,3 +118,68 @@ def test_normal_order_formula_reproduces_reference(name):
         i, jj = np.meshgrid(np.arange(nh), np.arange(nh), indexing="ij")
         e_ref = 0.5 * v(i.ravel(), jj.ravel(), i.ravel(), jj.ravel()).sum() + bare[:nh].sum()
         assert e_ref == pytest.approx(float(g["scalars"][0]), rel=1e-13)
+
+
+def _vgen_codes(qn, orb):
+    """Momentum of orbital(s) as three bytes biased by 64 (the ladder's VGenRow / VGenCol)."""
+    q = qn[orb]
+    return (q[..., 0] + 64) | ((q[..., 1] + 64) << 8) | ((q[..., 2] + 64) << 16)
+
+
+def _absdiff_dp4a(x, y):
+    """q^2 from two biased codes: per-byte |x - y| (vabsdiffu4), then the dot of the bytes with
+    themselves (dp4a)."""
+    out = np.zeros(np.broadcast(x, y).shape, dtype=np.int64)
+    for sh in (0, 8, 16, 24):
+        d = np.abs(((x >> sh) & 0xFF) - ((y >> sh) & 0xFF))
+        out += d * d
+    return out
+
+
+@pytest.mark.parametrize("name", ["eg14_s19", "eg14_r2"])
+def test_ladder_v_generator_codes_reproduce_reference_v(name):
+    """The electron-gas V generator inside the tensor-core ladder (pp_ladder_tc_kernel with
+    GEN): V[ab,cd] = [key_ab = key_cd] w(q1^2) - [key_ab = key_dc] w(q2^2), q1 = n_a - n_c,
+    q2 = n_c - n_b from biased byte codes, w an FP32 table by q^2.  Restated in numpy over every
+    packed row a <= b and K column c < d of every channel, against the reference's V_pppp
+    blocks (FP32 accuracy: the ladder splits the element into bf16 terms afterwards)."""
+    g = golden(name)
+    with system_for(g) as s:
+        qn = s.array("qn").reshape(s.n_sp, -1).astype(np.int64)
+        m = s.problem.contents.model.contents
+        L, e_sq = m.params[0], m.params[1]
+        assert np.abs(qn[:, :3]).max() <= 6
+        q2 = np.arange(512, dtype=np.float64)
+        with np.errstate(divide="ignore"):
+            tab = np.where(q2 > 0, e_sq / L ** 3 * 4 * np.pi / ((2 * np.pi / L) ** 2 * q2), 0.0)
+        tab = tab.astype(np.float32)
+        up = (qn[:, 3] > 0).astype(np.int64)
+        d = s.chan_dims().astype(np.int64)
+        pp = s.array("pp_map").reshape(-1, 2).astype(np.int64)
+        vp = s.array("v_pppp")
+        po = np.concatenate([[0], np.cumsum(d[:, 0])])
+        voff = 0
+        checked = 0
+        for c in np.nonzero((d[:, 0] > 0) & (d[:, 1] > 0))[0]:
+            P = pp[po[c]:po[c + 1]]
+            n = len(P)
+            ref = vp[voff:voff + n * n].reshape(n, n)
+            voff += n * n
+            rows = np.nonzero(P[:, 0] <= P[:, 1])[0]
+            cols = np.nonzero(P[:, 0] < P[:, 1])[0]
+            if not len(rows) or not len(cols):
+                continue
+            a, b = P[rows, 0][:, None], P[rows, 1][:, None]
+            cc, dd = P[cols, 0][None, :], P[cols, 1][None, :]
+            na, nb, nc = _vgen_codes(qn, a), _vgen_codes(qn, b), _vgen_codes(qn, cc)
+            q1, q2v = _absdiff_dp4a(na, nc), _absdiff_dp4a(nb, nc)
+            assert q1.max() < 512 and q2v.max() < 512
+            key = 2 * up[a] + up[b]
+            kcd, kdc = 2 * up[cc] + up[dd], 2 * up[dd] + up[cc]
+            v = (np.where(key == kcd, tab[q1], np.float32(0)) -
+                 np.where(key == kdc, tab[q2v], np.float32(0))).astype(np.float64)
+            want = ref[np.ix_(rows, cols)]
+            scale = max(float(np.abs(want).max()), 1e-300)
+            assert np.max(np.abs(v - want)) <= 2e-7 * scale, c
+            checked += 1
+        assert checked > 10
