@@ -440,6 +440,23 @@ __device__ __forceinline__ void opgemm(const double *__restrict__ A, int lda,
 }
 __host__ __device__ inline int even_up(int n) { return (n + 1) & ~1; }
 
+// cp.async (8- and 4-byte) global -> shared copies, committed and waited for by group.
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // ------------------------------------------------------------------------------------------
 // hh ladder intermediate (calc.cpp:141-160 and the one-body sums of calc.cpp:18-20, 82-84):
 //   P = V_hhpp T (K = pp),  X = V_hhhh + 0.5 P  (reference layout, and X/2 as B tiles),
@@ -552,6 +569,79 @@ hh_mma_kernel(const HHTile *__restrict__ tiles, int n, const ChanInfo *__restric
     }
 }
 
+// Channels with hh > 16: one CTA per K slice of kHHRowsL pp rows.  The slice's rows of V_pphh
+// and T (two contiguous ranges of rows * hh doubles) go to shared memory with cp.async, all in
+// flight at once, at a row stride of hh rounded up to 8, plus 4 (4 mod 8 doubles: conflict-free
+// fragment loads); rows up to the next multiple of 4 are zero.  Warp w computes P rows
+// [8c, 8c + 8) for c = w, w + 8, ... over every column tile (m8n8k4, K = the slice), so T is
+// read from HBM once per slice; the warps then form the slice's row dots r (lanes over the
+// columns, a fixed butterfly).  Partial P per slice as for hh_mma_kernel.
+constexpr int kHHRowsL = 64;
+constexpr int kHHSliceThreads = 256;
+__host__ __device__ inline int hh_slice_ld(int hh) { return ((hh + 7) & ~7) + 4; }
+__host__ __device__ inline size_t hh_slice_smem(int hh) {
+  return (size_t)2 * kHHRowsL * hh_slice_ld(hh) * sizeof(double);
+}
+__global__ void __launch_bounds__(kHHSliceThreads, 2)
+hh_slice_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ chans,
+                const double *__restrict__ v_pphh, const double *tbuf0, const double *tbuf1,
+                double *__restrict__ part, double *__restrict__ r_out, const Control *ctl,
+                int gate) {
+  if (skip_iteration(ctl, gate, kTrHHTiled)) return;
+  extern __shared__ __align__(16) double hs_smem[];
+  const HHTile tt = tiles[blockIdx.x];
+  const ChanInfo &ch = chans[tt.ch];
+  const double *t_old = ctl->parity ? tbuf1 : tbuf0;
+  const int hh = ch.hh, ld = hh_slice_ld(hh), rows = tt.rows, rows4 = (rows + 3) & ~3;
+  const int h8 = (hh + 7) >> 3;
+  double *Vs = hs_smem, *Ts = hs_smem + kHHRowsL * ld;
+  const int64_t base = ch.t_off + (int64_t)tt.k0 * hh;
+  const double *vb = v_pphh + base, *tb = t_old + base;
+  for (int e = threadIdx.x; e < rows * hh; e += kHHSliceThreads) {
+    const int k = e / hh, c = e - k * hh;
+    cp_async8(Vs + k * ld + c, vb + e);
+    cp_async8(Ts + k * ld + c, tb + e);
+  }
+  cp_async_commit();
+  for (int e = threadIdx.x; e < (rows4 - rows) * ld; e += kHHSliceThreads) {
+    Vs[rows * ld + e] = 0.0;
+    Ts[rows * ld + e] = 0.0;
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  double *pb = part + ch.part_off + (int64_t)tt.idx * hh * hh;
+  for (int mc = warp; mc < h8; mc += kHHSliceThreads / 32) {
+    double acc[kMaxCG][2];
+#pragma unroll
+    for (int c = 0; c < kMaxCG; ++c) acc[c][0] = acc[c][1] = 0.0;
+    const double *ap = Vs + t * ld + 8 * mc + g, *bp = Ts + t * ld + g;
+#pragma unroll 4
+    for (int k4 = 0; k4 < rows4 / 4; ++k4) {
+      const double a = ap[4 * k4 * ld];
+#pragma unroll
+      for (int c = 0; c < kMaxCG; ++c)
+        if (c < h8) dmma_884(acc[c], a, bp[4 * k4 * ld + 8 * c]);
+    }
+    const int kl = 8 * mc + g;
+#pragma unroll
+    for (int c = 0; c < kMaxCG; ++c) {
+      const int ij = 8 * c + 2 * t;
+      if (c < h8 && kl < hh) {
+        if (ij < hh) pb[kl * hh + ij] = acc[c][0];
+        if (ij + 1 < hh) pb[kl * hh + ij + 1] = acc[c][1];
+      }
+    }
+  }
+  for (int k = warp; k < rows; k += kHHSliceThreads / 32) {
+    double d = 0.0;
+    for (int c = lane; c < hh; c += 32) d = fma(Vs[k * ld + c], Ts[k * ld + c], d);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+    if (lane == 0) r_out[ch.pp_off + tt.k0 + k] = d;
+  }
+}
+
 // Item = 256 consecutive elements P[kl][ij] (row-major) of channel ch, from idx0.
 struct HHRed {
   int32_t ch, idx0;
@@ -568,8 +658,18 @@ hh_reduce_kernel(const HHRed *__restrict__ items, const ChanInfo *__restrict__ c
   const int hh = ch.hh, nout = hh * hh, idx = it.idx0 + threadIdx.x;
   if (idx >= nout) return;
   const double *pb = part + ch.part_off + idx;
-  double p = 0.0;
-  for (int sl = 0; sl < ch.nhht; ++sl) p += pb[(int64_t)sl * nout];
+  // Four interleaved partial sums over the slices (their loads independent, so they are in
+  // flight together), combined in a fixed order.
+  double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
+  int sl = 0;
+  for (; sl + 4 <= ch.nhht; sl += 4) {
+    p0 += __ldcg(pb + (int64_t)sl * nout);
+    p1 += __ldcg(pb + (int64_t)(sl + 1) * nout);
+    p2 += __ldcg(pb + (int64_t)(sl + 2) * nout);
+    p3 += __ldcg(pb + (int64_t)(sl + 3) * nout);
+  }
+  for (; sl < ch.nhht; ++sl) p0 += __ldcg(pb + (int64_t)sl * nout);
+  const double p = (p0 + p1) + (p2 + p3);
   hh_finish(ch, idx / hh, idx - (idx / hh) * hh, p, v_hhhh, x_ref, x_t, s_out, xt_tc,
             xt_tc_stride, nt);
 }
@@ -590,22 +690,6 @@ constexpr int kRingThreads = 256;
 __host__ __device__ constexpr int kRingThreadsOf(int nc) { return nc <= 2 ? 256 : 512; }
 constexpr int kRingSmall = 16;
 constexpr int kRingMid = 32;
-
-__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 // C (M8*8 x N8*8) = A B, K4*4 deep, on 8 x 8 tiles: warps warp, warp + nwarps, ... take items of
 // one 8-row tile by NC column tiles (the A fragment is reused NC times).  A[m][k] =
@@ -671,17 +755,25 @@ ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restr
   const int ph = m.ph, hp = m.hp, P = ring_pad8(ph), H = ring_pad8(hp), ld = kRingSmallLd;
   const int hs = H == 8 ? 3 : 4;  // log2 H
   double *Ts = buf[w], *Vt = Ts + kRingSmall * ld, *Ys = Vt + kRingSmall * ld;
+  // Operands by cp.async (every load of the warp in flight at once), pad cells zeroed.
   for (int e = lane; e < P * H; e += 32) {
     const int r = e >> hs, c = e & (H - 1);
-    const bool in = r < ph && c < hp;
-    const int64_t src = m.m_off + r * hp + c;
-    Ts[r * ld + c] = in ? t_phhp[src] : 0.0;
-    Vt[r * ld + c] = in ? v_hpph[src] : 0.0;
+    if (r < ph && c < hp) {
+      const int64_t src = m.m_off + r * hp + c;
+      cp_async8(Ts + r * ld + c, t_phhp + src);
+      cp_async8(Vt + r * ld + c, v_hpph + src);
+    } else {
+      Ts[r * ld + c] = 0.0;
+      Vt[r * ld + c] = 0.0;
+    }
   }
   for (int e = lane; e < H * H; e += 32) {
     const int r = e >> hs, c = e & (H - 1);
-    Ys[r * ld + c] = (r < hp && c < hp) ? v_hphp[m.y_off + r * hp + c] : 0.0;
+    if (r < hp && c < hp) cp_async8(Ys + r * ld + c, v_hphp + m.y_off + r * hp + c);
+    else Ys[r * ld + c] = 0.0;
   }
+  cp_async_commit();
+  cp_async_wait<0>();
   __syncwarp();
   // A[i][k] = V_hpph[i][k] = Vt[k][i]; each Y element is read and written by its owner lane.
   warp_mma_gemm<2>(Vt, 1, ld, Ts, ld, H / 8, H / 8, P / 4, 0, 1,

@@ -49,6 +49,7 @@ struct ccdgpu_handle {
   uint64_t nch = 0, nsp = 0, np = 0, npart = 0;
   int64_t n_t = 0, n_m = 0, n_h = 0, n_p = 0;
   int n_hh_small = 0;  // hh-ladder units of channels with hh <= 16 (first in hh_tiles)
+  size_t hh_slice_smem = 0;  // dynamic shared memory of hh_slice_kernel (largest hh > 16)
   int n_hh_red = 0;    // hh-ladder reduction items
   int n_act = 0, n_mod = 0, n_mod_small = 0, n_mod_mid = 0, n_tiles = 0, n_hh_tiles = 0;
   int n_ranges = 0;
@@ -813,7 +814,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     ci.nkc = (int)ceil_div(pk, kBK);
     ci.nkh = (int)ceil_div(hh, kBK);
     ci.nmt = (int)ceil_div(pr, ci.bm);
-    ci.nhht = (int)ceil_div(pp, kHHRows);
+    const int hh_rows = hh <= 16 ? kHHRows : kHHRowsL;  // K slice of the hh ladder
+    ci.nhht = (int)ceil_div(pp, hh_rows);
     ci.t_off = o_t[c];
     ci.tkt_base = tkt; ci.tmt_base = tmt; ci.xt_base = xt; ci.vkt_base = vt;
     ci.part_off = part_tot;
@@ -839,13 +841,11 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     vraw_off.push_back(vraw_tot);
     if (!on_the_fly) vraw_tot += (int64_t)ci.pr * pp;  // packed rows (a <= b) only
     maxhh = std::max<int>(maxhh, (int)hh);
-    // hh ladder: one unit per (K slice, chunk of P rows): hh <= 16 is a single chunk, larger
-    // hh one chunk per 8 rows of P.
-    const int nchunk = hh <= 16 ? 1 : (int)ceil_div(hh, 8);
+    // hh ladder: hh <= 16, one warp unit per K slice (the whole P); wider hh, one CTA unit per
+    // K slice of kHHRowsL rows (every P row tile, hh_slice_kernel).
     for (int t = 0; t < ci.nhht; t++)
-      for (int q = 0; q < nchunk; q++)
-        hh_tiles.push_back({ai, t * kHHRows, t,
-                            (int)std::min<int64_t>(kHHRows, pp - (int64_t)t * kHHRows), q, 0});
+      hh_tiles.push_back({ai, t * hh_rows, t,
+                          (int)std::min<int64_t>(hh_rows, pp - (int64_t)t * hh_rows), 0, 0});
     for (int64_t i0 = 0; i0 < hh * hh; i0 += 256) hh_red.push_back({ai, (int32_t)i0});
     chans.push_back(ci);
     act_chan.push_back(c);
@@ -861,6 +861,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     return (int64_t)x.rows * a.hh * a.hh > (int64_t)y.rows * b.hh * b.hh;
   });
   for (const HHTile &t : hh_tiles) h->n_hh_small += chans[t.ch].hh <= 16 ? 1 : 0;
+  for (const ChanInfo &a : chans)
+    if (a.hh > 16) h->hh_slice_smem = std::max(h->hh_slice_smem, hh_slice_smem(a.hh));
   std::vector<int64_t> list_off(nsp + 1, 0);
   for (uint64_t w = 0; w < nsp; w++) list_off[w + 1] = list_off[w] + (int64_t)seg[w].size();
   std::vector<int32_t> list(list_off[nsp]);
@@ -1403,6 +1405,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   CK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->opt.device));
   if (h->ring_smem_mid > (size_t)smem_optin || h->ring_smem > (size_t)smem_optin)
     return CCDGPU_ERR_UNSUPPORTED;
+  CK(cudaFuncSetAttribute(hh_slice_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)hh_slice_smem(8 * kMaxCG)));
   CK(cudaFuncSetAttribute(ring_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin));
   CK(cudaFuncSetAttribute(ring_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin));
   ccdgpu_schedule sch{};
@@ -1457,8 +1461,8 @@ int launch_hh_ladder(ccdgpu_handle *h, cudaStream_t st, int gate, int only = -1)
   const int nbig = h->n_hh_tiles - h->n_hh_small;
   if (nbig && (only < 0 || only == 1)) {
     h->launches++;
-    CK(launch_pdl(hh_mma_kernel<kMaxCG>, (int)ceil_div(nbig, kHHWarps), kHHWarps * 32, 0, st,
-                  (const HHTile *)(h->hh_tiles + h->n_hh_small), nbig, (const ChanInfo *)h->chans,
+    CK(launch_pdl(hh_slice_kernel, nbig, kHHSliceThreads, h->hh_slice_smem, st,
+                  (const HHTile *)(h->hh_tiles + h->n_hh_small), (const ChanInfo *)h->chans,
                   (const double *)h->v_pphh, (const double *)h->t[0], (const double *)h->t[1],
                   h->part, h->r, (const Control *)h->ctl, gate));
   }
