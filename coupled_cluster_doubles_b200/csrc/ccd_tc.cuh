@@ -31,6 +31,7 @@
 #include <cuda_bf16.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "ccd_device.cuh"
 #include "ccd_kernels.cuh"
@@ -49,9 +50,9 @@ __host__ __device__ constexpr int tc_threads(bool gen) {
   return kTcThreads + (gen ? 32 * kTcGenWarps : 0);
 }
 // Dynamic shared memory: 1024 bytes of alignment slack, the stages, then the barriers
-// (2 S + 5 of them), then (gen) the q^2 table.
-__host__ __device__ constexpr size_t tc_smem_bytes(int nt, bool gen = false) {
-  return 1024 + tc_stages(nt) * tc_stage_bytes(nt) + 256 + (gen ? kTcGenTab * 4 : 0);
+// (2 S + 5 of them).  (The generator's q^2 table is a static shared array.)
+__host__ __device__ constexpr size_t tc_smem_bytes(int nt) {
+  return 1024 + tc_stages(nt) * tc_stage_bytes(nt) + 256;
 }
 
 // ---- V_pppp of the electron gas generated in the ladder ----------------------------------
@@ -60,8 +61,9 @@ __host__ __device__ constexpr size_t tc_smem_bytes(int nt, bool gen = false) {
 // depends only on the momentum transfer, zero at q = 0), with n_a - n_d = n_c - n_b inside a
 // channel (n_a + n_b = n_c + n_d).  Momenta are stored as three bytes biased by 64, so one
 // vabsdiffu4 gives |dx|, |dy|, |dz| and one dp4a gives q^2; the spin keys are 2 s_a + s_b
-// (rows) and 2 s_c + s_d, 2 s_d + s_c (columns).  w is a float table by q^2, so an element is
-// exact to FP32 before its bf16 split (the split keeps about 16 bits).
+// (rows) and 2 s_c + s_d, 2 s_d + s_c (columns).  w is a table by q^2, FP32 for the 2-term
+// split (which keeps about 16 bits) and FP64 for the 3-term split, so the element is exact to
+// the precision its split carries.
 struct VGenRow {
   uint32_t na, nb, key, pad;
 };
@@ -69,13 +71,31 @@ constexpr uint32_t kVGenZero = 0x404040u;  // momentum (0, 0, 0), biased
 struct VGenCol {
   uint32_t nc, keys;  // keys: key | swapped key << 8
 };
-__device__ __forceinline__ float vgen_elem(const VGenRow &r, uint32_t nc, uint32_t keys,
-                                           const float *tab) {
+template <int NT>
+using VGenT = typename std::conditional<NT == 3, double, float>::type;
+template <typename T>
+__device__ __forceinline__ T vgen_elem(const VGenRow &r, uint32_t nc, uint32_t keys,
+                                       const T *tab) {
   const uint32_t d1 = __vabsdiffu4(r.na, nc), d2 = __vabsdiffu4(r.nb, nc);
   const uint32_t q1 = __dp4a(d1, d1, 0u), q2 = __dp4a(d2, d2, 0u);
-  const float dir = r.key == (keys & 0xFFu) ? tab[q1] : 0.f;
-  const float exc = r.key == (keys >> 8) ? tab[q2] : 0.f;
+  const T dir = r.key == (keys & 0xFFu) ? tab[q1] : T(0);
+  const T exc = r.key == (keys >> 8) ? tab[q2] : T(0);
   return dir - exc;
+}
+// Two K-adjacent elements -> one 32-bit word (element k in the low half) of the current bf16
+// term, and the remainders for the next term.
+__device__ __forceinline__ uint32_t vgen_split(float &x0, float &x1) {
+  const __nv_bfloat162 t = __floats2bfloat162_rn(x0, x1);
+  x0 -= __low2float(t);
+  x1 -= __high2float(t);
+  return *reinterpret_cast<const uint32_t *>(&t);
+}
+__device__ __forceinline__ uint32_t vgen_split(double &x0, double &x1) {
+  const __nv_bfloat16 a = __double2bfloat16(x0), b = __double2bfloat16(x1);
+  x0 -= (double)__bfloat162float(a);
+  x1 -= (double)__bfloat162float(b);
+  const __nv_bfloat162 t = __halves2bfloat162(a, b);
+  return *reinterpret_cast<const uint32_t *>(&t);
 }
 
 // --- tcgen05 / descriptor helpers --------------------------------------------------------
@@ -174,7 +194,7 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
                     const int32_t *__restrict__ rowmap, const int32_t *__restrict__ mirror,
                     double *__restrict__ d, double *part, const Control *ctl, int32_t *err,
                     const ChanInfo *__restrict__ chans, const VGenRow *__restrict__ vg_rows,
-                    const VGenCol *__restrict__ vg_cols, const float *__restrict__ vg_tab) {
+                    const VGenCol *__restrict__ vg_cols, const double *__restrict__ vg_tab) {
   if (skip_iteration(ctl, 1, kTrLadderTC)) return;
   constexpr int S = tc_stages(NT);
   constexpr uint32_t kStageBytes = (uint32_t)tc_stage_bytes(NT);
@@ -186,11 +206,14 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
   uint64_t *bars = reinterpret_cast<uint64_t *>(tc_smem_raw + (base - raw) + S * kStageBytes);
   uint64_t *full = bars, *empty = bars + S, *acc_full = bars + 2 * S,
            *acc_empty = bars + 2 * S + 2, *done = bars + 2 * S + 4;
-  float *gtab = reinterpret_cast<float *>(tc_smem_raw + (base - raw) + S * kStageBytes + 256);
+  // The generator's table: a separate shared array, so that its loads are independent of the
+  // generators' stores into the stages.
+  __shared__ VGenT<NT> gtab[GEN ? kTcGenTab : 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if constexpr (GEN) {
     if (warp >= 6)
-      for (int i = threadIdx.x - 192; i < kTcGenTab; i += 32 * kTcGenWarps) gtab[i] = vg_tab[i];
+      for (int i = threadIdx.x - 192; i < kTcGenTab; i += 32 * kTcGenWarps)
+        gtab[i] = (VGenT<NT>)vg_tab[i];
   }
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
@@ -316,9 +339,12 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
   } else if (GEN && warp >= 6) {
     // ---- V generators: warp gw owns row groups gw, gw + G, ... of each tile; a lane writes
     // row 8 rg + lane / 4, K columns 8 kg + 2 (lane % 4) + {0, 1} of every core matrix (one
-    // 32-bit word per plane: conflict-free) ----
+    // 32-bit word per plane: conflict-free).  The K columns' codes of the next chunk are
+    // loaded while the current one is generated. ----
+    using GT = VGenT<NT>;
     const int gw = warp - 6;
     constexpr int RG = (kTcBM / 8) / kTcGenWarps;  // row groups per generator warp
+    unsigned char *stage0 = tc_smem_raw + (base - raw);
     int gc = 0;
     bool stop = false;
     for (int ti = t_begin; ti < t_end && !stop; ++ti) {
@@ -335,8 +361,23 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
         rw[i] = r < tile.rows ? vg_rows[tile.row_off + (int64_t)tile.mt * kTcBM + r]
                               : VGenRow{kVGenZero, kVGenZero, 0xFFu, 0u};
       }
+      uint32_t cn[8], ck[8];
+      auto load_cols = [&](int c, uint32_t *n, uint32_t *k) {
+        const int kc = tile.kc0 + c;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {  // columns 8 (j / 2) + 2 (lane % 4) + j % 2
+          const int w = kc * kTcKC + 8 * (j >> 1) + 2 * (lane & 3) + (j & 1);
+          const VGenCol cl = w < pk ? vg_cols[pk_off + w] : VGenCol{kVGenZero, 0xFEFEu};
+          n[j] = cl.nc;
+          k[j] = cl.keys;
+        }
+      };
+      if (tile.nks > 0) load_cols(0, cn, ck);
       for (int c = 0; c < nchunks; ++c, ++gc) {
         const int s = gc % S;
+        uint32_t nn[8], nk[8];
+        const bool pre = c + 1 < tile.nks;
+        if (pre) load_cols(c + 1, nn, nk);
         if (read_flag(&abort_flag) ||
             (gc >= S && !mbar_wait(smem_u32(&empty[s]), ((gc / S) - 1) & 1))) {
           fail();
@@ -344,40 +385,34 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
           break;
         }
         if (c < tile.nks) {
-          const int kc = tile.kc0 + c;
-          uint32_t cn[8], ck[8];
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {  // columns 8 (j / 2) + 2 (lane % 4) + j % 2
-            const int w = kc * kTcKC + 8 * (j >> 1) + 2 * (lane & 3) + (j & 1);
-            const VGenCol cl = w < pk ? vg_cols[pk_off + w] : VGenCol{kVGenZero, 0xFEFEu};
-            cn[j] = cl.nc;
-            ck[j] = cl.keys;
-          }
-          const uint32_t sa = base + s * kStageBytes;
+          unsigned char *sa = stage0 + s * kStageBytes;
 #pragma unroll
           for (int i = 0; i < RG; ++i) {
             const int rg = gw + i * kTcGenWarps;
             if (8 * rg >= tile.rows) continue;
+            GT v[8];
 #pragma unroll
-            for (int kg = 0; kg < 4; ++kg) {
-              float v[2];
+            for (int j = 0; j < 8; ++j) v[j] = vgen_elem<GT>(rw[i], cn[j], ck[j], gtab);
+            const uint32_t off =
+                (uint32_t)(rg * kTcGroup + (lane >> 2) * 8 + 2 * (lane & 3)) * 2;
 #pragma unroll
-              for (int e = 0; e < 2; ++e) v[e] = vgen_elem(rw[i], cn[2 * kg + e], ck[2 * kg + e], gtab);
-              const uint32_t off = (uint32_t)(rg * kTcGroup + kg * 64 + (lane >> 2) * 8 + 2 * (lane & 3)) * 2;
+            for (int p = 0; p < NT; ++p)
 #pragma unroll
-              for (int p = 0; p < NT; ++p) {
-                const __nv_bfloat162 t = __floats2bfloat162_rn(v[0], v[1]);
-                asm volatile("st.shared.b32 [%0], %1;" ::"r"(sa + p * kTcAPlane * 2 + off),
-                             "r"(*reinterpret_cast<const uint32_t *>(&t)) : "memory");
-                v[0] -= __low2float(t);
-                v[1] -= __high2float(t);
-              }
-            }
+              for (int kg = 0; kg < 4; ++kg)
+                *reinterpret_cast<uint32_t *>(sa + p * kTcAPlane * 2 + off + kg * 128) =
+                    vgen_split(v[2 * kg], v[2 * kg + 1]);
           }
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(smem_u32(&full[s]));
+        if (pre) {
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            cn[j] = nn[j];
+            ck[j] = nk[j];
+          }
+        }
       }
     }
   } else {

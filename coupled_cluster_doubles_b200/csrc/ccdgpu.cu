@@ -139,7 +139,7 @@ struct ccdgpu_handle {
   bool tc_gen = false;
   VGenRow *vg_rows = nullptr;
   VGenCol *vg_cols = nullptr;
-  float *vg_tab = nullptr;
+  double *vg_tab = nullptr;
   int64_t n_vtc = 0, n_tkttc = 0, n_tmttc = 0, n_xttc = 0;  // plane strides (elements)
   size_t tc_smem = 0;
   double ladder_bytes_tc = 0;
@@ -712,7 +712,7 @@ using TcKernel = void (*)(const LadderTile *, const int32_t *, const __nv_bfloat
                          const __nv_bfloat16 *, int64_t, const __nv_bfloat16 *, int64_t,
                          const __nv_bfloat16 *, int64_t, const int32_t *, const int32_t *,
                          double *, double *, const Control *, int32_t *, const ChanInfo *,
-                         const VGenRow *, const VGenCol *, const float *);
+                         const VGenRow *, const VGenCol *, const double *);
 TcKernel tc_kernel_of(int nt, bool gen) {
   if (nt == 2) return gen ? pp_ladder_tc_kernel<2, true> : pp_ladder_tc_kernel<2, false>;
   return gen ? pp_ladder_tc_kernel<3, true> : pp_ladder_tc_kernel<3, false>;
@@ -1028,7 +1028,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   // keys of (c, d) and (d, c); the direct term by q^2.
   std::vector<VGenRow> vg_rows;
   std::vector<VGenCol> vg_cols;
-  std::vector<float> vg_tab;
+  std::vector<double> vg_tab;
   if (on_the_fly && h->nt && model_ok && M->kind == CCDGPU_MODEL_ELECTRON_GAS) {
     int nmax = 0;
     for (uint64_t o = 0; o < nsp; o++)
@@ -1056,10 +1056,10 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
       // w(q^2) = e^2 / L^3 * 4 pi / (2 pi / L)^2 q^2, zero for q = 0 (ElectronGasSPBasis.cpp:
       // 453-466 as a function of q^2).
       const double L = M->params[0], e_sq = M->params[1];
-      vg_tab.assign(kTcGenTab, 0.f);
+      vg_tab.assign(kTcGenTab, 0.0);
       for (int q2 = 1; q2 < kTcGenTab; q2++) {
         const double rel = (2 * M_PI / L) * (2 * M_PI / L) * q2;
-        vg_tab[q2] = (float)(e_sq / (L * L * L) * 4 * M_PI / rel);
+        vg_tab[q2] = e_sq / (L * L * L) * 4 * M_PI / rel;
       }
       // The ladder then moves no V bytes: the T and X operand images and D.
       double lbg = 0;
@@ -1415,7 +1415,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   sch.tc_split_mul = 2;
   if (int rc2 = make_ladder_tiles(h, sch)) return rc2;
   if (h->nt) {
-    h->tc_smem = tc_smem_bytes(h->nt, h->tc_gen);
+    h->tc_smem = tc_smem_bytes(h->nt);
     CK(cudaFuncSetAttribute(tc_kernel_of(h->nt, h->tc_gen),
                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->tc_smem));
   }
@@ -1485,7 +1485,7 @@ int launch_pp_ladder_tc(ccdgpu_handle *h, cudaStream_t st) {
                 (const __nv_bfloat16 *)h->xt_tc, h->n_xttc, (const int32_t *)h->rowmap,
                 (const int32_t *)h->mirror, h->dmat, h->tc_part, (const Control *)h->ctl, h->err,
                 (const ChanInfo *)h->chans, (const VGenRow *)h->vg_rows,
-                (const VGenCol *)h->vg_cols, (const float *)h->vg_tab));
+                (const VGenCol *)h->vg_cols, (const double *)h->vg_tab));
   if (h->n_red_tc) {
     CK(launch_pdl(ladder_reduce_kernel, h->n_red_tc, 256, 0, st, (const RedItem *)h->red_tc,
                   (const LadderTile *)h->tc_tiles, (const int32_t *)h->rowmap,

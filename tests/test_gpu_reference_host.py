@@ -29,7 +29,7 @@ def _run(cli, env_extra=None):
     env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1", **(env_extra or {}))
     out = subprocess.run([EXE, *cli.split()], env=env, capture_output=True, text=True,
                          timeout=600, check=True).stdout
-    val = {k: float(v) for k, v in re.findall(r"^([A-Za-z_/]+): ([-0-9.eE+]+)", out, re.M)}
+    val = {k: float(v) for k, v in re.findall(r"^([A-Za-z0-9_/]+): ([-0-9.eE+]+)", out, re.M)}
     return val
 
 
