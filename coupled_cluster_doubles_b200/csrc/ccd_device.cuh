@@ -177,9 +177,12 @@ struct QuadCol {
   int32_t c_ij, c_ji, i, j;
   double eij;
 };
-// Work item of the fused assembly: quads [q0, q1) (q = u * hk + w) of active channel ch.
+// Work item of the fused assembly: quads [q0, q1) (q = u * hk + w) of active channel ch, with
+// the channel's hk, block offset and table offsets (so a thread's table reads depend on the
+// item alone).
 struct QuadItem {
-  int32_t ch, q0, q1, pad;
+  int32_t ch, q0, q1, hk;
+  int64_t t_off, qrow_off, qcol_off;
 };
 
 // Per active modified channel.

@@ -1034,12 +1034,44 @@ __device__ __forceinline__ void loop_set_condition(const Control *ctl,
 // four elements, their phhp copies and the operand-image entries of rows ab (row ba is in
 // neither image).  The energy gains 4 V t_new per quad.
 // Persistent CTAs stride over work items of up to kQuadPerItem quads of one channel; a thread
-// takes kQuadPerThread quads of an item and issues all their loads before the first store.
+// takes one quad of an item and issues all its loads before the first store.
 // In a mixed iteration (nt > 0) only the bf16 operand images are written; retile_kernel
 // rebuilds the FP64 tiles if FP64 iterations follow.
-constexpr int kQuadPerThread = 1;
-constexpr int kQuadPerItem = kQuadPerThread * kAsmThreads;
+constexpr int kQuadPerItem = kAsmThreads;  // one quad per thread and item
 constexpr int kAsmCTAsPerSM = 4;
+
+// One thread's quad of a work item: where its four elements sit in the channel block, its
+// operand-image indices, one-body indices and denominator.  ok = false: no quad (past the
+// item or past the last item).
+struct QuadRef {
+  int32_t o_ab, o_ba, c_ij, c_ji, qx, qy, pa, pb, i, j, ch;
+  bool ok;
+  int64_t t_off;
+  double den;
+};
+__device__ __forceinline__ void quad_fetch(const QuadItem *__restrict__ items, int n_items,
+                                           const QuadRow *__restrict__ qrows,
+                                           const QuadCol *__restrict__ qcols, int it,
+                                           QuadRef &r) {
+  r.ok = false;
+  if (it >= n_items) return;
+  const QuadItem item = items[it];
+  const int q = item.q0 + threadIdx.x;
+  if (q >= item.q1) return;
+  // q / hk as a multiply-high by ceil(2^32 / hk) (Granlund-Montgomery): exact for
+  // q < 2^32 / hk (q < 2^21, hk < 2^11 here); hk = 1 has no 32-bit multiplier.
+  const int hk = item.hk;
+  const uint32_t magic = hk > 1 ? 0xFFFFFFFFu / (uint32_t)hk + 1u : 0u;
+  const int u = hk > 1 ? (int)__umulhi((uint32_t)q, magic) : q, w = q - u * hk;
+  const QuadRow rw = qrows[item.qrow_off + u];
+  const QuadCol cl = qcols[item.qcol_off + w];
+  r.o_ab = rw.o_ab; r.o_ba = rw.o_ba; r.qx = rw.qx; r.qy = rw.qy; r.pa = rw.pa; r.pb = rw.pb;
+  r.c_ij = cl.c_ij; r.c_ji = cl.c_ji; r.i = cl.i; r.j = cl.j;
+  r.den = cl.eij - rw.ea - rw.eb;
+  r.ch = item.ch;
+  r.t_off = item.t_off;
+  r.ok = true;
+}
 
 // value of element (ab, ij) (calc.cpp:384-418) with t_ab,ji = -t and t_ba,ij = -t:
 //   V + D + R_ai,jb - R_aj,ib - R_bi,ja + R_bj,ia + 0.5 x_i t_ab,ji - 0.5 x_j t_ab,ij
@@ -1090,72 +1122,54 @@ assemble_fused_kernel(const QuadItem *__restrict__ items, int n_items,
   double *__restrict__ t_new = ctl->parity ? tbuf0 : tbuf1;
   const double mixing = ctl->mixing;
   double corr = 0.0;
+  // Two-stage pipeline over the CTA's items: the next item's header and this thread's row and
+  // column table entries are fetched while the current quad's operand loads are in flight.
+  QuadRef nx;
+  quad_fetch(items, n_items, qrows, qcols, blockIdx.x, nx);
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
-    const QuadItem item = items[it];
-    const ChanInfo &ch = chans[item.ch];
-    const int hk = ch.hk, q1 = item.q1;
-    const int64_t t_off = ch.t_off;
-    const QuadRow *__restrict__ rtab = qrows + ch.qrow_off;
-    const QuadCol *__restrict__ ctab = qcols + ch.qcol_off;
-    // q / hk as a multiply-high by ceil(2^32 / hk) (Granlund-Montgomery): exact for
-    // q < 2^32 / hk (q < 2^21, hk < 2^11 here); hk = 1 has no 32-bit multiplier.
-    const uint32_t magic = hk > 1 ? 0xFFFFFFFFu / (uint32_t)hk + 1u : 0u;
-    double tv[kQuadPerThread], vv[kQuadPerThread], dv[kQuadPerThread], rv[kQuadPerThread][4];
-    double den[kQuadPerThread], xs[kQuadPerThread][2], ys[kQuadPerThread][2];
-    int32_t gv[kQuadPerThread][4], pos[kQuadPerThread][4], qx[kQuadPerThread],
-        qy[kQuadPerThread], cij[kQuadPerThread], cji[kQuadPerThread];
-#pragma unroll
-    for (int k = 0; k < kQuadPerThread; ++k) {
-      const int q = item.q0 + threadIdx.x + k * kAsmThreads;
-      if (q >= q1) continue;
-      const int u = hk > 1 ? (int)__umulhi((uint32_t)q, magic) : q, w = q - u * hk;
-      const QuadRow rw = rtab[u];
-      const QuadCol cl = ctab[w];
-      pos[k][0] = rw.o_ab + cl.c_ij;
-      pos[k][1] = rw.o_ab + cl.c_ji;
-      pos[k][2] = rw.o_ba + cl.c_ij;
-      pos[k][3] = rw.o_ba + cl.c_ji;
-      qx[k] = rw.qx;
-      qy[k] = rw.qy;
-      cij[k] = cl.c_ij;
-      cji[k] = cl.c_ji;
-      den[k] = cl.eij - rw.ea - rw.eb;
-      const int64_t p0 = t_off + pos[k][0];
-      tv[k] = t_old[p0];
-      vv[k] = __ldg(v_pphh + p0);
-      dv[k] = __ldcg(dmat + p0);
+    const QuadRef cu = nx;
+    double tv = 0.0, vv = 0.0, dv = 0.0, rv[4] = {0.0, 0.0, 0.0, 0.0}, xs[2] = {0.0, 0.0},
+           ys[2] = {0.0, 0.0};
+    int32_t gv[4] = {0, 0, 0, 0}, pos[4];
+    pos[0] = cu.o_ab + cu.c_ij;
+    pos[1] = cu.o_ab + cu.c_ji;
+    pos[2] = cu.o_ba + cu.c_ij;
+    pos[3] = cu.o_ba + cu.c_ji;
+    if (cu.ok) {
+      const int64_t p0 = cu.t_off + pos[0];
+      tv = t_old[p0];
+      vv = __ldg(v_pphh + p0);
+      dv = __ldcg(dmat + p0);
 #pragma unroll
       for (int m = 0; m < 4; ++m) {
-        rv[k][m] = __ldcg(d_ring + t_off + pos[k][m]);
-        gv[k][m] = __ldg(g_ai_jb + t_off + pos[k][m]);
+        rv[m] = __ldcg(d_ring + cu.t_off + pos[m]);
+        gv[m] = __ldg(g_ai_jb + cu.t_off + pos[m]);
       }
-      xs[k][0] = __ldcg(xh + cl.i);
-      xs[k][1] = __ldcg(xh + cl.j);
-      ys[k][0] = __ldcg(yp + rw.pa);
-      ys[k][1] = __ldcg(yp + rw.pb);
+      xs[0] = __ldcg(xh + cu.i);
+      xs[1] = __ldcg(xh + cu.j);
+      ys[0] = __ldcg(yp + cu.pa);
+      ys[1] = __ldcg(yp + cu.pb);
     }
+    quad_fetch(items, n_items, qrows, qcols, it + gridDim.x, nx);
+    if (!cu.ok) continue;
+    const double t1 = quad_value(vv, dv, rv[0], rv[1], rv[2], rv[3], tv, xs[0], xs[1], ys[0],
+                                 ys[1], cu.den, mixing);
+    const double sg[4] = {t1, -t1, -t1, t1};
 #pragma unroll
-    for (int k = 0; k < kQuadPerThread; ++k) {
-      const int q = item.q0 + threadIdx.x + k * kAsmThreads;
-      if (q >= q1) continue;
-      const double t1 = quad_value(vv[k], dv[k], rv[k][0], rv[k][1], rv[k][2], rv[k][3], tv[k],
-                                   xs[k][0], xs[k][1], ys[k][0], ys[k][1], den[k], mixing);
-      const double sg[4] = {t1, -t1, -t1, t1};
-#pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        t_new[t_off + pos[k][m]] = sg[m];
-        old_phhp[gv[k][m]] = sg[m];
-      }
-      const int2 qa = make_int2(qx[k], qy[k]);
-      if (nt) {
-        write_t_tiles_tc(ch, qa, cij[k], t1, nt, tkt_tc, tkt_tc_stride, tmt_tc, tmt_tc_stride);
-        write_t_tiles_tc(ch, qa, cji[k], -t1, nt, tkt_tc, tkt_tc_stride, tmt_tc, tmt_tc_stride);
-      } else {
-        write_t_tiles_q(ch, qa, cij[k], t1, t_kt, t_mt);
-        write_t_tiles_q(ch, qa, cji[k], -t1, t_kt, t_mt);
-      }
-      corr += 4.0 * (vv[k] * t1);
+    for (int m = 0; m < 4; ++m) {
+      t_new[cu.t_off + pos[m]] = sg[m];
+      old_phhp[gv[m]] = sg[m];
     }
+    const ChanInfo &ch = chans[cu.ch];
+    const int2 qa = make_int2(cu.qx, cu.qy);
+    if (nt) {
+      write_t_tiles_tc(ch, qa, cu.c_ij, t1, nt, tkt_tc, tkt_tc_stride, tmt_tc, tmt_tc_stride);
+      write_t_tiles_tc(ch, qa, cu.c_ji, -t1, nt, tkt_tc, tkt_tc_stride, tmt_tc, tmt_tc_stride);
+    } else {
+      write_t_tiles_q(ch, qa, cu.c_ij, t1, t_kt, t_mt);
+      write_t_tiles_q(ch, qa, cu.c_ji, -t1, t_kt, t_mt);
+    }
+    corr += 4.0 * (vv * t1);
   }
   const double sum = block_sum<kAsmThreads>(corr, scratch);
   // The last CTA to finish sums the partials and applies the stop rule (no extra launch).

@@ -990,7 +990,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     const int64_t nq = rows_q * a.hk;
     if (nq >= ((int64_t)1 << 31) / 2) return CCDGPU_ERR_UNSUPPORTED;
     for (int64_t q = 0; q < nq; q += kQuadPerItem)
-      quad_items.push_back({ai, (int32_t)q, (int32_t)std::min<int64_t>(nq, q + kQuadPerItem), 0});
+      quad_items.push_back({ai, (int32_t)q, (int32_t)std::min<int64_t>(nq, q + kQuadPerItem),
+                            a.hk, a.t_off, a.qrow_off, a.qcol_off});
   }
   h->host_chans = chans;
   h->n_quad_items = (int)quad_items.size();
