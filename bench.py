@@ -275,12 +275,27 @@ def golden_reference(name):
     return {"e_corr": float(g["energies"][-1]), "t2": g["t2"], "full": bool(g["t2_full"][0])}
 
 
-def assemble_bytes(n_t2, nt):
-    """Algorithmic bytes of one fused assembly launch: per amplitude, read t_old, R (the ring
-    term in pphh order), V, D and the int32 phhp index, write t_new and its phhp copy (52 B),
-    plus the next iteration's ladder operands: nt bf16 terms (mixed) or one FP64 value in the
-    operand image that holds its row (each amplitude is in one of them)."""
-    return n_t2 * (52.0 + (2.0 * nt if nt else 8.0))
+def quad_count(system):
+    """Quads of the fused assembly: (strict particle pair a < b, strict hole pair i < j) per
+    channel, summed over the channels."""
+    import numpy as np
+    d = system.chan_dims().astype(np.int64)
+    pp = system.array("pp_map").reshape(-1, 2)
+    hh = system.array("hh_map").reshape(-1, 2)
+    ps = np.concatenate([[0], np.cumsum((pp[:, 0] < pp[:, 1]).astype(np.int64))])
+    hs = np.concatenate([[0], np.cumsum((hh[:, 0] < hh[:, 1]).astype(np.int64))])
+    po = np.concatenate([[0], np.cumsum(d[:, 0])])
+    ho = np.concatenate([[0], np.cumsum(d[:, 1])])
+    return int(((ps[po[1:]] - ps[po[:-1]]) * (hs[ho[1:]] - hs[ho[:-1]])).sum())
+
+
+def assemble_bytes(n_quads, nt):
+    """Algorithmic bytes of one fused assembly launch, per quad (four amplitudes (ab,ij),
+    (ab,ji), (ba,ij), (ba,ji)): read t, V and D at (ab,ij), R and the int32 phhp index at the
+    four positions (72 B); write the four amplitudes and their phhp copies (64 B) and the next
+    iteration's operand-image entries of row ab, columns ij and ji, in both images: nt bf16
+    terms each (mixed) or one FP64 value."""
+    return n_quads * (136.0 + (8.0 * nt if nt else 32.0))
 
 
 def main():
@@ -409,6 +424,7 @@ def main():
     ladder_cls = {a: solvers[a].ladder_profile(reps=5) for a in arms}
     other_cls = solvers[arms[0]].kernel_profile(reps=5)  # shared by both arms
     n_t2 = solvers[arms[0]].n_t2
+    n_quads = quad_count(system)
     nt_of = {"mixed": 2, "fp64": 0}
 
     # e2e (headline arm): the public API from host buffers, every step: create (H2D upload)
@@ -475,7 +491,7 @@ def main():
             lad = "pp_ladder_tc_kernel<2>" if a == "mixed" else "pp_ladder_kernel<0,1,2>"
             fams = [
                 ("pp_ladder", lad, work[a]["ladder_bytes"], work[a]["ladder_flops"]),
-                ("assemble_energy", "assemble_fused_kernel", assemble_bytes(n_t2, nt), 0.0),
+                ("assemble_energy", "assemble_fused_kernel", assemble_bytes(n_quads, nt), 0.0),
                 ("ring", "ring_small_kernel + ring_kernel<2/4>",
                  cls_bytes("ring_small", "ring_mid", "ring_large"),
                  cls_flops("ring_small", "ring_mid", "ring_large")),
