@@ -936,18 +936,20 @@ __global__ void onebody_fused_kernel(int np, int nsp, const int64_t *__restrict_
   if (w >= nsp) return;
   const bool hole = w < np;
   const double *src = hole ? s : r;
-  double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+  // Eight lane-strided partial sums: the eight index loads of a round are issued together,
+  // then the eight value loads, so a round costs two memory latencies.
+  double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   const int64_t hi = list_off[w + 1];
   int64_t e = list_off[w] + lane;
-  for (; e + 96 < hi; e += 128) {
-    const int32_t i0 = list[e], i1 = list[e + 32], i2 = list[e + 64], i3 = list[e + 96];
-    v0 += src[i0];
-    v1 += src[i1];
-    v2 += src[i2];
-    v3 += src[i3];
+  for (; e + 224 < hi; e += 256) {
+    int32_t ix[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) ix[k] = __ldg(list + e + 32 * k);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc[k] += __ldcg(src + ix[k]);
   }
-  for (; e < hi; e += 32) v0 += src[list[e]];
-  double v = (v0 + v1) + (v2 + v3);
+  for (; e < hi; e += 32) acc[0] += __ldcg(src + __ldg(list + e));
+  double v = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   if (lane == 0) {
