@@ -515,7 +515,9 @@ def main():
             return out
 
         roof = {a: kernel_rooflines(a) for a in arms}
-        dominant = max(roof[head], key=lambda f: roof[head][f]["avg_launch_ms"])
+        # The table path has no per-family events (its stages are separate calls): no roofline.
+        dominant = (max(roof[head], key=lambda f: roof[head][f]["avg_launch_ms"])
+                    if roof[head] else None)
         arms_out = {}
         for a in arms:
             ta = timing[a]
@@ -595,7 +597,8 @@ def main():
                               "ccdgpu_destroy",
                     "rank0_ms_per_step": dict(zip(["create", "solve", "get_t2", "destroy"],
                                                   (1e3 * phase_s / args.steps).round(3).tolist()))},
-            "roofline": {**roof[head][dominant], "family": dominant, "peak_source": peak_kind},
+            "roofline": ({**roof[head][dominant], "family": dominant, "peak_source": peak_kind}
+                         if dominant else None),
             "gpu_launches": int(t["launches"]),
             "clocks": clocks.summary(),
         }
