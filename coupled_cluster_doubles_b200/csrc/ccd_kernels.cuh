@@ -658,18 +658,17 @@ hh_reduce_kernel(const HHRed *__restrict__ items, const ChanInfo *__restrict__ c
   const int hh = ch.hh, nout = hh * hh, idx = it.idx0 + threadIdx.x;
   if (idx >= nout) return;
   const double *pb = part + ch.part_off + idx;
-  // Four interleaved partial sums over the slices (their loads independent, so they are in
+  // Eight interleaved partial sums over the slices (their loads independent, so they are in
   // flight together), combined in a fixed order.
-  double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
+  double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   int sl = 0;
-  for (; sl + 4 <= ch.nhht; sl += 4) {
-    p0 += __ldcg(pb + (int64_t)sl * nout);
-    p1 += __ldcg(pb + (int64_t)(sl + 1) * nout);
-    p2 += __ldcg(pb + (int64_t)(sl + 2) * nout);
-    p3 += __ldcg(pb + (int64_t)(sl + 3) * nout);
+  for (; sl + 8 <= ch.nhht; sl += 8) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc[k] += __ldcg(pb + (int64_t)(sl + k) * nout);
   }
-  for (; sl < ch.nhht; ++sl) p0 += __ldcg(pb + (int64_t)sl * nout);
-  const double p = (p0 + p1) + (p2 + p3);
+  for (int k = 0; sl < ch.nhht; ++sl, ++k) acc[k] += __ldcg(pb + (int64_t)sl * nout);
+  const double p =
+      ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
   hh_finish(ch, idx / hh, idx - (idx / hh) * hh, p, v_hhhh, x_ref, x_t, s_out, xt_tc,
             xt_tc_stride, nt);
 }
@@ -1147,10 +1146,12 @@ assemble_fused_kernel(const QuadItem *__restrict__ items, int n_items,
         rv[m] = __ldcg(d_ring + cu.t_off + pos[m]);
         gv[m] = __ldg(g_ai_jb + cu.t_off + pos[m]);
       }
-      xs[0] = __ldcg(xh + cu.i);
-      xs[1] = __ldcg(xh + cu.j);
-      ys[0] = __ldcg(yp + cu.pa);
-      ys[1] = __ldcg(yp + cu.pb);
+      // The one-body sums are small arrays every quad reads: through L1 (an L2-only load
+      // would send every warp to the same few L2 slices).
+      xs[0] = xh[cu.i];
+      xs[1] = xh[cu.j];
+      ys[0] = yp[cu.pa];
+      ys[1] = yp[cu.pb];
     }
     quad_fetch(items, n_items, qrows, qcols, it + gridDim.x, nx);
     if (!cu.ok) continue;

@@ -42,10 +42,8 @@ __host__ __device__ constexpr int tc_stages(int nt) { return nt == 2 ? 4 : 3; }
 __host__ __device__ constexpr size_t tc_stage_bytes(int nt) {
   return (size_t)nt * (kTcAPlane + kTcBPlane) * 2;
 }
-// V_pppp generated inside the ladder (electron gas): generator warps, and the size of the
-// direct-term table by squared momentum transfer q^2 (|n| <= 6 per axis: q^2 <= 432).
+// V_pppp generated inside the ladder (electron gas): generator warps.
 constexpr int kTcGenWarps = 4;
-constexpr int kTcGenTab = 512;
 __host__ __device__ constexpr int tc_threads(bool gen) {
   return kTcThreads + (gen ? 32 * kTcGenWarps : 0);
 }
@@ -56,31 +54,33 @@ __host__ __device__ constexpr size_t tc_smem_bytes(int nt) {
 }
 
 // ---- V_pppp of the electron gas generated in the ladder ----------------------------------
-// <ab|v|cd> = [s_a = s_c, s_b = s_d] w(|n_a - n_c|^2) - [s_a = s_d, s_b = s_c] w(|n_a - n_d|^2)
+// <ab|v|cd> = [s_a = s_c] w(|n_a - n_c|^2) - [s_b = s_c] w(|n_c - n_b|^2)
 // (ElectronGasSPBasis.cpp:418-471: direct minus exchange, spin-diagonal Coulomb term that
-// depends only on the momentum transfer, zero at q = 0), with n_a - n_d = n_c - n_b inside a
-// channel (n_a + n_b = n_c + n_d).  Momenta are stored as three bytes biased by 64, so one
-// vabsdiffu4 gives |dx|, |dy|, |dz| and one dp4a gives q^2; the spin keys are 2 s_a + s_b
-// (rows) and 2 s_c + s_d, 2 s_d + s_c (columns).  w is a table by q^2, FP32 for the 2-term
-// split (which keeps about 16 bits) and FP64 for the 3-term split, so the element is exact to
-// the precision its split carries.
+// depends only on the momentum transfer, zero at q = 0).  Inside a channel n_a + n_b = n_c + n_d
+// and s_a + s_b = s_c + s_d, so n_a - n_d = n_c - n_b, and s_a = s_c implies s_b = s_d (the
+// direct term's other spin condition) as s_b = s_c implies s_a = s_d.  An orbital's code holds
+// n_x, n_y, n_z biased by 64 in bytes 0-2 and kVGenSpin * [s > 0] in byte 3.  For two codes,
+// (x - y + 0x80808080) ^ 0x80808080 holds the signed byte differences (every biased byte
+// difference lies in [107, 149], so nothing borrows across bytes), and one dp4a of it with
+// itself gives q^2 plus kVGenSpin^2 = 441 > 432 when the spins differ.  w is a table by that
+// index, zero at 0 and beyond 432: spin mismatches and q = 0 read zeros.  FP32 for the 2-term
+// split (which keeps about 16 bits), FP64 for the 3-term split, so the element is exact to the
+// precision its split carries.
 struct VGenRow {
-  uint32_t na, nb, key, pad;
+  uint32_t na, nb;
 };
-constexpr uint32_t kVGenZero = 0x404040u;  // momentum (0, 0, 0), biased
-struct VGenCol {
-  uint32_t nc, keys;  // keys: key | swapped key << 8
-};
+constexpr uint32_t kVGenZero = 0x404040u;  // momentum (0, 0, 0), spin down, biased
+constexpr int kVGenSpin = 21;
+constexpr int kTcGenTab = 3 * 12 * 12 + kVGenSpin * kVGenSpin + 1;  // |n_i| <= 6: 874 entries
 template <int NT>
 using VGenT = typename std::conditional<NT == 3, double, float>::type;
+__device__ __forceinline__ int vgen_q2(uint32_t x, uint32_t y) {
+  const int d = (int)((x - y + 0x80808080u) ^ 0x80808080u);
+  return __dp4a(d, d, 0);
+}
 template <typename T>
-__device__ __forceinline__ T vgen_elem(const VGenRow &r, uint32_t nc, uint32_t keys,
-                                       const T *tab) {
-  const uint32_t d1 = __vabsdiffu4(r.na, nc), d2 = __vabsdiffu4(r.nb, nc);
-  const uint32_t q1 = __dp4a(d1, d1, 0u), q2 = __dp4a(d2, d2, 0u);
-  const T dir = r.key == (keys & 0xFFu) ? tab[q1] : T(0);
-  const T exc = r.key == (keys >> 8) ? tab[q2] : T(0);
-  return dir - exc;
+__device__ __forceinline__ T vgen_elem(const VGenRow &r, uint32_t nc, const T *tab) {
+  return tab[vgen_q2(r.na, nc)] - tab[vgen_q2(r.nb, nc)];
 }
 // Two K-adjacent elements -> one 32-bit word (element k in the low half) of the current bf16
 // term, and the remainders for the next term.
@@ -194,7 +194,7 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
                     const int32_t *__restrict__ rowmap, const int32_t *__restrict__ mirror,
                     double *__restrict__ d, double *part, const Control *ctl, int32_t *err,
                     const ChanInfo *__restrict__ chans, const VGenRow *__restrict__ vg_rows,
-                    const VGenCol *__restrict__ vg_cols, const double *__restrict__ vg_tab) {
+                    const uint32_t *__restrict__ vg_cols, const double *__restrict__ vg_tab) {
   if (skip_iteration(ctl, 1, kTrLadderTC)) return;
   constexpr int S = tc_stages(NT);
   constexpr uint32_t kStageBytes = (uint32_t)tc_stage_bytes(NT);
@@ -356,20 +356,20 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
 #pragma unroll
       for (int i = 0; i < RG; ++i) {
         const int r = 8 * (gw + i * kTcGenWarps) + (lane >> 2);
-        // Rows past the tile: zero momenta (so q^2 stays inside the table) and a spin key that
-        // matches no column, so the element is 0.
+        // Rows past the tile: zero momenta, so the index stays inside the table (their
+        // accumulator rows are never read).
         rw[i] = r < tile.rows ? vg_rows[tile.row_off + (int64_t)tile.mt * kTcBM + r]
-                              : VGenRow{kVGenZero, kVGenZero, 0xFFu, 0u};
+                              : VGenRow{kVGenZero, kVGenZero};
       }
+      // Column codes of a chunk; K padding (w >= pk) is flagged by code 0 and becomes 0.
       uint32_t cn[8], ck[8];
       auto load_cols = [&](int c, uint32_t *n, uint32_t *k) {
         const int kc = tile.kc0 + c;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {  // columns 8 (j / 2) + 2 (lane % 4) + j % 2
           const int w = kc * kTcKC + 8 * (j >> 1) + 2 * (lane & 3) + (j & 1);
-          const VGenCol cl = w < pk ? vg_cols[pk_off + w] : VGenCol{kVGenZero, 0xFEFEu};
-          n[j] = cl.nc;
-          k[j] = cl.keys;
+          n[j] = w < pk ? vg_cols[pk_off + w] : kVGenZero;
+          k[j] = w < pk;
         }
       };
       if (tile.nks > 0) load_cols(0, cn, ck);
@@ -392,7 +392,7 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
             if (8 * rg >= tile.rows) continue;
             GT v[8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) v[j] = vgen_elem<GT>(rw[i], cn[j], ck[j], gtab);
+            for (int j = 0; j < 8; ++j) v[j] = ck[j] ? vgen_elem<GT>(rw[i], cn[j], gtab) : GT(0);
             const uint32_t off =
                 (uint32_t)(rg * kTcGroup + (lane >> 2) * 8 + 2 * (lane & 3)) * 2;
 #pragma unroll

@@ -138,7 +138,7 @@ struct ccdgpu_handle {
   // planes itself (no v_tc images) from these per-row / per-K-column codes and the q^2 table.
   bool tc_gen = false;
   VGenRow *vg_rows = nullptr;
-  VGenCol *vg_cols = nullptr;
+  uint32_t *vg_cols = nullptr;
   double *vg_tab = nullptr;
   int64_t n_vtc = 0, n_tkttc = 0, n_tmttc = 0, n_xttc = 0;  // plane strides (elements)
   size_t tc_smem = 0;
@@ -712,7 +712,7 @@ using TcKernel = void (*)(const LadderTile *, const int32_t *, const __nv_bfloat
                          const __nv_bfloat16 *, int64_t, const __nv_bfloat16 *, int64_t,
                          const __nv_bfloat16 *, int64_t, const int32_t *, const int32_t *,
                          double *, double *, const Control *, int32_t *, const ChanInfo *,
-                         const VGenRow *, const VGenCol *, const double *);
+                         const VGenRow *, const uint32_t *, const double *);
 TcKernel tc_kernel_of(int nt, bool gen) {
   if (nt == 2) return gen ? pp_ladder_tc_kernel<2, true> : pp_ladder_tc_kernel<2, false>;
   return gen ? pp_ladder_tc_kernel<3, true> : pp_ladder_tc_kernel<3, false>;
@@ -1024,41 +1024,38 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   h->n_tmt = tmt;
 
   // Tensor-core ladder with V generated in the kernel (electron gas, on-the-fly V, momenta
-  // |n_i| <= 6 so that q^2 fits the kTcGenTab table): per packed row u (rowmap order) the
-  // momenta of a and b and the spin key, per K index w (kcol order) the momentum of c and the
-  // keys of (c, d) and (d, c); the direct term by q^2.
+  // |n_i| <= 6 so that q^2 <= 432): per packed row u (rowmap order) the codes of a and b, per K
+  // index w (kcol order) the code of c (momentum bytes biased by 64, spin in byte 3), and the
+  // direct term by q^2.
   std::vector<VGenRow> vg_rows;
-  std::vector<VGenCol> vg_cols;
+  std::vector<uint32_t> vg_cols;
   std::vector<double> vg_tab;
   if (on_the_fly && h->nt && model_ok && M->kind == CCDGPU_MODEL_ELECTRON_GAS) {
     int nmax = 0;
     for (uint64_t o = 0; o < nsp; o++)
       for (int i = 0; i < 3; i++) nmax = std::max(nmax, std::abs(M->qn[o * M->qn_stride + i]));
-    if (3 * (2 * nmax) * (2 * nmax) < kTcGenTab) {
+    if (nmax <= 6) {
       h->tc_gen = true;
-      auto mom = [&](int o) {
+      auto code = [&](int o) {
         const int32_t *q = M->qn + (int64_t)o * M->qn_stride;
-        return (uint32_t)(q[0] + 64) | ((uint32_t)(q[1] + 64) << 8) | ((uint32_t)(q[2] + 64) << 16);
+        return (uint32_t)(q[0] + 64) | ((uint32_t)(q[1] + 64) << 8) |
+               ((uint32_t)(q[2] + 64) << 16) | ((uint32_t)(q[3] > 0 ? kVGenSpin : 0) << 24);
       };
-      auto up = [&](int o) { return M->qn[(int64_t)o * M->qn_stride + 3] > 0 ? 1u : 0u; };
       vg_rows.resize(rowmap.size());
       vg_cols.resize(kcol.size());
       for (const ChanInfo &a : chans) {
         for (int u = 0; u < a.pr; u++) {
           const int2 ab = pp_pairs[a.pp_off + rowmap[a.row_off + u]];
-          vg_rows[a.row_off + u] = VGenRow{mom(ab.x), mom(ab.y), 2 * up(ab.x) + up(ab.y), 0u};
+          vg_rows[a.row_off + u] = VGenRow{code(ab.x), code(ab.y)};
         }
-        for (int w = 0; w < a.pk; w++) {
-          const int2 cd = pp_pairs[a.pp_off + kcol[a.pk_off + w]];
-          vg_cols[a.pk_off + w] =
-              VGenCol{mom(cd.x), (2 * up(cd.x) + up(cd.y)) | ((2 * up(cd.y) + up(cd.x)) << 8)};
-        }
+        for (int w = 0; w < a.pk; w++)
+          vg_cols[a.pk_off + w] = code(pp_pairs[a.pp_off + kcol[a.pk_off + w]].x);
       }
       // w(q^2) = e^2 / L^3 * 4 pi / (2 pi / L)^2 q^2, zero for q = 0 (ElectronGasSPBasis.cpp:
       // 453-466 as a function of q^2).
       const double L = M->params[0], e_sq = M->params[1];
       vg_tab.assign(kTcGenTab, 0.0);
-      for (int q2 = 1; q2 < kTcGenTab; q2++) {
+      for (int q2 = 1; q2 <= 3 * 12 * 12; q2++) {  // beyond: spins differ, zero
         const double rel = (2 * M_PI / L) * (2 * M_PI / L) * q2;
         vg_tab[q2] = e_sq / (L * L * L) * 4 * M_PI / rel;
       }
@@ -1486,7 +1483,7 @@ int launch_pp_ladder_tc(ccdgpu_handle *h, cudaStream_t st) {
                 (const __nv_bfloat16 *)h->xt_tc, h->n_xttc, (const int32_t *)h->rowmap,
                 (const int32_t *)h->mirror, h->dmat, h->tc_part, (const Control *)h->ctl, h->err,
                 (const ChanInfo *)h->chans, (const VGenRow *)h->vg_rows,
-                (const VGenCol *)h->vg_cols, (const double *)h->vg_tab));
+                (const uint32_t *)h->vg_cols, (const double *)h->vg_tab));
   if (h->n_red_tc) {
     CK(launch_pdl(ladder_reduce_kernel, h->n_red_tc, 256, 0, st, (const RedItem *)h->red_tc,
                   (const LadderTile *)h->tc_tiles, (const int32_t *)h->rowmap,

@@ -121,39 +121,42 @@ def test_normal_order_formula_reproduces_reference(name):
 
 
 def _vgen_codes(qn, orb):
-    """Momentum of orbital(s) as three bytes biased by 64 (the ladder's VGenRow / VGenCol)."""
+    """An orbital's code in the ladder's generator: momentum bytes biased by 64, 21 in byte 3
+    for spin up."""
     q = qn[orb]
-    return (q[..., 0] + 64) | ((q[..., 1] + 64) << 8) | ((q[..., 2] + 64) << 16)
+    return ((q[..., 0] + 64) | ((q[..., 1] + 64) << 8) | ((q[..., 2] + 64) << 16) |
+            (np.where(q[..., 3] > 0, 21, 0) << 24)).astype(np.int64)
 
 
-def _absdiff_dp4a(x, y):
-    """q^2 from two biased codes: per-byte |x - y| (vabsdiffu4), then the dot of the bytes with
-    themselves (dp4a)."""
+def _q2_index(x, y):
+    """(x - y + 0x80808080) ^ 0x80808080 as four signed bytes, dotted with itself (dp4a)."""
+    d = ((x - y + 0x80808080) & 0xFFFFFFFF) ^ 0x80808080
     out = np.zeros(np.broadcast(x, y).shape, dtype=np.int64)
     for sh in (0, 8, 16, 24):
-        d = np.abs(((x >> sh) & 0xFF) - ((y >> sh) & 0xFF))
-        out += d * d
+        b = (d >> sh) & 0xFF
+        b = np.where(b >= 128, b - 256, b)
+        out += b * b
     return out
 
 
 @pytest.mark.parametrize("name", ["eg14_s19", "eg14_r2"])
 def test_ladder_v_generator_codes_reproduce_reference_v(name):
     """The electron-gas V generator inside the tensor-core ladder (pp_ladder_tc_kernel with
-    GEN): V[ab,cd] = [key_ab = key_cd] w(q1^2) - [key_ab = key_dc] w(q2^2), q1 = n_a - n_c,
-    q2 = n_c - n_b from biased byte codes, w an FP32 table by q^2.  Restated in numpy over every
-    packed row a <= b and K column c < d of every channel, against the reference's V_pppp
-    blocks (FP32 accuracy: the ladder splits the element into bf16 terms afterwards)."""
+    GEN): V[ab,cd] = w(idx(n_a, n_c)) - w(idx(n_b, n_c)), where the index is q^2 for equal spins
+    and q^2 + 441 (a zero entry) otherwise, from codes with the spin in byte 3 and a table w by
+    index.  Restated in numpy over every packed row a <= b and K column c < d of every channel,
+    against the reference's V_pppp blocks (FP32 table, as the 2-term split uses)."""
     g = golden(name)
     with system_for(g) as s:
         qn = s.array("qn").reshape(s.n_sp, -1).astype(np.int64)
         m = s.problem.contents.model.contents
         L, e_sq = m.params[0], m.params[1]
         assert np.abs(qn[:, :3]).max() <= 6
-        q2 = np.arange(512, dtype=np.float64)
+        q2 = np.arange(3 * 144 + 441 + 1, dtype=np.float64)
         with np.errstate(divide="ignore"):
-            tab = np.where(q2 > 0, e_sq / L ** 3 * 4 * np.pi / ((2 * np.pi / L) ** 2 * q2), 0.0)
+            tab = np.where((q2 > 0) & (q2 <= 432),
+                           e_sq / L ** 3 * 4 * np.pi / ((2 * np.pi / L) ** 2 * q2), 0.0)
         tab = tab.astype(np.float32)
-        up = (qn[:, 3] > 0).astype(np.int64)
         d = s.chan_dims().astype(np.int64)
         pp = s.array("pp_map").reshape(-1, 2).astype(np.int64)
         vp = s.array("v_pppp")
@@ -169,15 +172,12 @@ def test_ladder_v_generator_codes_reproduce_reference_v(name):
             cols = np.nonzero(P[:, 0] < P[:, 1])[0]
             if not len(rows) or not len(cols):
                 continue
-            a, b = P[rows, 0][:, None], P[rows, 1][:, None]
-            cc, dd = P[cols, 0][None, :], P[cols, 1][None, :]
-            na, nb, nc = _vgen_codes(qn, a), _vgen_codes(qn, b), _vgen_codes(qn, cc)
-            q1, q2v = _absdiff_dp4a(na, nc), _absdiff_dp4a(nb, nc)
-            assert q1.max() < 512 and q2v.max() < 512
-            key = 2 * up[a] + up[b]
-            kcd, kdc = 2 * up[cc] + up[dd], 2 * up[dd] + up[cc]
-            v = (np.where(key == kcd, tab[q1], np.float32(0)) -
-                 np.where(key == kdc, tab[q2v], np.float32(0))).astype(np.float64)
+            na = _vgen_codes(qn, P[rows, 0][:, None])
+            nb = _vgen_codes(qn, P[rows, 1][:, None])
+            nc = _vgen_codes(qn, P[cols, 0][None, :])
+            i1, i2 = _q2_index(na, nc), _q2_index(nb, nc)
+            assert i1.max() < len(tab) and i2.max() < len(tab)
+            v = (tab[i1] - tab[i2]).astype(np.float64)
             want = ref[np.ix_(rows, cols)]
             scale = max(float(np.abs(want).max()), 1e-300)
             assert np.max(np.abs(v - want)) <= 2e-7 * scale, c
