@@ -680,15 +680,10 @@ hh_reduce_kernel(const HHRed *__restrict__ items, const ChanInfo *__restrict__ c
 // layout: fused path (inv != null) scatters R into pphh order, out[inv[p]] = R[p] (inv =
 // inverse of the ai_jb table), so the assembly reads R_ai,jb / R_aj,ib / R_bi,ja / R_bj,ia from
 // the channel's own block; table path (inv == null) writes t2Diff_phhp, out[p] = R[p].
-// Channels with ph', hp' <= kRingSmall run one per warp; larger ones on resident CTAs that loop
-// over their channels with cp.async double buffering (the next channel's operands load while
-// the current one computes), in two classes (<= kRingMid and above) with their own shared
-// memory sizes.
+// Channels with ph', hp' <= kRingSmall run one per warp; larger ones one per CTA, grouped by
+// padded size (ring16_kernel).
 // ------------------------------------------------------------------------------------------
-constexpr int kRingThreads = 256;
-__host__ __device__ constexpr int kRingThreadsOf(int nc) { return nc <= 2 ? 256 : 512; }
 constexpr int kRingSmall = 16;
-constexpr int kRingMid = 32;
 
 // C (M8*8 x N8*8) = A B, K4*4 deep, on 8 x 8 tiles: warps warp, warp + nwarps, ... take items of
 // one 8-row tile by NC column tiles (the A fragment is reused NC times).  A[m][k] =
@@ -724,15 +719,7 @@ __device__ __forceinline__ void warp_mma_gemm(const double *A, int ars, int aks,
   }
 }
 
-// Shared-memory stage of one channel: ph' and hp' padded to multiples of 8 (P, H) with zeros,
-// row stride ld = H + 4 (ld = 4 mod 8 spreads the 4 k-rows of a fragment load over all banks):
-// T' [P][ld], Vt [P][ld], Y [H][ld] (V_hphp on arrival), then the ph' x hp' scatter indices
-// (int32, fused path).
 __host__ __device__ inline int ring_pad8(int n) { return (n + 7) & ~7; }
-__host__ __device__ inline int ring_stage_doubles(int ph, int hp) {
-  const int P = ring_pad8(ph), H = ring_pad8(hp), ld = H + 4;
-  return even_up((2 * P + H) * ld + (ph * hp + 1) / 2);  // 16-byte steps
-}
 
 // Channels with ph', hp' <= kRingSmall, one per warp (kRingSmallWarps per CTA), the same two
 // products on the FP64 MMA: the warp's stage is padded to P, H in {8, 16} with zeros and a row
@@ -786,91 +773,100 @@ ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restr
   });
 }
 
-// Y = V_hphp + 0.5 V_hpph T' (H x H, K = P), then R = T' Y (P x H, K = H) on the FP64 MMA;
-// R is stored (scattered through the inverse ai_jb table on the fused path) for r < ph', c < hp'.
-template <int NC, int THREADS>
-__device__ __forceinline__ void ring_compute(const ModInfo &m, double *st,
-                                             const int32_t *__restrict__ inv,
-                                             double *__restrict__ out) {
-  const int ph = m.ph, hp = m.hp, P = ring_pad8(ph), H = ring_pad8(hp), ld = H + 4;
-  double *Ts = st, *Vt = Ts + P * ld, *Ys = Vt + P * ld;
-  const int32_t *Is = reinterpret_cast<const int32_t *>(Ys + H * ld);
-  const int warp = threadIdx.x >> 5;
-  constexpr int kWarps = THREADS / 32;
-  // A[i][k] = V_hpph[i][k] = Vt[k][i].  Each Y element is read and written by its owner lane.
-  warp_mma_gemm<NC>(Vt, 1, ld, Ts, ld, H / 8, H / 8, P / 4, warp, kWarps,
-                    [&](int r, int c, double v) { Ys[r * ld + c] = 0.5 * v + Ys[r * ld + c]; });
-  __syncthreads();
-  warp_mma_gemm<NC>(Ts, ld, 1, Ys, ld, P / 8, H / 8, H / 4, warp, kWarps,
-                    [&](int r, int c, double v) {
-                      if (r < ph && c < hp) {
-                        const int p = r * hp + c;
-                        out[inv ? (int64_t)Is[p] : m.m_off + p] = v;
-                      }
-                    });
+// Channels with ph', hp' > kRingSmall: one CTA per channel, the two products on the FP64
+// m16n8k16 MMA (4 k-steps for a 64-wide channel instead of 14 with m8n8k4, so a warp's
+// accumulator chains are short).  The channel is padded to PAD (a multiple of 16) with zeros
+// in shared memory: T' [PAD][ld], Vt [PAD][ld], Y [PAD][ld] (V_hphp on arrival), ld = PAD + 4
+// (4 mod 16 doubles: conflict-free fragment loads), all loaded with cp.async.  Warp w takes
+// items of one 16-row tile by NC 8-column tiles.  Channels are grouped by PAD (32, 48, 64, 80),
+// one launch per group, so a CTA's shared memory fits its channel and several CTAs share an SM.
+constexpr int kRing16NC = 4;
+__host__ __device__ constexpr int ring16_warps(int pad) {
+  return (pad / 16) * ((pad / 8 + kRing16NC - 1) / kRing16NC);
 }
-
-// Resident CTAs: CTA b handles channels b, b + gridDim.x, ...  stage = doubles per buffer;
-// nbuf = 2 (prefetch the next channel) or 1 (largest channels, when two stages do not fit).
-// NC = 2: channels up to kRingMid (256 threads, 3 CTAs per SM); NC = 4: the rest (up to
-// kTcMaxNB; 512 threads, one CTA per SM, so that the 8 x 32 items of a channel run at once).
-template <int NC, int THREADS = kRingThreadsOf(NC)>
-__global__ void __launch_bounds__(THREADS, NC <= 2 ? 3 : 1)
-ring_kernel(const ModInfo *__restrict__ mods, int n, const double *__restrict__ v_hpph,
-            const double *__restrict__ v_hphp, const double *__restrict__ t_phhp,
-            const int32_t *__restrict__ inv, double *__restrict__ out, int stage, int nbuf,
-            const Control *ctl, int gate) {
-  if (skip_iteration(ctl, gate, NC <= 2 ? kTrRingMid : kTrRingLarge)) return;
-  extern __shared__ __align__(16) double rs[];
-  const int tid = threadIdx.x;
-  // Operands of channel ci into stage st (cp.async), pad cells zeroed with plain stores; a
-  // warp per row, lanes over the columns.
-  const int warp = tid >> 5, lane = tid & 31;
-  auto issue = [&](int ci, double *st) {
-    const ModInfo m = mods[ci];
-    const int ph = m.ph, hp = m.hp, P = ring_pad8(ph), H = ring_pad8(hp), ld = H + 4;
-    double *Ts = st, *Vt = Ts + P * ld, *Ys = Vt + P * ld;
-    int32_t *Is = reinterpret_cast<int32_t *>(Ys + H * ld);
-    for (int r = warp; r < P; r += THREADS / 32) {
-      const int64_t src = m.m_off + (int64_t)r * hp;
-      for (int c = lane; c < H; c += 32) {
-        if (r < ph && c < hp) {
-          cp_async8(Ts + r * ld + c, t_phhp + src + c);
-          cp_async8(Vt + r * ld + c, v_hpph + src + c);
-          if (inv) cp_async4(Is + r * hp + c, inv + src + c);
-        } else {
-          Ts[r * ld + c] = 0.0;
-          Vt[r * ld + c] = 0.0;
-        }
+__host__ __device__ constexpr size_t ring16_smem(int pad) {
+  return (size_t)3 * pad * (pad + 4) * sizeof(double);
+}
+template <int PAD, int MODE, class Epi>
+__device__ __forceinline__ void ring16_gemm(const double *As, const double *Bs, int warp,
+                                            const Epi &epi) {
+  // MODE 0: A[m][k] = As[k][m] (k-major); MODE 1: A[m][k] = As[m][k].  B[k][n] = Bs[k][n].
+  constexpr int ld = PAD + 4, N8 = PAD / 8, NCH = (N8 + kRing16NC - 1) / kRing16NC;
+  constexpr int ITEMS = (PAD / 16) * NCH;
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  for (int it = warp; it < ITEMS; it += ring16_warps(PAD)) {
+    const int mt = it / NCH, n0 = (it - mt * NCH) * kRing16NC;
+    double acc[kRing16NC][4];
+#pragma unroll
+    for (int n = 0; n < kRing16NC; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.0;
+#pragma unroll
+    for (int k16 = 0; k16 < PAD / 16; ++k16) {
+      double a[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int m = 16 * mt + g + 8 * (i % 2), k = 16 * k16 + t + 4 * (i / 2);
+        a[i] = MODE == 0 ? As[k * ld + m] : As[m * ld + k];
+      }
+#pragma unroll
+      for (int n = 0; n < kRing16NC; ++n) {
+        if (n0 + n >= N8) break;
+        double b[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) b[q] = Bs[(16 * k16 + t + 4 * q) * ld + 8 * (n0 + n) + g];
+        dmma_16816(acc[n], a, b);
       }
     }
-    for (int r = warp; r < H; r += THREADS / 32) {
-      const int64_t src = m.y_off + (int64_t)r * hp;
-      for (int c = lane; c < H; c += 32) {
-        if (r < hp && c < hp) cp_async8(Ys + r * ld + c, v_hphp + src + c);
-        else Ys[r * ld + c] = 0.0;
-      }
-    }
-  };
-  int ci = blockIdx.x;
-  if (ci < n) issue(ci, rs);
-  cp_async_commit();
-  for (int k = 0; ci < n; ++k, ci += gridDim.x) {
-    double *st = rs + (nbuf == 2 ? (k & 1) * stage : 0);
-    const int nxt = ci + gridDim.x;
-    if (nbuf == 2 && nxt < n) issue(nxt, rs + ((k + 1) & 1) * stage);
-    cp_async_commit();
-    if (nbuf == 2) cp_async_wait<1>();
-    else cp_async_wait<0>();
-    __syncthreads();
-    ring_compute<NC, THREADS>(mods[ci], st, inv, out);
-    __syncthreads();
-    if (nbuf == 1 && nxt < n) {
-      issue(nxt, rs);
-      cp_async_commit();
+#pragma unroll
+    for (int n = 0; n < kRing16NC; ++n) {
+      if (n0 + n >= N8) break;
+      const int r = 16 * mt + g, c = 8 * (n0 + n) + 2 * t;
+      epi(r, c, acc[n][0]);
+      epi(r, c + 1, acc[n][1]);
+      epi(r + 8, c, acc[n][2]);
+      epi(r + 8, c + 1, acc[n][3]);
     }
   }
+}
+template <int PAD>
+__global__ void __launch_bounds__(32 * ring16_warps(PAD))
+ring16_kernel(const ModInfo *__restrict__ mods, const double *__restrict__ v_hpph,
+              const double *__restrict__ v_hphp, const double *__restrict__ t_phhp,
+              const int32_t *__restrict__ inv, double *__restrict__ out, const Control *ctl,
+              int gate) {
+  if (skip_iteration(ctl, gate, PAD <= 32 ? kTrRingMid : kTrRingLarge)) return;
+  extern __shared__ __align__(16) double r16[];
+  constexpr int ld = PAD + 4, NT = 32 * ring16_warps(PAD);
+  double *Ts = r16, *Vs = r16 + PAD * ld, *Ys = r16 + 2 * PAD * ld;
+  const ModInfo m = mods[blockIdx.x];
+  const int ph = m.ph, hp = m.hp;
+  for (int e = threadIdx.x; e < PAD * PAD; e += NT) {
+    const int r = e / PAD, c = e - r * PAD;
+    if (r < ph && c < hp) {
+      const int64_t src = m.m_off + (int64_t)r * hp + c;
+      cp_async8(Ts + r * ld + c, t_phhp + src);
+      cp_async8(Vs + r * ld + c, v_hpph + src);
+    } else {
+      Ts[r * ld + c] = 0.0;
+      Vs[r * ld + c] = 0.0;
+    }
+    if (r < hp && c < hp) cp_async8(Ys + r * ld + c, v_hphp + m.y_off + (int64_t)r * hp + c);
+    else Ys[r * ld + c] = 0.0;
+  }
+  cp_async_commit();
   cp_async_wait<0>();
+  __syncthreads();
+  const int warp = threadIdx.x >> 5;
+  // Y = V_hphp + 0.5 V_hpph T' with V_hpph[i][k] = Vt[k][i]; each Y element has one owner lane.
+  ring16_gemm<PAD, 0>(Vs, Ts, warp,
+                      [&](int r, int c, double v) { Ys[r * ld + c] = 0.5 * v + Ys[r * ld + c]; });
+  __syncthreads();
+  // R = T' Y, stored for r < ph', c < hp' (through the inverse ai_jb table on the fused path).
+  ring16_gemm<PAD, 1>(Ts, Ys, warp, [&](int r, int c, double v) {
+    if (r < ph && c < hp) {
+      const int64_t p = m.m_off + (int64_t)r * hp + c;
+      out[inv ? (int64_t)__ldg(inv + p) : p] = v;
+    }
+  });
 }
 
 // Deterministic block reduction (fixed tree) of one double; result valid in thread 0.

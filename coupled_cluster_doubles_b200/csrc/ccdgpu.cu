@@ -56,14 +56,13 @@ struct ccdgpu_handle {
   int n_asm_blocks = 0;  // fused assembly CTAs (persistent, striding over quad_items)
   int n_cls[3] = {0, 0, 0};  // pp-ladder tiles per column class (thin, mid, wide), in that order
   size_t ladder_smem_thin = 0;
-  size_t ladder_smem = 0, ring_smem = 0, ring_smem_mid = 0, hh_smem = 0;
-  int ring_stage_mid = 0, ring_stage_large = 0, ring_nbuf_large = 2;
-  int ring_grid_mid = 0, ring_grid_large = 0;
+  size_t ladder_smem = 0, hh_smem = 0;
+  int n_mod_pad[4] = {0, 0, 0, 0};  // ring channels by padded size 32, 48, 64, 80 (after small)
   bool have_3body = false;
   std::vector<DevBuf> allocs;
 
   ChanInfo *chans = nullptr;
-  ModInfo *mods = nullptr;        // small (n_mod_small), mid (n_mod_mid), then large channels
+  ModInfo *mods = nullptr;        // small (n_mod_small), then by padded size 32 .. 80
   LadderTile *tiles = nullptr;
   HHTile *hh_tiles = nullptr;
   HHRed *hh_red = nullptr;
@@ -869,11 +868,11 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   h->n_list = list_off[nsp];
   for (uint64_t w = 0; w < nsp; w++) std::copy(seg[w].begin(), seg[w].end(), list.begin() + list_off[w]);
 
-  // Modified channels: small ones (one warp each) first, then mid and large ones.
-  std::vector<ModInfo> mods, mods_mid, mods_big;
+  // Modified channels: small ones (one warp each) first, then one group per padded size
+  // (32, 48, 64, 80; one CTA per channel).
+  std::vector<ModInfo> mods, mods_pad[4];
   std::vector<int2> mod_dims(nch);
   int64_t y_tot = 0;
-  size_t ring_smem = 0;
   std::vector<const double *> src_hpph, src_hphp;
   std::vector<int64_t> cnt_hpph, cnt_hphp;
   std::vector<ModGen> mod_gen;        // generated V: modified channels in channel order
@@ -904,34 +903,22 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
       src_hphp.push_back(P->v_hphp_mod[c]); cnt_hphp.push_back(hp * hp);
     }
     y_tot += hp * hp;
-    const int stage = ring_stage_doubles((int)ph, (int)hp);
-    if (ph <= kRingSmall && hp <= kRingSmall) {
-      mods.push_back(m);
-    } else if (ph <= kRingMid && hp <= kRingMid) {
-      h->ring_stage_mid = std::max(h->ring_stage_mid, stage);
-      mods_mid.push_back(m);
-    } else {
-      h->ring_stage_large = std::max(h->ring_stage_large, stage);
-      mods_big.push_back(m);
-    }
+    const int64_t w = std::max(ph, hp);
+    if (w <= kRingSmall) mods.push_back(m);
+    else mods_pad[w <= 32 ? 0 : w <= 48 ? 1 : w <= 64 ? 2 : 3].push_back(m);
   }
-  // Resident ring CTAs stride over their class: largest channels first for balance.
+  // Largest channels first within a group, so that the short ones fill in behind them.
   auto by_work = [](const ModInfo &x, const ModInfo &y) {
     return (int64_t)x.ph * x.hp * x.hp > (int64_t)y.ph * y.hp * y.hp;
   };
-  std::stable_sort(mods_mid.begin(), mods_mid.end(), by_work);
-  std::stable_sort(mods_big.begin(), mods_big.end(), by_work);
   h->n_mod_small = (int)mods.size();
-  h->n_mod_mid = (int)mods_mid.size();
-  h->ring_smem_mid = (size_t)2 * h->ring_stage_mid * 8;
-  h->ring_nbuf_large = (size_t)2 * h->ring_stage_large * 8 <= 200 * 1024 ? 2 : 1;
-  ring_smem = (size_t)h->ring_nbuf_large * h->ring_stage_large * 8;
-  h->ring_grid_mid = (int)std::min<int64_t>(h->n_mod_mid, 3 * 148);
-  h->ring_grid_large = (int)std::min<int64_t>((int64_t)mods_big.size(), 148);
-  mods.insert(mods.end(), mods_mid.begin(), mods_mid.end());
-  mods.insert(mods.end(), mods_big.begin(), mods_big.end());
+  for (int k = 0; k < 4; k++) {
+    std::stable_sort(mods_pad[k].begin(), mods_pad[k].end(), by_work);
+    h->n_mod_pad[k] = (int)mods_pad[k].size();
+    mods.insert(mods.end(), mods_pad[k].begin(), mods_pad[k].end());
+  }
+  h->n_mod_mid = h->n_mod_pad[0];
   h->n_mod = (int)mods.size();
-  h->ring_smem = ring_smem;
   h->host_mods = mods;
 
   std::vector<int64_t> o_h(np + 1, 0), o_p(h->npart + 1, 0);
@@ -1401,12 +1388,17 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   // (the same value for every handle), so that handles of different channel sizes coexist.
   int smem_optin = 0;
   CK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->opt.device));
-  if (h->ring_smem_mid > (size_t)smem_optin || h->ring_smem > (size_t)smem_optin)
-    return CCDGPU_ERR_UNSUPPORTED;
+  if (ring16_smem(80) > (size_t)smem_optin) return CCDGPU_ERR_UNSUPPORTED;
   CK(cudaFuncSetAttribute(hh_slice_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)hh_slice_smem(8 * kMaxCG)));
-  CK(cudaFuncSetAttribute(ring_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin));
-  CK(cudaFuncSetAttribute(ring_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin));
+  CK(cudaFuncSetAttribute(ring16_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)ring16_smem(32)));
+  CK(cudaFuncSetAttribute(ring16_kernel<48>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)ring16_smem(48)));
+  CK(cudaFuncSetAttribute(ring16_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)ring16_smem(64)));
+  CK(cudaFuncSetAttribute(ring16_kernel<80>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)ring16_smem(80)));
   ccdgpu_schedule sch{};
   sch.thin_split_mul = 1;
   sch.wide_split_mul = 3;
@@ -1556,20 +1548,25 @@ int launch_ring(ccdgpu_handle *h, cudaStream_t st, int gate, bool fused, int onl
     h->launches++;
     CK(cudaGetLastError());
   }
-  if (h->n_mod_mid && (only < 0 || only == 1)) {
-    ring_kernel<2><<<h->ring_grid_mid, kRingThreads, h->ring_smem_mid, st>>>(
-        h->mods + h->n_mod_small, h->n_mod_mid, h->v_hpph, h->v_hphp, h->old_phhp, inv, out,
-        h->ring_stage_mid, 2, h->ctl, gate);
-    h->launches++;
-    CK(cudaGetLastError());
-  }
-  const int nbig = h->n_mod - h->n_mod_small - h->n_mod_mid;
-  if (nbig && (only < 0 || only == 2)) {
-    ring_kernel<4><<<h->ring_grid_large, kRingThreadsOf(4), h->ring_smem, st>>>(
-        h->mods + h->n_mod_small + h->n_mod_mid, nbig, h->v_hpph, h->v_hphp, h->old_phhp, inv,
-        out, h->ring_stage_large, h->ring_nbuf_large, h->ctl, gate);
-    h->launches++;
-    CK(cudaGetLastError());
+  // Groups by padded size; only = 1 launches the 32 group, only = 2 the wider ones.
+  const ModInfo *mp = h->mods + h->n_mod_small;
+  for (int k = 0; k < 4; k++) {
+    const int n = h->n_mod_pad[k];
+    if (n && (only < 0 || only == (k == 0 ? 1 : 2))) {
+      switch (k) {
+        case 0: ring16_kernel<32><<<n, 32 * ring16_warps(32), ring16_smem(32), st>>>(
+                    mp, h->v_hpph, h->v_hphp, h->old_phhp, inv, out, h->ctl, gate); break;
+        case 1: ring16_kernel<48><<<n, 32 * ring16_warps(48), ring16_smem(48), st>>>(
+                    mp, h->v_hpph, h->v_hphp, h->old_phhp, inv, out, h->ctl, gate); break;
+        case 2: ring16_kernel<64><<<n, 32 * ring16_warps(64), ring16_smem(64), st>>>(
+                    mp, h->v_hpph, h->v_hphp, h->old_phhp, inv, out, h->ctl, gate); break;
+        default: ring16_kernel<80><<<n, 32 * ring16_warps(80), ring16_smem(80), st>>>(
+                    mp, h->v_hpph, h->v_hphp, h->old_phhp, inv, out, h->ctl, gate); break;
+      }
+      h->launches++;
+      CK(cudaGetLastError());
+    }
+    mp += n;
   }
   return CCDGPU_OK;
 }
@@ -2447,7 +2444,7 @@ int ccdgpu_kernel_profile(ccdgpu_handle *h, int32_t reps, double *ms, double *fl
   // ai_jb table, writes R.
   for (const ModInfo &m : h->host_mods) {
     const int k = (m.ph <= kRingSmall && m.hp <= kRingSmall) ? 0
-                  : (m.ph <= kRingMid && m.hp <= kRingMid) ? 1 : 2;
+                  : (m.ph <= 32 && m.hp <= 32) ? 1 : 2;
     flops[k] += 4.0 * m.ph * (double)m.hp * m.hp;
     bytes[k] += 28.0 * m.ph * m.hp + 8.0 * m.hp * m.hp;
   }
