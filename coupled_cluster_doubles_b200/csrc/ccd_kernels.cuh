@@ -571,14 +571,17 @@ hh_mma_kernel(const HHTile *__restrict__ tiles, int n, const ChanInfo *__restric
 
 // Channels with hh > 16: one CTA per K slice of kHHRowsL pp rows.  The slice's rows of V_pphh
 // and T (two contiguous ranges of rows * hh doubles) go to shared memory with cp.async, all in
-// flight at once, at a row stride of hh rounded up to 8, plus 4 (4 mod 8 doubles: conflict-free
-// fragment loads); rows up to the next multiple of 4 are zero.  Warp w computes P rows
-// [8c, 8c + 8) for c = w, w + 8, ... over every column tile (m8n8k4, K = the slice), so T is
-// read from HBM once per slice; the warps then form the slice's row dots r (lanes over the
-// columns, a fixed butterfly).  Partial P per slice as for hh_mma_kernel.
+// flight at once, at a row stride of hh rounded up to 16, plus 4 (4 mod 16 doubles:
+// conflict-free fragment loads); rows up to the next multiple of 16 and columns up to the
+// padded width are zero.  P = V^T T runs on the FP64 m16n8k16 MMA: warp w takes items of one
+// 16-row tile of P by kHHNC 8-column tiles, at most four k-steps per slice, so T is read from
+// HBM once per slice and the accumulator chains are short; the warps then form the slice's
+// row dots r (lanes over the columns, a fixed butterfly).  Partial P per slice as for
+// hh_mma_kernel.
 constexpr int kHHRowsL = 64;
 constexpr int kHHSliceThreads = 256;
-__host__ __device__ inline int hh_slice_ld(int hh) { return ((hh + 7) & ~7) + 4; }
+constexpr int kHHNC = 4;
+__host__ __device__ inline int hh_slice_ld(int hh) { return ((hh + 15) & ~15) + 4; }
 __host__ __device__ inline size_t hh_slice_smem(int hh) {
   return (size_t)2 * kHHRowsL * hh_slice_ld(hh) * sizeof(double);
 }
@@ -592,8 +595,8 @@ hh_slice_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ c
   const HHTile tt = tiles[blockIdx.x];
   const ChanInfo &ch = chans[tt.ch];
   const double *t_old = ctl->parity ? tbuf1 : tbuf0;
-  const int hh = ch.hh, ld = hh_slice_ld(hh), rows = tt.rows, rows4 = (rows + 3) & ~3;
-  const int h8 = (hh + 7) >> 3;
+  const int hh = ch.hh, ld = hh_slice_ld(hh), hh16 = ld - 4;
+  const int rows = tt.rows, rows16 = (rows + 15) & ~15;
   double *Vs = hs_smem, *Ts = hs_smem + kHHRowsL * ld;
   const int64_t base = ch.t_off + (int64_t)tt.k0 * hh;
   const double *vb = v_pphh + base, *tb = t_old + base;
@@ -603,7 +606,13 @@ hh_slice_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ c
     cp_async8(Ts + k * ld + c, tb + e);
   }
   cp_async_commit();
-  for (int e = threadIdx.x; e < (rows4 - rows) * ld; e += kHHSliceThreads) {
+  const int padc = hh16 - hh;  // zero columns [hh, hh16) of rows < rows, then rows >= rows
+  for (int e = threadIdx.x; e < rows * padc; e += kHHSliceThreads) {
+    const int k = e / padc, c = hh + (e - k * padc);
+    Vs[k * ld + c] = 0.0;
+    Ts[k * ld + c] = 0.0;
+  }
+  for (int e = threadIdx.x; e < (rows16 - rows) * ld; e += kHHSliceThreads) {
     Vs[rows * ld + e] = 0.0;
     Ts[rows * ld + e] = 0.0;
   }
@@ -611,25 +620,37 @@ hh_slice_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ c
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   double *pb = part + ch.part_off + (int64_t)tt.idx * hh * hh;
-  for (int mc = warp; mc < h8; mc += kHHSliceThreads / 32) {
-    double acc[kMaxCG][2];
+  const int n8 = (hh + 7) >> 3, nch = (n8 + kHHNC - 1) / kHHNC, items = (hh16 >> 4) * nch;
+  for (int it = warp; it < items; it += kHHSliceThreads / 32) {
+    const int mt = it / nch, n0 = (it - mt * nch) * kHHNC;
+    double acc[kHHNC][4];
 #pragma unroll
-    for (int c = 0; c < kMaxCG; ++c) acc[c][0] = acc[c][1] = 0.0;
-    const double *ap = Vs + t * ld + 8 * mc + g, *bp = Ts + t * ld + g;
-#pragma unroll 4
-    for (int k4 = 0; k4 < rows4 / 4; ++k4) {
-      const double a = ap[4 * k4 * ld];
+    for (int n = 0; n < kHHNC; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.0;
+    for (int k16 = 0; k16 < rows16 / 16; ++k16) {
+      double a[8];
 #pragma unroll
-      for (int c = 0; c < kMaxCG; ++c)
-        if (c < h8) dmma_884(acc[c], a, bp[4 * k4 * ld + 8 * c]);
+      for (int i = 0; i < 8; ++i)  // A[kl][k] = V[k][kl]
+        a[i] = Vs[(16 * k16 + t + 4 * (i / 2)) * ld + 16 * mt + g + 8 * (i % 2)];
+#pragma unroll
+      for (int n = 0; n < kHHNC; ++n) {
+        if (n0 + n >= n8) break;
+        double b[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) b[q] = Ts[(16 * k16 + t + 4 * q) * ld + 8 * (n0 + n) + g];
+        dmma_16816(acc[n], a, b);
+      }
     }
-    const int kl = 8 * mc + g;
 #pragma unroll
-    for (int c = 0; c < kMaxCG; ++c) {
-      const int ij = 8 * c + 2 * t;
-      if (c < h8 && kl < hh) {
-        if (ij < hh) pb[kl * hh + ij] = acc[c][0];
-        if (ij + 1 < hh) pb[kl * hh + ij + 1] = acc[c][1];
+    for (int n = 0; n < kHHNC; ++n) {
+      if (n0 + n >= n8) break;
+      const int ij = 8 * (n0 + n) + 2 * t;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int kl = 16 * mt + g + 8 * h;
+        if (kl < hh) {
+          if (ij < hh) pb[kl * hh + ij] = acc[n][2 * h];
+          if (ij + 1 < hh) pb[kl * hh + ij + 1] = acc[n][2 * h + 1];
+        }
       }
     }
   }
