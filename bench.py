@@ -308,9 +308,11 @@ def main():
     ap.add_argument("--path", default="fused", choices=["fused", "tables"])
     ap.add_argument("--precision", default="mixed", choices=list(PRECISIONS),
                     help="headline arm; the other precision is timed beside it")
-    ap.add_argument("--v-mode", default=None, choices=["stored", "on_the_fly"],
+    ap.add_argument("--v-mode", default=None, choices=["stored", "on_the_fly", "in_ladder"],
                     help="stored: V_pppp built on the host and uploaded; on_the_fly: generated "
-                         "on the device from the model (default: the workload's own setting)")
+                         "on the device from the model at create; in_ladder: as on_the_fly, and "
+                         "the electron gas's tensor-core ladder regenerates it every iteration "
+                         "(default: the workload's own setting)")
     ap.add_argument("--no-device-loop", action="store_true",
                     help="replay per-iteration graphs instead of the device solve loop (for "
                          "profilers, which cannot see kernels inside graph WHILE nodes)")
@@ -560,8 +562,10 @@ def main():
         if not args.no_cpu_baseline:
             cpu = _cpu_baseline(args.config)
         result = {"precision": PRECISIONS[head], "path": args.path,
-                  "v_pppp": ("generated on the device from the model" if v_mode == "on_the_fly"
-                             else "uploaded from the host"),
+                  "v_pppp": {"stored": "uploaded from the host",
+                             "on_the_fly": "generated on the device from the model at create",
+                             "in_ladder": "regenerated inside the tensor-core ladder every "
+                                          "iteration"}[v_mode],
                   "solve_loop": ("batched graph replay" if args.no_device_loop else
                                  "device (graph WHILE nodes)"),
                   "iterations_per_solve": t["iters_per_solve"],

@@ -361,7 +361,7 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
         rw[i] = r < tile.rows ? vg_rows[tile.row_off + (int64_t)tile.mt * kTcBM + r]
                               : VGenRow{kVGenZero, kVGenZero};
       }
-      // Column codes of a chunk; K padding (w >= pk) is flagged by code 0 and becomes 0.
+      // Column codes of a chunk; K padding (w >= pk) gets weight 0.
       uint32_t cn[8], ck[8];
       auto load_cols = [&](int c, uint32_t *n, uint32_t *k) {
         const int kc = tile.kc0 + c;
@@ -392,7 +392,7 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
             if (8 * rg >= tile.rows) continue;
             GT v[8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) v[j] = ck[j] ? vgen_elem<GT>(rw[i], cn[j], gtab) : GT(0);
+            for (int j = 0; j < 8; ++j) v[j] = vgen_elem<GT>(rw[i], cn[j], gtab) * (GT)ck[j];
             const uint32_t off =
                 (uint32_t)(rg * kTcGroup + (lane >> 2) * 8 + 2 * (lane & 3)) * 2;
 #pragma unroll

@@ -722,7 +722,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   h->nch = nch; h->nsp = nsp; h->np = np; h->npart = nsp - np;
   const ccdgpu_channel_dims *D = P->chan_dims, *MD = P->chan_mod_dims;
   // V_ON_THE_FLY: V_pppp is generated on the device from the model, P->v_pppp is not read.
-  const bool on_the_fly = h->opt.v_mode == CCDGPU_V_ON_THE_FLY;
+  const bool on_the_fly =
+      h->opt.v_mode == CCDGPU_V_ON_THE_FLY || h->opt.v_mode == CCDGPU_V_IN_LADDER;
   const ccdgpu_model *M = P->model;
   const bool model_ok = M && M->qn && M->kind >= CCDGPU_MODEL_PAIRING &&
                         M->kind <= CCDGPU_MODEL_ELECTRON_GAS &&
@@ -1017,7 +1018,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   std::vector<VGenRow> vg_rows;
   std::vector<uint32_t> vg_cols;
   std::vector<double> vg_tab;
-  if (on_the_fly && h->nt && model_ok && M->kind == CCDGPU_MODEL_ELECTRON_GAS) {
+  if (h->opt.v_mode == CCDGPU_V_IN_LADDER && h->nt && model_ok &&
+      M->kind == CCDGPU_MODEL_ELECTRON_GAS) {
     int nmax = 0;
     for (uint64_t o = 0; o < nsp; o++)
       for (int i = 0; i < 3; i++) nmax = std::max(nmax, std::abs(M->qn[o * M->qn_stride + i]));

@@ -20,7 +20,7 @@ from . import _native
 
 PREC = {"fp64": 0, "mixed": 1, "mixed_bf16": 1, "mixed_bf16x3": 2}
 PATH = {"fused": 0, "tables": 1}
-VMODE = {"stored": 0, "on_the_fly": 1}
+VMODE = {"stored": 0, "on_the_fly": 1, "in_ladder": 2}
 
 CHAIN_T2 = 0
 CHAIN_T2_OLD = 1

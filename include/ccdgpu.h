@@ -133,11 +133,13 @@ enum ccdgpu_precision {
 };
 enum ccdgpu_v_mode {
   CCDGPU_V_STORED = 0,         /* V_pppp uploaded from the host blocks */
-  CCDGPU_V_ON_THE_FLY = 1      /* V_pppp generated on the device from the model
-                                  (ccdgpu_problem.model) instead of uploaded: at create, into
-                                  the FP64 ladder tiles and bf16 images; electron gas with the
-                                  tensor-core ladder: regenerated inside the ladder kernel
-                                  every iteration and never stored */
+  CCDGPU_V_ON_THE_FLY = 1,     /* V_pppp generated on the device from the model
+                                  (ccdgpu_problem.model) instead of uploaded: once, at create,
+                                  into the FP64 ladder tiles and bf16 images */
+  CCDGPU_V_IN_LADDER = 2       /* as CCDGPU_V_ON_THE_FLY, and for the electron gas with a mixed
+                                  precision the tensor-core ladder regenerates its V operand
+                                  every iteration instead of reading bf16 images (less device
+                                  memory; slower than streaming the images on B200) */
 };
 enum ccdgpu_path {
   CCDGPU_PATH_FUSED = 0,       /* fused kernels: one-body terms from the ladder intermediates,

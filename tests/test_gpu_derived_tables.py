@@ -53,16 +53,14 @@ def test_derived_tables_mixed_precision_on_the_fly_v():
 def test_nothing_but_structure_from_the_host(name, precision):
     """No V block and no remap table from the host: ccdgpu_create generates every V block from
     the model (load.cpp:112-318 elements) and derives the tables.  Pairing and electron-gas
-    elements are bit-identical to the host's, so the FP64 solve is too; the Minnesota elements
-    use CUDA's exp/pow and may differ by an ulp, and the electron gas's mixed ladder generates
-    its V planes itself (exact to the precision of its bf16 split), so those solves are held to
-    the reference energy."""
+    elements are bit-identical to the host's, so the solve is too; the Minnesota elements use
+    CUDA's exp/pow and may differ by an ulp, so the PNM solve is held to the reference energy."""
     g = golden(name)
     with system_for(g) as s1, \
             getattr(System, g["kind"])(**g["params"], tables=False, v_blocks=False) as s2, \
             CCDSolver(s1, precision=precision) as a, \
             CCDSolver(s2, precision=precision, v_mode="on_the_fly") as b:
-        if g["kind"] == "inf_matter" or (g["kind"] == "electron_gas" and precision != "fp64"):
+        if g["kind"] == "inf_matter":
             rb = b.solve(tol=g["tol"], max_iters=100, mixing=0.5)
             ref = g["energies"][-1]
             rtol = 1e-10 if precision == "fp64" else 1e-6

@@ -54,7 +54,7 @@ def test_large_on_the_fly_fp64_matches_reference(name):
         _check_fp64(g, sol, res)
 
 
-@pytest.mark.parametrize("v_mode", ["stored", "on_the_fly"])
+@pytest.mark.parametrize("v_mode", ["stored", "on_the_fly", "in_ladder"])
 @pytest.mark.parametrize("name", LARGE)
 def test_large_mixed_matches_reference(name, v_mode):
     g = golden(name)

@@ -51,9 +51,9 @@ def test_tensor_core_ladder_matches_fp64(name, precision):
 @pytest.mark.parametrize("precision", ["mixed_bf16", "mixed_bf16x3"])
 @pytest.mark.parametrize("name", ["eg14_s19", "eg54_s19"])
 def test_generated_v_ladder_matches_fp64(name, precision):
-    """Electron gas with V generated on the device: the tensor-core ladder builds its V operand
-    planes itself (momentum/spin codes and a q^2 table, FP32 before the bf16 split) instead of
-    reading bf16 images; same tolerance against the FP64 ladder."""
+    """Electron gas with V regenerated inside the ladder (v_mode "in_ladder"): the tensor-core
+    ladder builds its V operand planes itself (momentum/spin codes and a q^2 table, exact to the
+    precision of the split) instead of reading bf16 images; checked against the FP64 ladder."""
     g = golden(name)
     with system_for(g) as s, system_for(g, load_v_pppp=False) as s_gen:
         with CCDSolver(s) as ref:
@@ -61,7 +61,7 @@ def test_generated_v_ladder_matches_fp64(name, precision):
                 ref.step(0.5)
             t2 = ref.t2()
         d64 = _ladder_after_one_step(s, "fp64", t2)
-        with CCDSolver(s_gen, precision=precision, v_mode="on_the_fly") as sol:
+        with CCDSolver(s_gen, precision=precision, v_mode="in_ladder") as sol:
             sol.set_t2(t2)
             sol.step(0.5)
             dmx = sol.chain(solver_mod.CHAIN_DIFF_PPHH)
