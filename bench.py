@@ -423,6 +423,17 @@ def main():
         prof[a] = sol.profile()
         sol.enable_profiling(False)
         work[a] = sol.work_per_iteration()
+    # Live schedule of one iteration inside the device solve loop: when the first and the last
+    # CTA of every kernel started (%globaltimer), relative to the earliest start.
+    trace = {}
+    for a in arms:
+        sol = solvers[a]
+        sol.reset()
+        sol.trace_arm(5)
+        sol.solve(tol=tol, max_iters=MAX_ITERS, mixing=MIXING)
+        trace[a] = {k: [round(f / 1e3, 2), round(l / 1e3, 2)] for k, (f, l) in
+                    sorted(sol.trace_read().items(), key=lambda x: x[1][0])}
+        sol.trace_arm(-1)
     ladder_cls = {a: solvers[a].ladder_profile(reps=5) for a in arms}
     other_cls = solvers[arms[0]].kernel_profile(reps=5)  # shared by both arms
     n_t2 = solvers[arms[0]].n_t2
@@ -533,6 +544,7 @@ def main():
                 "abs_de_per_particle_vs_reference": ta.get("abs_de_per_particle_vs_reference"),
                 "t2_max_abs_vs_reference": ta.get("t2_max_abs_vs_reference"),
                 "kernel_ms_per_iteration": per_it[a],
+                "trace_iteration5_us": trace[a],
                 "kernel_rooflines": roof[a],
                 "pp_ladder_tflops_algorithmic": work[a]["ladder_flops"] / (lms / 1000.0) / 1e12,
                 "gpu_launches": int(ta["launches"]),
