@@ -600,25 +600,23 @@ hh_slice_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ c
   double *Vs = hs_smem, *Ts = hs_smem + kHHRowsL * ld;
   const int64_t base = ch.t_off + (int64_t)tt.k0 * hh;
   const double *vb = v_pphh + base, *tb = t_old + base;
-  for (int e = threadIdx.x; e < rows * hh; e += kHHSliceThreads) {
-    const int k = e / hh, c = e - k * hh;
-    cp_async8(Vs + k * ld + c, vb + e);
-    cp_async8(Ts + k * ld + c, tb + e);
+  // A warp per row, lanes over the columns (no integer division); columns [hh, hh16) and rows
+  // [rows, rows16) are zero.
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  for (int k = warp; k < rows16; k += kHHSliceThreads / 32) {
+    for (int c = lane; c < hh16; c += 32) {
+      if (k < rows && c < hh) {
+        cp_async8(Vs + k * ld + c, vb + (int64_t)k * hh + c);
+        cp_async8(Ts + k * ld + c, tb + (int64_t)k * hh + c);
+      } else {
+        Vs[k * ld + c] = 0.0;
+        Ts[k * ld + c] = 0.0;
+      }
+    }
   }
   cp_async_commit();
-  const int padc = hh16 - hh;  // zero columns [hh, hh16) of rows < rows, then rows >= rows
-  for (int e = threadIdx.x; e < rows * padc; e += kHHSliceThreads) {
-    const int k = e / padc, c = hh + (e - k * padc);
-    Vs[k * ld + c] = 0.0;
-    Ts[k * ld + c] = 0.0;
-  }
-  for (int e = threadIdx.x; e < (rows16 - rows) * ld; e += kHHSliceThreads) {
-    Vs[rows * ld + e] = 0.0;
-    Ts[rows * ld + e] = 0.0;
-  }
   cp_async_wait<0>();
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   double *pb = part + ch.part_off + (int64_t)tt.idx * hh * hh;
   const int n8 = (hh + 7) >> 3, nch = (n8 + kHHNC - 1) / kHHNC, items = (hh16 >> 4) * nch;
   for (int it = warp; it < items; it += kHHSliceThreads / 32) {
@@ -755,6 +753,7 @@ ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restr
                   int gate) {
   if (skip_iteration(ctl, gate, kTrRingSmall)) return;
   __shared__ __align__(16) double buf[kRingSmallWarps][3 * kRingSmall * kRingSmallLd];
+  __shared__ int32_t ibuf[kRingSmallWarps][kRingSmall * kRingSmall];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int mi = blockIdx.x * kRingSmallWarps + w;
   if (mi >= n) return;  // whole warps: the MMAs below are warp-collective
@@ -779,6 +778,9 @@ ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restr
     if (r < hp && c < hp) cp_async8(Ys + r * ld + c, v_hphp + m.y_off + r * hp + c);
     else Ys[r * ld + c] = 0.0;
   }
+  int32_t *Is = ibuf[w];  // scatter destinations (fused path), staged with the operands
+  if (inv)
+    for (int p = lane; p < ph * hp; p += 32) cp_async4(Is + p, inv + m.m_off + p);
   cp_async_commit();
   cp_async_wait<0>();
   __syncwarp();
@@ -789,7 +791,7 @@ ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restr
   warp_mma_gemm<2>(Ts, ld, 1, Ys, ld, P / 8, H / 8, H / 4, 0, 1, [&](int r, int c, double v) {
     if (r < ph && c < hp) {
       const int p = r * hp + c;
-      out[inv ? (int64_t)inv[m.m_off + p] : m.m_off + p] = v;
+      out[inv ? (int64_t)Is[p] : m.m_off + p] = v;
     }
   });
 }
@@ -808,15 +810,25 @@ __host__ __device__ constexpr int ring16_warps(int pad) {
 __host__ __device__ constexpr size_t ring16_smem(int pad) {
   return (size_t)3 * pad * (pad + 4) * sizeof(double);
 }
-template <int PAD, int MODE, class Epi>
+// pre(r, c) is called for every output position of an item before its MMAs (it may start
+// loads that epi(r, c, v, slot) then uses: slot = n * 4 + the accumulator index).
+template <int PAD, int MODE, class Pre, class Epi>
 __device__ __forceinline__ void ring16_gemm(const double *As, const double *Bs, int warp,
-                                            const Epi &epi) {
+                                            const Pre &pre, const Epi &epi) {
   // MODE 0: A[m][k] = As[k][m] (k-major); MODE 1: A[m][k] = As[m][k].  B[k][n] = Bs[k][n].
   constexpr int ld = PAD + 4, N8 = PAD / 8, NCH = (N8 + kRing16NC - 1) / kRing16NC;
   constexpr int ITEMS = (PAD / 16) * NCH;
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   for (int it = warp; it < ITEMS; it += ring16_warps(PAD)) {
     const int mt = it / NCH, n0 = (it - mt * NCH) * kRing16NC;
+#pragma unroll
+    for (int n = 0; n < kRing16NC; ++n) {
+      const int r = 16 * mt + g, c = 8 * (n0 + n) + 2 * t;
+      pre(n * 4 + 0, r, c);
+      pre(n * 4 + 1, r, c + 1);
+      pre(n * 4 + 2, r + 8, c);
+      pre(n * 4 + 3, r + 8, c + 1);
+    }
     double acc[kRing16NC][4];
 #pragma unroll
     for (int n = 0; n < kRing16NC; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.0;
@@ -841,10 +853,10 @@ __device__ __forceinline__ void ring16_gemm(const double *As, const double *Bs, 
     for (int n = 0; n < kRing16NC; ++n) {
       if (n0 + n >= N8) break;
       const int r = 16 * mt + g, c = 8 * (n0 + n) + 2 * t;
-      epi(r, c, acc[n][0]);
-      epi(r, c + 1, acc[n][1]);
-      epi(r + 8, c, acc[n][2]);
-      epi(r + 8, c + 1, acc[n][3]);
+      epi(r, c, acc[n][0], n * 4 + 0);
+      epi(r, c + 1, acc[n][1], n * 4 + 1);
+      epi(r + 8, c, acc[n][2], n * 4 + 2);
+      epi(r + 8, c + 1, acc[n][3], n * 4 + 3);
     }
   }
 }
@@ -878,16 +890,22 @@ ring16_kernel(const ModInfo *__restrict__ mods, const double *__restrict__ v_hpp
   __syncthreads();
   const int warp = threadIdx.x >> 5;
   // Y = V_hphp + 0.5 V_hpph T' with V_hpph[i][k] = Vt[k][i]; each Y element has one owner lane.
-  ring16_gemm<PAD, 0>(Vs, Ts, warp,
-                      [&](int r, int c, double v) { Ys[r * ld + c] = 0.5 * v + Ys[r * ld + c]; });
+  ring16_gemm<PAD, 0>(
+      Vs, Ts, warp, [](int, int, int) {},
+      [&](int r, int c, double v, int) { Ys[r * ld + c] = 0.5 * v + Ys[r * ld + c]; });
   __syncthreads();
-  // R = T' Y, stored for r < ph', c < hp' (through the inverse ai_jb table on the fused path).
-  ring16_gemm<PAD, 1>(Ts, Ys, warp, [&](int r, int c, double v) {
-    if (r < ph && c < hp) {
-      const int64_t p = m.m_off + (int64_t)r * hp + c;
-      out[inv ? (int64_t)__ldg(inv + p) : p] = v;
-    }
-  });
+  // R = T' Y, stored for r < ph', c < hp' (through the inverse ai_jb table on the fused path);
+  // the destinations are loaded before the MMAs, so the stores do not wait on them.
+  int64_t dst[4 * kRing16NC];
+  ring16_gemm<PAD, 1>(
+      Ts, Ys, warp,
+      [&](int slot, int r, int c) {
+        const int64_t p = m.m_off + (int64_t)r * hp + c;
+        dst[slot] = (r < ph && c < hp) ? (inv ? (int64_t)__ldg(inv + p) : p) : -1;
+      },
+      [&](int, int, double v, int slot) {
+        if (dst[slot] >= 0) out[dst[slot]] = v;
+      });
 }
 
 // Deterministic block reduction (fixed tree) of one double; result valid in thread 0.
