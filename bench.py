@@ -424,15 +424,18 @@ def main():
         sol.enable_profiling(False)
         work[a] = sol.work_per_iteration()
     # Live schedule of one iteration inside the device solve loop: when the first and the last
-    # CTA of every kernel started (%globaltimer), relative to the earliest start.
+    # CTA of every kernel started and when the last one finished (%globaltimer, us), relative
+    # to the earliest start.
     trace = {}
     for a in arms:
         sol = solvers[a]
         sol.reset()
         sol.trace_arm(5)
         sol.solve(tol=tol, max_iters=MAX_ITERS, mixing=MIXING)
-        trace[a] = {k: [round(f / 1e3, 2), round(l / 1e3, 2)] for k, (f, l) in
-                    sorted(sol.trace_read().items(), key=lambda x: x[1][0])}
+        trace[a] = {k: [round(f / 1e3, 2), round(l / 1e3, 2),
+                        round(e / 1e3, 2) if e is not None else None]
+                    for k, (f, l, e) in sorted(sol.trace_read(with_end=True).items(),
+                                               key=lambda x: x[1][0])}
         sol.trace_arm(-1)
     ladder_cls = {a: solvers[a].ladder_profile(reps=5) for a in arms}
     other_cls = solvers[arms[0]].kernel_profile(reps=5)  # shared by both arms

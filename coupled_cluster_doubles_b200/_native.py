@@ -123,7 +123,7 @@ GPU_SYMBOLS = [
     "ccdgpu_trace_arm", "ccdgpu_trace_read", "ccdgpu_solve_batch", "ccdgpu_set_schedule",
     "ccdgpu_get_schedule", "ccdgpu_autotune", "ccdgpu_ladder_profile", "ccdgpu_kernel_profile",
     "ccdgpu_mbpt2", "ccdgpu_reference_energy", "ccdgpu_release_cached_memory",
-    "ccdgpu_build_channels", "ccdgpu_inject_wait_timeout",
+    "ccdgpu_build_channels", "ccdgpu_inject_wait_timeout", "ccdgpu_trace_read_end",
 ]
 
 
@@ -177,5 +177,6 @@ def gpu_lib():
         lib.ccdgpu_release_cached_memory.restype = None
         lib.ccdgpu_trace_read.argtypes = [vp, P(c_u64), P(c_u64), c_i32]
         lib.ccdgpu_inject_wait_timeout.argtypes = [vp]
+        lib.ccdgpu_trace_read_end.argtypes = [vp, P(c_u64), c_i32]
         _gpu = lib
     return _gpu

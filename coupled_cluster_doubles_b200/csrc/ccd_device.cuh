@@ -231,6 +231,7 @@ struct Control {
   int64_t trace_iter;    // kernel trace: the iteration whose kernels record start times
   uint64_t trace_first[kTraceKernels];  // %globaltimer of the first / last CTA start
   uint64_t trace_last[kTraceKernels];
+  uint64_t trace_end[kTraceKernels];    // %globaltimer when the last CTA finished
   double energies[128];  // corrCCD per iteration (first 128)
 };
 

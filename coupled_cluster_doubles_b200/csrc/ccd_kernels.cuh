@@ -106,6 +106,15 @@ __device__ __forceinline__ void trace_start(const Control *ctl, int tr) {
     atomicMax(reinterpret_cast<unsigned long long *>(&c->trace_last[tr]), t);
   }
 }
+// Records, for the traced iteration, when a CTA of kernel `tr` finished (thread 0, after the
+// CTA's work; the trace keeps the latest).
+__device__ __forceinline__ void trace_end(const Control *ctl, int tr) {
+  if (threadIdx.x == 0 && ctl->trace_iter == ctl->iterations) {
+    Control *c = const_cast<Control *>(ctl);
+    atomicMax(reinterpret_cast<unsigned long long *>(&c->trace_end[tr]),
+              (unsigned long long)global_ns());
+  }
+}
 __device__ __forceinline__ bool skip_iteration(const Control *ctl, int gate, int tr) {
   pdl_enter();
   trace_start(ctl, tr);
@@ -200,6 +209,7 @@ ladder_reduce_kernel(const RedItem *__restrict__ items, const LadderTile *__rest
     d[tile.t_off + (int64_t)ab * tile.hh + col] = v;
     if (mir >= 0) d[tile.t_off + (int64_t)mir * tile.hh + col] = -v;
   }
+  trace_end(ctl, kTrReduce);
 }
 
 // Thin channels (nb in {2,4,8}): consumer thread = one packed row, all nb columns.
@@ -396,6 +406,7 @@ pp_ladder_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restrict
     if (!ok) break;  // a timed-out tile leaves its row block unfinished (error already set)
     gc += tile.nks + tile.nkh;
   }
+  trace_end(ctl, kTrLadderThin + CLS);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -567,6 +578,7 @@ hh_mma_kernel(const HHTile *__restrict__ tiles, int n, const ChanInfo *__restric
         if (ij + 1 < hh) pb[kl * hh + ij + 1] = acc[m][c][1];
       }
     }
+  trace_end(ctl, NMAX <= 2 ? kTrHHSmall : kTrHHTiled);
 }
 
 // Channels with hh > 16: one CTA per K slice of kHHRowsL pp rows.  The slice's rows of V_pphh
@@ -659,6 +671,8 @@ hh_slice_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ c
     for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
     if (lane == 0) r_out[ch.pp_off + tt.k0 + k] = d;
   }
+  __syncthreads();
+  trace_end(ctl, kTrHHTiled);
 }
 
 // Item = 256 consecutive elements P[kl][ij] (row-major) of channel ch, from idx0.
@@ -690,6 +704,7 @@ hh_reduce_kernel(const HHRed *__restrict__ items, const ChanInfo *__restrict__ c
       ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
   hh_finish(ch, idx / hh, idx - (idx / hh) * hh, p, v_hhhh, x_ref, x_t, s_out, xt_tc,
             xt_tc_stride, nt);
+  trace_end(ctl, kTrHHReduce);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -794,6 +809,7 @@ ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restr
       out[inv ? (int64_t)Is[p] : m.m_off + p] = v;
     }
   });
+  trace_end(ctl, kTrRingSmall);
 }
 
 // Channels with ph', hp' > kRingSmall: one CTA per channel, the two products on the FP64
@@ -906,6 +922,8 @@ ring16_kernel(const ModInfo *__restrict__ mods, const double *__restrict__ v_hpp
       [&](int, int, double v, int slot) {
         if (dst[slot] >= 0) out[dst[slot]] = v;
       });
+  __syncthreads();
+  trace_end(ctl, PAD <= 32 ? kTrRingMid : kTrRingLarge);
 }
 
 // Deterministic block reduction (fixed tree) of one double; result valid in thread 0.
@@ -990,6 +1008,7 @@ __global__ void onebody_fused_kernel(int np, int nsp, const int64_t *__restrict_
     if (hole) xh[w] = v;
     else yp[w - np] = v;
   }
+  trace_end(ctl, kTrOneBody);
 }
 
 // Writes one amplitude into the ladder operand tiles: the B tiles of V T (rows c<d) and the A
@@ -1210,6 +1229,7 @@ assemble_fused_kernel(const QuadItem *__restrict__ items, int n_items,
     corr += 4.0 * (vv * t1);
   }
   const double sum = block_sum<kAsmThreads>(corr, scratch);
+  trace_end(ctl, kTrAssemble);
   // The last CTA to finish sums the partials and applies the stop rule (no extra launch).
   if (threadIdx.x == 0) {
     epart[blockIdx.x] = sum;

@@ -457,6 +457,7 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
                  ::"r"(tmem), "r"(2 * kTcAccCols) : "memory");
   }
+  trace_end(ctl, kTrLadderTC);
 }
 
 }  // namespace ccd

@@ -2626,6 +2626,7 @@ int ccdgpu_trace_arm(ccdgpu_handle *h, int64_t iteration) {
   for (int k = 0; k < kTraceKernels; k++) {
     c.trace_first[k] = ~0ull;
     c.trace_last[k] = 0;
+    c.trace_end[k] = 0;
   }
   CK(cudaMemcpyAsync(h->ctl, h->h_ctl, sizeof(Control), cudaMemcpyHostToDevice, h->s0));
   CK(cudaStreamSynchronize(h->s0));
@@ -2641,6 +2642,14 @@ int ccdgpu_trace_read(ccdgpu_handle *h, uint64_t *first, uint64_t *last, int32_t
     first[k] = h->h_ctl->trace_first[k];
     last[k] = h->h_ctl->trace_last[k];
   }
+  return CCDGPU_OK;
+}
+int ccdgpu_trace_read_end(ccdgpu_handle *h, uint64_t *end, int32_t n) {
+  if (!h || !end || n < 0) return CCDGPU_ERR_INVALID_ARGUMENT;
+  CK(cudaSetDevice(h->opt.device));
+  int rc = sync_ctl(h);
+  if (rc) return rc;
+  for (int k = 0; k < n && k < kTraceKernels; k++) end[k] = h->h_ctl->trace_end[k];
   return CCDGPU_OK;
 }
 int ccdgpu_work_per_iteration(const ccdgpu_handle *h, double *flops, double *v_pppp_bytes,

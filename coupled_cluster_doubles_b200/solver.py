@@ -231,17 +231,24 @@ class CCDSolver:
         """Record kernel start times of iteration `iteration` of the next solve (-1 disarms)."""
         _check(_native.gpu_lib().ccdgpu_trace_arm(self._h, int(iteration)), "ccdgpu_trace_arm")
 
-    def trace_read(self):
+    def trace_read(self, with_end=False):
         """{kernel: (first CTA start, last CTA start)} in ns, relative to the earliest start;
-        kernels that did not run in the traced iteration are left out."""
+        with_end=True adds the time the last CTA finished (None where a kernel does not record
+        it).  Kernels that did not run in the traced iteration are left out."""
         n = len(self.TRACE_KERNELS)
         first = (ctypes.c_uint64 * n)()
         last = (ctypes.c_uint64 * n)()
-        _check(_native.gpu_lib().ccdgpu_trace_read(self._h, first, last, n), "ccdgpu_trace_read")
+        end = (ctypes.c_uint64 * n)()
+        lib = _native.gpu_lib()
+        _check(lib.ccdgpu_trace_read(self._h, first, last, n), "ccdgpu_trace_read")
+        _check(lib.ccdgpu_trace_read_end(self._h, end, n), "ccdgpu_trace_read_end")
         ran = [k for k in range(n) if first[k] != 2**64 - 1]
         if not ran:
             return {}
         t0 = min(first[k] for k in ran)
+        if with_end:
+            return {self.TRACE_KERNELS[k]: (first[k] - t0, last[k] - t0,
+                                            end[k] - t0 if end[k] else None) for k in ran}
         return {self.TRACE_KERNELS[k]: (first[k] - t0, last[k] - t0) for k in ran}
 
     def inject_wait_timeout(self):

@@ -347,6 +347,9 @@ int ccdgpu_kernel_profile(ccdgpu_handle *h, int32_t reps, double ms[7], double f
  * refresh, split-K reduction, hh-ladder reduction (16). */
 int ccdgpu_trace_arm(ccdgpu_handle *h, int64_t iteration);
 int ccdgpu_trace_read(ccdgpu_handle *h, uint64_t *first, uint64_t *last, int32_t n);
+/* The same trace: when the last CTA of each kernel finished (%globaltimer ns; 0 for kernels
+ * that do not record it: the loop control, energy and FP64 tile refresh kernels). */
+int ccdgpu_trace_read_end(ccdgpu_handle *h, uint64_t *end, int32_t n);
 
 /* No counterpart in the reference.  The ladder term of one regular channel,
  *   D = 0.5 T X + 0.5 V_pppp T   with   X = V_hhhh + 0.5 V_hhpp T,
