@@ -1498,25 +1498,25 @@ int launch_pp_ladder(ccdgpu_handle *h, cudaStream_t st) {
     CK(launch_pdl(retile_done_kernel, 1, 32, 0, st, h->ctl));
     h->launches += 2;
   }
-  const bool side = h->n_cls[1] || h->n_cls[2];
-  if (side) {
-    CK(cudaEventRecord(h->ev_fork2, st));
-    CK(cudaStreamWaitEvent(h->s2, h->ev_fork2, 0));
+  // The classes run one after another on `st`: each is persistent over every SM (its tiles
+  // balanced for CTAs that all start together), so concurrent classes only delay each other's
+  // CTAs.
+  cudaStream_t s2 = st;
+  if (h->n_cls[1] || h->n_cls[2]) {
     if (h->n_cls[2]) {
-      pp_ladder_kernel<2><<<h->fp_grid[2], ladder_threads(2), h->ladder_smem, h->s2>>>(
+      pp_ladder_kernel<2><<<h->fp_grid[2], ladder_threads(2), h->ladder_smem, s2>>>(
           h->tiles, h->fp_cta_off + h->fp_off_base[2], h->v_t, h->t_kt, h->t_mt, h->x_t,
           h->rowmap, h->mirror, h->dmat, h->lpart, h->ctl, h->err, 0);
       h->launches++;
       CK(cudaGetLastError());
     }
     if (h->n_cls[1]) {
-      pp_ladder_kernel<1><<<h->fp_grid[1], ladder_threads(1), h->ladder_smem, h->s2>>>(
+      pp_ladder_kernel<1><<<h->fp_grid[1], ladder_threads(1), h->ladder_smem, s2>>>(
           h->tiles, h->fp_cta_off + h->fp_off_base[1], h->v_t, h->t_kt, h->t_mt, h->x_t,
           h->rowmap, h->mirror, h->dmat, h->lpart, h->ctl, h->err, 0);
       h->launches++;
       CK(cudaGetLastError());
     }
-    CK(cudaEventRecord(h->ev_join2, h->s2));
   }
   if (h->n_cls[0]) {
     CK(launch_pdl(pp_ladder_kernel<0>, h->fp_grid[0], kLadderThreads, h->ladder_smem_thin, st,
@@ -1526,7 +1526,6 @@ int launch_pp_ladder(ccdgpu_handle *h, cudaStream_t st) {
                   h->dmat, h->lpart, (const Control *)h->ctl, h->err, 0));
     h->launches++;
   }
-  if (side) CK(cudaStreamWaitEvent(st, h->ev_join2, 0));
   if (h->n_red_fp) {
     CK(launch_pdl(ladder_reduce_kernel, h->n_red_fp, 256, 0, st, (const RedItem *)h->red_fp,
                   (const LadderTile *)h->tiles, (const int32_t *)h->rowmap,
@@ -1544,29 +1543,29 @@ int launch_ring(ccdgpu_handle *h, cudaStream_t st, int gate, bool fused, int onl
   const int32_t *inv = fused ? h->inv4 : nullptr;
   double *out = fused ? h->d_ring : h->r_phhp;
   if (h->n_mod_small && (only < 0 || only == 0)) {
-    ring_small_kernel<<<(int)ceil_div(h->n_mod_small, kRingSmallWarps), kRingSmallWarps * 32, 0,
-                        st>>>(
-        h->mods, h->n_mod_small, h->v_hpph, h->v_hphp, h->old_phhp, inv, out, h->ctl, gate);
+    CK(launch_pdl(ring_small_kernel, (int)ceil_div(h->n_mod_small, kRingSmallWarps),
+                  kRingSmallWarps * 32, 0, st, (const ModInfo *)h->mods, h->n_mod_small,
+                  (const double *)h->v_hpph, (const double *)h->v_hphp,
+                  (const double *)h->old_phhp, inv, out, (const Control *)h->ctl, gate));
     h->launches++;
-    CK(cudaGetLastError());
   }
   // Groups by padded size; only = 1 launches the 32 group, only = 2 the wider ones.
   const ModInfo *mp = h->mods + h->n_mod_small;
   for (int k = 0; k < 4; k++) {
     const int n = h->n_mod_pad[k];
     if (n && (only < 0 || only == (k == 0 ? 1 : 2))) {
+      auto go = [&](auto kern, int pad) {
+        return launch_pdl(kern, n, 32 * ring16_warps(pad), ring16_smem(pad), st, mp,
+                          (const double *)h->v_hpph, (const double *)h->v_hphp,
+                          (const double *)h->old_phhp, inv, out, (const Control *)h->ctl, gate);
+      };
       switch (k) {
-        case 0: ring16_kernel<32><<<n, 32 * ring16_warps(32), ring16_smem(32), st>>>(
-                    mp, h->v_hpph, h->v_hphp, h->old_phhp, inv, out, h->ctl, gate); break;
-        case 1: ring16_kernel<48><<<n, 32 * ring16_warps(48), ring16_smem(48), st>>>(
-                    mp, h->v_hpph, h->v_hphp, h->old_phhp, inv, out, h->ctl, gate); break;
-        case 2: ring16_kernel<64><<<n, 32 * ring16_warps(64), ring16_smem(64), st>>>(
-                    mp, h->v_hpph, h->v_hphp, h->old_phhp, inv, out, h->ctl, gate); break;
-        default: ring16_kernel<80><<<n, 32 * ring16_warps(80), ring16_smem(80), st>>>(
-                    mp, h->v_hpph, h->v_hphp, h->old_phhp, inv, out, h->ctl, gate); break;
+        case 0: CK(go(ring16_kernel<32>, 32)); break;
+        case 1: CK(go(ring16_kernel<48>, 48)); break;
+        case 2: CK(go(ring16_kernel<64>, 64)); break;
+        default: CK(go(ring16_kernel<80>, 80)); break;
       }
       h->launches++;
-      CK(cudaGetLastError());
     }
     mp += n;
   }
@@ -1609,8 +1608,7 @@ int launch_map_to(ccdgpu_handle *h, cudaStream_t st, const double *src, double *
   return cuda_status(cudaGetLastError());
 }
 
-// One fused iteration: ring (s1) beside hh ladder, then pp ladder beside the one-body sums (s3),
-// then the assembly.
+// One fused iteration: hh ladder, one-body sums, pp ladder, ring, assembly.
 // mixed: the pp ladder runs on the tensor cores (split bf16) instead of the FP64 pipe.
 int enqueue_fused_iteration(ccdgpu_handle *h, bool mixed) {
   int rc;
@@ -1639,19 +1637,14 @@ int enqueue_fused_iteration(ccdgpu_handle *h, bool mixed) {
     CK(cudaEventRecord(h->ev[7], h->s0));
     return CCDGPU_OK;
   }
-  CK(cudaEventRecord(h->ev_fork, h->s0));
-  CK(cudaStreamWaitEvent(h->s1, h->ev_fork, 0));
-  if ((rc = launch_ring(h, h->s1, gate, true))) return rc;
-  CK(cudaEventRecord(h->ev_join, h->s1));
+  // One stream, one kernel at a time: every kernel is sized for the whole GPU (the ladders are
+  // persistent over every SM), and a trace of the concurrent schedule (ring beside the hh and
+  // pp ladders) showed the streams delaying each other's CTAs instead of filling idle SMs.
+  // Programmatic dependent launch overlaps each kernel's launch with its predecessor's tail.
   if ((rc = launch_hh_ladder(h, h->s0, gate))) return rc;
-  // The one-body sums feed only the assembly: they run on s3 beside the pp ladder.
-  CK(cudaEventRecord(h->ev_fork3, h->s0));
-  CK(cudaStreamWaitEvent(h->s3, h->ev_fork3, 0));
-  if ((rc = launch_onebody_fused(h, h->s3, gate))) return rc;
-  CK(cudaEventRecord(h->ev_join3, h->s3));
+  if ((rc = launch_onebody_fused(h, h->s0, gate))) return rc;
   if ((rc = ladder(h->s0))) return rc;
-  CK(cudaStreamWaitEvent(h->s0, h->ev_join, 0));
-  CK(cudaStreamWaitEvent(h->s0, h->ev_join3, 0));
+  if ((rc = launch_ring(h, h->s0, gate, true))) return rc;
   if ((rc = launch_assemble_fused(h, h->s0, gate))) return rc;  // + energy and stop rule
   if (h->loop_capture && !h->n_asm_blocks) {  // else the assembly set the loop condition
     h->launches++;
