@@ -1608,7 +1608,8 @@ int launch_map_to(ccdgpu_handle *h, cudaStream_t st, const double *src, double *
   return cuda_status(cudaGetLastError());
 }
 
-// One fused iteration: hh ladder, one-body sums, pp ladder, ring, assembly.
+// One fused iteration: ring on s1 beside hh ladder, one-body sums and pp ladder on s0, then the
+// assembly.
 // mixed: the pp ladder runs on the tensor cores (split bf16) instead of the FP64 pipe.
 int enqueue_fused_iteration(ccdgpu_handle *h, bool mixed) {
   int rc;
@@ -1637,14 +1638,18 @@ int enqueue_fused_iteration(ccdgpu_handle *h, bool mixed) {
     CK(cudaEventRecord(h->ev[7], h->s0));
     return CCDGPU_OK;
   }
-  // One stream, one kernel at a time: every kernel is sized for the whole GPU (the ladders are
-  // persistent over every SM), and a trace of the concurrent schedule (ring beside the hh and
-  // pp ladders) showed the streams delaying each other's CTAs instead of filling idle SMs.
-  // Programmatic dependent launch overlaps each kernel's launch with its predecessor's tail.
+  // The ring (s1) runs beside the hh ladder, the one-body sums and the pp ladder (s0); the
+  // latency-bound small ring channels fill SMs the hh ladder leaves idle.  The one-body sums
+  // stay on s0 ahead of the pp ladder: on a third stream their CTAs delayed the start of the
+  // persistent ladder's CTAs (device trace).
+  CK(cudaEventRecord(h->ev_fork, h->s0));
+  CK(cudaStreamWaitEvent(h->s1, h->ev_fork, 0));
+  if ((rc = launch_ring(h, h->s1, gate, true))) return rc;
+  CK(cudaEventRecord(h->ev_join, h->s1));
   if ((rc = launch_hh_ladder(h, h->s0, gate))) return rc;
   if ((rc = launch_onebody_fused(h, h->s0, gate))) return rc;
   if ((rc = ladder(h->s0))) return rc;
-  if ((rc = launch_ring(h, h->s0, gate, true))) return rc;
+  CK(cudaStreamWaitEvent(h->s0, h->ev_join, 0));
   if ((rc = launch_assemble_fused(h, h->s0, gate))) return rc;  // + energy and stop rule
   if (h->loop_capture && !h->n_asm_blocks) {  // else the assembly set the loop condition
     h->launches++;
