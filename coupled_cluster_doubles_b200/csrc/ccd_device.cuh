@@ -107,16 +107,23 @@ __device__ __forceinline__ __nv_bfloat16 bf16_of_short(double h) {
 // to 8 significant bits by Dekker's splitting (Dekker 1971: c = r (2^45 + 1), t = c - (c - r)),
 // which is exact in bf16, and the next remainder r - t_p is exact in FP64.  Only FP64 and
 // integer arithmetic, no conversion instructions.
+__device__ __forceinline__ double split_bf16_step(double &x) {
+  // Explicitly rounded operations: an FMA contraction of c - x would skip the rounding of c
+  // that the splitting relies on.
+  const double c = __dmul_rn(x, 35184372088833.0);  // 2^45 + 1
+  double hi = __dsub_rn(c, __dsub_rn(c, x));
+  if (fabs(hi) < 1.1754943508222875e-38) hi = 0.0;  // below bf16's normal range
+  x = __dsub_rn(x, hi);
+  return hi;
+}
 __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16 *out, int nt) {
-  for (int p = 0; p < nt; ++p) {
-    // Explicitly rounded operations: an FMA contraction of c - x would skip the rounding of c
-    // that the splitting relies on.
-    const double c = __dmul_rn(x, 35184372088833.0);  // 2^45 + 1
-    double hi = __dsub_rn(c, __dsub_rn(c, x));
-    if (fabs(hi) < 1.1754943508222875e-38) hi = 0.0;  // below bf16's normal range
-    out[p] = bf16_of_short(hi);
-    x = __dsub_rn(x, hi);
-  }
+  for (int p = 0; p < nt; ++p) out[p] = bf16_of_short(split_bf16_step(x));
+}
+// The same with the term count known at compile time (the terms stay in registers).
+template <int NT>
+__device__ __forceinline__ void split_bf16_n(double x, __nv_bfloat16 (&out)[NT]) {
+#pragma unroll
+  for (int p = 0; p < NT; ++p) out[p] = bf16_of_short(split_bf16_step(x));
 }
 
 // One pp-ladder work tile: packed rows [mt*bm, mt*bm+rows) of channel `ch`, V-part K chunks

@@ -162,20 +162,26 @@ struct LadderOut {
   const LadderTile &tile;
   const int32_t *rowmap, *mirror;
   double *d, *part;
-  __device__ __forceinline__ void row(int u_local, int c0, const double *v, int n) const {
+  // N is a compile-time count so that v stays in registers (every index is a constant).
+  template <int N>
+  __device__ __forceinline__ void row(int u_local, int c0, const double (&v)[N]) const {
     if (u_local >= tile.rows) return;
     if (tile.nseg > 1) {
       double *pp = part + tile.part_base + ((int64_t)tile.seg * tile.bm + u_local) * tile.nb + c0;
-      for (int j = 0; j < n; ++j) pp[j] = v[j];
+#pragma unroll
+      for (int j = 0; j < N; ++j) pp[j] = v[j];
       return;
     }
     const int u = tile.mt * tile.bm + u_local;
     const int ab = rowmap[tile.row_off + u], mir = mirror[tile.row_off + u];
     double *dr = d + tile.t_off + (int64_t)ab * tile.hh;
     double *mr = d + tile.t_off + (int64_t)mir * tile.hh;
-    for (int j = 0; j < n && c0 + j < tile.hh; ++j) {
-      dr[c0 + j] = v[j];
-      if (mir >= 0) mr[c0 + j] = -v[j];
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      if (c0 + j < tile.hh) {
+        dr[c0 + j] = v[j];
+        if (mir >= 0) mr[c0 + j] = -v[j];
+      }
     }
   }
 };
@@ -246,7 +252,7 @@ __device__ __forceinline__ bool consume_thin(const LadderTile &tile, const doubl
     __syncwarp();
     if (lane == 0) mbar_arrive(smem_u32(&bars[kStages + s]));
   }
-  out.row(tid, 0, acc, NB);
+  out.row<NB>(tid, 0, acc);
   return true;
 }
 
@@ -296,8 +302,9 @@ __device__ __forceinline__ bool consume_mma(const LadderTile &tile, const double
   if (halves > 0) {
 #pragma unroll
     for (int j = 0; j < C; ++j) {
-      out.row(16 * warp + g, 8 * j + 2 * t, acc[j], 2);
-      if (halves > 1) out.row(16 * warp + 8 + g, 8 * j + 2 * t, acc[j] + 2, 2);
+      const double lo[2] = {acc[j][0], acc[j][1]}, hi[2] = {acc[j][2], acc[j][3]};
+      out.row<2>(16 * warp + g, 8 * j + 2 * t, lo);
+      if (halves > 1) out.row<2>(16 * warp + 8 + g, 8 * j + 2 * t, hi);
     }
   }
   return true;
@@ -494,11 +501,19 @@ __device__ __forceinline__ void hh_finish(const ChanInfo &ch, int kl, int ij, do
   const int bs = ladder_bs(ch.nb);
   x_t[ch.xt_base + (int64_t)(kl / kBK) * kBK * bs + (kl % kBK) * bs + ij] = 0.5 * x;
   if (nt) {
-    __nv_bfloat16 hv[3];
-    split_bf16(0.5 * x, hv, nt);
     const int64_t o =
         ch.xt_tc_base + (int64_t)(kl >> 5) * (ch.nbt >> 3) * kTcGroup + tc_off_mn(ij, kl & 31);
-    for (int q = 0; q < nt; ++q) xt_tc[q * xt_tc_stride + o] = hv[q];
+    if (nt == 3) {
+      __nv_bfloat16 hv[3];
+      split_bf16_n<3>(0.5 * x, hv);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) xt_tc[q * xt_tc_stride + o] = hv[q];
+    } else {
+      __nv_bfloat16 hv[2];
+      split_bf16_n<2>(0.5 * x, hv);
+#pragma unroll
+      for (int q = 0; q < 2; ++q) xt_tc[q * xt_tc_stride + o] = hv[q];
+    }
   }
   if (kl == ij) s_out[ch.hh_off + ij] = p;
 }
@@ -699,7 +714,7 @@ hh_reduce_kernel(const HHRed *__restrict__ items, const ChanInfo *__restrict__ c
 #pragma unroll
     for (int k = 0; k < 8; ++k) acc[k] += __ldcg(pb + (int64_t)(sl + k) * nout);
   }
-  for (int k = 0; sl < ch.nhht; ++sl, ++k) acc[k] += __ldcg(pb + (int64_t)sl * nout);
+  for (; sl < ch.nhht; ++sl) acc[0] += __ldcg(pb + (int64_t)sl * nout);
   const double p =
       ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
   hh_finish(ch, idx / hh, idx - (idx / hh) * hh, p, v_hhhh, x_ref, x_t, s_out, xt_tc,
@@ -1035,25 +1050,34 @@ __device__ __forceinline__ void write_t_tiles(const ChanInfo &ch, const int2 *__
 // The same amplitude into the mixed-precision operand images: nt bf16 terms of T in the
 // tensor-core chunk layout (tc_off), V T operand B (K = c<d pair) and T X operand A (rows a<=b,
 // compact last 128-row tile, K = hh).
-__device__ __forceinline__ void write_t_tiles_tc(const ChanInfo &ch, int2 q, int ij, double t,
-                                                 int nt, __nv_bfloat16 *tkt_tc,
-                                                 int64_t tkt_stride, __nv_bfloat16 *tmt_tc,
-                                                 int64_t tmt_stride) {
-  if (q.x < 0 && q.y < 0) return;  // row ba of a mirrored pair: in neither image
-  __nv_bfloat16 hv[3];
-  split_bf16(t, hv, nt);
+template <int NT>
+__device__ __forceinline__ void write_t_tiles_tc_n(const ChanInfo &ch, int2 q, int ij, double t,
+                                                   __nv_bfloat16 *tkt_tc, int64_t tkt_stride,
+                                                   __nv_bfloat16 *tmt_tc, int64_t tmt_stride) {
+  __nv_bfloat16 hv[NT];
+  split_bf16_n<NT>(t, hv);
   if (q.x >= 0) {
     const int64_t o =
         ch.tkt_tc_base + (int64_t)(q.x >> 5) * (ch.nbt >> 3) * kTcGroup + tc_off_mn(ij, q.x & 31);
-    for (int p = 0; p < nt; ++p) tkt_tc[p * tkt_stride + o] = hv[p];
+#pragma unroll
+    for (int p = 0; p < NT; ++p) tkt_tc[p * tkt_stride + o] = hv[p];
   }
   if (q.y >= 0) {
     const int mt = q.y >> 7, r = q.y & 127;
     const int rg = (min(kTcBM, ch.pr - mt * kTcBM) + 7) >> 3;
     const int64_t o = ch.tmt_tc_base + (int64_t)mt * kTcBM * ch.nkht * kTcKC +
                       (int64_t)(ij >> 5) * rg * kTcGroup + tc_off(r, ij & 31);
-    for (int p = 0; p < nt; ++p) tmt_tc[p * tmt_stride + o] = hv[p];
+#pragma unroll
+    for (int p = 0; p < NT; ++p) tmt_tc[p * tmt_stride + o] = hv[p];
   }
+}
+__device__ __forceinline__ void write_t_tiles_tc(const ChanInfo &ch, int2 q, int ij, double t,
+                                                 int nt, __nv_bfloat16 *tkt_tc,
+                                                 int64_t tkt_stride, __nv_bfloat16 *tmt_tc,
+                                                 int64_t tmt_stride) {
+  if (q.x < 0 && q.y < 0) return;  // row ba of a mirrored pair: in neither image
+  if (nt == 3) write_t_tiles_tc_n<3>(ch, q, ij, t, tkt_tc, tkt_stride, tmt_tc, tmt_stride);
+  else write_t_tiles_tc_n<2>(ch, q, ij, t, tkt_tc, tkt_stride, tmt_tc, tmt_stride);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1093,7 +1117,7 @@ __device__ __forceinline__ void loop_set_condition(const Control *ctl,
 // In a mixed iteration (nt > 0) only the bf16 operand images are written; retile_kernel
 // rebuilds the FP64 tiles if FP64 iterations follow.
 constexpr int kQuadPerItem = kAsmThreads;  // one quad per thread and item
-constexpr int kAsmCTAsPerSM = 4;
+constexpr int kAsmCTAsPerSM = 3;
 
 // One thread's quad of a work item: where its four elements sit in the channel block, its
 // operand-image indices, one-body indices and denominator.  ok = false: no quad (past the

@@ -436,7 +436,7 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
           double dv[16];
 #pragma unroll
           for (int i = 0; i < 16; ++i) dv[i] = (double)v[i];
-          out.row(tid, c0, dv, 16);
+          out.row<16>(tid, c0, dv);
         }
       }
       tc_fence_before();
