@@ -794,12 +794,12 @@ ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restr
   double *Ts = buf[w], *Vt = Ts + kRingSmall * ld, *Ys = Vt + kRingSmall * ld;
   // Operands by cp.async (every load of the warp in flight at once), pad cells zeroed.  The
   // fused path (inv != null) reads T' straight from the amplitudes in pphh order through the
-  // inverse ai_jb table (T'[p] = t[inv[p]]: a lane loads its elements' indices, then gathers
-  // them), the table path reads the phhp slab; the table also goes to shared memory for R's
-  // scatter.
+  // inverse ai_jb table (T'[p] = t[inv[p]]), staged first; the table path reads the phhp slab.
   int32_t *Is = ibuf[w];
-  if (inv)
+  if (inv) {
     for (int p = lane; p < ph * hp; p += 32) cp_async4(Is + p, inv + m.m_off + p);
+    cp_async_commit();
+  }
   for (int e = lane; e < P * H; e += 32) {
     const int r = e >> hs, c = e & (H - 1);
     if (r < ph && c < hp) cp_async8(Vt + r * ld + c, v_hpph + m.m_off + r * hp + c);
@@ -810,21 +810,20 @@ ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restr
     if (r < hp && c < hp) cp_async8(Ys + r * ld + c, v_hphp + m.y_off + r * hp + c);
     else Ys[r * ld + c] = 0.0;
   }
-  constexpr int kPer = kRingSmall * kRingSmall / 32;
+  cp_async_commit();
   const double *tcur = ctl->parity ? tbuf1 : tbuf0;
-  int32_t src[kPer];
-#pragma unroll
-  for (int k = 0; k < kPer; ++k) {
-    const int e = lane + 32 * k, r = e >> hs, c = e & (H - 1);
-    src[k] = (e < P * H && r < ph && c < hp)
-                 ? (inv ? __ldg(inv + m.m_off + r * hp + c) : r * hp + c) : -1;
+  if (inv) {
+    cp_async_wait<1>();  // the indices (first group)
+    __syncwarp();
   }
-#pragma unroll
-  for (int k = 0; k < kPer; ++k) {
-    const int e = lane + 32 * k, r = e >> hs, c = e & (H - 1);
-    if (e >= P * H) break;
-    if (src[k] >= 0) cp_async8(Ts + r * ld + c, inv ? tcur + src[k] : t_phhp + m.m_off + src[k]);
-    else Ts[r * ld + c] = 0.0;
+  for (int e = lane; e < P * H; e += 32) {
+    const int r = e >> hs, c = e & (H - 1);
+    if (r < ph && c < hp) {
+      const int p = r * hp + c;
+      cp_async8(Ts + r * ld + c, inv ? tcur + Is[p] : t_phhp + m.m_off + p);
+    } else {
+      Ts[r * ld + c] = 0.0;
+    }
   }
   cp_async_commit();
   cp_async_wait<0>();
@@ -926,41 +925,62 @@ ring16_kernel(const ModInfo *__restrict__ mods, const double *__restrict__ v_hpp
   // 8 (n0 + n) + 2 t (+ 1); their destinations, -1 outside the channel.
   const int mt = warp / NCH, n0 = (warp - mt * NCH) * kRing16NC;
   int64_t dst[4 * kRing16NC];
-  // V_hpph and V_hphp by cp.async, pad cells zeroed.
-  for (int e = threadIdx.x; e < PAD * PAD; e += NT) {
-    const int r = e / PAD, c = e - r * PAD;
-    if (r < ph && c < hp) cp_async8(Vs + r * ld + c, v_hpph + m.m_off + (int64_t)r * hp + c);
-    else Vs[r * ld + c] = 0.0;
-    if (r < hp && c < hp) cp_async8(Ys + r * ld + c, v_hphp + m.y_off + (int64_t)r * hp + c);
-    else Ys[r * ld + c] = 0.0;
-  }
-  // R's destinations, loaded now (their latency overlaps everything below).
-#pragma unroll
-  for (int n = 0; n < kRing16NC; ++n)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int r = 16 * mt + g + 8 * (q >> 1), c = 8 * (n0 + n) + 2 * t + (q & 1);
-      const int64_t p = m.m_off + (int64_t)r * hp + c;
-      dst[4 * n + q] = (r < ph && c < hp && n0 + n < N8) ? (inv ? (int64_t)__ldg(inv + p) : p) : -1;
+  if (inv) {
+    // Fused path: T' read straight from the amplitudes in pphh order through the inverse ai_jb
+    // table (T'[p] = t[inv[p]]).  The table goes to the Y buffer first (it also gives R's
+    // destinations), then T' is gathered, then V_hphp replaces the table.
+    int32_t *Is = reinterpret_cast<int32_t *>(Ys);
+    for (int p = threadIdx.x; p < ph * hp; p += NT) cp_async4(Is + p, inv + m.m_off + p);
+    for (int e = threadIdx.x; e < PAD * PAD; e += NT) {
+      const int r = e / PAD, c = e - r * PAD;
+      if (r < ph && c < hp) cp_async8(Vs + r * ld + c, v_hpph + m.m_off + (int64_t)r * hp + c);
+      else Vs[r * ld + c] = 0.0;
     }
-  // T': on the fused path straight from the amplitudes in pphh order through the inverse
-  // ai_jb table (T'[p] = t[inv[p]]; a thread loads its elements' indices, then gathers them),
-  // on the table path from the phhp slab.
-  constexpr int PER = (PAD * PAD + NT - 1) / NT;
-  const double *tcur = ctl->parity ? tbuf1 : tbuf0;
-  int32_t src[PER];
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    const double *tcur = ctl->parity ? tbuf1 : tbuf0;
+    for (int e = threadIdx.x; e < PAD * PAD; e += NT) {
+      const int r = e / PAD, c = e - r * PAD;
+      if (r < ph && c < hp) cp_async8(Ts + r * ld + c, tcur + Is[r * hp + c]);
+      else Ts[r * ld + c] = 0.0;
+    }
+    cp_async_commit();
 #pragma unroll
-  for (int k = 0; k < PER; ++k) {
-    const int e = threadIdx.x + k * NT, r = e / PAD, c = e - r * PAD;
-    src[k] = (e < PAD * PAD && r < ph && c < hp)
-                 ? (inv ? __ldg(inv + m.m_off + r * hp + c) : r * hp + c) : -1;
-  }
+    for (int n = 0; n < kRing16NC; ++n)
 #pragma unroll
-  for (int k = 0; k < PER; ++k) {
-    const int e = threadIdx.x + k * NT, r = e / PAD, c = e - r * PAD;
-    if (e >= PAD * PAD) break;
-    if (src[k] >= 0) cp_async8(Ts + r * ld + c, inv ? tcur + src[k] : t_phhp + m.m_off + src[k]);
-    else Ts[r * ld + c] = 0.0;
+      for (int q = 0; q < 4; ++q) {
+        const int r = 16 * mt + g + 8 * (q >> 1), c = 8 * (n0 + n) + 2 * t + (q & 1);
+        dst[4 * n + q] = (r < ph && c < hp && n0 + n < N8) ? (int64_t)Is[r * hp + c] : -1;
+      }
+    cp_async_wait<0>();
+    __syncthreads();  // every read of the table is done
+    for (int e = threadIdx.x; e < PAD * PAD; e += NT) {
+      const int r = e / PAD, c = e - r * PAD;
+      if (r < hp && c < hp) cp_async8(Ys + r * ld + c, v_hphp + m.y_off + (int64_t)r * hp + c);
+      else Ys[r * ld + c] = 0.0;
+    }
+  } else {
+    for (int e = threadIdx.x; e < PAD * PAD; e += NT) {
+      const int r = e / PAD, c = e - r * PAD;
+      if (r < ph && c < hp) {
+        const int64_t src = m.m_off + (int64_t)r * hp + c;
+        cp_async8(Ts + r * ld + c, t_phhp + src);
+        cp_async8(Vs + r * ld + c, v_hpph + src);
+      } else {
+        Ts[r * ld + c] = 0.0;
+        Vs[r * ld + c] = 0.0;
+      }
+      if (r < hp && c < hp) cp_async8(Ys + r * ld + c, v_hphp + m.y_off + (int64_t)r * hp + c);
+      else Ys[r * ld + c] = 0.0;
+    }
+#pragma unroll
+    for (int n = 0; n < kRing16NC; ++n)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int r = 16 * mt + g + 8 * (q >> 1), c = 8 * (n0 + n) + 2 * t + (q & 1);
+        dst[4 * n + q] = (r < ph && c < hp && n0 + n < N8) ? m.m_off + (int64_t)r * hp + c : -1;
+      }
   }
   cp_async_commit();
   cp_async_wait<0>();
