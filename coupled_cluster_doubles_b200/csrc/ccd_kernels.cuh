@@ -779,7 +779,6 @@ constexpr int kRingSmallLd = kRingSmall + 4;
 __global__ void __launch_bounds__(kRingSmallWarps * 32)
 ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restrict__ v_hpph,
                   const double *__restrict__ v_hphp, const double *__restrict__ t_phhp,
-                  const double *tbuf0, const double *tbuf1,
                   const int32_t *__restrict__ inv, double *__restrict__ out, const Control *ctl,
                   int gate) {
   if (skip_iteration(ctl, gate, kTrRingSmall)) return;
@@ -792,39 +791,26 @@ ring_small_kernel(const ModInfo *__restrict__ mods, int n, const double *__restr
   const int ph = m.ph, hp = m.hp, P = ring_pad8(ph), H = ring_pad8(hp), ld = kRingSmallLd;
   const int hs = H == 8 ? 3 : 4;  // log2 H
   double *Ts = buf[w], *Vt = Ts + kRingSmall * ld, *Ys = Vt + kRingSmall * ld;
-  // Operands by cp.async (every load of the warp in flight at once), pad cells zeroed.  The
-  // fused path (inv != null) reads T' straight from the amplitudes in pphh order through the
-  // inverse ai_jb table (T'[p] = t[inv[p]]), staged first; the table path reads the phhp slab.
-  int32_t *Is = ibuf[w];
-  if (inv) {
-    for (int p = lane; p < ph * hp; p += 32) cp_async4(Is + p, inv + m.m_off + p);
-    cp_async_commit();
-  }
+  // Operands by cp.async (every load of the warp in flight at once), pad cells zeroed.
   for (int e = lane; e < P * H; e += 32) {
     const int r = e >> hs, c = e & (H - 1);
-    if (r < ph && c < hp) cp_async8(Vt + r * ld + c, v_hpph + m.m_off + r * hp + c);
-    else Vt[r * ld + c] = 0.0;
+    if (r < ph && c < hp) {
+      const int64_t src = m.m_off + r * hp + c;
+      cp_async8(Ts + r * ld + c, t_phhp + src);
+      cp_async8(Vt + r * ld + c, v_hpph + src);
+    } else {
+      Ts[r * ld + c] = 0.0;
+      Vt[r * ld + c] = 0.0;
+    }
   }
   for (int e = lane; e < H * H; e += 32) {
     const int r = e >> hs, c = e & (H - 1);
     if (r < hp && c < hp) cp_async8(Ys + r * ld + c, v_hphp + m.y_off + r * hp + c);
     else Ys[r * ld + c] = 0.0;
   }
-  cp_async_commit();
-  const double *tcur = ctl->parity ? tbuf1 : tbuf0;
-  if (inv) {
-    cp_async_wait<1>();  // the indices (first group)
-    __syncwarp();
-  }
-  for (int e = lane; e < P * H; e += 32) {
-    const int r = e >> hs, c = e & (H - 1);
-    if (r < ph && c < hp) {
-      const int p = r * hp + c;
-      cp_async8(Ts + r * ld + c, inv ? tcur + Is[p] : t_phhp + m.m_off + p);
-    } else {
-      Ts[r * ld + c] = 0.0;
-    }
-  }
+  int32_t *Is = ibuf[w];  // scatter destinations (fused path), staged with the operands
+  if (inv)
+    for (int p = lane; p < ph * hp; p += 32) cp_async4(Is + p, inv + m.m_off + p);
   cp_async_commit();
   cp_async_wait<0>();
   __syncwarp();
@@ -909,91 +895,45 @@ template <int PAD>
 __global__ void __launch_bounds__(32 * ring16_warps(PAD))
 ring16_kernel(const ModInfo *__restrict__ mods, const double *__restrict__ v_hpph,
               const double *__restrict__ v_hphp, const double *__restrict__ t_phhp,
-              const double *tbuf0, const double *tbuf1,
               const int32_t *__restrict__ inv, double *__restrict__ out, const Control *ctl,
               int gate) {
   if (skip_iteration(ctl, gate, PAD <= 32 ? kTrRingMid : kTrRingLarge)) return;
   extern __shared__ __align__(16) double r16[];
-  constexpr int ld = PAD + 4, NT = 32 * ring16_warps(PAD), N8 = PAD / 8;
-  constexpr int NCH = (N8 + kRing16NC - 1) / kRing16NC;
-  static_assert((PAD / 16) * NCH == ring16_warps(PAD), "one GEMM item per warp");
+  constexpr int ld = PAD + 4, NT = 32 * ring16_warps(PAD);
   double *Ts = r16, *Vs = r16 + PAD * ld, *Ys = r16 + 2 * PAD * ld;
   const ModInfo m = mods[blockIdx.x];
   const int ph = m.ph, hp = m.hp;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  // This thread's outputs of R = T' Y (its warp's one item): rows 16 mt + g (+ 8), columns
-  // 8 (n0 + n) + 2 t (+ 1); their destinations, -1 outside the channel.
-  const int mt = warp / NCH, n0 = (warp - mt * NCH) * kRing16NC;
-  int64_t dst[4 * kRing16NC];
-  if (inv) {
-    // Fused path: T' read straight from the amplitudes in pphh order through the inverse ai_jb
-    // table (T'[p] = t[inv[p]]).  The table goes to the Y buffer first (it also gives R's
-    // destinations), then T' is gathered, then V_hphp replaces the table.
-    int32_t *Is = reinterpret_cast<int32_t *>(Ys);
-    for (int p = threadIdx.x; p < ph * hp; p += NT) cp_async4(Is + p, inv + m.m_off + p);
-    for (int e = threadIdx.x; e < PAD * PAD; e += NT) {
-      const int r = e / PAD, c = e - r * PAD;
-      if (r < ph && c < hp) cp_async8(Vs + r * ld + c, v_hpph + m.m_off + (int64_t)r * hp + c);
-      else Vs[r * ld + c] = 0.0;
+  for (int e = threadIdx.x; e < PAD * PAD; e += NT) {
+    const int r = e / PAD, c = e - r * PAD;
+    if (r < ph && c < hp) {
+      const int64_t src = m.m_off + (int64_t)r * hp + c;
+      cp_async8(Ts + r * ld + c, t_phhp + src);
+      cp_async8(Vs + r * ld + c, v_hpph + src);
+    } else {
+      Ts[r * ld + c] = 0.0;
+      Vs[r * ld + c] = 0.0;
     }
-    cp_async_commit();
-    cp_async_wait<0>();
-    __syncthreads();
-    const double *tcur = ctl->parity ? tbuf1 : tbuf0;
-    for (int e = threadIdx.x; e < PAD * PAD; e += NT) {
-      const int r = e / PAD, c = e - r * PAD;
-      if (r < ph && c < hp) cp_async8(Ts + r * ld + c, tcur + Is[r * hp + c]);
-      else Ts[r * ld + c] = 0.0;
-    }
-    cp_async_commit();
-#pragma unroll
-    for (int n = 0; n < kRing16NC; ++n)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int r = 16 * mt + g + 8 * (q >> 1), c = 8 * (n0 + n) + 2 * t + (q & 1);
-        dst[4 * n + q] = (r < ph && c < hp && n0 + n < N8) ? (int64_t)Is[r * hp + c] : -1;
-      }
-    cp_async_wait<0>();
-    __syncthreads();  // every read of the table is done
-    for (int e = threadIdx.x; e < PAD * PAD; e += NT) {
-      const int r = e / PAD, c = e - r * PAD;
-      if (r < hp && c < hp) cp_async8(Ys + r * ld + c, v_hphp + m.y_off + (int64_t)r * hp + c);
-      else Ys[r * ld + c] = 0.0;
-    }
-  } else {
-    for (int e = threadIdx.x; e < PAD * PAD; e += NT) {
-      const int r = e / PAD, c = e - r * PAD;
-      if (r < ph && c < hp) {
-        const int64_t src = m.m_off + (int64_t)r * hp + c;
-        cp_async8(Ts + r * ld + c, t_phhp + src);
-        cp_async8(Vs + r * ld + c, v_hpph + src);
-      } else {
-        Ts[r * ld + c] = 0.0;
-        Vs[r * ld + c] = 0.0;
-      }
-      if (r < hp && c < hp) cp_async8(Ys + r * ld + c, v_hphp + m.y_off + (int64_t)r * hp + c);
-      else Ys[r * ld + c] = 0.0;
-    }
-#pragma unroll
-    for (int n = 0; n < kRing16NC; ++n)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int r = 16 * mt + g + 8 * (q >> 1), c = 8 * (n0 + n) + 2 * t + (q & 1);
-        dst[4 * n + q] = (r < ph && c < hp && n0 + n < N8) ? m.m_off + (int64_t)r * hp + c : -1;
-      }
+    if (r < hp && c < hp) cp_async8(Ys + r * ld + c, v_hphp + m.y_off + (int64_t)r * hp + c);
+    else Ys[r * ld + c] = 0.0;
   }
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
+  const int warp = threadIdx.x >> 5;
   // Y = V_hphp + 0.5 V_hpph T' with V_hpph[i][k] = Vt[k][i]; each Y element has one owner lane.
   ring16_gemm<PAD, 0>(
       Vs, Ts, warp, [](int, int, int) {},
       [&](int r, int c, double v, int) { Ys[r * ld + c] = 0.5 * v + Ys[r * ld + c]; });
   __syncthreads();
   // R = T' Y, stored for r < ph', c < hp' (through the inverse ai_jb table on the fused path);
-  // the destinations were read with the operands, so the stores wait on nothing.
+  // the destinations are loaded before the MMAs, so the stores do not wait on them.
+  int64_t dst[4 * kRing16NC];
   ring16_gemm<PAD, 1>(
-      Ts, Ys, warp, [](int, int, int) {},
+      Ts, Ys, warp,
+      [&](int slot, int r, int c) {
+        const int64_t p = m.m_off + (int64_t)r * hp + c;
+        dst[slot] = (r < ph && c < hp) ? (inv ? (int64_t)__ldg(inv + p) : p) : -1;
+      },
       [&](int, int, double v, int slot) {
         if (dst[slot] >= 0) out[dst[slot]] = v;
       });
@@ -1146,8 +1086,8 @@ __device__ __forceinline__ void write_t_tiles_tc(const ChanInfo &ch, int2 q, int
 //         + 0.5 x_i t_ab,ji - 0.5 x_j t_ab,ij                       (h2pp_h1 gathers, algebraically)
 //         + (-0.5 y_b) t_ab,ij - (-0.5 y_a) t_ba,ij                 (p2_p1hh gathers, algebraically)
 //   t_new = mixing value/(e_i+e_j-e_a-e_b) + (1-mixing) t_old;  E += V t_new
-// and the next iteration's ladder operands are written in the same pass (the ring gathers its
-// T' from the amplitudes through the inverse ai_jb table, mapToDistributed's counterpart).
+// and the next iteration's operands are written in the same pass: t_new into the phhp slab
+// (mapToDistributed ai_jb, a scattered write) and into the ladder operand tiles.
 // ------------------------------------------------------------------------------------------
 constexpr int kAsmThreads = 256;
 constexpr int kAsmPerThread = 2;  // table path: elements per thread of an ElemRange
@@ -1170,15 +1110,14 @@ __device__ __forceinline__ void loop_set_condition(const Control *ctl,
 // so (the ladders write D[ba] = -D[ab]; a quad writes its four elements as +t, -t, -t, +t), and
 // rows a = b or columns i = j hold zeros that no iteration changes.  One thread computes the
 // quad's element (ab, ij) from V, D, t at (ab, ij) and R at the four positions, and writes all
-// four elements and the operand-image entries of rows ab (row ba is in neither image).  The
-// ring reads the new amplitudes straight from pphh order through the inverse ai_jb table, so
-// nothing is scattered into the phhp layout.  The energy gains 4 V t_new per quad.
+// four elements, their phhp copies and the operand-image entries of rows ab (row ba is in
+// neither image).  The energy gains 4 V t_new per quad.
 // Persistent CTAs stride over work items of up to kQuadPerItem quads of one channel; a thread
 // takes one quad of an item and issues all its loads before the first store.
 // In a mixed iteration (nt > 0) only the bf16 operand images are written; retile_kernel
 // rebuilds the FP64 tiles if FP64 iterations follow.
 constexpr int kQuadPerItem = kAsmThreads;  // one quad per thread and item
-constexpr int kAsmCTAsPerSM = 4;
+constexpr int kAsmCTAsPerSM = 3;
 
 // One thread's quad of a work item: where its four elements sit in the channel block, its
 // operand-image indices, one-body indices and denominator.  ok = false: no quad (past the
@@ -1241,6 +1180,7 @@ assemble_fused_kernel(const QuadItem *__restrict__ items, int n_items,
                       const ChanInfo *__restrict__ chans, const QuadRow *__restrict__ qrows,
                       const QuadCol *__restrict__ qcols, const double *__restrict__ v_pphh,
                       const double *__restrict__ dmat, const double *__restrict__ d_ring,
+                      const int32_t *__restrict__ g_ai_jb, double *__restrict__ old_phhp,
                       const double *__restrict__ xh, const double *__restrict__ yp,
                       double *tbuf0, double *tbuf1, double *__restrict__ t_kt,
                       double *__restrict__ t_mt, double *__restrict__ epart, int32_t *ticket,
@@ -1269,7 +1209,7 @@ assemble_fused_kernel(const QuadItem *__restrict__ items, int n_items,
     const QuadRef cu = nx;
     double tv = 0.0, vv = 0.0, dv = 0.0, rv[4] = {0.0, 0.0, 0.0, 0.0}, xs[2] = {0.0, 0.0},
            ys[2] = {0.0, 0.0};
-    int32_t pos[4];
+    int32_t gv[4] = {0, 0, 0, 0}, pos[4];
     pos[0] = cu.o_ab + cu.c_ij;
     pos[1] = cu.o_ab + cu.c_ji;
     pos[2] = cu.o_ba + cu.c_ij;
@@ -1280,7 +1220,10 @@ assemble_fused_kernel(const QuadItem *__restrict__ items, int n_items,
       vv = __ldg(v_pphh + p0);
       dv = __ldcg(dmat + p0);
 #pragma unroll
-      for (int m = 0; m < 4; ++m) rv[m] = __ldcg(d_ring + cu.t_off + pos[m]);
+      for (int m = 0; m < 4; ++m) {
+        rv[m] = __ldcg(d_ring + cu.t_off + pos[m]);
+        gv[m] = __ldg(g_ai_jb + cu.t_off + pos[m]);
+      }
       // The one-body sums are small arrays every quad reads: through L1 (an L2-only load
       // would send every warp to the same few L2 slices).
       xs[0] = xh[cu.i];
@@ -1294,7 +1237,10 @@ assemble_fused_kernel(const QuadItem *__restrict__ items, int n_items,
                                  ys[1], cu.den, mixing);
     const double sg[4] = {t1, -t1, -t1, t1};
 #pragma unroll
-    for (int m = 0; m < 4; ++m) t_new[cu.t_off + pos[m]] = sg[m];
+    for (int m = 0; m < 4; ++m) {
+      t_new[cu.t_off + pos[m]] = sg[m];
+      old_phhp[gv[m]] = sg[m];
+    }
     const ChanInfo &ch = chans[cu.ch];
     const int2 qa = make_int2(cu.qx, cu.qy);
     if (nt) {

@@ -1546,8 +1546,7 @@ int launch_ring(ccdgpu_handle *h, cudaStream_t st, int gate, bool fused, int onl
     CK(launch_pdl(ring_small_kernel, (int)ceil_div(h->n_mod_small, kRingSmallWarps),
                   kRingSmallWarps * 32, 0, st, (const ModInfo *)h->mods, h->n_mod_small,
                   (const double *)h->v_hpph, (const double *)h->v_hphp,
-                  (const double *)h->old_phhp, (const double *)h->t[0], (const double *)h->t[1],
-                  inv, out, (const Control *)h->ctl, gate));
+                  (const double *)h->old_phhp, inv, out, (const Control *)h->ctl, gate));
     h->launches++;
   }
   // Groups by padded size; only = 1 launches the 32 group, only = 2 the wider ones.
@@ -1558,8 +1557,7 @@ int launch_ring(ccdgpu_handle *h, cudaStream_t st, int gate, bool fused, int onl
       auto go = [&](auto kern, int pad) {
         return launch_pdl(kern, n, 32 * ring16_warps(pad), ring16_smem(pad), st, mp,
                           (const double *)h->v_hpph, (const double *)h->v_hphp,
-                          (const double *)h->old_phhp, (const double *)h->t[0],
-                          (const double *)h->t[1], inv, out, (const Control *)h->ctl, gate);
+                          (const double *)h->old_phhp, inv, out, (const Control *)h->ctl, gate);
       };
       switch (k) {
         case 0: CK(go(ring16_kernel<32>, 32)); break;
@@ -1589,7 +1587,8 @@ int launch_assemble_fused(ccdgpu_handle *h, cudaStream_t st, int gate) {
       h->n_asm_blocks, kAsmThreads, 0, st, (const QuadItem *)h->quad_items, h->n_quad_items,
       (const ChanInfo *)h->chans, (const QuadRow *)h->quad_rows,
       (const QuadCol *)h->quad_cols, (const double *)h->v_pphh, (const double *)h->dmat,
-      (const double *)h->d_ring, (const double *)h->xh, (const double *)h->yp, h->t[0], h->t[1], h->t_kt, h->t_mt, h->epart,
+      (const double *)h->d_ring, (const int32_t *)(h->flat + 4 * h->n_t), h->old_phhp,
+      (const double *)h->xh, (const double *)h->yp, h->t[0], h->t[1], h->t_kt, h->t_mt, h->epart,
       h->ticket, h->ctl, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc, gate ? h->nt : 0,
       (cudaGraphConditionalHandle)(h->loop_capture ? h->loop_cond : 0), h->loop_capture, gate));
 }
