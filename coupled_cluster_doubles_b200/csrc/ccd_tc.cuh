@@ -48,7 +48,7 @@ __host__ __device__ constexpr int tc_threads(bool gen) {
   return kTcThreads + (gen ? 32 * kTcGenWarps : 0);
 }
 // Dynamic shared memory: 1024 bytes of alignment slack, the stages, then the barriers
-// (2 S + 5 of them).  (The generator's q^2 table is a static shared array.)
+// (2 S + 5 + 2 kTcTQ of them).  (The generator's q^2 table is a static shared array.)
 __host__ __device__ constexpr size_t tc_smem_bytes(int nt) {
   return 1024 + tc_stages(nt) * tc_stage_bytes(nt) + 256;
 }
@@ -169,16 +169,20 @@ __device__ __forceinline__ void tc_drain(const uint64_t *full, int issued, int s
     (void)mbar_wait(smem_u32(&full[c % stages]), (c / stages) & 1);
 }
 
-// Persistent CTAs: CTA b runs tiles cta_off[b] .. cta_off[b+1] (a balanced assignment made on
-// the host).  The producer streams K chunks through the S-stage ring without a break at tile
-// boundaries; the MMA thread accumulates tile number lt of the CTA into tensor-memory buffer
-// lt & 1 (two 128-column accumulators), so that the epilogue warps read tile lt back while
-// tile lt + 1 is loaded and multiplied.  Barriers: full / empty per stage, acc_full / acc_empty
-// per accumulator (tcgen05.commit, and one arrival per epilogue warp).  Every wait is bounded
-// and checks the CTA's abort flag.  Tiles are bm = 128 rows, nb = UMMA N columns, K chunks of
-// kTcKC; image arrays hold NT planes each, plane p at base + p * stride.  A mixed-phase kernel
-// (gate 1 of skip_iteration).
+// Persistent CTAs claim tiles from a launch-wide counter (tiles sorted by decreasing work, so
+// the claims are longest-first list scheduling, and a CTA that starts late because another
+// stream's kernel still holds its SM takes fewer tiles); the producer publishes each claimed
+// tile in a small shared-memory queue that the MMA thread, the epilogue warps and (GEN) the
+// generator warps follow.  The producer streams K chunks through the S-stage ring without a
+// break at tile boundaries; the MMA thread accumulates tile number lt of the CTA into
+// tensor-memory buffer lt & 1 (two 128-column accumulators), so that the epilogue warps read
+// tile lt back while tile lt + 1 is loaded and multiplied.  Barriers: full / empty per stage,
+// acc_full / acc_empty per accumulator (tcgen05.commit, and one arrival per epilogue warp),
+// tq_full / tq_empty per queue slot.  Every wait is bounded and checks the CTA's abort flag.
+// Tiles are bm = 128 rows, nb = UMMA N columns, K chunks of kTcKC; image arrays hold NT planes
+// each, plane p at base + p * stride.  A mixed-phase kernel (gate 1 of skip_iteration).
 constexpr uint32_t kTcAccCols = 128;  // columns of one accumulator buffer (nb <= kTcMaxNB)
+constexpr int kTcTQ = 4;              // slots of a CTA's queue of claimed tiles
 constexpr int kTcGrid = 2 * 148;      // persistent grid: two CTAs on each of the 148 SMs
 // GEN (electron gas, V generated in the ladder): warps 6 .. 6 + kTcGenWarps - 1 write the V
 // operand planes of every V T chunk into the stage (fence.proxy.async, then one arrival per
@@ -186,7 +190,7 @@ constexpr int kTcGrid = 2 * 148;      // persistent grid: two CTAs on each of th
 // those chunks.  No V image is read from HBM.
 template <int NT, bool GEN>
 __global__ void __launch_bounds__(tc_threads(GEN), GEN ? 2 : 1)
-pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restrict__ cta_off,
+pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, int n_tiles, int32_t *sched,
                     const __nv_bfloat16 *__restrict__ v_tc, int64_t v_stride,
                     const __nv_bfloat16 *__restrict__ tkt_tc, int64_t tkt_stride,
                     const __nv_bfloat16 *__restrict__ tmt_tc, int64_t tmt_stride,
@@ -206,6 +210,8 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
   uint64_t *bars = reinterpret_cast<uint64_t *>(tc_smem_raw + (base - raw) + S * kStageBytes);
   uint64_t *full = bars, *empty = bars + S, *acc_full = bars + 2 * S,
            *acc_empty = bars + 2 * S + 2, *done = bars + 2 * S + 4;
+  uint64_t *tq_full = bars + 2 * S + 5, *tq_empty = tq_full + kTcTQ;
+  __shared__ int tile_q[kTcTQ];
   // The generator's table: a separate shared array, so that its loads are independent of the
   // generators' stores into the stages.
   __shared__ VGenT<NT> gtab[GEN ? kTcGenTab : 1];
@@ -225,6 +231,10 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
       mbar_init(smem_u32(&acc_empty[b]), kLadderConsumers / 32);
     }
     mbar_init(smem_u32(done), 1);
+    for (int q = 0; q < kTcTQ; ++q) {
+      mbar_init(smem_u32(&tq_full[q]), 1);
+      mbar_init(smem_u32(&tq_empty[q]), 1 + kLadderConsumers / 32 + (GEN ? kTcGenWarps : 0));
+    }
     abort_flag = 0;
     issued_chunks = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -238,10 +248,20 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_holder;
-  const int t_begin = cta_off[blockIdx.x], t_end = cta_off[blockIdx.x + 1];
   auto fail = [&]() {
     atomicOr(err, kErrTimeout);
     atomicExch(&abort_flag, 1);
+  };
+  // The k-th tile of this CTA as the producer published it (waiting for it), -1 at the end;
+  // after the lanes in `mask` read it, one arrival per warp frees the slot.  `ok` = false: the
+  // wait ran out.
+  auto queued = [&](int k, bool &ok, unsigned mask) {
+    const int slot = k % kTcTQ;
+    ok = mbar_wait(smem_u32(&tq_full[slot]), (k / kTcTQ) & 1);
+    const int ti = ok ? *(volatile int *)&tile_q[slot] : -1;
+    __syncwarp(mask);
+    if (lane == 0 && ok) mbar_arrive(smem_u32(&tq_empty[slot]));
+    return ti;
   };
 
   if (warp == 4) {
@@ -249,7 +269,20 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
     if (lane == 0) {
       int gc = 0;  // chunks issued by this CTA (all its tiles)
       bool stop = false;
-      for (int ti = t_begin; ti < t_end && !stop; ++ti) {
+      for (int k = 0; !stop; ++k) {
+        // Claim the next tile of the launch (tiles are sorted by decreasing work, so this is
+        // longest-first list scheduling: a CTA that starts late simply takes fewer tiles) and
+        // publish it to the other roles.
+        const int slot = k % kTcTQ;
+        if (k >= kTcTQ && !mbar_wait(smem_u32(&tq_empty[slot]), ((k / kTcTQ) - 1) & 1)) {
+          fail();
+          break;
+        }
+        int ti = read_flag(&abort_flag) ? n_tiles : atomicAdd(&sched[0], 1);
+        if (ti >= n_tiles) ti = -1;
+        tile_q[slot] = ti;
+        mbar_arrive(smem_u32(&tq_full[slot]));
+        if (ti < 0) break;
         const LadderTile tile = tiles[ti];
         const int nchunks = tile.nks + tile.nkh;
         const int rg = (tile.rows + 7) >> 3;  // stored row groups of the A chunks
@@ -296,8 +329,15 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
   } else if (warp == 5) {
     // ---- MMA issuer ----
     if (lane == 0) {
-      int gc = 0, lt = 0;
-      for (int ti = t_begin; ti < t_end; ++ti, ++lt) {
+      int gc = 0;
+      for (int lt = 0;; ++lt) {
+        bool got;
+        const int ti = queued(lt, got, 1u);
+        if (!got) {
+          fail();
+          break;
+        }
+        if (ti < 0) break;
         const LadderTile tile = tiles[ti];
         const int buf = lt & 1, use = lt >> 1;
         if (read_flag(&abort_flag) ||
@@ -347,7 +387,14 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
     unsigned char *stage0 = tc_smem_raw + (base - raw);
     int gc = 0;
     bool stop = false;
-    for (int ti = t_begin; ti < t_end && !stop; ++ti) {
+    for (int k = 0; !stop; ++k) {
+      bool got;
+      const int ti = queued(k, got, 0xffffffffu);
+      if (!got) {
+        fail();
+        break;
+      }
+      if (ti < 0) break;
       const LadderTile tile = tiles[ti];
       const int nchunks = tile.nks + tile.nkh;
       const int64_t pk_off = chans[tile.ch].pk_off;
@@ -418,8 +465,14 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
   } else {
     // ---- epilogue: accumulator rows -> D (or split-K partials) ----
     const int tid = threadIdx.x;
-    int lt = 0;
-    for (int ti = t_begin; ti < t_end; ++ti, ++lt) {
+    for (int lt = 0;; ++lt) {
+      bool got;
+      const int ti = queued(lt, got, 0xffffffffu);
+      if (!consumers_all(got)) {  // one decision for all four warps
+        fail();
+        break;
+      }
+      if (ti < 0) break;  // every epilogue thread read the same slot
       const LadderTile tile = tiles[ti];
       const int buf = lt & 1, use = lt >> 1;
       const bool ok = mbar_wait(smem_u32(&acc_full[buf]), use & 1);
@@ -458,6 +511,16 @@ pp_ladder_tc_kernel(const LadderTile *__restrict__ tiles, const int32_t *__restr
                  ::"r"(tmem), "r"(2 * kTcAccCols) : "memory");
   }
   trace_end(ctl, kTrLadderTC);
+  // The last CTA to finish resets the tile counter for the next launch (every producer has
+  // claimed its last tile by then).
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&sched[1], 1) == (int)gridDim.x - 1) {
+      sched[0] = 0;
+      sched[1] = 0;
+      __threadfence();
+    }
+  }
 }
 
 }  // namespace ccd

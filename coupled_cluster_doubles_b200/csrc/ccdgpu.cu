@@ -120,7 +120,7 @@ struct ccdgpu_handle {
   void *tile_mem = nullptr;
   size_t tile_bytes = 0;
   RedItem *red_fp = nullptr, *red_tc = nullptr;  // split-K reduction items
-  int32_t *tc_cta_off = nullptr;  // tensor-core ladder: tile range of each persistent CTA
+  int32_t *tc_sched = nullptr;  // tensor-core ladder: tile counter, exit ticket (zero between launches)
   int tc_grid = 0;
   int32_t *fp_cta_off = nullptr;  // FP64 ladder classes: tile ranges of their persistent CTAs
   int fp_grid[3] = {0, 0, 0}, fp_off_base[3] = {0, 0, 0};
@@ -589,7 +589,6 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
     }
   }
   std::vector<LadderTile> tc_tiles;
-  std::vector<int32_t> tc_cta_off;
   int64_t tcpart_tot = 0;
   int32_t tc_groups = 0;
   if (h->nt) {
@@ -621,15 +620,14 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
         tc_groups++;
       }
     }
-    // Persistent CTAs (CTA b runs entries tc_cta_off[b] .. tc_cta_off[b+1]), LPT-balanced.
-    // Cost = bytes streamed per 32-deep chunk x chunks, plus two chunks' worth for the pipeline
-    // fill and the epilogue.
+    // The persistent CTAs claim tiles in list order from a launch-wide counter: sorted by
+    // decreasing cost, that is longest-first list scheduling.  Cost = bytes streamed per
+    // 32-deep chunk x chunks, plus two chunks' worth for the pipeline fill and the epilogue.
     auto tc_cost = [](const LadderTile &x) {
       return (int64_t)(x.nks + x.nkh + 2) * (((x.rows + 7) & ~7) + x.nb);
     };
-    if (!tc_tiles.empty())
-      lpt_group(tc_tiles, 0, tc_tiles.size(), (int)std::min<size_t>(tc_tiles.size(), kTcGrid),
-                tc_cost, tc_cta_off);
+    std::stable_sort(tc_tiles.begin(), tc_tiles.end(),
+                     [&](const LadderTile &x, const LadderTile &y) { return tc_cost(x) > tc_cost(y); });
   }
   // Reduction items of split row blocks.
   auto red_items = [](const std::vector<LadderTile> &tl, std::vector<RedItem> &out, int *per_cls,
@@ -665,13 +663,14 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
   h->tile_bytes = 0;
   h->tiles = h->tc_tiles = nullptr;
   h->lpart = h->tc_part = nullptr;
-  h->fp_cta_off = h->tc_cta_off = nullptr;
+  h->fp_cta_off = nullptr;
+  h->tc_sched = nullptr;
   h->red_fp = h->red_tc = nullptr;
   h->n_tiles = h->n_tc_tiles = 0;
   Arena ar;
   ar.add(&h->tiles, tiles.size()); ar.add(&h->lpart, lpart_tot);
   ar.add(&h->tc_tiles, tc_tiles.size());
-  ar.add(&h->fp_cta_off, fp_cta_off.size()); ar.add(&h->tc_cta_off, tc_cta_off.size());
+  ar.add(&h->fp_cta_off, fp_cta_off.size()); ar.add(&h->tc_sched, 2);
   ar.add(&h->tc_part, tcpart_tot);
   ar.add(&h->red_fp, red_fp.size()); ar.add(&h->red_tc, red_tc.size());
   CK(dev_alloc(ar.used, &h->tile_mem, &h->tile_bytes));
@@ -686,10 +685,7 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
   if (!fp_cta_off.empty())
     CK(cudaMemcpyAsync(h->fp_cta_off, fp_cta_off.data(), fp_cta_off.size() * sizeof(int32_t),
                        cudaMemcpyHostToDevice, h->s0));
-  if (!tc_cta_off.empty())
-    CK(cudaMemcpyAsync(h->tc_cta_off, tc_cta_off.data(), tc_cta_off.size() * sizeof(int32_t),
-                       cudaMemcpyHostToDevice, h->s0));
-  h->tc_grid = tc_cta_off.empty() ? 0 : (int)tc_cta_off.size() - 1;
+  h->tc_grid = (int)std::min<size_t>(tc_tiles.size(), kTcGrid);
   if (!red_fp.empty())
     CK(cudaMemcpyAsync(h->red_fp, red_fp.data(), red_fp.size() * sizeof(RedItem),
                        cudaMemcpyHostToDevice, h->s0));
@@ -707,7 +703,7 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
   return CCDGPU_OK;
 }
 
-using TcKernel = void (*)(const LadderTile *, const int32_t *, const __nv_bfloat16 *, int64_t,
+using TcKernel = void (*)(const LadderTile *, int, int32_t *, const __nv_bfloat16 *, int64_t,
                          const __nv_bfloat16 *, int64_t, const __nv_bfloat16 *, int64_t,
                          const __nv_bfloat16 *, int64_t, const int32_t *, const int32_t *,
                          double *, double *, const Control *, int32_t *, const ChanInfo *,
@@ -1471,7 +1467,7 @@ int launch_pp_ladder_tc(ccdgpu_handle *h, cudaStream_t st) {
   h->launches++;
   // Persistent: two CTAs per SM (shared memory and 2 x 128 tensor-memory columns each).
   CK(launch_pdl(tc_kernel_of(h->nt, h->tc_gen), h->tc_grid, tc_threads(h->tc_gen), h->tc_smem,
-                st, (const LadderTile *)h->tc_tiles, (const int32_t *)h->tc_cta_off,
+                st, (const LadderTile *)h->tc_tiles, h->n_tc_tiles, h->tc_sched,
                 (const __nv_bfloat16 *)h->v_tc, h->n_vtc, (const __nv_bfloat16 *)h->tkt_tc,
                 h->n_tkttc, (const __nv_bfloat16 *)h->tmt_tc, h->n_tmttc,
                 (const __nv_bfloat16 *)h->xt_tc, h->n_xttc, (const int32_t *)h->rowmap,
