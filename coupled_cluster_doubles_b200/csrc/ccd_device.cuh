@@ -210,7 +210,7 @@ struct ElemRange {
 enum TraceKernel {
   kTrRingSmall = 0, kTrRingMid, kTrRingLarge, kTrHHSmall, kTrHHTiled, kTrOneBody, kTrLadderThin,
   kTrLadderMid, kTrLadderWide, kTrLadderTC, kTrAssemble, kTrLoopCtl, kTrEnergy, kTrRetile,
-  kTrReduce, kTrHHReduce, kTraceKernels
+  kTrReduce, kTrHHReduce, kTrGather, kTraceKernels
 };
 
 // Device control block: iteration state of the solve loop lives on the device so that a

@@ -734,6 +734,42 @@ hh_reduce_kernel(const HHRed *__restrict__ items, const ChanInfo *__restrict__ c
 // ------------------------------------------------------------------------------------------
 constexpr int kRingSmall = 16;
 
+// T' for the ring on the fused path: the phhp slab gathered from the current amplitudes,
+// phhp[p] = t[inv[p]] (inv = inverse of the ai_jb table, a permutation of the n elements), at
+// the head of the ring stream: coalesced index loads and slab stores, scattered reads of t
+// (which the previous assembly has just written, so mostly L2 hits).  Eight elements per
+// thread, all their loads in flight together.  gate < 0: run outside the iteration gating
+// (a read of the slab after a solve).
+constexpr int kGatherPer = 8;
+__global__ void __launch_bounds__(256)
+phhp_gather_kernel(const int32_t *__restrict__ inv, int64_t n, const double *tbuf0,
+                   const double *tbuf1, double *__restrict__ phhp, const Control *ctl, int gate) {
+  if (gate >= 0) {
+    if (skip_iteration(ctl, gate, kTrGather)) return;
+  } else {
+    pdl_enter();
+  }
+  const double *__restrict__ t = ctl->parity ? tbuf1 : tbuf0;
+  const int64_t p0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * kGatherPer;
+  if (p0 >= n) return;
+  int32_t idx[kGatherPer];
+  double v[kGatherPer];
+  if (p0 + kGatherPer <= n) {
+    const int4 a = __ldg(reinterpret_cast<const int4 *>(inv + p0));
+    const int4 b = __ldg(reinterpret_cast<const int4 *>(inv + p0) + 1);
+    idx[0] = a.x; idx[1] = a.y; idx[2] = a.z; idx[3] = a.w;
+    idx[4] = b.x; idx[5] = b.y; idx[6] = b.z; idx[7] = b.w;
+#pragma unroll
+    for (int k = 0; k < kGatherPer; ++k) v[k] = __ldcg(t + idx[k]);
+    double2 *o = reinterpret_cast<double2 *>(phhp + p0);
+#pragma unroll
+    for (int k = 0; k < kGatherPer / 2; ++k) o[k] = make_double2(v[2 * k], v[2 * k + 1]);
+  } else {
+    for (int64_t p = p0; p < n; ++p) phhp[p] = __ldcg(t + inv[p]);
+  }
+  if (gate >= 0) trace_end(ctl, kTrGather);
+}
+
 // C (M8*8 x N8*8) = A B, K4*4 deep, on 8 x 8 tiles: warps warp, warp + nwarps, ... take items of
 // one 8-row tile by NC column tiles (the A fragment is reused NC times).  A[m][k] =
 // A[m * ars + k * aks], B[k][n] = B[k * ldb + n]; epi(row, col, value) stores each result.
@@ -1086,8 +1122,9 @@ __device__ __forceinline__ void write_t_tiles_tc(const ChanInfo &ch, int2 q, int
 //         + 0.5 x_i t_ab,ji - 0.5 x_j t_ab,ij                       (h2pp_h1 gathers, algebraically)
 //         + (-0.5 y_b) t_ab,ij - (-0.5 y_a) t_ba,ij                 (p2_p1hh gathers, algebraically)
 //   t_new = mixing value/(e_i+e_j-e_a-e_b) + (1-mixing) t_old;  E += V t_new
-// and the next iteration's operands are written in the same pass: t_new into the phhp slab
-// (mapToDistributed ai_jb, a scattered write) and into the ladder operand tiles.
+// and the next iteration's ladder operand tiles are written in the same pass (the ring's phhp
+// slab is gathered from t_new by phhp_gather_kernel at the head of the next iteration's ring
+// stream: mapToDistributed ai_jb as a coalesced write instead of a scattered one here).
 // ------------------------------------------------------------------------------------------
 constexpr int kAsmThreads = 256;
 constexpr int kAsmPerThread = 2;  // table path: elements per thread of an ElemRange
@@ -1110,8 +1147,7 @@ __device__ __forceinline__ void loop_set_condition(const Control *ctl,
 // so (the ladders write D[ba] = -D[ab]; a quad writes its four elements as +t, -t, -t, +t), and
 // rows a = b or columns i = j hold zeros that no iteration changes.  One thread computes the
 // quad's element (ab, ij) from V, D, t at (ab, ij) and R at the four positions, and writes all
-// four elements, their phhp copies and the operand-image entries of rows ab (row ba is in
-// neither image).  The energy gains 4 V t_new per quad.
+// four elements and the operand-image entries of rows ab (row ba is in neither image).  The energy gains 4 V t_new per quad.
 // Persistent CTAs stride over work items of up to kQuadPerItem quads of one channel; a thread
 // takes one quad of an item and issues all its loads before the first store.
 // In a mixed iteration (nt > 0) only the bf16 operand images are written; retile_kernel
@@ -1180,7 +1216,6 @@ assemble_fused_kernel(const QuadItem *__restrict__ items, int n_items,
                       const ChanInfo *__restrict__ chans, const QuadRow *__restrict__ qrows,
                       const QuadCol *__restrict__ qcols, const double *__restrict__ v_pphh,
                       const double *__restrict__ dmat, const double *__restrict__ d_ring,
-                      const int32_t *__restrict__ g_ai_jb, double *__restrict__ old_phhp,
                       const double *__restrict__ xh, const double *__restrict__ yp,
                       double *tbuf0, double *tbuf1, double *__restrict__ t_kt,
                       double *__restrict__ t_mt, double *__restrict__ epart, int32_t *ticket,
@@ -1209,7 +1244,7 @@ assemble_fused_kernel(const QuadItem *__restrict__ items, int n_items,
     const QuadRef cu = nx;
     double tv = 0.0, vv = 0.0, dv = 0.0, rv[4] = {0.0, 0.0, 0.0, 0.0}, xs[2] = {0.0, 0.0},
            ys[2] = {0.0, 0.0};
-    int32_t gv[4] = {0, 0, 0, 0}, pos[4];
+    int32_t pos[4];
     pos[0] = cu.o_ab + cu.c_ij;
     pos[1] = cu.o_ab + cu.c_ji;
     pos[2] = cu.o_ba + cu.c_ij;
@@ -1220,10 +1255,7 @@ assemble_fused_kernel(const QuadItem *__restrict__ items, int n_items,
       vv = __ldg(v_pphh + p0);
       dv = __ldcg(dmat + p0);
 #pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        rv[m] = __ldcg(d_ring + cu.t_off + pos[m]);
-        gv[m] = __ldg(g_ai_jb + cu.t_off + pos[m]);
-      }
+      for (int m = 0; m < 4; ++m) rv[m] = __ldcg(d_ring + cu.t_off + pos[m]);
       // The one-body sums are small arrays every quad reads: through L1 (an L2-only load
       // would send every warp to the same few L2 slices).
       xs[0] = xh[cu.i];
@@ -1237,10 +1269,7 @@ assemble_fused_kernel(const QuadItem *__restrict__ items, int n_items,
                                  ys[1], cu.den, mixing);
     const double sg[4] = {t1, -t1, -t1, t1};
 #pragma unroll
-    for (int m = 0; m < 4; ++m) {
-      t_new[cu.t_off + pos[m]] = sg[m];
-      old_phhp[gv[m]] = sg[m];
-    }
+    for (int m = 0; m < 4; ++m) t_new[cu.t_off + pos[m]] = sg[m];
     const ChanInfo &ch = chans[cu.ch];
     const int2 qa = make_int2(cu.qx, cu.qy);
     if (nt) {

@@ -1535,9 +1535,21 @@ int launch_pp_ladder(ccdgpu_handle *h, cudaStream_t st) {
 // T' from the phhp slab in both paths.  fused: R scattered into pphh order for the fused
 // assembly; else the table path's t2Diff_phhp slab.
 // only: -1 every class, else 0 small, 1 mid, 2 large.
+int launch_phhp_gather(ccdgpu_handle *h, cudaStream_t st, int gate) {
+  if (!h->n_m) return CCDGPU_OK;
+  h->launches++;
+  const unsigned blocks = (unsigned)ceil_div(h->n_m, (int64_t)256 * kGatherPer);
+  return cuda_status(launch_pdl(phhp_gather_kernel, blocks, 256, 0, st, (const int32_t *)h->inv4,
+                                h->n_m, (const double *)h->t[0], (const double *)h->t[1],
+                                h->old_phhp, (const Control *)h->ctl, gate));
+}
 int launch_ring(ccdgpu_handle *h, cudaStream_t st, int gate, bool fused, int only = -1) {
   const int32_t *inv = fused ? h->inv4 : nullptr;
   double *out = fused ? h->d_ring : h->r_phhp;
+  // Fused path: T' (the phhp slab) gathered from the current amplitudes first; the profile's
+  // small class includes it.
+  if (fused && (only < 0 || only == 0))
+    if (int rc = launch_phhp_gather(h, st, gate)) return rc;
   if (h->n_mod_small && (only < 0 || only == 0)) {
     CK(launch_pdl(ring_small_kernel, (int)ceil_div(h->n_mod_small, kRingSmallWarps),
                   kRingSmallWarps * 32, 0, st, (const ModInfo *)h->mods, h->n_mod_small,
@@ -1583,8 +1595,7 @@ int launch_assemble_fused(ccdgpu_handle *h, cudaStream_t st, int gate) {
       h->n_asm_blocks, kAsmThreads, 0, st, (const QuadItem *)h->quad_items, h->n_quad_items,
       (const ChanInfo *)h->chans, (const QuadRow *)h->quad_rows,
       (const QuadCol *)h->quad_cols, (const double *)h->v_pphh, (const double *)h->dmat,
-      (const double *)h->d_ring, (const int32_t *)(h->flat + 4 * h->n_t), h->old_phhp,
-      (const double *)h->xh, (const double *)h->yp, h->t[0], h->t[1], h->t_kt, h->t_mt, h->epart,
+      (const double *)h->d_ring, (const double *)h->xh, (const double *)h->yp, h->t[0], h->t[1], h->t_kt, h->t_mt, h->epart,
       h->ticket, h->ctl, h->tkt_tc, h->n_tkttc, h->tmt_tc, h->n_tmttc, gate ? h->nt : 0,
       (cudaGraphConditionalHandle)(h->loop_capture ? h->loop_cond : 0), h->loop_capture, gate));
 }
@@ -2402,6 +2413,12 @@ int ccdgpu_read_chain(ccdgpu_handle *h, int32_t chain, double *out, uint64_t n, 
   if (!out) return CCDGPU_OK;
   if (!src) return CCDGPU_ERR_UNSUPPORTED;
   if (n < len) return CCDGPU_ERR_INVALID_ARGUMENT;
+  if (chain == CCDGPU_CHAIN_OLD_PHHP && h->opt.path != CCDGPU_PATH_TABLES) {
+    // The fused path gathers the slab at the head of each iteration's ring: bring it up to
+    // the current amplitudes first.
+    if ((rc = launch_phhp_gather(h, h->s0, -1))) return rc;
+    CK(cudaStreamSynchronize(h->s0));
+  }
   CK(cudaMemcpy(out, src, len * 8, cudaMemcpyDeviceToHost));
   return CCDGPU_OK;
 }

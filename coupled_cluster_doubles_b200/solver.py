@@ -225,7 +225,7 @@ class CCDSolver:
 
     TRACE_KERNELS = ["ring_small", "ring_mid", "ring_large", "hh_small", "hh_large", "onebody",
                      "ladder_thin", "ladder_mid", "ladder_wide", "ladder_tc", "assemble",
-                     "loop_ctl", "energy", "retile", "ladder_reduce", "hh_reduce"]
+                     "loop_ctl", "energy", "retile", "ladder_reduce", "hh_reduce", "phhp_gather"]
 
     def trace_arm(self, iteration):
         """Record kernel start times of iteration `iteration` of the next solve (-1 disarms)."""
