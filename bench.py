@@ -454,11 +454,14 @@ def main():
                                        v_blocks=stored)
     h2d = _problem_bytes(system_e2e, with_v_pppp=stored, with_tables=False, with_v=stored)
     phase_s = np.zeros(4)  # create, solve (graph capture included), T2 read-back, destroy
+    create_ms = np.zeros(5)  # ccdgpu_create by phase (host metadata, uploads, device set-up, schedules, all)
     for k in range(args.warmup + args.steps):
         t0 = time.perf_counter()
         s2 = CCDSolver(system_e2e, device=local, path=args.path, precision=PRECISIONS[arms[0]],
                        v_mode=v_mode, device_loop=not args.no_device_loop)
         ta = time.perf_counter()
+        if k >= args.warmup:
+            create_ms += np.array(s2.profile()["ms_create"])
         r2 = s2.solve(tol=tol, max_iters=MAX_ITERS, mixing=MIXING)
         tb = time.perf_counter()
         s2.t2(host_t2)
@@ -615,7 +618,10 @@ def main():
                             + " made on the device) + ccdgpu_solve + ccdgpu_get_t2 + "
                               "ccdgpu_destroy",
                     "rank0_ms_per_step": dict(zip(["create", "solve", "get_t2", "destroy"],
-                                                  (1e3 * phase_s / args.steps).round(3).tolist()))},
+                                                  (1e3 * phase_s / args.steps).round(3).tolist())),
+                    "rank0_create_ms_by_phase": dict(zip(
+                        ["host_metadata", "alloc_upload", "device_setup", "schedules", "total"],
+                        (create_ms / args.steps).round(3).tolist()))},
             "roofline": ({**roof[head][dominant], "family": dominant, "peak_source": peak_kind}
                          if dominant else None),
             "gpu_launches": int(t["launches"]),

@@ -85,6 +85,7 @@ struct ccdgpu_handle {
   double *s = nullptr, *r = nullptr, *xh = nullptr, *yp = nullptr, *epart = nullptr;
   int32_t *flat = nullptr;
   int32_t *inv4 = nullptr;   // phhp position -> pphh element (inverse of the ai_jb table)
+  double create_ms[5] = {};   // ccdgpu_profile::ms_create
   double *d_ring = nullptr;  // fused path: ring result R in pphh order
   int64_t *o_h = nullptr, *o_p = nullptr;
   double *v_h_hpp = nullptr, *v_phh_p = nullptr;
@@ -713,7 +714,12 @@ TcKernel tc_kernel_of(int nt, bool gen) {
   return gen ? pp_ladder_tc_kernel<3, true> : pp_ladder_tc_kernel<3, false>;
 }
 
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
 int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
+  const auto t_build = std::chrono::steady_clock::now();
   const uint64_t nch = P->n_channels, nsp = P->n_sp, np = P->n_particles;
   h->nch = nch; h->nsp = nsp; h->np = np; h->npart = nsp - np;
   const ccdgpu_channel_dims *D = P->chan_dims, *MD = P->chan_mod_dims;
@@ -1054,6 +1060,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   }
 
   // ---- one device allocation ----
+  h->create_ms[0] = ms_since(t_build);
   Arena ar;
   ar.add(&h->chans, chans.size()); ar.add(&h->mods, mods.size());
   ar.add(&h->hh_tiles, hh_tiles.size()); ar.add(&h->hh_red, hh_red.size());
@@ -1283,6 +1290,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     }
   }
   // Device layout transforms.
+  h->create_ms[1] = ms_since(t_build) - h->create_ms[0];
   if (gen_v && !mod_gen.empty()) {
     gen_v_mod_kernel<<<(unsigned)mod_gen.size(), 256, 0, h->s0>>>(d_mod_gen, d_mod_ph, d_mod_hp,
                                                                  md, h->v_hpph, h->v_hphp);
@@ -1358,6 +1366,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   int32_t e = 0;
   CK(cudaMemcpyAsync(&e, h->err, sizeof(e), cudaMemcpyDeviceToHost, h->s0));
   CK(cudaStreamSynchronize(h->s0));
+  h->create_ms[2] = ms_since(t_build) - h->create_ms[0] - h->create_ms[1];
   // Release the scratch allocation.
   for (size_t i = n_allocs; i < h->allocs.size(); i++) dev_free(h->allocs[i].p, h->allocs[i].bytes);
   h->allocs.resize(n_allocs);
@@ -1407,6 +1416,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     CK(cudaFuncSetAttribute(tc_kernel_of(h->nt, h->tc_gen),
                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->tc_smem));
   }
+  h->create_ms[3] = ms_since(t_build) - h->create_ms[0] - h->create_ms[1] - h->create_ms[2];
   return CCDGPU_OK;
 }
 
@@ -1884,6 +1894,7 @@ const char *ccdgpu_strerror(int status) {
 
 int ccdgpu_create(const ccdgpu_problem *prob, const ccdgpu_options *opt, ccdgpu_handle **out) {
   if (!prob || !out) return CCDGPU_ERR_INVALID_ARGUMENT;
+  const auto t_create = std::chrono::steady_clock::now();
   *out = nullptr;
   if (!prob->sp_energy || !prob->chan_dims || !prob->chan_mod_dims || !prob->chan_maps ||
       !prob->three_body_dims || prob->n_particles == 0 || prob->n_particles >= prob->n_sp)
@@ -1920,6 +1931,7 @@ int ccdgpu_create(const ccdgpu_problem *prob, const ccdgpu_options *opt, ccdgpu_
   if (!rc) rc = set_ctl(h, 0, 0.0, 100, 0.5, true);
   if (!rc) rc = ccdgpu_trace_arm(h, -1);
   if (rc) { release(h); delete h; return rc; }
+  h->create_ms[4] = ms_since(t_create);
   *out = h;
   return CCDGPU_OK;
 }
@@ -2427,6 +2439,7 @@ int ccdgpu_get_profile(ccdgpu_handle *h, ccdgpu_profile *prof) {
   if (!h || !prof) return CCDGPU_ERR_INVALID_ARGUMENT;
   *prof = h->prof;
   prof->launches = h->launches;
+  for (int k = 0; k < 5; k++) prof->ms_create[k] = h->create_ms[k];
   return CCDGPU_OK;
 }
 int ccdgpu_enable_profiling(ccdgpu_handle *h, int32_t on) {

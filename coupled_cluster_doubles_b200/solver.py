@@ -164,7 +164,8 @@ class CCDSolver:
     def profile(self):
         p = _native.Profile()
         _check(_native.gpu_lib().ccdgpu_get_profile(self._h, ctypes.byref(p)), "profile")
-        return {k: getattr(p, k) for k, _ in p._fields_}
+        return {k: (list(getattr(p, k)) if k == "ms_create" else getattr(p, k))
+                for k, _ in p._fields_}
 
     def schedule(self):
         sch = _native.Schedule()

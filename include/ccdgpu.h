@@ -282,6 +282,11 @@ typedef struct ccdgpu_profile {
   double ms_total;       /* whole iterations */
   int64_t launches;      /* kernels launched by this library since create */
   int64_t iterations;    /* iterations covered by the ms_* sums */
+  /* Host wall time of ccdgpu_create by phase: [0] per-channel metadata and work lists on the
+   * host, [1] device allocation and uploads (enqueue), [2] device set-up kernels (tables, V,
+   * operand images) until they finish, [3] kernel attributes and ladder schedules, [4] the
+   * whole call. */
+  double ms_create[5];
 } ccdgpu_profile;
 int ccdgpu_get_profile(ccdgpu_handle *h, ccdgpu_profile *prof);
 /* When on, ccdgpu_solve runs the fused iteration without graph capture and brackets each
