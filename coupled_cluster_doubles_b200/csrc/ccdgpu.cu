@@ -13,6 +13,7 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <atomic>
 #include <queue>
 #include <chrono>
 #include <cmath>
@@ -186,6 +187,35 @@ int find_pair(const ccdgpu_pair *list, int64_t n, uint64_t p, uint64_t q) {
   if (lo < n && list[lo].p == p && list[lo].q == q) return (int)lo;
   return -1;
 }
+
+// Swap partner of every pair of a channel map sorted by (p, q): sw[k] = index of (q_k, p_k),
+// -1 if absent.  One pass records where each first index's run starts (row[p], stamped with
+// the channel so that the array is never cleared), then each partner is found by a scan of
+// its run (a channel holds few pairs per first index), O(n) instead of n binary searches
+// whose unpredictable branches dominated create on the largest bases.
+struct SwapIndex {
+  std::vector<int32_t> row;
+  std::vector<uint32_t> stamp;
+  uint32_t cur = 0;
+  explicit SwapIndex(size_t nsp) : row(nsp, 0), stamp(nsp, 0) {}
+  bool build(const ccdgpu_pair *m, int64_t n, int32_t *sw) {
+    ++cur;
+    for (int64_t k = 0; k < n; k++)
+      if (k == 0 || m[k].p != m[k - 1].p) {
+        if (m[k].p >= row.size()) return false;
+        row[m[k].p] = (int32_t)k;
+        stamp[m[k].p] = cur;
+      }
+    for (int64_t k = 0; k < n; k++) {
+      const uint64_t a = m[k].p, b = m[k].q;
+      sw[k] = -1;
+      if (b >= row.size() || stamp[b] != cur) continue;
+      for (int64_t j = row[b]; j < n && m[j].p == b && m[j].q <= a; j++)
+        if (m[j].q == a) { sw[k] = (int32_t)j; break; }
+    }
+    return true;
+  }
+};
 
 // Process-wide cache of device blocks given back by destroyed handles, by create's scratch
 // and by schedule changes, reused by later allocations on the same device instead of
@@ -714,6 +744,20 @@ TcKernel tc_kernel_of(int nt, bool gen) {
   return gen ? pp_ladder_tc_kernel<3, true> : pp_ladder_tc_kernel<3, false>;
 }
 
+// Host work lists of build(), kept per thread between creates: their pages are touched once
+// (first-touch page faults of ~20 MB of fresh vectors were most of a warm create's host time
+// on the largest bases), later creates only clear them.
+struct BuildScratch {
+  std::vector<int32_t> rowmap, mirror, kcol, pp_swap, hh_swap, list;
+  std::vector<int2> pk_idx, pp_pairs, hh_pairs, vrows, mod_ph, mod_hp, mod_dims;
+  std::vector<QuadRow> quad_rows;
+  std::vector<QuadCol> quad_cols;
+  std::vector<QuadItem> quad_items;
+  std::vector<ElemRange> ranges;
+  std::vector<int64_t> o_t, o_m, o_m_scratch;
+};
+thread_local BuildScratch t_build_scratch;
+
 double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -745,7 +789,10 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   if (n_maps != 0 && n_maps != 8) return CCDGPU_ERR_INVALID_ARGUMENT;
   const bool derive_tables = n_maps == 0;
 
-  std::vector<int64_t> o_t(nch + 1, 0), o_m(nch + 1, 0);
+  BuildScratch &bs = t_build_scratch;
+  std::vector<int64_t> &o_t = bs.o_t, &o_m = bs.o_m;
+  o_t.assign(nch + 1, 0);
+  o_m.assign(nch + 1, 0);
   for (uint64_t c = 0; c < nch; c++) {
     o_t[c + 1] = o_t[c] + (int64_t)(D[c].pp * D[c].hh);
     o_m[c + 1] = o_m[c] + (int64_t)(MD[c].ph * MD[c].hp);
@@ -757,61 +804,120 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   const int64_t n_t = h->n_t;
 
   // ---- per-channel metadata (O(sum pp) host work) ----
+  // Active channels (pp, hh > 0) and their pair offsets; then two passes over the channels,
+  // run in parallel (each writes its own ranges): pairs, swap partners and validation, then the
+  // packed-row and K index lists, whose offsets need every channel's counts from the first.
   std::vector<ChanInfo> chans;
   std::vector<uint64_t> act_chan;  // reference channel of each active channel
-  std::vector<int32_t> rowmap, mirror, kcol;
-  std::vector<int2> pk_idx, pp_pairs, hh_pairs, vrows;
-  std::vector<int32_t> pp_swap, hh_swap;
-  std::vector<HHTile> hh_tiles;
-  std::vector<HHRed> hh_red;
-  std::vector<std::vector<int32_t>> seg(nsp);
-  int64_t pp_tot = 0, hh_tot = 0, x_tot = 0, tkt = 0, tmt = 0, xt = 0, vt = 0, part_tot = 0;
-  int64_t vraw_tot = 0;
-  int64_t vtc = 0, tkttc = 0, tmttc = 0, xttc = 0;
-  std::vector<int64_t> vraw_off;
-  int maxhh = 1;
+  std::vector<int64_t> a_pp_off(1, 0), a_hh_off(1, 0);
   for (uint64_t c = 0; c < nch; c++) {
     const int64_t pp = D[c].pp, hh = D[c].hh;
     if (!pp || !hh) continue;
     if (hh > 8 * kMaxCG || pp > (1 << 20)) return CCDGPU_ERR_UNSUPPORTED;
-    const ccdgpu_pair *pm = P->chan_maps[c].pp, *hm = P->chan_maps[c].hh;
-    if (!pm || !hm) return CCDGPU_ERR_INVALID_ARGUMENT;
+    if (!P->chan_maps[c].pp || !P->chan_maps[c].hh) return CCDGPU_ERR_INVALID_ARGUMENT;
+    act_chan.push_back(c);
+    a_pp_off.push_back(a_pp_off.back() + pp);
+    a_hh_off.push_back(a_hh_off.back() + hh);
+  }
+  const int n_act = (int)act_chan.size();
+  std::vector<int32_t> &rowmap = bs.rowmap, &mirror = bs.mirror, &kcol = bs.kcol;
+  std::vector<int2> &pk_idx = bs.pk_idx, &pp_pairs = bs.pp_pairs, &hh_pairs = bs.hh_pairs,
+                    &vrows = bs.vrows;
+  std::vector<int32_t> &pp_swap = bs.pp_swap, &hh_swap = bs.hh_swap;
+  pp_pairs.resize(a_pp_off[n_act]);
+  pp_swap.resize(a_pp_off[n_act]);
+  pk_idx.resize(a_pp_off[n_act]);
+  hh_pairs.resize(a_hh_off[n_act]);
+  hh_swap.resize(a_hh_off[n_act]);
+  std::vector<int32_t> a_pr(n_act), a_pk(n_act);
+  std::atomic<int> bad{0};
+  const int host_threads = std::max(1, std::min(omp_get_max_threads(), 16));
+#pragma omp parallel num_threads(host_threads)
+  {
+    SwapIndex swap_index(nsp);
+#pragma omp for schedule(dynamic, 4)
+    for (int ai = 0; ai < n_act; ai++) {
+      const uint64_t c = act_chan[ai];
+      const ccdgpu_pair *pm = P->chan_maps[c].pp, *hm = P->chan_maps[c].hh;
+      const int64_t pp = D[c].pp, hh = D[c].hh, off = a_pp_off[ai], hoff = a_hh_off[ai];
+      if (!swap_index.build(pm, pp, pp_swap.data() + off)) {
+        bad = CCDGPU_ERR_BAD_TABLE;
+        continue;
+      }
+      int pr = 0, pk = 0;
+      for (int64_t k = 0; k < pp; k++) {
+        const uint64_t a = pm[k].p, b = pm[k].q;
+        if (a < np || b < np || a >= nsp || b >= nsp || pp_swap[off + k] < 0) {
+          bad = CCDGPU_ERR_BAD_TABLE;
+          break;
+        }
+        pp_pairs[off + k] = make_int2((int)a, (int)b);
+        pk += a < b;
+        pr += a <= b;
+      }
+      a_pr[ai] = pr;
+      a_pk[ai] = pk;
+      for (int64_t k = 0; k < hh; k++) {
+        const uint64_t i = hm[k].p, j = hm[k].q;
+        const int sw = (i < np && j < np) ? find_pair(hm, hh, j, i) : -1;
+        if (sw < 0) {
+          bad = CCDGPU_ERR_BAD_TABLE;
+          break;
+        }
+        hh_pairs[hoff + k] = make_int2((int)i, (int)j);
+        hh_swap[hoff + k] = sw;
+      }
+    }
+  }
+  if (bad) return bad;
+  std::vector<int64_t> a_row_off(n_act + 1, 0), a_pk_off(n_act + 1, 0);
+  for (int ai = 0; ai < n_act; ai++) {
+    a_row_off[ai + 1] = a_row_off[ai] + a_pr[ai];
+    a_pk_off[ai + 1] = a_pk_off[ai] + a_pk[ai];
+  }
+  rowmap.resize(a_row_off[n_act]);
+  mirror.resize(a_row_off[n_act]);
+  vrows.resize(a_row_off[n_act]);
+  kcol.resize(a_pk_off[n_act]);
+#pragma omp parallel for num_threads(host_threads) schedule(dynamic, 4)
+  for (int ai = 0; ai < n_act; ai++) {
+    const int64_t pp = D[act_chan[ai]].pp, off = a_pp_off[ai];
+    int32_t *rm = rowmap.data() + a_row_off[ai], *mr = mirror.data() + a_row_off[ai];
+    int2 *vr = vrows.data() + a_row_off[ai];
+    int32_t *kc = kcol.data() + a_pk_off[ai];
+    int pr = 0, pk = 0;
+    for (int64_t k = 0; k < pp; k++) {
+      const int a = pp_pairs[off + k].x, b = pp_pairs[off + k].y;
+      int2 q = make_int2(-1, -1);
+      if (a < b) { q.x = pk; kc[pk++] = (int32_t)k; }
+      if (a <= b) {
+        q.y = pr;
+        rm[pr] = (int32_t)k;
+        mr[pr] = a < b ? pp_swap[off + k] : -1;
+        vr[pr] = make_int2(ai, pr);
+        pr++;
+      }
+      pk_idx[off + k] = q;
+    }
+  }
+  std::vector<HHTile> hh_tiles;
+  std::vector<HHRed> hh_red;
+  int64_t x_tot = 0, tkt = 0, tmt = 0, xt = 0, vt = 0, part_tot = 0;
+  int64_t vraw_tot = 0;
+  int64_t vtc = 0, tkttc = 0, tmttc = 0, xttc = 0;
+  std::vector<int64_t> vraw_off;
+  int maxhh = 1;
+  for (int ai = 0; ai < n_act; ai++) {
+    const uint64_t c = act_chan[ai];
+    const int64_t pp = D[c].pp, hh = D[c].hh;
+    const int pr = a_pr[ai], pk = a_pk[ai];
     ChanInfo ci{};
     ci.pp = (int)pp; ci.hh = (int)hh;
     ci.nb = ladder_nb((int)hh);
     ci.bm = ladder_bm(ci.nb);
-    ci.row_off = (int64_t)rowmap.size();
-    ci.pk_off = (int64_t)kcol.size();
-    ci.pp_off = pp_tot; ci.hh_off = hh_tot; ci.x_off = x_tot;
-    const int ai = (int)chans.size();
-    int pr = 0, pk = 0;
-    for (int k = 0; k < ci.pp; k++) {
-      const uint64_t a = pm[k].p, b = pm[k].q;
-      if (a < np || b < np || a >= nsp || b >= nsp) return CCDGPU_ERR_BAD_TABLE;
-      const int sw = find_pair(pm, ci.pp, b, a);
-      if (sw < 0) return CCDGPU_ERR_BAD_TABLE;
-      pp_pairs.push_back(make_int2((int)a, (int)b));
-      pp_swap.push_back(sw);
-      seg[a].push_back((int32_t)(pp_tot + k));
-      int2 q = make_int2(-1, -1);
-      if (a < b) { q.x = pk++; kcol.push_back(k); }
-      if (a <= b) {
-        q.y = pr++;
-        rowmap.push_back(k);
-        mirror.push_back(a < b ? sw : -1);
-        vrows.push_back(make_int2(ai, q.y));
-      }
-      pk_idx.push_back(q);
-    }
-    for (int k = 0; k < ci.hh; k++) {
-      const uint64_t i = hm[k].p, j = hm[k].q;
-      if (i >= np || j >= np) return CCDGPU_ERR_BAD_TABLE;
-      const int sw = find_pair(hm, ci.hh, j, i);
-      if (sw < 0) return CCDGPU_ERR_BAD_TABLE;
-      hh_pairs.push_back(make_int2((int)i, (int)j));
-      hh_swap.push_back(sw);
-      seg[i].push_back((int32_t)(hh_tot + k));
-    }
+    ci.row_off = a_row_off[ai];
+    ci.pk_off = a_pk_off[ai];
+    ci.pp_off = a_pp_off[ai]; ci.hh_off = a_hh_off[ai]; ci.x_off = x_tot;
     ci.pr = pr; ci.pk = pk;
     ci.nkc = (int)ceil_div(pk, kBK);
     ci.nkh = (int)ceil_div(hh, kBK);
@@ -831,7 +937,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     tkttc += (int64_t)ci.nkct * (ci.nbt / 8) * kTcGroup;
     xttc += (int64_t)ci.nkht * (ci.nbt / 8) * kTcGroup;
     const int nb = ci.nb;
-    pp_tot += pp; hh_tot += hh; x_tot += hh * hh;
+    x_tot += hh * hh;
     tkt += (int64_t)ci.nkc * kBK * ladder_bs(nb);
     // Full row tiles at their A stride, then the compact last one.
     const int64_t arows_tot = (int64_t)(ci.nmt - 1) * ladder_arows_full(ci.nb) +
@@ -850,9 +956,9 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
                           (int)std::min<int64_t>(hh_rows, pp - (int64_t)t * hh_rows), 0, 0});
     for (int64_t i0 = 0; i0 < hh * hh; i0 += 256) hh_red.push_back({ai, (int32_t)i0});
     chans.push_back(ci);
-    act_chan.push_back(c);
   }
-  h->n_act = (int)chans.size();
+  const int64_t pp_tot = a_pp_off[n_act], hh_tot = a_hh_off[n_act];
+  h->n_act = n_act;
   h->n_hh_tiles = (int)hh_tiles.size();
   h->n_hh_red = (int)hh_red.size();
   // Channels with hh <= 16 first (their own launch), then the rest; largest units
@@ -865,21 +971,34 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   for (const HHTile &t : hh_tiles) h->n_hh_small += chans[t.ch].hh <= 16 ? 1 : 0;
   for (const ChanInfo &a : chans)
     if (a.hh > 16) h->hh_slice_smem = std::max(h->hh_slice_smem, hh_slice_smem(a.hh));
+  // Per orbital w, the pair elements whose first index is w, ascending (particles: pp
+  // elements, holes: hh elements): a counting sort.
   std::vector<int64_t> list_off(nsp + 1, 0);
-  for (uint64_t w = 0; w < nsp; w++) list_off[w + 1] = list_off[w] + (int64_t)seg[w].size();
-  std::vector<int32_t> list(list_off[nsp]);
+  for (int64_t e = 0; e < pp_tot; e++) list_off[pp_pairs[e].x + 1]++;
+  for (int64_t e = 0; e < hh_tot; e++) list_off[hh_pairs[e].x + 1]++;
+  for (uint64_t w = 0; w < nsp; w++) list_off[w + 1] += list_off[w];
+  std::vector<int32_t> &list = bs.list;
+  list.resize(list_off[nsp]);
   h->n_list = list_off[nsp];
-  for (uint64_t w = 0; w < nsp; w++) std::copy(seg[w].begin(), seg[w].end(), list.begin() + list_off[w]);
+  {
+    std::vector<int64_t> &cur = bs.o_m_scratch;
+    cur.assign(list_off.begin(), list_off.end() - 1);
+    for (int64_t e = 0; e < pp_tot; e++) list[cur[pp_pairs[e].x]++] = (int32_t)e;
+    for (int64_t e = 0; e < hh_tot; e++) list[cur[hh_pairs[e].x]++] = (int32_t)e;
+  }
 
   // Modified channels: small ones (one warp each) first, then one group per padded size
   // (32, 48, 64, 80; one CTA per channel).
   std::vector<ModInfo> mods, mods_pad[4];
-  std::vector<int2> mod_dims(nch);
+  std::vector<int2> &mod_dims = bs.mod_dims;
+  mod_dims.resize(nch);
   int64_t y_tot = 0;
   std::vector<const double *> src_hpph, src_hphp;
   std::vector<int64_t> cnt_hpph, cnt_hphp;
   std::vector<ModGen> mod_gen;        // generated V: modified channels in channel order
-  std::vector<int2> mod_ph, mod_hp;   // ... and their ph' (b, j) and hp' (i, a) pairs
+  std::vector<int2> &mod_ph = bs.mod_ph, &mod_hp = bs.mod_hp;  // ... their ph' (b, j), hp' (i, a) pairs
+  mod_ph.clear();
+  mod_hp.clear();
   for (uint64_t c = 0; c < nch; c++) {
     const int64_t ph = MD[c].ph, hp = MD[c].hp;
     mod_dims[c] = make_int2((int)ph, (int)hp);
@@ -938,7 +1057,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
 
   h->host_chans = chans;
 
-  std::vector<ElemRange> ranges;
+  std::vector<ElemRange> &ranges = bs.ranges;
+  ranges.clear();
   const int64_t per = (int64_t)kAsmThreads * kAsmPerThread;
   for (int ai = 0; ai < h->n_act; ai++) {
     const ChanInfo &a = chans[ai];
@@ -948,9 +1068,12 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   h->n_ranges = (int)ranges.size();
   // Fused assembly: quads (strict packed row a < b, strict hole pair i < j) per channel, their
   // static tables, and work items of up to kQuadPerItem quads of one channel.
-  std::vector<QuadRow> quad_rows;
-  std::vector<QuadCol> quad_cols;
-  std::vector<QuadItem> quad_items;
+  std::vector<QuadRow> &quad_rows = bs.quad_rows;
+  std::vector<QuadCol> &quad_cols = bs.quad_cols;
+  std::vector<QuadItem> &quad_items = bs.quad_items;
+  quad_rows.clear();
+  quad_cols.clear();
+  quad_items.clear();
   for (int ai = 0; ai < h->n_act; ai++) {
     ChanInfo &a = chans[ai];
     a.qrow_off = (int64_t)quad_rows.size();
