@@ -511,10 +511,10 @@ def main():
             fams = [
                 ("pp_ladder", lad, work[a]["ladder_bytes"], work[a]["ladder_flops"]),
                 ("assemble_energy", "assemble_fused_kernel", assemble_bytes(n_quads, nt), 0.0),
-                ("ring", "ring_small_kernel + ring_kernel<2/4>",
+                ("ring", "phhp_gather_kernel + ring_small_kernel + ring16_kernel<32/48/64>",
                  cls_bytes("ring_small", "ring_mid", "ring_large"),
                  cls_flops("ring_small", "ring_mid", "ring_large")),
-                ("hh_ladder", "hh_mma_kernel<2/9> + hh_reduce_kernel",
+                ("hh_ladder", "hh_mma_kernel<2> + hh_slice_kernel + hh_reduce_kernel",
                  cls_bytes("hh_small", "hh_large", "hh_reduce"),
                  cls_flops("hh_small", "hh_large")),
                 ("onebody", "onebody_fused_kernel", cls_bytes("onebody"), 0.0),
@@ -552,7 +552,9 @@ def main():
                 "kernel_ms_per_iteration": per_it[a],
                 "trace_iteration5_us": trace[a],
                 "kernel_rooflines": roof[a],
-                "pp_ladder_tflops_algorithmic": work[a]["ladder_flops"] / (lms / 1000.0) / 1e12,
+                # (None on the table path, whose stages have no per-family events.)
+                "pp_ladder_tflops_algorithmic": (work[a]["ladder_flops"] / (lms / 1000.0) / 1e12
+                                                 if lms > 0 else None),
                 "gpu_launches": int(ta["launches"]),
                 "schedule": tuned[a][0],
                 "schedule_source": "autotuned" if not args.no_autotune else "default",

@@ -1007,18 +1007,11 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     ModInfo m{};
     m.ph = (int)ph; m.hp = (int)hp; m.m_off = o_m[c]; m.y_off = y_tot;
     if (gen_v) {
-      const ccdgpu_pair *phm = P->chan_mod_maps[c].ph, *hpm = P->chan_mod_maps[c].hp;
-      if (!phm || !hpm) return CCDGPU_ERR_INVALID_ARGUMENT;
-      mod_gen.push_back(ModGen{(int)ph, (int)hp, m.m_off, m.y_off, (int64_t)mod_ph.size(),
-                               (int64_t)mod_hp.size()});
-      for (int64_t k = 0; k < ph; k++) {
-        if (phm[k].p < np || phm[k].p >= nsp || phm[k].q >= np) return CCDGPU_ERR_BAD_TABLE;
-        mod_ph.push_back(make_int2((int)phm[k].p, (int)phm[k].q));
-      }
-      for (int64_t k = 0; k < hp; k++) {
-        if (hpm[k].p >= np || hpm[k].q < np || hpm[k].q >= nsp) return CCDGPU_ERR_BAD_TABLE;
-        mod_hp.push_back(make_int2((int)hpm[k].p, (int)hpm[k].q));
-      }
+      // The pairs themselves are copied in parallel after this loop.
+      if (!P->chan_mod_maps[c].ph || !P->chan_mod_maps[c].hp) return CCDGPU_ERR_INVALID_ARGUMENT;
+      const int64_t ph0 = mod_gen.empty() ? 0 : mod_gen.back().ph_off + mod_gen.back().ph;
+      const int64_t hp0 = mod_gen.empty() ? 0 : mod_gen.back().hp_off + mod_gen.back().hp;
+      mod_gen.push_back(ModGen{(int)ph, (int)hp, m.m_off, m.y_off, ph0, hp0});
     } else {
       if (!P->v_hpph_mod[c] || !P->v_hphp_mod[c]) return CCDGPU_ERR_INVALID_ARGUMENT;
       src_hpph.push_back(P->v_hpph_mod[c]); cnt_hpph.push_back(ph * hp);
@@ -1028,6 +1021,28 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     const int64_t w = std::max(ph, hp);
     if (w <= kRingSmall) mods.push_back(m);
     else mods_pad[w <= 32 ? 0 : w <= 48 ? 1 : w <= 64 ? 2 : 3].push_back(m);
+  }
+  if (!mod_gen.empty()) {
+    mod_ph.resize(mod_gen.back().ph_off + mod_gen.back().ph);
+    mod_hp.resize(mod_gen.back().hp_off + mod_gen.back().hp);
+    std::vector<uint64_t> mod_chan;
+    for (uint64_t c = 0; c < nch; c++)
+      if (MD[c].ph && MD[c].hp) mod_chan.push_back(c);
+    std::atomic<int> bad_mod{0};
+#pragma omp parallel for num_threads(host_threads) schedule(dynamic, 16)
+    for (int64_t g = 0; g < (int64_t)mod_gen.size(); g++) {
+      const ModGen &mg = mod_gen[g];
+      const ccdgpu_pair *phm = P->chan_mod_maps[mod_chan[g]].ph, *hpm = P->chan_mod_maps[mod_chan[g]].hp;
+      for (int64_t k = 0; k < mg.ph; k++) {
+        if (phm[k].p < np || phm[k].p >= nsp || phm[k].q >= np) bad_mod = 1;
+        mod_ph[mg.ph_off + k] = make_int2((int)phm[k].p, (int)phm[k].q);
+      }
+      for (int64_t k = 0; k < mg.hp; k++) {
+        if (hpm[k].p >= np || hpm[k].q < np || hpm[k].q >= nsp) bad_mod = 1;
+        mod_hp[mg.hp_off + k] = make_int2((int)hpm[k].p, (int)hpm[k].q);
+      }
+    }
+    if (bad_mod) return CCDGPU_ERR_BAD_TABLE;
   }
   // Largest channels first within a group, so that the short ones fill in behind them.
   auto by_work = [](const ModInfo &x, const ModInfo &y) {
@@ -1074,10 +1089,34 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   quad_rows.clear();
   quad_cols.clear();
   quad_items.clear();
+  // Rows: the packed rows with a < b (pk of them per channel), filled in parallel below;
+  // columns (i < j) and work items here.
+  int64_t qrows_tot = 0;
   for (int ai = 0; ai < h->n_act; ai++) {
     ChanInfo &a = chans[ai];
-    a.qrow_off = (int64_t)quad_rows.size();
+    a.qrow_off = qrows_tot;
+    qrows_tot += a.pk;
     a.qcol_off = (int64_t)quad_cols.size();
+    for (int j = 0; j < a.hh; j++) {
+      const int2 pij = hh_pairs[a.hh_off + j];
+      if (pij.x >= pij.y) continue;  // i = j: zero column; i > j: the mirror of (j, i)
+      QuadCol c{};
+      c.c_ij = j; c.c_ji = hh_swap[a.hh_off + j]; c.i = pij.x; c.j = pij.y;
+      c.eij = P->sp_energy[pij.x] + P->sp_energy[pij.y];
+      quad_cols.push_back(c);
+    }
+    a.hk = (int)((int64_t)quad_cols.size() - a.qcol_off);
+    const int64_t nq = (int64_t)a.pk * a.hk;
+    if (nq >= ((int64_t)1 << 31) / 2) return CCDGPU_ERR_UNSUPPORTED;
+    for (int64_t q = 0; q < nq; q += kQuadPerItem)
+      quad_items.push_back({ai, (int32_t)q, (int32_t)std::min<int64_t>(nq, q + kQuadPerItem),
+                            a.hk, a.t_off, a.qrow_off, a.qcol_off});
+  }
+  quad_rows.resize(qrows_tot);
+#pragma omp parallel for num_threads(host_threads) schedule(dynamic, 4)
+  for (int ai = 0; ai < h->n_act; ai++) {
+    const ChanInfo &a = chans[ai];
+    QuadRow *out = quad_rows.data() + a.qrow_off;
     for (int u = 0; u < a.pr; u++) {
       const int ab = rowmap[a.row_off + u], ba = mirror[a.row_off + u];
       if (ba < 0) continue;  // a = b: zero row
@@ -1088,23 +1127,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
       r.qx = qa.x; r.qy = qa.y;
       r.pa = pab.x - (int)np; r.pb = pab.y - (int)np;
       r.ea = P->sp_energy[pab.x]; r.eb = P->sp_energy[pab.y];
-      quad_rows.push_back(r);
+      *out++ = r;
     }
-    for (int j = 0; j < a.hh; j++) {
-      const int2 pij = hh_pairs[a.hh_off + j];
-      if (pij.x >= pij.y) continue;  // i = j: zero column; i > j: the mirror of (j, i)
-      QuadCol c{};
-      c.c_ij = j; c.c_ji = hh_swap[a.hh_off + j]; c.i = pij.x; c.j = pij.y;
-      c.eij = P->sp_energy[pij.x] + P->sp_energy[pij.y];
-      quad_cols.push_back(c);
-    }
-    const int64_t rows_q = (int64_t)quad_rows.size() - a.qrow_off;
-    a.hk = (int)((int64_t)quad_cols.size() - a.qcol_off);
-    const int64_t nq = rows_q * a.hk;
-    if (nq >= ((int64_t)1 << 31) / 2) return CCDGPU_ERR_UNSUPPORTED;
-    for (int64_t q = 0; q < nq; q += kQuadPerItem)
-      quad_items.push_back({ai, (int32_t)q, (int32_t)std::min<int64_t>(nq, q + kQuadPerItem),
-                            a.hk, a.t_off, a.qrow_off, a.qcol_off});
   }
   h->host_chans = chans;
   h->n_quad_items = (int)quad_items.size();
@@ -2597,6 +2621,9 @@ int ccdgpu_kernel_profile(ccdgpu_handle *h, int32_t reps, double *ms, double *fl
     flops[k] += 4.0 * m.ph * (double)m.hp * m.hp;
     bytes[k] += 28.0 * m.ph * m.hp + 8.0 * m.hp * m.hp;
   }
+  // The small class is launched with the phhp gather ahead of it (fused path): per slab
+  // element an index, one read of t and the slab store.
+  bytes[0] += 20.0 * (double)h->n_m;
   // hh ladder: P = V_hhpp T over the pp rows and r = row dots; reads V_pphh and T, writes the
   // slice partials of P and r.  Reduction: reads the partials and V_hhhh, writes X (reference
   // layout and FP64 operand tiles) and s.

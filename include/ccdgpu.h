@@ -338,7 +338,8 @@ int ccdgpu_ladder_profile(ccdgpu_handle *h, int32_t reps, double ms[4], double f
 
 /* The other kernels of an iteration, each class launched alone `reps` times on the handle's
  * stream (after one warm-up launch): average ms per launch, FP64 flops and algorithmic bytes
- * per launch, indexed ring small (ph', hp' <= 16), ring mid (<= 32), ring large, hh ladder
+ * per launch, indexed ring small (ph', hp' <= 16; with the phhp gather that precedes the ring
+ * on the fused path), ring mid (<= 32), ring large, hh ladder
  * small (hh <= 16), hh ladder rest, one-body sums, hh-ladder slice reduction.  Amplitudes are
  * not changed (the kernels write only intermediates).  No counterpart in the reference. */
 int ccdgpu_kernel_profile(ccdgpu_handle *h, int32_t reps, double ms[7], double flops[7],
