@@ -525,7 +525,7 @@ def main():
                 if ms <= 0 or by <= 0:
                     continue
                 gbs = by / (ms / 1e3) / 1e9
-                tr = traffic.get(f"{args.config}|{v_mode}|{kname}")
+                tr = traffic.get(f"{args.config}|{v_mode}|{a}|{kname}")
                 out[fam] = {"kernel": kname, "bound": "hbm", "achieved": gbs, "peak": hbm,
                             "unit": "GB/s", "frac": gbs / hbm, "traffic": tr,
                             "algorithmic_bytes_per_launch": by, "avg_launch_ms": ms}
