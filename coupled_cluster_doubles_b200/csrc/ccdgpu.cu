@@ -1864,8 +1864,11 @@ int check_errors(ccdgpu_handle *h) {
   CK(cudaMemcpy(&e, h->err, sizeof(int32_t), cudaMemcpyDeviceToHost));
   if (e & kErrTimeout) {
     // Reported once: the handle stays usable (the timed-out iteration's amplitudes are
-    // incomplete; ccdgpu_reset or ccdgpu_set_t2 starts over).
+    // incomplete; ccdgpu_reset or ccdgpu_set_t2 starts over).  A tensor-core ladder CTA that
+    // gave up may have left the tile counter and exit ticket behind: zero them for the next
+    // launch.
     CK(cudaMemset(h->err, 0, sizeof(int32_t)));
+    if (h->tc_sched) CK(cudaMemset(h->tc_sched, 0, 2 * sizeof(int32_t)));
     return CCDGPU_ERR_TIMEOUT;
   }
   if (h->h_ctl->error & kErrNonFinite) return CCDGPU_ERR_NONFINITE;
