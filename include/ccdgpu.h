@@ -350,7 +350,7 @@ int ccdgpu_kernel_profile(ccdgpu_handle *h, int32_t reps, double ms[7], double f
  * the %globaltimer time (ns) at which its first and its last CTA started.  Kernel ids, in this
  * order: ring small, ring mid, ring large, hh ladder small, hh ladder tiled, one-body, pp
  * ladder thin, mid, wide, tensor-core pp ladder, assembly, loop control, energy, FP64 tile
- * refresh, split-K reduction, hh-ladder reduction (16). */
+ * refresh, split-K reduction, hh-ladder reduction, phhp gather (17). */
 int ccdgpu_trace_arm(ccdgpu_handle *h, int64_t iteration);
 int ccdgpu_trace_read(ccdgpu_handle *h, uint64_t *first, uint64_t *last, int32_t n);
 /* The same trace: when the last CTA of each kernel finished (%globaltimer ns; 0 for kernels
