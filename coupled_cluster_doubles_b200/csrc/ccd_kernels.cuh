@@ -874,31 +874,38 @@ constexpr int kRing16NC = 4;
 __host__ __device__ constexpr int ring16_warps(int pad) {
   return (pad / 16) * ((pad / 8 + kRing16NC - 1) / kRing16NC);
 }
+// Operand buffers: the 32 group keeps two (T', V_hpph; Y replaces V_hpph, V_hphp is read into
+// the accumulators), so that 8 CTAs share an SM; the wider groups three (T', V_hpph, V_hphp ->
+// Y), which measured faster for them.
+__host__ __device__ constexpr int ring16_bufs(int pad) { return pad <= 32 ? 2 : 3; }
 __host__ __device__ constexpr size_t ring16_smem(int pad) {
-  return (size_t)3 * pad * (pad + 4) * sizeof(double);
+  return (size_t)ring16_bufs(pad) * pad * (pad + 4) * sizeof(double);
 }
-// pre(r, c) is called for every output position of an item before its MMAs (it may start
-// loads that epi(r, c, v, slot) then uses: slot = n * 4 + the accumulator index).
-template <int PAD, int MODE, class Pre, class Epi>
+// CTAs per SM that the shared memory allows (227 KB), kept by the register budget too.
+__host__ __device__ constexpr int ring16_ctas(int pad) {
+  return (int)((227 * 1024) / ring16_smem(pad)) > 8 ? 8 : (int)((227 * 1024) / ring16_smem(pad));
+}
+// init(slot, r, c) gives the starting accumulator of every output position of an item before
+// its MMAs (it may also start loads that epi(r, c, v, slot) then uses: slot = n * 4 + the
+// accumulator index).
+template <int PAD, int MODE, class Init, class Epi>
 __device__ __forceinline__ void ring16_gemm(const double *As, const double *Bs, int warp,
-                                            const Pre &pre, const Epi &epi) {
+                                            const Init &init, const Epi &epi) {
   // MODE 0: A[m][k] = As[k][m] (k-major); MODE 1: A[m][k] = As[m][k].  B[k][n] = Bs[k][n].
   constexpr int ld = PAD + 4, N8 = PAD / 8, NCH = (N8 + kRing16NC - 1) / kRing16NC;
   constexpr int ITEMS = (PAD / 16) * NCH;
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   for (int it = warp; it < ITEMS; it += ring16_warps(PAD)) {
     const int mt = it / NCH, n0 = (it - mt * NCH) * kRing16NC;
+    double acc[kRing16NC][4];
 #pragma unroll
     for (int n = 0; n < kRing16NC; ++n) {
       const int r = 16 * mt + g, c = 8 * (n0 + n) + 2 * t;
-      pre(n * 4 + 0, r, c);
-      pre(n * 4 + 1, r, c + 1);
-      pre(n * 4 + 2, r + 8, c);
-      pre(n * 4 + 3, r + 8, c + 1);
+      acc[n][0] = init(n * 4 + 0, r, c);
+      acc[n][1] = init(n * 4 + 1, r, c + 1);
+      acc[n][2] = init(n * 4 + 2, r + 8, c);
+      acc[n][3] = init(n * 4 + 3, r + 8, c + 1);
     }
-    double acc[kRing16NC][4];
-#pragma unroll
-    for (int n = 0; n < kRing16NC; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.0;
 #pragma unroll
     for (int k16 = 0; k16 < PAD / 16; ++k16) {
       double a[8];
@@ -928,15 +935,18 @@ __device__ __forceinline__ void ring16_gemm(const double *As, const double *Bs, 
   }
 }
 template <int PAD>
-__global__ void __launch_bounds__(32 * ring16_warps(PAD))
+__global__ void __launch_bounds__(32 * ring16_warps(PAD), ring16_ctas(PAD))
 ring16_kernel(const ModInfo *__restrict__ mods, const double *__restrict__ v_hpph,
               const double *__restrict__ v_hphp, const double *__restrict__ t_phhp,
               const int32_t *__restrict__ inv, double *__restrict__ out, const Control *ctl,
               int gate) {
   if (skip_iteration(ctl, gate, PAD <= 32 ? kTrRingMid : kTrRingLarge)) return;
   extern __shared__ __align__(16) double r16[];
-  constexpr int ld = PAD + 4, NT = 32 * ring16_warps(PAD);
-  double *Ts = r16, *Vs = r16 + PAD * ld, *Ys = r16 + 2 * PAD * ld;
+  constexpr int ld = PAD + 4, NT = 32 * ring16_warps(PAD), N8 = PAD / 8;
+  constexpr int NCH = (N8 + kRing16NC - 1) / kRing16NC;
+  constexpr bool TWO = ring16_bufs(PAD) == 2;
+  static_assert((PAD / 16) * NCH == ring16_warps(PAD), "one GEMM item per warp");
+  double *Ts = r16, *Vs = r16 + PAD * ld, *Ys = TWO ? Vs : r16 + 2 * PAD * ld;
   const ModInfo m = mods[blockIdx.x];
   const int ph = m.ph, hp = m.hp;
   for (int e = threadIdx.x; e < PAD * PAD; e += NT) {
@@ -949,31 +959,57 @@ ring16_kernel(const ModInfo *__restrict__ mods, const double *__restrict__ v_hpp
       Ts[r * ld + c] = 0.0;
       Vs[r * ld + c] = 0.0;
     }
-    if (r < hp && c < hp) cp_async8(Ys + r * ld + c, v_hphp + m.y_off + (int64_t)r * hp + c);
-    else Ys[r * ld + c] = 0.0;
+    if constexpr (!TWO) {
+      if (r < hp && c < hp) cp_async8(Ys + r * ld + c, v_hphp + m.y_off + (int64_t)r * hp + c);
+      else Ys[r * ld + c] = 0.0;
+    }
   }
   cp_async_commit();
-  cp_async_wait<0>();
-  __syncthreads();
   const int warp = threadIdx.x >> 5;
-  // Y = V_hphp + 0.5 V_hpph T' with V_hpph[i][k] = Vt[k][i]; each Y element has one owner lane.
-  ring16_gemm<PAD, 0>(
-      Vs, Ts, warp, [](int, int, int) {},
-      [&](int r, int c, double v, int) { Ys[r * ld + c] = 0.5 * v + Ys[r * ld + c]; });
+  if constexpr (TWO) {
+    // 2 Y = 2 V_hphp + V_hpph T' (V_hpph[i][k] = Vt[k][i]): the accumulators start from
+    // 2 V_hphp (global loads issued while the stage lands) and are halved on the way into the
+    // V_hpph buffer, once every warp is done reading it.
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int mt = warp / NCH, n0 = (warp - mt * NCH) * kRing16NC;
+    double y[4 * kRing16NC];
+    cp_async_wait<0>();
+    __syncthreads();
+    ring16_gemm<PAD, 0>(
+        Vs, Ts, warp,
+        [&](int, int r, int c) {
+          return (r < hp && c < hp) ? 2.0 * __ldg(v_hphp + m.y_off + (int64_t)r * hp + c) : 0.0;
+        },
+        [&](int, int, double v, int slot) { y[slot] = 0.5 * v; });
+    __syncthreads();
+#pragma unroll
+    for (int slot = 0; slot < 4 * kRing16NC; ++slot) {
+      const int n = slot >> 2, q = slot & 3;
+      if (n0 + n < N8)
+        Ys[(16 * mt + g + 8 * (q >> 1)) * ld + 8 * (n0 + n) + 2 * t + (q & 1)] = y[slot];
+    }
+  } else {
+    // Y = V_hphp + 0.5 V_hpph T' in the third buffer; each Y element has one owner lane.
+    cp_async_wait<0>();
+    __syncthreads();
+    ring16_gemm<PAD, 0>(
+        Vs, Ts, warp, [](int, int, int) { return 0.0; },
+        [&](int r, int c, double v, int) { Ys[r * ld + c] = 0.5 * v + Ys[r * ld + c]; });
+  }
   __syncthreads();
   // R = T' Y, stored for r < ph', c < hp' (through the inverse ai_jb table on the fused path);
   // the destinations are loaded before the MMAs, so the stores do not wait on them.
-  int64_t dst[4 * kRing16NC];
+  int32_t dst[4 * kRing16NC];
   ring16_gemm<PAD, 1>(
       Ts, Ys, warp,
       [&](int slot, int r, int c) {
-        const int64_t p = m.m_off + (int64_t)r * hp + c;
-        dst[slot] = (r < ph && c < hp) ? (inv ? (int64_t)__ldg(inv + p) : p) : -1;
+        const int32_t p = (int32_t)(m.m_off + (int64_t)r * hp + c);
+        dst[slot] = (r < ph && c < hp) ? (inv ? __ldg(inv + p) : p) : -1;
+        return 0.0;
       },
       [&](int, int, double v, int slot) {
         if (dst[slot] >= 0) out[dst[slot]] = v;
       });
-  __syncthreads();
   trace_end(ctl, PAD <= 32 ? kTrRingMid : kTrRingLarge);
 }
 
