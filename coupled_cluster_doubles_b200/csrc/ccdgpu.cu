@@ -493,6 +493,64 @@ int copy_runs_to_device(ccdgpu_handle *h, char *dst, const std::vector<const cha
   return CCDGPU_OK;
 }
 
+// Device bytes [src, src + total) to host memory dst, through the staging buffers for large
+// totals: chunk k + 1 is copied by the copy engine into one buffer while host threads move
+// chunk k from the other into dst (a pageable device-to-host copy runs at about half of that).
+// Returns after every byte has arrived.
+int copy_from_device(ccdgpu_handle *h, char *dst, const char *src, size_t total) {
+  if (!total) return CCDGPU_OK;
+  Staging &S = staging();
+  std::unique_lock<std::mutex> lock(S.mu, std::defer_lock);
+  if (total >= kStageMin && lock.try_lock()) {
+    if (!S.buf && !S.failed &&
+        cudaHostAlloc(reinterpret_cast<void **>(&S.buf), 2 * kStageChunk,
+                      cudaHostAllocPortable) != cudaSuccess) {
+      (void)cudaGetLastError();
+      S.buf = nullptr;
+      S.failed = true;
+    }
+    if (S.buf) {
+      cudaEvent_t ev[2] = {nullptr, nullptr};
+      cudaError_t e = cudaSuccess;
+      for (int k = 0; k < 2 && e == cudaSuccess; k++)
+        e = cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming);
+      const int threads = std::max(1, std::min(omp_get_max_threads(), 16));
+      const size_t nchunks = (total + kStageChunk - 1) / kStageChunk;
+      auto issue = [&](size_t c) {
+        const size_t off = c * kStageChunk, n = std::min(kStageChunk, total - off);
+        cudaError_t r = cudaMemcpyAsync(S.buf + (c & 1) * kStageChunk, src + off, n,
+                                        cudaMemcpyDeviceToHost, h->s0);
+        if (r == cudaSuccess) r = cudaEventRecord(ev[c & 1], h->s0);
+        return r;
+      };
+      if (e == cudaSuccess) e = issue(0);
+      for (size_t c = 0; c < nchunks && e == cudaSuccess; c++) {
+        if (c + 1 < nchunks && (e = issue(c + 1)) != cudaSuccess) break;
+        if ((e = cudaEventSynchronize(ev[c & 1])) != cudaSuccess) break;
+        const size_t off = c * kStageChunk, n = std::min(kStageChunk, total - off);
+        const char *stage = S.buf + (c & 1) * kStageChunk;
+        const size_t piece = std::max<size_t>(size_t(64) << 10, (n + threads - 1) / threads);
+#pragma omp parallel for num_threads(threads) schedule(static)
+        for (int64_t x = 0; x < (int64_t)((n + piece - 1) / piece); x++) {
+          const size_t lo = (size_t)x * piece;
+          std::memcpy(dst + off + lo, stage + lo, std::min(piece, n - lo));
+        }
+      }
+      (void)cudaStreamSynchronize(h->s0);
+      for (int k = 0; k < 2; k++)
+        if (ev[k]) cudaEventDestroy(ev[k]);
+      if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        return CCDGPU_ERR_CUDA;
+      }
+      return CCDGPU_OK;
+    }
+  }
+  CK(cudaMemcpyAsync(dst, src, total, cudaMemcpyDeviceToHost, h->s0));
+  CK(cudaStreamSynchronize(h->s0));
+  return CCDGPU_OK;
+}
+
 int copy_to_device(ccdgpu_handle *h, void *dst, const void *src, size_t bytes) {
   return copy_runs_to_device(h, static_cast<char *>(dst), {static_cast<const char *>(src)},
                              {bytes});
@@ -2310,9 +2368,8 @@ int ccdgpu_get_t2(ccdgpu_handle *h, double *t2, uint64_t n) {
   if (rc) return rc;
   const double *src = h->t[h->h_ctl->parity];
   if (h->opt.path == CCDGPU_PATH_TABLES) src = h->t[1];
-  CK(cudaMemcpyAsync(t2, src, n * 8, cudaMemcpyDeviceToHost, h->s0));
-  CK(cudaStreamSynchronize(h->s0));
-  return CCDGPU_OK;
+  return copy_from_device(h, reinterpret_cast<char *>(t2), reinterpret_cast<const char *>(src),
+                          n * 8);
 }
 
 int ccdgpu_step(ccdgpu_handle *h, double mixing, double *e_corr) {
