@@ -81,6 +81,10 @@ struct ModelDev {
   int32_t R, W;
   double g;            // pairing strength
   double Lb;           // PNM box length, (N / rho)^(1/3)
+  // Electron gas with |n_i| <= 63: per orbital its momentum components biased by 64 in bytes
+  // 0-2 and its spin in byte 3, so that a matrix element reads four words instead of twelve
+  // quantum numbers (null otherwise).
+  const uint32_t *ocode;
 };
 
 __device__ __forceinline__ double direct_pnm_dev(const int32_t *qi, const int32_t *qj,
@@ -110,6 +114,22 @@ __device__ __forceinline__ double direct_pnm_dev(const int32_t *qi, const int32_
   const double is_pt = d_s * iso_ex;
   return 0.5 * (vr + 0.5 * vt + 0.5 * vs) * is_it + 0.25 * (vt - vs) * ps_it -
          0.5 * (vr + 0.5 * vt + 0.5 * vs) * ps_pt - 0.25 * (vt - vs) * is_pt;
+}
+
+// The electron gas's <ab|v|cd> from the orbital codes (ModelDev::ocode): the same table
+// entries and the same difference as tbme_dev, so the same value.
+__device__ __forceinline__ double eg_tbme_code(const ModelDev &m, uint32_t a, uint32_t b,
+                                               uint32_t c, uint32_t d) {
+  auto vq = [&](uint32_t x, uint32_t y) {
+    const int dx = (int)(x & 0xff) - (int)(y & 0xff);
+    const int dy = (int)((x >> 8) & 0xff) - (int)((y >> 8) & 0xff);
+    const int dz = (int)((x >> 16) & 0xff) - (int)((y >> 16) & 0xff);
+    return m.vq[((dx + m.R) * m.W + (dy + m.R)) * m.W + (dz + m.R)];
+  };
+  const uint32_t sa = a >> 24, sb = b >> 24, sc = c >> 24, sd = d >> 24;
+  const double dir = (sa == sc && sb == sd) ? vq(a, c) : 0.;
+  const double exc = (sa == sd && sb == sc) ? vq(a, d) : 0.;
+  return dir - exc;
 }
 
 // <ab|v|cd> for orbitals a, b, c, d of one regular channel (momentum is conserved).
@@ -242,33 +262,71 @@ __global__ void normal_order_kernel(ModelDev m, const double *__restrict__ bare,
   }
 }
 
-// One CTA per packed row u of a channel (items as for tile_v_kernel): the FP64 ladder tile
-// element and, for a mixed handle (nt > 0), its nt bf16 terms.
-__global__ void gen_v_kernel(const ChanInfo *__restrict__ chans, const int2 *__restrict__ items,
-                             const int32_t *__restrict__ rowmap, const int32_t *__restrict__ kcol,
-                             const int2 *__restrict__ pp_pairs, ModelDev m,
-                             double *__restrict__ v_t, __nv_bfloat16 *__restrict__ v_tc,
-                             int64_t tc_stride, int nt) {
-  const int2 it = items[blockIdx.x];
+
+// V_pppp generated straight into the ladders' operand images, one CTA per image chunk, so that
+// each CTA writes one contiguous block (the chunk's elements in image order; padding rows and
+// K columns past pk get zeros).  FP64 ladder: items (channel, row tile, 16-deep K chunk), block
+// of ar x kBK doubles, k-major (mid and wide classes) or XOR-swizzled rows (thin class).
+// Tensor-core ladder: items (channel, 128-row tile, 32-deep K chunk), block of rg x kTcGroup
+// bf16 per term in 8 x 8 core matrices.
+__global__ void __launch_bounds__(256)
+gen_v_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restrict__ items,
+                    const int32_t *__restrict__ rowmap, const int32_t *__restrict__ kcol,
+                    const int2 *__restrict__ pp_pairs, ModelDev m, double *__restrict__ v_t) {
+  const int4 it = items[blockIdx.x];
   const ChanInfo ch = chans[it.x];
-  const int u = it.y;
-  const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + u]];
-  const int mt = u / ch.bm, rows = min(ch.bm, ch.pr - mt * ch.bm);
-  const int ar = ladder_arows(ch.nb, rows);
-  const int64_t tb = ch.vkt_base + (int64_t)mt * ladder_arows_full(ch.nb) * ch.nkc * kBK;
-  const int mtc = u >> 7, r = u & 127;
-  const int rg = (min(kTcBM, ch.pr - mtc * kTcBM) + 7) >> 3;
-  const int64_t tbc = ch.vtc_base + (int64_t)mtc * kTcBM * ch.nkct * kTcKC;
-  for (int w = threadIdx.x; w < ch.pk; w += blockDim.x) {
-    const int2 cd = pp_pairs[ch.pp_off + kcol[ch.pk_off + w]];
-    const double v = tbme_dev(m, ab.x, ab.y, cd.x, cd.y);
-    v_t[tb + (int64_t)(w / kBK) * ar * kBK + ladder_aoff(ch.nb, ar, u - mt * ch.bm, w % kBK)] = v;
-    if (nt) {
-      __nv_bfloat16 hv[3];
-      split_bf16(v, hv, nt);
-      const int64_t o = tbc + (int64_t)(w >> 5) * rg * kTcGroup + tc_off(r, w & 31);
-      for (int p = 0; p < nt; ++p) v_tc[p * tc_stride + o] = hv[p];
+  const int mt = it.y, kc = it.z;
+  const int rows = min(ch.bm, ch.pr - mt * ch.bm), ar = ladder_arows(ch.nb, rows);
+  const bool kmajor = ladder_kmajor(ch.nb);
+  double *out = v_t + ch.vkt_base + (int64_t)mt * ladder_arows_full(ch.nb) * ch.nkc * kBK +
+                (int64_t)kc * ar * kBK;
+  for (int e = threadIdx.x; e < ar * kBK; e += blockDim.x) {
+    int r, k;
+    if (kmajor) {
+      k = e / ar;
+      r = e - k * ar;
+    } else {
+      r = e >> 4;
+      k = (e & 15) ^ (r & 15);  // swzA(r, k) = 16 r + (k ^ (r & 15))
     }
+    const int u = mt * ch.bm + r, w = kc * kBK + k;
+    double v = 0.0;
+    if (r < rows && w < ch.pk) {
+      const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + u]];
+      const int2 cd = pp_pairs[ch.pp_off + kcol[ch.pk_off + w]];
+      v = m.ocode ? eg_tbme_code(m, m.ocode[ab.x], m.ocode[ab.y], m.ocode[cd.x], m.ocode[cd.y])
+                  : tbme_dev(m, ab.x, ab.y, cd.x, cd.y);
+    }
+    out[e] = v;
+  }
+}
+template <int NT>
+__global__ void __launch_bounds__(256)
+gen_v_tc_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restrict__ items,
+                       const int32_t *__restrict__ rowmap, const int32_t *__restrict__ kcol,
+                       const int2 *__restrict__ pp_pairs, ModelDev m,
+                       __nv_bfloat16 *__restrict__ v_tc, int64_t tc_stride) {
+  const int4 it = items[blockIdx.x];
+  const ChanInfo ch = chans[it.x];
+  const int mt = it.y, kc = it.z;
+  const int rows = min(kTcBM, ch.pr - mt * kTcBM), rg = (rows + 7) >> 3;
+  const int64_t base = ch.vtc_base + (int64_t)mt * kTcBM * ch.nkct * kTcKC + (int64_t)kc * rg * kTcGroup;
+  for (int e = threadIdx.x; e < rg * kTcGroup; e += blockDim.x) {
+    // e = (r / 8) kTcGroup + (k / 8) 64 + (r % 8) 8 + k % 8 (tc_off)
+    const int rem = e & (kTcGroup - 1);
+    const int r = (e / kTcGroup) * 8 + ((rem >> 3) & 7), k = (rem >> 6) * 8 + (rem & 7);
+    const int u = mt * kTcBM + r, w = kc * kTcKC + k;
+    double v = 0.0;
+    if (r < rows && w < ch.pk) {
+      const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + u]];
+      const int2 cd = pp_pairs[ch.pp_off + kcol[ch.pk_off + w]];
+      v = m.ocode ? eg_tbme_code(m, m.ocode[ab.x], m.ocode[ab.y], m.ocode[cd.x], m.ocode[cd.y])
+                  : tbme_dev(m, ab.x, ab.y, cd.x, cd.y);
+    }
+    __nv_bfloat16 hv[NT];
+    split_bf16_n<NT>(v, hv);
+#pragma unroll
+    for (int p = 0; p < NT; ++p) v_tc[p * tc_stride + base + e] = hv[p];
   }
 }
 

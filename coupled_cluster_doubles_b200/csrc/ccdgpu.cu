@@ -1124,8 +1124,9 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   h->n_p = o_p[h->npart];
   if (h->n_h != n_t || h->n_p != n_t) return CCDGPU_ERR_BAD_TABLE;
   // Three-body V of the table path: from the host, or generated with the other V blocks when
-  // the problem carries none of them.
-  const bool gen_v3 = gen_v && !P->v_h_hpp && !P->v_phh_p;
+  // the problem carries none of them and the handle runs the table path (the fused path reads
+  // none: its one-body sums come from the hh ladder's row dots).
+  const bool gen_v3 = gen_v && !P->v_h_hpp && !P->v_phh_p && h->opt.path == CCDGPU_PATH_TABLES;
   h->have_3body = (P->v_h_hpp && P->v_phh_p) || gen_v3;
 
   h->host_chans = chans;
@@ -1319,6 +1320,19 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   RawIndex *raw_idx = nullptr;
   int32_t *counts = nullptr;
   int2 *d_vrows = nullptr, *d_mod_dims = nullptr;
+  int4 *d_gv_items = nullptr, *d_gvt_items = nullptr;
+  // Generated V_pppp: one item per operand-image chunk (channel, row tile, K chunk).
+  std::vector<int4> gv_items, gvt_items;
+  if (on_the_fly) {
+    for (int ai = 0; ai < h->n_act; ai++) {
+      const ChanInfo &a = chans[ai];
+      for (int mt = 0; mt < a.nmt; mt++)
+        for (int kc = 0; kc < a.nkc; kc++) gv_items.push_back(make_int4(ai, mt, kc, 0));
+      if (h->nt && !h->tc_gen)
+        for (int mt = 0; mt < (int)ceil_div(a.pr, kTcBM); mt++)
+          for (int kc = 0; kc < a.nkct; kc++) gvt_items.push_back(make_int4(ai, mt, kc, 0));
+    }
+  }
   int64_t *d_vraw_off = nullptr, *d_o_m = nullptr;
   // Derived tables: per-pair block offsets and the modified-channel lookup of (particle, hole)
   // pairs, built here from the ph' / hp' maps (O(npart * np)).
@@ -1364,15 +1378,18 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   }
   sc.add(&vraw, vraw_tot); sc.add(&hhpp_raw, gen_v ? 0 : n_t);
   sc.add(&hpph_raw, gen_v ? 0 : h->n_m);
-  sc.add(&counts, (size_t)5 * n_t); sc.add(&d_vrows, vrows.size()); 
+  sc.add(&counts, (size_t)5 * n_t); sc.add(&d_vrows, vrows.size());
+  sc.add(&d_gv_items, gv_items.size()); sc.add(&d_gvt_items, gvt_items.size());
   sc.add(&d_vraw_off, vraw_off.size()); sc.add(&d_mod_dims, mod_dims.size()); sc.add(&d_o_m, o_m.size());
   // The model on the device (on-the-fly V, E_ref and normal ordering): quantum numbers and
   // (electron gas) the direct Coulomb term by momentum transfer, computed here with the
   // reference's expression (ElectronGasSPBasis.cpp:424-448).  Kept for the handle's lifetime.
   ModelDev md{};
   std::vector<double> vq;
+  std::vector<uint32_t> ocode;
   int32_t *d_qn = nullptr;
   double *d_vq = nullptr;
+  uint32_t *d_ocode = nullptr;
   if (model_ok) {
     md.kind = M->kind;
     md.stride = M->qn_stride;
@@ -1399,18 +1416,30 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
             const double v = rel < 1.e-5 ? 0.0 : prefactor * 4 * M_PI / (rel + mu * mu);
             vq[((size_t)(dx + md.R) * md.W + (dy + md.R)) * md.W + (dz + md.R)] = v;
           }
+      if (nmax <= 63) {
+        ocode.resize(nsp);
+        for (uint64_t o = 0; o < nsp; o++) {
+          const int32_t *q = M->qn + o * M->qn_stride;
+          ocode[o] = (uint32_t)(q[0] + 64) | ((uint32_t)(q[1] + 64) << 8) |
+                     ((uint32_t)(q[2] + 64) << 16) | ((uint32_t)(q[3] & 0xff) << 24);
+        }
+      }
     }
     Arena mr;
     mr.add(&d_qn, (size_t)nsp * M->qn_stride);
     mr.add(&d_vq, vq.size());
+    mr.add(&d_ocode, ocode.size());
     mr.add(&h->eps_io, 2 * nsp + 1);
     TRY(mr.commit(h));
     CK(cudaMemcpyAsync(d_qn, M->qn, (size_t)nsp * M->qn_stride * sizeof(int32_t),
                        cudaMemcpyHostToDevice, h->s0));
     if (!vq.empty())
       CK(cudaMemcpyAsync(d_vq, vq.data(), vq.size() * 8, cudaMemcpyHostToDevice, h->s0));
+    if (!ocode.empty())
+      CK(cudaMemcpyAsync(d_ocode, ocode.data(), ocode.size() * 4, cudaMemcpyHostToDevice, h->s0));
     md.qn = d_qn;
     md.vq = d_vq;
+    md.ocode = ocode.empty() ? nullptr : d_ocode;
     h->md = md;
     h->has_model = true;
   }
@@ -1434,6 +1463,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   TRY(put(h->rowmap, rowmap)); TRY(put(h->mirror, mirror)); TRY(put(h->pk_idx, pk_idx));
   TRY(put(h->o_h, o_h)); TRY(put(h->o_p, o_p));
   TRY(put(d_vrows, vrows)); TRY(put(d_vraw_off, vraw_off));
+  TRY(put(d_gv_items, gv_items)); TRY(put(d_gvt_items, gvt_items));
   TRY(put(d_mod_dims, mod_dims)); TRY(put(d_o_m, o_m));
   CK(cudaMemcpyAsync(h->eps, P->sp_energy, nsp * 8, cudaMemcpyHostToDevice, h->s0));
 
@@ -1552,11 +1582,19 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   }
   if (!vrows.empty()) {
     if (on_the_fly) {
-      // FP64 tiles, and the bf16 images unless the tensor-core ladder generates its own V.
-      gen_v_kernel<<<(unsigned)vrows.size(), 128, 0, h->s0>>>(h->chans, d_vrows, h->rowmap,
-                                                              h->kcol, h->pp_pairs, md, h->v_t,
-                                                              h->v_tc, h->n_vtc,
-                                                              h->tc_gen ? 0 : h->nt);
+      // FP64 tiles, and the bf16 images unless the tensor-core ladder generates its own V: one
+      // CTA per image chunk.
+      if (!gv_items.empty()) {
+        gen_v_chunks_kernel<<<(unsigned)gv_items.size(), 256, 0, h->s0>>>(
+            h->chans, d_gv_items, h->rowmap, h->kcol, h->pp_pairs, md, h->v_t);
+        CK(cudaGetLastError());
+      }
+      if (h->nt && !h->tc_gen && !gvt_items.empty()) {
+        auto kern = h->nt == 3 ? gen_v_tc_chunks_kernel<3> : gen_v_tc_chunks_kernel<2>;
+        kern<<<(unsigned)gvt_items.size(), 256, 0, h->s0>>>(h->chans, d_gvt_items, h->rowmap,
+                                                           h->kcol, h->pp_pairs, md, h->v_tc,
+                                                           h->n_vtc);
+      }
     } else {
       tile_v_kernel<<<(unsigned)vrows.size(), 128, 0, h->s0>>>(h->chans, d_vrows, h->rowmap,
                                                                h->kcol, d_vraw_off, vraw, h->v_t);

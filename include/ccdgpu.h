@@ -247,7 +247,10 @@ int ccdgpu_solve_batch(ccdgpu_handle *const *handles, int32_t n, double tol, int
 int ccdgpu_energy_history(ccdgpu_handle *h, double *out, int64_t cap, int64_t *n_out);
 
 /* Stage entry points with the reference's names, for stage-level parity tests and for a
- * host that keeps the reference loop structure.  They act on the handle's device chains. */
+ * host that keeps the reference loop structure.  They act on the handle's device chains.  The
+ * one-body stages need the three-body V blocks (v_h_hpp, v_phh_p): given by the problem, or
+ * generated on the device for a handle of the table path; otherwise they return
+ * CCDGPU_ERR_UNSUPPORTED. */
 int ccdgpu_calc_t2diff_p2_p1hh(ccdgpu_handle *h);   /* calc.cpp:27-43 */
 int ccdgpu_calc_t2diff_h2pp_h1(ccdgpu_handle *h);   /* calc.cpp:91-107 */
 int ccdgpu_calc_t2diff_phhp(ccdgpu_handle *h);      /* calc.cpp:315-339 */
