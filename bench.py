@@ -455,6 +455,7 @@ def main():
     h2d = _problem_bytes(system_e2e, with_v_pppp=stored, with_tables=False, with_v=stored)
     phase_s = np.zeros(4)  # create, solve (graph capture included), T2 read-back, destroy
     create_ms = np.zeros(5)  # ccdgpu_create by phase (host metadata, uploads, device set-up, schedules, all)
+    graph_ms = 0.0  # the solve's building of its device-loop graphs
     for k in range(args.warmup + args.steps):
         t0 = time.perf_counter()
         s2 = CCDSolver(system_e2e, device=local, path=args.path, precision=PRECISIONS[arms[0]],
@@ -464,6 +465,8 @@ def main():
             create_ms += np.array(s2.profile()["ms_create"])
         r2 = s2.solve(tol=tol, max_iters=MAX_ITERS, mixing=MIXING)
         tb = time.perf_counter()
+        if k >= args.warmup:
+            graph_ms += s2.profile()["ms_loop_graph"]
         s2.t2(host_t2)
         tc = time.perf_counter()
         s2.close()
@@ -623,7 +626,8 @@ def main():
                                                   (1e3 * phase_s / args.steps).round(3).tolist())),
                     "rank0_create_ms_by_phase": dict(zip(
                         ["host_metadata", "alloc_upload", "device_setup", "schedules", "total"],
-                        (create_ms / args.steps).round(3).tolist()))},
+                        (create_ms / args.steps).round(3).tolist())),
+                    "rank0_solve_loop_graph_build_ms": round(graph_ms / args.steps, 3)},
             "roofline": ({**roof[head][dominant], "family": dominant, "peak_source": peak_kind}
                          if dominant else None),
             "gpu_launches": int(t["launches"]),

@@ -77,7 +77,8 @@ class Result(ctypes.Structure):
 class Profile(ctypes.Structure):
     _fields_ = [("ms_ladder", c_dbl), ("ms_hh_ladder", c_dbl), ("ms_ring", c_dbl),
                 ("ms_onebody", c_dbl), ("ms_assemble", c_dbl), ("ms_total", c_dbl),
-                ("launches", c_i64), ("iterations", c_i64), ("ms_create", c_dbl * 5)]
+                ("launches", c_i64), ("iterations", c_i64), ("ms_create", c_dbl * 5),
+                ("ms_loop_graph", c_dbl)]
 
 
 _host = None

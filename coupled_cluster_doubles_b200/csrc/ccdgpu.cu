@@ -41,8 +41,16 @@ struct DevBuf {
 
 }  // namespace
 
+// A handle's streams and events (see the pool below).
+struct StreamSet {
+  int dev = -1;
+  cudaStream_t s[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev[16] = {};
+};
+
 struct ccdgpu_handle {
   ccdgpu_options opt{};
+  StreamSet sset;  // the streams and events below, from the process-wide pool
   cudaStream_t s0 = nullptr, s1 = nullptr, s2 = nullptr, s3 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork2 = nullptr, ev_join2 = nullptr;
   cudaEvent_t ev_fork3 = nullptr, ev_join3 = nullptr;  // one-body sums beside the pp ladder
@@ -87,6 +95,7 @@ struct ccdgpu_handle {
   int32_t *flat = nullptr;
   int32_t *inv4 = nullptr;   // phhp position -> pphh element (inverse of the ai_jb table)
   double create_ms[5] = {};   // ccdgpu_profile::ms_create
+  double loop_graph_ms = 0;   // ccdgpu_profile::ms_loop_graph
   double *d_ring = nullptr;  // fused path: ring result R in pphh order
   int64_t *o_h = nullptr, *o_p = nullptr;
   double *v_h_hpp = nullptr, *v_phh_p = nullptr;
@@ -347,6 +356,74 @@ void ctl_release(Control *c) {
   pool.free.push_back(c);
 }
 
+// Process-wide pool of the streams and events a handle uses (four streams, sixteen events per
+// set), by device: a create takes a set that a destroyed handle gave back instead of creating
+// twenty objects, and a destroy returns its set (after its streams are idle) instead of
+// destroying them.  Emptied by ccdgpu_release_cached_memory.
+struct StreamPool {
+  std::mutex mu;
+  std::vector<StreamSet> sets;
+};
+StreamPool &stream_pool() {
+  static StreamPool p;
+  return p;
+}
+void destroy_set(StreamSet &ss) {
+  for (cudaEvent_t &e : ss.ev)
+    if (e) cudaEventDestroy(e);
+  for (cudaStream_t &st : ss.s)
+    if (st) cudaStreamDestroy(st);
+}
+// A set for the current device: from the pool, else new (events 0-9 time, the rest only order).
+cudaError_t acquire_set(StreamSet &ss) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  {
+    StreamPool &P = stream_pool();
+    std::lock_guard<std::mutex> lock(P.mu);
+    for (size_t i = 0; i < P.sets.size(); i++)
+      if (P.sets[i].dev == dev) {
+        ss = P.sets[i];
+        P.sets.erase(P.sets.begin() + i);
+        return cudaSuccess;
+      }
+  }
+  ss.dev = dev;
+  for (int k = 0; k < 4 && e == cudaSuccess; k++)
+    e = cudaStreamCreateWithFlags(&ss.s[k], cudaStreamNonBlocking);
+  for (int k = 0; k < 16 && e == cudaSuccess; k++)
+    e = k < 10 ? cudaEventCreate(&ss.ev[k]) : cudaEventCreateWithFlags(&ss.ev[k], cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    destroy_set(ss);
+    ss = StreamSet{};
+  }
+  return e;
+}
+void release_set(StreamSet &ss) {
+  if (ss.dev < 0) return;
+  StreamPool &P = stream_pool();
+  std::lock_guard<std::mutex> lock(P.mu);
+  P.sets.push_back(ss);
+  ss = StreamSet{};
+}
+void release_stream_pool() {
+  std::vector<StreamSet> drop;
+  {
+    StreamPool &P = stream_pool();
+    std::lock_guard<std::mutex> lock(P.mu);
+    drop.swap(P.sets);
+  }
+  int cur = 0;
+  if (cudaGetDevice(&cur) != cudaSuccess) cur = -1;
+  for (StreamSet &ss : drop) {
+    cudaSetDevice(ss.dev);
+    destroy_set(ss);
+  }
+  if (cur >= 0) cudaSetDevice(cur);
+  (void)cudaGetLastError();
+}
+
 void release(ccdgpu_handle *h) {
   if (!h) return;
   // Cached blocks are handed to other handles: nothing of this one may still run on them.
@@ -362,18 +439,9 @@ void release(ccdgpu_handle *h) {
   h->tile_mem = nullptr;
   if (h->h_ctl) ctl_release(h->h_ctl);
   h->h_ctl = nullptr;
-  for (auto &e : h->ev)
-    if (e) cudaEventDestroy(e);
-  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
-  if (h->ev_join) cudaEventDestroy(h->ev_join);
-  if (h->ev_fork2) cudaEventDestroy(h->ev_fork2);
-  if (h->ev_join2) cudaEventDestroy(h->ev_join2);
-  if (h->s2) cudaStreamDestroy(h->s2);
-  if (h->ev_fork3) cudaEventDestroy(h->ev_fork3);
-  if (h->ev_join3) cudaEventDestroy(h->ev_join3);
-  if (h->s3) cudaStreamDestroy(h->s3);
-  if (h->s1) cudaStreamDestroy(h->s1);
-  if (h->s0) cudaStreamDestroy(h->s0);
+  // The streams are idle (synchronised above): their set goes back to the pool.
+  if (cudaGetLastError() == cudaSuccess) release_set(h->sset);
+  else destroy_set(h->sset);
 }
 
 // Bump allocator over one device allocation (256-byte aligned pieces).
@@ -2074,6 +2142,7 @@ int capture_loop_graph(ccdgpu_handle *h, bool mixed, cudaGraphExec_t *exec) {
 // or without programmatic launches inside them, retried without) leaves the batched replay.
 void ready_loop_graphs(ccdgpu_handle *h) {
   if (h->loop_state) return;
+  const auto t0 = std::chrono::steady_clock::now();
   for (int attempt = 0; attempt < 2 && h->loop_state == 0; attempt++) {
     t_pdl = attempt == 0;
     int rc = capture_loop_graph(h, false, &h->loop64);
@@ -2088,6 +2157,7 @@ void ready_loop_graphs(ccdgpu_handle *h) {
   }
   t_pdl = true;
   if (h->loop_state == 0) h->loop_state = -1;
+  h->loop_graph_ms = ms_since(t0);
 }
 
 // One table-path iteration: exactly the reference loop body.
@@ -2162,17 +2232,14 @@ int ccdgpu_create(const ccdgpu_problem *prob, const ccdgpu_options *opt, ccdgpu_
   if (e != cudaSuccess || ndev == 0) { (void)cudaGetLastError(); delete h; return CCDGPU_ERR_NO_DEVICE; }
   if (h->opt.device < 0 || h->opt.device >= ndev) { delete h; return CCDGPU_ERR_INVALID_ARGUMENT; }
   int rc = cuda_status(cudaSetDevice(h->opt.device));
-  if (!rc) rc = cuda_status(cudaStreamCreateWithFlags(&h->s0, cudaStreamNonBlocking));
-  if (!rc) rc = cuda_status(cudaStreamCreateWithFlags(&h->s1, cudaStreamNonBlocking));
-  if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
-  if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
-  if (!rc) rc = cuda_status(cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking));
-  if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->ev_fork2, cudaEventDisableTiming));
-  if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->ev_join2, cudaEventDisableTiming));
-  if (!rc) rc = cuda_status(cudaStreamCreateWithFlags(&h->s3, cudaStreamNonBlocking));
-  if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->ev_fork3, cudaEventDisableTiming));
-  if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->ev_join3, cudaEventDisableTiming));
-  for (int i = 0; i < 10 && !rc; i++) rc = cuda_status(cudaEventCreate(&h->ev[i]));
+  if (!rc) rc = cuda_status(acquire_set(h->sset));
+  if (!rc) {
+    h->s0 = h->sset.s[0]; h->s1 = h->sset.s[1]; h->s2 = h->sset.s[2]; h->s3 = h->sset.s[3];
+    for (int i = 0; i < 10; i++) h->ev[i] = h->sset.ev[i];
+    h->ev_fork = h->sset.ev[10]; h->ev_join = h->sset.ev[11];
+    h->ev_fork2 = h->sset.ev[12]; h->ev_join2 = h->sset.ev[13];
+    h->ev_fork3 = h->sset.ev[14]; h->ev_join3 = h->sset.ev[15];
+  }
   if (!rc) rc = build(h, prob);
   if (!rc) rc = set_ctl(h, 0, 0.0, 100, 0.5, true);
   if (!rc) rc = ccdgpu_trace_arm(h, -1);
@@ -2182,7 +2249,10 @@ int ccdgpu_create(const ccdgpu_problem *prob, const ccdgpu_options *opt, ccdgpu_
   return CCDGPU_OK;
 }
 
-void ccdgpu_release_cached_memory(void) { release_cache(-1); }
+void ccdgpu_release_cached_memory(void) {
+  release_cache(-1);
+  release_stream_pool();
+}
 
 void ccdgpu_destroy(ccdgpu_handle *h) {
   if (!h) return;
@@ -2685,6 +2755,7 @@ int ccdgpu_get_profile(ccdgpu_handle *h, ccdgpu_profile *prof) {
   *prof = h->prof;
   prof->launches = h->launches;
   for (int k = 0; k < 5; k++) prof->ms_create[k] = h->create_ms[k];
+  prof->ms_loop_graph = h->loop_graph_ms;
   return CCDGPU_OK;
 }
 int ccdgpu_enable_profiling(ccdgpu_handle *h, int32_t on) {

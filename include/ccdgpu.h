@@ -290,6 +290,8 @@ typedef struct ccdgpu_profile {
    * operand images) until they finish, [3] kernel attributes and ladder schedules, [4] the
    * whole call. */
   double ms_create[5];
+  double ms_loop_graph;  /* host time of building the device solve loop's graphs (capture and
+                            instantiation, on the handle's first device-loop solve) */
 } ccdgpu_profile;
 int ccdgpu_get_profile(ccdgpu_handle *h, ccdgpu_profile *prof);
 /* When on, ccdgpu_solve runs the fused iteration without graph capture and brackets each
