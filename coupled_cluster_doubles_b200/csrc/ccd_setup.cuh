@@ -330,6 +330,33 @@ gen_v_tc_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restric
   }
 }
 
+// The fused assembly's row table (one CTA per active channel): for each packed row u with
+// a < b (row ab, mirror row ba), at the row's index among those rows (its K index qx), the
+// offsets of rows ab and ba in the channel block, its operand-image indices, the particle
+// indices and energies.
+__global__ void __launch_bounds__(256)
+quad_rows_kernel(const ChanInfo *__restrict__ chans, const int32_t *__restrict__ rowmap,
+                 const int32_t *__restrict__ mirror, const int2 *__restrict__ pk_idx,
+                 const int2 *__restrict__ pp_pairs, const double *__restrict__ eps, int np,
+                 QuadRow *__restrict__ out) {
+  const ChanInfo ch = chans[blockIdx.x];
+  for (int u = threadIdx.x; u < ch.pr; u += blockDim.x) {
+    const int ab = rowmap[ch.row_off + u], ba = mirror[ch.row_off + u];
+    if (ba < 0) continue;  // a = b: zero row
+    const int2 q = pk_idx[ch.pp_off + ab], pab = pp_pairs[ch.pp_off + ab];
+    QuadRow r;
+    r.o_ab = ab * ch.hh;
+    r.o_ba = ba * ch.hh;
+    r.qx = q.x;
+    r.qy = q.y;
+    r.pa = pab.x - np;
+    r.pb = pab.y - np;
+    r.ea = eps[pab.x];
+    r.eb = eps[pab.y];
+    out[ch.qrow_off + q.x] = r;
+  }
+}
+
 // The eight loadMaps tables -> int32 flat offsets into their target chains, with range checks
 // and, for the five tables that are also scatter targets (mapToDistributed), hit counts that
 // check_counts_kernel then requires to be exactly one.

@@ -81,6 +81,7 @@ struct ccdgpu_handle {
   ElemRange *ranges = nullptr;
   QuadItem *quad_items = nullptr;  // fused assembly: work items of quads (u, w)
   QuadRow *quad_rows = nullptr;    // fused assembly: per strict packed row / hole pair tables
+  int64_t n_quad_rows = 0;
   QuadCol *quad_cols = nullptr;
   int n_quad_items = 0;
   int2 *pp_pairs = nullptr, *hh_pairs = nullptr;
@@ -876,7 +877,6 @@ TcKernel tc_kernel_of(int nt, bool gen) {
 struct BuildScratch {
   std::vector<int32_t> rowmap, mirror, kcol, pp_swap, hh_swap, list;
   std::vector<int2> pk_idx, pp_pairs, hh_pairs, vrows, mod_ph, mod_hp, mod_dims;
-  std::vector<QuadRow> quad_rows;
   std::vector<QuadCol> quad_cols;
   std::vector<QuadItem> quad_items;
   std::vector<ElemRange> ranges;
@@ -1003,13 +1003,14 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   }
   rowmap.resize(a_row_off[n_act]);
   mirror.resize(a_row_off[n_act]);
-  vrows.resize(a_row_off[n_act]);
+  // Row items of the stored-V tiling kernels (not needed when V_pppp is generated).
+  vrows.resize(on_the_fly ? 0 : a_row_off[n_act]);
   kcol.resize(a_pk_off[n_act]);
 #pragma omp parallel for num_threads(host_threads) schedule(dynamic, 4)
   for (int ai = 0; ai < n_act; ai++) {
     const int64_t pp = D[act_chan[ai]].pp, off = a_pp_off[ai];
     int32_t *rm = rowmap.data() + a_row_off[ai], *mr = mirror.data() + a_row_off[ai];
-    int2 *vr = vrows.data() + a_row_off[ai];
+    int2 *vr = on_the_fly ? nullptr : vrows.data() + a_row_off[ai];
     int32_t *kc = kcol.data() + a_pk_off[ai];
     int pr = 0, pk = 0;
     for (int64_t k = 0; k < pp; k++) {
@@ -1020,7 +1021,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
         q.y = pr;
         rm[pr] = (int32_t)k;
         mr[pr] = a < b ? pp_swap[off + k] : -1;
-        vr[pr] = make_int2(ai, pr);
+        if (vr) vr[pr] = make_int2(ai, pr);
         pr++;
       }
       pk_idx[off + k] = q;
@@ -1210,10 +1211,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   h->n_ranges = (int)ranges.size();
   // Fused assembly: quads (strict packed row a < b, strict hole pair i < j) per channel, their
   // static tables, and work items of up to kQuadPerItem quads of one channel.
-  std::vector<QuadRow> &quad_rows = bs.quad_rows;
   std::vector<QuadCol> &quad_cols = bs.quad_cols;
   std::vector<QuadItem> &quad_items = bs.quad_items;
-  quad_rows.clear();
   quad_cols.clear();
   quad_items.clear();
   // Rows: the packed rows with a < b (pk of them per channel), filled in parallel below;
@@ -1239,24 +1238,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
       quad_items.push_back({ai, (int32_t)q, (int32_t)std::min<int64_t>(nq, q + kQuadPerItem),
                             a.hk, a.t_off, a.qrow_off, a.qcol_off});
   }
-  quad_rows.resize(qrows_tot);
-#pragma omp parallel for num_threads(host_threads) schedule(dynamic, 4)
-  for (int ai = 0; ai < h->n_act; ai++) {
-    const ChanInfo &a = chans[ai];
-    QuadRow *out = quad_rows.data() + a.qrow_off;
-    for (int u = 0; u < a.pr; u++) {
-      const int ab = rowmap[a.row_off + u], ba = mirror[a.row_off + u];
-      if (ba < 0) continue;  // a = b: zero row
-      const int2 pab = pp_pairs[a.pp_off + ab];
-      const int2 qa = pk_idx[a.pp_off + ab];
-      QuadRow r{};
-      r.o_ab = ab * a.hh; r.o_ba = ba * a.hh;
-      r.qx = qa.x; r.qy = qa.y;
-      r.pa = pab.x - (int)np; r.pb = pab.y - (int)np;
-      r.ea = P->sp_energy[pab.x]; r.eb = P->sp_energy[pab.y];
-      *out++ = r;
-    }
-  }
+  h->n_quad_rows = qrows_tot;  // built on the device (quad_rows_kernel)
+
   h->host_chans = chans;
   h->n_quad_items = (int)quad_items.size();
   // Persistent assembly grid: kAsmCTAsPerSM resident CTAs per SM at most (one CTA if there is no quad,
@@ -1355,7 +1338,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   ar.add(&h->x, x_tot); ar.add(&h->x_t, xt); ar.add(&h->t_kt, tkt); ar.add(&h->t_mt, tmt);
   ar.add(&h->s, hh_tot); ar.add(&h->r, pp_tot); ar.add(&h->xh, np); ar.add(&h->yp, h->npart);
   ar.add(&h->quad_items, quad_items.size());
-  ar.add(&h->quad_rows, quad_rows.size()); ar.add(&h->quad_cols, quad_cols.size());
+  ar.add(&h->quad_rows, h->n_quad_rows); ar.add(&h->quad_cols, quad_cols.size());
   ar.add(&h->kcol, kcol.size());  // V tiling at create
   ar.add(&h->epart, std::max(h->n_ranges, h->n_asm_blocks)); ar.add(&h->ctl, 1); ar.add(&h->e_out, 1); ar.add(&h->err, 1);
   ar.add(&h->ticket, 1);
@@ -1519,7 +1502,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   };
   TRY(put(h->chans, chans)); TRY(put(h->mods, mods));
   TRY(put(h->hh_tiles, hh_tiles)); TRY(put(h->hh_red, hh_red)); TRY(put(h->ranges, ranges)); TRY(put(h->quad_items, quad_items));
-  TRY(put(h->quad_rows, quad_rows)); TRY(put(h->quad_cols, quad_cols));
+  TRY(put(h->quad_cols, quad_cols));
 
   TRY(put(h->kcol, kcol));
   if (h->tc_gen) {
@@ -1594,6 +1577,12 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   }
   // Device layout transforms.
   h->create_ms[1] = ms_since(t_build) - h->create_ms[0];
+  if (h->n_quad_rows) {
+    quad_rows_kernel<<<(unsigned)h->n_act, 256, 0, h->s0>>>(h->chans, h->rowmap, h->mirror,
+                                                           h->pk_idx, h->pp_pairs, h->eps,
+                                                           (int)np, h->quad_rows);
+    CK(cudaGetLastError());
+  }
   if (gen_v && !mod_gen.empty()) {
     gen_v_mod_kernel<<<(unsigned)mod_gen.size(), 256, 0, h->s0>>>(d_mod_gen, d_mod_ph, d_mod_hp,
                                                                  md, h->v_hpph, h->v_hphp);
@@ -1648,7 +1637,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
                                                      h->flat, n_t, h->inv4, h->err);
     CK(cudaGetLastError());
   }
-  if (!vrows.empty()) {
+  if (a_row_off[n_act] > 0) {
     if (on_the_fly) {
       // FP64 tiles, and the bf16 images unless the tensor-core ladder generates its own V: one
       // CTA per image chunk.
