@@ -242,6 +242,31 @@ __global__ void gen_v_mod_kernel(const ModGen *__restrict__ mods, const int2 *__
   }
 }
 
+// The (particle a, hole i) -> modified-channel lookup that derive_tables_kernel reads, from
+// the ph' (a, i) and hp' (i, a) pair lists of the generated-V path (their ranges checked on the
+// host): slot (a - np) * np + i holds (channel, ph' index, channel, hp' index).  One CTA per
+// active modified channel; the slots start at -1 and each half is claimed once (atomicCAS), so
+// a pair named twice sets kErrBadIndex.
+__global__ void mod_lookup_kernel(const ModGen *__restrict__ mods, const int32_t *__restrict__ chan,
+                                  const int2 *__restrict__ ph_pairs,
+                                  const int2 *__restrict__ hp_pairs, int np, int4 *mlook,
+                                  int32_t *err) {
+  const ModGen g = mods[blockIdx.x];
+  const int c = chan[blockIdx.x];
+  for (int k = threadIdx.x; k < g.ph; k += blockDim.x) {
+    const int2 ai = ph_pairs[g.ph_off + k];
+    int *m = reinterpret_cast<int *>(mlook + (int64_t)(ai.x - np) * np + ai.y);
+    if (atomicCAS(m, -1, c) != -1) atomicOr(err, kErrBadIndex);
+    else m[1] = k;
+  }
+  for (int k = threadIdx.x; k < g.hp; k += blockDim.x) {
+    const int2 ia = hp_pairs[g.hp_off + k];
+    int *m = reinterpret_cast<int *>(mlook + (int64_t)(ia.y - np) * np + ia.x) + 2;
+    if (atomicCAS(m, -1, c) != -1) atomicOr(err, kErrBadIndex);
+    else m[1] = k;
+  }
+}
+
 // E_ref and the normal-ordered single-particle energies from the bare ones (SPBasis.cpp:7-40).
 // Thread p < nsp: e_p + sum_{j < nh} <pj|v|pj>, summed in the reference's order.  Thread nsp:
 // E_ref = sum_{i,j < nh} 0.5 <ij|v|ij> + sum_{i < nh} e_i, one running sum in the reference's

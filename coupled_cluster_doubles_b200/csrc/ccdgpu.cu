@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <new>
 #include <vector>
 
@@ -159,9 +160,12 @@ struct ccdgpu_handle {
 
   // Device solve loop: graphs of WHILE conditional nodes whose bodies are one iteration each
   // (loop64: FP64 iterations; loop_tc: mixed iterations, then FP64 ones).  loop_state: 0 not
-  // built yet, 1 built, -1 unavailable (the batched graph replay is used instead).
+  // built yet, 1 built, -1 unavailable (the batched graph replay is used instead).  A mixed
+  // handle builds loop_tc first and loop64 only when a launch needs it (a solve still in FP64
+  // iterations after a whole loop chunk); loop_pdl: the capture that worked used PDL launches.
   cudaGraphExec_t loop64 = nullptr, loop_tc = nullptr;
   int loop_state = 0;
+  bool loop_pdl = true;
   int loop_capture = 0;  // while capturing a loop body: 1 FP64 body, 2 mixed body
   cudaGraphConditionalHandle loop_cond = 0;
   int64_t kernels_per_body64 = 0, kernels_per_body_tc = 0;
@@ -425,15 +429,88 @@ void release_stream_pool() {
   (void)cudaGetLastError();
 }
 
+// Graph executables of released handles, torn down later: by a helper thread of the next
+// create on the same device (beside its host work, while the device is idle), or by
+// ccdgpu_release_cached_memory, so that ccdgpu_destroy does not wait for their teardown
+// (about 0.3 ms each, longer while the device is busy).  At most kRetiredMax are held; beyond
+// that they are destroyed at once.
+constexpr size_t kRetiredMax = 64;
+
+struct RetiredGraphs {
+  std::mutex mu;
+  std::vector<std::pair<int, cudaGraphExec_t>> g;  // (device, executable)
+};
+
+RetiredGraphs &retired_graphs() {
+  static RetiredGraphs r;
+  return r;
+}
+
+void retire_graph(int dev, cudaGraphExec_t g) {
+  if (!g) return;
+  RetiredGraphs &R = retired_graphs();
+  {
+    std::lock_guard<std::mutex> lock(R.mu);
+    if (R.g.size() < kRetiredMax) {
+      R.g.push_back({dev, g});
+      return;
+    }
+  }
+  cudaGraphExecDestroy(g);
+}
+
+// Destroys the retired graphs of device dev (of every device for dev < 0).
+void destroy_retired_graphs(int dev) {
+  std::vector<std::pair<int, cudaGraphExec_t>> take;
+  {
+    RetiredGraphs &R = retired_graphs();
+    std::lock_guard<std::mutex> lock(R.mu);
+    std::vector<std::pair<int, cudaGraphExec_t>> keep;
+    for (const auto &x : R.g) (dev < 0 || x.first == dev ? take : keep).push_back(x);
+    R.g.swap(keep);
+  }
+  if (take.empty()) return;
+  int cur = -1;
+  if (dev < 0) cudaGetDevice(&cur);
+  for (const auto &x : take) {
+    if (dev < 0) cudaSetDevice(x.first);
+    cudaGraphExecDestroy(x.second);
+  }
+  if (cur >= 0) cudaSetDevice(cur);
+  (void)cudaGetLastError();
+}
+
+bool retired_graphs_pending(int dev) {
+  RetiredGraphs &R = retired_graphs();
+  std::lock_guard<std::mutex> lock(R.mu);
+  for (const auto &x : R.g)
+    if (x.first == dev) return true;
+  return false;
+}
+
+// Tears down device dev's retired graphs on a helper thread; the returned thread is joined by
+// the caller (or, if no thread could be started, the teardown has run on the calling thread).
+std::thread reap_retired_graphs(int dev) {
+  if (!retired_graphs_pending(dev)) return std::thread();
+  try {
+    return std::thread([dev] {
+      cudaSetDevice(dev);
+      destroy_retired_graphs(dev);
+    });
+  } catch (...) {
+    destroy_retired_graphs(dev);
+    return std::thread();
+  }
+}
+
 void release(ccdgpu_handle *h) {
   if (!h) return;
   // Cached blocks are handed to other handles: nothing of this one may still run on them.
   for (cudaStream_t st : {h->s0, h->s1, h->s2, h->s3})
     if (st) cudaStreamSynchronize(st);
-  if (h->graph) cudaGraphExecDestroy(h->graph);
-  if (h->graph_tc) cudaGraphExecDestroy(h->graph_tc);
-  if (h->loop64) cudaGraphExecDestroy(h->loop64);
-  if (h->loop_tc) cudaGraphExecDestroy(h->loop_tc);
+  for (cudaGraphExec_t g : {h->graph, h->graph_tc, h->loop64, h->loop_tc})
+    retire_graph(h->opt.device, g);
+  h->graph = h->graph_tc = h->loop64 = h->loop_tc = nullptr;
   for (auto &b : h->allocs) dev_free(b.p, b.bytes);
   h->allocs.clear();
   dev_free(h->tile_mem, h->tile_bytes);
@@ -563,9 +640,13 @@ int copy_runs_to_device(ccdgpu_handle *h, char *dst, const std::vector<const cha
 }
 
 // Device bytes [src, src + total) to host memory dst, through the staging buffers for large
-// totals: chunk k + 1 is copied by the copy engine into one buffer while host threads move
-// chunk k from the other into dst (a pageable device-to-host copy runs at about half of that).
-// Returns after every byte has arrived.
+// totals, in slots of kD2HSlot bytes: the copy engine fills up to kD2HSlots slots ahead while
+// host threads move each landed slot into dst, so only the last slot's host copy trails the
+// transfer (a pageable device-to-host copy runs at about half of that).  Returns after every
+// byte has arrived.
+constexpr size_t kD2HSlot = size_t(4) << 20;
+constexpr int kD2HSlots = (int)(2 * kStageChunk / kD2HSlot);
+
 int copy_from_device(ccdgpu_handle *h, char *dst, const char *src, size_t total) {
   if (!total) return CCDGPU_OK;
   Staging &S = staging();
@@ -579,34 +660,38 @@ int copy_from_device(ccdgpu_handle *h, char *dst, const char *src, size_t total)
       S.failed = true;
     }
     if (S.buf) {
-      cudaEvent_t ev[2] = {nullptr, nullptr};
+      cudaEvent_t ev[kD2HSlots] = {};
       cudaError_t e = cudaSuccess;
-      for (int k = 0; k < 2 && e == cudaSuccess; k++)
+      for (int k = 0; k < kD2HSlots && e == cudaSuccess; k++)
         e = cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming);
       const int threads = std::max(1, std::min(omp_get_max_threads(), 16));
-      const size_t nchunks = (total + kStageChunk - 1) / kStageChunk;
+      const size_t nchunks = (total + kD2HSlot - 1) / kD2HSlot;
       auto issue = [&](size_t c) {
-        const size_t off = c * kStageChunk, n = std::min(kStageChunk, total - off);
-        cudaError_t r = cudaMemcpyAsync(S.buf + (c & 1) * kStageChunk, src + off, n,
+        const size_t off = c * kD2HSlot, n = std::min(kD2HSlot, total - off);
+        const int k = (int)(c % kD2HSlots);
+        cudaError_t r = cudaMemcpyAsync(S.buf + k * kD2HSlot, src + off, n,
                                         cudaMemcpyDeviceToHost, h->s0);
-        if (r == cudaSuccess) r = cudaEventRecord(ev[c & 1], h->s0);
+        if (r == cudaSuccess) r = cudaEventRecord(ev[k], h->s0);
         return r;
       };
-      if (e == cudaSuccess) e = issue(0);
+      size_t issued = 0;
+      for (; e == cudaSuccess && issued < std::min<size_t>(nchunks, kD2HSlots); issued++)
+        e = issue(issued);
       for (size_t c = 0; c < nchunks && e == cudaSuccess; c++) {
-        if (c + 1 < nchunks && (e = issue(c + 1)) != cudaSuccess) break;
-        if ((e = cudaEventSynchronize(ev[c & 1])) != cudaSuccess) break;
-        const size_t off = c * kStageChunk, n = std::min(kStageChunk, total - off);
-        const char *stage = S.buf + (c & 1) * kStageChunk;
+        const int k = (int)(c % kD2HSlots);
+        if ((e = cudaEventSynchronize(ev[k])) != cudaSuccess) break;
+        const size_t off = c * kD2HSlot, n = std::min(kD2HSlot, total - off);
+        const char *stage = S.buf + k * kD2HSlot;
         const size_t piece = std::max<size_t>(size_t(64) << 10, (n + threads - 1) / threads);
 #pragma omp parallel for num_threads(threads) schedule(static)
         for (int64_t x = 0; x < (int64_t)((n + piece - 1) / piece); x++) {
           const size_t lo = (size_t)x * piece;
           std::memcpy(dst + off + lo, stage + lo, std::min(piece, n - lo));
         }
+        if (issued < nchunks) e = issue(issued++);  // into the slot just emptied
       }
       (void)cudaStreamSynchronize(h->s0);
-      for (int k = 0; k < 2; k++)
+      for (int k = 0; k < kD2HSlots; k++)
         if (ev[k]) cudaEventDestroy(ev[k]);
       if (e != cudaSuccess) {
         (void)cudaGetLastError();
@@ -620,9 +705,104 @@ int copy_from_device(ccdgpu_handle *h, char *dst, const char *src, size_t total)
   return CCDGPU_OK;
 }
 
-int copy_to_device(ccdgpu_handle *h, void *dst, const void *src, size_t bytes) {
-  return copy_runs_to_device(h, static_cast<char *>(dst), {static_cast<const char *>(src)},
-                             {bytes});
+// One host array bound for its own device destination.
+struct UploadPiece {
+  char *dst;
+  const char *src;
+  size_t n;
+};
+
+// Many host arrays to their device destinations in one pass.  Large batches go through the
+// staging buffers: host threads pack the next pieces into one buffer (16-byte aligned), then
+// every piece is one asynchronous copy out of page-locked memory, so the copy engine runs
+// them back to back while the host packs the other buffer.  Small batches are pageable copies.
+// Returns after every byte has arrived, except with `hold` when the batch fit one buffer: the
+// copies are then left in flight on s0 and the staging lock moves to *hold, which the caller
+// keeps until s0 has passed them (no staging use by this thread meanwhile).
+int copy_pieces_to_device(ccdgpu_handle *h, const std::vector<UploadPiece> &pcs,
+                          std::unique_lock<std::mutex> *hold = nullptr) {
+  size_t total = 0;
+  for (const UploadPiece &p : pcs) total += p.n;
+  if (!total) return CCDGPU_OK;
+  Staging &S = staging();
+  std::unique_lock<std::mutex> lock(S.mu, std::defer_lock);
+  if (total >= kStageMin && lock.try_lock()) {
+    if (!S.buf && !S.failed &&
+        cudaHostAlloc(reinterpret_cast<void **>(&S.buf), 2 * kStageChunk,
+                      cudaHostAllocPortable) != cudaSuccess) {
+      (void)cudaGetLastError();
+      S.buf = nullptr;
+      S.failed = true;
+    }
+    if (S.buf) {
+      cudaEvent_t ev[2] = {nullptr, nullptr};
+      bool pending[2] = {false, false};
+      cudaError_t e = cudaSuccess;
+      for (int k = 0; k < 2 && e == cudaSuccess; k++)
+        e = cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming);
+      const int threads = std::max(1, std::min(omp_get_max_threads(), 16));
+      struct Part {
+        size_t off;  // in the staging buffer
+        const char *src;
+        char *dst;
+        size_t n;
+      };
+      std::vector<Part> parts, work;
+      size_t i = 0, done = 0;  // current piece, and its bytes already placed
+      for (int k = 0; i < pcs.size() && e == cudaSuccess; k ^= 1) {
+        char *stage = S.buf + k * kStageChunk;
+        if (pending[k] && (e = cudaEventSynchronize(ev[k])) != cudaSuccess) break;
+        parts.clear();
+        size_t used = 0;
+        while (i < pcs.size() && used < kStageChunk) {
+          const size_t n = std::min(pcs[i].n - done, kStageChunk - used);
+          if (n) parts.push_back(Part{used, pcs[i].src + done, pcs[i].dst + done, n});
+          used = std::min(kStageChunk, used + ((n + 15) & ~size_t(15)));
+          done += n;
+          if (done == pcs[i].n) {
+            i++;
+            done = 0;
+          }
+        }
+        // Host threads fill the buffer in slices of at most used / threads bytes.
+        const size_t slice = std::max<size_t>(size_t(64) << 10, (used + threads - 1) / threads);
+        work.clear();
+        for (const Part &p : parts)
+          for (size_t x = 0; x < p.n; x += slice)
+            work.push_back(Part{p.off + x, p.src + x, nullptr, std::min(slice, p.n - x)});
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 4)
+        for (int64_t j = 0; j < (int64_t)work.size(); j++)
+          std::memcpy(stage + work[j].off, work[j].src, work[j].n);
+        for (size_t j = 0; j < parts.size() && e == cudaSuccess; j++)
+          e = cudaMemcpyAsync(parts[j].dst, stage + parts[j].off, parts[j].n,
+                              cudaMemcpyHostToDevice, h->s0);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[k], h->s0);
+        pending[k] = e == cudaSuccess;
+      }
+      if (hold && e == cudaSuccess && total <= kStageChunk) {
+        for (int k = 0; k < 2; k++)
+          if (ev[k]) cudaEventDestroy(ev[k]);
+        *hold = std::move(lock);
+        return CCDGPU_OK;
+      }
+      for (int k = 0; k < 2; k++) {
+        if (pending[k]) {
+          const cudaError_t w = cudaEventSynchronize(ev[k]);
+          if (e == cudaSuccess) e = w;
+        }
+        if (ev[k]) cudaEventDestroy(ev[k]);
+      }
+      if (e != cudaSuccess) {
+        (void)cudaStreamSynchronize(h->s0);
+        (void)cudaGetLastError();
+        return CCDGPU_ERR_CUDA;
+      }
+      return CCDGPU_OK;
+    }
+  }
+  for (const UploadPiece &p : pcs)
+    if (p.n) CK(cudaMemcpyAsync(p.dst, p.src, p.n, cudaMemcpyHostToDevice, h->s0));
+  return CCDGPU_OK;
 }
 
 // Copies per-channel host blocks (block k of `count[k]` elements at src[k]) to consecutive
@@ -809,9 +989,16 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
   std::vector<RedItem> red_fp, red_tc;
   red_items(tiles, red_fp, h->n_red_cls, true, [](int nb) { return nb <= 8 ? 0 : nb <= 32 ? 1 : 2; });
   red_items(tc_tiles, red_tc, nullptr, false, nullptr);
-  // Device copies: one allocation, counters zeroed.
-  CK(cudaStreamSynchronize(h->s0));
-  CK(cudaStreamSynchronize(h->s2));
+  // Device copies: one allocation, counters zeroed, written on s3, which s0 then waits for.
+  // A schedule that replaces another first waits for the handle's work in flight (the old
+  // lists may be in use); the first one, made in create while the set-up kernels run on s0,
+  // has nothing to wait for, so create's host work goes on beside them.
+  const bool first = h->tile_mem == nullptr;
+  if (!first) {
+    CK(cudaStreamSynchronize(h->s0));
+    CK(cudaStreamSynchronize(h->s2));
+    CK(cudaStreamSynchronize(h->s3));
+  }
   // Captured graphs hold the previous lists; they go before the block they point into.
   for (cudaGraphExec_t *g : {&h->graph, &h->graph_tc, &h->loop64, &h->loop_tc})
     if (*g) { cudaGraphExecDestroy(*g); *g = nullptr; }
@@ -832,27 +1019,29 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
   ar.add(&h->tc_part, tcpart_tot);
   ar.add(&h->red_fp, red_fp.size()); ar.add(&h->red_tc, red_tc.size());
   CK(dev_alloc(ar.used, &h->tile_mem, &h->tile_bytes));
-  CK(cudaMemsetAsync(h->tile_mem, 0, ar.used, h->s0));
+  CK(cudaMemsetAsync(h->tile_mem, 0, ar.used, h->s3));
   for (auto &r : ar.reqs) *r.first = static_cast<char *>(h->tile_mem) + r.second;
   if (!tiles.empty())
     CK(cudaMemcpyAsync(h->tiles, tiles.data(), tiles.size() * sizeof(LadderTile),
-                       cudaMemcpyHostToDevice, h->s0));
+                       cudaMemcpyHostToDevice, h->s3));
   if (!tc_tiles.empty())
     CK(cudaMemcpyAsync(h->tc_tiles, tc_tiles.data(), tc_tiles.size() * sizeof(LadderTile),
-                       cudaMemcpyHostToDevice, h->s0));
+                       cudaMemcpyHostToDevice, h->s3));
   if (!fp_cta_off.empty())
     CK(cudaMemcpyAsync(h->fp_cta_off, fp_cta_off.data(), fp_cta_off.size() * sizeof(int32_t),
-                       cudaMemcpyHostToDevice, h->s0));
+                       cudaMemcpyHostToDevice, h->s3));
   h->tc_grid = (int)std::min<size_t>(tc_tiles.size(), kTcGrid);
   if (!red_fp.empty())
     CK(cudaMemcpyAsync(h->red_fp, red_fp.data(), red_fp.size() * sizeof(RedItem),
-                       cudaMemcpyHostToDevice, h->s0));
+                       cudaMemcpyHostToDevice, h->s3));
   if (!red_tc.empty())
     CK(cudaMemcpyAsync(h->red_tc, red_tc.data(), red_tc.size() * sizeof(RedItem),
-                       cudaMemcpyHostToDevice, h->s0));
+                       cudaMemcpyHostToDevice, h->s3));
   h->n_red_fp = (int)red_fp.size();
   h->n_red_tc = (int)red_tc.size();
-  CK(cudaStreamSynchronize(h->s0));
+  CK(cudaEventRecord(h->ev_fork2, h->s3));
+  CK(cudaStreamWaitEvent(h->s0, h->ev_fork2, 0));
+  if (!first) CK(cudaStreamSynchronize(h->s0));
   h->n_tiles = (int)tiles.size();
   h->n_cls[0] = h->n_cls[1] = h->n_cls[2] = 0;
   for (const LadderTile &t : tiles) h->n_cls[cls_of(t.nb)]++;
@@ -880,7 +1069,10 @@ struct BuildScratch {
   std::vector<QuadCol> quad_cols;
   std::vector<QuadItem> quad_items;
   std::vector<ElemRange> ranges;
-  std::vector<int64_t> o_t, o_m, o_m_scratch;
+  std::vector<int64_t> o_t, o_m, o_m_scratch, list_cnt;
+  std::vector<int4> gv_items, gvt_items, mlook;
+  std::vector<uint64_t> mod_chan;
+  std::vector<int32_t> mod_gen_chan;
 };
 thread_local BuildScratch t_build_scratch;
 
@@ -888,8 +1080,17 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
+void ready_loop_graphs(ccdgpu_handle *h);
+
 int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   const auto t_build = std::chrono::steady_clock::now();
+  // Earlier handles' graphs are torn down beside this create's host work; joined on return.
+  struct Joined {
+    std::thread t;
+    ~Joined() {
+      if (t.joinable()) t.join();
+    }
+  } reaper{reap_retired_graphs(h->opt.device)};
   const uint64_t nch = P->n_channels, nsp = P->n_sp, np = P->n_particles;
   h->nch = nch; h->nsp = nsp; h->np = np; h->npart = nsp - np;
   const ccdgpu_channel_dims *D = P->chan_dims, *MD = P->chan_mod_dims;
@@ -1099,20 +1300,51 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   for (const ChanInfo &a : chans)
     if (a.hh > 16) h->hh_slice_smem = std::max(h->hh_slice_smem, hh_slice_smem(a.hh));
   // Per orbital w, the pair elements whose first index is w, ascending (particles: pp
-  // elements, holes: hh elements): a counting sort.
+  // elements, holes: hh elements): a counting sort.  The pp elements (first index a particle)
+  // are split into one contiguous range per host thread: per-thread bucket counts, then each
+  // thread places its range from its own start in every bucket, so a bucket keeps ascending
+  // element order.  The hh elements (first index a hole, buckets of their own) follow serially.
   std::vector<int64_t> list_off(nsp + 1, 0);
-  for (int64_t e = 0; e < pp_tot; e++) list_off[pp_pairs[e].x + 1]++;
-  for (int64_t e = 0; e < hh_tot; e++) list_off[hh_pairs[e].x + 1]++;
-  for (uint64_t w = 0; w < nsp; w++) list_off[w + 1] += list_off[w];
   std::vector<int32_t> &list = bs.list;
-  list.resize(list_off[nsp]);
-  h->n_list = list_off[nsp];
   {
+    std::vector<int64_t> &cnt = bs.list_cnt;  // [thread][orbital]: counts, then start offsets
+    cnt.assign((size_t)host_threads * nsp, 0);
+    int team = 1;
+#pragma omp parallel num_threads(host_threads)
+    {
+#pragma omp single
+      team = omp_get_num_threads();
+      const int t = omp_get_thread_num();
+      const int64_t lo = pp_tot * t / team, hi = pp_tot * (t + 1) / team;
+      int64_t *c = cnt.data() + (size_t)t * nsp;
+      for (int64_t e = lo; e < hi; e++) c[pp_pairs[e].x]++;
+#pragma omp barrier
+#pragma omp single
+      {
+        for (int64_t e = 0; e < hh_tot; e++) list_off[hh_pairs[e].x + 1]++;
+        for (uint64_t w = 0; w < nsp; w++) {
+          int64_t s = 0;
+          for (int u = 0; u < team; u++) s += cnt[(size_t)u * nsp + w];
+          list_off[w + 1] += s;
+        }
+        for (uint64_t w = 0; w < nsp; w++) list_off[w + 1] += list_off[w];
+        list.resize(list_off[nsp]);
+        for (uint64_t w = 0; w < nsp; w++) {
+          int64_t at = list_off[w];
+          for (int u = 0; u < team; u++) {
+            const int64_t n = cnt[(size_t)u * nsp + w];
+            cnt[(size_t)u * nsp + w] = at;
+            at += n;
+          }
+        }
+      }
+      for (int64_t e = lo; e < hi; e++) list[c[pp_pairs[e].x]++] = (int32_t)e;
+    }
     std::vector<int64_t> &cur = bs.o_m_scratch;
     cur.assign(list_off.begin(), list_off.end() - 1);
-    for (int64_t e = 0; e < pp_tot; e++) list[cur[pp_pairs[e].x]++] = (int32_t)e;
     for (int64_t e = 0; e < hh_tot; e++) list[cur[hh_pairs[e].x]++] = (int32_t)e;
   }
+  h->n_list = list_off[nsp];
 
   // Modified channels: small ones (one warp each) first, then one group per padded size
   // (32, 48, 64, 80; one CTA per channel).
@@ -1123,6 +1355,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   std::vector<const double *> src_hpph, src_hphp;
   std::vector<int64_t> cnt_hpph, cnt_hphp;
   std::vector<ModGen> mod_gen;        // generated V: modified channels in channel order
+  std::vector<int32_t> &mod_gen_chan = bs.mod_gen_chan;  // ... and their channel slots
+  mod_gen_chan.clear();
   std::vector<int2> &mod_ph = bs.mod_ph, &mod_hp = bs.mod_hp;  // ... their ph' (b, j), hp' (i, a) pairs
   mod_ph.clear();
   mod_hp.clear();
@@ -1139,6 +1373,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
       const int64_t ph0 = mod_gen.empty() ? 0 : mod_gen.back().ph_off + mod_gen.back().ph;
       const int64_t hp0 = mod_gen.empty() ? 0 : mod_gen.back().hp_off + mod_gen.back().hp;
       mod_gen.push_back(ModGen{(int)ph, (int)hp, m.m_off, m.y_off, ph0, hp0});
+      mod_gen_chan.push_back((int32_t)c);
     } else {
       if (!P->v_hpph_mod[c] || !P->v_hphp_mod[c]) return CCDGPU_ERR_INVALID_ARGUMENT;
       src_hpph.push_back(P->v_hpph_mod[c]); cnt_hpph.push_back(ph * hp);
@@ -1152,9 +1387,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   if (!mod_gen.empty()) {
     mod_ph.resize(mod_gen.back().ph_off + mod_gen.back().ph);
     mod_hp.resize(mod_gen.back().hp_off + mod_gen.back().hp);
-    std::vector<uint64_t> mod_chan;
-    for (uint64_t c = 0; c < nch; c++)
-      if (MD[c].ph && MD[c].hp) mod_chan.push_back(c);
+    const std::vector<int32_t> &mod_chan = mod_gen_chan;
     std::atomic<int> bad_mod{0};
 #pragma omp parallel for num_threads(host_threads) schedule(dynamic, 16)
     for (int64_t g = 0; g < (int64_t)mod_gen.size(); g++) {
@@ -1373,15 +1606,30 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   int2 *d_vrows = nullptr, *d_mod_dims = nullptr;
   int4 *d_gv_items = nullptr, *d_gvt_items = nullptr;
   // Generated V_pppp: one item per operand-image chunk (channel, row tile, K chunk).
-  std::vector<int4> gv_items, gvt_items;
+  // Counted per channel, then filled in parallel, each channel at its offset.
+  std::vector<int4> &gv_items = bs.gv_items, &gvt_items = bs.gvt_items;
+  gv_items.clear();
+  gvt_items.clear();
   if (on_the_fly) {
+    const bool tc_images = h->nt && !h->tc_gen;
+    std::vector<int64_t> go(h->n_act + 1, 0), gto(h->n_act + 1, 0);
     for (int ai = 0; ai < h->n_act; ai++) {
       const ChanInfo &a = chans[ai];
+      go[ai + 1] = go[ai] + (int64_t)a.nmt * a.nkc;
+      gto[ai + 1] = gto[ai] + (tc_images ? (int64_t)ceil_div(a.pr, kTcBM) * a.nkct : 0);
+    }
+    gv_items.resize(go[h->n_act]);
+    gvt_items.resize(gto[h->n_act]);
+#pragma omp parallel for num_threads(host_threads) schedule(dynamic, 4)
+    for (int ai = 0; ai < h->n_act; ai++) {
+      const ChanInfo &a = chans[ai];
+      int4 *g = gv_items.data() + go[ai];
       for (int mt = 0; mt < a.nmt; mt++)
-        for (int kc = 0; kc < a.nkc; kc++) gv_items.push_back(make_int4(ai, mt, kc, 0));
-      if (h->nt && !h->tc_gen)
+        for (int kc = 0; kc < a.nkc; kc++) *g++ = make_int4(ai, mt, kc, 0);
+      int4 *gt = gvt_items.data() + gto[ai];
+      if (tc_images)
         for (int mt = 0; mt < (int)ceil_div(a.pr, kTcBM); mt++)
-          for (int kc = 0; kc < a.nkct; kc++) gvt_items.push_back(make_int4(ai, mt, kc, 0));
+          for (int kc = 0; kc < a.nkct; kc++) *gt++ = make_int4(ai, mt, kc, 0);
     }
   }
   int64_t *d_vraw_off = nullptr, *d_o_m = nullptr;
@@ -1389,30 +1637,61 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   // pairs, built here from the ph' / hp' maps (O(npart * np)).
   int32_t *d_hblk = nullptr, *d_pblk = nullptr;
   int4 *d_mlook = nullptr;
-  std::vector<int4> mlook;
-  if (derive_tables) {
+  std::vector<int4> &mlook = bs.mlook;
+  mlook.clear();
+  // With generated V the ph' / hp' pairs go to the device anyway: the lookup is built there
+  // (mod_lookup_kernel); otherwise here.
+  const bool mlook_dev = derive_tables && gen_v;
+  const uint64_t n_mlook = (nsp - np) * np;
+  if (mlook_dev) {
+    sc.add(&d_mlook, n_mlook);
+  } else if (derive_tables) {
     const uint64_t npart = nsp - np;
     mlook.assign(npart * np, make_int4(-1, -1, -1, -1));
+    std::vector<uint64_t> &mc = bs.mod_chan;
+    mc.clear();
     for (uint64_t c = 0; c < nch; c++) {
-      const uint64_t ph = MD[c].ph, hp = MD[c].hp;
-      if (!ph || !hp) continue;
-      const ccdgpu_pair *phm = P->chan_mod_maps[c].ph, *hpm = P->chan_mod_maps[c].hp;
-      if (!phm || !hpm) return CCDGPU_ERR_INVALID_ARGUMENT;
-      for (uint64_t k = 0; k < ph; k++) {
-        const uint64_t a = phm[k].p, i = phm[k].q;
-        if (a < np || a >= nsp || i >= np) return CCDGPU_ERR_BAD_TABLE;
-        int4 &m = mlook[(a - np) * np + i];
-        if (m.x >= 0) return CCDGPU_ERR_BAD_TABLE;
-        m.x = (int)c; m.y = (int)k;
-      }
-      for (uint64_t k = 0; k < hp; k++) {
-        const uint64_t i = hpm[k].p, a = hpm[k].q;
-        if (i >= np || a < np || a >= nsp) return CCDGPU_ERR_BAD_TABLE;
-        int4 &m = mlook[(a - np) * np + i];
-        if (m.z >= 0) return CCDGPU_ERR_BAD_TABLE;
-        m.z = (int)c; m.w = (int)k;
-      }
+      if (!MD[c].ph || !MD[c].hp) continue;
+      if (!P->chan_mod_maps[c].ph || !P->chan_mod_maps[c].hp) return CCDGPU_ERR_INVALID_ARGUMENT;
+      mc.push_back(c);
     }
+    // In a valid problem every (particle, hole) slot is named by exactly one ph' entry and one
+    // hp' entry, so the channels fill their slots in parallel (relaxed atomic stores, so that
+    // an invalid problem's duplicates race harmlessly); a second pass checks that each entry's
+    // slot holds that entry, which fails for every duplicate but one.
+    std::atomic<int> bad_m{0};
+    int32_t *ml = reinterpret_cast<int32_t *>(mlook.data());
+    auto each_entry = [&](int64_t g, auto &&f) {
+      const uint64_t c = mc[g];
+      const ccdgpu_pair *phm = P->chan_mod_maps[c].ph, *hpm = P->chan_mod_maps[c].hp;
+      for (uint64_t k = 0; k < MD[c].ph; k++) {
+        const uint64_t a = phm[k].p, i = phm[k].q;
+        if (a < np || a >= nsp || i >= np) bad_m = 1;
+        else f(ml + 4 * ((a - np) * np + i), (int)c, (int)k);
+      }
+      for (uint64_t k = 0; k < MD[c].hp; k++) {
+        const uint64_t i = hpm[k].p, a = hpm[k].q;
+        if (i >= np || a < np || a >= nsp) bad_m = 1;
+        else f(ml + 4 * ((a - np) * np + i) + 2, (int)c, (int)k);
+      }
+    };
+#pragma omp parallel num_threads(host_threads)
+    {
+#pragma omp for schedule(dynamic, 16)
+      for (int64_t g = 0; g < (int64_t)mc.size(); g++)
+        each_entry(g, [](int32_t *m, int c, int k) {
+          __atomic_store_n(m, c, __ATOMIC_RELAXED);
+          __atomic_store_n(m + 1, k, __ATOMIC_RELAXED);
+        });
+#pragma omp for schedule(dynamic, 16)
+      for (int64_t g = 0; g < (int64_t)mc.size(); g++)
+        each_entry(g, [&](int32_t *m, int c, int k) {
+          if (__atomic_load_n(m, __ATOMIC_RELAXED) != c ||
+              __atomic_load_n(m + 1, __ATOMIC_RELAXED) != k)
+            bad_m = 1;
+        });
+    }
+    if (bad_m) return CCDGPU_ERR_BAD_TABLE;
     sc.add(&d_mlook, mlook.size());
   } else {
     sc.add(&raw_idx, (size_t)8 * n_t);
@@ -1423,9 +1702,10 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   }
   ModGen *d_mod_gen = nullptr;
   int2 *d_mod_ph = nullptr, *d_mod_hp = nullptr;
+  int32_t *d_mod_chan = nullptr;
   if (gen_v) {
     sc.add(&d_mod_gen, mod_gen.size()); sc.add(&d_mod_ph, mod_ph.size());
-    sc.add(&d_mod_hp, mod_hp.size());
+    sc.add(&d_mod_hp, mod_hp.size()); sc.add(&d_mod_chan, mod_gen_chan.size());
   }
   sc.add(&vraw, vraw_tot); sc.add(&hhpp_raw, gen_v ? 0 : n_t);
   sc.add(&hpph_raw, gen_v ? 0 : h->n_m);
@@ -1436,6 +1716,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   // (electron gas) the direct Coulomb term by momentum transfer, computed here with the
   // reference's expression (ElectronGasSPBasis.cpp:424-448).  Kept for the handle's lifetime.
   ModelDev md{};
+  std::vector<UploadPiece> batch;  // host -> device copies made together, after the lists
+  std::unique_lock<std::mutex> staging_hold;  // staging buffers with copies still in flight
   std::vector<double> vq;
   std::vector<uint32_t> ocode;
   int32_t *d_qn = nullptr;
@@ -1482,12 +1764,13 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     mr.add(&d_ocode, ocode.size());
     mr.add(&h->eps_io, 2 * nsp + 1);
     TRY(mr.commit(h));
-    CK(cudaMemcpyAsync(d_qn, M->qn, (size_t)nsp * M->qn_stride * sizeof(int32_t),
-                       cudaMemcpyHostToDevice, h->s0));
-    if (!vq.empty())
-      CK(cudaMemcpyAsync(d_vq, vq.data(), vq.size() * 8, cudaMemcpyHostToDevice, h->s0));
-    if (!ocode.empty())
-      CK(cudaMemcpyAsync(d_ocode, ocode.data(), ocode.size() * 4, cudaMemcpyHostToDevice, h->s0));
+    batch.push_back(UploadPiece{reinterpret_cast<char *>(d_qn),
+                                reinterpret_cast<const char *>(M->qn),
+                                (size_t)nsp * M->qn_stride * sizeof(int32_t)});
+    batch.push_back(UploadPiece{reinterpret_cast<char *>(d_vq),
+                                reinterpret_cast<const char *>(vq.data()), vq.size() * 8});
+    batch.push_back(UploadPiece{reinterpret_cast<char *>(d_ocode),
+                                reinterpret_cast<const char *>(ocode.data()), ocode.size() * 4});
     md.qn = d_qn;
     md.vq = d_vq;
     md.ocode = ocode.empty() ? nullptr : d_ocode;
@@ -1497,8 +1780,14 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   const size_t n_allocs = h->allocs.size();
   TRY(sc.commit(h));
 
+  // The host lists go up together with the model's (copy_pieces_to_device below); they stay
+  // alive until then.
   auto put = [&](auto *dst, const auto &v) -> int {
-    return v.empty() ? CCDGPU_OK : copy_to_device(h, dst, v.data(), v.size() * sizeof(v[0]));
+    if (!v.empty())
+      batch.push_back(UploadPiece{reinterpret_cast<char *>(dst),
+                                  reinterpret_cast<const char *>(v.data()),
+                                  v.size() * sizeof(v[0])});
+    return CCDGPU_OK;
   };
   TRY(put(h->chans, chans)); TRY(put(h->mods, mods));
   TRY(put(h->hh_tiles, hh_tiles)); TRY(put(h->hh_red, hh_red)); TRY(put(h->ranges, ranges)); TRY(put(h->quad_items, quad_items));
@@ -1516,7 +1805,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   TRY(put(d_vrows, vrows)); TRY(put(d_vraw_off, vraw_off));
   TRY(put(d_gv_items, gv_items)); TRY(put(d_gvt_items, gvt_items));
   TRY(put(d_mod_dims, mod_dims)); TRY(put(d_o_m, o_m));
-  CK(cudaMemcpyAsync(h->eps, P->sp_energy, nsp * 8, cudaMemcpyHostToDevice, h->s0));
+  batch.push_back(UploadPiece{reinterpret_cast<char *>(h->eps),
+                              reinterpret_cast<const char *>(P->sp_energy), nsp * 8});
 
   // V blocks and tables, uploaded in their reference layouts (runs of adjacent blocks).
   {
@@ -1550,11 +1840,12 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     static_assert(sizeof(RawIndex) == sizeof(ccdgpu_chain_index), "ChainIndex layout");
     for (int k = 0; k < 8 && !derive_tables; k++)
       TRY(upload_runs(h, reinterpret_cast<ccdgpu_chain_index *>(raw_idx) + (size_t)k * n_t, sm[k], nm));
-    if (derive_tables) TRY(put(d_mlook, mlook));
+    if (derive_tables && !mlook_dev) TRY(put(d_mlook, mlook));
     if (gen_v) {
       TRY(put(d_mod_gen, mod_gen));
       TRY(put(d_mod_ph, mod_ph));
       TRY(put(d_mod_hp, mod_hp));
+      TRY(put(d_mod_chan, mod_gen_chan));
     }
     TRY(upload_runs(h, hpph_raw, src_hpph, cnt_hpph));
     TRY(upload_runs(h, h->v_hphp, src_hphp, cnt_hphp));
@@ -1574,6 +1865,9 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
       TRY(upload_runs(h, h->v_h_hpp, s5, n5));
       TRY(upload_runs(h, h->v_phh_p, s6, n6));
     }
+    // The last use of the staging buffers in create: the lists' copies stay in flight (the
+    // staging lock is held until the set-up's final synchronisation).
+    TRY(copy_pieces_to_device(h, batch, &staging_hold));
   }
   // Device layout transforms.
   h->create_ms[1] = ms_since(t_build) - h->create_ms[0];
@@ -1617,6 +1911,14 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
           h->chans, h->pp_pairs, h->hh_pairs, md, h->o_h, h->o_p, d_hblk, d_pblk, (int)np,
           (int)h->npart, h->v_h_hpp, h->v_phh_p, h->err);
       CK(cudaGetLastError());
+    }
+    if (mlook_dev) {
+      CK(cudaMemsetAsync(d_mlook, 0xff, n_mlook * sizeof(int4), h->s0));  // every field -1
+      if (!mod_gen.empty()) {
+        mod_lookup_kernel<<<(unsigned)mod_gen.size(), 128, 0, h->s0>>>(
+            d_mod_gen, d_mod_chan, d_mod_ph, d_mod_hp, (int)np, d_mlook, h->err);
+        CK(cudaGetLastError());
+      }
     }
     if (derive_tables) {
       DeriveGeometry dg{h->o_h, h->o_p, d_o_m, d_mod_dims, d_hblk, d_pblk, d_mlook,
@@ -1663,18 +1965,10 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
       CK(cudaGetLastError());
     }
   }
-  int32_t e = 0;
-  CK(cudaMemcpyAsync(&e, h->err, sizeof(e), cudaMemcpyDeviceToHost, h->s0));
-  CK(cudaStreamSynchronize(h->s0));
-  h->create_ms[2] = ms_since(t_build) - h->create_ms[0] - h->create_ms[1];
-  // Release the scratch allocation.
-  for (size_t i = n_allocs; i < h->allocs.size(); i++) dev_free(h->allocs[i].p, h->allocs[i].bytes);
-  h->allocs.resize(n_allocs);
-  if (e & kErrBadIndex) return CCDGPU_ERR_BAD_TABLE;
-  // The fused path relies on the structure of the ring tables; the table path does not.
-  if ((e & kErrRingMaps) && h->opt.path == CCDGPU_PATH_FUSED) return CCDGPU_ERR_BAD_TABLE;
-  if (e & ~kErrRingMaps) return CCDGPU_ERR_CUDA;
-  if (e) CK(cudaMemsetAsync(h->err, 0, sizeof(int32_t), h->s0));
+  // Host work that needs no result of the set-up kernels runs while they do: kernel
+  // attributes, the ladder schedules and, for device-loop handles, the loop graph's capture
+  // (nothing of it executes until a solve launches it).  Then the set-up's error word is read.
+  const auto t_sched = std::chrono::steady_clock::now();
 #undef TRY
   h->h_ctl = ctl_acquire();
   if (!h->h_ctl) return CCDGPU_ERR_OUT_OF_MEMORY;
@@ -1716,7 +2010,23 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     CK(cudaFuncSetAttribute(tc_kernel_of(h->nt, h->tc_gen),
                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->tc_smem));
   }
-  h->create_ms[3] = ms_since(t_build) - h->create_ms[0] - h->create_ms[1] - h->create_ms[2];
+  if (h->opt.path == CCDGPU_PATH_FUSED && h->opt.use_graph && h->opt.device_loop) {
+    ready_loop_graphs(h);
+    if (h->loop_state != 1) h->loop_state = 0;  // retried by the first solve, on an idle stream
+  }
+  h->create_ms[3] = ms_since(t_sched);
+  int32_t e = 0;
+  CK(cudaMemcpyAsync(&e, h->err, sizeof(e), cudaMemcpyDeviceToHost, h->s0));
+  CK(cudaStreamSynchronize(h->s0));
+  h->create_ms[2] = ms_since(t_build) - h->create_ms[0] - h->create_ms[1];
+  // Release the scratch allocation.
+  for (size_t i = n_allocs; i < h->allocs.size(); i++) dev_free(h->allocs[i].p, h->allocs[i].bytes);
+  h->allocs.resize(n_allocs);
+  if (e & kErrBadIndex) return CCDGPU_ERR_BAD_TABLE;
+  // The fused path relies on the structure of the ring tables; the table path does not.
+  if ((e & kErrRingMaps) && h->opt.path == CCDGPU_PATH_FUSED) return CCDGPU_ERR_BAD_TABLE;
+  if (e & ~kErrRingMaps) return CCDGPU_ERR_CUDA;
+  if (e) CK(cudaMemsetAsync(h->err, 0, sizeof(int32_t), h->s0));
   return CCDGPU_OK;
 }
 
@@ -2138,17 +2448,19 @@ int capture_loop_graph(ccdgpu_handle *h, bool mixed, cudaGraphExec_t *exec) {
   return rc;
 }
 
-// Builds both loop graphs once; any failure (for example a driver without conditional nodes,
-// or without programmatic launches inside them, retried without) leaves the batched replay.
+// Builds the loop graph a solve starts with (loop_tc for mixed handles, loop64 otherwise)
+// once; any failure (for example a driver without conditional nodes, or without programmatic
+// launches inside them, retried without) leaves the batched replay.
 void ready_loop_graphs(ccdgpu_handle *h) {
   if (h->loop_state) return;
   const auto t0 = std::chrono::steady_clock::now();
   for (int attempt = 0; attempt < 2 && h->loop_state == 0; attempt++) {
     t_pdl = attempt == 0;
-    int rc = capture_loop_graph(h, false, &h->loop64);
-    if (!rc && h->nt) rc = capture_loop_graph(h, true, &h->loop_tc);
+    const int rc = h->nt ? capture_loop_graph(h, true, &h->loop_tc)
+                         : capture_loop_graph(h, false, &h->loop64);
     if (!rc) {
       h->loop_state = 1;
+      h->loop_pdl = t_pdl;
     } else {
       if (h->loop64) cudaGraphExecDestroy(h->loop64);
       if (h->loop_tc) cudaGraphExecDestroy(h->loop_tc);
@@ -2250,6 +2562,7 @@ int ccdgpu_create(const ccdgpu_problem *prob, const ccdgpu_options *opt, ccdgpu_
 }
 
 void ccdgpu_release_cached_memory(void) {
+  destroy_retired_graphs(-1);
   release_cache(-1);
   release_stream_pool();
 }
@@ -2526,7 +2839,14 @@ int loop_launch(ccdgpu_handle *h, SolveState &st) {
   c.stop_at = c.iterations + kLoopChunk;
   CK(cudaMemcpyAsync(&h->ctl->stop_at, &c.stop_at, sizeof(int64_t), cudaMemcpyHostToDevice,
                      h->s0));
-  CK(cudaGraphLaunch(st.mixed && c.phase == 1 ? h->loop_tc : h->loop64, h->s0));
+  cudaGraphExec_t &g = st.mixed && c.phase == 1 ? h->loop_tc : h->loop64;
+  if (!g) {  // a mixed handle's FP64 loop, first needed now (the stream is idle here)
+    t_pdl = h->loop_pdl;
+    const int rc = capture_loop_graph(h, false, &g);
+    t_pdl = true;
+    if (rc) return rc;
+  }
+  CK(cudaGraphLaunch(g, h->s0));
   return CCDGPU_OK;
 }
 

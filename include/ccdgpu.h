@@ -183,7 +183,9 @@ int ccdgpu_create(const ccdgpu_problem *prob, const ccdgpu_options *opt, ccdgpu_
 void ccdgpu_destroy(ccdgpu_handle *h);
 /* Device memory of destroyed handles stays in a process-wide cache (at most 16 GiB) and is
  * reused by later handles on the same device, so that repeated create/destroy cycles do not
- * call cudaMalloc/cudaFree.  This returns the cached memory to the device. */
+ * call cudaMalloc/cudaFree; their CUDA graphs are torn down by the next create on the same
+ * device (at most 64 are held).  This returns the cached memory to the device and tears down
+ * the held graphs. */
 void ccdgpu_release_cached_memory(void);
 const char *ccdgpu_strerror(int status);
 
@@ -286,12 +288,14 @@ typedef struct ccdgpu_profile {
   int64_t launches;      /* kernels launched by this library since create */
   int64_t iterations;    /* iterations covered by the ms_* sums */
   /* Host wall time of ccdgpu_create by phase: [0] per-channel metadata and work lists on the
-   * host, [1] device allocation and uploads (enqueue), [2] device set-up kernels (tables, V,
-   * operand images) until they finish, [3] kernel attributes and ladder schedules, [4] the
-   * whole call. */
+   * host, [1] device allocation and uploads, [2] device set-up kernels (tables, V, operand
+   * images) from their launch until they finish, [3] kernel attributes, ladder schedules and
+   * the device-loop graph's capture, host work done while the set-up kernels run (so [3] is
+   * part of [2]), [4] the whole call. */
   double ms_create[5];
-  double ms_loop_graph;  /* host time of building the device solve loop's graphs (capture and
-                            instantiation, on the handle's first device-loop solve) */
+  double ms_loop_graph;  /* host time of building the device solve loop's graph (capture and
+                            instantiation; in ccdgpu_create, or on the first device-loop solve
+                            after a schedule change) */
 } ccdgpu_profile;
 int ccdgpu_get_profile(ccdgpu_handle *h, ccdgpu_profile *prof);
 /* When on, ccdgpu_solve runs the fused iteration without graph capture and brackets each
