@@ -74,9 +74,12 @@ __global__ void tile_v_tc_kernel(const ChanInfo *__restrict__ chans, const int2 
 struct ModelDev {
   int32_t kind, stride;
   const int32_t *qn;   // [n_sp * stride] quantum numbers (SPBasis::indexMap)
-  // Electron gas: direct Coulomb term by momentum transfer n_a - n_c in [-R, R]^3,
-  // vq[((dx + R) * W + dy + R) * W + dz + R], W = 2R + 1, built on the host with the reference's
-  // own expression (ElectronGasSPBasis.cpp:424-448), so generated elements are bit-identical.
+  // Electron gas: direct Coulomb term by momentum transfer d = n_a - n_c, d_i in [-R, R],
+  // stored by component magnitude: vq[(|dx| W + |dy|) W + |dz|], W = R + 1, built on the host
+  // with the reference's own expression (ElectronGasSPBasis.cpp:424-448), so generated elements
+  // are bit-identical.  The expression sees each component only through (2 pi d_i / L)^2, and
+  // a negated d_i gives the same bits, so the folded table (17.6 KB at R = 12, instead of
+  // 125 KB) stays in L1 beside the generators' random reads.
   const double *vq;
   int32_t R, W;
   double g;            // pairing strength
@@ -121,10 +124,10 @@ __device__ __forceinline__ double direct_pnm_dev(const int32_t *qi, const int32_
 __device__ __forceinline__ double eg_tbme_code(const ModelDev &m, uint32_t a, uint32_t b,
                                                uint32_t c, uint32_t d) {
   auto vq = [&](uint32_t x, uint32_t y) {
-    const int dx = (int)(x & 0xff) - (int)(y & 0xff);
-    const int dy = (int)((x >> 8) & 0xff) - (int)((y >> 8) & 0xff);
-    const int dz = (int)((x >> 16) & 0xff) - (int)((y >> 16) & 0xff);
-    return m.vq[((dx + m.R) * m.W + (dy + m.R)) * m.W + (dz + m.R)];
+    const int dx = abs((int)(x & 0xff) - (int)(y & 0xff));
+    const int dy = abs((int)((x >> 8) & 0xff) - (int)((y >> 8) & 0xff));
+    const int dz = abs((int)((x >> 16) & 0xff) - (int)((y >> 16) & 0xff));
+    return __ldg(m.vq + (dx * m.W + dy) * m.W + dz);
   };
   const uint32_t sa = a >> 24, sb = b >> 24, sc = c >> 24, sd = d >> 24;
   const double dir = (sa == sc && sb == sd) ? vq(a, c) : 0.;
@@ -146,7 +149,7 @@ __device__ __forceinline__ double tbme_dev(const ModelDev &m, int a, int b, int 
   }
   if (m.kind == CCDGPU_MODEL_ELECTRON_GAS) {  // direct - exchange, spin diagonal
     auto vq = [&](const int32_t *x, const int32_t *y) {
-      return m.vq[((x[0] - y[0] + m.R) * m.W + (x[1] - y[1] + m.R)) * m.W + (x[2] - y[2] + m.R)];
+      return __ldg(m.vq + (abs(x[0] - y[0]) * m.W + abs(x[1] - y[1])) * m.W + abs(x[2] - y[2]));
     };
     const double dir = (qa[3] == qc[3] && qb[3] == qd[3]) ? vq(qa, qc) : 0.;
     const double exc = (qa[3] == qd[3] && qb[3] == qc[3]) ? vq(qa, qd) : 0.;
@@ -298,6 +301,8 @@ __global__ void __launch_bounds__(256)
 gen_v_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restrict__ items,
                     const int32_t *__restrict__ rowmap, const int32_t *__restrict__ kcol,
                     const int2 *__restrict__ pp_pairs, ModelDev m, double *__restrict__ v_t) {
+  __shared__ uint2 s_ab[kMaxBM];  // electron gas: orbital codes of the chunk's rows (a, b)
+  __shared__ uint2 s_cd[kBK];     // ... and of its K columns (c, d)
   const int4 it = items[blockIdx.x];
   const ChanInfo ch = chans[it.x];
   const int mt = it.y, kc = it.z;
@@ -305,6 +310,20 @@ gen_v_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restrict__
   const bool kmajor = ladder_kmajor(ch.nb);
   double *out = v_t + ch.vkt_base + (int64_t)mt * ladder_arows_full(ch.nb) * ch.nkc * kBK +
                 (int64_t)kc * ar * kBK;
+  if (m.ocode) {  // the codes once per chunk, not once per element
+    for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+      const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + mt * ch.bm + r]];
+      s_ab[r] = make_uint2(m.ocode[ab.x], m.ocode[ab.y]);
+    }
+    for (int k = threadIdx.x; k < kBK; k += blockDim.x) {
+      const int w = kc * kBK + k;
+      if (w < ch.pk) {
+        const int2 cd = pp_pairs[ch.pp_off + kcol[ch.pk_off + w]];
+        s_cd[k] = make_uint2(m.ocode[cd.x], m.ocode[cd.y]);
+      }
+    }
+    __syncthreads();
+  }
   for (int e = threadIdx.x; e < ar * kBK; e += blockDim.x) {
     int r, k;
     if (kmajor) {
@@ -317,10 +336,13 @@ gen_v_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restrict__
     const int u = mt * ch.bm + r, w = kc * kBK + k;
     double v = 0.0;
     if (r < rows && w < ch.pk) {
-      const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + u]];
-      const int2 cd = pp_pairs[ch.pp_off + kcol[ch.pk_off + w]];
-      v = m.ocode ? eg_tbme_code(m, m.ocode[ab.x], m.ocode[ab.y], m.ocode[cd.x], m.ocode[cd.y])
-                  : tbme_dev(m, ab.x, ab.y, cd.x, cd.y);
+      if (m.ocode) {
+        v = eg_tbme_code(m, s_ab[r].x, s_ab[r].y, s_cd[k].x, s_cd[k].y);
+      } else {
+        const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + u]];
+        const int2 cd = pp_pairs[ch.pp_off + kcol[ch.pk_off + w]];
+        v = tbme_dev(m, ab.x, ab.y, cd.x, cd.y);
+      }
     }
     out[e] = v;
   }
@@ -331,11 +353,27 @@ gen_v_tc_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restric
                        const int32_t *__restrict__ rowmap, const int32_t *__restrict__ kcol,
                        const int2 *__restrict__ pp_pairs, ModelDev m,
                        __nv_bfloat16 *__restrict__ v_tc, int64_t tc_stride) {
+  __shared__ uint2 s_ab[kTcBM];  // electron gas: orbital codes of the chunk's rows (a, b)
+  __shared__ uint2 s_cd[kTcKC];  // ... and of its K columns (c, d)
   const int4 it = items[blockIdx.x];
   const ChanInfo ch = chans[it.x];
   const int mt = it.y, kc = it.z;
   const int rows = min(kTcBM, ch.pr - mt * kTcBM), rg = (rows + 7) >> 3;
   const int64_t base = ch.vtc_base + (int64_t)mt * kTcBM * ch.nkct * kTcKC + (int64_t)kc * rg * kTcGroup;
+  if (m.ocode) {  // the codes once per chunk, not once per element
+    for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+      const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + mt * kTcBM + r]];
+      s_ab[r] = make_uint2(m.ocode[ab.x], m.ocode[ab.y]);
+    }
+    for (int k = threadIdx.x; k < kTcKC; k += blockDim.x) {
+      const int w = kc * kTcKC + k;
+      if (w < ch.pk) {
+        const int2 cd = pp_pairs[ch.pp_off + kcol[ch.pk_off + w]];
+        s_cd[k] = make_uint2(m.ocode[cd.x], m.ocode[cd.y]);
+      }
+    }
+    __syncthreads();
+  }
   for (int e = threadIdx.x; e < rg * kTcGroup; e += blockDim.x) {
     // e = (r / 8) kTcGroup + (k / 8) 64 + (r % 8) 8 + k % 8 (tc_off)
     const int rem = e & (kTcGroup - 1);
@@ -343,10 +381,13 @@ gen_v_tc_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restric
     const int u = mt * kTcBM + r, w = kc * kTcKC + k;
     double v = 0.0;
     if (r < rows && w < ch.pk) {
-      const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + u]];
-      const int2 cd = pp_pairs[ch.pp_off + kcol[ch.pk_off + w]];
-      v = m.ocode ? eg_tbme_code(m, m.ocode[ab.x], m.ocode[ab.y], m.ocode[cd.x], m.ocode[cd.y])
-                  : tbme_dev(m, ab.x, ab.y, cd.x, cd.y);
+      if (m.ocode) {
+        v = eg_tbme_code(m, s_ab[r].x, s_ab[r].y, s_cd[k].x, s_cd[k].y);
+      } else {
+        const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + u]];
+        const int2 cd = pp_pairs[ch.pp_off + kcol[ch.pk_off + w]];
+        v = tbme_dev(m, ab.x, ab.y, cd.x, cd.y);
+      }
     }
     __nv_bfloat16 hv[NT];
     split_bf16_n<NT>(v, hv);

@@ -19,7 +19,6 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
-#include <thread>
 #include <new>
 #include <vector>
 
@@ -429,87 +428,13 @@ void release_stream_pool() {
   (void)cudaGetLastError();
 }
 
-// Graph executables of released handles, torn down later: by a helper thread of the next
-// create on the same device (beside its host work, while the device is idle), or by
-// ccdgpu_release_cached_memory, so that ccdgpu_destroy does not wait for their teardown
-// (about 0.3 ms each, longer while the device is busy).  At most kRetiredMax are held; beyond
-// that they are destroyed at once.
-constexpr size_t kRetiredMax = 64;
-
-struct RetiredGraphs {
-  std::mutex mu;
-  std::vector<std::pair<int, cudaGraphExec_t>> g;  // (device, executable)
-};
-
-RetiredGraphs &retired_graphs() {
-  static RetiredGraphs r;
-  return r;
-}
-
-void retire_graph(int dev, cudaGraphExec_t g) {
-  if (!g) return;
-  RetiredGraphs &R = retired_graphs();
-  {
-    std::lock_guard<std::mutex> lock(R.mu);
-    if (R.g.size() < kRetiredMax) {
-      R.g.push_back({dev, g});
-      return;
-    }
-  }
-  cudaGraphExecDestroy(g);
-}
-
-// Destroys the retired graphs of device dev (of every device for dev < 0).
-void destroy_retired_graphs(int dev) {
-  std::vector<std::pair<int, cudaGraphExec_t>> take;
-  {
-    RetiredGraphs &R = retired_graphs();
-    std::lock_guard<std::mutex> lock(R.mu);
-    std::vector<std::pair<int, cudaGraphExec_t>> keep;
-    for (const auto &x : R.g) (dev < 0 || x.first == dev ? take : keep).push_back(x);
-    R.g.swap(keep);
-  }
-  if (take.empty()) return;
-  int cur = -1;
-  if (dev < 0) cudaGetDevice(&cur);
-  for (const auto &x : take) {
-    if (dev < 0) cudaSetDevice(x.first);
-    cudaGraphExecDestroy(x.second);
-  }
-  if (cur >= 0) cudaSetDevice(cur);
-  (void)cudaGetLastError();
-}
-
-bool retired_graphs_pending(int dev) {
-  RetiredGraphs &R = retired_graphs();
-  std::lock_guard<std::mutex> lock(R.mu);
-  for (const auto &x : R.g)
-    if (x.first == dev) return true;
-  return false;
-}
-
-// Tears down device dev's retired graphs on a helper thread; the returned thread is joined by
-// the caller (or, if no thread could be started, the teardown has run on the calling thread).
-std::thread reap_retired_graphs(int dev) {
-  if (!retired_graphs_pending(dev)) return std::thread();
-  try {
-    return std::thread([dev] {
-      cudaSetDevice(dev);
-      destroy_retired_graphs(dev);
-    });
-  } catch (...) {
-    destroy_retired_graphs(dev);
-    return std::thread();
-  }
-}
-
 void release(ccdgpu_handle *h) {
   if (!h) return;
   // Cached blocks are handed to other handles: nothing of this one may still run on them.
   for (cudaStream_t st : {h->s0, h->s1, h->s2, h->s3})
     if (st) cudaStreamSynchronize(st);
   for (cudaGraphExec_t g : {h->graph, h->graph_tc, h->loop64, h->loop_tc})
-    retire_graph(h->opt.device, g);
+    if (g) cudaGraphExecDestroy(g);
   h->graph = h->graph_tc = h->loop64 = h->loop_tc = nullptr;
   for (auto &b : h->allocs) dev_free(b.p, b.bytes);
   h->allocs.clear();
@@ -1084,13 +1009,6 @@ void ready_loop_graphs(ccdgpu_handle *h);
 
 int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   const auto t_build = std::chrono::steady_clock::now();
-  // Earlier handles' graphs are torn down beside this create's host work; joined on return.
-  struct Joined {
-    std::thread t;
-    ~Joined() {
-      if (t.joinable()) t.join();
-    }
-  } reaper{reap_retired_graphs(h->opt.device)};
   const uint64_t nch = P->n_channels, nsp = P->n_sp, np = P->n_particles;
   h->nch = nch; h->nsp = nsp; h->np = np; h->npart = nsp - np;
   const ccdgpu_channel_dims *D = P->chan_dims, *MD = P->chan_mod_dims;
@@ -1733,12 +1651,12 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
       for (uint64_t o = 0; o < nsp; o++)
         for (int i = 0; i < 3; i++) nmax = std::max(nmax, std::abs(M->qn[o * M->qn_stride + i]));
       md.R = 2 * nmax;
-      md.W = 2 * md.R + 1;
+      md.W = md.R + 1;  // components of the transfer by magnitude (see ModelDev)
       const double L = M->params[0], e_sq = M->params[1];
       vq.assign((size_t)md.W * md.W * md.W, 0.0);
-      for (int dx = -md.R; dx <= md.R; dx++)
-        for (int dy = -md.R; dy <= md.R; dy++)
-          for (int dz = -md.R; dz <= md.R; dz++) {
+      for (int dx = 0; dx <= md.R; dx++)
+        for (int dy = 0; dy <= md.R; dy++)
+          for (int dz = 0; dz <= md.R; dz++) {
             const int d[3] = {dx, dy, dz};
             const double prefactor = e_sq / (L * L * L);
             double rel = 0.0, mu = 0.0;
@@ -1747,7 +1665,7 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
               rel += term * term;
             }
             const double v = rel < 1.e-5 ? 0.0 : prefactor * 4 * M_PI / (rel + mu * mu);
-            vq[((size_t)(dx + md.R) * md.W + (dy + md.R)) * md.W + (dz + md.R)] = v;
+            vq[((size_t)dx * md.W + dy) * md.W + dz] = v;
           }
       if (nmax <= 63) {
         ocode.resize(nsp);
@@ -2375,6 +2293,23 @@ int set_ctl(ccdgpu_handle *h, int active, double tol, int64_t max_iters, double 
   return CCDGPU_OK;
 }
 
+// The Control block of a new handle in one upload: what set_ctl(h, 0, 0.0, 100, 0.5, true)
+// and ccdgpu_trace_arm(h, -1) would write over the zeroed device copy.
+int init_ctl(ccdgpu_handle *h) {
+  Control &c = *h->h_ctl;
+  std::memset(&c, 0, sizeof(Control));
+  c.e_prev = 100.0;
+  c.e_diff = 1.0;
+  c.polish_rel = h->opt.polish_threshold;
+  c.max_iters = 100;
+  c.mixing = 0.5;
+  c.trace_iter = -1;
+  for (int k = 0; k < kTraceKernels; k++) c.trace_first[k] = ~0ull;
+  CK(cudaMemcpyAsync(h->ctl, h->h_ctl, sizeof(Control), cudaMemcpyHostToDevice, h->s0));
+  CK(cudaStreamSynchronize(h->s0));
+  return CCDGPU_OK;
+}
+
 int fused_ready_graph(ccdgpu_handle *h, bool mixed) {
   cudaGraphExec_t &exec = mixed ? h->graph_tc : h->graph;
   if (exec) return CCDGPU_OK;
@@ -2553,8 +2488,7 @@ int ccdgpu_create(const ccdgpu_problem *prob, const ccdgpu_options *opt, ccdgpu_
     h->ev_fork3 = h->sset.ev[14]; h->ev_join3 = h->sset.ev[15];
   }
   if (!rc) rc = build(h, prob);
-  if (!rc) rc = set_ctl(h, 0, 0.0, 100, 0.5, true);
-  if (!rc) rc = ccdgpu_trace_arm(h, -1);
+  if (!rc) rc = init_ctl(h);
   if (rc) { release(h); delete h; return rc; }
   h->create_ms[4] = ms_since(t_create);
   *out = h;
@@ -2562,7 +2496,6 @@ int ccdgpu_create(const ccdgpu_problem *prob, const ccdgpu_options *opt, ccdgpu_
 }
 
 void ccdgpu_release_cached_memory(void) {
-  destroy_retired_graphs(-1);
   release_cache(-1);
   release_stream_pool();
 }

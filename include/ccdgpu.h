@@ -183,9 +183,7 @@ int ccdgpu_create(const ccdgpu_problem *prob, const ccdgpu_options *opt, ccdgpu_
 void ccdgpu_destroy(ccdgpu_handle *h);
 /* Device memory of destroyed handles stays in a process-wide cache (at most 16 GiB) and is
  * reused by later handles on the same device, so that repeated create/destroy cycles do not
- * call cudaMalloc/cudaFree; their CUDA graphs are torn down by the next create on the same
- * device (at most 64 are held).  This returns the cached memory to the device and tears down
- * the held graphs. */
+ * call cudaMalloc/cudaFree.  This returns the cached memory to the device. */
 void ccdgpu_release_cached_memory(void);
 const char *ccdgpu_strerror(int status);
 

@@ -40,6 +40,20 @@ def test_on_the_fly_ladder_equals_stored(name):
             np.testing.assert_array_equal(a.t2(), b.t2())
 
 
+@pytest.mark.parametrize("name", ["eg14_s19", "eg54_s19"])
+def test_on_the_fly_tc_images_equal_stored(name):
+    """The tensor-core ladder's bf16 V images generated on the device equal the ones tiled from
+    uploaded V (the same doubles, split the same way): three mixed iterations agree bit for bit."""
+    g = golden(name)
+    with system_for(g) as s_stored, system_for(g, load_v_pppp=False) as s_gen:
+        with CCDSolver(s_stored, precision="mixed_bf16") as a, \
+                CCDSolver(s_gen, v_mode="on_the_fly", precision="mixed_bf16") as b:
+            for _ in range(3):
+                ea, eb = a.step(0.5), b.step(0.5)
+                assert ea == eb
+            np.testing.assert_array_equal(a.t2(), b.t2())
+
+
 def test_on_the_fly_mixed_precision():
     g = golden("eg54_s19")
     e_ref = float(g["energies"][-1])

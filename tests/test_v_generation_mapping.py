@@ -183,3 +183,32 @@ def test_ladder_v_generator_codes_reproduce_reference_v(name):
             assert np.max(np.abs(v - want)) <= 2e-7 * scale, c
             checked += 1
         assert checked > 10
+
+
+@pytest.mark.parametrize("name", ["eg14_s19", "eg54c36_r2", "eg54c36_r05"])
+def test_folded_momentum_table_is_exact(name):
+    """The device keeps the electron gas's direct term by momentum transfer d = n_a - n_c stored
+    by component magnitude (|dx|, |dy|, |dz|).  The reference's expression
+    (ElectronGasSPBasis.cpp:424-448) sees each component through (2 pi d_i / L)^2, and a
+    negated component gives the same bits, so every entry of the full range [-R, R]^3 equals
+    its folded one exactly."""
+    g = golden(name)
+    with system_for(g, load_v_pppp=False) as s:
+        qn = s.array("qn").reshape(s.n_sp, -1).astype(np.int64)
+        m = s.problem.contents.model.contents
+        L, e_sq = m.params[0], m.params[1]
+    R = 2 * int(np.abs(qn[:, :3]).max())
+    d = np.stack(np.meshgrid(*[np.arange(-R, R + 1)] * 3, indexing="ij"), -1).reshape(-1, 3)
+
+    def direct(dd):
+        prefactor = e_sq / (L * L * L)
+        rel = np.zeros(len(dd))
+        for i in range(3):
+            term = 2 * np.pi * dd[:, i] / L
+            rel = rel + term * term
+        with np.errstate(divide="ignore"):
+            val = prefactor * 4 * np.pi / (rel + 0.0 * 0.0)
+        return np.where(rel >= 1e-5, val, 0.0)
+
+    full, folded = direct(d), direct(np.abs(d))
+    assert np.array_equal(full.view(np.uint64), folded.view(np.uint64))
