@@ -294,9 +294,8 @@ __global__ void normal_order_kernel(ModelDev m, const double *__restrict__ bare,
 // V_pppp generated straight into the ladders' operand images, one CTA per image chunk, so that
 // each CTA writes one contiguous block (the chunk's elements in image order; padding rows and
 // K columns past pk get zeros).  FP64 ladder: items (channel, row tile, 16-deep K chunk), block
-// of ar x kBK doubles, k-major (mid and wide classes) or XOR-swizzled rows (thin class).
-// Tensor-core ladder: items (channel, 128-row tile, 32-deep K chunk), block of rg x kTcGroup
-// bf16 per term in 8 x 8 core matrices.
+// of ar x kBK doubles, k-major (mid and wide classes) or XOR-swizzled rows (thin class).  The
+// tensor-core images of mixed handles come with the FP64 tiles from gen_v_both_chunks_kernel.
 __global__ void __launch_bounds__(256)
 gen_v_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restrict__ items,
                     const int32_t *__restrict__ rowmap, const int32_t *__restrict__ kcol,
@@ -347,20 +346,30 @@ gen_v_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restrict__
     out[e] = v;
   }
 }
+
+// Mixed handles with generated V: both images from one evaluation of each element.  Items are
+// the tensor-core chunks (channel, 128-row tile, 32-deep K chunk); the FP64 ladder's row tiles
+// are also 128 rows (ladder_bm), so a chunk covers FP64 K chunks 2 kc and 2 kc + 1 of the same
+// rows.  The CTA evaluates its 128 x 32 elements once into shared memory (k-major, row stride
+// kGenLd; zero past the channel's rows and columns), four per thread at a time, then writes
+// the NT bf16 terms of each element in the tensor core's K-major core-matrix order (8 x 8
+// blocks, block of 8 rows by 32 K contiguous) and the FP64 chunks in the order of
+// gen_v_chunks_kernel (padding included).
+constexpr int kGenLd = kTcBM + 4;
 template <int NT>
 __global__ void __launch_bounds__(256)
-gen_v_tc_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restrict__ items,
-                       const int32_t *__restrict__ rowmap, const int32_t *__restrict__ kcol,
-                       const int2 *__restrict__ pp_pairs, ModelDev m,
-                       __nv_bfloat16 *__restrict__ v_tc, int64_t tc_stride) {
-  __shared__ uint2 s_ab[kTcBM];  // electron gas: orbital codes of the chunk's rows (a, b)
-  __shared__ uint2 s_cd[kTcKC];  // ... and of its K columns (c, d)
+gen_v_both_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restrict__ items,
+                         const int32_t *__restrict__ rowmap, const int32_t *__restrict__ kcol,
+                         const int2 *__restrict__ pp_pairs, ModelDev m, double *__restrict__ v_t,
+                         __nv_bfloat16 *__restrict__ v_tc, int64_t tc_stride) {
+  __shared__ uint2 s_ab[kTcBM];
+  __shared__ uint2 s_cd[kTcKC];
+  __shared__ double tile[kTcKC * kGenLd];  // tile[k * kGenLd + r]
   const int4 it = items[blockIdx.x];
   const ChanInfo ch = chans[it.x];
   const int mt = it.y, kc = it.z;
   const int rows = min(kTcBM, ch.pr - mt * kTcBM), rg = (rows + 7) >> 3;
-  const int64_t base = ch.vtc_base + (int64_t)mt * kTcBM * ch.nkct * kTcKC + (int64_t)kc * rg * kTcGroup;
-  if (m.ocode) {  // the codes once per chunk, not once per element
+  if (m.ocode) {
     for (int r = threadIdx.x; r < rows; r += blockDim.x) {
       const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + mt * kTcBM + r]];
       s_ab[r] = make_uint2(m.ocode[ab.x], m.ocode[ab.y]);
@@ -374,25 +383,62 @@ gen_v_tc_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restric
     }
     __syncthreads();
   }
-  for (int e = threadIdx.x; e < rg * kTcGroup; e += blockDim.x) {
-    // e = (r / 8) kTcGroup + (k / 8) 64 + (r % 8) 8 + k % 8 (tc_off)
-    const int rem = e & (kTcGroup - 1);
-    const int r = (e / kTcGroup) * 8 + ((rem >> 3) & 7), k = (rem >> 6) * 8 + (rem & 7);
-    const int u = mt * kTcBM + r, w = kc * kTcKC + k;
-    double v = 0.0;
-    if (r < rows && w < ch.pk) {
-      if (m.ocode) {
-        v = eg_tbme_code(m, s_ab[r].x, s_ab[r].y, s_cd[k].x, s_cd[k].y);
-      } else {
-        const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + u]];
-        const int2 cd = pp_pairs[ch.pp_off + kcol[ch.pk_off + w]];
-        v = tbme_dev(m, ab.x, ab.y, cd.x, cd.y);
+  // Evaluate: element e -> (r = e % 128, k = e / 128), 4096 per chunk, 16 per thread.
+  constexpr int kPer = kTcBM * kTcKC / 256;
+  for (int j0 = 0; j0 < kPer; j0 += 4) {
+    double v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = (j0 + q) * 256 + threadIdx.x;
+      const int r = e & (kTcBM - 1), k = e >> 7;
+      const int w = kc * kTcKC + k;
+      v[q] = 0.0;
+      if (r < rows && w < ch.pk) {
+        if (m.ocode) {
+          v[q] = eg_tbme_code(m, s_ab[r].x, s_ab[r].y, s_cd[k].x, s_cd[k].y);
+        } else {
+          const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + mt * kTcBM + r]];
+          const int2 cd = pp_pairs[ch.pp_off + kcol[ch.pk_off + w]];
+          v[q] = tbme_dev(m, ab.x, ab.y, cd.x, cd.y);
+        }
       }
     }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = (j0 + q) * 256 + threadIdx.x;
+      tile[(e >> 7) * kGenLd + (e & (kTcBM - 1))] = v[q];
+    }
+  }
+  __syncthreads();
+  // bf16 terms: e = (r / 8) kTcGroup + (k / 8) 64 + (r % 8) 8 + k % 8 (tc_off).
+  const int64_t base = ch.vtc_base + (int64_t)mt * kTcBM * ch.nkct * kTcKC + (int64_t)kc * rg * kTcGroup;
+  for (int e = threadIdx.x; e < rg * kTcGroup; e += blockDim.x) {
+    const int rem = e & (kTcGroup - 1);
+    const int r = (e / kTcGroup) * 8 + ((rem >> 3) & 7), k = (rem >> 6) * 8 + (rem & 7);
     __nv_bfloat16 hv[NT];
-    split_bf16_n<NT>(v, hv);
+    split_bf16_n<NT>(tile[k * kGenLd + r], hv);
 #pragma unroll
     for (int p = 0; p < NT; ++p) v_tc[p * tc_stride + base + e] = hv[p];
+  }
+  // FP64 chunks 2 kc and 2 kc + 1, as gen_v_chunks_kernel (rows past `rows` are zero).
+  const int ar = ladder_arows(ch.nb, rows);
+  const bool kmajor = ladder_kmajor(ch.nb);
+  for (int h = 0; h < 2; ++h) {
+    const int kc64 = 2 * kc + h;
+    if (kc64 >= ch.nkc) break;
+    double *out = v_t + ch.vkt_base + (int64_t)mt * ladder_arows_full(ch.nb) * ch.nkc * kBK +
+                  (int64_t)kc64 * ar * kBK;
+    for (int e = threadIdx.x; e < ar * kBK; e += blockDim.x) {
+      int r, k;
+      if (kmajor) {
+        k = e / ar;
+        r = e - k * ar;
+      } else {
+        r = e >> 4;
+        k = (e & 15) ^ (r & 15);  // swzA(r, k) = 16 r + (k ^ (r & 15))
+      }
+      out[e] = r < rows ? tile[(h * kBK + k) * kGenLd + r] : 0.0;
+    }
   }
 }
 

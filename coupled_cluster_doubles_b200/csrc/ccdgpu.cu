@@ -1529,11 +1529,12 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   gv_items.clear();
   gvt_items.clear();
   if (on_the_fly) {
+    // With bf16 images both images come from the tensor-core chunks (gen_v_both_chunks_kernel).
     const bool tc_images = h->nt && !h->tc_gen;
     std::vector<int64_t> go(h->n_act + 1, 0), gto(h->n_act + 1, 0);
     for (int ai = 0; ai < h->n_act; ai++) {
       const ChanInfo &a = chans[ai];
-      go[ai + 1] = go[ai] + (int64_t)a.nmt * a.nkc;
+      go[ai + 1] = go[ai] + (tc_images ? 0 : (int64_t)a.nmt * a.nkc);
       gto[ai + 1] = gto[ai] + (tc_images ? (int64_t)ceil_div(a.pr, kTcBM) * a.nkct : 0);
     }
     gv_items.resize(go[h->n_act]);
@@ -1542,8 +1543,9 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
     for (int ai = 0; ai < h->n_act; ai++) {
       const ChanInfo &a = chans[ai];
       int4 *g = gv_items.data() + go[ai];
-      for (int mt = 0; mt < a.nmt; mt++)
-        for (int kc = 0; kc < a.nkc; kc++) *g++ = make_int4(ai, mt, kc, 0);
+      if (!tc_images)
+        for (int mt = 0; mt < a.nmt; mt++)
+          for (int kc = 0; kc < a.nkc; kc++) *g++ = make_int4(ai, mt, kc, 0);
       int4 *gt = gvt_items.data() + gto[ai];
       if (tc_images)
         for (int mt = 0; mt < (int)ceil_div(a.pr, kTcBM); mt++)
@@ -1860,17 +1862,17 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   if (a_row_off[n_act] > 0) {
     if (on_the_fly) {
       // FP64 tiles, and the bf16 images unless the tensor-core ladder generates its own V: one
-      // CTA per image chunk.
+      // CTA per image chunk; with bf16 images, one CTA per tensor-core chunk writes both.
       if (!gv_items.empty()) {
         gen_v_chunks_kernel<<<(unsigned)gv_items.size(), 256, 0, h->s0>>>(
             h->chans, d_gv_items, h->rowmap, h->kcol, h->pp_pairs, md, h->v_t);
         CK(cudaGetLastError());
       }
       if (h->nt && !h->tc_gen && !gvt_items.empty()) {
-        auto kern = h->nt == 3 ? gen_v_tc_chunks_kernel<3> : gen_v_tc_chunks_kernel<2>;
+        auto kern = h->nt == 3 ? gen_v_both_chunks_kernel<3> : gen_v_both_chunks_kernel<2>;
         kern<<<(unsigned)gvt_items.size(), 256, 0, h->s0>>>(h->chans, d_gvt_items, h->rowmap,
-                                                           h->kcol, h->pp_pairs, md, h->v_tc,
-                                                           h->n_vtc);
+                                                           h->kcol, h->pp_pairs, md, h->v_t,
+                                                           h->v_tc, h->n_vtc);
       }
     } else {
       tile_v_kernel<<<(unsigned)vrows.size(), 128, 0, h->s0>>>(h->chans, d_vrows, h->rowmap,
