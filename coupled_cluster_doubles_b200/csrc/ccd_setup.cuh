@@ -296,6 +296,7 @@ __global__ void normal_order_kernel(ModelDev m, const double *__restrict__ bare,
 // K columns past pk get zeros).  FP64 ladder: items (channel, row tile, 16-deep K chunk), block
 // of ar x kBK doubles, k-major (mid and wide classes) or XOR-swizzled rows (thin class).  The
 // tensor-core images of mixed handles come with the FP64 tiles from gen_v_both_chunks_kernel.
+template <bool EG>  // EG: the electron gas's orbital-code path only (fewer registers)
 __global__ void __launch_bounds__(256)
 gen_v_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restrict__ items,
                     const int32_t *__restrict__ rowmap, const int32_t *__restrict__ kcol,
@@ -309,7 +310,7 @@ gen_v_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restrict__
   const bool kmajor = ladder_kmajor(ch.nb);
   double *out = v_t + ch.vkt_base + (int64_t)mt * ladder_arows_full(ch.nb) * ch.nkc * kBK +
                 (int64_t)kc * ar * kBK;
-  if (m.ocode) {  // the codes once per chunk, not once per element
+  if (EG) {  // the codes once per chunk, not once per element
     for (int r = threadIdx.x; r < rows; r += blockDim.x) {
       const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + mt * ch.bm + r]];
       s_ab[r] = make_uint2(m.ocode[ab.x], m.ocode[ab.y]);
@@ -335,7 +336,7 @@ gen_v_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restrict__
     const int u = mt * ch.bm + r, w = kc * kBK + k;
     double v = 0.0;
     if (r < rows && w < ch.pk) {
-      if (m.ocode) {
+      if constexpr (EG) {
         v = eg_tbme_code(m, s_ab[r].x, s_ab[r].y, s_cd[k].x, s_cd[k].y);
       } else {
         const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + u]];
@@ -355,8 +356,10 @@ gen_v_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restrict__
 // the NT bf16 terms of each element in the tensor core's K-major core-matrix order (8 x 8
 // blocks, block of 8 rows by 32 K contiguous) and the FP64 chunks in the order of
 // gen_v_chunks_kernel (padding included).
+// EG: the electron gas's orbital-code path only (m.ocode set), without the other models' element
+// code, so the instantiation needs fewer registers and more CTAs share an SM.
 constexpr int kGenLd = kTcBM + 4;
-template <int NT>
+template <int NT, bool EG>
 __global__ void __launch_bounds__(256)
 gen_v_both_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restrict__ items,
                          const int32_t *__restrict__ rowmap, const int32_t *__restrict__ kcol,
@@ -369,7 +372,7 @@ gen_v_both_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restr
   const ChanInfo ch = chans[it.x];
   const int mt = it.y, kc = it.z;
   const int rows = min(kTcBM, ch.pr - mt * kTcBM), rg = (rows + 7) >> 3;
-  if (m.ocode) {
+  if (EG) {
     for (int r = threadIdx.x; r < rows; r += blockDim.x) {
       const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + mt * kTcBM + r]];
       s_ab[r] = make_uint2(m.ocode[ab.x], m.ocode[ab.y]);
@@ -394,7 +397,7 @@ gen_v_both_chunks_kernel(const ChanInfo *__restrict__ chans, const int4 *__restr
       const int w = kc * kTcKC + k;
       v[q] = 0.0;
       if (r < rows && w < ch.pk) {
-        if (m.ocode) {
+        if constexpr (EG) {
           v[q] = eg_tbme_code(m, s_ab[r].x, s_ab[r].y, s_cd[k].x, s_cd[k].y);
         } else {
           const int2 ab = pp_pairs[ch.pp_off + rowmap[ch.row_off + mt * kTcBM + r]];

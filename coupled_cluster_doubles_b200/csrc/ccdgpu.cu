@@ -1209,11 +1209,34 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   h->n_hh_red = (int)hh_red.size();
   // Channels with hh <= 16 first (their own launch), then the rest; largest units
   // (rows x hh^2) first within each, so the short ones fill in behind them.
-  std::stable_sort(hh_tiles.begin(), hh_tiles.end(), [&](const HHTile &x, const HHTile &y) {
-    const ChanInfo &a = chans[x.ch], &b = chans[y.ch];
-    if ((a.hh > 16) != (b.hh > 16)) return a.hh <= 16;
-    return (int64_t)x.rows * a.hh * a.hh > (int64_t)y.rows * b.hh * b.hh;
-  });
+  // A stable sort by (class, -cost): the units come channel by channel as runs of equal cost
+  // (the full slices, then a shorter last one), so the runs are stably sorted and expanded,
+  // which gives the same order as sorting the units themselves.
+  {
+    struct Run {
+      int32_t first, n;
+      bool wide;
+      int64_t cost;
+    };
+    std::vector<Run> runs;
+    for (int32_t i = 0; i < (int32_t)hh_tiles.size(); i++) {
+      const HHTile &t = hh_tiles[i];
+      const int64_t hh = chans[t.ch].hh, cost = (int64_t)t.rows * hh * hh;
+      if (!runs.empty() && hh_tiles[runs.back().first].ch == t.ch && runs.back().cost == cost)
+        runs.back().n++;
+      else
+        runs.push_back(Run{i, 1, hh > 16, cost});
+    }
+    std::stable_sort(runs.begin(), runs.end(), [](const Run &x, const Run &y) {
+      if (x.wide != y.wide) return !x.wide;
+      return x.cost > y.cost;
+    });
+    std::vector<HHTile> sorted;
+    sorted.reserve(hh_tiles.size());
+    for (const Run &r : runs)
+      sorted.insert(sorted.end(), hh_tiles.begin() + r.first, hh_tiles.begin() + r.first + r.n);
+    hh_tiles.swap(sorted);
+  }
   for (const HHTile &t : hh_tiles) h->n_hh_small += chans[t.ch].hh <= 16 ? 1 : 0;
   for (const ChanInfo &a : chans)
     if (a.hh > 16) h->hh_slice_smem = std::max(h->hh_slice_smem, hh_slice_smem(a.hh));
@@ -1864,12 +1887,16 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
       // FP64 tiles, and the bf16 images unless the tensor-core ladder generates its own V: one
       // CTA per image chunk; with bf16 images, one CTA per tensor-core chunk writes both.
       if (!gv_items.empty()) {
-        gen_v_chunks_kernel<<<(unsigned)gv_items.size(), 256, 0, h->s0>>>(
+        auto kern64 = md.ocode ? gen_v_chunks_kernel<true> : gen_v_chunks_kernel<false>;
+        kern64<<<(unsigned)gv_items.size(), 256, 0, h->s0>>>(
             h->chans, d_gv_items, h->rowmap, h->kcol, h->pp_pairs, md, h->v_t);
         CK(cudaGetLastError());
       }
       if (h->nt && !h->tc_gen && !gvt_items.empty()) {
-        auto kern = h->nt == 3 ? gen_v_both_chunks_kernel<3> : gen_v_both_chunks_kernel<2>;
+        auto kern = md.ocode ? (h->nt == 3 ? gen_v_both_chunks_kernel<3, true>
+                                           : gen_v_both_chunks_kernel<2, true>)
+                             : (h->nt == 3 ? gen_v_both_chunks_kernel<3, false>
+                                           : gen_v_both_chunks_kernel<2, false>);
         kern<<<(unsigned)gvt_items.size(), 256, 0, h->s0>>>(h->chans, d_gvt_items, h->rowmap,
                                                            h->kcol, h->pp_pairs, md, h->v_t,
                                                            h->v_tc, h->n_vtc);
