@@ -767,24 +767,30 @@ int upload_runs(ccdgpu_handle *h, T *dst, const std::vector<const T *> &src,
 template <class Cost>
 void lpt_group(std::vector<LadderTile> &tiles, size_t lo, size_t hi, int G, Cost cost,
                std::vector<int32_t> &off) {
-  std::stable_sort(tiles.begin() + lo, tiles.begin() + hi,
-                   [&](const LadderTile &x, const LadderTile &y) { return cost(x) > cost(y); });
-  std::vector<std::vector<LadderTile>> per(G);
+  // Costs once; (-cost, position) pairs sorted ascending give the order of a stable sort by
+  // decreasing cost.
+  const size_t n = hi - lo;
+  std::vector<std::pair<int64_t, int32_t>> order(n);
+  for (size_t i = 0; i < n; i++) order[i] = {-cost(tiles[lo + i]), (int32_t)i};
+  std::sort(order.begin(), order.end());
   std::priority_queue<std::pair<int64_t, int>, std::vector<std::pair<int64_t, int>>,
                       std::greater<std::pair<int64_t, int>>> load;
   for (int b = 0; b < G; b++) load.push({0, b});
-  for (size_t i = lo; i < hi; i++) {
+  std::vector<int32_t> owner(n), count(G + 1, 0);
+  for (size_t i = 0; i < n; i++) {
     auto [w, b] = load.top();
     load.pop();
-    per[b].push_back(tiles[i]);
-    load.push({w + cost(tiles[i]), b});
+    owner[i] = b;
+    count[b + 1]++;
+    load.push({w - order[i].first, b});
   }
-  size_t pos = lo;
-  off.push_back((int32_t)pos);
-  for (int b = 0; b < G; b++) {
-    for (const LadderTile &t : per[b]) tiles[pos++] = t;
-    off.push_back((int32_t)pos);
-  }
+  // Each CTA's tiles in the order they were assigned, CTA after CTA.
+  for (int b = 0; b < G; b++) count[b + 1] += count[b];
+  std::vector<LadderTile> placed(n);
+  std::vector<int32_t> next(count.begin(), count.end() - 1);
+  for (size_t i = 0; i < n; i++) placed[next[owner[i]]++] = tiles[lo + order[i].second];
+  std::copy(placed.begin(), placed.end(), tiles.begin() + lo);
+  for (int b = 0; b <= G; b++) off.push_back((int32_t)(lo + count[b]));
 }
 
 int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
@@ -832,9 +838,14 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
   // Thin channels first, then mid and wide ones; each class runs on persistent CTAs (3, 2 and
   // 1 per SM) with a balanced (LPT) assignment.  Cost = bytes per 16-deep chunk x chunks, plus
   // two chunks' worth for the pipeline fill and the epilogue.
-  std::stable_sort(tiles.begin(), tiles.end(), [&](const LadderTile &x, const LadderTile &y) {
-    return cls_of(x.nb) < cls_of(y.nb);
-  });
+  {  // stable by class: three passes
+    std::vector<LadderTile> by_cls;
+    by_cls.reserve(tiles.size());
+    for (int k = 0; k < 3; k++)
+      for (const LadderTile &t : tiles)
+        if (cls_of(t.nb) == k) by_cls.push_back(t);
+    tiles.swap(by_cls);
+  }
   std::vector<int32_t> fp_cta_off;
   {
     auto fp_cost = [](const LadderTile &x) {
@@ -889,8 +900,13 @@ int make_ladder_tiles(ccdgpu_handle *h, const ccdgpu_schedule &sch) {
     auto tc_cost = [](const LadderTile &x) {
       return (int64_t)(x.nks + x.nkh + 2) * (((x.rows + 7) & ~7) + x.nb);
     };
-    std::stable_sort(tc_tiles.begin(), tc_tiles.end(),
-                     [&](const LadderTile &x, const LadderTile &y) { return tc_cost(x) > tc_cost(y); });
+    // (-cost, position) pairs sorted ascending: the order of a stable sort by decreasing cost.
+    std::vector<std::pair<int64_t, int32_t>> ord(tc_tiles.size());
+    for (size_t i = 0; i < tc_tiles.size(); i++) ord[i] = {-tc_cost(tc_tiles[i]), (int32_t)i};
+    std::sort(ord.begin(), ord.end());
+    std::vector<LadderTile> sorted(tc_tiles.size());
+    for (size_t i = 0; i < ord.size(); i++) sorted[i] = tc_tiles[ord[i].second];
+    tc_tiles.swap(sorted);
   }
   // Reduction items of split row blocks.
   auto red_items = [](const std::vector<LadderTile> &tl, std::vector<RedItem> &out, int *per_cls,
