@@ -447,23 +447,31 @@ void release(ccdgpu_handle *h) {
   else destroy_set(h->sset);
 }
 
-// Bump allocator over one device allocation (256-byte aligned pieces).
+// Bump allocator over one device allocation (256-byte aligned pieces), zero-filled on s0 at
+// commit, except the pieces added with add_unset, which follow the others and which the
+// caller writes in full before anything reads them.
 struct Arena {
-  size_t used = 0;
-  std::vector<std::pair<void **, size_t>> reqs;
+  size_t used = 0, unset = 0;
+  std::vector<std::pair<void **, size_t>> reqs, unset_reqs;
+  static size_t piece(size_t bytes) { return (std::max<size_t>(bytes, 1) + 255) & ~size_t(255); }
   template <typename T>
   void add(T **p, size_t count) {
-    size_t bytes = (std::max<size_t>(count, 1) * sizeof(T) + 255) & ~size_t(255);
     reqs.push_back({reinterpret_cast<void **>(p), used});
-    used += bytes;
+    used += piece(count * sizeof(T));
+  }
+  template <typename T>
+  void add_unset(T **p, size_t count) {
+    unset_reqs.push_back({reinterpret_cast<void **>(p), unset});
+    unset += piece(count * sizeof(T));
   }
   int commit(ccdgpu_handle *h) {
     void *base = nullptr;
     size_t got = 0;
-    CK(dev_alloc(used, &base, &got));
+    CK(dev_alloc(used + unset, &base, &got));
     h->allocs.push_back({base, got});
     CK(cudaMemsetAsync(base, 0, used, h->s0));
     for (auto &r : reqs) *r.first = static_cast<char *>(base) + r.second;
+    for (auto &r : unset_reqs) *r.first = static_cast<char *>(base) + used + r.second;
     return CCDGPU_OK;
   }
 };
@@ -1520,7 +1528,10 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
   ar.add(&h->part, part_tot);
 
   ar.add(&h->eps, nsp);
-  ar.add(&h->v_pphh, n_t); ar.add(&h->v_hhhh, x_tot); ar.add(&h->v_t, vt);
+  // Generated V images are written in full (padding included) by the V generators.
+  ar.add(&h->v_pphh, n_t); ar.add(&h->v_hhhh, x_tot);
+  if (on_the_fly) ar.add_unset(&h->v_t, vt);
+  else ar.add(&h->v_t, vt);
   ar.add(&h->v_hpph, h->n_m); ar.add(&h->v_hphp, y_tot);
   ar.add(&h->flat, (size_t)8 * n_t); ar.add(&h->inv4, n_t); ar.add(&h->d_ring, n_t); ar.add(&h->o_h, o_h.size()); ar.add(&h->o_p, o_p.size());
   ar.add(&h->t[0], n_t); ar.add(&h->t[1], n_t); ar.add(&h->dmat, n_t);
@@ -1540,6 +1551,8 @@ int build(ccdgpu_handle *h, const ccdgpu_problem *P) {
       h->n_vtc = 0;  // V planes generated in the ladder
       ar.add(&h->vg_rows, vg_rows.size()); ar.add(&h->vg_cols, vg_cols.size());
       ar.add(&h->vg_tab, vg_tab.size());
+    } else if (on_the_fly) {
+      ar.add_unset(&h->v_tc, (size_t)h->nt * h->n_vtc);
     } else {
       ar.add(&h->v_tc, (size_t)h->nt * h->n_vtc);
     }
