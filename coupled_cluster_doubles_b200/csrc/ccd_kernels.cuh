@@ -207,9 +207,19 @@ ladder_reduce_kernel(const RedItem *__restrict__ items, const LadderTile *__rest
   for (int e = threadIdx.x; e < n; e += blockDim.x) {
     const int u_local = it.r0 + e / tile.nb, col = e % tile.nb;
     if (col >= tile.hh) continue;
+    // Eight segments' loads in flight together, then added in segment order.
+    const double *pc = part + tile.part_base + (int64_t)u_local * tile.nb + col;
+    const int64_t seg_stride = (int64_t)tile.bm * tile.nb;
     double v = 0.0;
-    for (int sg = 0; sg < tile.nseg; ++sg)
-      v += part[tile.part_base + ((int64_t)sg * tile.bm + u_local) * tile.nb + col];
+    int sg = 0;
+    for (; sg + 8 <= tile.nseg; sg += 8) {
+      double x[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) x[k] = pc[(int64_t)(sg + k) * seg_stride];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v += x[k];
+    }
+    for (; sg < tile.nseg; ++sg) v += pc[(int64_t)sg * seg_stride];
     const int u = tile.mt * tile.bm + u_local;
     const int ab = rowmap[tile.row_off + u], mir = mirror[tile.row_off + u];
     d[tile.t_off + (int64_t)ab * tile.hh + col] = v;
@@ -710,6 +720,15 @@ hh_reduce_kernel(const HHRed *__restrict__ items, const ChanInfo *__restrict__ c
   // flight together), combined in a fixed order.
   double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   int sl = 0;
+  // Sixteen slices' loads in flight together, then added to the same partial sums in the same
+  // order as the eight-slice rounds below.
+  for (; sl + 16 <= ch.nhht; sl += 16) {
+    double x[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) x[k] = __ldcg(pb + (int64_t)(sl + k) * nout);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) acc[k & 7] += x[k];
+  }
   for (; sl + 8 <= ch.nhht; sl += 8) {
 #pragma unroll
     for (int k = 0; k < 8; ++k) acc[k] += __ldcg(pb + (int64_t)(sl + k) * nout);
