@@ -1095,18 +1095,18 @@ __global__ void onebody_fused_kernel(int np, int nsp, const int64_t *__restrict_
   const bool hole = w < np;
   const double *src = hole ? s : r;
   // Eight lane-strided partial sums: the eight index loads of a round are issued together,
-  // then the eight value loads, so a round costs two memory latencies.
+  // then the eight value loads, so a round costs two memory latencies; the last round of a
+  // list is guarded (lists are mostly shorter than one round).
   double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   const int64_t hi = list_off[w + 1];
-  int64_t e = list_off[w] + lane;
-  for (; e + 224 < hi; e += 256) {
+  for (int64_t e = list_off[w] + lane; e < hi; e += 256) {
     int32_t ix[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) ix[k] = __ldg(list + e + 32 * k);
+    for (int k = 0; k < 8; ++k) ix[k] = e + 32 * k < hi ? __ldg(list + e + 32 * k) : -1;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) acc[k] += __ldcg(src + ix[k]);
+    for (int k = 0; k < 8; ++k)
+      if (ix[k] >= 0) acc[k] += __ldcg(src + ix[k]);
   }
-  for (; e < hi; e += 32) acc[0] += __ldcg(src + __ldg(list + e));
   double v = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
