@@ -622,7 +622,7 @@ __host__ __device__ inline int hh_slice_ld(int hh) { return ((hh + 15) & ~15) + 
 __host__ __device__ inline size_t hh_slice_smem(int hh) {
   return (size_t)2 * kHHRowsL * hh_slice_ld(hh) * sizeof(double);
 }
-__global__ void __launch_bounds__(kHHSliceThreads, 2)
+__global__ void __launch_bounds__(kHHSliceThreads, 3)
 hh_slice_kernel(const HHTile *__restrict__ tiles, const ChanInfo *__restrict__ chans,
                 const double *__restrict__ v_pphh, const double *tbuf0, const double *tbuf1,
                 double *__restrict__ part, double *__restrict__ r_out, const Control *ctl,
